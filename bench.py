@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark of the SharpClaw WENO step on B200 (one JSON line on rank 0).
+
+Workload (the configuration the headline metric is quoted on): 1-D Euler,
+gamma = 1.4, Shu-Osher shock/entropy-wave data on [-5,5] with extrapolation
+bc, mx = 2^20 cells, Roe solver with Harten-Hyman entropy fix
+(apps/euler/shockentropy/rp1eu.f), characteristic-wise WENO5 with Roe
+eigenvectors, tfluct_solver = 0 (swap + second Riemann solve), SSPRK(10,4),
+cfl_desired 2.45 / cfl_max 2.5, variable dt.  Synthetic data of exactly that
+recipe (no dataset is involved).
+
+One benchmark step = one sharpclaw() call advancing the grid by 10 time
+steps (100 fused stage launches + 20 controller launches), i.e.
+2^20 * 10 * 10 cell-stage updates.
+
+  value    device-resident throughput of the headline form (FP32
+           reconstruction/Riemann on FP64 state, `--precision mixed`),
+           CUDA events on the library stream, L2 flushed between steps
+  fp64     the plain FP64 path on the same workload, same timing
+  e2e      the public C ABI with host buffers: H2D of q from pinned memory,
+           sharpclaw(), D2H of q, every step, host wall clock
+  roofline the fused stage kernel against the measured HBM copy bandwidth
+  cpu_baseline  the C oracle (a restatement of the reference Fortran, which
+           cannot be compiled here: no Fortran compiler) on a bounded sample
+
+`--impl reference` times that CPU restatement alone, on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-stage updates/s on 1 B200, FP32+batched vs plain FP64 at stated L1 err; %HBM"
+UNIT = "cell-stage/s"
+MX = 1 << 20
+NSTEP = 10          # time steps per benchmark step
+NSTAGES = 10        # SSPRK(10,4)
+CFL_MAX, CFL_DESIRED = 2.5, 2.45
+DT0 = 4.5e-6        # below 2.45*dx/max(|u|+c) of the Shu-Osher data: no rejected first step
+GAMMA = 1.4
+WORKLOAD = ("1-D Euler Shu-Osher, mx=2^20, Roe+entropy fix, char-wise WENO5, tfluct_solver=0, "
+            "SSPRK(10,4), cfl 2.45/2.5, variable dt, extrapolation bc")
+
+
+def shu_osher(mx):
+    import numpy as np
+    xlower, xupper = -5.0, 5.0
+    dx = (xupper - xlower) / mx
+    xc = xlower + (np.arange(1, mx + 1) - 0.5) * dx
+    g1 = GAMMA - 1.0
+    rhol, ul, pl = 3.857143, 2.629369, 10.333333
+    q = np.zeros((3, mx + 6))
+    left = xc < -4.0
+    q[0, 3:-3] = np.where(left, rhol, 1.0 + 0.2 * np.sin(5.0 * xc))
+    q[1, 3:-3] = np.where(left, rhol * ul, 0.0)
+    q[2, 3:-3] = np.where(left, pl / g1 + 0.5 * rhol * ul ** 2, 1.0 / g1)
+    return q, dx
+
+
+def config(extra=None):
+    c = {"workload": WORKLOAD, "mx": MX, "time_steps_per_step": NSTEP, "stages_per_time_step": NSTAGES,
+         "cells_x_stages_per_step": MX * NSTEP * NSTAGES,
+         "l2": "flushed (256 MiB write) between timed steps; the 4 state registers (~100 MB) "
+               "stay L2-resident within a step",
+         "parallelism": "replicas (one independent grid per GPU)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# --------------------------------------------------------------------------
+# CPU restatement (oracle) timing: used for cpu_baseline and --impl reference
+# --------------------------------------------------------------------------
+def _oracle_one(args):
+    mx, nsteps = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    q, dx = shu_osher(mx)
+    p = O.make_params(mx=mx, meqn=3, mwaves=3, dx=dx, xlower=-5.0, rp=O.RP_EULER, gamma=GAMMA,
+                      mthbc=(1, 1), char_decomp=2, tfluct_solver=0)
+    t0 = time.perf_counter()
+    qq, res = O.sharpclaw(p, q, None, tstart=0.0, tend=1e30, dt_initial=DT0, cfl_max=CFL_MAX,
+                          cfl_desired=CFL_DESIRED, max_steps=nsteps, time_integrator=4)
+    dt = time.perf_counter() - t0
+    return mx * NSTAGES * res.steps_taken, dt
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# --------------------------------------------------------------------------
+# clocks sampler (nvidia-smi during the timed region)
+# --------------------------------------------------------------------------
+class Clocks:
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        import statistics
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if len(s) > 3 + k and s[3 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    """--impl reference: the CPU restatement on all host cores (rank 0 only)."""
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    cores = cpu_cores()
+    sample_mx = 1 << 17
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        pool.map(_oracle_one, [(1024, 1)] * cores)  # import + warm the workers
+        for _ in range(args.warmup):
+            pool.map(_oracle_one, [(sample_mx, 1)] * cores)
+        rates, walls = [], []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            out = pool.map(_oracle_one, [(sample_mx, 1)] * cores)
+            wall = time.perf_counter() - t0
+            walls.append(wall)
+            rates.append(sum(n for n, _ in out) / wall)
+    value = sum(rates) / len(rates)
+    ms = 1000.0 * sum(walls) / len(walls)
+    sample = (f"{cores} independent processes, each one SSPRK(10,4) time step of the same "
+              f"Shu-Osher problem at mx=2^17 (C restatement of the reference, gcc -O2, no FMA)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config({"sample_mx": sample_mx}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gpu(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import sharpclaw_b200 as S
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    q0, dx = shu_osher(MX)
+    ps = S.ClawParams(rp=S.RP_EULER, mx=MX, dx=dx, xlower=-5.0, gamma=GAMMA, mthbc=(1, 1),
+                      char_decomp=2, tfluct_solver=0, time_integrator=4)
+    cells = MX * NSTEP * NSTAGES
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def device_run(precision, clocks=None):
+        s = S.Solver(ps, precision)
+        s.set_q(q0)
+        for _ in range(args.warmup):
+            s.time_steps(NSTEP, DT0, CFL_MAX, CFL_DESIRED)
+        barrier()
+        total_ms = 0.0
+        ctx = clocks if clocks is not None else _Null()
+        with ctx:
+            for _ in range(args.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                ms, res = s.time_steps(NSTEP, DT0, CFL_MAX, CFL_DESIRED)
+                assert res["steps_taken"] == NSTEP and res["rejected"] == 0 and res["status"] == 0, res
+                total_ms += ms
+        barrier()
+        dt_last = res["dt_last"]
+        return s, max_over_ranks(total_ms), dt_last
+
+    clocks = Clocks(local_rank)
+    s_mix, ms_mix, dt_mix = device_run(args.precision, clocks)
+    value = world * cells * args.steps / (ms_mix / 1000.0)
+    s_64, ms_64, dt_64 = device_run("fp64")
+    value64 = world * cells * args.steps / (ms_64 / 1000.0)
+
+    # fused stage kernel alone (roofline): all 10 stage launches of a step
+    peak, peak_kind = measured_peaks()
+    reps = 20
+    roof = {}
+    for name, s in (("mixed", s_mix), ("fp64", s_64)):
+        st_ms, n_launch = s.time_stages(dt_mix, reps)
+        avg_ms = st_ms / n_launch
+        bytes_per_launch = 2.3 * 3 * 8 * MX          # k_I * meqn * sizeof(double) per cell-stage
+        gbs = bytes_per_launch / (avg_ms / 1000.0) / 1e9
+        roof[name] = {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                      "frac": gbs / peak, "traffic": None, "avg_launch_us": avg_ms * 1000.0,
+                      "algorithmic_bytes_per_launch": bytes_per_launch, "peak_source": peak_kind}
+
+    # end to end through the public API with host buffers
+    qh = torch.from_numpy(q0.copy()).pin_memory()
+    qout = torch.empty_like(qh).pin_memory()
+    qh_np, qout_np = qh.numpy(), qout.numpy()
+    s_e2e = s_mix
+    for _ in range(args.warmup):
+        s_e2e.set_q(qh_np)
+        s_e2e.sharpclaw(0.0, 1e30, DT0, CFL_MAX, CFL_DESIRED, max_steps=NSTEP)
+        qout_np[...] = s_e2e.get_q()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s_e2e.set_q(qh_np)
+        r = s_e2e.sharpclaw(0.0, 1e30, DT0, CFL_MAX, CFL_DESIRED, max_steps=NSTEP)
+        _ = _get_q_into(s_e2e, qout_np)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = world * cells * args.steps / e2e_s
+    nbytes = q0.nbytes
+
+    # accuracy: mixed vs plain FP64 after 20 fixed-dt steps on the full grid
+    acc = {}
+    if rank == 0:
+        outs = {}
+        for name in ("fp64", args.precision):
+            with S.Solver(ps, name) as s:
+                s.set_q(q0)
+                s.sharpclaw(0.0, 20 * DT0, DT0, 1e9, 0.5, dt_variable=0)
+                outs[name] = s.get_q()[:, 3:-3]
+        a, b = outs[args.precision], outs["fp64"]
+        acc = {"rel_l1_vs_fp64": max(float(np.abs(a[m] - b[m]).sum() / np.abs(b[m]).sum()) for m in range(3)),
+               "rel_linf_vs_fp64": float(np.abs(a - b).max() / np.abs(b).max()),
+               "steps": 20, "dt": DT0}
+
+    # CPU baseline: the oracle on a bounded sample, one core
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        n, t = _oracle_one((1 << 18, 2))
+        cpu = {"value": n / t, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": "mx=2^18 Shu-Osher, 2 SSPRK(10,4) time steps, C restatement of the reference "
+                         "(gcc -O2, no FMA), single thread"}
+
+    kps = s_mix.kernels_per_step
+    launches = args.steps * NSTEP * kps
+    ck = clocks.summary()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_mix / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 state/accumulation)",
+                "data": "synthetic",
+                "config": config({"precision": args.precision}),
+                "roofline": roof["mixed"],
+                "fp64": {"value": value64, "unit": UNIT, "ms_per_step": ms_64 / args.steps,
+                         "roofline": roof["fp64"], "speedup_of_headline": value / value64},
+                "accuracy": acc,
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                        "ms_per_step": 1000.0 * e2e_s / args.steps},
+                "gpu_launches": launches,
+                "clocks": ck}
+        print(json.dumps(line), flush=True)
+    s_mix.close()
+    s_64.close()
+    return 0
+
+
+def _get_q_into(s, out):
+    import ctypes
+    from sharpclaw_b200 import _capi as C
+    C.check(C.lib().scl_get_q(s._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "scl_get_q")
+    return out
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp64", "fp64_strict"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "b200":
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        return run_gpu(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,158 @@
+/*
+ * sharpclaw_cuda.h -- C ABI of the B200 SharpClaw semi-discrete WENO step.
+ *
+ * Drop-in boundary for the reference's hot path.  The reference binds these
+ * operations as Fortran subroutines; a Fortran host replaces them with
+ * bind(C) shims that forward here (see INTEGRATION.md for the
+ * iso_c_binding module).  Every entry point returns an int status (0 = ok,
+ * negative = SCL_E_*) and never calls exit/abort, replacing the reference's
+ * `stop` statements.
+ *
+ * Arrays crossing the boundary are host (or, for the *_device variants,
+ * device) arrays of double in the reference layout: Fortran column-major
+ * q(1-mbc:mx+mbc[,1-mbc:my+mbc], meqn) (src/1d/qalloc1.f90:10,
+ * src/2d/qalloc2.f90:11), i.e. element (i[,j],m) at
+ *   (i+mbc-1) [+ (j+mbc-1)*(mx+2mbc)] + (m-1)*plane.
+ * No torch types appear here.
+ */
+#ifndef SHARPCLAW_CUDA_H
+#define SHARPCLAW_CUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SCL_OK 0
+#define SCL_E_INVALID (-1)      /* bad parameter (the reference would `stop`)      */
+#define SCL_E_CUDA (-2)         /* a CUDA call failed; see scl_last_error()         */
+#define SCL_E_UNSUPPORTED (-3)  /* valid in the reference, not built here           */
+#define SCL_E_NONFINITE (-4)    /* NaN/Inf met in the CFL number                    */
+#define SCL_E_TIMEOUT (-5)      /* a bounded device wait ran out                    */
+
+/* device status bits (scl_result.status) */
+#define SCL_STATUS_NONFINITE 1
+#define SCL_STATUS_TIMEOUT 2
+#define SCL_STATUS_BOUNDS 4
+
+/* sharpclaw() info codes (src/sharpclaw.f90:35-63,225-228) plus one new one */
+#define SCL_INFO_DT_NOT_DIVIDING 2
+#define SCL_INFO_CFL_DESIRED_GT_MAX 3
+#define SCL_INFO_TOO_MANY_STEPS 11
+#define SCL_INFO_CFL_FIXED_DT 12
+#define SCL_INFO_NONFINITE 20
+
+/* ---- plugins (device Riemann solvers selected by id) ------------------- */
+#define SCL_RP_ADVECTION 1    /* apps/advection/1d/{rp1.f,tfluct1.f,evec.f}                 */
+#define SCL_RP_EULER 2        /* apps/euler/shockentropy/rp1eu.f (+ Roe evec, new)           */
+#define SCL_RP_SW2D 3         /* apps/shallowWater/2dRadialDam/{rpn2sw.f,tfluct1sw.f} (+evec) */
+#define SCL_RP_ACOUSTICS1D 4  /* apps/acoustics/1d/interface/{rp1acv.f,tfluct1acv.f,evec.f90} */
+#define SCL_RP_ACOUSTICS2D 5  /* 2-D variable-coefficient acoustics rpn2/tfluct/evec (new)    */
+
+/* ---- arithmetic ---------------------------------------------------------- */
+#define SCL_FP64 0         /* plain FP64 (FMA contraction allowed)                       */
+#define SCL_FP64_STRICT 1  /* FP64, no FMA contraction: the reference's evaluation order */
+#define SCL_MIXED 2        /* FP32 reconstruction/Riemann, FP64 state and RK accumulation */
+#define SCL_FP32 3         /* FP32 throughout (FP32 state)                               */
+
+/* Mirrors module ClawParams (src/ClawParams.f90:1-16) plus the plugin COMMON
+ * blocks (/comrp/ u or g, /param/ gamma) and the integrator choice. */
+typedef struct scl_params {
+  int ndim;             /* 1 or 2                                                  */
+  int mx, my;           /* nx(1), nx(2)                                            */
+  int meqn, mwaves, mbc, maux, mcapa;
+  int lim_type;         /* 2 = WENO (reconstruct.f90)                              */
+  int char_decomp;      /* 0 componentwise weno5, 2 characteristic-wise weno5_char */
+  int tfluct_solver;    /* 1 tfluct plugin, 0 swap + second rp (flux1.f90:136-188) */
+  int mthbc[4];         /* 1 extrapolation, 2 periodic, 3 solid wall               */
+  double dx, dy, xlower, ylower;
+  int rp;               /* SCL_RP_*                                                */
+  int efix;             /* entropy fix (rp1eu.f:40 .true., rpn2sw.f:48 .false.)    */
+  double u, gamma, grav;
+  int time_integrator;  /* 1 SSP22, 2 SSP42, 3 SSP33, 4 SSP104 (sharpclaw.f90:159) */
+  int precision;        /* SCL_FP64, SCL_FP64_STRICT, SCL_MIXED, SCL_FP32          */
+} scl_params;
+
+/* Arguments of sharpclaw() (src/sharpclaw.f90:2-5). */
+typedef struct scl_run {
+  double tstart, tend;
+  double dt_initial, dt_max, cfl_max, cfl_desired;
+  int max_steps, dt_variable;
+} scl_run;
+
+/* Outputs of sharpclaw() (cfl_maxused, cfl_last, dt_minused, dt_maxused,
+ * dt_last, steps_taken, info) plus rejected-step and device status counts. */
+typedef struct scl_result {
+  double tend, cfl_maxused, cfl_last, dt_minused, dt_maxused, dt_last;
+  int steps_taken, info, rejected, status;
+} scl_result;
+
+typedef struct scl_handle scl_handle;
+
+/* Library identification and the last error message of this thread. */
+const char* scl_version(void);
+const char* scl_last_error(void);
+
+/* Create a solver for one grid; allocates its device buffers on the current
+ * device and one stream.  Replaces module allocation in src/main.f90:128-133
+ * (qalloc, alloc_recon_workspace) and the griddat allocation in
+ * src/sharpclaw.f90:66-111. */
+int scl_create(const scl_params* p, scl_handle** out);
+int scl_destroy(scl_handle* h);
+
+/* Copy q / aux (reference layout, double, ghost cells included) to and from
+ * the device state.  scl_set_q also fills ghost cells as bc1/bc2 would. */
+int scl_set_q(scl_handle* h, const double* q);
+int scl_get_q(scl_handle* h, double* q);
+int scl_set_aux(scl_handle* h, const double* aux);
+
+/* One evaluation of dq = dt*L(q): bc + src + flux1 (1-D) or flux2 (2-D),
+ * step1d.f90:2-31 / step2d.f90:2-41.  q is updated in place with its ghost
+ * cells (as bc does), dq receives the interior update, cfl the CFL number
+ * (flux1.f90:126-133, flux2.f90:47,80).  Host arrays. */
+int scl_step_dq(scl_handle* h, double* q, double* dq, double dt, double t, double* cfl);
+
+/* flux1.f90:2 on one line of mx cells (ixy = 1 or 2 selects the normal
+ * direction for the 2-D plugins): q1d(1-mbc:mx+mbc,meqn) in, dq1d out
+ * (interior cells), cfl out.  aux1d may be NULL when maux == 0. */
+int scl_flux1(scl_handle* h, const double* q1d, const double* aux1d, double* dq1d,
+              double dt, int ixy, int mx, double* cfl);
+
+/* One SSP-RK time step on the device-resident q (ts_ssp22/42/33/104,
+ * sharpclaw.f90:247-464), qold = q on entry; returns the last stage's CFL. */
+int scl_rk_step(scl_handle* h, double dt, double told, double* cfl);
+
+/* The time loop of sharpclaw() (src/sharpclaw.f90:118-228) run on the
+ * device: dt control, rejection/retake and stopping are decided by a
+ * one-thread controller kernel between steps, captured in CUDA graphs, so the
+ * host does not synchronise per step.  b4step is the default no-op. */
+int scl_sharpclaw(scl_handle* h, const scl_run* run, scl_result* res);
+
+/* Same with device pointers: q_dev holds the initial data / receives the
+ * final state in the reference layout (double). */
+int scl_sharpclaw_device(scl_handle* h, const scl_run* run, double* q_dev, scl_result* res);
+
+/* Timing helper for benchmarks: replays `nsteps` steps of the controller on
+ * the device-resident state with stage kernels only (no host copies) and
+ * returns the elapsed device time in milliseconds, measured with CUDA events
+ * on the handle's stream. */
+int scl_time_steps(scl_handle* h, const scl_run* run, int nsteps, float* ms, scl_result* res);
+
+/* Roofline helper: launches the integrator's stage kernels (one pass of all
+ * stages = one time step's worth, no controller) `reps` times back to back on
+ * the device-resident state with step size dt and returns the elapsed device
+ * time (CUDA events on the handle's stream) and the number of launches.  The
+ * state is not advanced (every pass restarts from q^n). */
+int scl_time_stages(scl_handle* h, double dt, int reps, float* ms, long long* launches);
+
+/* Kernel launches per controller step (begin + stages + end, + 1 ghost-line
+ * CFL kernel in 2-D). */
+int scl_kernels_per_step(scl_handle* h);
+
+/* Stream of the handle (cudaStream_t as void*), for callers that overlap work. */
+void* scl_stream(scl_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SHARPCLAW_CUDA_H */

@@ -1,0 +1,1011 @@
+/*
+ * sclaw_oracle.c -- CPU oracle (test infrastructure only; see sclaw_oracle.h).
+ *
+ * Each routine restates one reference routine with the same loops, index
+ * ranges and floating-point evaluation order (Fortran left-to-right
+ * association, x**2 as x*x, REAL(4) literals widened to double, no FMA:
+ * compiled with -ffp-contract=off).  File:line citations are relative to the
+ * reference project root.
+ *
+ * Deliberate, documented differences from the reference:
+ *  - workspace entries that the reference leaves uninitialised at the two
+ *    outermost ghost interfaces (reconstruct.f90:113 dq1m(1), :375 hh(mbc,:))
+ *    are zeroed; they never reach interior cells or the CFL number;
+ *  - fixed plugin array limits (rp1eu.f:34 max2=2002, rpn2sw.f:42 maxm2=603)
+ *    are lifted by allocating per call;
+ *  - qold is refreshed every step, also when dt_variable == 0
+ *    (sharpclaw.f90:132-135 only does so for variable dt);
+ *  - plugins that the reference lacks (Euler evec, shallow-water evec, 2-D
+ *    acoustics rpn2/tfluct/evec) are new and are written identically here and
+ *    in the CUDA kernels.
+ */
+#include "sclaw_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* reconstruct.f90:6  double precision :: epweno = 1.e-36  (REAL(4) literal) */
+#define EPWENO ((double)1.0e-36f)
+
+static double dmax1(double a, double b) { return a > b ? a : b; }
+static double dmin1(double a, double b) { return a < b ? a : b; }
+
+long ocl_plane(const ocl_params *p) {
+  long n = (long)p->mx + 2L * p->mbc;
+  if (p->ndim == 2) n *= (long)p->my + 2L * p->mbc;
+  return n;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Line arrays: index i in [1-mbc, mx+mbc], 1-based component m, wave w.     */
+/* ------------------------------------------------------------------------ */
+#define L2(a, i, m) (a)[((i) + mbc - 1) + (long)((m) - 1) * ld]
+#define L3(a, i, m, w) (a)[((i) + mbc - 1) + (long)((m) - 1) * ld + (long)((w) - 1) * ld * meqn]
+
+/* ======================================================================== */
+/* Boundary conditions: src/1d/bc1.f90:1-112 and src/2d/bc2.f90:2-209.      */
+/* ======================================================================== */
+static int bc1(const ocl_params *p, double *q) {
+  const int mbc = p->mbc, mx = p->mx, meqn = p->meqn;
+  const long ld = mx + 2 * mbc;
+  switch (p->mthbc[0]) {                       /* bc1.f90:198 left */
+    case 1:
+      for (int m = 1; m <= meqn; ++m)
+        for (int ibc = 1; ibc <= mbc; ++ibc) L2(q, 1 - ibc, m) = L2(q, 1, m);
+      break;
+    case 2:
+      for (int m = 1; m <= meqn; ++m)
+        for (int ibc = 1; ibc <= mbc; ++ibc) L2(q, 1 - ibc, m) = L2(q, mx + 1 - ibc, m);
+      break;
+    case 3:
+      for (int m = 1; m <= meqn; ++m)
+        for (int ibc = 1; ibc <= mbc; ++ibc) L2(q, 1 - ibc, m) = L2(q, ibc, m);
+      for (int ibc = 1; ibc <= mbc; ++ibc) L2(q, 1 - ibc, 2) = -L2(q, ibc, 2);
+      break;
+    default:
+      return -2;
+  }
+  switch (p->mthbc[1]) {                       /* bc1.f90:240 right */
+    case 1:
+      for (int m = 1; m <= meqn; ++m)
+        for (int ibc = 1; ibc <= mbc; ++ibc) L2(q, mx + ibc, m) = L2(q, mx, m);
+      break;
+    case 2:
+      for (int m = 1; m <= meqn; ++m)
+        for (int ibc = 1; ibc <= mbc; ++ibc) L2(q, mx + ibc, m) = L2(q, ibc, m);
+      break;
+    case 3:
+      for (int m = 1; m <= meqn; ++m)
+        for (int ibc = 1; ibc <= mbc; ++ibc) L2(q, mx + ibc, m) = L2(q, mx + 1 - ibc, m);
+      for (int ibc = 1; ibc <= mbc; ++ibc) L2(q, mx + ibc, 2) = -L2(q, mx + 1 - ibc, 2);
+      break;
+    default:
+      return -2;
+  }
+  return 0;
+}
+
+#define G3(a, i, j, m) \
+  (a)[((i) + mbc - 1) + (long)((j) + mbc - 1) * ldx + (long)((m) - 1) * ldx * ldy]
+
+static int bc2(const ocl_params *p, double *q) {
+  const int mbc = p->mbc, nx = p->mx, ny = p->my, meqn = p->meqn;
+  const long ldx = nx + 2 * mbc, ldy = ny + 2 * mbc;
+  /* left (bc2.f90:31-69) */
+  for (int m = 1; m <= meqn; ++m)
+    for (int ibc = 1; ibc <= mbc; ++ibc)
+      for (int j = 1 - mbc; j <= ny + mbc; ++j) {
+        if (p->mthbc[0] == 1) G3(q, 1 - ibc, j, m) = G3(q, 1, j, m);
+        else if (p->mthbc[0] == 2) G3(q, 1 - ibc, j, m) = G3(q, nx + 1 - ibc, j, m);
+        else if (p->mthbc[0] == 3) G3(q, 1 - ibc, j, m) = G3(q, ibc, j, m);
+        else return -2;
+      }
+  if (p->mthbc[0] == 3)
+    for (int ibc = 1; ibc <= mbc; ++ibc)
+      for (int j = 1 - mbc; j <= ny + mbc; ++j) G3(q, 1 - ibc, j, 2) = -G3(q, ibc, j, 2);
+  /* right (bc2.f90:76-114) */
+  for (int m = 1; m <= meqn; ++m)
+    for (int ibc = 1; ibc <= mbc; ++ibc)
+      for (int j = 1 - mbc; j <= ny + mbc; ++j) {
+        if (p->mthbc[1] == 1) G3(q, nx + ibc, j, m) = G3(q, nx, j, m);
+        else if (p->mthbc[1] == 2) G3(q, nx + ibc, j, m) = G3(q, ibc, j, m);
+        else if (p->mthbc[1] == 3) G3(q, nx + ibc, j, m) = G3(q, nx + 1 - ibc, j, m);
+        else return -2;
+      }
+  if (p->mthbc[1] == 3)
+    for (int ibc = 1; ibc <= mbc; ++ibc)
+      for (int j = 1 - mbc; j <= ny + mbc; ++j) G3(q, nx + ibc, j, 2) = -G3(q, nx + 1 - ibc, j, 2);
+  /* bottom (bc2.f90:121-159) */
+  for (int m = 1; m <= meqn; ++m)
+    for (int jbc = 1; jbc <= mbc; ++jbc)
+      for (int i = 1 - mbc; i <= nx + mbc; ++i) {
+        if (p->mthbc[2] == 1) G3(q, i, 1 - jbc, m) = G3(q, i, 1, m);
+        else if (p->mthbc[2] == 2) G3(q, i, 1 - jbc, m) = G3(q, i, ny + 1 - jbc, m);
+        else if (p->mthbc[2] == 3) G3(q, i, 1 - jbc, m) = G3(q, i, jbc, m);
+        else return -2;
+      }
+  if (p->mthbc[2] == 3)
+    for (int jbc = 1; jbc <= mbc; ++jbc)
+      for (int i = 1 - mbc; i <= nx + mbc; ++i) G3(q, i, 1 - jbc, 3) = -G3(q, i, jbc, 3);
+  /* top (bc2.f90:166-204) */
+  for (int m = 1; m <= meqn; ++m)
+    for (int jbc = 1; jbc <= mbc; ++jbc)
+      for (int i = 1 - mbc; i <= nx + mbc; ++i) {
+        if (p->mthbc[3] == 1) G3(q, i, ny + jbc, m) = G3(q, i, ny, m);
+        else if (p->mthbc[3] == 2) G3(q, i, ny + jbc, m) = G3(q, i, jbc, m);
+        else if (p->mthbc[3] == 3) G3(q, i, ny + jbc, m) = G3(q, i, ny + 1 - jbc, m);
+        else return -2;
+      }
+  if (p->mthbc[3] == 3)
+    for (int jbc = 1; jbc <= mbc; ++jbc)
+      for (int i = 1 - mbc; i <= nx + mbc; ++i) G3(q, i, ny + jbc, 3) = -G3(q, i, ny + 1 - jbc, 3);
+  return 0;
+}
+
+int ocl_bc(const ocl_params *p, double *q) {
+  if (p->mbc != 3) return -1;
+  /* a solid wall negates component 2 (x) or 3 (y): bc1.f90:230, bc2.f90:67,157;
+   * with fewer components the reference writes out of bounds */
+  for (int k = 0; k < 2 * p->ndim; ++k)
+    if (p->mthbc[k] == 3 && p->meqn < (k < 2 ? 2 : 3)) return -2;
+  return p->ndim == 1 ? bc1(p, q) : bc2(p, q);
+}
+
+/* ======================================================================== */
+/* WENO5 reconstructions, src/reconstruct.f90.  Indices are the rebased      */
+/* (1-based, assumed-shape) array indices of the reference: array index k    */
+/* is cell k-mbc.                                                            */
+/* ======================================================================== */
+#define R2(a, k, m) (a)[((k) - 1) + (long)((m) - 1) * mx2]
+#define R3(a, k, p_, m) (a)[((k) - 1) + (long)((p_) - 1) * mx2 + (long)((m) - 1) * mx2 * meqn]
+
+/* reconstruct.f90:77-143 */
+int ocl_weno5(int mx2, int meqn, const double *q, double *ql, double *qr) {
+  const int mbc = 3;
+  double *dq1m = (double *)calloc((size_t)mx2 + 1, sizeof(double));
+  double *uu = (double *)calloc(2 * ((size_t)mx2 + 1), sizeof(double));
+  if (!dq1m || !uu) { free(dq1m); free(uu); return -3; }
+#define D1(k) dq1m[(k) - 1]
+#define UU(k, s) uu[((k) - 1) + (long)((s) - 1) * mx2]
+  for (int m = 1; m <= meqn; ++m) {
+    D1(1) = 0.0;  /* never assigned in the reference (ghost interface only) */
+    for (int i = 2; i <= mx2; ++i) D1(i) = R2(q, i, m) - R2(q, i - 1, m);   /* :96-99 */
+    for (int m1 = 1; m1 <= 2; ++m1) {
+      const int im = (m1 == 1) ? 1 : -1;        /* im=(-1)**(m1+1) :108 */
+      const int ione = im, inone = -im, intwo = -2 * im;
+      const double dim = (double)im;
+      for (int i = mbc; i <= mx2 - mbc + 1; ++i) {
+        double t1 = dim * (D1(i + intwo) - D1(i + inone));
+        double t2 = dim * (D1(i + inone) - D1(i));
+        double t3 = dim * (D1(i) - D1(i + ione));
+        double x1 = D1(i + intwo) - 3.0 * D1(i + inone);
+        double x2 = D1(i + inone) + D1(i);
+        double x3 = 3.0 * D1(i) - D1(i + ione);
+        double tt1 = 13.0 * (t1 * t1) + 3.0 * (x1 * x1);
+        double tt2 = 13.0 * (t2 * t2) + 3.0 * (x2 * x2);
+        double tt3 = 13.0 * (t3 * t3) + 3.0 * (x3 * x3);
+        tt1 = (EPWENO + tt1) * (EPWENO + tt1);
+        tt2 = (EPWENO + tt2) * (EPWENO + tt2);
+        tt3 = (EPWENO + tt3) * (EPWENO + tt3);
+        double s1 = tt2 * tt3;
+        double s2 = (6.0 * tt1) * tt3;
+        double s3 = (3.0 * tt1) * tt2;
+        double t0 = 1.0 / ((s1 + s2) + s3);
+        s1 = s1 * t0;
+        s3 = s3 * t0;
+        double c = ((-R2(q, i - 2, m)) + 7.0 * (R2(q, i - 1, m) + R2(q, i, m))) - R2(q, i + 1, m);
+        UU(i, m1) = ((s1 * (t2 - t1)) + ((0.5 * s3 - 0.25) * (t3 - t2))) / 3.0 + c / 12.0;
+      }
+    }
+    for (int i = mbc; i <= mx2 - mbc + 1; ++i) {    /* :137-138 */
+      R2(qr, i - 1, m) = UU(i, 1);
+      R2(ql, i, m) = UU(i, 2);
+    }
+  }
+#undef D1
+#undef UU
+  free(dq1m);
+  free(uu);
+  return 0;
+}
+
+/* reconstruct.f90:146-241 */
+int ocl_weno5_char(int mx2, int meqn, const double *q, const double *evl,
+                   const double *evr, double *ql, double *qr) {
+  const int mbc = 3;
+  double *dq = (double *)calloc((size_t)mx2 * meqn, sizeof(double));
+  double *hh = (double *)calloc((size_t)mx2 * 5, sizeof(double));
+  double *uu = (double *)calloc((size_t)mx2 * 2, sizeof(double));
+  if (!dq || !hh || !uu) { free(dq); free(hh); free(uu); return -3; }
+#define HH(k, o) hh[((k) - 1) + (long)((o) + 2) * mx2]
+#define UU(k, s) uu[((k) - 1) + (long)((s) - 1) * mx2]
+  for (int m = 1; m <= meqn; ++m)
+    for (int i = 2; i <= mx2; ++i) R2(dq, i, m) = R2(q, i, m) - R2(q, i - 1, m);  /* :166-169 */
+  for (int m = 1; m <= meqn; ++m)
+    for (int i = 3; i <= mx2 - 1; ++i) {                                           /* :171-176 */
+      double c = ((-R2(q, i - 2, m)) + 7.0 * (R2(q, i - 1, m) + R2(q, i, m))) - R2(q, i + 1, m);
+      R2(qr, i - 1, m) = c / 12.0;
+      R2(ql, i, m) = R2(qr, i - 1, m);
+    }
+  for (int ip = 1; ip <= meqn; ++ip) {
+    for (int m2 = -2; m2 <= 2; ++m2)                                                 /* :184-191 */
+      for (int i = mbc + 1; i <= mx2 - 2; ++i) {
+        double h = 0.0;
+        for (int m = 1; m <= meqn; ++m) h = h + R3(evl, i, ip, m) * R2(dq, i + m2, m);
+        HH(i, m2) = h;
+      }
+    for (int m1 = 1; m1 <= 2; ++m1) {                                                /* :196-229 */
+      const int im = (m1 == 1) ? 1 : -1;
+      const int ione = im, inone = -im, intwo = -2 * im;
+      const double dim = (double)im;
+      for (int i = mbc; i <= mx2 - mbc + 1; ++i) {
+        double t1 = dim * (HH(i, intwo) - HH(i, inone));
+        double t2 = dim * (HH(i, inone) - HH(i, 0));
+        double t3 = dim * (HH(i, 0) - HH(i, ione));
+        double x1 = HH(i, intwo) - 3.0 * HH(i, inone);
+        double x2 = HH(i, inone) + HH(i, 0);
+        double x3 = 3.0 * HH(i, 0) - HH(i, ione);
+        double tt1 = 13.0 * (t1 * t1) + 3.0 * (x1 * x1);
+        double tt2 = 13.0 * (t2 * t2) + 3.0 * (x2 * x2);
+        double tt3 = 13.0 * (t3 * t3) + 3.0 * (x3 * x3);
+        tt1 = (EPWENO + tt1) * (EPWENO + tt1);
+        tt2 = (EPWENO + tt2) * (EPWENO + tt2);
+        tt3 = (EPWENO + tt3) * (EPWENO + tt3);
+        double s1 = tt2 * tt3;
+        double s2 = (6.0 * tt1) * tt3;
+        double s3 = (3.0 * tt1) * tt2;
+        double t0 = 1.0 / ((s1 + s2) + s3);
+        s1 = s1 * t0;
+        s3 = s3 * t0;
+        UU(i, m1) = ((s1 * (t2 - t1)) + ((0.5 * s3 - 0.25) * (t3 - t2))) / 3.0;
+      }
+    }
+    for (int m = 1; m <= meqn; ++m)                                                  /* :232-237 */
+      for (int i = mbc; i <= mx2 - mbc + 1; ++i) {
+        R2(qr, i - 1, m) = R2(qr, i - 1, m) + R3(evr, i, m, ip) * UU(i, 1);
+        R2(ql, i, m) = R2(ql, i, m) + R3(evr, i, m, ip) * UU(i, 2);
+      }
+  }
+#undef HH
+#undef UU
+  free(dq);
+  free(hh);
+  free(uu);
+  return 0;
+}
+
+/* ======================================================================== */
+/* Plugins.  Each keeps the reference loop i = 2-mbc .. mx+mbc and its      */
+/* arithmetic order.  ld = mx+2*mbc for every line array.                  */
+/* ======================================================================== */
+
+/* apps/advection/1d/rp1.f:35-43 */
+static void rp_advection(const ocl_params *p, int mx, const double *ql, const double *qr,
+                         double *wave, double *s, double *amdq, double *apdq) {
+  const int mbc = p->mbc, meqn = p->meqn;
+  const long ld = mx + 2 * mbc;
+  const double u = p->u;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    L3(wave, i, 1, 1) = L2(ql, i, 1) - L2(qr, i - 1, 1);
+    L2(s, i, 1) = u;
+    L2(amdq, i, 1) = dmin1(u, 0.0) * L3(wave, i, 1, 1);
+    L2(apdq, i, 1) = dmax1(u, 0.0) * L3(wave, i, 1, 1);
+  }
+}
+
+/* apps/advection/1d/tfluct1.f:78-87 */
+static void tfluct_advection(const ocl_params *p, int mx, const double *ql, const double *qr,
+                             double *s, double *adq) {
+  const int mbc = p->mbc;
+  const long ld = mx + 2 * mbc;
+  const double u = p->u;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    double w = L2(qr, i, 1) - L2(ql, i, 1);
+    L2(s, i, 1) = u;
+    double am = dmin1(u, 0.0) * w;
+    double ap = dmax1(u, 0.0) * w;
+    L2(adq, i, 1) = am + ap;
+  }
+}
+
+/* apps/euler/shockentropy/rp1eu.f:44-213 (efix as p->efix, default .true.) */
+static void rp_euler(const ocl_params *p, int mx, const double *ql, const double *qr,
+                     double *wave, double *s, double *amdq, double *apdq) {
+  const int mbc = p->mbc, meqn = p->meqn, mwaves = p->mwaves;
+  const long ld = mx + 2 * mbc;
+  const double gamma = p->gamma, gamma1 = p->gamma - 1.0;
+  double *u = (double *)malloc(sizeof(double) * ld);
+  double *enth = (double *)malloc(sizeof(double) * ld);
+  double *a = (double *)malloc(sizeof(double) * ld);
+#define LOC(v, i) (v)[(i) + mbc - 1]
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {                                        /* :44-55 */
+    double rhsqrtl = sqrt(L2(qr, i - 1, 1));
+    double rhsqrtr = sqrt(L2(ql, i, 1));
+    double pl = gamma1 * (L2(qr, i - 1, 3) - (0.5 * (L2(qr, i - 1, 2) * L2(qr, i - 1, 2))) / L2(qr, i - 1, 1));
+    double pr = gamma1 * (L2(ql, i, 3) - (0.5 * (L2(ql, i, 2) * L2(ql, i, 2))) / L2(ql, i, 1));
+    double rhsq2 = rhsqrtl + rhsqrtr;
+    LOC(u, i) = (L2(qr, i - 1, 2) / rhsqrtl + L2(ql, i, 2) / rhsqrtr) / rhsq2;
+    LOC(enth, i) = ((L2(qr, i - 1, 3) + pl) / rhsqrtl + (L2(ql, i, 3) + pr) / rhsqrtr) / rhsq2;
+    double a2 = gamma1 * (LOC(enth, i) - 0.5 * (LOC(u, i) * LOC(u, i)));
+    LOC(a, i) = sqrt(a2);
+  }
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {                                        /* :58-86 */
+    double d1 = L2(ql, i, 1) - L2(qr, i - 1, 1);
+    double d2 = L2(ql, i, 2) - L2(qr, i - 1, 2);
+    double d3 = L2(ql, i, 3) - L2(qr, i - 1, 3);
+    double ui = LOC(u, i), ai = LOC(a, i), hi = LOC(enth, i);
+    double a2 = (gamma1 / (ai * ai)) * (((hi - ui * ui) * d1 + ui * d2) - d3);
+    double a3 = ((d2 + (ai - ui) * d1) - ai * a2) / (2.0 * ai);
+    double a1 = (d1 - a2) - a3;
+    L3(wave, i, 1, 1) = a1;
+    L3(wave, i, 2, 1) = a1 * (ui - ai);
+    L3(wave, i, 3, 1) = a1 * (hi - ui * ai);
+    L2(s, i, 1) = ui - ai;
+    L3(wave, i, 1, 2) = a2;
+    L3(wave, i, 2, 2) = a2 * ui;
+    L3(wave, i, 3, 2) = (a2 * 0.5) * (ui * ui);
+    L2(s, i, 2) = ui;
+    L3(wave, i, 1, 3) = a3;
+    L3(wave, i, 2, 3) = a3 * (ui + ai);
+    L3(wave, i, 3, 3) = a3 * (hi + ui * ai);
+    L2(s, i, 3) = ui + ai;
+  }
+  if (!p->efix) {                                                                    /* :100-111 */
+    for (int m = 1; m <= 3; ++m)
+      for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double am = 0.0, ap = 0.0;
+        for (int mw = 1; mw <= mwaves; ++mw) {
+          if (L2(s, i, mw) < 0.0) am = am + L2(s, i, mw) * L3(wave, i, m, mw);
+          else ap = ap + L2(s, i, mw) * L3(wave, i, m, mw);
+        }
+        L2(amdq, i, m) = am;
+        L2(apdq, i, m) = ap;
+      }
+  } else {
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {                                      /* :126-201 */
+      double rhoim1 = L2(qr, i - 1, 1);
+      double pim1 = gamma1 * (L2(qr, i - 1, 3) - (0.5 * (L2(qr, i - 1, 2) * L2(qr, i - 1, 2))) / rhoim1);
+      double cim1 = sqrt((gamma * pim1) / rhoim1);
+      double s0 = L2(qr, i - 1, 2) / rhoim1 - cim1;
+      if (s0 >= 0.0 && L2(s, i, 1) > 0.0) {
+        for (int m = 1; m <= 3; ++m) L2(amdq, i, m) = 0.0;
+        continue;
+      }
+      double rho1 = L2(qr, i - 1, 1) + L3(wave, i, 1, 1);
+      double rhou1 = L2(qr, i - 1, 2) + L3(wave, i, 2, 1);
+      double en1 = L2(qr, i - 1, 3) + L3(wave, i, 3, 1);
+      double p1 = gamma1 * (en1 - (0.5 * (rhou1 * rhou1)) / rho1);
+      double c1 = sqrt((gamma * p1) / rho1);
+      double s1 = rhou1 / rho1 - c1;
+      double sfract;
+      if (s0 < 0.0 && s1 > 0.0) sfract = (s0 * (s1 - L2(s, i, 1))) / (s1 - s0);
+      else if (L2(s, i, 1) < 0.0) sfract = L2(s, i, 1);
+      else sfract = 0.0;
+      for (int m = 1; m <= 3; ++m) L2(amdq, i, m) = sfract * L3(wave, i, m, 1);
+      if (L2(s, i, 2) >= 0.0) continue;
+      for (int m = 1; m <= 3; ++m) L2(amdq, i, m) = L2(amdq, i, m) + L2(s, i, 2) * L3(wave, i, m, 2);
+      double rhoi = L2(ql, i, 1);
+      double pi = gamma1 * (L2(ql, i, 3) - (0.5 * (L2(ql, i, 2) * L2(ql, i, 2))) / rhoi);
+      double ci = sqrt((gamma * pi) / rhoi);
+      double s3 = L2(ql, i, 2) / rhoi + ci;
+      double rho2 = L2(ql, i, 1) - L3(wave, i, 1, 3);
+      double rhou2 = L2(ql, i, 2) - L3(wave, i, 2, 3);
+      double en2 = L2(ql, i, 3) - L3(wave, i, 3, 3);
+      double p2 = gamma1 * (en2 - (0.5 * (rhou2 * rhou2)) / rho2);
+      double c2 = sqrt((gamma * p2) / rho2);
+      double s2 = rhou2 / rho2 + c2;
+      if (s2 < 0.0 && s3 > 0.0) sfract = (s2 * (s3 - L2(s, i, 3))) / (s3 - s2);
+      else if (L2(s, i, 3) < 0.0) sfract = L2(s, i, 3);
+      else continue;
+      for (int m = 1; m <= 3; ++m) L2(amdq, i, m) = L2(amdq, i, m) + sfract * L3(wave, i, m, 3);
+    }
+    for (int m = 1; m <= 3; ++m)                                                     /* :206-213 */
+      for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double df = 0.0;
+        for (int mw = 1; mw <= mwaves; ++mw) df = df + L2(s, i, mw) * L3(wave, i, m, mw);
+        L2(apdq, i, m) = df - L2(amdq, i, m);
+      }
+  }
+#undef LOC
+  free(u);
+  free(enth);
+  free(a);
+}
+
+/* Roe-averaged right/left eigenvectors of the 1-D Euler equations at
+ * interface i-1/2 (new; the reference's evec1eu.f is incomplete).  Averages
+ * are computed exactly as rp1eu.f:44-55 does, from the cell averages
+ * q(i-1), q(i).  evr(i,:,p) = p-th right eigenvector, evl(i,p,:) = p-th row
+ * of its inverse, the convention weno5_char uses (reconstruct.f90:188,234). */
+static void evec_euler(const ocl_params *p, int mx, const double *q, double *evl, double *evr) {
+  const int mbc = p->mbc, meqn = 3;
+  const long ld = mx + 2 * mbc;
+  const double gamma1 = p->gamma - 1.0;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    double rhsqrtl = sqrt(L2(q, i - 1, 1));
+    double rhsqrtr = sqrt(L2(q, i, 1));
+    double pl = gamma1 * (L2(q, i - 1, 3) - (0.5 * (L2(q, i - 1, 2) * L2(q, i - 1, 2))) / L2(q, i - 1, 1));
+    double pr = gamma1 * (L2(q, i, 3) - (0.5 * (L2(q, i, 2) * L2(q, i, 2))) / L2(q, i, 1));
+    double rhsq2 = rhsqrtl + rhsqrtr;
+    double u = (L2(q, i - 1, 2) / rhsqrtl + L2(q, i, 2) / rhsqrtr) / rhsq2;
+    double h = ((L2(q, i - 1, 3) + pl) / rhsqrtl + (L2(q, i, 3) + pr) / rhsqrtr) / rhsq2;
+    double a2 = gamma1 * (h - 0.5 * (u * u));
+    double a = sqrt(a2);
+    L3(evr, i, 1, 1) = 1.0; L3(evr, i, 1, 2) = 1.0; L3(evr, i, 1, 3) = 1.0;
+    L3(evr, i, 2, 1) = u - a; L3(evr, i, 2, 2) = u; L3(evr, i, 2, 3) = u + a;
+    L3(evr, i, 3, 1) = h - u * a; L3(evr, i, 3, 2) = 0.5 * (u * u); L3(evr, i, 3, 3) = h + u * a;
+    double b1 = gamma1 / a2;
+    double b2 = 0.5 * (b1 * (u * u));
+    double ua = u / a;
+    double ra = 1.0 / a;
+    double b1u = b1 * u;
+    L3(evl, i, 1, 1) = 0.5 * (b2 + ua);
+    L3(evl, i, 1, 2) = -0.5 * (b1u + ra);
+    L3(evl, i, 1, 3) = 0.5 * b1;
+    L3(evl, i, 2, 1) = 1.0 - b2;
+    L3(evl, i, 2, 2) = b1u;
+    L3(evl, i, 2, 3) = -b1;
+    L3(evl, i, 3, 1) = 0.5 * (b2 - ua);
+    L3(evl, i, 3, 2) = -0.5 * (b1u - ra);
+    L3(evl, i, 3, 3) = 0.5 * b1;
+  }
+}
+
+/* apps/shallowWater/2dRadialDam/rpn2sw.f:60-228 */
+static void rp_sw(const ocl_params *p, int ixy, int mx, const double *ql, const double *qr,
+                  double *wave, double *s, double *amdq, double *apdq, int cell_internal) {
+  /* cell_internal: tfluct1sw.f:317-467 variant (left ql(i), right qr(i)) */
+  const int mbc = p->mbc, meqn = p->meqn, mwaves = p->mwaves;
+  const long ld = mx + 2 * mbc;
+  const double g = p->grav;
+  const int mu = (ixy == 1) ? 2 : 3, mv = (ixy == 1) ? 3 : 2;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    const double *L = cell_internal ? ql : qr;
+    const double *R = cell_internal ? qr : ql;
+    const int il = cell_internal ? i : i - 1;
+#define QLT(m) L2(L, il, m)
+#define QRT(m) L2(R, i, m)
+    double h = (QLT(1) + QRT(1)) * 0.50;
+    double hsqrtl = sqrt(QLT(1));
+    double hsqrtr = sqrt(QRT(1));
+    double hsq2 = hsqrtl + hsqrtr;
+    double u = (QLT(mu) / hsqrtl + QRT(mu) / hsqrtr) / hsq2;
+    double v = (QLT(mv) / hsqrtl + QRT(mv) / hsqrtr) / hsq2;
+    double a = sqrt(g * h);
+    double d1 = QRT(1) - QLT(1);
+    double d2 = QRT(mu) - QLT(mu);
+    double d3 = QRT(mv) - QLT(mv);
+    double a1 = ((u + a) * d1 - d2) * (0.50 / a);
+    double a2 = -(v * d1) + d3;
+    double a3 = (-((u - a) * d1) + d2) * (0.50 / a);
+    L3(wave, i, 1, 1) = a1;
+    L3(wave, i, mu, 1) = a1 * (u - a);
+    L3(wave, i, mv, 1) = a1 * v;
+    L2(s, i, 1) = u - a;
+    L3(wave, i, 1, 2) = 0.0;
+    L3(wave, i, mu, 2) = 0.0;
+    L3(wave, i, mv, 2) = a2;
+    L2(s, i, 2) = u;
+    L3(wave, i, 1, 3) = a3;
+    L3(wave, i, mu, 3) = a3 * (u + a);
+    L3(wave, i, mv, 3) = a3 * v;
+    L2(s, i, 3) = u + a;
+  }
+  if (!p->efix) {
+    for (int m = 1; m <= 3; ++m)
+      for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double am = 0.0, ap = 0.0;
+        for (int mw = 1; mw <= mwaves; ++mw) {
+          if (L2(s, i, mw) < 0.0) am = am + L2(s, i, mw) * L3(wave, i, m, mw);
+          else ap = ap + L2(s, i, mw) * L3(wave, i, m, mw);
+        }
+        L2(amdq, i, m) = am;
+        L2(apdq, i, m) = ap;
+      }
+    return;
+  }
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    const double *L = cell_internal ? ql : qr;
+    const double *R = cell_internal ? qr : ql;
+    const int il = cell_internal ? i : i - 1;
+    double him1 = QLT(1);
+    double s0 = QLT(mu) / him1 - sqrt(g * him1);
+    if (s0 > 0.0 && L2(s, i, 1) > 0.0) {
+      for (int m = 1; m <= 3; ++m) L2(amdq, i, m) = 0.0;
+      continue;
+    }
+    double h1 = QLT(1) + L3(wave, i, 1, 1);
+    double hu1 = QLT(mu) + L3(wave, i, mu, 1);
+    double s1 = hu1 / h1 - sqrt(g * h1);
+    double sfract;
+    if (s0 < 0.0 && s1 > 0.0) sfract = s0 * ((s1 - L2(s, i, 1)) / (s1 - s0));
+    else if (L2(s, i, 1) < 0.0) sfract = L2(s, i, 1);
+    else sfract = 0.0;
+    for (int m = 1; m <= 3; ++m) L2(amdq, i, m) = sfract * L3(wave, i, m, 1);
+    if (L2(s, i, 2) > 0.0) continue;
+    for (int m = 1; m <= 3; ++m) L2(amdq, i, m) = L2(amdq, i, m) + L2(s, i, 2) * L3(wave, i, m, 2);
+    double hi = QRT(1);
+    double s03 = QRT(mu) / hi + sqrt(g * hi);
+    double h3 = QRT(1) - L3(wave, i, 1, 3);
+    double hu3 = QRT(mu) - L3(wave, i, mu, 3);
+    double s3 = hu3 / h3 + sqrt(g * h3);
+    if (s3 < 0.0 && s03 > 0.0) sfract = s3 * ((s03 - L2(s, i, 3)) / (s03 - s3));
+    else if (L2(s, i, 3) < 0.0) sfract = L2(s, i, 3);
+    else continue;
+    for (int m = 1; m <= 3; ++m) L2(amdq, i, m) = L2(amdq, i, m) + sfract * L3(wave, i, m, 3);
+  }
+#undef QLT
+#undef QRT
+  for (int m = 1; m <= 3; ++m)
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+      double df = 0.0;
+      for (int mw = 1; mw <= mwaves; ++mw) df = df + L2(s, i, mw) * L3(wave, i, m, mw);
+      L2(apdq, i, m) = df - L2(amdq, i, m);
+    }
+}
+
+/* Shallow-water Roe eigenvectors along direction ixy at interface i-1/2 (new;
+ * the reference has none).  Roe averages as rpn2sw.f:80-88 from q(i-1), q(i);
+ * the left eigenvectors are the rows that rpn2sw.f:98-100 uses for a1..a3. */
+static void evec_sw(const ocl_params *p, int ixy, int mx, const double *q, double *evl, double *evr) {
+  const int mbc = p->mbc, meqn = 3;
+  const long ld = mx + 2 * mbc;
+  const double g = p->grav;
+  const int mu = (ixy == 1) ? 2 : 3, mv = (ixy == 1) ? 3 : 2;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    double h = (L2(q, i - 1, 1) + L2(q, i, 1)) * 0.50;
+    double hsqrtl = sqrt(L2(q, i - 1, 1));
+    double hsqrtr = sqrt(L2(q, i, 1));
+    double hsq2 = hsqrtl + hsqrtr;
+    double u = (L2(q, i - 1, mu) / hsqrtl + L2(q, i, mu) / hsqrtr) / hsq2;
+    double v = (L2(q, i - 1, mv) / hsqrtl + L2(q, i, mv) / hsqrtr) / hsq2;
+    double a = sqrt(g * h);
+    double ha = 0.50 / a;
+    L3(evr, i, 1, 1) = 1.0;    L3(evr, i, mu, 1) = u - a; L3(evr, i, mv, 1) = v;
+    L3(evr, i, 1, 2) = 0.0;    L3(evr, i, mu, 2) = 0.0;   L3(evr, i, mv, 2) = 1.0;
+    L3(evr, i, 1, 3) = 1.0;    L3(evr, i, mu, 3) = u + a; L3(evr, i, mv, 3) = v;
+    L3(evl, i, 1, 1) = (u + a) * ha;    L3(evl, i, 1, mu) = -ha; L3(evl, i, 1, mv) = 0.0;
+    L3(evl, i, 2, 1) = -v;              L3(evl, i, 2, mu) = 0.0; L3(evl, i, 2, mv) = 1.0;
+    L3(evl, i, 3, 1) = -((u - a) * ha); L3(evl, i, 3, mu) = ha;  L3(evl, i, 3, mv) = 0.0;
+  }
+}
+
+/* apps/acoustics/1d/interface/rp1acv.f:49-80; with ixy it is also the new 2-D
+ * normal solver (mu = normal velocity, tangential components carry 0). */
+static void rp_acoustics(const ocl_params *p, int ixy, int mx, const double *ql, const double *qr,
+                         const double *auxl, const double *auxr, double *wave, double *s,
+                         double *amdq, double *apdq) {
+  const int mbc = p->mbc, meqn = p->meqn;
+  const long ld = mx + 2 * mbc;
+  const int mu = (ixy == 1) ? 2 : 3, mv = (ixy == 1) ? 3 : 2;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    double d1 = L2(ql, i, 1) - L2(qr, i - 1, 1);
+    double d2 = L2(ql, i, mu) - L2(qr, i - 1, mu);
+    double zi = L2(auxl, i, 1);
+    double zim = L2(auxr, i - 1, 1);
+    double a1 = ((-d1) + zi * d2) / (zim + zi);
+    double a2 = (d1 + zim * d2) / (zim + zi);
+    L3(wave, i, 1, 1) = -(a1 * zim);
+    L3(wave, i, mu, 1) = a1;
+    L2(s, i, 1) = -L2(auxr, i - 1, 2);
+    L3(wave, i, 1, 2) = a2 * zi;
+    L3(wave, i, mu, 2) = a2;
+    L2(s, i, 2) = L2(auxl, i, 2);
+    if (meqn == 3) { L3(wave, i, mv, 1) = 0.0; L3(wave, i, mv, 2) = 0.0; }
+  }
+  for (int m = 1; m <= meqn; ++m)
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+      L2(amdq, i, m) = L2(s, i, 1) * L3(wave, i, m, 1);
+      L2(apdq, i, m) = L2(s, i, 2) * L3(wave, i, m, 2);
+    }
+}
+
+/* apps/acoustics/1d/interface/tfluct1acv.f:134-166 (2-D: normal by ixy) */
+static void tfluct_acoustics(const ocl_params *p, int ixy, int mx, const double *ql, const double *qr,
+                             const double *auxl, double *s, double *adq) {
+  const int mbc = p->mbc, meqn = p->meqn;
+  const long ld = mx + 2 * mbc;
+  const int mu = (ixy == 1) ? 2 : 3, mv = (ixy == 1) ? 3 : 2;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    double d1 = L2(qr, i, 1) - L2(ql, i, 1);
+    double d2 = L2(qr, i, mu) - L2(ql, i, mu);
+    double zi = L2(auxl, i, 1);
+    double zim = L2(auxl, i, 1);
+    double a1 = ((-d1) + zi * d2) / (zim + zi);
+    double a2 = (d1 + zim * d2) / (zim + zi);
+    double w[3][2];
+    w[0][0] = -(a1 * zim); w[0][1] = a2 * zi;
+    w[mu - 1][0] = a1;     w[mu - 1][1] = a2;
+    if (meqn == 3) { w[mv - 1][0] = 0.0; w[mv - 1][1] = 0.0; }
+    double s1 = -L2(auxl, i, 2), s2 = L2(auxl, i, 2);
+    L2(s, i, 1) = s1;
+    L2(s, i, 2) = s2;
+    for (int m = 1; m <= meqn; ++m) {
+      double am = s1 * w[m - 1][0];
+      double ap = s2 * w[m - 1][1];
+      L2(adq, i, m) = am + ap;
+    }
+  }
+}
+
+/* apps/acoustics/1d/interface/evec.f90:196-206; 2-D adds the tangential
+ * velocity as a third, zero-speed field (new). */
+static void evec_acoustics(const ocl_params *p, int ixy, int mx, const double *auxl,
+                           double *evl, double *evr) {
+  const int mbc = p->mbc, meqn = p->meqn;
+  const long ld = mx + 2 * mbc;
+  const int mu = (ixy == 1) ? 2 : 3, mv = (ixy == 1) ? 3 : 2;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    L3(evr, i, 1, 1) = -L2(auxl, i - 1, 1);
+    L3(evr, i, 1, 2) = L2(auxl, i, 1);
+    L3(evr, i, mu, 1) = 1.0;
+    L3(evr, i, mu, 2) = 1.0;
+    double z = 1.0 / (L2(auxl, i - 1, 1) + L2(auxl, i, 1));
+    L3(evl, i, 1, 1) = -1.0 * z;
+    L3(evl, i, 1, mu) = L2(auxl, i, 1) * z;
+    L3(evl, i, 2, 1) = 1.0 * z;
+    L3(evl, i, 2, mu) = L2(auxl, i - 1, 1) * z;
+    if (meqn == 3) {
+      L3(evr, i, mv, 1) = 0.0; L3(evr, i, mv, 2) = 0.0;
+      L3(evr, i, 1, 3) = 0.0;  L3(evr, i, mu, 3) = 0.0; L3(evr, i, mv, 3) = 1.0;
+      L3(evl, i, 1, mv) = 0.0; L3(evl, i, 2, mv) = 0.0;
+      L3(evl, i, 3, 1) = 0.0;  L3(evl, i, 3, mu) = 0.0; L3(evl, i, 3, mv) = 1.0;
+    }
+  }
+}
+
+/* apps/advection/1d/evec.f:118-121 */
+static void evec_advection(const ocl_params *p, int mx, double *evl, double *evr) {
+  const int mbc = p->mbc, meqn = 1;
+  const long ld = mx + 2 * mbc;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    L3(evr, i, 1, 1) = 1.0;
+    L3(evl, i, 1, 1) = 1.0;
+  }
+}
+
+int ocl_rp(const ocl_params *p, int ixy, int mx, const double *ql, const double *qr,
+           const double *auxl, const double *auxr, double *wave, double *s,
+           double *amdq, double *apdq) {
+  switch (p->rp) {
+    case OCL_RP_ADVECTION: rp_advection(p, mx, ql, qr, wave, s, amdq, apdq); return 0;
+    case OCL_RP_EULER: rp_euler(p, mx, ql, qr, wave, s, amdq, apdq); return 0;
+    case OCL_RP_SW2D: rp_sw(p, ixy, mx, ql, qr, wave, s, amdq, apdq, 0); return 0;
+    case OCL_RP_ACOUSTICS1D:
+    case OCL_RP_ACOUSTICS2D:
+      rp_acoustics(p, ixy, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq); return 0;
+  }
+  return -4;
+}
+
+int ocl_tfluct(const ocl_params *p, int ixy, int mx, const double *ql, const double *qr,
+               const double *auxl, const double *auxr, double *s, double *adq) {
+  (void)auxr;
+  switch (p->rp) {
+    case OCL_RP_ADVECTION: tfluct_advection(p, mx, ql, qr, s, adq); return 0;
+    case OCL_RP_SW2D: {
+      /* tfluct1sw.f: the Roe solve with left ql(i), right qr(i); adq = amdq+apdq */
+      const long ld = mx + 2L * p->mbc;
+      double *wave = (double *)calloc((size_t)ld * p->meqn * p->mwaves, sizeof(double));
+      double *am = (double *)calloc((size_t)ld * p->meqn, sizeof(double));
+      double *ap = (double *)calloc((size_t)ld * p->meqn, sizeof(double));
+      rp_sw(p, ixy, mx, ql, qr, wave, s, am, ap, 1);
+      for (long k = 0; k < ld * p->meqn; ++k) adq[k] = am[k] + ap[k];
+      free(wave); free(am); free(ap);
+      return 0;
+    }
+    case OCL_RP_ACOUSTICS1D:
+    case OCL_RP_ACOUSTICS2D:
+      tfluct_acoustics(p, ixy, mx, ql, qr, auxl, s, adq); return 0;
+  }
+  return -4;  /* src/tfluct.f90: no tfluct for this family */
+}
+
+int ocl_evec(const ocl_params *p, int ixy, int mx, const double *q, const double *auxl,
+             const double *auxr, double *evl, double *evr) {
+  (void)auxr;
+  switch (p->rp) {
+    case OCL_RP_ADVECTION: evec_advection(p, mx, evl, evr); return 0;
+    case OCL_RP_EULER: evec_euler(p, mx, q, evl, evr); return 0;
+    case OCL_RP_SW2D: evec_sw(p, ixy, mx, q, evl, evr); return 0;
+    case OCL_RP_ACOUSTICS1D:
+    case OCL_RP_ACOUSTICS2D: evec_acoustics(p, ixy, mx, auxl, evl, evr); return 0;
+  }
+  return -4;
+}
+
+/* ======================================================================== */
+/* src/flux1.f90:55-190                                                      */
+/* ======================================================================== */
+int ocl_flux1(const ocl_params *p, const double *q1d, double *dq1d, const double *aux1d,
+              double dt, double *cfl, int ixy, int mx) {
+  const int mbc = p->mbc, meqn = p->meqn, mwaves = p->mwaves, maux = p->maux;
+  const long ld = mx + 2 * mbc;
+  const int mx2 = (int)ld;
+  int rc = 0;
+  if (p->lim_type != 2) return -5;
+  double dx = (ixy == 1) ? p->dx : p->dy;
+  double *dtdx = (double *)calloc((size_t)ld, sizeof(double));
+  double *ql = (double *)calloc((size_t)ld * meqn, sizeof(double));
+  double *qr = (double *)calloc((size_t)ld * meqn, sizeof(double));
+  double *wave = (double *)calloc((size_t)ld * meqn * mwaves, sizeof(double));
+  double *s = (double *)calloc((size_t)ld * mwaves, sizeof(double));
+  double *amdq = (double *)calloc((size_t)ld * meqn, sizeof(double));
+  double *apdq = (double *)calloc((size_t)ld * meqn, sizeof(double));
+  double *amdq2 = (double *)calloc((size_t)ld * meqn, sizeof(double));
+  double *apdq2 = (double *)calloc((size_t)ld * meqn, sizeof(double));
+  double *evl = (double *)calloc((size_t)ld * meqn * meqn, sizeof(double));
+  double *evr = (double *)calloc((size_t)ld * meqn * meqn, sizeof(double));
+  double *auxl = (double *)calloc((size_t)ld * (maux > 0 ? maux : 1), sizeof(double));
+  double *auxr = (double *)calloc((size_t)ld * (maux > 0 ? maux : 1), sizeof(double));
+  if (!dtdx || !ql || !qr || !wave || !s || !amdq || !apdq || !amdq2 || !apdq2 || !evl ||
+      !evr || !auxl || !auxr) { rc = -3; goto done; }
+
+  for (int i = 1 - mbc; i <= mx + mbc; ++i) {                                 /* :57-61 */
+    if (p->mcapa > 0) dtdx[i + mbc - 1] = dt / (dx * L2(aux1d, i, p->mcapa));
+    else dtdx[i + mbc - 1] = dt / dx;
+  }
+  if (p->ndim > 1)                                                            /* :62 */
+    for (long k = 0; k < ld * meqn; ++k) dq1d[k] = 0.0;
+
+  switch (p->char_decomp) {                                                   /* :92-116 */
+    case 0: rc = ocl_weno5(mx2, meqn, q1d, ql, qr); break;
+    case 2:
+      rc = ocl_evec(p, ixy, mx, q1d, aux1d, aux1d, evl, evr);
+      if (!rc) rc = ocl_weno5_char(mx2, meqn, q1d, evl, evr, ql, qr);
+      break;
+    default: rc = -5;
+  }
+  if (rc) goto done;
+
+  rc = ocl_rp(p, ixy, mx, ql, qr, aux1d, aux1d, wave, s, amdq, apdq);        /* :122-123 */
+  if (rc) goto done;
+
+  {
+    double c = 0.0;                                                           /* :126-133 */
+    for (int mw = 1; mw <= mwaves; ++mw)
+      for (int i = 1; i <= mx + 1; ++i) {
+        double a = dtdx[i + mbc - 1] * L2(s, i, mw);
+        double b = -dtdx[i + mbc - 2] * L2(s, i, mw);
+        c = dmax1(c, dmax1(a, b));
+      }
+    *cfl = c;
+  }
+
+  if (p->tfluct_solver == 1) {                                                /* :136-153 */
+    rc = ocl_tfluct(p, ixy, mx, ql, qr, aux1d, aux1d, s, amdq2);
+    if (rc) goto done;
+    for (int m = 1; m <= meqn; ++m)
+      for (int i = 1; i <= mx; ++i)
+        L2(dq1d, i, m) = L2(dq1d, i, m) -
+            dtdx[i + mbc - 1] * ((L2(apdq, i, m) + L2(amdq2, i, m)) + L2(amdq, i + 1, m));
+  } else {                                                                    /* :155-188 */
+    for (int i = 1 - mbc + 1; i <= mx + mbc; ++i)
+      for (int m = 1; m <= meqn; ++m) {
+        L2(qr, i - 1, m) = L2(ql, i, m);
+        L2(ql, i, m) = L2(qr, i, m);
+      }
+    if (maux > 0)
+      for (int i = 1 - mbc + 1; i <= mx + mbc; ++i)
+        for (int m = 1; m <= maux; ++m) {
+          L2(auxr, i - 1, m) = L2(aux1d, i, m);
+          L2(auxl, i, m) = L2(aux1d, i, m);
+        }
+    rc = ocl_rp(p, ixy, mx, ql, qr, auxl, auxr, wave, s, amdq2, apdq2);
+    if (rc) goto done;
+    for (int m = 1; m <= meqn; ++m)
+      for (int i = 1; i <= mx; ++i)
+        L2(dq1d, i, m) = L2(dq1d, i, m) -
+            dtdx[i + mbc - 1] * (((L2(amdq, i + 1, m) + L2(apdq, i, m)) + L2(amdq2, i, m)) + L2(apdq2, i, m));
+  }
+done:
+  free(dtdx); free(ql); free(qr); free(wave); free(s); free(amdq); free(apdq);
+  free(amdq2); free(apdq2); free(evl); free(evr); free(auxl); free(auxr);
+  return rc;
+}
+
+/* ======================================================================== */
+/* src/2d/flux2.f90:30-92                                                    */
+/* ======================================================================== */
+static int flux2(const ocl_params *p, const double *q, double *dq, const double *aux,
+                 double dt, double *cfl) {
+  const int mbc = p->mbc, nx = p->mx, ny = p->my, meqn = p->meqn, maux = p->maux;
+  const long ldx = nx + 2 * mbc, ldy = ny + 2 * mbc;
+  const long lmax = (ldx > ldy ? ldx : ldy);
+  double *q1d = (double *)calloc((size_t)lmax * meqn, sizeof(double));
+  double *dq1d = (double *)calloc((size_t)lmax * meqn, sizeof(double));
+  double *a1d = (double *)calloc((size_t)lmax * (maux > 0 ? maux : 1), sizeof(double));
+  int rc = 0;
+  if (!q1d || !dq1d || !a1d) { rc = -3; goto out; }
+  *cfl = 0.0;
+  for (int j = 0; j <= ny + 1; ++j) {                                          /* :36-62 */
+    for (int m = 1; m <= meqn; ++m)
+      for (int i = 1 - mbc; i <= nx + mbc; ++i) q1d[(i + mbc - 1) + (m - 1) * ldx] = G3(q, i, j, m);
+    for (int m = 1; m <= maux; ++m)
+      for (int i = 1 - mbc; i <= nx + mbc; ++i) a1d[(i + mbc - 1) + (m - 1) * ldx] = G3(aux, i, j, m);
+    double c1d;
+    rc = ocl_flux1(p, q1d, dq1d, a1d, dt, &c1d, 1, nx);
+    if (rc) goto out;
+    *cfl = dmax1(*cfl, c1d);
+    for (int m = 1; m <= meqn; ++m)
+      for (int i = 1; i <= nx; ++i) G3(dq, i, j, m) = G3(dq, i, j, m) + dq1d[(i + mbc - 1) + (m - 1) * ldx];
+  }
+  for (int i = 0; i <= nx + 1; ++i) {                                          /* :68-92 */
+    for (int m = 1; m <= meqn; ++m)
+      for (int j = 1 - mbc; j <= ny + mbc; ++j) q1d[(j + mbc - 1) + (m - 1) * ldy] = G3(q, i, j, m);
+    for (int m = 1; m <= maux; ++m)
+      for (int j = 1 - mbc; j <= ny + mbc; ++j) a1d[(j + mbc - 1) + (m - 1) * ldy] = G3(aux, i, j, m);
+    double c1d;
+    rc = ocl_flux1(p, q1d, dq1d, a1d, dt, &c1d, 2, ny);
+    if (rc) goto out;
+    *cfl = dmax1(*cfl, c1d);
+    for (int m = 1; m <= meqn; ++m)
+      for (int j = 1; j <= ny; ++j) G3(dq, i, j, m) = G3(dq, i, j, m) + dq1d[(j + mbc - 1) + (m - 1) * ldy];
+  }
+out:
+  free(q1d); free(dq1d); free(a1d);
+  return rc;
+}
+
+/* src/1d/step1d.f90:2-31, src/2d/step2d.f90:2-41 (with src1/src2 zeroing) */
+int ocl_step(const ocl_params *p, double *q, double *dq, const double *aux, double dt,
+             double t, double *cfl) {
+  (void)t;
+  int rc = ocl_bc(p, q);
+  if (rc) return rc;
+  const long n = ocl_plane(p) * p->meqn;
+  for (long k = 0; k < n; ++k) dq[k] = 0.0;   /* src: interior zeroed; ghosts unused */
+  if (p->ndim == 1) return ocl_flux1(p, q, dq, aux, dt, cfl, 1, p->mx);
+  return flux2(p, q, dq, aux, dt, cfl);
+}
+
+/* ======================================================================== */
+/* SSP-RK stages, src/sharpclaw.f90:247-464 (whole-array updates).           */
+/* ======================================================================== */
+int ocl_rk_step(const ocl_params *p, int ti, double *q, const double *qold,
+                const double *aux, double dt, double told, double *cfl) {
+  const long n = ocl_plane(p) * p->meqn;
+  double *r1 = (double *)calloc((size_t)n, sizeof(double));
+  double *r2 = (ti == 4) ? (double *)calloc((size_t)n, sizeof(double)) : NULL;
+  int rc = 0;
+  if (!r1 || (ti == 4 && !r2)) { free(r1); free(r2); return -3; }
+#define STEP(dst, tt) do { rc = ocl_step(p, q, (dst), aux, dt, (tt), cfl); if (rc) goto out; } while (0)
+  if (ti == 1) {                                           /* ts_ssp22 :247-276 */
+    const double c2 = 1.0;
+    STEP(r1, told);
+    for (long k = 0; k < n; ++k) q[k] = q[k] + r1[k];
+    STEP(r1, told + c2 * dt);
+    for (long k = 0; k < n; ++k) q[k] = 0.5 * ((qold[k] + q[k]) + r1[k]);
+  } else if (ti == 2) {                                    /* ts_ssp42 :280-333 */
+    const double third = 1.0 / 3.0, a21 = third, b4 = 0.25;
+    STEP(r1, told);
+    for (long k = 0; k < n; ++k) q[k] = q[k] + a21 * r1[k];
+    STEP(r1, told + third * dt);
+    for (long k = 0; k < n; ++k) q[k] = q[k] + third * r1[k];
+    STEP(r1, told + (2.0 * third) * dt);
+    for (long k = 0; k < n; ++k) q[k] = q[k] + third * r1[k];
+    STEP(r1, told + 1.0 * dt);
+    for (long k = 0; k < n; ++k) q[k] = (0.25 * qold[k] + 0.75 * q[k]) + b4 * r1[k];
+  } else if (ti == 3) {                                    /* ts_ssp33 :337-376 */
+    STEP(r1, told);
+    for (long k = 0; k < n; ++k) q[k] = q[k] + r1[k];
+    STEP(r1, told + 1.0 * dt);
+    for (long k = 0; k < n; ++k) q[k] = 0.75 * qold[k] + 0.25 * (q[k] + r1[k]);
+    STEP(r1, told + 0.5 * dt);
+    for (long k = 0; k < n; ++k) q[k] = (qold[k] + 2.0 * (q[k] + r1[k])) / 3.0;
+  } else if (ti == 4) {                                    /* ts_ssp104 :380-464 */
+    const double c6 = 1.0 / 6.0;
+    double that = told;
+    STEP(r1, that);
+    for (long k = 0; k < n; ++k) q[k] = q[k] + c6 * r1[k];
+    that = told + dt / 6.0;
+    STEP(r1, that);
+    for (long k = 0; k < n; ++k) q[k] = q[k] + c6 * r1[k];
+    that = told + dt / 3.0;
+    STEP(r1, that);
+    for (long k = 0; k < n; ++k) q[k] = q[k] + c6 * r1[k];
+    that = told + 0.5 * dt;
+    STEP(r1, that);
+    for (long k = 0; k < n; ++k) q[k] = q[k] + c6 * r1[k];
+    that = told + (2.0 / 3.0) * dt;
+    STEP(r1, that);
+    for (long k = 0; k < n; ++k) {
+      r2[k] = q[k] + c6 * r1[k];
+      r1[k] = 0.04 * qold[k] + 0.36 * r2[k];
+      q[k] = 0.6 * qold[k] + 0.4 * r2[k];
+    }
+    that = told + (1.0 / 3.0) * dt;
+    STEP(r2, that);
+    for (long k = 0; k < n; ++k) q[k] = q[k] + c6 * r2[k];
+    that = told + 0.5 * dt;
+    STEP(r2, that);
+    for (long k = 0; k < n; ++k) q[k] = q[k] + c6 * r2[k];
+    that = told + (2.0 / 3.0) * dt;
+    STEP(r2, that);
+    for (long k = 0; k < n; ++k) q[k] = q[k] + c6 * r2[k];
+    that = told + (5.0 / 6.0) * dt;
+    STEP(r2, that);
+    for (long k = 0; k < n; ++k) q[k] = q[k] + c6 * r2[k];
+    that = told + dt;
+    STEP(r2, that);
+    for (long k = 0; k < n; ++k) q[k] = (r1[k] + 0.6 * q[k]) + 0.1 * r2[k];
+  } else {
+    rc = -6;
+  }
+#undef STEP
+out:
+  free(r1);
+  free(r2);
+  return rc;
+}
+
+/* ======================================================================== */
+/* src/sharpclaw.f90:2-243 driver                                            */
+/* ======================================================================== */
+int ocl_sharpclaw(const ocl_params *p, const ocl_run *run, double *q, const double *aux,
+                  ocl_result *res) {
+  const long n = ocl_plane(p) * p->meqn;
+  double tstart = run->tstart, tend = run->tend;
+  double t = tstart, told = tstart, dt = run->dt_initial, cfl = 0.0, cflmax = 0.0;
+  double dtmin = dt, dtmax = dt;
+  int maxn = run->max_steps, info = 0, steps = 0, rejected = 0, retake = 0, rc = 0;
+  memset(res, 0, sizeof(*res));
+  if (run->dt_variable == 0) {                                                 /* :44-58 */
+    if (tend < tstart) maxn = 1;
+    else {
+      maxn = (int)((tend - tstart + 1e-10) / dt);
+      if (fabs(maxn * dt - (tend - tstart)) > 1e-5 * (tend - tstart)) { res->info = 2; return 0; }
+    }
+  }
+  if (run->dt_variable == 1 && run->cfl_desired > run->cfl_max) { res->info = 3; return 0; }
+  double *qold = (double *)malloc(sizeof(double) * (size_t)n);
+  if (!qold) return -3;
+  for (int it = 1; it <= maxn; ++it) {                                          /* :118-222 */
+    if (!retake) {
+      told = t;
+      if (told + dt > tend && tstart < tend) dt = tend - told;
+      /* b4step: default no-op (src/b4step.f90) */
+      memcpy(qold, q, sizeof(double) * (size_t)n);
+    }
+    retake = 0;
+    t = told + dt;
+    if (p->ndim == 1) { rc = ocl_bc(p, q); if (rc) break; }
+    rc = ocl_rk_step(p, run->time_integrator, q, qold, aux, dt, told, &cfl);
+    if (rc) break;
+    if (run->dt_variable == 1) {                                               /* :184-192 */
+      if (cfl > 0.0) {
+        dt = dmin1(run->dt_max, dt * run->cfl_desired / cfl);
+        dtmin = dmin1(dt, dtmin);
+        dtmax = dmax1(dt, dtmax);
+      } else {
+        dt = run->dt_max;
+      }
+    }
+    if (cfl <= run->cfl_max) {                                                 /* :195-216 */
+      cflmax = dmax1(cfl, cflmax);
+    } else {
+      t = told;
+      memcpy(q, qold, sizeof(double) * (size_t)n);
+      ++rejected;
+      if (run->dt_variable == 1) retake = 1;
+      else { cflmax = dmax1(cfl, cflmax); break; }
+    }
+    steps = steps + 1;
+    if (t >= tend) break;
+  }
+  free(qold);
+  if (rc) return rc;
+  if (run->dt_variable == 1 && t < tend && steps == maxn) info = 11;           /* :225 */
+  if (run->dt_variable == 0 && cflmax > run->cfl_max) info = 12;               /* :228 */
+  res->tend = t;
+  res->cfl_maxused = cflmax;
+  res->cfl_last = cfl;
+  res->dt_minused = dtmin;
+  res->dt_maxused = dtmax;
+  res->dt_last = dt;
+  res->steps_taken = steps;
+  res->info = info;
+  res->rejected = rejected;
+  return 0;
+}

@@ -1,0 +1,107 @@
+/*
+ * sclaw_oracle.h -- CPU oracle for the SharpClaw semi-discrete WENO step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product (sharpclaw_b200/, include/)
+ * links or calls this code; only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / reference legs of bench.py load it, as the checker.
+ *
+ * The oracle restates, array by array and loop by loop, the reference Fortran:
+ *   src/flux1.f90, src/reconstruct.f90 (weno5, weno5_char), src/2d/flux2.f90,
+ *   src/1d/bc1.f90, src/2d/bc2.f90, src/1d/src1.f90, src/2d/src2.f90,
+ *   src/1d/step1d.f90, src/2d/step2d.f90, src/sharpclaw.f90 (driver + ts_ssp*),
+ * and the application plugins named in sclaw_oracle.c.  Arrays use the
+ * reference layout: Fortran column-major with lower bound 1-mbc, i.e. element
+ * (i,m) of a 1-D field is at (i+mbc-1) + (m-1)*(mx+2*mbc), and element (i,j,m)
+ * of a 2-D field is at (i+mbc-1) + (j+mbc-1)*(mx+2*mbc) + (m-1)*(mx+2*mbc)*(my+2*mbc).
+ *
+ * Parity status: the reference ships no golden vectors and no Fortran compiler
+ * exists on this machine, so the restatement is pinned by the reference's own
+ * known-answer test (the exact acoustics interface solution used by
+ * apps/acoustics/1d/interface/sharpclawtest.py) and by analytic invariants.
+ */
+#ifndef SCLAW_ORACLE_H
+#define SCLAW_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Plugin families (device and oracle share the numbering). */
+enum {
+  OCL_RP_ADVECTION = 1,     /* apps/advection/1d/{rp1.f,tfluct1.f,evec.f}            */
+  OCL_RP_EULER = 2,         /* apps/euler/shockentropy/rp1eu.f + new Roe evec          */
+  OCL_RP_SW2D = 3,          /* apps/shallowWater/2dRadialDam/{rpn2sw.f,tfluct1sw.f}   */
+  OCL_RP_ACOUSTICS1D = 4,   /* apps/acoustics/1d/interface/{rp1acv,tfluct1acv,evec}   */
+  OCL_RP_ACOUSTICS2D = 5    /* new 2-D variable-coefficient acoustics rpn2/tfluct/evec */
+};
+
+typedef struct {
+  int ndim;             /* 1 or 2                                  ClawParams%ndim  */
+  int mx, my;           /* interior cells                          ClawParams%nx    */
+  int meqn, mwaves, mbc, maux, mcapa;
+  int lim_type;         /* only 2 (WENO) is on the path                              */
+  int char_decomp;      /* 0 componentwise, 2 characteristic-wise                   */
+  int tfluct_solver;    /* 1: tfluct plugin, 0: swap + second rp                    */
+  int mthbc[4];         /* 1 extrap, 2 periodic, 3 wall                              */
+  double dx, dy, xlower, ylower;
+  int rp;               /* OCL_RP_* */
+  int efix;             /* entropy fix flag (Euler default 1, SW default 0)          */
+  double u;             /* advection speed        common /comrp/ u                  */
+  double gamma;         /* ratio of specific heats common /param/ gamma,gamma1       */
+  double grav;          /* gravity                 common /comrp/ g                  */
+} ocl_params;
+
+typedef struct {
+  double tstart, tend;
+  double dt_initial, dt_max, cfl_max, cfl_desired;
+  int max_steps, dt_variable, time_integrator;
+} ocl_run;
+
+typedef struct {
+  double tend;          /* time reached */
+  double cfl_maxused, cfl_last, dt_minused, dt_maxused, dt_last;
+  int steps_taken, info, rejected;
+} ocl_result;
+
+/* size of a field with ghost cells (number of doubles per component) */
+long ocl_plane(const ocl_params *p);
+
+int ocl_bc(const ocl_params *p, double *q);
+
+/* reconstruct.f90 weno5 / weno5_char on one line of mx2 = mx+2*mbc cells.
+ * q, ql, qr: (mx2, meqn); evl, evr: (mx2, meqn, meqn). */
+int ocl_weno5(int mx2, int meqn, const double *q, double *ql, double *qr);
+int ocl_weno5_char(int mx2, int meqn, const double *q, const double *evl,
+                   const double *evr, double *ql, double *qr);
+
+/* plugin calls on one line (Fortran loop ranges i = 2-mbc .. mx+mbc) */
+int ocl_rp(const ocl_params *p, int ixy, int mx, const double *ql, const double *qr,
+           const double *auxl, const double *auxr, double *wave, double *s,
+           double *amdq, double *apdq);
+int ocl_tfluct(const ocl_params *p, int ixy, int mx, const double *ql, const double *qr,
+               const double *auxl, const double *auxr, double *s, double *adq);
+int ocl_evec(const ocl_params *p, int ixy, int mx, const double *q, const double *auxl,
+             const double *auxr, double *evl, double *evr);
+
+/* flux1.f90: one line of mx cells; dq1d (mx+2mbc, meqn) is accumulated into
+ * exactly as the reference does (zeroed first when ndim > 1). */
+int ocl_flux1(const ocl_params *p, const double *q1d, double *dq1d, const double *aux1d,
+              double dt, double *cfl, int ixy, int mx);
+
+/* step1d/step2d: bc (in place on q), src (zero interior dq), flux1/flux2 */
+int ocl_step(const ocl_params *p, double *q, double *dq, const double *aux, double dt,
+             double t, double *cfl);
+
+/* one time step of the SSP-RK integrator (ts_ssp22/42/33/104), q updated in
+ * place, qold must hold q on entry (sharpclaw.f90:132-135). */
+int ocl_rk_step(const ocl_params *p, int time_integrator, double *q, const double *qold,
+                const double *aux, double dt, double told, double *cfl);
+
+/* sharpclaw.f90:2-243 driver (b4step is the default no-op). */
+int ocl_sharpclaw(const ocl_params *p, const ocl_run *run, double *q, const double *aux,
+                  ocl_result *res);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,250 @@
+"""sharpclaw_b200 -- SharpClaw's semi-discrete WENO step on NVIDIA B200 (sm_100a).
+
+Host-side mirror of the reference's operator interface for the hot path:
+
+===========================  ==============================================
+reference (Fortran)          here
+===========================  ==============================================
+module ClawParams            :class:`ClawParams`
+step (1d/step1d.f90,         :meth:`Solver.step`   -> (q with ghosts, dq, cfl)
+      2d/step2d.f90)
+flux1 (src/flux1.f90)        :meth:`Solver.flux1`  -> (dq1d, cfl)
+ts_ssp22/42/33/104           :meth:`Solver.rk_step`
+sharpclaw (src/sharpclaw.f90) :meth:`Solver.sharpclaw` / :func:`sharpclaw`
+===========================  ==============================================
+
+Arrays use the reference layout: numpy float64 arrays of shape
+``(meqn, mx+2*mbc)`` (1-D) or ``(meqn, my+2*mbc, mx+2*mbc)`` (2-D), C order,
+which is byte-for-byte the Fortran column-major ``q(1-mbc:mx+mbc[,1-mbc:my+mbc],meqn)``.
+All compute runs in the CUDA library; a missing library is an error.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _capi as C
+from ._capi import (FP32, FP64, FP64_STRICT, MIXED, RP_ACOUSTICS1D, RP_ACOUSTICS2D,  # noqa: F401
+                    RP_ADVECTION, RP_EULER, RP_SW2D, SharpClawError)
+
+__all__ = ["ClawParams", "Solver", "sharpclaw", "SharpClawError", "RP_ADVECTION", "RP_EULER",
+           "RP_SW2D", "RP_ACOUSTICS1D", "RP_ACOUSTICS2D"]
+
+# plugin id -> (meqn, mwaves, maux, ndim)
+PLUGINS = {
+    RP_ADVECTION: (1, 1, 0, 1),
+    RP_EULER: (3, 3, 0, 1),
+    RP_SW2D: (3, 3, 0, 2),
+    RP_ACOUSTICS1D: (2, 2, 2, 1),
+    RP_ACOUSTICS2D: (3, 2, 2, 2),
+}
+
+
+@dataclass
+class ClawParams:
+    """Module ClawParams (src/ClawParams.f90:1-16) plus the plugin COMMON
+    blocks (/comrp/ u or g, /param/ gamma) and the integrator choice."""
+    rp: int
+    mx: int
+    dx: float
+    my: int = 1
+    dy: float = 1.0
+    ndim: Optional[int] = None
+    meqn: Optional[int] = None
+    mwaves: Optional[int] = None
+    maux: Optional[int] = None
+    mbc: int = 3
+    mcapa: int = 0
+    lim_type: int = 2
+    char_decomp: int = 0
+    tfluct_solver: int = 1
+    mthbc: Sequence[int] = field(default_factory=lambda: (2, 2, 2, 2))
+    xlower: float = 0.0
+    ylower: float = 0.0
+    efix: Optional[int] = None
+    u: float = 1.0
+    gamma: float = 1.4
+    grav: float = 1.0
+    time_integrator: int = 3
+
+    def __post_init__(self):
+        meqn, mwaves, maux, ndim = PLUGINS.get(self.rp, (None, None, 0, None))
+        if self.meqn is None:
+            self.meqn = meqn
+        if self.mwaves is None:
+            self.mwaves = mwaves
+        if self.maux is None:
+            self.maux = maux
+        if self.ndim is None:
+            self.ndim = ndim
+        if self.efix is None:
+            self.efix = 1 if self.rp == RP_EULER else 0
+        if self.ndim == 1:
+            self.my = 1
+
+    def shape(self, ncomp: Optional[int] = None):
+        n = self.meqn if ncomp is None else ncomp
+        if self.ndim == 1:
+            return (n, self.mx + 2 * self.mbc)
+        return (n, self.my + 2 * self.mbc, self.mx + 2 * self.mbc)
+
+    def to_c(self, precision: int) -> C.scl_params:
+        p = C.scl_params()
+        p.ndim, p.mx, p.my = self.ndim, self.mx, self.my
+        p.meqn, p.mwaves, p.mbc, p.maux, p.mcapa = self.meqn, self.mwaves, self.mbc, self.maux, self.mcapa
+        p.lim_type, p.char_decomp, p.tfluct_solver = self.lim_type, self.char_decomp, self.tfluct_solver
+        for k in range(4):
+            p.mthbc[k] = int(self.mthbc[k]) if k < len(self.mthbc) else 2
+        p.dx, p.dy, p.xlower, p.ylower = self.dx, self.dy, self.xlower, self.ylower
+        p.rp, p.efix = self.rp, int(self.efix)
+        p.u, p.gamma, p.grav = self.u, self.gamma, self.grav
+        p.time_integrator, p.precision = self.time_integrator, precision
+        return p
+
+
+def _ptr(a: Optional[np.ndarray]):
+    if a is None:
+        return ctypes.POINTER(ctypes.c_double)()
+    if a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise TypeError("arrays must be C-contiguous float64 in the reference layout")
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _precision(precision) -> int:
+    if isinstance(precision, str):
+        return C.PRECISIONS[precision]
+    return int(precision)
+
+
+class Solver:
+    """One grid on the current CUDA device (a handle of the C ABI)."""
+
+    def __init__(self, params: ClawParams, precision="fp64"):
+        self.params = params
+        self.precision = _precision(precision)
+        self._cp = params.to_c(self.precision)
+        h = ctypes.c_void_p()
+        C.check(C.lib().scl_create(ctypes.byref(self._cp), ctypes.byref(h)), "scl_create")
+        self._h = h
+
+    # -- lifetime ---------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            C.lib().scl_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state ------------------------------------------------------------------
+    def _check_field(self, a, ncomp=None):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if a.shape != self.params.shape(ncomp):
+            raise ValueError(f"expected shape {self.params.shape(ncomp)}, got {a.shape}")
+        return a
+
+    def set_q(self, q):
+        q = self._check_field(q)
+        C.check(C.lib().scl_set_q(self._h, _ptr(q)), "scl_set_q")
+
+    def get_q(self) -> np.ndarray:
+        q = np.empty(self.params.shape(), dtype=np.float64)
+        C.check(C.lib().scl_get_q(self._h, _ptr(q)), "scl_get_q")
+        return q
+
+    def set_aux(self, aux):
+        if self.params.maux == 0:
+            return
+        aux = self._check_field(aux, self.params.maux)
+        C.check(C.lib().scl_set_aux(self._h, _ptr(aux)), "scl_set_aux")
+
+    # -- operators ----------------------------------------------------------------
+    def step(self, q, dt: float, t: float = 0.0):
+        """step1d/step2d: bc + src + flux1/flux2.  Returns (q with ghost cells
+        filled, dq = dt*L(q) on interior cells, cfl)."""
+        q = self._check_field(q).copy()
+        dq = np.zeros_like(q)
+        cfl = ctypes.c_double(0.0)
+        C.check(C.lib().scl_step_dq(self._h, _ptr(q), _ptr(dq), dt, t, ctypes.byref(cfl)), "scl_step_dq")
+        return q, dq, cfl.value
+
+    def flux1(self, q1d, dt: float, aux1d=None, ixy: int = 1):
+        """flux1.f90 on one line: q1d shape (meqn, mx+2mbc); returns (dq1d, cfl)."""
+        q1d = np.ascontiguousarray(q1d, dtype=np.float64)
+        meqn, ld = q1d.shape
+        mx = ld - 2 * self.params.mbc
+        a = None if aux1d is None else np.ascontiguousarray(aux1d, dtype=np.float64)
+        dq = np.zeros_like(q1d)
+        cfl = ctypes.c_double(0.0)
+        C.check(C.lib().scl_flux1(self._h, _ptr(q1d), _ptr(a), _ptr(dq), dt, ixy, mx, ctypes.byref(cfl)),
+                "scl_flux1")
+        return dq, cfl.value
+
+    def rk_step(self, dt: float, told: float = 0.0) -> float:
+        """One SSP-RK step on the device-resident q; returns the last stage's CFL."""
+        cfl = ctypes.c_double(0.0)
+        C.check(C.lib().scl_rk_step(self._h, dt, told, ctypes.byref(cfl)), "scl_rk_step")
+        return cfl.value
+
+    @staticmethod
+    def _run(tstart, tend, dt_initial, dt_max, cfl_max, cfl_desired, max_steps, dt_variable):
+        return C.scl_run(tstart, tend, dt_initial, dt_max, cfl_max, cfl_desired, max_steps, dt_variable)
+
+    def sharpclaw(self, tstart: float, tend: float, dt_initial: float, cfl_max: float,
+                  cfl_desired: float, dt_max: float = 1e99, max_steps: int = 50000,
+                  dt_variable: int = 1) -> dict:
+        """The time loop of sharpclaw() on the device; returns its outputs."""
+        run = self._run(tstart, tend, dt_initial, dt_max, cfl_max, cfl_desired, max_steps, dt_variable)
+        res = C.scl_result()
+        rc = C.lib().scl_sharpclaw(self._h, ctypes.byref(run), ctypes.byref(res))
+        if rc not in (C.SCL_OK, C.SCL_E_NONFINITE):
+            C.check(rc, "scl_sharpclaw")
+        return {k: getattr(res, k) for k, _ in C.scl_result._fields_}
+
+    def time_steps(self, nsteps: int, dt_initial: float, cfl_max: float, cfl_desired: float,
+                   tend: float = 1e30, dt_variable: int = 1):
+        """Run exactly `nsteps` controller steps from the device-resident state and
+        return (elapsed device ms, result dict)."""
+        run = self._run(0.0, tend, dt_initial, 1e99, cfl_max, cfl_desired, nsteps, dt_variable)
+        res = C.scl_result()
+        ms = ctypes.c_float(0.0)
+        C.check(C.lib().scl_time_steps(self._h, ctypes.byref(run), nsteps, ctypes.byref(ms),
+                                       ctypes.byref(res)), "scl_time_steps")
+        return ms.value, {k: getattr(res, k) for k, _ in C.scl_result._fields_}
+
+
+    def time_stages(self, dt: float, reps: int):
+        """Time `reps` passes of the stage kernels (no controller, state not
+        advanced); returns (elapsed device ms, number of kernel launches)."""
+        ms = ctypes.c_float(0.0)
+        n = ctypes.c_longlong(0)
+        C.check(C.lib().scl_time_stages(self._h, dt, reps, ctypes.byref(ms), ctypes.byref(n)),
+                "scl_time_stages")
+        return ms.value, n.value
+
+    @property
+    def kernels_per_step(self) -> int:
+        return C.lib().scl_kernels_per_step(self._h)
+
+
+def sharpclaw(params: ClawParams, q, aux=None, *, tstart: float, tend: float, dt_initial: float,
+              cfl_max: float, cfl_desired: float, dt_max: float = 1e99, max_steps: int = 50000,
+              dt_variable: int = 1, precision="fp64"):
+    """Functional form of sharpclaw(): returns (q at the final time, outputs)."""
+    with Solver(params, precision) as s:
+        s.set_aux(aux) if aux is not None else None
+        s.set_q(q)
+        res = s.sharpclaw(tstart, tend, dt_initial, cfl_max, cfl_desired, dt_max, max_steps, dt_variable)
+        return s.get_q(), res

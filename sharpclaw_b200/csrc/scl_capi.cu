@@ -1,0 +1,807 @@
+// scl_capi.cu -- C ABI of the SharpClaw B200 step (include/sharpclaw_cuda.h).
+//
+// Host side of the drop-in boundary: handle lifetime, the device layout,
+// host<->device transfers, the integrator stage tables of src/sharpclaw.f90
+// and the device-resident time loop (controller kernels + CUDA graphs).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "scl_common.cuh"
+#include "scl_launch.h"
+
+using namespace scl;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(SCL_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Controller kernels: one thread each, src/sharpclaw.f90:118-221.
+// ---------------------------------------------------------------------------
+__global__ void k_begin_step(Ctl* c) {
+  if (c->done) return;
+  if (c->n_iter >= c->maxn) { c->done = 1; return; }   // do n=1,maxn exhausted
+  c->n_iter += 1;
+  if (!c->retake) {
+    c->told = c->t;                                                  // :120
+    if (c->told + c->dt > c->tend && c->tstart < c->tend) c->dt = c->tend - c->told;  // :124
+    // b4step: default no-op (src/b4step.f90); qold = q is the Q role (:132-135)
+  }
+  c->retake = 0;
+  c->t = c->told + c->dt;                                            // :139
+  for (int s = 0; s < MAXSTAGES; ++s) c->stage_cfl[s] = 0.0;
+}
+
+__global__ void k_end_step(Ctl* c, int last_stage, int final_role) {
+  if (c->done) return;
+  const double cfl = c->stage_cfl[last_stage];   // the last stage's CFL (:184, A2)
+  c->cfl_last = cfl;
+  // A NaN CFL number cannot drive dt control (the reference would reject and
+  // retake with a NaN or dt_max step forever): stop with q = qold.
+  if (cfl != cfl) {
+    c->status |= SCL_STATUS_NONFINITE;
+    c->info = SCL_INFO_NONFINITE;
+    c->t = c->told;
+    c->done = 1;
+    return;
+  }
+  // Non-finite stage outputs matter only if the step is accepted; a rejected
+  // step's stages are discarded (q = qold) as in the reference.
+  if (cfl <= c->cfl_max && (c->status & SCL_STATUS_NONFINITE)) {
+    c->info = SCL_INFO_NONFINITE;
+    c->t = c->told;
+    c->done = 1;
+    return;
+  }
+  c->status &= ~SCL_STATUS_NONFINITE;
+  if (c->dt_variable == 1) {                                        // :184-192
+    if (cfl > 0.0) {
+      c->dt = fmin(c->dt_max, c->dt * c->cfl_desired / cfl);
+      c->dtmin = fmin(c->dt, c->dtmin);
+      c->dtmax = fmax(c->dt, c->dtmax);
+    } else {
+      c->dt = c->dt_max;
+    }
+  }
+  if (cfl <= c->cfl_max) {                                          // :195-197 accept
+    c->cflmax = fmax(cfl, c->cflmax);
+    const int tmp = c->role[ROLE_Q];
+    c->role[ROLE_Q] = c->role[final_role];
+    c->role[final_role] = tmp;
+  } else {                                                          // :198-216 reject
+    c->t = c->told;
+    c->rejected += 1;
+    if (c->dt_variable == 1) {
+      c->retake = 1;
+    } else {
+      c->cflmax = fmax(cfl, c->cflmax);
+      c->done = 1;
+      return;
+    }
+  }
+  c->steps_taken += 1;                                              // :219
+  if (c->t >= c->tend) c->done = 1;                                 // :220
+}
+
+// bc1.f90 on device (initial fill after an upload); one thread per (m, ibc)
+template <class S>
+__global__ void k_bc1(S* q, long plane, int mx, int meqn, int bl, int br) {
+  const int t = threadIdx.x;
+  if (t >= meqn * 3) return;
+  const int m = t / 3, ibc = t % 3 + 1;
+  S* p = q + (long)m * plane;
+  auto at = [&](int i) -> S& { return p[i + 2]; };
+  if (bl == 1) at(1 - ibc) = at(1);
+  else if (bl == 2) at(1 - ibc) = at(mx + 1 - ibc);
+  else if (bl == 3) at(1 - ibc) = (m == 1) ? -at(ibc) : at(ibc);
+  if (br == 1) at(mx + ibc) = at(mx);
+  else if (br == 2) at(mx + ibc) = at(ibc);
+  else if (br == 3) at(mx + ibc) = (m == 1) ? -at(mx + 1 - ibc) : at(mx + 1 - ibc);
+}
+
+// bc2.f90 x-sides (all rows j = 1-mbc..ny+mbc), then y-sides (all columns)
+template <class S>
+__global__ void k_bc2(S* q, long plane, long pitch, int nx, int ny, int meqn, int b0, int b1,
+                      int ydir) {
+  const int len = ydir ? nx + 6 : ny + 6;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= meqn * 3 * len) return;
+  const int k = t % len, ibc = (t / len) % 3 + 1, m = t / (3 * len);
+  S* p = q + (long)m * plane;
+  const int n = ydir ? ny : nx;
+  const int neg_m = ydir ? 2 : 1;
+  auto at = [&](int c) -> S& {
+    return ydir ? p[(long)(c + 2) * pitch + k] : p[(long)(k) * pitch + c + 2];
+  };
+  if (b0 == 1) at(1 - ibc) = at(1);
+  else if (b0 == 2) at(1 - ibc) = at(n + 1 - ibc);
+  else if (b0 == 3) at(1 - ibc) = (m == neg_m) ? -at(ibc) : at(ibc);
+  if (b1 == 1) at(n + ibc) = at(n);
+  else if (b1 == 2) at(n + ibc) = at(ibc);
+  else if (b1 == 3) at(n + ibc) = (m == neg_m) ? -at(n + 1 - ibc) : at(n + 1 - ibc);
+}
+
+__global__ void k_f64_to_f32(const double* a, float* b, long n) {
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
+    b[k] = (float)a[k];
+}
+__global__ void k_f32_to_f64(const float* a, double* b, long n) {
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
+    b[k] = (double)a[k];
+}
+
+bool get_launchers(int prec, int rp, int ndim, int cd, int tf, int variant, Launchers* L) {
+  switch (prec) {
+    case SCL_FP64: return get_launchers_fp64(rp, ndim, cd, tf, variant, L);
+    case SCL_FP64_STRICT: return get_launchers_fp64s(rp, ndim, cd, tf, variant, L);
+    case SCL_MIXED: return get_launchers_mixed(rp, ndim, cd, tf, variant, L);
+    case SCL_FP32: return get_launchers_fp32(rp, ndim, cd, tf, variant, L);
+  }
+  return false;
+}
+
+// Stage tables of ts_ssp22/42/33/104 (src/sharpclaw.f90:247-464) with the
+// register rotation; `final` is the role holding q^{n+1}.
+int stage_table(int ti, StageDesc* sd, int* final_role) {
+  auto S = [](int k, int in, int out, int out2, int ai) { return StageDesc{k, in, out, out2, ai}; };
+  int n = 0;
+  switch (ti) {
+    case 1:
+      sd[n++] = S(SK_ADD, ROLE_Q, ROLE_A, -1, -1);
+      sd[n++] = S(SK_SSP22_2, ROLE_A, ROLE_B, -1, ROLE_Q);
+      *final_role = ROLE_B;
+      break;
+    case 2:
+      sd[n++] = S(SK_ADD_THIRD, ROLE_Q, ROLE_A, -1, -1);
+      sd[n++] = S(SK_ADD_THIRD, ROLE_A, ROLE_B, -1, -1);
+      sd[n++] = S(SK_ADD_THIRD, ROLE_B, ROLE_A, -1, -1);
+      sd[n++] = S(SK_SSP42_4, ROLE_A, ROLE_B, -1, ROLE_Q);
+      *final_role = ROLE_B;
+      break;
+    case 3:
+      sd[n++] = S(SK_ADD, ROLE_Q, ROLE_A, -1, -1);
+      sd[n++] = S(SK_SSP33_2, ROLE_A, ROLE_B, -1, ROLE_Q);
+      sd[n++] = S(SK_SSP33_3, ROLE_B, ROLE_A, -1, ROLE_Q);
+      *final_role = ROLE_A;
+      break;
+    case 4:
+      sd[n++] = S(SK_ADD_SIXTH, ROLE_Q, ROLE_A, -1, -1);
+      sd[n++] = S(SK_ADD_SIXTH, ROLE_A, ROLE_B, -1, -1);
+      sd[n++] = S(SK_ADD_SIXTH, ROLE_B, ROLE_A, -1, -1);
+      sd[n++] = S(SK_ADD_SIXTH, ROLE_A, ROLE_B, -1, -1);
+      sd[n++] = S(SK_SSP104_5, ROLE_B, ROLE_A, ROLE_R1, ROLE_Q);
+      sd[n++] = S(SK_ADD_SIXTH, ROLE_A, ROLE_B, -1, -1);
+      sd[n++] = S(SK_ADD_SIXTH, ROLE_B, ROLE_A, -1, -1);
+      sd[n++] = S(SK_ADD_SIXTH, ROLE_A, ROLE_B, -1, -1);
+      sd[n++] = S(SK_ADD_SIXTH, ROLE_B, ROLE_A, -1, -1);
+      sd[n++] = S(SK_SSP104_10, ROLE_A, ROLE_B, -1, ROLE_R1);
+      *final_role = ROLE_B;
+      break;
+    default:
+      return 0;
+  }
+  return n;
+}
+
+}  // namespace
+
+struct scl_handle {
+  scl_params p{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  size_t ssize = 8;      // bytes per stored value
+  long ld = 0;           // reference row length (mx+2mbc)
+  long rows = 1;         // rows per plane (my+2mbc in 2-D)
+  long pitch = 0;        // device row pitch (elements)
+  long plane = 0;        // elements per component plane
+  void* buf[NROLES] = {nullptr, nullptr, nullptr, nullptr};
+  void* aux = nullptr;
+  double* stage64 = nullptr;   // double staging (FP32 storage) and dq output
+  Ctl* ctl = nullptr;          // device controller
+  Ctl* hctl = nullptr;         // pinned host mirror
+  int* hdone = nullptr;        // pinned flag
+  Launchers L{};
+  int variant = 0;
+  StageDesc sd[MAXSTAGES];
+  int nstages = 0, final_role = ROLE_A;
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t evq[2] = {nullptr, nullptr};
+};
+
+namespace {
+
+StageArgs make_args(const scl_handle* h, int s) {
+  StageArgs a{};
+  a.ctl = h->ctl;
+  for (int r = 0; r < NROLES; ++r) a.buf[r] = h->buf[r];
+  a.aux = h->aux;
+  a.dq_out = h->stage64;
+  a.sd = h->sd[s];
+  a.stage = s;
+  a.ixy = 1;
+  a.mx = h->p.mx;
+  a.my = h->p.ndim == 2 ? h->p.my : 1;
+  a.pitch = h->pitch;
+  a.plane = h->plane;
+  a.dx = h->p.dx;
+  a.dy = h->p.dy;
+  for (int k = 0; k < 4; ++k) a.mthbc[k] = h->p.mthbc[k];
+  a.mcapa = h->p.mcapa;
+  a.ph.u = h->p.u;
+  a.ph.gamma = h->p.gamma;
+  a.ph.gamma1 = h->p.gamma - 1.0;
+  a.ph.grav = h->p.grav;
+  a.ph.efix = h->p.efix;
+  return a;
+}
+
+int upload_ctl(scl_handle* h) {
+  CK(cudaMemcpyAsync(h->ctl, h->hctl, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream));
+  return SCL_OK;
+}
+int download_ctl(scl_handle* h) {
+  CK(cudaMemcpyAsync(h->hctl, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return SCL_OK;
+}
+
+// enqueue the stages of one RK step on the handle's stream
+int enqueue_stages(scl_handle* h) {
+  for (int s = 0; s < h->nstages; ++s) {
+    StageArgs a = make_args(h, s);
+    h->L.stage(a, h->stream);
+    if (h->L.ghost && s == h->nstages - 1) h->L.ghost(a, h->stream);
+  }
+  CK(cudaGetLastError());
+  return SCL_OK;
+}
+
+int enqueue_step(scl_handle* h) {
+  k_begin_step<<<1, 1, 0, h->stream>>>(h->ctl);
+  int rc = enqueue_stages(h);
+  if (rc) return rc;
+  k_end_step<<<1, 1, 0, h->stream>>>(h->ctl, h->nstages - 1, h->final_role);
+  CK(cudaGetLastError());
+  return SCL_OK;
+}
+
+int kernels_per_step(const scl_handle* h) { return h->nstages + 2 + (h->L.ghost ? 1 : 0); }
+
+// Capture `steps` controller steps (begin, stages, end) into one executable
+// graph; rebuilt only when a different step count is asked for.
+int build_graph(scl_handle* h, int steps) {
+  if (h->graph && h->graph_steps == steps) return SCL_OK;
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  h->graph_steps = steps;
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = SCL_OK;
+  for (int k = 0; k < steps && rc == SCL_OK; ++k) rc = enqueue_step(h);
+  cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+  if (e != cudaSuccess) return fail(SCL_E_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&h->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(SCL_E_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+  return SCL_OK;
+}
+
+int default_graph_steps(const scl_handle* h) { return std::max(1, 160 / kernels_per_step(h)); }
+
+template <class S>
+void launch_bc(scl_handle* h, S* q) {
+  const scl_params& p = h->p;
+  if (p.ndim == 1) {
+    k_bc1<S><<<1, 32, 0, h->stream>>>(q, h->plane, p.mx, p.meqn, p.mthbc[0], p.mthbc[1]);
+  } else {
+    int n = p.meqn * 3 * (p.my + 6);
+    k_bc2<S><<<(n + 255) / 256, 256, 0, h->stream>>>(q, h->plane, h->pitch, p.mx, p.my, p.meqn,
+                                                      p.mthbc[0], p.mthbc[1], 0);
+    n = p.meqn * 3 * (p.mx + 6);
+    k_bc2<S><<<(n + 255) / 256, 256, 0, h->stream>>>(q, h->plane, h->pitch, p.mx, p.my, p.meqn,
+                                                      p.mthbc[2], p.mthbc[3], 1);
+  }
+}
+
+// host (reference layout, double) -> device buffer (storage type, pitched)
+int upload_field(scl_handle* h, void* dst, const double* src, int ncomp, bool from_device) {
+  const cudaMemcpyKind kind = from_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  const size_t w = sizeof(double) * h->ld;
+  const size_t nrows = (size_t)h->rows * ncomp;
+  if (h->ssize == sizeof(double)) {
+    CK(cudaMemcpy2DAsync(dst, sizeof(double) * h->pitch, src, w, w, nrows, kind, h->stream));
+  } else {
+    CK(cudaMemcpy2DAsync(h->stage64, sizeof(double) * h->pitch, src, w, w, nrows, kind, h->stream));
+    const long n = h->plane * ncomp;
+    k_f64_to_f32<<<592, 256, 0, h->stream>>>(h->stage64, static_cast<float*>(dst), n);
+    CK(cudaGetLastError());
+  }
+  return SCL_OK;
+}
+
+int download_field(scl_handle* h, double* dst, const void* src, int ncomp, bool to_device) {
+  const cudaMemcpyKind kind = to_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  const size_t w = sizeof(double) * h->ld;
+  const size_t nrows = (size_t)h->rows * ncomp;
+  const void* from = src;
+  if (h->ssize != sizeof(double)) {
+    const long n = h->plane * ncomp;
+    k_f32_to_f64<<<592, 256, 0, h->stream>>>(static_cast<const float*>(src), h->stage64, n);
+    CK(cudaGetLastError());
+    from = h->stage64;
+  }
+  CK(cudaMemcpy2DAsync(dst, w, from, sizeof(double) * h->pitch, w, nrows, kind, h->stream));
+  return SCL_OK;
+}
+
+int validate(const scl_params* p) {
+  if (!p) return fail(SCL_E_INVALID, "null params");
+  if (p->ndim != 1 && p->ndim != 2) return fail(SCL_E_INVALID, "ndim must be 1 or 2");
+  if (p->mbc != 3) return fail(SCL_E_INVALID, "WENO5 requires mbc = 3 (reconstruct.f90:85)");
+  if (p->mx < 3 || (p->ndim == 2 && p->my < 3)) return fail(SCL_E_INVALID, "need at least 3 cells per direction");
+  if (p->lim_type != 2) return fail(SCL_E_UNSUPPORTED, "only lim_type = 2 (WENO) is built");
+  if (p->char_decomp != 0 && p->char_decomp != 2)
+    return fail(SCL_E_UNSUPPORTED, "char_decomp must be 0 or 2");
+  if (p->tfluct_solver != 0 && p->tfluct_solver != 1) return fail(SCL_E_INVALID, "tfluct_solver must be 0 or 1");
+  for (int k = 0; k < 2 * p->ndim; ++k)
+    if (p->mthbc[k] < 1 || p->mthbc[k] > 3)
+      return fail(SCL_E_INVALID, "mthbc must be 1, 2 or 3 (0 = user bc is not built)");
+  for (int k = 0; k < 2 * p->ndim; ++k)
+    if (p->mthbc[k] == 3 && p->meqn < (k < 2 ? 2 : 3))
+      return fail(SCL_E_INVALID, "solid wall bc negates component 2 (x) / 3 (y): meqn too small");
+  if ((p->mthbc[0] == 2) != (p->mthbc[1] == 2) ||
+      (p->ndim == 2 && (p->mthbc[2] == 2) != (p->mthbc[3] == 2)))
+    return fail(SCL_E_INVALID, "periodic bc must be set on both sides");
+  if (p->time_integrator < 1 || p->time_integrator > 4)
+    return fail(SCL_E_INVALID, "time_integrator should be between 1 and 4");
+  if (p->precision < SCL_FP64 || p->precision > SCL_FP32) return fail(SCL_E_INVALID, "bad precision");
+  if (!(p->dx > 0) || (p->ndim == 2 && !(p->dy > 0))) return fail(SCL_E_INVALID, "dx, dy must be > 0");
+  struct { int rp, meqn, mwaves, maux, ndim; } tab[] = {
+      {SCL_RP_ADVECTION, 1, 1, 0, 1}, {SCL_RP_EULER, 3, 3, 0, 1}, {SCL_RP_SW2D, 3, 3, 0, 2},
+      {SCL_RP_ACOUSTICS1D, 2, 2, 2, 1}, {SCL_RP_ACOUSTICS2D, 3, 2, 2, 2}};
+  for (auto& t : tab)
+    if (t.rp == p->rp) {
+      if (p->meqn != t.meqn || p->mwaves != t.mwaves)
+        return fail(SCL_E_INVALID, "meqn/mwaves do not match the plugin");
+      if (p->maux < t.maux) return fail(SCL_E_INVALID, "plugin needs more aux fields");
+      if (p->ndim != t.ndim) return fail(SCL_E_INVALID, "plugin dimension does not match ndim");
+      if (p->mcapa < 0 || p->mcapa > p->maux) return fail(SCL_E_INVALID, "mcapa out of range");
+      if (p->rp == SCL_RP_EULER && p->tfluct_solver == 1)
+        return fail(SCL_E_INVALID, "no tfluct exists for the Euler plugin (src/tfluct.f90 stub)");
+      return SCL_OK;
+    }
+  return fail(SCL_E_INVALID, "unknown rp id");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* scl_version(void) { return "sharpclaw_b200 0.1 (sm_100a)"; }
+const char* scl_last_error(void) { return g_err.c_str(); }
+void* scl_stream(scl_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+int scl_create(const scl_params* p, scl_handle** out) {
+  if (!out) return fail(SCL_E_INVALID, "null out");
+  *out = nullptr;
+  int rc = validate(p);
+  if (rc) return rc;
+  scl_handle* h = new scl_handle();
+  h->p = *p;
+  CK(cudaGetDevice(&h->device));
+  h->ssize = (p->precision == SCL_FP32) ? sizeof(float) : sizeof(double);
+  h->ld = p->mx + 2 * p->mbc;
+  h->rows = p->ndim == 2 ? p->my + 2 * p->mbc : 1;
+  h->pitch = (h->ld + 31) / 32 * 32;
+  h->plane = h->pitch * h->rows;
+  if (!get_launchers(p->precision, p->rp, p->ndim, p->char_decomp, p->tfluct_solver, h->variant, &h->L)) {
+    delete h;
+    return fail(SCL_E_UNSUPPORTED, "no kernel for this plugin / char_decomp / tfluct_solver");
+  }
+  h->nstages = stage_table(p->time_integrator, h->sd, &h->final_role);
+  auto cleanup = [&](int code) { scl_destroy(h); return code; };
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(fail(SCL_E_CUDA, "stream create failed"));
+  const size_t fbytes = h->ssize * h->plane * p->meqn;
+  for (int r = 0; r < NROLES; ++r) {
+    if (cudaMalloc(&h->buf[r], fbytes) != cudaSuccess) return cleanup(fail(SCL_E_CUDA, "cudaMalloc q buffers"));
+    cudaMemsetAsync(h->buf[r], 0, fbytes, h->stream);
+  }
+  const size_t abytes = h->ssize * h->plane * std::max(1, p->maux);
+  if (cudaMalloc(&h->aux, abytes) != cudaSuccess) return cleanup(fail(SCL_E_CUDA, "cudaMalloc aux"));
+  cudaMemsetAsync(h->aux, 0, abytes, h->stream);
+  const size_t sbytes = sizeof(double) * h->plane * std::max(p->meqn, std::max(1, p->maux));
+  if (cudaMalloc(&h->stage64, sbytes) != cudaSuccess) return cleanup(fail(SCL_E_CUDA, "cudaMalloc staging"));
+  cudaMemsetAsync(h->stage64, 0, sbytes, h->stream);
+  if (cudaMalloc(&h->ctl, sizeof(Ctl)) != cudaSuccess) return cleanup(fail(SCL_E_CUDA, "cudaMalloc ctl"));
+  if (cudaMallocHost(&h->hctl, sizeof(Ctl)) != cudaSuccess) return cleanup(fail(SCL_E_CUDA, "cudaMallocHost"));
+  if (cudaMallocHost(&h->hdone, 2 * sizeof(int)) != cudaSuccess) return cleanup(fail(SCL_E_CUDA, "cudaMallocHost"));
+  memset(h->hctl, 0, sizeof(Ctl));
+  for (int r = 0; r < NROLES; ++r) h->hctl->role[r] = r;
+  h->hctl->done = 0;
+  cudaEventCreate(&h->ev0);
+  cudaEventCreate(&h->ev1);
+  cudaEventCreateWithFlags(&h->evq[0], cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&h->evq[1], cudaEventDisableTiming);
+  rc = upload_ctl(h);
+  if (rc) return cleanup(rc);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return cleanup(fail(SCL_E_CUDA, "create sync"));
+  *out = h;
+  return SCL_OK;
+}
+
+int scl_destroy(scl_handle* h) {
+  if (!h) return SCL_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  for (int r = 0; r < NROLES; ++r) if (h->buf[r]) cudaFree(h->buf[r]);
+  if (h->aux) cudaFree(h->aux);
+  if (h->stage64) cudaFree(h->stage64);
+  if (h->ctl) cudaFree(h->ctl);
+  if (h->hctl) cudaFreeHost(h->hctl);
+  if (h->hdone) cudaFreeHost(h->hdone);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  for (int k = 0; k < 2; ++k) if (h->evq[k]) cudaEventDestroy(h->evq[k]);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return SCL_OK;
+}
+
+int scl_set_q(scl_handle* h, const double* q) {
+  if (!h || !q) return fail(SCL_E_INVALID, "null argument");
+  void* dst = h->buf[h->hctl->role[ROLE_Q]];
+  int rc = upload_field(h, dst, q, h->p.meqn, false);
+  if (rc) return rc;
+  if (h->ssize == sizeof(double)) launch_bc<double>(h, static_cast<double*>(dst));
+  else launch_bc<float>(h, static_cast<float*>(dst));
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
+  return SCL_OK;
+}
+
+int scl_get_q(scl_handle* h, double* q) {
+  if (!h || !q) return fail(SCL_E_INVALID, "null argument");
+  int rc = download_field(h, q, h->buf[h->hctl->role[ROLE_Q]], h->p.meqn, false);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  return SCL_OK;
+}
+
+int scl_set_aux(scl_handle* h, const double* aux) {
+  if (!h || !aux) return fail(SCL_E_INVALID, "null argument");
+  if (h->p.maux == 0) return SCL_OK;
+  int rc = upload_field(h, h->aux, aux, h->p.maux, false);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  return SCL_OK;
+}
+
+int scl_step_dq(scl_handle* h, double* q, double* dq, double dt, double t, double* cfl) {
+  (void)t;
+  if (!h || !q || !dq) return fail(SCL_E_INVALID, "null argument");
+  int rc = scl_set_q(h, q);   // upload + bc
+  if (rc) return rc;
+  h->hctl->dt = dt;
+  h->hctl->done = 0;
+  for (int s = 0; s < MAXSTAGES; ++s) h->hctl->stage_cfl[s] = 0.0;
+  rc = upload_ctl(h);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(h->stage64, 0, sizeof(double) * h->plane * h->p.meqn, h->stream));
+  StageArgs a = make_args(h, 0);
+  a.sd = StageDesc{SK_DQ, ROLE_Q, -1, -1, -1};
+  h->L.stage(a, h->stream);
+  if (h->L.ghost) h->L.ghost(a, h->stream);
+  CK(cudaGetLastError());
+  // dq in double, pitched -> reference layout
+  const size_t w = sizeof(double) * h->ld;
+  CK(cudaMemcpy2DAsync(dq, w, h->stage64, sizeof(double) * h->pitch, w, (size_t)h->rows * h->p.meqn,
+                       cudaMemcpyDeviceToHost, h->stream));
+  rc = download_field(h, q, h->buf[h->hctl->role[ROLE_Q]], h->p.meqn, false);
+  if (rc) return rc;
+  rc = download_ctl(h);
+  if (rc) return rc;
+  if (cfl) *cfl = h->hctl->stage_cfl[0];
+  return SCL_OK;
+}
+
+int scl_flux1(scl_handle* h, const double* q1d, const double* aux1d, double* dq1d, double dt,
+              int ixy, int mx, double* cfl) {
+  if (!h || !q1d || !dq1d) return fail(SCL_E_INVALID, "null argument");
+  if (ixy != 1 && ixy != 2) return fail(SCL_E_INVALID, "ixy must be 1 or 2");
+  if (mx < 3) return fail(SCL_E_INVALID, "mx too small");
+  if (h->p.maux > 0 && !aux1d) return fail(SCL_E_INVALID, "aux1d required");
+  // A one-line problem of the same plugin: a temporary 1-D handle.
+  scl_params p1 = h->p;
+  p1.ndim = 1;
+  p1.mx = mx;
+  p1.my = 1;
+  p1.dx = (ixy == 1) ? h->p.dx : h->p.dy;
+  p1.mthbc[0] = p1.mthbc[1] = 1;
+  Launchers L1{};
+  if (!get_launchers(p1.precision, p1.rp, 1, p1.char_decomp, p1.tfluct_solver, 0, &L1))
+    return fail(SCL_E_UNSUPPORTED, "no 1-D kernel for this plugin");
+  const long ld = mx + 2 * p1.mbc, pitch = (ld + 31) / 32 * 32;
+  const size_t ss = h->ssize;
+  void *dq_in = nullptr, *dq_aux = nullptr;
+  double *d64 = nullptr, *dctl_dummy = nullptr;
+  Ctl* dctl = nullptr;
+  (void)dctl_dummy;
+  auto cleanup = [&]() {
+    cudaFree(dq_in); cudaFree(dq_aux); cudaFree(d64); cudaFree(dctl);
+  };
+  if (cudaMalloc(&dq_in, ss * pitch * p1.meqn) != cudaSuccess ||
+      cudaMalloc(&dq_aux, ss * pitch * std::max(1, p1.maux)) != cudaSuccess ||
+      cudaMalloc(&d64, sizeof(double) * pitch * std::max(p1.meqn, std::max(1, p1.maux))) != cudaSuccess ||
+      cudaMalloc(&dctl, sizeof(Ctl)) != cudaSuccess) {
+    cleanup();
+    return fail(SCL_E_CUDA, "cudaMalloc in scl_flux1");
+  }
+  int rc = SCL_OK;
+  auto put = [&](void* dst, const double* src, int nc) -> int {
+    const size_t w = sizeof(double) * ld;
+    if (ss == sizeof(double)) {
+      CK(cudaMemcpy2DAsync(dst, sizeof(double) * pitch, src, w, w, nc, cudaMemcpyHostToDevice, h->stream));
+    } else {
+      CK(cudaMemcpy2DAsync(d64, sizeof(double) * pitch, src, w, w, nc, cudaMemcpyHostToDevice, h->stream));
+      k_f64_to_f32<<<64, 256, 0, h->stream>>>(d64, static_cast<float*>(dst), pitch * nc);
+    }
+    return SCL_OK;
+  };
+  Ctl c{};
+  c.dt = dt;
+  for (int r = 0; r < NROLES; ++r) c.role[r] = r;
+  rc = put(dq_in, q1d, p1.meqn);
+  if (!rc && p1.maux > 0) rc = put(dq_aux, aux1d, p1.maux);
+  if (!rc && cudaMemcpyAsync(dctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
+    rc = fail(SCL_E_CUDA, "ctl upload");
+  if (!rc && cudaMemsetAsync(d64, 0, sizeof(double) * pitch * p1.meqn, h->stream) != cudaSuccess)
+    rc = fail(SCL_E_CUDA, "memset");
+  if (!rc) {
+    StageArgs a{};
+    a.ctl = dctl;
+    a.buf[0] = dq_in;
+    a.aux = dq_aux;
+    a.dq_out = d64;
+    a.sd = StageDesc{SK_DQ, 0, -1, -1, -1};
+    a.stage = 0;
+    a.ixy = ixy;
+    a.mx = mx;
+    a.my = 1;
+    a.pitch = pitch;
+    a.plane = pitch;
+    a.dx = p1.dx;
+    a.dy = p1.dx;
+    for (int k = 0; k < 4; ++k) a.mthbc[k] = 1;
+    a.mcapa = p1.mcapa;
+    a.ph.u = p1.u; a.ph.gamma = p1.gamma; a.ph.gamma1 = p1.gamma - 1.0; a.ph.grav = p1.grav;
+    a.ph.efix = p1.efix;
+    L1.stage(a, h->stream);
+    if (cudaGetLastError() != cudaSuccess) rc = fail(SCL_E_CUDA, "flux1 launch");
+  }
+  if (!rc) {
+    const size_t w = sizeof(double) * ld;
+    if (cudaMemcpy2DAsync(dq1d, w, d64, sizeof(double) * pitch, w, p1.meqn, cudaMemcpyDeviceToHost,
+                          h->stream) != cudaSuccess ||
+        cudaMemcpyAsync(&c, dctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess)
+      rc = fail(SCL_E_CUDA, "flux1 download");
+    else if (cfl)
+      *cfl = c.stage_cfl[0];
+  }
+  cudaStreamSynchronize(h->stream);
+  cleanup();
+  return rc;
+}
+
+int scl_rk_step(scl_handle* h, double dt, double told, double* cfl) {
+  if (!h) return fail(SCL_E_INVALID, "null handle");
+  Ctl* c = h->hctl;
+  c->dt = dt;
+  c->told = told;
+  c->t = told + dt;
+  c->done = 0;
+  c->status = 0;
+  for (int s = 0; s < MAXSTAGES; ++s) c->stage_cfl[s] = 0.0;
+  int rc = upload_ctl(h);
+  if (rc) return rc;
+  rc = enqueue_stages(h);
+  if (rc) return rc;
+  rc = download_ctl(h);
+  if (rc) return rc;
+  const double cv = c->stage_cfl[h->nstages - 1];
+  std::swap(c->role[ROLE_Q], c->role[h->final_role]);
+  if (cfl) *cfl = cv;
+  if ((c->status & SCL_STATUS_NONFINITE) || cv != cv) return fail(SCL_E_NONFINITE, "non-finite stage output");
+  return SCL_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Initialise the controller from sharpclaw()'s arguments (sharpclaw.f90:35-64).
+int init_run(scl_handle* h, const scl_run* run, int max_steps, scl_result* res, bool* early) {
+  *early = false;
+  Ctl* c = h->hctl;
+  c->t = run->tstart;
+  c->told = run->tstart;
+  c->tstart = run->tstart;
+  c->tend = run->tend;
+  c->dt = run->dt_initial;
+  c->dt_max = run->dt_max;
+  c->cfl_max = run->cfl_max;
+  c->cfl_desired = run->cfl_desired;
+  c->cflmax = 0.0;
+  c->dtmin = run->dt_initial;
+  c->dtmax = run->dt_initial;
+  c->cfl_last = 0.0;
+  c->n_iter = 0;
+  c->maxn = max_steps;
+  c->steps_taken = 0;
+  c->rejected = 0;
+  c->retake = 0;
+  c->done = 0;
+  c->info = 0;
+  c->status = 0;
+  c->dt_variable = run->dt_variable;
+  memset(res, 0, sizeof(*res));
+  if (run->dt_variable == 0) {
+    if (run->tend < run->tstart) {
+      c->maxn = 1;
+    } else {
+      c->maxn = (int)((run->tend - run->tstart + 1e-10) / run->dt_initial);
+      if (std::fabs(c->maxn * run->dt_initial - (run->tend - run->tstart)) > 1e-5 * (run->tend - run->tstart)) {
+        res->info = SCL_INFO_DT_NOT_DIVIDING;
+        *early = true;
+        return SCL_OK;
+      }
+    }
+  }
+  if (run->dt_variable == 1 && run->cfl_desired > run->cfl_max) {
+    res->info = SCL_INFO_CFL_DESIRED_GT_MAX;
+    *early = true;
+    return SCL_OK;
+  }
+  return upload_ctl(h);
+}
+
+void finish_run(scl_handle* h, scl_result* res) {
+  const Ctl* c = h->hctl;
+  int info = c->info;
+  if (!info) {
+    if (c->dt_variable == 1 && c->t < c->tend && c->steps_taken == c->maxn) info = SCL_INFO_TOO_MANY_STEPS;
+    if (c->dt_variable == 0 && c->cflmax > c->cfl_max) info = SCL_INFO_CFL_FIXED_DT;
+  }
+  res->tend = c->t;
+  res->cfl_maxused = c->cflmax;
+  res->cfl_last = c->cfl_last;
+  res->dt_minused = c->dtmin;
+  res->dt_maxused = c->dtmax;
+  res->dt_last = c->dt;
+  res->steps_taken = c->steps_taken;
+  res->info = info;
+  res->rejected = c->rejected;
+  res->status = c->status;
+}
+
+// Replay the K-step graph until the controller reports done.  The done flag
+// of replay k is copied to pinned memory behind replay k+1, so the device
+// never idles waiting for the host.
+int run_loop(scl_handle* h, int graph_steps, long max_replays, float* ms) {
+  int rc = build_graph(h, graph_steps);
+  if (rc) return rc;
+  if (ms) CK(cudaEventRecord(h->ev0, h->stream));
+  h->hdone[0] = h->hdone[1] = 0;
+  for (long r = 0; r < max_replays; ++r) {
+    CK(cudaGraphLaunch(h->graph, h->stream));
+    if (ms) continue;
+    CK(cudaMemcpyAsync(&h->hdone[r & 1], &h->ctl->done, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaEventRecord(h->evq[r & 1], h->stream));
+    if (r > 0) {  // replay r is already queued while we look at replay r-1
+      CK(cudaEventSynchronize(h->evq[(r - 1) & 1]));
+      if (h->hdone[(r - 1) & 1]) break;
+    }
+  }
+  if (ms) {
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    CK(cudaEventElapsedTime(ms, h->ev0, h->ev1));
+  }
+  return download_ctl(h);
+}
+
+}  // namespace
+
+extern "C" {
+
+int scl_sharpclaw(scl_handle* h, const scl_run* run, scl_result* res) {
+  if (!h || !run || !res) return fail(SCL_E_INVALID, "null argument");
+  bool early = false;
+  int rc = init_run(h, run, run->max_steps, res, &early);
+  if (rc || early) return rc;
+  // a graph replay runs gs controller steps; after maxn iterations the
+  // controller is done, so no more than ceil(maxn/gs) replays are launched
+  const int gs = std::min(std::max(1, h->hctl->maxn), default_graph_steps(h));
+  const long replays = ((long)h->hctl->maxn + gs - 1) / gs;
+  rc = run_loop(h, gs, replays, nullptr);
+  if (rc) return rc;
+  finish_run(h, res);
+  if (res->status & SCL_STATUS_NONFINITE) return fail(SCL_E_NONFINITE, "non-finite CFL number");
+  return SCL_OK;
+}
+
+int scl_sharpclaw_device(scl_handle* h, const scl_run* run, double* q_dev, scl_result* res) {
+  if (!h || !run || !res || !q_dev) return fail(SCL_E_INVALID, "null argument");
+  void* dst = h->buf[h->hctl->role[ROLE_Q]];
+  int rc = upload_field(h, dst, q_dev, h->p.meqn, true);
+  if (rc) return rc;
+  if (h->ssize == sizeof(double)) launch_bc<double>(h, static_cast<double*>(dst));
+  else launch_bc<float>(h, static_cast<float*>(dst));
+  rc = scl_sharpclaw(h, run, res);
+  if (rc && rc != SCL_E_NONFINITE) return rc;
+  int rc2 = download_field(h, q_dev, h->buf[h->hctl->role[ROLE_Q]], h->p.meqn, true);
+  if (rc2) return rc2;
+  CK(cudaStreamSynchronize(h->stream));
+  return rc;
+}
+
+int scl_time_steps(scl_handle* h, const scl_run* run, int nsteps, float* ms, scl_result* res) {
+  if (!h || !run || !ms || !res || nsteps < 1) return fail(SCL_E_INVALID, "bad argument");
+  bool early = false;
+  int rc = init_run(h, run, nsteps, res, &early);
+  if (rc || early) return rc ? rc : fail(SCL_E_INVALID, "run parameters rejected (info set)");
+  const int gs = nsteps <= 64 ? nsteps : default_graph_steps(h);
+  const long replays = (nsteps + gs - 1) / gs;
+  rc = run_loop(h, gs, replays, ms);
+  if (rc) return rc;
+  finish_run(h, res);
+  return SCL_OK;
+}
+
+int scl_time_stages(scl_handle* h, double dt, int reps, float* ms, long long* launches) {
+  if (!h || !ms || reps < 1) return fail(SCL_E_INVALID, "bad argument");
+  Ctl* c = h->hctl;
+  c->dt = dt;
+  c->done = 0;
+  c->status = 0;
+  for (int s = 0; s < MAXSTAGES; ++s) c->stage_cfl[s] = 0.0;
+  int rc = upload_ctl(h);
+  if (rc) return rc;
+  rc = enqueue_stages(h);  // warm-up pass
+  if (rc) return rc;
+  CK(cudaEventRecord(h->ev0, h->stream));
+  for (int r = 0; r < reps; ++r) {
+    for (int s = 0; s < h->nstages; ++s) h->L.stage(make_args(h, s), h->stream);
+  }
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(h->ev1, h->stream));
+  CK(cudaEventSynchronize(h->ev1));
+  CK(cudaEventElapsedTime(ms, h->ev0, h->ev1));
+  if (launches) *launches = (long long)reps * h->nstages;
+  return SCL_OK;
+}
+
+int scl_kernels_per_step(scl_handle* h) { return h ? kernels_per_step(h) : 0; }
+
+}  // extern "C"

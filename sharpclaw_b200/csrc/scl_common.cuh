@@ -1,0 +1,114 @@
+// scl_common.cuh -- shared device types for the SharpClaw B200 kernels.
+//
+// Layout in HBM: every field is a set of component planes ("structure of
+// arrays"), exactly the column-major order of the reference
+// (src/1d/qalloc1.f90:10, src/2d/qalloc2.f90:11) with the lower bound 1-mbc
+// mapped to offset 0.  Rows are padded to `pitch` elements (a multiple of 32)
+// so every row start is 256-byte aligned; a 2-D plane holds (my+2*mbc) rows.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/sharpclaw_cuda.h"
+
+namespace scl {
+
+constexpr int MBC = 3;       // WENO5 needs three ghost cells (reconstruct.f90:85,158)
+constexpr int MAXEQ = 3;     // largest meqn of the supported plugins
+constexpr int MAXSTAGES = 10;
+
+// Stage-update kinds: one per distinct Shu-Osher combination written in
+// src/sharpclaw.f90 (ts_ssp22 247-276, ts_ssp42 280-333, ts_ssp33 337-376,
+// ts_ssp104 380-464).  Each keeps the reference's evaluation order.
+enum StageKind : int {
+  SK_ADD = 0,        // q + dq                               ssp33 :356, ssp22 :264
+  SK_SSP33_2 = 1,    // 0.75*qold + 0.25*(q + dq)            ssp33 :365
+  SK_SSP33_3 = 2,    // (qold + 2*(q + dq))/3                ssp33 :374
+  SK_ADD_SIXTH = 3,  // q + (1/6)*dq                         ssp104 :396 ...
+  SK_SSP104_5 = 4,   // r2=q+dq/6; r1=.04qold+.36r2; q=.6qold+.4r2   ssp104 :424-426
+  SK_SSP104_10 = 5,  // (r1 + 0.6*q) + 0.1*dq                ssp104 :462
+  SK_SSP22_2 = 6,    // 0.5*((qold + q) + dq)                ssp22 :274
+  SK_ADD_THIRD = 7,  // q + (1/3)*dq                         ssp42 :304,313,322
+  SK_SSP42_4 = 8,    // (0.25*qold + 0.75*q) + 0.25*dq       ssp42 :331
+  SK_DQ = 9          // write dq itself (step1d/step2d output, no combination)
+};
+
+// Buffer roles for the register rotation (no whole-array copies: the
+// reference's qold=q (sharpclaw.f90:134) becomes "Q keeps q^n").
+enum Role : int { ROLE_Q = 0, ROLE_A = 1, ROLE_B = 2, ROLE_R1 = 3, NROLES = 4 };
+
+// One stage of an integrator: which roles it reads/writes and how it combines.
+struct StageDesc {
+  int kind;       // StageKind
+  int in;         // role read with halo (the stage input q)
+  int out;        // role written (new q, with ghost images)
+  int out2;       // second output (SSP104 stage 5 writes r1), -1 if none
+  int aux_in;     // pointwise extra input (qold role for most; r1 for SSP104 stage 10), -1 if none
+};
+
+// Device-resident controller state: the scalars of src/sharpclaw.f90:18-41 and
+// the per-stage CFL numbers.  One per handle (or per batched instance).
+struct __align__(16) Ctl {
+  double t, told, dt, tstart, tend;
+  double dt_max, cfl_max, cfl_desired;
+  double cflmax, dtmin, dtmax, cfl_last;
+  double stage_cfl[MAXSTAGES];  // written by the stage kernels (atomic max on bits)
+  int role[NROLES];             // physical buffer index of each role
+  int n_iter, maxn, steps_taken, rejected;
+  int retake, done, info, dt_variable;
+  int status;                   // OR of SCL_STATUS_* raised by kernels
+  int accept_always;            // single-step mode (scl_rk_step): no dt update, always accept
+  int pad[2];
+};
+
+// Physics constants of the plugins (COMMON blocks /comrp/, /param/).
+struct Phys {
+  double u;       // advection speed        apps/advection/1d/rp1.f:31
+  double gamma;   // ratio of specific heats apps/euler/shockentropy/setprob.f:392
+  double gamma1;  // gamma - 1
+  double grav;    // gravity                apps/shallowWater/2dRadialDam/setprob.f90
+  int efix;
+};
+
+// Arguments of one stage launch (all by value; pointers are device pointers).
+struct StageArgs {
+  Ctl* ctl;
+  void* buf[NROLES];        // physical buffers (storage type S), each meqn planes
+  const void* aux;          // aux planes (storage type S), or nullptr
+  double* dq_out;           // SK_DQ only: dt*L(q) in double, same layout
+  StageDesc sd;
+  int stage;                // stage index (slot in ctl->stage_cfl)
+  int ixy;                  // normal direction of a 1-D line (flux1.f90 ixy)
+  int mx, my;
+  long pitch;               // row pitch (elements)
+  long plane;               // elements per component plane
+  double dx, dy;
+  int mthbc[4];
+  int mcapa;                // 1-based aux index of capacity, 0 if none
+  Phys ph;
+};
+
+// NaN-propagating maximum used for the CFL number: a NaN anywhere makes the
+// block result NaN so the controller can flag a non-finite state.
+template <class R>
+__device__ __forceinline__ R nanmax(R a, R b) {
+  return (b > a || b != b) ? b : a;
+}
+
+// Atomic max of a non-negative double (or NaN) through its bit pattern:
+// for +0.0 .. +inf and positive NaN, unsigned order equals value order.
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+  if (!(v > 0.0) && v == v) return;  // +0/-0 never raise the max
+  unsigned long long bits = __double_as_longlong(v);
+  if (v != v) bits = 0x7ff8000000000000ULL;
+  atomicMax(reinterpret_cast<unsigned long long*>(addr), bits);
+}
+
+template <class T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+}  // namespace scl

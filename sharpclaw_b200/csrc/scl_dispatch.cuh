@@ -1,0 +1,109 @@
+// scl_dispatch.cuh -- instantiates the stage kernels of one arithmetic form.
+// Included by one translation unit per form (scl_prec_*.cu) with
+// SCL_PREC_VALUE defined; the FP64_STRICT unit is compiled without FMA
+// contraction so its arithmetic follows the reference's evaluation order.
+#pragma once
+#include "scl_kernels.cuh"
+#include "scl_launch.h"
+
+#ifndef SCL_PREC_VALUE
+#error "SCL_PREC_VALUE must be defined"
+#endif
+
+namespace scl {
+namespace SCL_PREC_NS {
+
+constexpr int PREC = SCL_PREC_VALUE;
+using R = typename Prec<PREC>::R;
+using S = typename Prec<PREC>::S;
+
+constexpr int NT1 = 128;
+
+template <class P, int CD, int TF>
+void launch1d(const StageArgs& a, cudaStream_t st) {
+  const int nb = (a.mx + NT1 - 2) / (NT1 - 1);
+  k_stage1d<P, CD, TF, PREC, NT1><<<nb, NT1, 0, st>>>(a);
+}
+
+template <class P, int CD, int TF, int TX, int TY, int NT>
+constexpr size_t smem2d() {
+  using T = Tile2D<TX, TY>;
+  return sizeof(S) * P::MEQN * T::WX * T::WY + sizeof(R) * 4 * P::MEQN * (T::NXI + T::NYI);
+}
+
+template <class P, int CD, int TF, int TX, int TY, int NT>
+void launch2d(const StageArgs& a, cudaStream_t st) {
+  dim3 grid((a.mx + TX - 1) / TX, (a.my + TY - 1) / TY);
+  k_stage2d<P, CD, TF, PREC, TX, TY, NT><<<grid, NT, smem2d<P, CD, TF, TX, TY, NT>(), st>>>(a);
+}
+
+// dynamic shared memory above 48 KB must be opted into before launch (and
+// outside any stream capture), so it is done when the kernel is picked
+template <class P, int CD, int TF, int TX, int TY, int NT>
+bool prepare2d(Launchers* L) {
+  if (cudaFuncSetAttribute(k_stage2d<P, CD, TF, PREC, TX, TY, NT>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem2d<P, CD, TF, TX, TY, NT>()) != cudaSuccess)
+    return false;
+  L->stage = &launch2d<P, CD, TF, TX, TY, NT>;
+  return true;
+}
+
+template <class P, int CD>
+void launch_ghost2d(const StageArgs& a, cudaStream_t st) {
+  const int n = 2 * (a.mx + 1) + 2 * (a.my + 1);
+  k_ghost_cfl2d<P, CD, PREC><<<(n + 127) / 128, 128, 0, st>>>(a);
+}
+
+template <class P, int CD, int TF>
+bool fill2d(int variant, Launchers* L) {
+  switch (variant) {
+    case 0: if (!prepare2d<P, CD, TF, 16, 7, 128>(L)) return false; break;
+    case 1: if (!prepare2d<P, CD, TF, 32, 7, 256>(L)) return false; break;
+    case 2: if (!prepare2d<P, CD, TF, 16, 15, 256>(L)) return false; break;
+    default: return false;
+  }
+  L->ghost = &launch_ghost2d<P, CD>;
+  return true;
+}
+
+template <class P>
+bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
+  L->stage = nullptr;
+  L->ghost = nullptr;
+  if (ndim == 1) {
+    if (variant != 0) return false;
+    if (cd == 0 && tf == 0) L->stage = &launch1d<P, 0, 0>;
+    if (cd == 2 && tf == 0) L->stage = &launch1d<P, 2, 0>;
+    if constexpr (P::HAS_TFLUCT) {
+      if (cd == 0 && tf == 1) L->stage = &launch1d<P, 0, 1>;
+      if (cd == 2 && tf == 1) L->stage = &launch1d<P, 2, 1>;
+    }
+    return L->stage != nullptr;
+  }
+  if constexpr (P::NDIM == 2) {
+    if (cd == 0 && tf == 0) return fill2d<P, 0, 0>(variant, L);
+    if (cd == 2 && tf == 0) return fill2d<P, 2, 0>(variant, L);
+    if constexpr (P::HAS_TFLUCT) {
+      if (cd == 0 && tf == 1) return fill2d<P, 0, 1>(variant, L);
+      if (cd == 2 && tf == 1) return fill2d<P, 2, 1>(variant, L);
+    }
+  }
+  return false;
+}
+
+}  // namespace SCL_PREC_NS
+
+bool SCL_PREC_GETTER(int rp, int ndim, int cd, int tf, int variant, Launchers* L) {
+  using namespace SCL_PREC_NS;
+  switch (rp) {
+    case SCL_RP_ADVECTION: return ndim == 1 && pick<PAdvection>(ndim, cd, tf, variant, L);
+    case SCL_RP_EULER: return ndim == 1 && pick<PEuler>(ndim, cd, tf, variant, L);
+    case SCL_RP_SW2D: return pick<PShallow2D>(ndim, cd, tf, variant, L);
+    case SCL_RP_ACOUSTICS1D: return ndim == 1 && pick<PAcoustics<2>>(ndim, cd, tf, variant, L);
+    case SCL_RP_ACOUSTICS2D: return pick<PAcoustics<3>>(ndim, cd, tf, variant, L);
+  }
+  return false;
+}
+
+}  // namespace scl

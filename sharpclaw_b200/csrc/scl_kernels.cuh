@@ -1,0 +1,562 @@
+// scl_kernels.cuh -- fused SSP-RK stage kernels for the SharpClaw WENO step.
+//
+// One launch = one Runge-Kutta stage over the whole grid: bc (as ghost
+// images written with the stage output), src (dq starts at zero), the
+// reconstruction + Riemann solves of flux1/flux2, the CFL maximum, the total
+// fluctuation and the Shu-Osher stage combination of src/sharpclaw.f90.  No
+// intermediate array (ql, qr, amdq, apdq, wave, s, dq) touches HBM: a CTA
+// stages its cells plus ghosts in shared memory, solves one interface per
+// thread into shared memory, then updates one cell per thread.
+#pragma once
+#include "scl_common.cuh"
+#include "scl_plugins.cuh"
+#include "scl_weno.cuh"
+
+namespace scl {
+
+// Arithmetic forms (template parameter PREC): SCL_FP64 / SCL_FP64_STRICT
+// (double throughout; strict is the same source compiled without FMA
+// contraction), SCL_MIXED (float reconstruction and Riemann solves on
+// double state), SCL_FP32 (float state).
+template <int PREC> struct Prec;
+template <> struct Prec<SCL_FP64> { using R = double; using S = double; using A = double; static constexpr bool EXACT = true; };
+template <> struct Prec<SCL_FP64_STRICT> { using R = double; using S = double; using A = double; static constexpr bool EXACT = true; };
+template <> struct Prec<SCL_MIXED> { using R = float; using S = double; using A = double; static constexpr bool EXACT = false; };
+template <> struct Prec<SCL_FP32> { using R = float; using S = float; using A = float; static constexpr bool EXACT = false; };
+
+
+
+// ---------------------------------------------------------------------------
+// Shu-Osher stage combinations (src/sharpclaw.f90), evaluated in A precision.
+// ---------------------------------------------------------------------------
+template <class A>
+__device__ __forceinline__ void combine(int kind, A q, A qo, A dq, A& out, A& out2) {
+  switch (kind) {
+    case SK_ADD: out = q + dq; break;                                            // :264,:356
+    case SK_SSP33_2: out = (A)0.75 * qo + (A)0.25 * (q + dq); break;             // :365
+    case SK_SSP33_3: out = (qo + (A)2.0 * (q + dq)) / (A)3.0; break;             // :374
+    case SK_ADD_SIXTH: out = q + (A)(1.0 / 6.0) * dq; break;                     // :396..455
+    case SK_SSP104_5: {                                                          // :424-426
+      A r2 = q + (A)(1.0 / 6.0) * dq;
+      out2 = (A)0.04 * qo + (A)0.36 * r2;
+      out = (A)0.6 * qo + (A)0.4 * r2;
+      break;
+    }
+    case SK_SSP104_10: out = (qo + (A)0.6 * q) + (A)0.1 * dq; break;             // :462 (qo = r1)
+    case SK_SSP22_2: out = (A)0.5 * ((qo + q) + dq); break;                      // :274
+    case SK_ADD_THIRD: out = q + (A)(1.0 / 3.0) * dq; break;                     // :304,313,322
+    case SK_SSP42_4: out = ((A)0.25 * qo + (A)0.75 * q) + (A)0.25 * dq; break;   // :331
+    default: out = dq; break;                                                    // SK_DQ
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Ghost images.  bc1.f90/bc2.f90 fill ghost cells from interior cells before
+// every stage; here the thread that writes interior cell i also writes every
+// ghost cell whose bc source is i.  The map ghost -> source is a function, so
+// each ghost is written exactly once, and in 2-D the corners come out as the
+// reference's x-then-y sweep leaves them.
+// ---------------------------------------------------------------------------
+struct Images {
+  int n;
+  int idx[6];
+  bool neg[6];
+};
+
+// images along one direction of cell c (1-based) for normal component `mnorm`
+// (0-based) of the wall condition.
+__device__ __forceinline__ Images images_1d(int c, int n, int bl, int br) {
+  Images im;
+  im.n = 1; im.idx[0] = c; im.neg[0] = false;
+  if (bl == 1 && c == 1) { for (int g = -2; g <= 0; ++g) { im.idx[im.n] = g; im.neg[im.n++] = false; } }
+  if (bl == 2 && c >= n - 2) { im.idx[im.n] = c - n; im.neg[im.n++] = false; }
+  if (bl == 3 && c <= 3) { im.idx[im.n] = 1 - c; im.neg[im.n++] = true; }
+  if (br == 1 && c == n) { for (int g = n + 1; g <= n + 3; ++g) { im.idx[im.n] = g; im.neg[im.n++] = false; } }
+  if (br == 2 && c <= 3) { im.idx[im.n] = c + n; im.neg[im.n++] = false; }
+  if (br == 3 && c >= n - 2) { im.idx[im.n] = 2 * n + 1 - c; im.neg[im.n++] = true; }
+  return im;
+}
+
+template <class S, class A>
+__device__ __forceinline__ void put_1d(S* base, long plane, int m, int c, const Images& im, A v) {
+  S* p = base + (long)m * plane;
+  p[c + 2] = (S)v;
+  for (int k = 1; k < im.n; ++k) p[im.idx[k] + 2] = (S)((m == 1 && im.neg[k]) ? -v : v);
+}
+
+template <class S, class A>
+__device__ __forceinline__ void put_2d(S* base, long plane, long pitch, int m, int i, int j,
+                                       const Images& ix, const Images& iy, A v) {
+  S* p = base + (long)m * plane;
+  for (int a = 0; a < ix.n; ++a) {
+    A vx = (m == 1 && ix.neg[a]) ? -v : v;
+    for (int b = 0; b < iy.n; ++b) {
+      A vy = (m == 2 && iy.neg[b]) ? -vx : vx;
+      p[(long)(iy.idx[b] + 2) * pitch + (ix.idx[a] + 2)] = (S)vy;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One interface c-1/2 (between cells c-1 and c) of a line: reconstruction,
+// Riemann solve and the CFL contribution.  `qs(k, m)` returns cell c-3+k.
+// Results: xl = qr(c-1), xr = ql(c) (states in the exact form, offsets from
+// q(c-1)/q(c) in the offset form), fluctuations amdq(c), apdq(c).
+// ---------------------------------------------------------------------------
+template <class P, int CD, int PREC, class QS>
+__device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs,
+                                                const typename Prec<PREC>::R* auxm,
+                                                const typename Prec<PREC>::R* aux0,
+                                                typename Prec<PREC>::R xl[P::MEQN],
+                                                typename Prec<PREC>::R xr[P::MEQN],
+                                                typename Prec<PREC>::R amdq[P::MEQN],
+                                                typename Prec<PREC>::R apdq[P::MEQN],
+                                                typename Prec<PREC>::R s[P::MWAVES]) {
+  using R = typename Prec<PREC>::R;
+  constexpr int M = P::MEQN;
+  if constexpr (Prec<PREC>::EXACT) {
+    double q[6][M];
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+#pragma unroll
+      for (int m = 0; m < M; ++m) q[k][m] = (double)qs(k, m);
+    if constexpr (CD == 2) {
+      double evl[M][M], evr[M][M];
+      P::template evec<double>(ph, ixy, q[2], q[3], auxm, aux0, evl, evr);
+      weno5_char_exact<M>(q, evl, evr, xl, xr);
+    } else {
+      weno5_exact<M>(q, xl, xr);
+    }
+    double dl[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) dl[m] = xr[m] - xl[m];   // delta = ql(i) - qr(i-1)
+    P::template rp<double>(ph, ixy, xl, xr, dl, auxm, aux0, s, amdq, apdq);
+  } else {
+    float d[5][M];
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+#pragma unroll
+      for (int m = 0; m < M; ++m) d[k][m] = (float)(qs(k + 1, m) - qs(k, m));
+    if constexpr (CD == 2) {
+      float qm[M], q0[M], evl[M][M], evr[M][M];
+#pragma unroll
+      for (int m = 0; m < M; ++m) { qm[m] = (float)qs(2, m); q0[m] = (float)qs(3, m); }
+      P::template evec<float>(ph, ixy, qm, q0, auxm, aux0, evl, evr);
+      weno5_char_offset<M>(d, evl, evr, xl, xr);
+    } else {
+      weno5_offset<M>(d, xl, xr);
+    }
+    float L[M], Rt[M], dl[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      L[m] = (float)qs(2, m) + xl[m];
+      Rt[m] = (float)qs(3, m) + xr[m];
+      dl[m] = d[2][m] + (xr[m] - xl[m]);   // (q(c)-q(c-1)) + (el - er)
+    }
+    P::template rp<float>(ph, ixy, L, Rt, dl, auxm, aux0, s, amdq, apdq);
+  }
+}
+
+// Total fluctuation of cell c from its edge values (flux1.f90:136-188):
+// returns the bracket that multiplies -dtdx, in the reference's order.
+template <class P, int TF, int PREC>
+__device__ __forceinline__ void cell_bracket(const Phys& ph, int ixy, const typename Prec<PREC>::R* qc,
+                                             const typename Prec<PREC>::R* auxc,
+                                             const typename Prec<PREC>::R* qlc,   // ql(c)
+                                             const typename Prec<PREC>::R* qrc,   // qr(c)
+                                             const typename Prec<PREC>::R* apdq_c,
+                                             const typename Prec<PREC>::R* amdq_c1,
+                                             typename Prec<PREC>::R* br) {
+  using R = typename Prec<PREC>::R;
+  constexpr int M = P::MEQN;
+  R L[M], Rt[M], dl[M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    if constexpr (Prec<PREC>::EXACT) {
+      L[m] = qlc[m]; Rt[m] = qrc[m]; dl[m] = qrc[m] - qlc[m];
+    } else {
+      L[m] = qc[m] + qlc[m]; Rt[m] = qc[m] + qrc[m]; dl[m] = qrc[m] - qlc[m];
+    }
+  }
+  if constexpr (TF == 1) {
+    R adq[M];
+    P::template tfluct<R>(ph, ixy, L, Rt, dl, auxc, adq);
+#pragma unroll
+    for (int m = 0; m < M; ++m) br[m] = (apdq_c[m] + adq[m]) + amdq_c1[m];       // :151-152
+  } else {
+    R s2[P::MWAVES], am2[M], ap2[M];
+    P::template rp<R>(ph, ixy, L, Rt, dl, auxc, auxc, s2, am2, ap2);             // :181-182
+#pragma unroll
+    for (int m = 0; m < M; ++m) br[m] = ((amdq_c1[m] + apdq_c[m]) + am2[m]) + ap2[m];  // :185-186
+  }
+}
+
+template <class R>
+__device__ __forceinline__ R load_aux(const void* aux, long off) {
+  return (R)static_cast<const R*>(aux)[off];
+}
+
+// ---------------------------------------------------------------------------
+// 1-D stage kernel.  CTA b solves interfaces c = c0 .. c0+NT-1 and updates
+// cells c0 .. c0+NT-2 (c0 = 1 + b*(NT-1)); neighbouring CTAs both solve the
+// interface on their common edge (1/NT redundant work).
+// ---------------------------------------------------------------------------
+template <class P, int CD, int TF, int PREC, int NT>
+__global__ void __launch_bounds__(NT) k_stage1d(StageArgs a) {
+  using R = typename Prec<PREC>::R;
+  using S = typename Prec<PREC>::S;
+  using Ac = typename Prec<PREC>::A;
+  constexpr int M = P::MEQN, MW = P::MWAVES, MA = P::MAUX;
+  __shared__ S sq[M][NT + 8];
+  __shared__ R rec[4][M][NT];   // 0: qr(c-1)  1: ql(c)  2: amdq(c)  3: apdq(c)
+  __shared__ R sred[NT / 32];
+
+  const Ctl* ctl = a.ctl;
+  if (ctl->done) return;
+  const int tid = threadIdx.x;
+  const int mx = a.mx;
+  const int c0 = 1 + blockIdx.x * (NT - 1);
+  const S* qin = static_cast<const S*>(a.buf[ctl->role[a.sd.in]]);
+  const double dt = ctl->dt;
+  const double dtdx0 = dt / a.dx;
+
+  // stage cells c0-3 .. c0+NT+1 (global offset c+2)
+  for (int k = tid; k < NT + 5; k += NT) {
+    const long g = (long)c0 - 1 + k;
+    const bool ok = g < (long)mx + 6;
+#pragma unroll
+    for (int m = 0; m < M; ++m) sq[m][k] = ok ? qin[(long)m * a.plane + g] : (S)1;
+  }
+  __syncthreads();
+
+  // ---- interface phase ----
+  R cflmax = (R)0;
+  int bad = 0;   // a non-finite stage output (reported through ctl->status)
+  {
+    const int c = c0 + tid;
+    if (c <= mx + 1) {
+      R auxm[MA > 0 ? MA : 1], aux0[MA > 0 ? MA : 1];
+#pragma unroll
+      for (int k = 0; k < MA; ++k) {
+        auxm[k] = load_aux<S>(a.aux, (long)k * a.plane + c + 1);
+        aux0[k] = load_aux<S>(a.aux, (long)k * a.plane + c + 2);
+      }
+      auto qs = [&](int k, int m) -> S { return sq[m][tid + k]; };
+      R xl[M], xr[M], am[M], ap[M], s[MW];
+      solve_interface<P, CD, PREC>(a.ph, a.ixy, qs, auxm, aux0, xl, xr, am, ap, s);
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        rec[0][m][tid] = xl[m]; rec[1][m][tid] = xr[m];
+        rec[2][m][tid] = am[m]; rec[3][m][tid] = ap[m];
+      }
+      // flux1.f90:126-133: max(dtdx(i)*s, -dtdx(i-1)*s)
+      double dtdx_c = dtdx0, dtdx_m = dtdx0;
+      if (a.mcapa > 0) {
+        const S* cap = static_cast<const S*>(a.aux) + (long)(a.mcapa - 1) * a.plane;
+        dtdx_c = dt / (a.dx * (double)cap[c + 2]);
+        dtdx_m = dt / (a.dx * (double)cap[c + 1]);
+      }
+#pragma unroll
+      for (int w = 0; w < MW; ++w) {
+        R v1 = (R)dtdx_c * s[w];
+        R v2 = -(R)dtdx_m * s[w];
+        cflmax = nanmax(cflmax, nanmax(v1, v2));
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- cell phase ----
+  {
+    const int c = c0 + tid;
+    if (tid < NT - 1 && c <= mx) {
+      R qc[M], qlc[M], qrc[M], apc[M], amc1[M], br[M];
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        qc[m] = (R)sq[m][tid + 3];
+        qlc[m] = rec[1][m][tid];
+        apc[m] = rec[3][m][tid];
+        qrc[m] = rec[0][m][tid + 1];
+        amc1[m] = rec[2][m][tid + 1];
+      }
+      R auxc[MA > 0 ? MA : 1];
+#pragma unroll
+      for (int k = 0; k < MA; ++k) auxc[k] = load_aux<S>(a.aux, (long)k * a.plane + c + 2);
+      cell_bracket<P, TF, PREC>(a.ph, a.ixy, qc, auxc, qlc, qrc, apc, amc1, br);
+      double dtdx_c = dtdx0;
+      if (a.mcapa > 0) {
+        const S* cap = static_cast<const S*>(a.aux) + (long)(a.mcapa - 1) * a.plane;
+        dtdx_c = dt / (a.dx * (double)cap[c + 2]);
+      }
+      const int kind = a.sd.kind;
+      if (kind == SK_DQ) {
+#pragma unroll
+        for (int m = 0; m < M; ++m)
+          a.dq_out[(long)m * a.plane + c + 2] = (double)((R)0 - (R)dtdx_c * br[m]);
+      } else {
+        S* out = static_cast<S*>(a.buf[ctl->role[a.sd.out]]);
+        S* out2 = a.sd.out2 >= 0 ? static_cast<S*>(a.buf[ctl->role[a.sd.out2]]) : nullptr;
+        const S* qo = a.sd.aux_in >= 0 ? static_cast<const S*>(a.buf[ctl->role[a.sd.aux_in]]) : nullptr;
+        const Images im = images_1d(c, mx, a.mthbc[0], a.mthbc[1]);
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          Ac dqv = (Ac)((R)0 - (R)dtdx_c * br[m]);
+          Ac qv = (Ac)sq[m][tid + 3];
+          Ac qov = qo ? (Ac)qo[(long)m * a.plane + c + 2] : (Ac)0;
+          Ac o1, o2 = (Ac)0;
+          combine<Ac>(kind, qv, qov, dqv, o1, o2);
+          bad |= !isfinite(o1);
+          put_1d<S, Ac>(out, a.plane, m, c, im, o1);
+          if (out2) out2[(long)m * a.plane + c + 2] = (S)o2;
+        }
+      }
+    }
+  }
+
+  // ---- CFL reduction: warp max, block max, one atomic per CTA ----
+  cflmax = warp_max(cflmax);
+  if ((tid & 31) == 0) sred[tid >> 5] = cflmax;
+  const int anybad = __syncthreads_or(bad);
+  if (tid < 32) {
+    R v = (tid < NT / 32) ? sred[tid] : (R)0;
+    v = warp_max(v);
+    if (tid == 0) {
+      atomic_max_nonneg(&a.ctl->stage_cfl[a.stage], (double)v);
+      if (anybad) atomicOr(&a.ctl->status, SCL_STATUS_NONFINITE);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2-D stage kernel (flux2.f90 dimension by dimension).  A CTA owns a TX x TY
+// block of cells; it stages the block plus three ghost layers, solves the
+// (TX+1)*TY x-interfaces and TX*(TY+1) y-interfaces into shared memory, then
+// updates each cell with dq = (0 + dq_x) + dq_y as flux2.f90:52-53,84-85
+// accumulate it.
+// ---------------------------------------------------------------------------
+template <int TX, int TY>
+struct Tile2D {
+  static constexpr int WX = TX + 6, WY = TY + 6;
+  static constexpr int NXI = (TX + 1) * TY, NYI = TX * (TY + 1);
+};
+
+template <class P, int CD, int TF, int PREC, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
+  using R = typename Prec<PREC>::R;
+  using S = typename Prec<PREC>::S;
+  using Ac = typename Prec<PREC>::A;
+  using T = Tile2D<TX, TY>;
+  constexpr int M = P::MEQN, MW = P::MWAVES, MA = P::MAUX;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* sq = reinterpret_cast<S*>(smem_raw);                                  // [M][WY][WX]
+  R* recx = reinterpret_cast<R*>(sq + M * T::WX * T::WY);                  // [4][M][NXI]
+  R* recy = recx + 4 * M * T::NXI;                                         // [4][M][NYI]
+  __shared__ R sred[NT / 32];
+
+  const Ctl* ctl = a.ctl;
+  if (ctl->done) return;
+  const int tid = threadIdx.x;
+  const int nx = a.mx, ny = a.my;
+  const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
+  const S* qin = static_cast<const S*>(a.buf[ctl->role[a.sd.in]]);
+  const double dt = ctl->dt;
+  const double dtdx0 = dt / a.dx, dtdy0 = dt / a.dy;
+
+  // stage the block: cells (i0-3 .. i0+TX+2, j0-3 .. j0+TY+2)
+  for (int k = tid; k < T::WX * T::WY; k += NT) {
+    const int kx = k % T::WX, ky = k / T::WX;
+    const int gi = i0 - 3 + kx, gj = j0 - 3 + ky;  // 1-based cell indices
+    const bool ok = gi <= nx + 3 && gj <= ny + 3;
+    const long off = (long)(gj + 2) * a.pitch + (gi + 2);
+#pragma unroll
+    for (int m = 0; m < M; ++m) sq[(m * T::WY + ky) * T::WX + kx] = ok ? qin[(long)m * a.plane + off] : (S)1;
+  }
+  __syncthreads();
+
+  R cflmax = (R)0;
+  int bad = 0;
+  for (int w = tid; w < T::NXI + T::NYI; w += NT) {
+    const bool isx = w < T::NXI;
+    int li, lj, gi, gj;  // interface between (gi-1,gj) and (gi,gj) [x] or (gi,gj-1) and (gi,gj) [y]
+    if (isx) { li = w % (TX + 1); lj = w / (TX + 1); }
+    else { li = (w - T::NXI) % TX; lj = (w - T::NXI) / TX; }
+    gi = i0 + li; gj = j0 + lj;
+    const bool valid = isx ? (gi <= nx + 1 && gj <= ny) : (gi <= nx && gj <= ny + 1);
+    if (!valid) continue;
+    const int ixy = isx ? 1 : 2;
+    R auxm[MA > 0 ? MA : 1], aux0[MA > 0 ? MA : 1];
+    const long o0 = (long)(gj + 2) * a.pitch + (gi + 2);
+    const long om = isx ? o0 - 1 : o0 - a.pitch;
+#pragma unroll
+    for (int k = 0; k < MA; ++k) {
+      auxm[k] = load_aux<S>(a.aux, (long)k * a.plane + om);
+      aux0[k] = load_aux<S>(a.aux, (long)k * a.plane + o0);
+    }
+    // local smem coordinates of cell (gi, gj): (li+3, lj+3)
+    const int bx = li + 3, by = lj + 3;
+    auto qs = [&](int k, int m) -> S {
+      return isx ? sq[(m * T::WY + by) * T::WX + (bx - 3 + k)]
+                 : sq[(m * T::WY + (by - 3 + k)) * T::WX + bx];
+    };
+    R xl[M], xr[M], am[M], ap[M], s[MW];
+    solve_interface<P, CD, PREC>(a.ph, ixy, qs, auxm, aux0, xl, xr, am, ap, s);
+    R* rec = isx ? recx : recy;
+    const int n = isx ? T::NXI : T::NYI;
+    const int slot = isx ? w : w - T::NXI;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      rec[(0 * M + m) * n + slot] = xl[m];
+      rec[(1 * M + m) * n + slot] = xr[m];
+      rec[(2 * M + m) * n + slot] = am[m];
+      rec[(3 * M + m) * n + slot] = ap[m];
+    }
+    double d_c = isx ? dtdx0 : dtdy0, d_m = d_c;
+    if (a.mcapa > 0) {
+      const S* cap = static_cast<const S*>(a.aux) + (long)(a.mcapa - 1) * a.plane;
+      const double h = isx ? a.dx : a.dy;
+      d_c = dt / (h * (double)cap[o0]);
+      d_m = dt / (h * (double)cap[om]);
+    }
+    // interior lines only; flux2.f90 also scans the ghost lines j=0,ny+1 /
+    // i=0,nx+1, which the ghost-line kernel covers.
+#pragma unroll
+    for (int k = 0; k < MW; ++k) cflmax = nanmax(cflmax, nanmax((R)d_c * s[k], -(R)d_m * s[k]));
+  }
+  __syncthreads();
+
+  const int kind = a.sd.kind;
+  for (int w = tid; w < TX * TY; w += NT) {
+    const int li = w % TX, lj = w / TX;
+    const int gi = i0 + li, gj = j0 + lj;
+    if (gi > nx || gj > ny) continue;
+    const long o0 = (long)(gj + 2) * a.pitch + (gi + 2);
+    R auxc[MA > 0 ? MA : 1];
+#pragma unroll
+    for (int k = 0; k < MA; ++k) auxc[k] = load_aux<S>(a.aux, (long)k * a.plane + o0);
+    R qc[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) qc[m] = (R)sq[(m * T::WY + lj + 3) * T::WX + li + 3];
+    double dx_c = dtdx0, dy_c = dtdy0;
+    if (a.mcapa > 0) {
+      const S* cap = static_cast<const S*>(a.aux) + (long)(a.mcapa - 1) * a.plane;
+      dx_c = dt / (a.dx * (double)cap[o0]);
+      dy_c = dt / (a.dy * (double)cap[o0]);
+    }
+    R dqs[M];
+    {
+      const int sa = li + lj * (TX + 1), sb = sa + 1;
+      R qlc[M], qrc[M], apc[M], amc1[M], br[M];
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        qlc[m] = recx[(1 * M + m) * T::NXI + sa];
+        apc[m] = recx[(3 * M + m) * T::NXI + sa];
+        qrc[m] = recx[(0 * M + m) * T::NXI + sb];
+        amc1[m] = recx[(2 * M + m) * T::NXI + sb];
+      }
+      cell_bracket<P, TF, PREC>(a.ph, 1, qc, auxc, qlc, qrc, apc, amc1, br);
+#pragma unroll
+      for (int m = 0; m < M; ++m) dqs[m] = (R)0 + ((R)0 - (R)dx_c * br[m]);
+    }
+    {
+      const int sa = li + lj * TX, sb = sa + TX;
+      R qlc[M], qrc[M], apc[M], amc1[M], br[M];
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        qlc[m] = recy[(1 * M + m) * T::NYI + sa];
+        apc[m] = recy[(3 * M + m) * T::NYI + sa];
+        qrc[m] = recy[(0 * M + m) * T::NYI + sb];
+        amc1[m] = recy[(2 * M + m) * T::NYI + sb];
+      }
+      cell_bracket<P, TF, PREC>(a.ph, 2, qc, auxc, qlc, qrc, apc, amc1, br);
+#pragma unroll
+      for (int m = 0; m < M; ++m) dqs[m] = dqs[m] + ((R)0 - (R)dy_c * br[m]);
+    }
+    if (kind == SK_DQ) {
+#pragma unroll
+      for (int m = 0; m < M; ++m) a.dq_out[(long)m * a.plane + o0] = (double)dqs[m];
+    } else {
+      S* out = static_cast<S*>(a.buf[ctl->role[a.sd.out]]);
+      S* out2 = a.sd.out2 >= 0 ? static_cast<S*>(a.buf[ctl->role[a.sd.out2]]) : nullptr;
+      const S* qo = a.sd.aux_in >= 0 ? static_cast<const S*>(a.buf[ctl->role[a.sd.aux_in]]) : nullptr;
+      const Images ix = images_1d(gi, nx, a.mthbc[0], a.mthbc[1]);
+      const Images iy = images_1d(gj, ny, a.mthbc[2], a.mthbc[3]);
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        Ac qv = (Ac)sq[(m * T::WY + lj + 3) * T::WX + li + 3];
+        Ac qov = qo ? (Ac)qo[(long)m * a.plane + o0] : (Ac)0;
+        Ac o1, o2 = (Ac)0;
+        combine<Ac>(kind, qv, qov, (Ac)dqs[m], o1, o2);
+        bad |= !isfinite(o1);
+        put_2d<S, Ac>(out, a.plane, a.pitch, m, gi, gj, ix, iy, o1);
+        if (out2) out2[(long)m * a.plane + o0] = (S)o2;
+      }
+    }
+  }
+
+  cflmax = warp_max(cflmax);
+  if ((tid & 31) == 0) sred[tid >> 5] = cflmax;
+  const int anybad = __syncthreads_or(bad);
+  if (tid < 32) {
+    R v = (tid < NT / 32) ? sred[tid] : (R)0;
+    v = warp_max(v);
+    if (tid == 0) {
+      atomic_max_nonneg(&a.ctl->stage_cfl[a.stage], (double)v);
+      if (anybad) atomicOr(&a.ctl->status, SCL_STATUS_NONFINITE);
+    }
+  }
+}
+
+// CFL contribution of the ghost lines that flux2.f90 also sweeps: x-lines
+// j = 0 and ny+1 (interfaces i = 1..nx+1) and y-lines i = 0 and nx+1
+// (interfaces j = 1..ny+1).  One thread per interface, global loads.
+template <class P, int CD, int PREC>
+__global__ void __launch_bounds__(128) k_ghost_cfl2d(StageArgs a) {
+  using R = typename Prec<PREC>::R;
+  using S = typename Prec<PREC>::S;
+  constexpr int M = P::MEQN, MW = P::MWAVES, MA = P::MAUX;
+  __shared__ R sred[4];
+  const Ctl* ctl = a.ctl;
+  if (ctl->done) return;
+  const int nx = a.mx, ny = a.my;
+  const int nxl = nx + 1, nyl = ny + 1;
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  const S* qin = static_cast<const S*>(a.buf[ctl->role[a.sd.in]]);
+  const double dt = ctl->dt;
+  R cflmax = (R)0;
+  if (w < 2 * nxl + 2 * nyl) {
+    int ixy, gi, gj;
+    if (w < 2 * nxl) { ixy = 1; gi = 1 + (w % nxl); gj = (w < nxl) ? 0 : ny + 1; }
+    else { const int v = w - 2 * nxl; ixy = 2; gj = 1 + (v % nyl); gi = (v < nyl) ? 0 : nx + 1; }
+    const long o0 = (long)(gj + 2) * a.pitch + (gi + 2);
+    const long st = (ixy == 1) ? 1 : a.pitch;
+    const long om = o0 - st;
+    R auxm[MA > 0 ? MA : 1], aux0[MA > 0 ? MA : 1];
+#pragma unroll
+    for (int k = 0; k < MA; ++k) {
+      auxm[k] = load_aux<S>(a.aux, (long)k * a.plane + om);
+      aux0[k] = load_aux<S>(a.aux, (long)k * a.plane + o0);
+    }
+    auto qs = [&](int k, int m) -> S { return qin[(long)m * a.plane + o0 + (long)(k - 3) * st]; };
+    R xl[M], xr[M], am[M], ap[M], s[MW];
+    solve_interface<P, CD, PREC>(a.ph, ixy, qs, auxm, aux0, xl, xr, am, ap, s);
+    double d_c = dt / (ixy == 1 ? a.dx : a.dy), d_m = d_c;
+    if (a.mcapa > 0) {
+      const S* cap = static_cast<const S*>(a.aux) + (long)(a.mcapa - 1) * a.plane;
+      const double h = ixy == 1 ? a.dx : a.dy;
+      d_c = dt / (h * (double)cap[o0]);
+      d_m = dt / (h * (double)cap[om]);
+    }
+#pragma unroll
+    for (int k = 0; k < MW; ++k) cflmax = nanmax(cflmax, nanmax((R)d_c * s[k], -(R)d_m * s[k]));
+  }
+  cflmax = warp_max(cflmax);
+  if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = cflmax;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    R v = (threadIdx.x < 4) ? sred[threadIdx.x] : (R)0;
+    v = warp_max(v);
+    if (threadIdx.x == 0) atomic_max_nonneg(&a.ctl->stage_cfl[a.stage], (double)v);
+  }
+}
+
+}  // namespace scl

@@ -1,0 +1,21 @@
+// scl_launch.h -- launcher table shared by the C ABI and the per-precision
+// kernel translation units.
+#pragma once
+#include "scl_common.cuh"
+
+namespace scl {
+
+struct Launchers {
+  void (*stage)(const StageArgs&, cudaStream_t);  // one fused RK stage over the grid
+  void (*ghost)(const StageArgs&, cudaStream_t);  // 2-D ghost-line CFL (nullptr in 1-D)
+};
+
+// One getter per arithmetic form; `variant` selects a tile shape (2-D).
+bool get_launchers_fp64(int rp, int ndim, int cd, int tf, int variant, Launchers* L);
+bool get_launchers_fp64s(int rp, int ndim, int cd, int tf, int variant, Launchers* L);
+bool get_launchers_mixed(int rp, int ndim, int cd, int tf, int variant, Launchers* L);
+bool get_launchers_fp32(int rp, int ndim, int cd, int tf, int variant, Launchers* L);
+
+constexpr int N2D_VARIANTS = 3;
+
+}  // namespace scl

@@ -1,0 +1,383 @@
+// scl_plugins.cuh -- device Riemann solvers, total-fluctuation solvers and
+// eigenvector routines, selected by plugin id.
+//
+// Every reference plugin loops `do i = 2-mbc, mx+mbc` over independent
+// interfaces, so each is restated here as a pointwise function of one
+// interface (rp, evec) or one cell (tfluct), keeping the arithmetic order of
+// the loop body.  States are passed as (left, right) of the Riemann problem:
+// for rp at interface i-1/2 left = qr(i-1), right = ql(i); for tfluct of cell i
+// left = ql(i), right = qr(i).  `dl` is right - left, formed by the caller:
+// in FP64 it is the same subtraction the reference does; in the FP32 forms it
+// is computed from FP64 cell-average jumps, so it keeps the precision of the
+// jump rather than of the states.
+#pragma once
+#include "scl_common.cuh"
+
+namespace scl {
+
+template <class R>
+__device__ __forceinline__ R rmin(R a, R b) { return a < b ? a : b; }
+template <class R>
+__device__ __forceinline__ R rmax(R a, R b) { return a > b ? a : b; }
+
+// ------------------------------------------------------------------------
+// Linear advection, apps/advection/1d/rp1.f:35-43, tfluct1.f:78-87, evec.f:118-121
+// ------------------------------------------------------------------------
+struct PAdvection {
+  static constexpr int MEQN = 1, MWAVES = 1, MAUX = 0, NDIM = 1;
+  static constexpr bool HAS_TFLUCT = true;
+  template <class R>
+  __device__ static void rp(const Phys& ph, int, const R*, const R*, const R* dl, const R*,
+                            const R*, R* s, R* amdq, R* apdq) {
+    const R u = (R)ph.u;
+    s[0] = u;
+    amdq[0] = rmin(u, (R)0) * dl[0];
+    apdq[0] = rmax(u, (R)0) * dl[0];
+  }
+  template <class R>
+  __device__ static void tfluct(const Phys& ph, int, const R*, const R*, const R* dl, const R*,
+                                R* adq) {
+    const R u = (R)ph.u;
+    R am = rmin(u, (R)0) * dl[0];
+    R ap = rmax(u, (R)0) * dl[0];
+    adq[0] = am + ap;
+  }
+  template <class R>
+  __device__ static void evec(const Phys&, int, const R*, const R*, const R*, const R*,
+                              R evl[1][1], R evr[1][1]) {
+    evl[0][0] = (R)1;
+    evr[0][0] = (R)1;
+  }
+};
+
+// ------------------------------------------------------------------------
+// 1-D Euler, Roe solver with Harten-Hyman entropy fix,
+// apps/euler/shockentropy/rp1eu.f:44-213.  No tfluct exists for this family
+// (the app runs with tfluct_solver = 0, the swap path of flux1.f90:155-188).
+// ------------------------------------------------------------------------
+struct PEuler {
+  static constexpr int MEQN = 3, MWAVES = 3, MAUX = 0, NDIM = 1;
+  static constexpr bool HAS_TFLUCT = false;
+
+  template <class R>
+  __device__ static void roe(const Phys& ph, const R* L, const R* Rt, R& u, R& enth, R& a) {
+    const R g1 = (R)ph.gamma1;
+    R rhsqrtl = sqrt(L[0]);
+    R rhsqrtr = sqrt(Rt[0]);
+    R pl = g1 * (L[2] - ((R)0.5 * (L[1] * L[1])) / L[0]);
+    R pr = g1 * (Rt[2] - ((R)0.5 * (Rt[1] * Rt[1])) / Rt[0]);
+    R rhsq2 = rhsqrtl + rhsqrtr;
+    u = (L[1] / rhsqrtl + Rt[1] / rhsqrtr) / rhsq2;
+    enth = ((L[2] + pl) / rhsqrtl + (Rt[2] + pr) / rhsqrtr) / rhsq2;
+    R a2 = g1 * (enth - (R)0.5 * (u * u));
+    a = sqrt(a2);
+  }
+
+  template <class R>
+  __device__ static void rp(const Phys& ph, int, const R* L, const R* Rt, const R* dl, const R*,
+                            const R*, R* s, R* amdq, R* apdq) {
+    const R gamma = (R)ph.gamma, g1 = (R)ph.gamma1;
+    R u, enth, a;
+    roe(ph, L, Rt, u, enth, a);                                   // rp1eu.f:44-55
+    R a2 = (g1 / (a * a)) * (((enth - u * u) * dl[0] + u * dl[1]) - dl[2]);   // :65-66
+    R a3 = ((dl[1] + (a - u) * dl[0]) - a * a2) / ((R)2 * a);                   // :67
+    R a1 = (dl[0] - a2) - a3;                                                   // :68
+    R w[3][3];  // w[wave][component]
+    w[0][0] = a1; w[0][1] = a1 * (u - a); w[0][2] = a1 * (enth - u * a);
+    w[1][0] = a2; w[1][1] = a2 * u;       w[1][2] = (a2 * (R)0.5) * (u * u);
+    w[2][0] = a3; w[2][1] = a3 * (u + a); w[2][2] = a3 * (enth + u * a);
+    s[0] = u - a; s[1] = u; s[2] = u + a;
+    if (!ph.efix) {                                                            // :100-111
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        R am = (R)0, ap = (R)0;
+#pragma unroll
+        for (int mw = 0; mw < 3; ++mw) {
+          if (s[mw] < (R)0) am = am + s[mw] * w[mw][m];
+          else ap = ap + s[mw] * w[mw][m];
+        }
+        amdq[m] = am; apdq[m] = ap;
+      }
+      return;
+    }
+    // entropy fix, rp1eu.f:126-201
+    do {
+      R rhoim1 = L[0];
+      R pim1 = g1 * (L[2] - ((R)0.5 * (L[1] * L[1])) / rhoim1);
+      R cim1 = sqrt((gamma * pim1) / rhoim1);
+      R s0 = L[1] / rhoim1 - cim1;
+      if (s0 >= (R)0 && s[0] > (R)0) {
+        amdq[0] = amdq[1] = amdq[2] = (R)0;
+        break;
+      }
+      R rho1 = L[0] + w[0][0];
+      R rhou1 = L[1] + w[0][1];
+      R en1 = L[2] + w[0][2];
+      R p1 = g1 * (en1 - ((R)0.5 * (rhou1 * rhou1)) / rho1);
+      R c1 = sqrt((gamma * p1) / rho1);
+      R s1 = rhou1 / rho1 - c1;
+      R sfract;
+      if (s0 < (R)0 && s1 > (R)0) sfract = (s0 * (s1 - s[0])) / (s1 - s0);
+      else if (s[0] < (R)0) sfract = s[0];
+      else sfract = (R)0;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) amdq[m] = sfract * w[0][m];
+      if (s[1] >= (R)0) break;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) amdq[m] = amdq[m] + s[1] * w[1][m];
+      R rhoi = Rt[0];
+      R pi = g1 * (Rt[2] - ((R)0.5 * (Rt[1] * Rt[1])) / rhoi);
+      R ci = sqrt((gamma * pi) / rhoi);
+      R s3 = Rt[1] / rhoi + ci;
+      R rho2 = Rt[0] - w[2][0];
+      R rhou2 = Rt[1] - w[2][1];
+      R en2 = Rt[2] - w[2][2];
+      R p2 = g1 * (en2 - ((R)0.5 * (rhou2 * rhou2)) / rho2);
+      R c2 = sqrt((gamma * p2) / rho2);
+      R s2 = rhou2 / rho2 + c2;
+      if (s2 < (R)0 && s3 > (R)0) sfract = (s2 * (s3 - s[2])) / (s3 - s2);
+      else if (s[2] < (R)0) sfract = s[2];
+      else break;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) amdq[m] = amdq[m] + sfract * w[2][m];
+    } while (0);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {                                                // :206-213
+      R df = (R)0;
+#pragma unroll
+      for (int mw = 0; mw < 3; ++mw) df = df + s[mw] * w[mw][m];
+      apdq[m] = df - amdq[m];
+    }
+  }
+
+  template <class R>
+  __device__ static void tfluct(const Phys&, int, const R*, const R*, const R*, const R*, R*) {}
+
+  // Roe eigenvectors (new; the reference's evec1eu.f is incomplete).  Averages
+  // as rp1eu.f:44-55 from the cell averages q(i-1), q(i).
+  template <class R>
+  __device__ static void evec(const Phys& ph, int, const R* qm, const R* q0, const R*, const R*,
+                              R evl[3][3], R evr[3][3]) {
+    const R g1 = (R)ph.gamma1;
+    R rhsqrtl = sqrt(qm[0]);
+    R rhsqrtr = sqrt(q0[0]);
+    R pl = g1 * (qm[2] - ((R)0.5 * (qm[1] * qm[1])) / qm[0]);
+    R pr = g1 * (q0[2] - ((R)0.5 * (q0[1] * q0[1])) / q0[0]);
+    R rhsq2 = rhsqrtl + rhsqrtr;
+    R u = (qm[1] / rhsqrtl + q0[1] / rhsqrtr) / rhsq2;
+    R h = ((qm[2] + pl) / rhsqrtl + (q0[2] + pr) / rhsqrtr) / rhsq2;
+    R a2 = g1 * (h - (R)0.5 * (u * u));
+    R a = sqrt(a2);
+    // evr[m][p] = evr(i,m,p): component m of right eigenvector p
+    evr[0][0] = (R)1;        evr[0][1] = (R)1;               evr[0][2] = (R)1;
+    evr[1][0] = u - a;       evr[1][1] = u;                  evr[1][2] = u + a;
+    evr[2][0] = h - u * a;   evr[2][1] = (R)0.5 * (u * u);   evr[2][2] = h + u * a;
+    R b1 = g1 / a2;
+    R b2 = (R)0.5 * (b1 * (u * u));
+    R ua = u / a;
+    R ra = (R)1 / a;
+    R b1u = b1 * u;
+    // evl[p][m] = evl(i,p,m): component m of left eigenvector p
+    evl[0][0] = (R)0.5 * (b2 + ua); evl[0][1] = (R)(-0.5) * (b1u + ra); evl[0][2] = (R)0.5 * b1;
+    evl[1][0] = (R)1 - b2;          evl[1][1] = b1u;                    evl[1][2] = -b1;
+    evl[2][0] = (R)0.5 * (b2 - ua); evl[2][1] = (R)(-0.5) * (b1u - ra); evl[2][2] = (R)0.5 * b1;
+  }
+};
+
+// ------------------------------------------------------------------------
+// 2-D shallow water Roe solver along a slice,
+// apps/shallowWater/2dRadialDam/rpn2sw.f:60-228 and tfluct1sw.f:297-467.
+// ------------------------------------------------------------------------
+struct PShallow2D {
+  static constexpr int MEQN = 3, MWAVES = 3, MAUX = 0, NDIM = 2;
+  static constexpr bool HAS_TFLUCT = true;
+
+  template <class R>
+  __device__ static void solve(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl,
+                               R* s, R* amdq, R* apdq) {
+    const R g = (R)ph.grav;
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    R h = (L[0] + Rt[0]) * (R)0.50;                                       // rpn2sw.f:80-88
+    R hsqrtl = sqrt(L[0]);
+    R hsqrtr = sqrt(Rt[0]);
+    R hsq2 = hsqrtl + hsqrtr;
+    R u = (L[mu] / hsqrtl + Rt[mu] / hsqrtr) / hsq2;
+    R v = (L[mv] / hsqrtl + Rt[mv] / hsqrtr) / hsq2;
+    R a = sqrt(g * h);
+    R a1 = ((u + a) * dl[0] - dl[mu]) * ((R)0.50 / a);                   // :98-100
+    R a2 = -(v * dl[0]) + dl[mv];
+    R a3 = (-((u - a) * dl[0]) + dl[mu]) * ((R)0.50 / a);
+    R w[3][3];
+    w[0][0] = a1; w[0][mu] = a1 * (u - a); w[0][mv] = a1 * v;
+    w[1][0] = (R)0; w[1][mu] = (R)0;       w[1][mv] = a2;
+    w[2][0] = a3; w[2][mu] = a3 * (u + a); w[2][mv] = a3 * v;
+    s[0] = u - a; s[1] = u; s[2] = u + a;
+    if (!ph.efix) {                                                         // :132-143
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        R am = (R)0, ap = (R)0;
+#pragma unroll
+        for (int mw = 0; mw < 3; ++mw) {
+          if (s[mw] < (R)0) am = am + s[mw] * w[mw][m];
+          else ap = ap + s[mw] * w[mw][m];
+        }
+        amdq[m] = am; apdq[m] = ap;
+      }
+      return;
+    }
+    do {                                                                    // :158-217
+      R him1 = L[0];
+      R s0 = L[mu] / him1 - sqrt(g * him1);
+      if (s0 > (R)0 && s[0] > (R)0) {
+        amdq[0] = amdq[1] = amdq[2] = (R)0;
+        break;
+      }
+      R h1 = L[0] + w[0][0];
+      R hu1 = L[mu] + w[0][mu];
+      R s1 = hu1 / h1 - sqrt(g * h1);
+      R sfract;
+      if (s0 < (R)0 && s1 > (R)0) sfract = s0 * ((s1 - s[0]) / (s1 - s0));
+      else if (s[0] < (R)0) sfract = s[0];
+      else sfract = (R)0;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) amdq[m] = sfract * w[0][m];
+      if (s[1] > (R)0) break;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) amdq[m] = amdq[m] + s[1] * w[1][m];
+      R hi = Rt[0];
+      R s03 = Rt[mu] / hi + sqrt(g * hi);
+      R h3 = Rt[0] - w[2][0];
+      R hu3 = Rt[mu] - w[2][mu];
+      R s3 = hu3 / h3 + sqrt(g * h3);
+      if (s3 < (R)0 && s03 > (R)0) sfract = s3 * ((s03 - s[2]) / (s03 - s3));
+      else if (s[2] < (R)0) sfract = s[2];
+      else break;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) amdq[m] = amdq[m] + sfract * w[2][m];
+    } while (0);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {                                           // :221-228
+      R df = (R)0;
+#pragma unroll
+      for (int mw = 0; mw < 3; ++mw) df = df + s[mw] * w[mw][m];
+      apdq[m] = df - amdq[m];
+    }
+  }
+
+  template <class R>
+  __device__ static void rp(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl, const R*,
+                            const R*, R* s, R* amdq, R* apdq) {
+    solve(ph, ixy, L, Rt, dl, s, amdq, apdq);
+  }
+  // tfluct1sw.f: the same Roe solve with left ql(i), right qr(i); adq = amdq+apdq
+  template <class R>
+  __device__ static void tfluct(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl,
+                                const R*, R* adq) {
+    R s[3], am[3], ap[3];
+    solve(ph, ixy, L, Rt, dl, s, am, ap);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) adq[m] = am[m] + ap[m];
+  }
+  // Shallow-water Roe eigenvectors along ixy (new; the reference has none).
+  // Averages as rpn2sw.f:80-88; left eigenvectors are the rows rpn2sw.f:98-100
+  // uses for a1..a3.
+  template <class R>
+  __device__ static void evec(const Phys& ph, int ixy, const R* qm, const R* q0, const R*,
+                              const R*, R evl[3][3], R evr[3][3]) {
+    const R g = (R)ph.grav;
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    R h = (qm[0] + q0[0]) * (R)0.50;
+    R hsqrtl = sqrt(qm[0]);
+    R hsqrtr = sqrt(q0[0]);
+    R hsq2 = hsqrtl + hsqrtr;
+    R u = (qm[mu] / hsqrtl + q0[mu] / hsqrtr) / hsq2;
+    R v = (qm[mv] / hsqrtl + q0[mv] / hsqrtr) / hsq2;
+    R a = sqrt(g * h);
+    R ha = (R)0.50 / a;
+    evr[0][0] = (R)1;  evr[mu][0] = u - a; evr[mv][0] = v;
+    evr[0][1] = (R)0;  evr[mu][1] = (R)0;  evr[mv][1] = (R)1;
+    evr[0][2] = (R)1;  evr[mu][2] = u + a; evr[mv][2] = v;
+    evl[0][0] = (u + a) * ha;    evl[0][mu] = -ha;    evl[0][mv] = (R)0;
+    evl[1][0] = -v;              evl[1][mu] = (R)0;   evl[1][mv] = (R)1;
+    evl[2][0] = -((u - a) * ha); evl[2][mu] = ha;     evl[2][mv] = (R)0;
+  }
+};
+
+// ------------------------------------------------------------------------
+// Variable-coefficient acoustics, aux(:,1) = impedance Z, aux(:,2) = c.
+// 1-D: apps/acoustics/1d/interface/rp1acv.f:49-80, tfluct1acv.f:134-166,
+// evec.f90:196-206.  2-D (new): the same solve normal to the slice
+// (mu = normal velocity), the tangential velocity carries no wave.
+// ------------------------------------------------------------------------
+template <int NEQ>
+struct PAcoustics {
+  static constexpr int MEQN = NEQ, MWAVES = 2, MAUX = 2, NDIM = (NEQ == 2 ? 1 : 2);
+  static constexpr bool HAS_TFLUCT = true;
+  template <class R>
+  __device__ static void rp(const Phys&, int ixy, const R*, const R*, const R* dl, const R* auxl,
+                            const R* auxr, R* s, R* amdq, R* apdq) {
+    // auxl = aux of the left cell (auxr(i-1,:)), auxr = aux of the right cell (auxl(i,:))
+    const int mu = (ixy == 1) ? 1 : 2;
+    R zi = auxr[0];
+    R zim = auxl[0];
+    R a1 = ((-dl[0]) + zi * dl[mu]) / (zim + zi);
+    R a2 = (dl[0] + zim * dl[mu]) / (zim + zi);
+    s[0] = -auxl[1];
+    s[1] = auxr[1];
+    R w1[NEQ], w2[NEQ];
+#pragma unroll
+    for (int m = 0; m < NEQ; ++m) { w1[m] = (R)0; w2[m] = (R)0; }
+    w1[0] = -(a1 * zim); w1[mu] = a1;
+    w2[0] = a2 * zi;     w2[mu] = a2;
+#pragma unroll
+    for (int m = 0; m < NEQ; ++m) {
+      amdq[m] = s[0] * w1[m];
+      apdq[m] = s[1] * w2[m];
+    }
+  }
+  template <class R>
+  __device__ static void tfluct(const Phys&, int ixy, const R*, const R*, const R* dl,
+                                const R* aux, R* adq) {
+    const int mu = (ixy == 1) ? 1 : 2;
+    R zi = aux[0];
+    R zim = aux[0];
+    R a1 = ((-dl[0]) + zi * dl[mu]) / (zim + zi);
+    R a2 = (dl[0] + zim * dl[mu]) / (zim + zi);
+    R s1 = -aux[1], s2 = aux[1];
+    R w1[NEQ], w2[NEQ];
+#pragma unroll
+    for (int m = 0; m < NEQ; ++m) { w1[m] = (R)0; w2[m] = (R)0; }
+    w1[0] = -(a1 * zim); w1[mu] = a1;
+    w2[0] = a2 * zi;     w2[mu] = a2;
+#pragma unroll
+    for (int m = 0; m < NEQ; ++m) {
+      R am = s1 * w1[m];
+      R ap = s2 * w2[m];
+      adq[m] = am + ap;
+    }
+  }
+  template <class R>
+  __device__ static void evec(const Phys&, int ixy, const R*, const R*, const R* auxm,
+                              const R* aux0, R evl[NEQ][NEQ], R evr[NEQ][NEQ]) {
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+#pragma unroll
+    for (int a = 0; a < NEQ; ++a)
+#pragma unroll
+      for (int b = 0; b < NEQ; ++b) { evl[a][b] = (R)0; evr[a][b] = (R)0; }
+    evr[0][0] = -auxm[0];
+    evr[0][1] = aux0[0];
+    evr[mu][0] = (R)1;
+    evr[mu][1] = (R)1;
+    R z = (R)1 / (auxm[0] + aux0[0]);
+    evl[0][0] = (R)(-1) * z;
+    evl[0][mu] = aux0[0] * z;
+    evl[1][0] = (R)1 * z;
+    evl[1][mu] = auxm[0] * z;
+    if (NEQ == 3) {
+      evr[mv][2] = (R)1;
+      evl[2][mv] = (R)1;
+    }
+  }
+};
+
+}  // namespace scl

@@ -1,0 +1,5 @@
+// Kernel instantiations of one arithmetic form (SCL_FP32).
+#define SCL_PREC_VALUE SCL_FP32
+#define SCL_PREC_NS prec_fp32
+#define SCL_PREC_GETTER get_launchers_fp32
+#include "scl_dispatch.cuh"

@@ -1,0 +1,193 @@
+// scl_weno.cuh -- WENO5 reconstruction at one interface (src/reconstruct.f90).
+//
+// Interface c-1/2 sits between cells c-1 and c.  The five cell-average jumps
+// d[k] = q(c-3+k+1) - q(c-3+k), k = 0..4, are dq(c-2) .. dq(c+2) of the
+// reference (reconstruct.f90:96-99, 166-169).  Side 1 (m1=1) builds qr(c-1)
+// from dq(c-2..c+1); side 2 (m1=2) builds ql(c) from dq(c+2..c-1) with
+// im = -1 (reconstruct.f90:108-132, 196-229).
+//
+// Two arithmetic forms:
+//  * exact (double): the reference's operations in the reference's order;
+//  * scaled (float): the same algebra on jumps divided by their largest
+//    magnitude, with epsilon set in the scaled range.  The reference's product
+//    form s1 = tt2*tt3 of fourth powers under- and overflows in FP32; scaling
+//    keeps every product within float range while leaving the weights
+//    unchanged (they are homogeneous of degree 0 in the jumps).
+#pragma once
+#include "scl_common.cuh"
+
+namespace scl {
+
+// reconstruct.f90:6 `double precision :: epweno = 1.e-36` (a REAL(4) literal)
+__device__ __forceinline__ double epweno() { return (double)1.0e-36f; }
+// epsilon of the scaled FP32 form: the squared smoothness indicators then lie
+// in [1e-16, 1e4], so every weight product stays between 1e-32 and 1e9.
+constexpr float EPS_SCALED = 1.0e-8f;
+
+// One side of the WENO5 correction, reference order (reconstruct.f90:113-132).
+__device__ __forceinline__ double weno_side(double dm2, double dm1, double d0, double dp1,
+                                            double im) {
+  double t1 = im * (dm2 - dm1);
+  double t2 = im * (dm1 - d0);
+  double t3 = im * (d0 - dp1);
+  double x1 = dm2 - 3.0 * dm1;
+  double x2 = dm1 + d0;
+  double x3 = 3.0 * d0 - dp1;
+  double tt1 = 13.0 * (t1 * t1) + 3.0 * (x1 * x1);
+  double tt2 = 13.0 * (t2 * t2) + 3.0 * (x2 * x2);
+  double tt3 = 13.0 * (t3 * t3) + 3.0 * (x3 * x3);
+  const double ep = epweno();
+  tt1 = (ep + tt1) * (ep + tt1);
+  tt2 = (ep + tt2) * (ep + tt2);
+  tt3 = (ep + tt3) * (ep + tt3);
+  double s1 = tt2 * tt3;
+  double s2 = (6.0 * tt1) * tt3;
+  double s3 = (3.0 * tt1) * tt2;
+  double t0 = 1.0 / ((s1 + s2) + s3);
+  s1 = s1 * t0;
+  s3 = s3 * t0;
+  return ((s1 * (t2 - t1)) + ((0.5 * s3 - 0.25) * (t3 - t2))) / 3.0;
+}
+
+// Scaled FP32 form of weno_side on jumps already divided by `scale`.
+__device__ __forceinline__ float weno_side_scaled(float dm2, float dm1, float d0, float dp1,
+                                                  float im) {
+  float t1 = im * (dm2 - dm1);
+  float t2 = im * (dm1 - d0);
+  float t3 = im * (d0 - dp1);
+  float x1 = dm2 - 3.0f * dm1;
+  float x2 = dm1 + d0;
+  float x3 = 3.0f * d0 - dp1;
+  float tt1 = 13.0f * (t1 * t1) + 3.0f * (x1 * x1);
+  float tt2 = 13.0f * (t2 * t2) + 3.0f * (x2 * x2);
+  float tt3 = 13.0f * (t3 * t3) + 3.0f * (x3 * x3);
+  tt1 = (EPS_SCALED + tt1) * (EPS_SCALED + tt1);
+  tt2 = (EPS_SCALED + tt2) * (EPS_SCALED + tt2);
+  tt3 = (EPS_SCALED + tt3) * (EPS_SCALED + tt3);
+  float s1 = tt2 * tt3;
+  float s2 = (6.0f * tt1) * tt3;
+  float s3 = (3.0f * tt1) * tt2;
+  float t0 = __frcp_rn((s1 + s2) + s3);
+  s1 = s1 * t0;
+  s3 = s3 * t0;
+  return ((s1 * (t2 - t1)) + ((0.5f * s3 - 0.25f) * (t3 - t2))) * (1.0f / 3.0f);
+}
+
+// Both sides of the scaled correction for one set of five jumps h[0..4].
+__device__ __forceinline__ void weno_pair_scaled(const float h[5], float& u1, float& u2) {
+  float sc = fmaxf(fmaxf(fmaxf(fabsf(h[0]), fabsf(h[1])), fmaxf(fabsf(h[2]), fabsf(h[3]))),
+                   fabsf(h[4]));
+  if (!(sc > 0.0f) || !(sc < 3.0e38f)) {  // all-zero stencil (or non-finite)
+    u1 = (sc == 0.0f) ? 0.0f : sc;
+    u2 = u1;
+    return;
+  }
+  float inv = __frcp_rn(sc);
+  float n0 = h[0] * inv, n1 = h[1] * inv, n2 = h[2] * inv, n3 = h[3] * inv, n4 = h[4] * inv;
+  u1 = weno_side_scaled(n0, n1, n2, n3, 1.0f) * sc;
+  u2 = weno_side_scaled(n4, n3, n2, n1, -1.0f) * sc;
+}
+
+// ---------------------------------------------------------------------------
+// Exact form (FP64): returns the reconstructed states qr(c-1) (qrl) and ql(c)
+// (qlr).  q[k][m] holds cells c-3+k, k = 0..5.
+// ---------------------------------------------------------------------------
+template <int M>
+__device__ __forceinline__ void weno5_exact(const double q[6][M], double qrl[M], double qlr[M]) {
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    double d[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) d[k] = q[k + 1][m] - q[k][m];
+    double c = ((-q[1][m]) + 7.0 * (q[2][m] + q[3][m])) - q[4][m];
+    qrl[m] = weno_side(d[0], d[1], d[2], d[3], 1.0) + c / 12.0;
+    qlr[m] = weno_side(d[4], d[3], d[2], d[1], -1.0) + c / 12.0;
+  }
+}
+
+// reconstruct.f90:146-241 for one interface; evl[p][m] = evl(i,p,m),
+// evr[m][p] = evr(i,m,p).
+template <int M>
+__device__ __forceinline__ void weno5_char_exact(const double q[6][M], const double evl[M][M],
+                                                 const double evr[M][M], double qrl[M],
+                                                 double qlr[M]) {
+  double d[5][M];
+#pragma unroll
+  for (int k = 0; k < 5; ++k)
+#pragma unroll
+    for (int m = 0; m < M; ++m) d[k][m] = q[k + 1][m] - q[k][m];
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    double c = ((-q[1][m]) + 7.0 * (q[2][m] + q[3][m])) - q[4][m];
+    qrl[m] = c / 12.0;
+    qlr[m] = qrl[m];
+  }
+#pragma unroll
+  for (int p = 0; p < M; ++p) {
+    double h[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      double s = 0.0;
+#pragma unroll
+      for (int m = 0; m < M; ++m) s = s + evl[p][m] * d[k][m];
+      h[k] = s;
+    }
+    double u1 = weno_side(h[0], h[1], h[2], h[3], 1.0);
+    double u2 = weno_side(h[4], h[3], h[2], h[1], -1.0);
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      qrl[m] = qrl[m] + evr[m][p] * u1;
+      qlr[m] = qlr[m] + evr[m][p] * u2;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Offset form (FP32): from the jumps d[k][m] (formed in the storage precision)
+// return er = qr(c-1) - q(c-1) and el = ql(c) - q(c).  The linear part is the
+// reference's central stencil (-q(c-2)+7q(c-1)+7q(c)-q(c+1))/12 rewritten in
+// jumps: minus q(c-1) it is (d(c-1)+6d(c)-d(c+1))/12, minus q(c) it is
+// (d(c-1)-6d(c)-d(c+1))/12.
+// ---------------------------------------------------------------------------
+template <int M>
+__device__ __forceinline__ void weno5_offset(const float d[5][M], float er[M], float el[M]) {
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    float h[5] = {d[0][m], d[1][m], d[2][m], d[3][m], d[4][m]};
+    float u1, u2;
+    weno_pair_scaled(h, u1, u2);
+    er[m] = (d[1][m] + 6.0f * d[2][m] - d[3][m]) * (1.0f / 12.0f) + u1;
+    el[m] = (d[1][m] - 6.0f * d[2][m] - d[3][m]) * (1.0f / 12.0f) + u2;
+  }
+}
+
+template <int M>
+__device__ __forceinline__ void weno5_char_offset(const float d[5][M], const float evl[M][M],
+                                                  const float evr[M][M], float er[M],
+                                                  float el[M]) {
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    er[m] = (d[1][m] + 6.0f * d[2][m] - d[3][m]) * (1.0f / 12.0f);
+    el[m] = (d[1][m] - 6.0f * d[2][m] - d[3][m]) * (1.0f / 12.0f);
+  }
+#pragma unroll
+  for (int p = 0; p < M; ++p) {
+    float h[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      float s = 0.0f;
+#pragma unroll
+      for (int m = 0; m < M; ++m) s = s + evl[p][m] * d[k][m];
+      h[k] = s;
+    }
+    float u1, u2;
+    weno_pair_scaled(h, u1, u2);
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      er[m] = er[m] + evr[m][p] * u1;
+      el[m] = el[m] + evr[m][p] * u2;
+    }
+  }
+}
+
+}  // namespace scl

@@ -1,0 +1,121 @@
+"""Problem set-ups shared by the oracle and GPU tests (seeded, small)."""
+import numpy as np
+
+from oracle import oracle as O
+import sharpclaw_b200 as S
+
+
+def advection(mx=200, seed=1, mthbc=(2, 2), char_decomp=0, tfluct_solver=1):
+    """Periodic advection with the C1 initial data: a Gaussian, a square pulse
+    and four seeded sinusoids, point values at cell centres."""
+    dx = 1.0 / mx
+    rng = np.random.default_rng(seed)
+    xc = (np.arange(mx) + 0.5) * dx
+    q0 = np.exp(-200.0 * (xc - 0.3) ** 2) + ((xc > 0.6) & (xc < 0.8))
+    for _ in range(4):
+        k = rng.integers(1, 9)
+        q0 = q0 + rng.uniform(0, 0.1) * np.sin(2 * np.pi * k * xc)
+    q = np.zeros((1, mx + 6))
+    q[0, 3:-3] = q0
+    kw = dict(mx=mx, dx=dx, mthbc=mthbc, char_decomp=char_decomp, tfluct_solver=tfluct_solver)
+    po = O.make_params(meqn=1, mwaves=1, rp=O.RP_ADVECTION, u=1.0, **kw)
+    ps = S.ClawParams(rp=S.RP_ADVECTION, u=1.0, **kw)
+    return po, ps, q, None
+
+
+def shu_osher(mx=400, gamma=1.4, char_decomp=2, mthbc=(1, 1), perturb=0.0, seed=2):
+    """Shu-Osher shock/entropy-wave interaction on [-5, 5]
+    (apps/euler/shockentropy/qinit.f:299-323)."""
+    xlower, xupper = -5.0, 5.0
+    dx = (xupper - xlower) / mx
+    xc = xlower + (np.arange(1, mx + 1) - 0.5) * dx
+    g1 = gamma - 1.0
+    rhol, ul, pl = 3.857143, 2.629369, 10.333333
+    rho = np.where(xc < -4.0, rhol, 1.0 + 0.2 * np.sin(5.0 * xc))
+    mom = np.where(xc < -4.0, rhol * ul, 0.0)
+    en = np.where(xc < -4.0, pl / g1 + 0.5 * rhol * ul ** 2, 1.0 / g1)
+    if perturb:
+        rng = np.random.default_rng(seed)
+        mom = mom + perturb * rng.standard_normal(mx)
+    q = np.zeros((3, mx + 6))
+    q[0, 3:-3], q[1, 3:-3], q[2, 3:-3] = rho, mom, en
+    kw = dict(mx=mx, dx=dx, xlower=xlower, mthbc=mthbc, char_decomp=char_decomp, tfluct_solver=0)
+    po = O.make_params(meqn=3, mwaves=3, rp=O.RP_EULER, gamma=gamma, **kw)
+    ps = S.ClawParams(rp=S.RP_EULER, gamma=gamma, **kw)
+    return po, ps, q, None
+
+
+def riemann(mx=300, rho=(1.0, 0.125), u=(0.0, 0.0), p=(1.0, 0.1), gamma=1.4, char_decomp=0):
+    """1-D Euler Riemann problem on [0,1], jump at 0.5, extrapolation bc."""
+    dx = 1.0 / mx
+    xc = (np.arange(mx) + 0.5) * dx
+    left = xc < 0.5
+    r = np.where(left, rho[0], rho[1])
+    v = np.where(left, u[0], u[1])
+    pr = np.where(left, p[0], p[1])
+    q = np.zeros((3, mx + 6))
+    q[0, 3:-3], q[1, 3:-3], q[2, 3:-3] = r, r * v, pr / (gamma - 1) + 0.5 * r * v * v
+    kw = dict(mx=mx, dx=dx, mthbc=(1, 1), char_decomp=char_decomp, tfluct_solver=0)
+    po = O.make_params(meqn=3, mwaves=3, rp=O.RP_EULER, gamma=gamma, **kw)
+    ps = S.ClawParams(rp=S.RP_EULER, gamma=gamma, **kw)
+    return po, ps, q, None
+
+
+def acoustics1d(mx=200, rho=(1.0, 4.0), c=(1.0, 0.5), char_decomp=0, tfluct_solver=1, mthbc=(2, 2)):
+    from acoustics_exact import InterfaceProblem
+    ap = InterfaceProblem(rho=rho, c=c)
+    dx = 20.0 / mx
+    aux = ap.setaux(mx)
+    q = ap.qinit(mx, aux)
+    kw = dict(mx=mx, dx=dx, xlower=-10.0, mthbc=mthbc, char_decomp=char_decomp,
+              tfluct_solver=tfluct_solver)
+    po = O.make_params(meqn=2, mwaves=2, maux=2, rp=O.RP_ACOUSTICS1D, **kw)
+    ps = S.ClawParams(rp=S.RP_ACOUSTICS1D, **kw)
+    return po, ps, q, aux
+
+
+def radial_dam(n=48, noise=1e-3, seed=3, char_decomp=2, tfluct_solver=1, mthbc=(2, 2, 2, 2), efix=0):
+    """2-D shallow-water radial dam break on [-2.5,2.5]^2: h = 2 inside r < 0.5,
+    1 outside (cell-centre test), hu = hv = 0, seeded N(0, noise) on h."""
+    lo, hi = -2.5, 2.5
+    d = (hi - lo) / n
+    xc = lo + (np.arange(n) + 0.5) * d
+    X, Y = np.meshgrid(xc, xc, indexing="xy")   # [j, i]
+    h = np.where(X ** 2 + Y ** 2 < 0.25, 2.0, 1.0)
+    if noise:
+        h = h + noise * np.random.default_rng(seed).standard_normal(h.shape)
+    q = np.zeros((3, n + 6, n + 6))
+    q[0, 3:-3, 3:-3] = h
+    kw = dict(mx=n, my=n, dx=d, dy=d, xlower=lo, ylower=lo, mthbc=mthbc, char_decomp=char_decomp,
+              tfluct_solver=tfluct_solver, efix=efix)
+    po = O.make_params(ndim=2, meqn=3, mwaves=3, rp=O.RP_SW2D, grav=1.0, **kw)
+    ps = S.ClawParams(rp=S.RP_SW2D, grav=1.0, **kw)
+    return po, ps, q, None
+
+
+def acoustics2d(n=40, seed=5, char_decomp=0, tfluct_solver=1, mthbc=(2, 2, 2, 2)):
+    """2-D variable-coefficient acoustics on [0,1]^2: rho, K log-normal,
+    smoothed; aux = (Z = sqrt(rho K), c = sqrt(K/rho)); p0 = Gaussian bumps."""
+    rng = np.random.default_rng(seed)
+    d = 1.0 / n
+    ln_rho = rng.normal(0, 0.3, (n + 6, n + 6))
+    ln_k = rng.normal(0, 0.3, (n + 6, n + 6))
+    ker = np.exp(-0.5 * (np.arange(-6, 7) / 2.0) ** 2)
+    ker /= ker.sum()
+    for a in (ln_rho, ln_k):
+        for ax in (0, 1):
+            a[...] = np.apply_along_axis(lambda v: np.convolve(v, ker, mode="same"), ax, a)
+    rho, K = np.exp(ln_rho), np.exp(ln_k)
+    aux = np.stack([np.sqrt(rho * K), np.sqrt(K / rho)])
+    xc = (np.arange(-3, n + 3) + 0.5) * d
+    X, Y = np.meshgrid(xc, xc, indexing="xy")
+    p = np.zeros_like(X)
+    for _ in range(3):
+        cx, cy = rng.uniform(0.2, 0.8, 2)
+        p += np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * 0.05 ** 2))
+    q = np.zeros((3, n + 6, n + 6))
+    q[0] = p
+    kw = dict(mx=n, my=n, dx=d, dy=d, mthbc=mthbc, char_decomp=char_decomp, tfluct_solver=tfluct_solver)
+    po = O.make_params(ndim=2, meqn=3, mwaves=2, maux=2, rp=O.RP_ACOUSTICS2D, **kw)
+    ps = S.ClawParams(rp=S.RP_ACOUSTICS2D, **kw)
+    return po, ps, q, aux

@@ -1,0 +1,176 @@
+"""GPU parity: the CUDA path against the CPU oracle, through the C ABI.
+
+FP64_STRICT (no FMA contraction) must be bit-identical to the oracle; FP64
+(FMA allowed) within 1e-12 relative L-infinity per evaluation, the tolerance
+the hot path is specified with.  The FP32 forms are checked against the FP64
+oracle with the error bounds stated in each test.
+"""
+import numpy as np
+import pytest
+
+import cases
+from oracle import oracle as O
+import sharpclaw_b200 as S
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-12
+
+STEP_CASES = [
+    ("advection_cd0_tf1", lambda: cases.advection(mx=257)),
+    ("advection_cd2_tf0", lambda: cases.advection(mx=130, char_decomp=2, tfluct_solver=0)),
+    ("advection_extrap", lambda: cases.advection(mx=64, mthbc=(1, 1))),
+    ("euler_char_swap", lambda: cases.shu_osher(mx=517)),
+    ("euler_comp_swap", lambda: cases.shu_osher(mx=300, char_decomp=0)),
+    ("euler_wall", lambda: cases.shu_osher(mx=128, mthbc=(3, 3), perturb=0.05)),
+    ("euler_riemann_noefix_cd2", lambda: cases.riemann(mx=255, char_decomp=2)),
+    ("acoustics1d_cd0_tf1", lambda: cases.acoustics1d(mx=200)),
+    ("acoustics1d_cd2_tf1", lambda: cases.acoustics1d(mx=333, char_decomp=2)),
+    ("acoustics1d_cd0_tf0", lambda: cases.acoustics1d(mx=150, tfluct_solver=0, mthbc=(1, 3))),
+    ("sw2d_char_tf1", lambda: cases.radial_dam(n=37)),
+    ("sw2d_char_tf0_wall", lambda: cases.radial_dam(n=20, tfluct_solver=0, mthbc=(3, 3, 1, 1))),
+    ("sw2d_comp_efix", lambda: cases.radial_dam(n=24, char_decomp=0, efix=1)),
+    ("acoustics2d_cd0", lambda: cases.acoustics2d(n=33)),
+    ("acoustics2d_cd2_tf0", lambda: cases.acoustics2d(n=18, char_decomp=2, tfluct_solver=0)),
+]
+
+
+def _interior(a, ndim):
+    return a[:, 3:-3] if ndim == 1 else a[:, 3:-3, 3:-3]
+
+
+def _rel_inf(a, b):
+    scale = max(np.abs(b).max(), 1e-300)
+    return np.abs(a - b).max() / scale
+
+
+def _dt_for(po, q, aux, target=0.5):
+    _, _, cfl = O.step(po, q, aux, 1.0)
+    return target / cfl
+
+
+@pytest.mark.parametrize("name,make", STEP_CASES, ids=[c[0] for c in STEP_CASES])
+@pytest.mark.parametrize("precision", ["fp64_strict", "fp64"])
+def test_step_parity(name, make, precision):
+    po, ps, q, aux = make()
+    dt = _dt_for(po, q, aux)
+    qo, dqo, cflo = O.step(po, q, aux, dt)
+    with S.Solver(ps, precision) as s:
+        s.set_aux(aux) if aux is not None else None
+        qg, dqg, cflg = s.step(q, dt)
+    nd = ps.ndim
+    assert np.array_equal(qg, qo), "ghost-cell fill differs from bc1/bc2"
+    if precision == "fp64_strict":
+        assert np.array_equal(_interior(dqg, nd), _interior(dqo, nd)), \
+            f"max |diff| {np.abs(_interior(dqg - dqo, nd)).max()}"
+        assert cflg == cflo
+    else:
+        assert _rel_inf(_interior(dqg, nd), _interior(dqo, nd)) <= TOL_FP64
+        assert abs(cflg - cflo) <= TOL_FP64 * cflo
+
+
+@pytest.mark.parametrize("ti", [1, 2, 3, 4])
+@pytest.mark.parametrize("precision", ["fp64_strict", "fp64"])
+def test_rk_step_parity(ti, precision):
+    po, ps, q, aux = cases.shu_osher(mx=300)
+    ps.time_integrator = ti
+    dt = _dt_for(po, q, aux, 0.4)
+    qb = O.bc(po, q)
+    ref, cflr = O.rk_step(po, ti, qb, aux, dt)
+    with S.Solver(ps, precision) as s:
+        s.set_q(q)
+        cfl = s.rk_step(dt)
+        got = s.get_q()
+    if precision == "fp64_strict":
+        assert np.array_equal(got[:, 3:-3], ref[:, 3:-3])
+        assert cfl == cflr
+    else:
+        assert _rel_inf(got[:, 3:-3], ref[:, 3:-3]) <= TOL_FP64
+        assert abs(cfl - cflr) <= TOL_FP64 * cflr
+
+
+def test_rk_step_2d_ssp104_strict():
+    po, ps, q, aux = cases.radial_dam(n=30)
+    ps.time_integrator = 4
+    dt = _dt_for(po, q, aux, 1.0)
+    ref, cflr = O.rk_step(po, 4, O.bc(po, q), aux, dt)
+    with S.Solver(ps, "fp64_strict") as s:
+        s.set_q(q)
+        cfl = s.rk_step(dt)
+        got = s.get_q()
+    assert np.array_equal(got[:, 3:-3, 3:-3], ref[:, 3:-3, 3:-3])
+    assert cfl == cflr
+
+
+RUN_CASES = [
+    ("advection_ssp33", lambda: cases.advection(mx=160), 3, dict(tend=0.25, dt_initial=0.002, cfl_max=0.85, cfl_desired=0.8)),
+    ("euler_ssp104", lambda: cases.shu_osher(mx=200), 4, dict(tend=0.05, dt_initial=0.001, cfl_max=2.5, cfl_desired=2.45)),
+    ("acoustics_ssp104", lambda: cases.acoustics1d(mx=100), 4, dict(tend=1.0, dt_initial=0.025, cfl_max=2.9, cfl_desired=2.85)),
+    ("sw2d_ssp33", lambda: cases.radial_dam(n=24), 3, dict(tend=0.1, dt_initial=0.01, cfl_max=0.9, cfl_desired=0.8)),
+    ("euler_reject_retake", lambda: cases.shu_osher(mx=120), 3, dict(tend=0.05, dt_initial=0.05, cfl_max=0.9, cfl_desired=0.8)),
+]
+
+
+@pytest.mark.parametrize("name,make,ti,run", RUN_CASES, ids=[c[0] for c in RUN_CASES])
+def test_sharpclaw_run_strict(name, make, ti, run):
+    po, ps, q, aux = make()
+    ps.time_integrator = ti
+    qo, ro = O.sharpclaw(po, q, aux, tstart=0.0, time_integrator=ti, **run)
+    with S.Solver(ps, "fp64_strict") as s:
+        s.set_aux(aux) if aux is not None else None
+        s.set_q(q)
+        res = s.sharpclaw(0.0, run["tend"], run["dt_initial"], run["cfl_max"], run["cfl_desired"])
+        qg = s.get_q()
+    assert res["steps_taken"] == ro.steps_taken
+    assert res["rejected"] == ro.rejected
+    assert res["info"] == ro.info
+    assert res["tend"] == ro.tend
+    assert res["dt_last"] == ro.dt_last
+    assert res["cfl_maxused"] == ro.cfl_maxused
+    nd = ps.ndim
+    assert np.array_equal(_interior(qg, nd), _interior(qo, nd))
+    if name == "euler_reject_retake":
+        assert ro.rejected >= 1
+
+
+def test_info_codes():
+    po, ps, q, aux = cases.advection(mx=64)
+    with S.Solver(ps, "fp64") as s:
+        s.set_q(q)
+        # cfl_desired > cfl_max -> info 3 (sharpclaw.f90:61-64)
+        r = s.sharpclaw(0.0, 1.0, 0.01, cfl_max=0.5, cfl_desired=0.8)
+        assert r["info"] == 3
+        # fixed dt not dividing the interval -> info 2 (sharpclaw.f90:50-56)
+        r = s.sharpclaw(0.0, 1.0, 0.3, cfl_max=10.0, cfl_desired=0.8, dt_variable=0)
+        assert r["info"] == 2
+        # too many steps -> info 11 (sharpclaw.f90:225)
+        r = s.sharpclaw(0.0, 1.0, 0.001, cfl_max=0.9, cfl_desired=0.8, max_steps=5)
+        assert r["info"] == 11 and r["steps_taken"] == 5
+
+
+def test_nonfinite_is_reported():
+    po, ps, q, aux = cases.advection(mx=64)
+    q = q.copy()
+    q[0, 20] = np.nan
+    with S.Solver(ps, "fp64") as s:
+        s.set_q(q)
+        r = s.sharpclaw(0.0, 1.0, 0.001, cfl_max=0.9, cfl_desired=0.8)
+    assert r["info"] == S._capi.INFO_NONFINITE
+    assert r["status"] & S._capi.STATUS_NONFINITE
+
+
+@pytest.mark.parametrize("precision,tol", [("mixed", 2e-5), ("fp32", 2e-5)])
+def test_reduced_precision_error(precision, tol):
+    """FP32 reconstruction/Riemann solves against the FP64 oracle: relative L1
+    of each component after a short Shu-Osher run."""
+    po, ps, q, aux = cases.shu_osher(mx=400)
+    ps.time_integrator = 4
+    run = dict(tend=0.2, dt_initial=0.001, cfl_max=2.5, cfl_desired=2.45)
+    qo, ro = O.sharpclaw(po, q, aux, tstart=0.0, time_integrator=4, **run)
+    with S.Solver(ps, precision) as s:
+        s.set_q(q)
+        s.sharpclaw(0.0, run["tend"], run["dt_initial"], run["cfl_max"], run["cfl_desired"])
+        qg = s.get_q()
+    for m in range(3):
+        rel = np.abs(qg[m, 3:-3] - qo[m, 3:-3]).sum() / np.abs(qo[m, 3:-3]).sum()
+        assert rel <= tol, (m, rel)
