@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(NT) k_stage1d(StageArgs a) {
         S* out = static_cast<S*>(a.buf[ctl->role[a.sd.out]]);
         S* out2 = a.sd.out2 >= 0 ? static_cast<S*>(a.buf[ctl->role[a.sd.out2]]) : nullptr;
         const S* qo = a.sd.aux_in >= 0 ? static_cast<const S*>(a.buf[ctl->role[a.sd.aux_in]]) : nullptr;
-        const Images im = images_1d(c, mx, a.mthbc[0], a.mthbc[1]);
+        const bool edge = c <= 3 || c >= mx - 2;   // only these cells have ghost images
 #pragma unroll
         for (int m = 0; m < M; ++m) {
           Ac dqv = (Ac)((R)0 - (R)dtdx_c * br[m]);
@@ -306,7 +306,8 @@ __global__ void __launch_bounds__(NT) k_stage1d(StageArgs a) {
           Ac o1, o2 = (Ac)0;
           combine<Ac>(kind, qv, qov, dqv, o1, o2);
           bad |= !isfinite(o1);
-          put_1d<S, Ac>(out, a.plane, m, c, im, o1);
+          if (edge) put_1d<S, Ac>(out, a.plane, m, c, images_1d(c, mx, a.mthbc[0], a.mthbc[1]), o1);
+          else out[(long)m * a.plane + c + 2] = (S)o1;
           if (out2) out2[(long)m * a.plane + c + 2] = (S)o2;
         }
       }
@@ -478,8 +479,7 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
       S* out = static_cast<S*>(a.buf[ctl->role[a.sd.out]]);
       S* out2 = a.sd.out2 >= 0 ? static_cast<S*>(a.buf[ctl->role[a.sd.out2]]) : nullptr;
       const S* qo = a.sd.aux_in >= 0 ? static_cast<const S*>(a.buf[ctl->role[a.sd.aux_in]]) : nullptr;
-      const Images ix = images_1d(gi, nx, a.mthbc[0], a.mthbc[1]);
-      const Images iy = images_1d(gj, ny, a.mthbc[2], a.mthbc[3]);
+      const bool edge = gi <= 3 || gi >= nx - 2 || gj <= 3 || gj >= ny - 2;
 #pragma unroll
       for (int m = 0; m < M; ++m) {
         Ac qv = (Ac)sq[(m * T::WY + lj + 3) * T::WX + li + 3];
@@ -487,7 +487,11 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
         Ac o1, o2 = (Ac)0;
         combine<Ac>(kind, qv, qov, (Ac)dqs[m], o1, o2);
         bad |= !isfinite(o1);
-        put_2d<S, Ac>(out, a.plane, a.pitch, m, gi, gj, ix, iy, o1);
+        if (edge)
+          put_2d<S, Ac>(out, a.plane, a.pitch, m, gi, gj, images_1d(gi, nx, a.mthbc[0], a.mthbc[1]),
+                        images_1d(gj, ny, a.mthbc[2], a.mthbc[3]), o1);
+        else
+          out[(long)m * a.plane + o0] = (S)o1;
         if (out2) out2[(long)m * a.plane + o0] = (S)o2;
       }
     }
