@@ -1,0 +1,127 @@
+"""CPU tests of the oracle: known answers and invariants (no GPU).
+
+The reference ships no golden vectors; its own known-answer test is
+apps/acoustics/1d/interface/sharpclawtest.py, which compares SharpClaw cell
+averages with the exact characteristic solution of actools.py in the 1-norm.
+These tests do the same with the oracle (restated exact solution in
+tests/golden/acoustics_exact.py) and add analytic invariants.
+"""
+import numpy as np
+import pytest
+
+import cases
+from acoustics_exact import InterfaceProblem
+from oracle import oracle as O
+
+
+def _interface_error(mx, char_decomp):
+    ap = InterfaceProblem(rho=(1.0, 4.0), c=(1.0, 0.5))
+    po, _, q, aux = cases.acoustics1d(mx=mx, char_decomp=char_decomp)
+    qf, res = O.sharpclaw(po, q, aux, tstart=0.0, tend=8.0, dt_initial=0.025, cfl_max=2.9,
+                          cfl_desired=2.85, time_integrator=4)
+    assert res.info == 0 and res.tend == 8.0
+    pe, ue = ap.cell_averages(mx, res.tend)
+    dx = 20.0 / mx
+    return np.abs(pe - qf[0, 3:-3]).sum() * dx, np.abs(ue - qf[1, 3:-3]).sum() * dx
+
+
+@pytest.mark.parametrize("char_decomp", [0, 2])
+def test_acoustics_interface_known_answer(char_decomp):
+    """sharpclawtest.py 'interface 1' (WENO5 / WENO5 Char, SSPRK(10,4), cfl
+    2.85/2.9, t = 8): errors against the exact solution fall with mx."""
+    e400, u400 = _interface_error(400, char_decomp)
+    e800, u800 = _interface_error(800, char_decomp)
+    assert e400 < 0.06 and e800 < 0.013
+    assert np.log2(e400 / e800) > 2.0         # observed order of the pressure error
+    assert np.log2(u400 / u800) > 2.0
+
+
+def test_weno5_fifth_order_on_smooth_advection():
+    errs = []
+    for mx in (40, 80, 160):
+        dx = 1.0 / mx
+        po = O.make_params(mx=mx, meqn=1, mwaves=1, dx=dx, rp=O.RP_ADVECTION, u=1.0, mthbc=(2, 2))
+        xe = dx * np.arange(mx + 1)
+        q = np.zeros((1, mx + 6))
+        q[0, 3:-3] = -(np.cos(2 * np.pi * xe[1:]) - np.cos(2 * np.pi * xe[:-1])) / (2 * np.pi * dx)
+        qf, res = O.sharpclaw(po, q, None, tstart=0, tend=1.0, dt_initial=0.5 * dx, cfl_max=0.85,
+                              cfl_desired=0.8, time_integrator=4)
+        errs.append(np.abs(qf[0, 3:-3] - q[0, 3:-3]).sum() * dx)
+    orders = [np.log2(errs[k] / errs[k + 1]) for k in range(2)]
+    assert min(orders) > 4.5, orders
+
+
+@pytest.mark.parametrize("make", [lambda: cases.advection(mx=200),
+                                  lambda: cases.shu_osher(mx=200, mthbc=(2, 2)),
+                                  lambda: cases.radial_dam(n=24)])
+def test_conservation_periodic(make):
+    po, _, q, aux = make()
+    qb = O.bc(po, q)
+    _, dq, _ = O.step(po, qb, aux, 1e-3)
+    inner = dq[:, 3:-3] if po.ndim == 1 else dq[:, 3:-3, 3:-3]
+    tot = np.abs(qb).sum()
+    assert np.abs(inner.reshape(inner.shape[0], -1).sum(1)).max() <= 1e-12 * tot
+
+
+def test_free_stream_preserved():
+    po, _, q, aux = cases.shu_osher(mx=64, mthbc=(2, 2))
+    q[0, :], q[1, :], q[2, :] = 1.3, 0.7, 2.9
+    _, dq, _ = O.step(po, q, aux, 1e-3)
+    assert np.abs(dq[:, 3:-3]).max() <= 1e-14
+
+
+def test_radial_dam_xy_symmetry_is_exact():
+    """Dimension-by-dimension flux2 on transposed data is the transpose."""
+    po, _, q, aux = cases.radial_dam(n=30, noise=0.0)
+    qT = np.stack([q[0].T, q[2].T, q[1].T])
+    _, dq, _ = O.step(po, q, aux, 1e-2)
+    _, dqT, _ = O.step(po, qT, aux, 1e-2)
+    assert np.array_equal(dq[0], dqT[0].T)
+    assert np.array_equal(dq[1], dqT[2].T)
+
+
+@pytest.mark.parametrize("rp,meqn,ixys", [(O.RP_EULER, 3, (1,)), (O.RP_SW2D, 3, (1, 2))])
+def test_eigenvector_plugins_are_inverse_pairs(rp, meqn, ixys):
+    rng = np.random.default_rng(7)
+    p = O.make_params(mx=10, meqn=meqn, mwaves=3, dx=0.1, rp=rp, mthbc=(1, 1), char_decomp=2)
+    q = np.zeros((3, 16))
+    q[0] = rng.uniform(0.5, 2.0, 16)
+    q[1] = rng.uniform(-1, 1, 16) * q[0]
+    q[2] = (rng.uniform(0.5, 2.0, 16) / 0.4 + 0.5 * q[1] ** 2 / q[0]) if rp == O.RP_EULER else rng.uniform(-1, 1, 16)
+    for ixy in ixys:
+        evl, evr = O.evec(p, q, ixy=ixy)
+        for i in range(1, 16):
+            L, R = evl[:, :, i].T, evr[:, :, i].T
+            assert np.allclose(L @ R, np.eye(3), atol=1e-12)
+
+
+def test_roe_property_euler_and_sw():
+    """amdq + apdq = f(right) - f(left) for the Roe solvers (with and without
+    the entropy fix): the flux-difference splitting the scheme relies on."""
+    rng = np.random.default_rng(11)
+    n = 20
+    for rp, efix in ((O.RP_EULER, 1), (O.RP_EULER, 0), (O.RP_SW2D, 0), (O.RP_SW2D, 1)):
+        p = O.make_params(mx=n - 6, meqn=3, mwaves=3, dx=0.1, rp=rp, efix=efix, mthbc=(1, 1))
+        rho = rng.uniform(0.5, 2.0, n)
+        u = rng.uniform(-2, 2, n)
+        if rp == O.RP_EULER:
+            pr = rng.uniform(0.5, 2.0, n)
+            q = np.stack([rho, rho * u, pr / 0.4 + 0.5 * rho * u * u])
+
+            def flux(s):
+                r, m, e = s
+                pp = 0.4 * (e - 0.5 * m * m / r)
+                return np.array([m, m * m / r + pp, (e + pp) * m / r])
+        else:
+            v = rng.uniform(-1, 1, n)
+            q = np.stack([rho, rho * u, rho * v])
+
+            def flux(s):
+                h, hu, hv = s
+                return np.array([hu, hu * hu / h + 0.5 * h * h, hu * hv / h])
+        # rp solves interface i with left state qr(i-1) and right state ql(i)
+        ql, qr = q.copy(), q.copy()
+        wave, s, am, ap = O.rp(p, ql, qr)
+        for i in range(1, n):
+            df = flux(ql[:, i]) - flux(qr[:, i - 1])
+            assert np.allclose(am[:, i] + ap[:, i], df, rtol=1e-10, atol=1e-10)
