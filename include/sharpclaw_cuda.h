@@ -149,6 +149,23 @@ int scl_time_stages(scl_handle* h, double dt, int reps, float* ms, long long* la
  * CFL kernel in 2-D). */
 int scl_kernels_per_step(scl_handle* h);
 
+/* One SSP-RK time step of a 1-D grid that allocates nothing, for callers
+ * that cannot call cudaMalloc (no counterpart in the reference).  The caller
+ * owns every array: q_dev (device, reference layout, double, ghost cells
+ * included) is stepped in place, aux_dev is read (NULL when maux == 0); the
+ * Runge-Kutta stage registers live in a fixed device array inside the library
+ * of 3 * SCL_NOALLOC_MAX_VALUES doubles (4.5 MiB per GPU, held while the
+ * library is loaded).  Grids with meqn*(mx+2*mbc) > SCL_NOALLOC_MAX_VALUES are
+ * rejected (SCL_E_INVALID).  Calls on one GPU share that array: calls whose
+ * work overlaps on the same GPU race, so serialise them.  The first call on a
+ * device resolves the array's address; make it before any stream capture.
+ * stream is a cudaStream_t (NULL = default stream); when cfl is not NULL the
+ * call waits for the step and returns the last stage's CFL number.  Double
+ * state only (FP64, FP64_STRICT, MIXED). */
+#define SCL_NOALLOC_MAX_VALUES 196608
+int scl_rk_step_noalloc(const scl_params* p, double* q_dev, const double* aux_dev, double dt,
+                        double* cfl, void* stream);
+
 /* Stream of the handle (cudaStream_t as void*), for callers that overlap work. */
 void* scl_stream(scl_handle* h);
 

@@ -74,6 +74,8 @@ SIGNATURES = [
     ("scl_time_stages", ctypes.c_int, [_h, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
                                         ctypes.POINTER(ctypes.c_longlong)]),
     ("scl_kernels_per_step", ctypes.c_int, [_h]),
+    ("scl_rk_step_noalloc", ctypes.c_int, [ctypes.POINTER(scl_params), ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_double, _dp, ctypes.c_void_p]),
     ("scl_stream", ctypes.c_void_p, [_h]),
 ]
 

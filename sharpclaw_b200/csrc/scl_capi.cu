@@ -805,3 +805,7 @@ int scl_time_stages(scl_handle* h, double dt, int reps, float* ms, long long* la
 int scl_kernels_per_step(scl_handle* h) { return h ? kernels_per_step(h) : 0; }
 
 }  // extern "C"
+
+namespace scl {
+void set_last_error(const char* msg) { g_err = msg ? msg : ""; }
+}  // namespace scl

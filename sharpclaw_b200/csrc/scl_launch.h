@@ -18,4 +18,7 @@ bool get_launchers_fp32(int rp, int ndim, int cd, int tf, int variant, Launchers
 
 constexpr int N2D_VARIANTS = 3;
 
+// Sets the message returned by scl_last_error() on this thread.
+void set_last_error(const char* msg);
+
 }  // namespace scl
