@@ -67,10 +67,8 @@ def shu_osher(mx):
 
 
 def config(extra=None):
-    c = {"workload": WORKLOAD, "mx": MX, "time_steps_per_step": NSTEP, "stages_per_time_step": NSTAGES,
-         "cells_x_stages_per_step": MX * NSTEP * NSTAGES,
-         "l2": "flushed (256 MiB write) between timed steps; the 4 state registers (~100 MB) "
-               "stay L2-resident within a step",
+    c = {"workload": WORKLOAD, "cells": MX, "time_steps_per_step": NSTEP, "stages_per_time_step": NSTAGES,
+         "l2": "flushed (256 MiB write) between timed steps",
          "parallelism": "replicas (one independent grid per GPU)"}
     if extra:
         c.update(extra)
@@ -191,6 +189,88 @@ def run_reference(args, rank, world):
     return 0
 
 
+def shu_osher_params(S, mx, dx):
+    return S.ClawParams(rp=S.RP_EULER, mx=mx, dx=dx, xlower=-5.0, gamma=GAMMA, mthbc=(1, 1),
+                        char_decomp=2, tfluct_solver=0, time_integrator=4)
+
+
+def workloads():
+    """Benchmark workloads (BASELINE configurations).  Each returns the solver
+    parameters, initial data, aux, run settings and the bytes one cell-stage
+    must move (k_I * meqn * 8 + maux * 8, double state)."""
+    import numpy as np
+    import sharpclaw_b200 as S
+
+    def c2():
+        q, dx = shu_osher(MX)
+        return dict(params=shu_osher_params(S, MX, dx), q=q, aux=None, dt0=DT0, cfl=(CFL_MAX, CFL_DESIRED),
+                    dt_variable=1, tend=1e30, nstep=NSTEP, cells=MX, stages=10, bytes_cell_stage=2.3 * 3 * 8,
+                    desc=WORKLOAD, traffic_key="k_stage1d_euler_charwise_mixed")
+
+    def c1():
+        mx = 1000
+        dx = 1.0 / mx
+        rng = np.random.default_rng(1)
+        xc = (np.arange(mx) + 0.5) * dx
+        q0 = np.exp(-200.0 * (xc - 0.3) ** 2) + ((xc > 0.6) & (xc < 0.8))
+        for _ in range(4):
+            k = rng.integers(1, 9)
+            q0 = q0 + rng.uniform(0, 0.1) * np.sin(2 * np.pi * k * xc)
+        q = np.zeros((1, mx + 6))
+        q[0, 3:-3] = q0
+        p = S.ClawParams(rp=S.RP_ADVECTION, mx=mx, dx=dx, u=1.0, mthbc=(2, 2), char_decomp=0,
+                         tfluct_solver=1, time_integrator=3)
+        return dict(params=p, q=q, aux=None, dt0=0.8 * dx, cfl=(0.85, 0.8), dt_variable=1, tend=1.0,
+                    nstep=2000, cells=mx, stages=3, bytes_cell_stage=8.0 / 3.0 * 8,
+                    desc="1-D advection a=1, periodic [0,1], mx=1000, WENO5 componentwise + Godunov rp, "
+                         "tfluct, SSPRK3, cfl 0.8/0.85, full run to t=1 per step", traffic_key=None)
+
+    def c3():
+        n = 4096
+        d = 5.0 / n
+        xc = -2.5 + (np.arange(n) + 0.5) * d
+        X, Y = np.meshgrid(xc, xc, indexing="xy")
+        q = np.zeros((3, n + 6, n + 6))
+        q[0, 3:-3, 3:-3] = np.where(X ** 2 + Y ** 2 < 0.25, 2.0, 1.0) + \
+            1e-3 * np.random.default_rng(3).standard_normal((n, n))
+        p = S.ClawParams(rp=S.RP_SW2D, mx=n, my=n, dx=d, dy=d, xlower=-2.5, ylower=-2.5, grav=1.0,
+                         mthbc=(2, 2, 2, 2), char_decomp=2, tfluct_solver=1, time_integrator=3)
+        return dict(params=p, q=q, aux=None, dt0=0.3 * d / 1.5, cfl=(0.5, 0.45), dt_variable=1, tend=1e30,
+                    nstep=5, cells=n * n, stages=3, bytes_cell_stage=8.0 / 3.0 * 3 * 8,
+                    desc="2-D shallow water g=1, radial dam break h=2 in r<0.5 else 1 + N(0,1e-3), "
+                         "4096x4096 periodic on [-2.5,2.5]^2, Roe rpn2 + tfluct, char-wise WENO5, SSPRK3, "
+                         "cfl 0.45/0.5", traffic_key=None)
+
+    def c5():
+        n = 1024
+        d = 1.0 / n
+        rng = np.random.default_rng(5)
+        ln = rng.normal(0, 0.3, (2, n + 6, n + 6))
+        ker = np.exp(-0.5 * (np.arange(-12, 13) / 4.0) ** 2)
+        ker /= ker.sum()
+        for a in ln:
+            for ax in (0, 1):
+                a[...] = np.apply_along_axis(lambda v: np.convolve(v, ker, mode="same"), ax, a)
+        rho, K = np.exp(ln[0]), np.exp(ln[1])
+        aux = np.ascontiguousarray(np.stack([np.sqrt(rho * K), np.sqrt(K / rho)]))
+        xc = (np.arange(-3, n + 3) + 0.5) * d
+        X, Y = np.meshgrid(xc, xc, indexing="xy")
+        q = np.zeros((3, n + 6, n + 6))
+        for _ in range(4):
+            cx, cy = rng.uniform(0.2, 0.8, 2)
+            q[0] += np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * 0.03 ** 2))
+        p = S.ClawParams(rp=S.RP_ACOUSTICS2D, mx=n, my=n, dx=d, dy=d, mthbc=(2, 2, 2, 2), char_decomp=0,
+                         tfluct_solver=1, time_integrator=3)
+        dt = 0.4 * d / float(aux[1].max())
+        return dict(params=p, q=q, aux=aux, dt0=dt, cfl=(1e9, 0.5), dt_variable=0, tend=20 * dt,
+                    nstep=20, cells=n * n, stages=3, bytes_cell_stage=8.0 / 3.0 * 3 * 8 + 2 * 8,
+                    desc="2-D variable-coefficient acoustics 1024x1024 periodic, rho,K log-normal(0,0.3) "
+                         "smoothed, WENO5 componentwise + rpn2/tfluct, SSPRK3, fixed dt, 20 steps per step",
+                    traffic_key=None)
+
+    return {"c2": c2, "c1": c1, "c3": c3, "c5": c5}
+
+
 def run_gpu(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -199,10 +279,11 @@ def run_gpu(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    q0, dx = shu_osher(MX)
-    ps = S.ClawParams(rp=S.RP_EULER, mx=MX, dx=dx, xlower=-5.0, gamma=GAMMA, mthbc=(1, 1),
-                      char_decomp=2, tfluct_solver=0, time_integrator=4)
-    cells = MX * NSTEP * NSTAGES
+    W = workloads()[args.workload]()
+    ps, q0, aux0 = W["params"], W["q"], W["aux"]
+    cfl_max, cfl_des = W["cfl"]
+    nstep = W["nstep"]
+    cells = W["cells"] * nstep * W["stages"]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def barrier():
@@ -218,99 +299,134 @@ def run_gpu(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def device_run(precision, clocks=None):
+    def timed_steps(s):
+        return s.time_steps(nstep, W["dt0"], cfl_max, cfl_des, tend=W["tend"], dt_variable=W["dt_variable"])
+
+    def device_run(precision, clocks):
         s = S.Solver(ps, precision)
+        if aux0 is not None:
+            s.set_aux(aux0)
         s.set_q(q0)
         for _ in range(args.warmup):
-            s.time_steps(NSTEP, DT0, CFL_MAX, CFL_DESIRED)
+            if W["tend"] < 1e29:
+                s.set_q(q0)
+            timed_steps(s)
         barrier()
-        total_ms = 0.0
-        ctx = clocks if clocks is not None else _Null()
-        with ctx:
+        total_ms, taken, rejected = 0.0, 0, 0
+        with clocks:
             for _ in range(args.steps):
+                if W["tend"] < 1e29:          # runs to a final time restart from q0
+                    s.set_q(q0)
                 flush.zero_()
                 torch.cuda.synchronize()
-                ms, res = s.time_steps(NSTEP, DT0, CFL_MAX, CFL_DESIRED)
-                assert res["steps_taken"] == NSTEP and res["rejected"] == 0 and res["status"] == 0, res
+                ms, res = timed_steps(s)
+                assert res["status"] == 0 and res["info"] in (0, 11), res
                 total_ms += ms
+                taken += res["steps_taken"] - res["rejected"]
+                rejected += res["rejected"]
         barrier()
-        dt_last = res["dt_last"]
-        return s, max_over_ranks(total_ms), dt_last
+        return s, max_over_ranks(total_ms), res, taken, rejected
 
     clocks = Clocks(local_rank)
-    s_mix, ms_mix, dt_mix = device_run(args.precision, clocks)
-    value = world * cells * args.steps / (ms_mix / 1000.0)
-    s_64, ms_64, dt_64 = device_run("fp64", clocks)
-    value64 = world * cells * args.steps / (ms_64 / 1000.0)
+    s_mix, ms_mix, res_mix, taken_mix, rej_mix = device_run(args.precision, clocks)
+    value = world * W["cells"] * W["stages"] * taken_mix / (ms_mix / 1000.0)
+    s_64, ms_64, res_64, taken_64, rej_64 = device_run("fp64", clocks)
+    value64 = world * W["cells"] * W["stages"] * taken_64 / (ms_64 / 1000.0)
 
-    # fused stage kernel alone (roofline): all 10 stage launches of a step
+    # the fused stage kernels alone (roofline): the stage launches of one step
     peak, peak_kind = measured_peaks()
-    reps = 20
+    traffic_per_cell = None
+    if W["traffic_key"]:
+        try:
+            with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+                traffic_per_cell = json.load(f)[W["traffic_key"]]["dram_bytes_per_cell"]
+        except Exception:
+            traffic_per_cell = None
     roof = {}
-    for name, s in (("mixed", s_mix), ("fp64", s_64)):
-        st_ms, n_launch = s.time_stages(dt_mix, reps)
+    for name, s in (("headline", s_mix), ("fp64", s_64)):
+        st_ms, n_launch = s.time_stages(res_mix["dt_last"], 20)
         avg_ms = st_ms / n_launch
-        bytes_per_launch = 2.3 * 3 * 8 * MX          # k_I * meqn * sizeof(double) per cell-stage
+        bytes_per_launch = W["bytes_cell_stage"] * W["cells"]
         gbs = bytes_per_launch / (avg_ms / 1000.0) / 1e9
         roof[name] = {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
-                      "frac": gbs / peak, "traffic": None, "avg_launch_us": avg_ms * 1000.0,
-                      "algorithmic_bytes_per_launch": bytes_per_launch, "peak_source": peak_kind}
+                      "frac": gbs / peak,
+                      "traffic": (traffic_per_cell * W["cells"]) if traffic_per_cell else None,
+                      "avg_launch_us": avg_ms * 1000.0, "algorithmic_bytes_per_launch": bytes_per_launch,
+                      "peak_source": peak_kind}
 
     # end to end through the public API with host buffers
     qh = torch.from_numpy(q0.copy()).pin_memory()
     qout = torch.empty_like(qh).pin_memory()
     qh_np, qout_np = qh.numpy(), qout.numpy()
     s_e2e = s_mix
-    for _ in range(args.warmup):
+
+    def e2e_step():
         s_e2e.set_q(qh_np)
-        s_e2e.sharpclaw(0.0, 1e30, DT0, CFL_MAX, CFL_DESIRED, max_steps=NSTEP)
-        qout_np[...] = s_e2e.get_q()
+        r = s_e2e.sharpclaw(0.0, W["tend"], W["dt0"], cfl_max, cfl_des, max_steps=nstep,
+                            dt_variable=W["dt_variable"])
+        _get_q_into(s_e2e, qout_np)
+        return r
+
+    for _ in range(args.warmup):
+        e2e_step()
     barrier()
+    e2e_taken = 0
     with clocks:
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            s_e2e.set_q(qh_np)
-            r = s_e2e.sharpclaw(0.0, 1e30, DT0, CFL_MAX, CFL_DESIRED, max_steps=NSTEP)
-            _ = _get_q_into(s_e2e, qout_np)
+            r = e2e_step()
+            e2e_taken += r["steps_taken"] - r["rejected"]
         barrier()
         e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e = world * cells * args.steps / e2e_s
+    e2e = world * W["cells"] * W["stages"] * e2e_taken / e2e_s
     nbytes = q0.nbytes
 
-    # accuracy: mixed vs plain FP64 after 20 fixed-dt steps on the full grid
+    # accuracy: the headline form against plain FP64 after 20 fixed-dt steps
     acc = {}
     if rank == 0:
         outs = {}
+        dt = W["dt0"]
         for name in ("fp64", args.precision):
             with S.Solver(ps, name) as s:
+                if aux0 is not None:
+                    s.set_aux(aux0)
                 s.set_q(q0)
-                s.sharpclaw(0.0, 20 * DT0, DT0, 1e9, 0.5, dt_variable=0)
-                outs[name] = s.get_q()[:, 3:-3]
+                s.sharpclaw(0.0, 20 * dt, dt, 1e9, 0.5, dt_variable=0)
+                q = s.get_q()
+                outs[name] = q[:, 3:-3] if ps.ndim == 1 else q[:, 3:-3, 3:-3]
         a, b = outs[args.precision], outs["fp64"]
-        acc = {"rel_l1_vs_fp64": max(float(np.abs(a[m] - b[m]).sum() / np.abs(b[m]).sum()) for m in range(3)),
+        nc = a.shape[0]
+        acc = {"rel_l1_vs_fp64": max(float(np.abs(a[m] - b[m]).sum() / max(np.abs(b[m]).sum(), 1e-300))
+                                     for m in range(nc)),
                "rel_linf_vs_fp64": float(np.abs(a - b).max() / np.abs(b).max()),
-               "steps": 20, "dt": DT0}
+               "steps": 20, "dt": dt}
 
-    # CPU baseline: the oracle on a bounded sample, one core
+    # CPU baseline: the oracle on a bounded sample, one core (C2 only)
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and args.workload == "c2":
         n, t = _oracle_one((1 << 18, 2))
         cpu = {"value": n / t, "unit": UNIT, "cores": 1, "kind": "port",
                "sample": "mx=2^18 Shu-Osher, 2 SSPRK(10,4) time steps, C restatement of the reference "
                          "(gcc -O2, no FMA), single thread"}
 
     kps = s_mix.kernels_per_step
-    launches = args.steps * NSTEP * kps
+    launches = (res_mix["steps_taken"]) * kps * args.steps
     ck = clocks.summary()
     if rank == 0:
+        cfg = {"workload": W["desc"], "cells": W["cells"], "time_steps_per_step": nstep,
+               "stages_per_time_step": W["stages"], "precision": args.precision,
+               "l2": "flushed (256 MiB write) between timed steps",
+               "parallelism": "replicas (one independent grid per GPU)"}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_mix / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 state/accumulation)",
-                "data": "synthetic",
-                "config": config({"precision": args.precision}),
-                "roofline": roof["mixed"],
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": {"mixed": "f32 (f64 state/accumulation)", "fp32": "f32", "fp64": "f64",
+                          "fp64_strict": "f64"}[args.precision],
+                "data": "synthetic", "config": cfg,
+                "roofline": roof["headline"],
                 "fp64": {"value": value64, "unit": UNIT, "ms_per_step": ms_64 / args.steps,
                          "roofline": roof["fp64"], "speedup_of_headline": value / value64},
+                "rejected_steps": rej_mix,
                 "accuracy": acc,
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
@@ -346,6 +462,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp64", "fp64_strict"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c5"],
+                    help="c2 (default, the headline): 1-D Euler mx=2^20; c1 advection; c3 2-D shallow "
+                         "water 4096^2; c5 2-D acoustics 1024^2")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3

@@ -715,7 +715,7 @@ int run_loop(scl_handle* h, int graph_steps, long max_replays, float* ms) {
   h->hdone[0] = h->hdone[1] = 0;
   for (long r = 0; r < max_replays; ++r) {
     CK(cudaGraphLaunch(h->graph, h->stream));
-    if (ms) continue;
+    if (max_replays == 1) break;
     CK(cudaMemcpyAsync(&h->hdone[r & 1], &h->ctl->done, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaEventRecord(h->evq[r & 1], h->stream));
     if (r > 0) {  // replay r is already queued while we look at replay r-1
