@@ -166,6 +166,31 @@ int scl_kernels_per_step(scl_handle* h);
 int scl_rk_step_noalloc(const scl_params* p, double* q_dev, const double* aux_dev, double dt,
                         double* cfl, void* stream);
 
+/* ---- batched solver: many independent 1-D problems of uneven size ------ */
+/* Replaces a host loop that calls sharpclaw() once per problem: every
+ * instance k (mx[k] cells, spacing dx[k]) has its own controller (t, dt,
+ * CFL, rejections, info) and all of them advance together, one persistent
+ * launch per RK stage walking the active instances' tiles, captured in CUDA
+ * graphs.  The plugin, options, integrator and precision come from p (its
+ * mx/dx are ignored).  1-D plugins only. */
+typedef struct scl_batch scl_batch;
+int scl_batch_create(const scl_params* p, int ninst, const int* mx, const double* dx, scl_batch** out);
+int scl_batch_destroy(scl_batch* b);
+/* q: all instances concatenated, instance k in the reference layout
+ * q(1-mbc:mx[k]+mbc, meqn) (double), ghost cells included; set_q fills ghosts. */
+int scl_batch_set_q(scl_batch* b, const double* q);
+int scl_batch_get_q(scl_batch* b, double* q);
+int scl_batch_set_aux(scl_batch* b, const double* aux);
+/* sharpclaw() on every instance with the same run parameters; dt_initial
+ * (nullable) gives a first step per instance.  res has ninst entries; ms
+ * (nullable) receives the device time of the time loop (CUDA events).  The
+ * first run picks the faster tile width by timing a few steps of each from
+ * the same start state (autotuning), then restores that state. */
+int scl_batch_run(scl_batch* b, const scl_run* run, const double* dt_initial, scl_result* res, float* ms);
+/* The autotuner's choice: variant index, threads per CTA, persistent grid
+ * size and the trial time of each variant (2 entries). */
+int scl_batch_tuning(scl_batch* b, int* variant, int* threads, int* grid, float* trial_ms);
+
 /* Stream of the handle (cudaStream_t as void*), for callers that overlap work. */
 void* scl_stream(scl_handle* h);
 

@@ -30,7 +30,7 @@ from . import _capi as C
 from ._capi import (FP32, FP64, FP64_STRICT, MIXED, RP_ACOUSTICS1D, RP_ACOUSTICS2D,  # noqa: F401
                     RP_ADVECTION, RP_EULER, RP_SW2D, SharpClawError)
 
-__all__ = ["ClawParams", "Solver", "sharpclaw", "SharpClawError", "RP_ADVECTION", "RP_EULER",
+__all__ = ["ClawParams", "Solver", "Batch", "sharpclaw", "SharpClawError", "RP_ADVECTION", "RP_EULER",
            "RP_SW2D", "RP_ACOUSTICS1D", "RP_ACOUSTICS2D"]
 
 # plugin id -> (meqn, mwaves, maux, ndim)
@@ -248,3 +248,90 @@ def sharpclaw(params: ClawParams, q, aux=None, *, tstart: float, tend: float, dt
         s.set_q(q)
         res = s.sharpclaw(tstart, tend, dt_initial, cfl_max, cfl_desired, dt_max, max_steps, dt_variable)
         return s.get_q(), res
+
+
+class Batch:
+    """Many independent 1-D problems of uneven size, each with its own
+    sharpclaw() controller, advanced together (batched persistent launches).
+
+    ``params`` gives the plugin, options, integrator (its mx/dx are ignored);
+    ``mx`` and ``dx`` give every instance's cells and spacing.  State arrays
+    are the instances' reference-layout arrays concatenated."""
+
+    def __init__(self, params: ClawParams, mx, dx, precision="fp32"):
+        self.params = params
+        self.mx = np.ascontiguousarray(mx, dtype=np.int32)
+        self.dx = np.ascontiguousarray(dx, dtype=np.float64)
+        self.ninst = len(self.mx)
+        self.precision = _precision(precision)
+        self._cp = params.to_c(self.precision)
+        h = ctypes.c_void_p()
+        C.check(C.lib().scl_batch_create(ctypes.byref(self._cp), self.ninst, self.mx.ctypes.data,
+                                         self.dx.ctypes.data, ctypes.byref(h)), "scl_batch_create")
+        self._h = h
+        ld = self.mx.astype(np.int64) + 2 * params.mbc
+        self.offsets = np.concatenate([[0], np.cumsum(ld * params.meqn)])
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            C.lib().scl_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def pack(self, qs):
+        """Concatenate per-instance arrays of shape (meqn, mx[k]+6)."""
+        return np.ascontiguousarray(np.concatenate([np.ascontiguousarray(q, np.float64).ravel() for q in qs]))
+
+    def unpack(self, flat, ncomp=None):
+        n = self.params.meqn if ncomp is None else ncomp
+        out, o = [], 0
+        for m in self.mx:
+            size = n * (int(m) + 2 * self.params.mbc)
+            out.append(flat[o:o + size].reshape(n, int(m) + 2 * self.params.mbc))
+            o += size
+        return out
+
+    def set_q(self, qs):
+        flat = self.pack(qs)
+        C.check(C.lib().scl_batch_set_q(self._h, _ptr(flat)), "scl_batch_set_q")
+
+    def get_q(self):
+        flat = np.empty(int(self.offsets[-1]), dtype=np.float64)
+        C.check(C.lib().scl_batch_get_q(self._h, _ptr(flat)), "scl_batch_get_q")
+        return self.unpack(flat)
+
+    def set_aux(self, auxs):
+        flat = self.pack(auxs)
+        C.check(C.lib().scl_batch_set_aux(self._h, _ptr(flat)), "scl_batch_set_aux")
+
+    def sharpclaw(self, tstart, tend, dt_initial, cfl_max, cfl_desired, dt_max=1e99, max_steps=50000,
+                  dt_variable=1):
+        """sharpclaw() on every instance; dt_initial is a scalar or one value
+        per instance.  Returns (list of per-instance output dicts, device ms)."""
+        run = C.scl_run(tstart, tend, float(np.max(dt_initial)), dt_max, cfl_max, cfl_desired, max_steps,
+                        dt_variable)
+        dt0 = np.ascontiguousarray(np.broadcast_to(np.asarray(dt_initial, np.float64), (self.ninst,)))
+        res = (C.scl_result * self.ninst)()
+        ms = ctypes.c_float(0.0)
+        C.check(C.lib().scl_batch_run(self._h, ctypes.byref(run), dt0.ctypes.data, ctypes.addressof(res),
+                                      ctypes.byref(ms)), "scl_batch_run")
+        out = [{k: getattr(r, k) for k, _ in C.scl_result._fields_} for r in res]
+        return out, ms.value
+
+    def tuning(self):
+        v, nt, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        tm = (ctypes.c_float * 2)()
+        C.check(C.lib().scl_batch_tuning(self._h, ctypes.byref(v), ctypes.byref(nt), ctypes.byref(g), tm),
+                "scl_batch_tuning")
+        return {"variant": v.value, "threads": nt.value, "grid": g.value, "trial_ms": list(tm)}

@@ -76,6 +76,16 @@ SIGNATURES = [
     ("scl_kernels_per_step", ctypes.c_int, [_h]),
     ("scl_rk_step_noalloc", ctypes.c_int, [ctypes.POINTER(scl_params), ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_double, _dp, ctypes.c_void_p]),
+    ("scl_batch_create", ctypes.c_int, [ctypes.POINTER(scl_params), ctypes.c_int, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    ("scl_batch_destroy", ctypes.c_int, [_h]),
+    ("scl_batch_set_q", ctypes.c_int, [_h, _dp]),
+    ("scl_batch_get_q", ctypes.c_int, [_h, _dp]),
+    ("scl_batch_set_aux", ctypes.c_int, [_h, _dp]),
+    ("scl_batch_run", ctypes.c_int, [_h, ctypes.POINTER(scl_run), ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.POINTER(ctypes.c_float)]),
+    ("scl_batch_tuning", ctypes.c_int, [_h, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]),
     ("scl_stream", ctypes.c_void_p, [_h]),
 ]
 

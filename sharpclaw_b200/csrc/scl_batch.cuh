@@ -1,0 +1,199 @@
+// scl_batch.cuh -- many independent 1-D problems of uneven size in one
+// persistent launch per stage.
+//
+// Every instance k keeps its own controller (t, dt, CFL, roles, status: the
+// scalars of src/sharpclaw.f90) in ctl[k], so instances take their own
+// adaptive steps, rejections and final times.  A step of the batch is
+//   begin (one CTA: per-instance k_begin_step logic, then the list of active
+//   instances and the prefix sum of their tiles),
+//   one persistent stage kernel per RK stage (a fixed grid of CTAs walks the
+//   active tiles of all instances: tile -> instance by binary search),
+//   end (one thread per instance: k_end_step logic).
+// The host captures K such steps in a CUDA graph and replays it until no
+// instance is active.
+#pragma once
+#include "scl_kernels.cuh"
+
+namespace scl {
+
+struct BatchArgs {
+  Ctl* ctl;                 // [ninst]
+  const long* off;          // [ninst] element offset of instance k in a state arena
+  const long* aoff;         // [ninst] element offset of instance k in the aux arena
+  const long* plane;        // [ninst] component stride of instance k
+  const int* mx;            // [ninst]
+  const double* dx;         // [ninst]
+  const int* active;        // [ninst] ids of the active instances (first nact entries)
+  const int* prefix;        // [ninst+1] tile prefix over the active list
+  const int* nact;          // number of active instances (device scalar)
+  void* arena[NROLES];      // state arenas, one per register role
+  const void* aux;          // aux arena or nullptr
+  StageDesc sd;
+  int stage;
+  int mthbc[2];
+  int mcapa;
+  Phys ph;
+};
+
+// The per-instance controller logic is the single-grid controller's
+// (src/sharpclaw.f90:118-221) applied to ctl[k].
+__device__ __forceinline__ void begin_one(Ctl* c) {
+  if (c->done) return;
+  if (c->n_iter >= c->maxn) { c->done = 1; return; }
+  c->n_iter += 1;
+  if (!c->retake) {
+    c->told = c->t;
+    if (c->told + c->dt > c->tend && c->tstart < c->tend) c->dt = c->tend - c->told;
+  }
+  c->retake = 0;
+  c->t = c->told + c->dt;
+  for (int s = 0; s < MAXSTAGES; ++s) c->stage_cfl[s] = 0.0;
+}
+
+__device__ __forceinline__ void end_one(Ctl* c, int last_stage, int final_role) {
+  if (c->done) return;
+  const double cfl = c->stage_cfl[last_stage];
+  c->cfl_last = cfl;
+  if (cfl != cfl) {
+    c->status |= SCL_STATUS_NONFINITE;
+    c->info = SCL_INFO_NONFINITE;
+    c->t = c->told;
+    c->done = 1;
+    return;
+  }
+  if (cfl <= c->cfl_max && (c->status & SCL_STATUS_NONFINITE)) {
+    c->info = SCL_INFO_NONFINITE;
+    c->t = c->told;
+    c->done = 1;
+    return;
+  }
+  c->status &= ~SCL_STATUS_NONFINITE;
+  if (c->dt_variable == 1) {
+    if (cfl > 0.0) {
+      c->dt = fmin(c->dt_max, c->dt * c->cfl_desired / cfl);
+      c->dtmin = fmin(c->dt, c->dtmin);
+      c->dtmax = fmax(c->dt, c->dtmax);
+    } else {
+      c->dt = c->dt_max;
+    }
+  }
+  if (cfl <= c->cfl_max) {
+    c->cflmax = fmax(cfl, c->cflmax);
+    const int tmp = c->role[ROLE_Q];
+    c->role[ROLE_Q] = c->role[final_role];
+    c->role[final_role] = tmp;
+  } else {
+    c->t = c->told;
+    c->rejected += 1;
+    if (c->dt_variable == 1) {
+      c->retake = 1;
+    } else {
+      c->cflmax = fmax(cfl, c->cflmax);
+      c->done = 1;
+      return;
+    }
+  }
+  c->steps_taken += 1;
+  if (c->t >= c->tend) c->done = 1;
+}
+
+// Begin of a batch step on one CTA of 1024 threads: controller begin for every
+// instance, then the ordered list of active instances with the exclusive
+// prefix sum of their tile counts (a block-wide scan in chunks of 1024).
+template <int NT>
+__global__ void __launch_bounds__(1024) k_batch_begin(Ctl* ctl, const int* mx, int ninst, int* active,
+                                                      int* prefix, int* nact) {
+  __shared__ int wact[32], wtiles[32];
+  __shared__ int base_tiles, base_act;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) { base_tiles = 0; base_act = 0; }
+  __syncthreads();
+  for (int k0 = 0; k0 < ninst; k0 += 1024) {
+    const int k = k0 + tid;
+    int act = 0, tiles = 0;
+    if (k < ninst) {
+      begin_one(&ctl[k]);
+      act = ctl[k].done ? 0 : 1;
+      tiles = act ? (mx[k] + NT - 2) / (NT - 1) : 0;
+    }
+    // inclusive warp scans of (act, tiles)
+    int a = act, t = tiles;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int ya = __shfl_up_sync(0xffffffffu, a, o), yt = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) { a += ya; t += yt; }
+    }
+    if (lane == 31) { wact[wid] = a; wtiles[wid] = t; }
+    __syncthreads();
+    if (wid == 0) {   // inclusive scan of the 32 warp totals
+      int wa = wact[lane], wt = wtiles[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int ya = __shfl_up_sync(0xffffffffu, wa, o), yt = __shfl_up_sync(0xffffffffu, wt, o);
+        if (lane >= o) { wa += ya; wt += yt; }
+      }
+      wact[lane] = wa;
+      wtiles[lane] = wt;
+    }
+    __syncthreads();
+    const int wa_ex = wid ? wact[wid - 1] : 0, wt_ex = wid ? wtiles[wid - 1] : 0;
+    if (act) {
+      const int pos = base_act + wa_ex + a - 1;
+      active[pos] = k;
+      prefix[pos] = base_tiles + wt_ex + t - tiles;
+    }
+    __syncthreads();
+    if (tid == 0) { base_act += wact[31]; base_tiles += wtiles[31]; }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    prefix[base_act] = base_tiles;
+    *nact = base_act;
+  }
+}
+
+static __global__ void k_batch_end(Ctl* ctl, int ninst, int last_stage, int final_role) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < ninst) end_one(&ctl[k], last_stage, final_role);
+}
+
+// Persistent stage kernel: a fixed grid walks the active tiles.
+template <class P, int CD, int TF, int PREC, int NT>
+__global__ void __launch_bounds__(NT) k_batch_stage(BatchArgs a) {
+  using S = typename Prec<PREC>::S;
+  __shared__ Tile1DSmem<P, PREC, NT> sm;
+  const int na = *a.nact;
+  if (na == 0) return;
+  const int ntiles = a.prefix[na];
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    // find the active slot j with prefix[j] <= t < prefix[j+1]
+    int lo = 0, hi = na - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (a.prefix[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    const int k = a.active[lo];
+    Ctl* ctl = &a.ctl[k];
+    const long off = a.off[k];
+    Line<S> L;
+    L.ctl = ctl;
+    L.qin = static_cast<const S*>(a.arena[ctl->role[a.sd.in]]) + off;
+    L.qo = a.sd.aux_in >= 0 ? static_cast<const S*>(a.arena[ctl->role[a.sd.aux_in]]) + off : nullptr;
+    L.out = static_cast<S*>(a.arena[ctl->role[a.sd.out]]) + off;
+    L.out2 = a.sd.out2 >= 0 ? static_cast<S*>(a.arena[ctl->role[a.sd.out2]]) + off : nullptr;
+    L.dq_out = nullptr;
+    L.aux = a.aux ? static_cast<const void*>(static_cast<const S*>(a.aux) + a.aoff[k]) : nullptr;
+    L.mx = a.mx[k];
+    L.plane = a.plane[k];
+    L.dx = a.dx[k];
+    L.bl = a.mthbc[0];
+    L.br = a.mthbc[1];
+    L.mcapa = a.mcapa;
+    L.kind = a.sd.kind;
+    L.stage = a.stage;
+    L.ixy = 1;
+    stage1d_tile<P, CD, TF, PREC, NT>(L, a.ph, 1 + (t - a.prefix[lo]) * (NT - 1), sm);
+  }
+}
+
+}  // namespace scl

@@ -3,6 +3,7 @@
 // SCL_PREC_VALUE defined; the FP64_STRICT unit is compiled without FMA
 // contraction so its arithmetic follows the reference's evaluation order.
 #pragma once
+#include "scl_batch.cuh"
 #include "scl_kernels.cuh"
 #include "scl_launch.h"
 
@@ -92,7 +93,57 @@ bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
   return false;
 }
 
+// ---- batched persistent launchers ----
+template <class P, int CD, int TF, int NT>
+void launch_batch_stage(const BatchArgs& a, int grid, cudaStream_t st) {
+  k_batch_stage<P, CD, TF, PREC, NT><<<grid, NT, 0, st>>>(a);
+}
+template <int NT>
+void launch_batch_begin(Ctl* ctl, const int* mx, int ninst, int* active, int* prefix, int* nact,
+                        cudaStream_t st) {
+  k_batch_begin<NT><<<1, 1024, 0, st>>>(ctl, mx, ninst, active, prefix, nact);
+}
+template <class P, int CD, int TF, int NT>
+int batch_blocks_per_sm() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<P, CD, TF, PREC, NT>, NT, 0);
+  return n;
+}
+template <class P, int CD, int TF, int NT>
+void fill_batch(BatchLaunchers* L) {
+  L->stage = &launch_batch_stage<P, CD, TF, NT>;
+  L->begin = &launch_batch_begin<NT>;
+  L->blocks_per_sm = &batch_blocks_per_sm<P, CD, TF, NT>;
+  L->nt = NT;
+}
+template <class P, int CD, int TF>
+bool pick_batch_nt(int variant, BatchLaunchers* L) {
+  if (variant == 0) { fill_batch<P, CD, TF, 128>(L); return true; }
+  if (variant == 1) { fill_batch<P, CD, TF, 256>(L); return true; }
+  return false;
+}
+template <class P>
+bool pick_batch(int cd, int tf, int variant, BatchLaunchers* L) {
+  if (cd == 0 && tf == 0) return pick_batch_nt<P, 0, 0>(variant, L);
+  if (cd == 2 && tf == 0) return pick_batch_nt<P, 2, 0>(variant, L);
+  if constexpr (P::HAS_TFLUCT) {
+    if (cd == 0 && tf == 1) return pick_batch_nt<P, 0, 1>(variant, L);
+    if (cd == 2 && tf == 1) return pick_batch_nt<P, 2, 1>(variant, L);
+  }
+  return false;
+}
+
 }  // namespace SCL_PREC_NS
+
+bool SCL_BATCH_GETTER(int rp, int cd, int tf, int variant, BatchLaunchers* L) {
+  using namespace SCL_PREC_NS;
+  switch (rp) {
+    case SCL_RP_ADVECTION: return pick_batch<PAdvection>(cd, tf, variant, L);
+    case SCL_RP_EULER: return pick_batch<PEuler>(cd, tf, variant, L);
+    case SCL_RP_ACOUSTICS1D: return pick_batch<PAcoustics<2>>(cd, tf, variant, L);
+  }
+  return false;
+}
 
 bool SCL_PREC_GETTER(int rp, int ndim, int cd, int tf, int variant, Launchers* L) {
   using namespace SCL_PREC_NS;

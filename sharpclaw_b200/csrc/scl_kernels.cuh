@@ -197,35 +197,54 @@ __device__ __forceinline__ R load_aux(const void* aux, long off) {
 }
 
 // ---------------------------------------------------------------------------
-// 1-D stage kernel.  CTA b solves interfaces c = c0 .. c0+NT-1 and updates
-// cells c0 .. c0+NT-2 (c0 = 1 + b*(NT-1)); neighbouring CTAs both solve the
-// interface on their common edge (1/NT redundant work).
+// One line (a 1-D grid, a batched instance, or a line of a 2-D plugin) as a
+// stage sees it: buffers already resolved through the controller's roles.
 // ---------------------------------------------------------------------------
+template <class S>
+struct Line {
+  Ctl* ctl;            // controller of this line (dt, stage CFL slots, status)
+  const S* qin;        // stage input (read with halo)
+  const S* qo;         // pointwise extra input (qold or r1), or nullptr
+  S* out;              // stage output (with ghost images), unused for SK_DQ
+  S* out2;             // second output (SSP104 stage 5), or nullptr
+  double* dq_out;      // SK_DQ output
+  const void* aux;     // aux planes, or nullptr
+  int mx;
+  long plane;          // component stride (elements)
+  double dx;
+  int bl, br;          // mthbc of the two ends
+  int mcapa, kind, stage, ixy;
+};
+
+template <class P, int PREC, int NT>
+struct Tile1DSmem {
+  typename Prec<PREC>::S sq[P::MEQN][NT + 8];
+  typename Prec<PREC>::R rec[4][P::MEQN][NT];   // 0: qr(c-1)  1: ql(c)  2: amdq(c)  3: apdq(c)
+  typename Prec<PREC>::R sred[NT / 32];
+};
+
+// One tile of a 1-D stage: the CTA solves interfaces c = c0 .. c0+NT-1 and
+// updates cells c0 .. c0+NT-2; neighbouring tiles both solve the interface on
+// their common edge (1/NT redundant work).  Ends with a CTA-wide barrier, so
+// a CTA may run tiles back to back.
 template <class P, int CD, int TF, int PREC, int NT>
-__global__ void __launch_bounds__(NT) k_stage1d(StageArgs a) {
+__device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>& L, const Phys& ph,
+                                             int c0, Tile1DSmem<P, PREC, NT>& sm) {
   using R = typename Prec<PREC>::R;
   using S = typename Prec<PREC>::S;
   using Ac = typename Prec<PREC>::A;
   constexpr int M = P::MEQN, MW = P::MWAVES, MA = P::MAUX;
-  __shared__ S sq[M][NT + 8];
-  __shared__ R rec[4][M][NT];   // 0: qr(c-1)  1: ql(c)  2: amdq(c)  3: apdq(c)
-  __shared__ R sred[NT / 32];
-
-  const Ctl* ctl = a.ctl;
-  if (ctl->done) return;
   const int tid = threadIdx.x;
-  const int mx = a.mx;
-  const int c0 = 1 + blockIdx.x * (NT - 1);
-  const S* qin = static_cast<const S*>(a.buf[ctl->role[a.sd.in]]);
-  const double dt = ctl->dt;
-  const double dtdx0 = dt / a.dx;
+  const int mx = L.mx;
+  const double dt = L.ctl->dt;
+  const double dtdx0 = dt / L.dx;
 
   // stage cells c0-3 .. c0+NT+1 (global offset c+2)
   for (int k = tid; k < NT + 5; k += NT) {
     const long g = (long)c0 - 1 + k;
     const bool ok = g < (long)mx + 6;
 #pragma unroll
-    for (int m = 0; m < M; ++m) sq[m][k] = ok ? qin[(long)m * a.plane + g] : (S)1;
+    for (int m = 0; m < M; ++m) sm.sq[m][k] = ok ? L.qin[(long)m * L.plane + g] : (S)1;
   }
   __syncthreads();
 
@@ -238,23 +257,23 @@ __global__ void __launch_bounds__(NT) k_stage1d(StageArgs a) {
       R auxm[MA > 0 ? MA : 1], aux0[MA > 0 ? MA : 1];
 #pragma unroll
       for (int k = 0; k < MA; ++k) {
-        auxm[k] = load_aux<S>(a.aux, (long)k * a.plane + c + 1);
-        aux0[k] = load_aux<S>(a.aux, (long)k * a.plane + c + 2);
+        auxm[k] = load_aux<S>(L.aux, (long)k * L.plane + c + 1);
+        aux0[k] = load_aux<S>(L.aux, (long)k * L.plane + c + 2);
       }
-      auto qs = [&](int k, int m) -> S { return sq[m][tid + k]; };
+      auto qs = [&](int k, int m) -> S { return sm.sq[m][tid + k]; };
       R xl[M], xr[M], am[M], ap[M], s[MW];
-      solve_interface<P, CD, PREC>(a.ph, a.ixy, qs, auxm, aux0, xl, xr, am, ap, s);
+      solve_interface<P, CD, PREC>(ph, L.ixy, qs, auxm, aux0, xl, xr, am, ap, s);
 #pragma unroll
       for (int m = 0; m < M; ++m) {
-        rec[0][m][tid] = xl[m]; rec[1][m][tid] = xr[m];
-        rec[2][m][tid] = am[m]; rec[3][m][tid] = ap[m];
+        sm.rec[0][m][tid] = xl[m]; sm.rec[1][m][tid] = xr[m];
+        sm.rec[2][m][tid] = am[m]; sm.rec[3][m][tid] = ap[m];
       }
       // flux1.f90:126-133: max(dtdx(i)*s, -dtdx(i-1)*s)
       double dtdx_c = dtdx0, dtdx_m = dtdx0;
-      if (a.mcapa > 0) {
-        const S* cap = static_cast<const S*>(a.aux) + (long)(a.mcapa - 1) * a.plane;
-        dtdx_c = dt / (a.dx * (double)cap[c + 2]);
-        dtdx_m = dt / (a.dx * (double)cap[c + 1]);
+      if (L.mcapa > 0) {
+        const S* cap = static_cast<const S*>(L.aux) + (long)(L.mcapa - 1) * L.plane;
+        dtdx_c = dt / (L.dx * (double)cap[c + 2]);
+        dtdx_m = dt / (L.dx * (double)cap[c + 1]);
       }
 #pragma unroll
       for (int w = 0; w < MW; ++w) {
@@ -273,59 +292,85 @@ __global__ void __launch_bounds__(NT) k_stage1d(StageArgs a) {
       R qc[M], qlc[M], qrc[M], apc[M], amc1[M], br[M];
 #pragma unroll
       for (int m = 0; m < M; ++m) {
-        qc[m] = (R)sq[m][tid + 3];
-        qlc[m] = rec[1][m][tid];
-        apc[m] = rec[3][m][tid];
-        qrc[m] = rec[0][m][tid + 1];
-        amc1[m] = rec[2][m][tid + 1];
+        qc[m] = (R)sm.sq[m][tid + 3];
+        qlc[m] = sm.rec[1][m][tid];
+        apc[m] = sm.rec[3][m][tid];
+        qrc[m] = sm.rec[0][m][tid + 1];
+        amc1[m] = sm.rec[2][m][tid + 1];
       }
       R auxc[MA > 0 ? MA : 1];
 #pragma unroll
-      for (int k = 0; k < MA; ++k) auxc[k] = load_aux<S>(a.aux, (long)k * a.plane + c + 2);
-      cell_bracket<P, TF, PREC>(a.ph, a.ixy, qc, auxc, qlc, qrc, apc, amc1, br);
+      for (int k = 0; k < MA; ++k) auxc[k] = load_aux<S>(L.aux, (long)k * L.plane + c + 2);
+      cell_bracket<P, TF, PREC>(ph, L.ixy, qc, auxc, qlc, qrc, apc, amc1, br);
       double dtdx_c = dtdx0;
-      if (a.mcapa > 0) {
-        const S* cap = static_cast<const S*>(a.aux) + (long)(a.mcapa - 1) * a.plane;
-        dtdx_c = dt / (a.dx * (double)cap[c + 2]);
+      if (L.mcapa > 0) {
+        const S* cap = static_cast<const S*>(L.aux) + (long)(L.mcapa - 1) * L.plane;
+        dtdx_c = dt / (L.dx * (double)cap[c + 2]);
       }
-      const int kind = a.sd.kind;
+      const int kind = L.kind;
       if (kind == SK_DQ) {
 #pragma unroll
         for (int m = 0; m < M; ++m)
-          a.dq_out[(long)m * a.plane + c + 2] = (double)((R)0 - (R)dtdx_c * br[m]);
+          L.dq_out[(long)m * L.plane + c + 2] = (double)((R)0 - (R)dtdx_c * br[m]);
       } else {
-        S* out = static_cast<S*>(a.buf[ctl->role[a.sd.out]]);
-        S* out2 = a.sd.out2 >= 0 ? static_cast<S*>(a.buf[ctl->role[a.sd.out2]]) : nullptr;
-        const S* qo = a.sd.aux_in >= 0 ? static_cast<const S*>(a.buf[ctl->role[a.sd.aux_in]]) : nullptr;
         const bool edge = c <= 3 || c >= mx - 2;   // only these cells have ghost images
 #pragma unroll
         for (int m = 0; m < M; ++m) {
           Ac dqv = (Ac)((R)0 - (R)dtdx_c * br[m]);
-          Ac qv = (Ac)sq[m][tid + 3];
-          Ac qov = qo ? (Ac)qo[(long)m * a.plane + c + 2] : (Ac)0;
+          Ac qv = (Ac)sm.sq[m][tid + 3];
+          Ac qov = L.qo ? (Ac)L.qo[(long)m * L.plane + c + 2] : (Ac)0;
           Ac o1, o2 = (Ac)0;
           combine<Ac>(kind, qv, qov, dqv, o1, o2);
           bad |= !isfinite(o1);
-          if (edge) put_1d<S, Ac>(out, a.plane, m, c, images_1d(c, mx, a.mthbc[0], a.mthbc[1]), o1);
-          else out[(long)m * a.plane + c + 2] = (S)o1;
-          if (out2) out2[(long)m * a.plane + c + 2] = (S)o2;
+          if (edge) put_1d<S, Ac>(L.out, L.plane, m, c, images_1d(c, mx, L.bl, L.br), o1);
+          else L.out[(long)m * L.plane + c + 2] = (S)o1;
+          if (L.out2) L.out2[(long)m * L.plane + c + 2] = (S)o2;
         }
       }
     }
   }
 
-  // ---- CFL reduction: warp max, block max, one atomic per CTA ----
+  // ---- CFL reduction: warp max, block max, one atomic per tile ----
   cflmax = warp_max(cflmax);
-  if ((tid & 31) == 0) sred[tid >> 5] = cflmax;
+  if ((tid & 31) == 0) sm.sred[tid >> 5] = cflmax;
   const int anybad = __syncthreads_or(bad);
   if (tid < 32) {
-    R v = (tid < NT / 32) ? sred[tid] : (R)0;
+    R v = (tid < NT / 32) ? sm.sred[tid] : (R)0;
     v = warp_max(v);
     if (tid == 0) {
-      atomic_max_nonneg(&a.ctl->stage_cfl[a.stage], (double)v);
-      if (anybad) atomicOr(&a.ctl->status, SCL_STATUS_NONFINITE);
+      atomic_max_nonneg(&L.ctl->stage_cfl[L.stage], (double)v);
+      if (anybad) atomicOr(&L.ctl->status, SCL_STATUS_NONFINITE);
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// 1-D stage kernel: one tile per CTA over a single grid.
+// ---------------------------------------------------------------------------
+template <class P, int CD, int TF, int PREC, int NT>
+__global__ void __launch_bounds__(NT) k_stage1d(StageArgs a) {
+  using S = typename Prec<PREC>::S;
+  __shared__ Tile1DSmem<P, PREC, NT> sm;
+  Ctl* ctl = a.ctl;
+  if (ctl->done) return;
+  Line<S> L;
+  L.ctl = ctl;
+  L.qin = static_cast<const S*>(a.buf[ctl->role[a.sd.in]]);
+  L.qo = a.sd.aux_in >= 0 ? static_cast<const S*>(a.buf[ctl->role[a.sd.aux_in]]) : nullptr;
+  L.out = a.sd.kind == SK_DQ ? nullptr : static_cast<S*>(a.buf[ctl->role[a.sd.out]]);
+  L.out2 = a.sd.out2 >= 0 ? static_cast<S*>(a.buf[ctl->role[a.sd.out2]]) : nullptr;
+  L.dq_out = a.dq_out;
+  L.aux = a.aux;
+  L.mx = a.mx;
+  L.plane = a.plane;
+  L.dx = a.dx;
+  L.bl = a.mthbc[0];
+  L.br = a.mthbc[1];
+  L.mcapa = a.mcapa;
+  L.kind = a.sd.kind;
+  L.stage = a.stage;
+  L.ixy = a.ixy;
+  stage1d_tile<P, CD, TF, PREC, NT>(L, a.ph, 1 + blockIdx.x * (NT - 1), sm);
 }
 
 // ---------------------------------------------------------------------------

@@ -22,3 +22,24 @@ constexpr int N2D_VARIANTS = 3;
 void set_last_error(const char* msg);
 
 }  // namespace scl
+
+namespace scl {
+
+struct BatchArgs;
+
+// Batched persistent launchers of one plugin / precision / tile width.
+struct BatchLaunchers {
+  void (*stage)(const BatchArgs&, int grid, cudaStream_t);
+  void (*begin)(Ctl* ctl, const int* mx, int ninst, int* active, int* prefix, int* nact, cudaStream_t);
+  int (*blocks_per_sm)();
+  int nt;   // threads per CTA = interfaces per tile
+};
+
+constexpr int NBATCH_VARIANTS = 2;   // tile width 128 or 256
+
+bool get_batch_launchers_fp64(int rp, int cd, int tf, int variant, BatchLaunchers* L);
+bool get_batch_launchers_fp64s(int rp, int cd, int tf, int variant, BatchLaunchers* L);
+bool get_batch_launchers_mixed(int rp, int cd, int tf, int variant, BatchLaunchers* L);
+bool get_batch_launchers_fp32(int rp, int cd, int tf, int variant, BatchLaunchers* L);
+
+}  // namespace scl
