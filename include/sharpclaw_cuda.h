@@ -166,6 +166,16 @@ int scl_kernels_per_step(scl_handle* h);
 int scl_rk_step_noalloc(const scl_params* p, double* q_dev, const double* aux_dev, double dt,
                         double* cfl, void* stream);
 
+/* Discrete adjoint of one SSPRK(3,3) step (ts_ssp33, sharpclaw.f90:337-376)
+ * of dq = dt*L(q) (flux2 with componentwise WENO5 and a Riemann solver that
+ * is linear in the jumps): given q^n and lam_in = dJ/dq^{n+1}, returns
+ * lam_out = dJ/dq^n.  Device arrays in the reference layout (interior cells
+ * are meaningful).  Built for the 2-D acoustics plugin with periodic bc and
+ * double state; computed in FP64.  No reference counterpart (the reference
+ * has no adjoint). */
+int scl_adjoint_step(scl_handle* h, const double* q_dev, const double* lam_in_dev, double* lam_out_dev,
+                     double dt);
+
 /* ---- batched solver: many independent 1-D problems of uneven size ------ */
 /* Replaces a host loop that calls sharpclaw() once per problem: every
  * instance k (mx[k] cells, spacing dx[k]) has its own controller (t, dt,

@@ -86,6 +86,8 @@ SIGNATURES = [
                                       ctypes.POINTER(ctypes.c_float)]),
     ("scl_batch_tuning", ctypes.c_int, [_h, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]),
+    ("scl_adjoint_step", ctypes.c_int, [_h, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_double]),
     ("scl_stream", ctypes.c_void_p, [_h]),
 ]
 

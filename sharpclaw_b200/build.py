@@ -29,6 +29,7 @@ UNITS = {
     "scl_capi.cu": [],
     "scl_noalloc.cu": [],
     "scl_batch.cu": [],
+    "scl_adjoint.cu": ["--fmad=false"],
     "scl_prec_fp64.cu": ["--fmad=true"],
     "scl_prec_fp64s.cu": ["--fmad=false"],
     "scl_prec_mixed.cu": ["--fmad=true"] + FAST32,

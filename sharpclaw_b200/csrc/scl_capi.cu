@@ -226,6 +226,7 @@ struct scl_handle {
   int graph_steps = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t evq[2] = {nullptr, nullptr};
+  double* adj = nullptr;       // adjoint work fields (5 x meqn planes), allocated on first use
 };
 
 namespace {
@@ -457,6 +458,7 @@ int scl_destroy(scl_handle* h) {
   for (int r = 0; r < NROLES; ++r) if (h->buf[r]) cudaFree(h->buf[r]);
   if (h->aux) cudaFree(h->aux);
   if (h->stage64) cudaFree(h->stage64);
+  if (h->adj) cudaFree(h->adj);
   if (h->ctl) cudaFree(h->ctl);
   if (h->hctl) cudaFreeHost(h->hctl);
   if (h->hdone) cudaFreeHost(h->hdone);
@@ -809,3 +811,58 @@ int scl_kernels_per_step(scl_handle* h) { return h ? kernels_per_step(h) : 0; }
 namespace scl {
 void set_last_error(const char* msg) { g_err = msg ? msg : ""; }
 }  // namespace scl
+
+extern "C" int scl_adjoint_step(scl_handle* h, const double* q_dev, const double* lam_in_dev,
+                                double* lam_out_dev, double dt) {
+  if (!h || !q_dev || !lam_in_dev || !lam_out_dev) return fail(SCL_E_INVALID, "null argument");
+  const scl_params& p = h->p;
+  if (!adjoint_supported(p.rp, p.ndim, p.char_decomp, p.time_integrator, p.mthbc))
+    return fail(SCL_E_UNSUPPORTED,
+                "the adjoint covers 2-D acoustics, componentwise WENO5, SSPRK(3,3), periodic bc");
+  if (h->ssize != sizeof(double)) return fail(SCL_E_UNSUPPORTED, "the adjoint needs double state");
+  const long nfield = h->plane * p.meqn;
+  if (!h->adj) {
+    if (cudaMalloc(&h->adj, sizeof(double) * nfield * 5) != cudaSuccess)
+      return fail(SCL_E_CUDA, "cudaMalloc adjoint fields");
+    CK(cudaMemsetAsync(h->adj, 0, sizeof(double) * nfield * 5, h->stream));
+  }
+  double* L3 = h->adj;
+  double* L2 = L3 + nfield;
+  double* L1 = L2 + nfield;
+  double* T = L1 + nfield;
+  double* L0 = T + nfield;
+  // q^n into the Q register, ghost cells filled, then the forward stages
+  // q1 = q + D(q) (role A) and q2 = 3/4 q + 1/4 (q1 + D(q1)) (role B)
+  Ctl* c = h->hctl;
+  c->dt = dt;
+  c->done = 0;
+  c->status = 0;
+  for (int s = 0; s < MAXSTAGES; ++s) c->stage_cfl[s] = 0.0;
+  int rc = upload_ctl(h);
+  if (rc) return rc;
+  double* Q = static_cast<double*>(h->buf[c->role[ROLE_Q]]);
+  rc = upload_field(h, Q, q_dev, p.meqn, true);
+  if (rc) return rc;
+  launch_bc<double>(h, Q);
+  for (int s = 0; s < 2; ++s) h->L.stage(make_args(h, s), h->stream);
+  CK(cudaGetLastError());
+  const double* A = static_cast<const double*>(h->buf[c->role[ROLE_A]]);
+  const double* B = static_cast<const double*>(h->buf[c->role[ROLE_B]]);
+  const size_t w = sizeof(double) * h->ld;
+  CK(cudaMemcpy2DAsync(L3, sizeof(double) * h->pitch, lam_in_dev, w, w, (size_t)h->rows * p.meqn,
+                       cudaMemcpyDeviceToDevice, h->stream));
+  Phys ph{};
+  ph.u = p.u; ph.gamma = p.gamma; ph.gamma1 = p.gamma - 1.0; ph.grav = p.grav; ph.efix = p.efix;
+  const double* aux = static_cast<const double*>(h->aux);
+  launch_vjp2d(B, L3, aux, T, h->pitch, h->plane, p.mx, p.my, p.dx, p.dy, dt, ph, h->stream);
+  launch_adj_combine(0, L2, L3, T, nfield, h->stream);          // l2 = 2/3 (l3 + D'(q2) l3)
+  launch_vjp2d(A, L2, aux, T, h->pitch, h->plane, p.mx, p.my, p.dx, p.dy, dt, ph, h->stream);
+  launch_adj_combine(1, L1, L2, T, nfield, h->stream);          // l1 = 1/4 (l2 + D'(q1) l2)
+  launch_vjp2d(Q, L1, aux, T, h->pitch, h->plane, p.mx, p.my, p.dx, p.dy, dt, ph, h->stream);
+  launch_adj_final(L0, L3, L2, L1, T, nfield, h->stream);       // l0 = l3/3 + 3/4 l2 + l1 + D'(q0) l1
+  CK(cudaGetLastError());
+  CK(cudaMemcpy2DAsync(lam_out_dev, w, L0, sizeof(double) * h->pitch, w, (size_t)h->rows * p.meqn,
+                       cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return SCL_OK;
+}

@@ -93,9 +93,10 @@ def radial_dam(n=48, noise=1e-3, seed=3, char_decomp=2, tfluct_solver=1, mthbc=(
     return po, ps, q, None
 
 
-def acoustics2d(n=40, seed=5, char_decomp=0, tfluct_solver=1, mthbc=(2, 2, 2, 2)):
+def acoustics2d(n=40, seed=5, char_decomp=0, tfluct_solver=1, mthbc=(2, 2, 2, 2), background=0.0):
     """2-D variable-coefficient acoustics on [0,1]^2: rho, K log-normal,
-    smoothed; aux = (Z = sqrt(rho K), c = sqrt(K/rho)); p0 = Gaussian bumps."""
+    smoothed; aux = (Z = sqrt(rho K), c = sqrt(K/rho)); p0 = Gaussian bumps
+    plus `background` * cos(2 pi x) cos(2 pi y)."""
     rng = np.random.default_rng(seed)
     d = 1.0 / n
     ln_rho = rng.normal(0, 0.3, (n + 6, n + 6))
@@ -113,6 +114,7 @@ def acoustics2d(n=40, seed=5, char_decomp=0, tfluct_solver=1, mthbc=(2, 2, 2, 2)
     for _ in range(3):
         cx, cy = rng.uniform(0.2, 0.8, 2)
         p += np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * 0.05 ** 2))
+    p += background * np.cos(2 * np.pi * X) * np.cos(2 * np.pi * Y)
     q = np.zeros((3, n + 6, n + 6))
     q[0] = p
     kw = dict(mx=n, my=n, dx=d, dy=d, mthbc=mthbc, char_decomp=char_decomp, tfluct_solver=tfluct_solver)

@@ -1,0 +1,72 @@
+"""Plain PyTorch FP64 restatement of the 2-D acoustics WENO step (periodic).
+
+Used as the floating-point reference of the adjoint: torch.autograd through
+this restatement gives the exact vector-Jacobian product of the same
+discrete operator -- dq = dt*L(q) of src/2d/flux2.f90 with componentwise
+weno5 (src/reconstruct.f90:77-143), the acoustics Riemann solver
+(apps/acoustics/1d/interface/rp1acv.f:49-80 applied normal to each sweep)
+and tfluct (tfluct1acv.f:134-166) -- and SSPRK(3,3) (src/sharpclaw.f90:337-376).
+Arrays are interior cells only, (3, ny, nx); periodic bc are rolls.
+"""
+import numpy as np
+import torch
+
+EPS = float(np.float32(1e-36))
+
+
+def weno_side(dm2, dm1, d0, dp1, im):
+    t1 = im * (dm2 - dm1)
+    t2 = im * (dm1 - d0)
+    t3 = im * (d0 - dp1)
+    # 13.*t**2 + 3.*x**2 associated as the Fortran source (reconstruct.f90:117-119)
+    x1, x2, x3 = dm2 - 3.0 * dm1, dm1 + d0, 3.0 * d0 - dp1
+    tt1 = (EPS + (13.0 * (t1 * t1) + 3.0 * (x1 * x1))) ** 2
+    tt2 = (EPS + (13.0 * (t2 * t2) + 3.0 * (x2 * x2))) ** 2
+    tt3 = (EPS + (13.0 * (t3 * t3) + 3.0 * (x3 * x3))) ** 2
+    s1 = tt2 * tt3
+    s2 = 6.0 * tt1 * tt3
+    s3 = 3.0 * tt1 * tt2
+    t0 = 1.0 / ((s1 + s2) + s3)
+    s1 = s1 * t0
+    s3 = s3 * t0
+    return ((s1 * (t2 - t1)) + ((0.5 * s3 - 0.25) * (t3 - t2))) / 3.0
+
+
+def sweep(q, Z, c, dtdx, axis, mu):
+    r = lambda a, s: torch.roll(a, s, dims=axis)   # r(a, 1)[i] = a[i-1]
+    d = q - r(q, 1)
+    D0, D1, D2, D3 = r(d, 1), d, r(d, -1), r(d, -2)
+    qr = weno_side(D0, D1, D2, D3, 1.0) + (-r(q, 1) + 7.0 * (q + r(q, -1)) - r(q, -2)) / 12.0
+    ql = weno_side(D3, D2, D1, D0, -1.0) + (-r(q, 2) + 7.0 * (r(q, 1) + q) - r(q, -1)) / 12.0
+    dl = ql - r(qr, 1)                      # interface i: ql(i) - qr(i-1)
+    zi, zim = Z, r(Z, 1)
+    a1 = (-dl[0] + zi * dl[mu]) / (zim + zi)
+    a2 = (dl[0] + zim * dl[mu]) / (zim + zi)
+    s1, s2 = -r(c, 1), c
+    zero = torch.zeros_like(a1)
+    w1 = [-a1 * zim, zero, zero]
+    w1[mu] = a1
+    w2 = [a2 * zi, zero, zero]
+    w2[mu] = a2
+    amdq = torch.stack([s1 * w for w in w1])
+    apdq = torch.stack([s2 * w for w in w2])
+    dt_ = qr - ql                           # tfluct: left ql(i), right qr(i), aux of cell i
+    b1 = (-dt_[0] + Z * dt_[mu]) / (2.0 * Z)
+    b2 = (dt_[0] + Z * dt_[mu]) / (2.0 * Z)
+    v1 = [-b1 * Z, zero, zero]
+    v1[mu] = b1
+    v2 = [b2 * Z, zero, zero]
+    v2[mu] = b2
+    adq = torch.stack([-c * a + c * b for a, b in zip(v1, v2)])
+    amdq_next = torch.roll(amdq, -1, dims=axis)
+    return -dtdx * (apdq + adq + amdq_next)
+
+
+def D(q, Z, c, dt, dx, dy):
+    return sweep(q, Z, c, dt / dx, -1, 1) + sweep(q, Z, c, dt / dy, -2, 2)
+
+
+def ssprk3(q, Z, c, dt, dx, dy):
+    q1 = q + D(q, Z, c, dt, dx, dy)
+    q2 = 0.75 * q + 0.25 * (q1 + D(q1, Z, c, dt, dx, dy))
+    return (q + 2.0 * (q2 + D(q2, Z, c, dt, dx, dy))) / 3.0
