@@ -97,6 +97,24 @@ __device__ __forceinline__ void put_2d(S* base, long plane, long pitch, int m, i
   }
 }
 
+// Out-of-line entry points of the plugins for the FP32 forms (see SCL_FP32_FN).
+template <class P>
+__device__ SCL_FP32_FN void rp_f32(const Phys& ph, int ixy, const float* L, const float* Rt, const float* dl,
+                                    const float* al, const float* ar, float* s, float* am, float* ap) {
+  P::template rp<float>(ph, ixy, L, Rt, dl, al, ar, s, am, ap);
+}
+template <class P>
+__device__ SCL_FP32_FN void tfluct_f32(const Phys& ph, int ixy, const float* L, const float* Rt,
+                                        const float* dl, const float* aux, float* adq) {
+  P::template tfluct<float>(ph, ixy, L, Rt, dl, aux, adq);
+}
+template <class P>
+__device__ SCL_FP32_FN void evec_f32(const Phys& ph, int ixy, const float* qm, const float* q0,
+                                      const float* am, const float* a0, float (*evl)[P::MEQN],
+                                      float (*evr)[P::MEQN]) {
+  P::template evec<float>(ph, ixy, qm, q0, am, a0, evl, evr);
+}
+
 // ---------------------------------------------------------------------------
 // One interface c-1/2 (between cells c-1 and c) of a line: reconstruction,
 // Riemann solve and the CFL contribution.  `qs(k, m)` returns cell c-3+k.
@@ -141,7 +159,7 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs,
       float qm[M], q0[M], evl[M][M], evr[M][M];
 #pragma unroll
       for (int m = 0; m < M; ++m) { qm[m] = (float)qs(2, m); q0[m] = (float)qs(3, m); }
-      P::template evec<float>(ph, ixy, qm, q0, auxm, aux0, evl, evr);
+      evec_f32<P>(ph, ixy, qm, q0, auxm, aux0, evl, evr);
       weno5_char_offset<M>(d, evl, evr, xl, xr);
     } else {
       weno5_offset<M>(d, xl, xr);
@@ -153,7 +171,7 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs,
       Rt[m] = (float)qs(3, m) + xr[m];
       dl[m] = d[2][m] + (xr[m] - xl[m]);   // (q(c)-q(c-1)) + (el - er)
     }
-    P::template rp<float>(ph, ixy, L, Rt, dl, auxm, aux0, s, amdq, apdq);
+    rp_f32<P>(ph, ixy, L, Rt, dl, auxm, aux0, s, amdq, apdq);
   }
 }
 
@@ -180,12 +198,14 @@ __device__ __forceinline__ void cell_bracket(const Phys& ph, int ixy, const type
   }
   if constexpr (TF == 1) {
     R adq[M];
-    P::template tfluct<R>(ph, ixy, L, Rt, dl, auxc, adq);
+    if constexpr (Prec<PREC>::EXACT) P::template tfluct<R>(ph, ixy, L, Rt, dl, auxc, adq);
+    else tfluct_f32<P>(ph, ixy, L, Rt, dl, auxc, adq);
 #pragma unroll
     for (int m = 0; m < M; ++m) br[m] = (apdq_c[m] + adq[m]) + amdq_c1[m];       // :151-152
   } else {
     R s2[P::MWAVES], am2[M], ap2[M];
-    P::template rp<R>(ph, ixy, L, Rt, dl, auxc, auxc, s2, am2, ap2);             // :181-182
+    if constexpr (Prec<PREC>::EXACT) P::template rp<R>(ph, ixy, L, Rt, dl, auxc, auxc, s2, am2, ap2);  // :181-182
+    else rp_f32<P>(ph, ixy, L, Rt, dl, auxc, auxc, s2, am2, ap2);
 #pragma unroll
     for (int m = 0; m < M; ++m) br[m] = ((amdq_c1[m] + apdq_c[m]) + am2[m]) + ap2[m];  // :185-186
   }

@@ -15,6 +15,13 @@
 
 namespace scl {
 
+// FP32 Euler plugins use reciprocal-square-root forms of the Roe averages and
+// the entropy-fix sound speeds (algebraically the reference's, not its
+// operation order; the FP64 forms keep the reference's order).
+#ifndef SCL_FAST_ROE
+#define SCL_FAST_ROE 1
+#endif
+
 template <class R>
 __device__ __forceinline__ R rmin(R a, R b) { return a < b ? a : b; }
 template <class R>
@@ -61,6 +68,22 @@ struct PEuler {
 
   template <class R>
   __device__ static void roe(const Phys& ph, const R* L, const R* Rt, R& u, R& enth, R& a) {
+#if SCL_FAST_ROE
+    if constexpr (sizeof(R) == 4) {
+      // FP32 form: the same Roe averages with reciprocal square roots,
+      // sqrt(rho) = rho*w and m/sqrt(rho) = m*w for w = 1/sqrt(rho)
+      const float g1 = (float)ph.gamma1;
+      const float wl = rsqrtf(L[0]), wr = rsqrtf(Rt[0]);
+      const float pl = g1 * (L[2] - 0.5f * (L[1] * L[1]) * (wl * wl));
+      const float pr = g1 * (Rt[2] - 0.5f * (Rt[1] * Rt[1]) * (wr * wr));
+      const float inv = __frcp_rn(L[0] * wl + Rt[0] * wr);
+      u = (L[1] * wl + Rt[1] * wr) * inv;
+      enth = ((L[2] + pl) * wl + (Rt[2] + pr) * wr) * inv;
+      const float a2 = g1 * (enth - 0.5f * (u * u));
+      a = a2 * rsqrtf(a2);
+      return;
+    }
+#endif
     const R g1 = (R)ph.gamma1;
     R rhsqrtl = sqrt(L[0]);
     R rhsqrtr = sqrt(Rt[0]);
@@ -79,8 +102,18 @@ struct PEuler {
     const R gamma = (R)ph.gamma, g1 = (R)ph.gamma1;
     R u, enth, a;
     roe(ph, L, Rt, u, enth, a);                                   // rp1eu.f:44-55
-    R a2 = (g1 / (a * a)) * (((enth - u * u) * dl[0] + u * dl[1]) - dl[2]);   // :65-66
-    R a3 = ((dl[1] + (a - u) * dl[0]) - a * a2) / ((R)2 * a);                   // :67
+    R a2, a3;
+#if SCL_FAST_ROE
+    if constexpr (sizeof(R) == 4) {
+      const float ia = __frcp_rn(a);
+      a2 = (g1 * (ia * ia)) * (((enth - u * u) * dl[0] + u * dl[1]) - dl[2]);
+      a3 = ((dl[1] + (a - u) * dl[0]) - a * a2) * (0.5f * ia);
+    } else
+#endif
+    {
+      a2 = (g1 / (a * a)) * (((enth - u * u) * dl[0] + u * dl[1]) - dl[2]);   // :65-66
+      a3 = ((dl[1] + (a - u) * dl[0]) - a * a2) / ((R)2 * a);                   // :67
+    }
     R a1 = (dl[0] - a2) - a3;                                                   // :68
     R w[3][3];  // w[wave][component]
     w[0][0] = a1; w[0][1] = a1 * (u - a); w[0][2] = a1 * (enth - u * a);
@@ -158,6 +191,21 @@ struct PEuler {
   template <class R>
   __device__ static void evec(const Phys& ph, int, const R* qm, const R* q0, const R*, const R*,
                               R evl[3][3], R evr[3][3]) {
+#if SCL_FAST_ROE
+    if constexpr (sizeof(R) == 4) {
+      float u, h, a;
+      roe(ph, qm, q0, u, h, a);
+      const float g1 = (float)ph.gamma1, ia = __frcp_rn(a);
+      evr[0][0] = 1.0f;      evr[0][1] = 1.0f;             evr[0][2] = 1.0f;
+      evr[1][0] = u - a;     evr[1][1] = u;                evr[1][2] = u + a;
+      evr[2][0] = h - u * a; evr[2][1] = 0.5f * (u * u);   evr[2][2] = h + u * a;
+      const float b1 = g1 * (ia * ia), b2 = 0.5f * (b1 * (u * u)), ua = u * ia, b1u = b1 * u;
+      evl[0][0] = 0.5f * (b2 + ua); evl[0][1] = -0.5f * (b1u + ia); evl[0][2] = 0.5f * b1;
+      evl[1][0] = 1.0f - b2;        evl[1][1] = b1u;                evl[1][2] = -b1;
+      evl[2][0] = 0.5f * (b2 - ua); evl[2][1] = -0.5f * (b1u - ia); evl[2][2] = 0.5f * b1;
+      return;
+    }
+#endif
     const R g1 = (R)ph.gamma1;
     R rhsqrtl = sqrt(qm[0]);
     R rhsqrtr = sqrt(q0[0]);

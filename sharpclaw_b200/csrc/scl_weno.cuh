@@ -73,8 +73,21 @@ __device__ __forceinline__ float weno_side_scaled(float dm2, float dm1, float d0
   return ((s1 * (t2 - t1)) + ((0.5f * s3 - 0.25f) * (t3 - t2))) * (1.0f / 3.0f);
 }
 
+// The FP32 forms can call their large device functions out of line:
+// one shared copy shrinks the kernel's instruction footprint, but the call
+// overhead made the char-wise Euler stage kernel 1.85x slower on B200, so it
+// is off by default.
+#ifndef SCL_OUTLINE_FP32
+#define SCL_OUTLINE_FP32 0
+#endif
+#if SCL_OUTLINE_FP32
+#define SCL_FP32_FN __noinline__
+#else
+#define SCL_FP32_FN __forceinline__
+#endif
+
 // Both sides of the scaled correction for one set of five jumps h[0..4].
-__device__ __forceinline__ void weno_pair_scaled(const float h[5], float& u1, float& u2) {
+static __device__ SCL_FP32_FN void weno_pair_scaled(const float h[5], float& u1, float& u2) {
   float sc = fmaxf(fmaxf(fmaxf(fabsf(h[0]), fabsf(h[1])), fmaxf(fabsf(h[2]), fabsf(h[3]))),
                    fabsf(h[4]));
   if (!(sc > 0.0f) || !(sc < 3.0e38f)) {  // all-zero stencil (or non-finite)
