@@ -425,6 +425,8 @@ def run_gpu(args, rank, world, local_rank):
                "stages_per_time_step": W["stages"], "precision": args.precision,
                "l2": "flushed (256 MiB write) between timed steps",
                "parallelism": "replicas (one independent grid per GPU)"}
+        if ps.ndim == 2:
+            cfg["tiles"] = {"headline": s_mix.tiles(), "fp64": s_64.tiles()}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_mix / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,

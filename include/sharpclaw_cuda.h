@@ -149,6 +149,22 @@ int scl_time_stages(scl_handle* h, double dt, int reps, float* ms, long long* la
  * CFL kernel in 2-D). */
 int scl_kernels_per_step(scl_handle* h);
 
+/* Tile shape of the fused 2-D stage kernel (no counterpart in the reference;
+ * flux2.f90 sweeps whole lines).  Shapes: 0 = 16x7 cells on 128 threads,
+ * 1 = 32x7 on 256, 2 = 16x15 on 256.  variant -1 (the default) makes the next
+ * scl_sharpclaw / scl_time_steps time one stage of every shape on the current
+ * state and keep the fastest; 0..SCL_TILE_SHAPES-1 fixes a shape.  Every
+ * shape evaluates each interface and cell with the same arithmetic, so the
+ * results are bitwise identical.  1-D handles accept -1 and 0 only. */
+#define SCL_TILE_SHAPES 3
+int scl_select_tiles(scl_handle* h, int variant);
+
+/* Shape in use (0 until a run has tuned or one was fixed), whether it was
+ * chosen by timing (1) or not (0), and the trial time in ms of one stage per
+ * shape (SCL_TILE_SHAPES entries, 0 for shapes not timed); any out pointer
+ * may be NULL. */
+int scl_tiles(scl_handle* h, int* variant, int* tuned, float* trial_ms);
+
 /* One SSP-RK time step of a 1-D grid that allocates nothing, for callers
  * that cannot call cudaMalloc (no counterpart in the reference).  The caller
  * owns every array: q_dev (device, reference layout, double, ghost cells

@@ -238,6 +238,21 @@ class Solver:
     def kernels_per_step(self) -> int:
         return C.lib().scl_kernels_per_step(self._h)
 
+    TILE_SHAPES = ((16, 7, 128), (32, 7, 256), (16, 15, 256))  # (cells x, cells y, threads)
+
+    def select_tiles(self, variant: int = -1):
+        """Fix the 2-D stage kernel's tile shape (index into TILE_SHAPES), or
+        with -1 let the next run time every shape and keep the fastest."""
+        C.check(C.lib().scl_select_tiles(self._h, int(variant)), "scl_select_tiles")
+
+    def tiles(self):
+        """Shape in use, whether it was chosen by timing, per-shape trial ms."""
+        v, t = ctypes.c_int(), ctypes.c_int()
+        tm = (ctypes.c_float * len(self.TILE_SHAPES))()
+        C.check(C.lib().scl_tiles(self._h, ctypes.byref(v), ctypes.byref(t), tm), "scl_tiles")
+        return {"variant": v.value, "shape": self.TILE_SHAPES[v.value], "tuned": bool(t.value),
+                "trial_ms": list(tm)}
+
 
 def sharpclaw(params: ClawParams, q, aux=None, *, tstart: float, tend: float, dt_initial: float,
               cfl_max: float, cfl_desired: float, dt_max: float = 1e99, max_steps: int = 50000,

@@ -74,6 +74,9 @@ SIGNATURES = [
     ("scl_time_stages", ctypes.c_int, [_h, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
                                         ctypes.POINTER(ctypes.c_longlong)]),
     ("scl_kernels_per_step", ctypes.c_int, [_h]),
+    ("scl_select_tiles", ctypes.c_int, [_h, ctypes.c_int]),
+    ("scl_tiles", ctypes.c_int, [_h, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                 ctypes.POINTER(ctypes.c_float)]),
     ("scl_rk_step_noalloc", ctypes.c_int, [ctypes.POINTER(scl_params), ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_double, _dp, ctypes.c_void_p]),
     ("scl_batch_create", ctypes.c_int, [ctypes.POINTER(scl_params), ctypes.c_int, ctypes.c_void_p,

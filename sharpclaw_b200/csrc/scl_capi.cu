@@ -203,6 +203,8 @@ int stage_table(int ti, StageDesc* sd, int* final_role) {
 
 }  // namespace
 
+static_assert(N2D_VARIANTS == SCL_TILE_SHAPES, "tile shape count of the C interface");
+
 struct scl_handle {
   scl_params p{};
   int device = 0;
@@ -218,8 +220,13 @@ struct scl_handle {
   Ctl* ctl = nullptr;          // device controller
   Ctl* hctl = nullptr;         // pinned host mirror
   int* hdone = nullptr;        // pinned flag
-  Launchers L{};
+  Launchers L{};                    // launchers in use (LV[variant])
+  Launchers LV[N2D_VARIANTS]{};     // every tile shape (LV[0] only in 1-D)
+  int nvariants = 1;
   int variant = 0;
+  int tiles_fixed = 0;              // 1: shape set by scl_select_tiles
+  int tiles_tuned = 0;              // 1: shape chosen by timing
+  float tile_ms[N2D_VARIANTS] = {0.f, 0.f, 0.f};
   StageDesc sd[MAXSTAGES];
   int nstages = 0, final_role = ROLE_A;
   cudaGraphExec_t graph = nullptr;
@@ -308,6 +315,53 @@ int build_graph(scl_handle* h, int steps) {
 }
 
 int default_graph_steps(const scl_handle* h) { return std::max(1, 160 / kernels_per_step(h)); }
+
+// Switch the stage launchers to tile shape v; a captured graph holds the old
+// kernel, so it is dropped and rebuilt by the next run.
+void use_variant(scl_handle* h, int v) {
+  if (v == h->variant) return;
+  h->variant = v;
+  h->L = h->LV[v];
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+}
+
+// Time the first RK stage of every 2-D tile shape on the current state and
+// keep the fastest.  The trials run against a copy of the controller (ctl[1]),
+// so the run's CFL record and status are untouched, and stage 0 writes only
+// register A, which every step overwrites before reading.
+int tune_tiles(scl_handle* h) {
+  Ctl* trial = h->ctl + 1;
+  CK(cudaMemcpyAsync(trial, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToDevice, h->stream));
+  StageArgs a = make_args(h, 0);
+  a.ctl = trial;
+  int best = 0;
+  for (int v = 0; v < h->nvariants; ++v) {
+    h->LV[v].stage(a, h->stream);  // warm-up (first launch of a kernel)
+    CK(cudaEventRecord(h->ev0, h->stream));
+    h->LV[v].stage(a, h->stream);
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    float one = 0.f;
+    CK(cudaEventElapsedTime(&one, h->ev0, h->ev1));
+    // about 2 ms of launches per shape, 3 to 50 of them
+    const int reps = std::min(50, std::max(3, (int)(2.0f / std::max(one, 1e-3f))));
+    CK(cudaEventRecord(h->ev0, h->stream));
+    for (int r = 0; r < reps; ++r) h->LV[v].stage(a, h->stream);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->tile_ms[v] = ms / reps;
+    if (h->tile_ms[v] < h->tile_ms[best]) best = v;
+  }
+  // near-ties keep shape 0, so that timing noise does not flip the choice
+  // (in the FMA forms a different shape can change the last bits)
+  if (!(h->tile_ms[best] < 0.98f * h->tile_ms[0])) best = 0;
+  use_variant(h, best);
+  h->tiles_tuned = 1;
+  return SCL_OK;
+}
 
 template <class S>
 void launch_bc(scl_handle* h, S* q) {
@@ -415,10 +469,16 @@ int scl_create(const scl_params* p, scl_handle** out) {
   h->rows = p->ndim == 2 ? p->my + 2 * p->mbc : 1;
   h->pitch = (h->ld + 31) / 32 * 32;
   h->plane = h->pitch * h->rows;
-  if (!get_launchers(p->precision, p->rp, p->ndim, p->char_decomp, p->tfluct_solver, h->variant, &h->L)) {
+  if (!get_launchers(p->precision, p->rp, p->ndim, p->char_decomp, p->tfluct_solver, 0, &h->LV[0])) {
     delete h;
     return fail(SCL_E_UNSUPPORTED, "no kernel for this plugin / char_decomp / tfluct_solver");
   }
+  h->L = h->LV[0];
+  if (p->ndim == 2)
+    while (h->nvariants < N2D_VARIANTS &&
+           get_launchers(p->precision, p->rp, p->ndim, p->char_decomp, p->tfluct_solver, h->nvariants,
+                         &h->LV[h->nvariants]))
+      h->nvariants += 1;
   h->nstages = stage_table(p->time_integrator, h->sd, &h->final_role);
   auto cleanup = [&](int code) { scl_destroy(h); return code; };
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
@@ -434,7 +494,8 @@ int scl_create(const scl_params* p, scl_handle** out) {
   const size_t sbytes = sizeof(double) * h->plane * std::max(p->meqn, std::max(1, p->maux));
   if (cudaMalloc(&h->stage64, sbytes) != cudaSuccess) return cleanup(fail(SCL_E_CUDA, "cudaMalloc staging"));
   cudaMemsetAsync(h->stage64, 0, sbytes, h->stream);
-  if (cudaMalloc(&h->ctl, sizeof(Ctl)) != cudaSuccess) return cleanup(fail(SCL_E_CUDA, "cudaMalloc ctl"));
+  // ctl[0] is the controller, ctl[1] a copy the tile-shape trials write into
+  if (cudaMalloc(&h->ctl, 2 * sizeof(Ctl)) != cudaSuccess) return cleanup(fail(SCL_E_CUDA, "cudaMalloc ctl"));
   if (cudaMallocHost(&h->hctl, sizeof(Ctl)) != cudaSuccess) return cleanup(fail(SCL_E_CUDA, "cudaMallocHost"));
   if (cudaMallocHost(&h->hdone, 2 * sizeof(int)) != cudaSuccess) return cleanup(fail(SCL_E_CUDA, "cudaMallocHost"));
   memset(h->hctl, 0, sizeof(Ctl));
@@ -685,7 +746,9 @@ int init_run(scl_handle* h, const scl_run* run, int max_steps, scl_result* res, 
     *early = true;
     return SCL_OK;
   }
-  return upload_ctl(h);
+  int rc = upload_ctl(h);
+  if (rc == SCL_OK && h->nvariants > 1 && !h->tiles_fixed && !h->tiles_tuned) rc = tune_tiles(h);
+  return rc;
 }
 
 void finish_run(scl_handle* h, scl_result* res) {
@@ -805,6 +868,28 @@ int scl_time_stages(scl_handle* h, double dt, int reps, float* ms, long long* la
 }
 
 int scl_kernels_per_step(scl_handle* h) { return h ? kernels_per_step(h) : 0; }
+
+int scl_select_tiles(scl_handle* h, int variant) {
+  if (!h) return fail(SCL_E_INVALID, "null handle");
+  if (variant < -1 || variant >= h->nvariants) return fail(SCL_E_UNSUPPORTED, "no such tile shape for this handle");
+  for (int v = 0; v < N2D_VARIANTS; ++v) h->tile_ms[v] = 0.f;
+  h->tiles_tuned = 0;
+  h->tiles_fixed = variant >= 0;
+  if (variant >= 0) {
+    CK(cudaStreamSynchronize(h->stream));  // no launch of the old graph in flight
+    use_variant(h, variant);
+  }
+  return SCL_OK;
+}
+
+int scl_tiles(scl_handle* h, int* variant, int* tuned, float* trial_ms) {
+  if (!h) return fail(SCL_E_INVALID, "null handle");
+  if (variant) *variant = h->variant;
+  if (tuned) *tuned = h->tiles_tuned;
+  if (trial_ms)
+    for (int v = 0; v < N2D_VARIANTS; ++v) trial_ms[v] = h->tile_ms[v];
+  return SCL_OK;
+}
 
 }  // extern "C"
 

@@ -444,8 +444,12 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
   for (int w = tid; w < T::NXI + T::NYI; w += NT) {
     const bool isx = w < T::NXI;
     int li, lj, gi, gj;  // interface between (gi-1,gj) and (gi,gj) [x] or (gi,gj-1) and (gi,gj) [y]
-    if (isx) { li = w % (TX + 1); lj = w / (TX + 1); }
-    else { li = (w - T::NXI) % TX; lj = (w - T::NXI) / TX; }
+    // x-interfaces: columns 0..TX-1 row by row (a half-warp reads 16
+    // consecutive cells of one smem row), then column TX of every row
+    if (isx) {
+      if (w < TX * TY) { li = w % TX; lj = w / TX; }
+      else { li = TX; lj = w - TX * TY; }
+    } else { li = (w - T::NXI) % TX; lj = (w - T::NXI) / TX; }
     gi = i0 + li; gj = j0 + lj;
     const bool valid = isx ? (gi <= nx + 1 && gj <= ny) : (gi <= nx && gj <= ny + 1);
     if (!valid) continue;
@@ -510,7 +514,9 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
     }
     R dqs[M];
     {
-      const int sa = li + lj * (TX + 1), sb = sa + 1;
+      // x records follow the interface order above: (li, lj) at li + lj*TX
+      // for li < TX, column TX at TX*TY + lj
+      const int sa = li + lj * TX, sb = li + 1 < TX ? sa + 1 : TX * TY + lj;
       R qlc[M], qrc[M], apc[M], amc1[M], br[M];
 #pragma unroll
       for (int m = 0; m < M; ++m) {

@@ -53,14 +53,17 @@ def main():
     ap.add_argument("--mx", type=int, default=1 << 23)
     ap.add_argument("--precision", default="mixed")
     ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--tiles", type=int, default=0, help="2-D tile shape (Solver.TILE_SHAPES index)")
     a = ap.parse_args()
     p, q, aux, dt = WORKLOADS[a.workload](a.mx)
     with S.Solver(p, a.precision) as s:
         if aux is not None:
             s.set_aux(aux)
         s.set_q(q)
+        if p.ndim == 2:
+            s.select_tiles(a.tiles)
         ms, n = s.time_stages(dt, a.reps)
-    print(json.dumps({"workload": a.workload, "mx": a.mx, "precision": a.precision,
+    print(json.dumps({"workload": a.workload, "mx": a.mx, "precision": a.precision, "tiles": a.tiles,
                       "launches": n, "avg_launch_us": 1000.0 * ms / n}))
 
 
