@@ -111,4 +111,22 @@ __device__ __forceinline__ T warp_max(T v) {
   return v;
 }
 
+// Reciprocal of the FP32 forms: the hardware approximation (at most 1 ulp
+// from the rounded reciprocal over the whole range; subnormal results flush
+// to zero).  Every use is a scale factor (WENO stencil scaling and weight
+// normalisation, Roe averages, 1/rho), so results stay within a few ulp of
+// the correctly rounded ones, inside the rounding of those forms.
+#ifndef SCL_FAST_RCP
+#define SCL_FAST_RCP 1
+#endif
+__device__ __forceinline__ float rcp32(float x) {
+#if SCL_FAST_RCP
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+#else
+  return __frcp_rn(x);
+#endif
+}
+
 }  // namespace scl

@@ -66,8 +66,10 @@ struct PEuler {
   static constexpr int MEQN = 3, MWAVES = 3, MAUX = 0, NDIM = 1;
   static constexpr bool HAS_TFLUCT = false;
 
+  // `ia` (FP32 form only) receives 1/a.
   template <class R>
-  __device__ static void roe(const Phys& ph, const R* L, const R* Rt, R& u, R& enth, R& a) {
+  __device__ static void roe(const Phys& ph, const R* L, const R* Rt, R& u, R& enth, R& a,
+                             R* ia = nullptr) {
 #if SCL_FAST_ROE
     if constexpr (sizeof(R) == 4) {
       // FP32 form: the same Roe averages with reciprocal square roots,
@@ -76,11 +78,13 @@ struct PEuler {
       const float wl = rsqrtf(L[0]), wr = rsqrtf(Rt[0]);
       const float pl = g1 * (L[2] - 0.5f * (L[1] * L[1]) * (wl * wl));
       const float pr = g1 * (Rt[2] - 0.5f * (Rt[1] * Rt[1]) * (wr * wr));
-      const float inv = __frcp_rn(L[0] * wl + Rt[0] * wr);
+      const float inv = rcp32(L[0] * wl + Rt[0] * wr);
       u = (L[1] * wl + Rt[1] * wr) * inv;
       enth = ((L[2] + pl) * wl + (Rt[2] + pr) * wr) * inv;
       const float a2 = g1 * (enth - 0.5f * (u * u));
-      a = a2 * rsqrtf(a2);
+      const float ra = rsqrtf(a2);
+      a = a2 * ra;
+      if (ia) *ia = ra;
       return;
     }
 #endif
@@ -96,16 +100,34 @@ struct PEuler {
     a = sqrt(a2);
   }
 
+  // u - c (PLUS false) or u + c (PLUS true) of one state, the four
+  // characteristic speeds of the entropy fix (rp1eu.f:132-134, 150-152,
+  // 170-172, 180-182).
+  template <bool PLUS, class R>
+  __device__ static R efix_speed(const Phys& ph, R rho, R m, R en) {
+#if SCL_FAST_ROE
+    if constexpr (sizeof(R) == 4) {  // one reciprocal, one square root
+      const float ir = rcp32(rho), u = m * ir;
+      const float p = (float)ph.gamma1 * (en - 0.5f * (m * u));
+      const float c = sqrtf(((float)ph.gamma * p) * ir);
+      return PLUS ? u + c : u - c;
+    }
+#endif
+    const R g1 = (R)ph.gamma1, gamma = (R)ph.gamma;
+    R p = g1 * (en - ((R)0.5 * (m * m)) / rho);
+    R c = sqrt((gamma * p) / rho);
+    return PLUS ? m / rho + c : m / rho - c;
+  }
+
   template <class R>
   __device__ static void rp(const Phys& ph, int, const R* L, const R* Rt, const R* dl, const R*,
                             const R*, R* s, R* amdq, R* apdq) {
-    const R gamma = (R)ph.gamma, g1 = (R)ph.gamma1;
-    R u, enth, a;
-    roe(ph, L, Rt, u, enth, a);                                   // rp1eu.f:44-55
+    const R g1 = (R)ph.gamma1;
+    R u, enth, a, ia = (R)0;
+    roe(ph, L, Rt, u, enth, a, &ia);                              // rp1eu.f:44-55
     R a2, a3;
 #if SCL_FAST_ROE
     if constexpr (sizeof(R) == 4) {
-      const float ia = __frcp_rn(a);
       a2 = (g1 * (ia * ia)) * (((enth - u * u) * dl[0] + u * dl[1]) - dl[2]);
       a3 = ((dl[1] + (a - u) * dl[0]) - a * a2) * (0.5f * ia);
     } else
@@ -135,10 +157,7 @@ struct PEuler {
     }
     // entropy fix, rp1eu.f:126-201
     do {
-      R rhoim1 = L[0];
-      R pim1 = g1 * (L[2] - ((R)0.5 * (L[1] * L[1])) / rhoim1);
-      R cim1 = sqrt((gamma * pim1) / rhoim1);
-      R s0 = L[1] / rhoim1 - cim1;
+      R s0 = efix_speed<false>(ph, L[0], L[1], L[2]);
       if (s0 >= (R)0 && s[0] > (R)0) {
         amdq[0] = amdq[1] = amdq[2] = (R)0;
         break;
@@ -146,9 +165,7 @@ struct PEuler {
       R rho1 = L[0] + w[0][0];
       R rhou1 = L[1] + w[0][1];
       R en1 = L[2] + w[0][2];
-      R p1 = g1 * (en1 - ((R)0.5 * (rhou1 * rhou1)) / rho1);
-      R c1 = sqrt((gamma * p1) / rho1);
-      R s1 = rhou1 / rho1 - c1;
+      R s1 = efix_speed<false>(ph, rho1, rhou1, en1);
       R sfract;
       if (s0 < (R)0 && s1 > (R)0) sfract = (s0 * (s1 - s[0])) / (s1 - s0);
       else if (s[0] < (R)0) sfract = s[0];
@@ -158,16 +175,11 @@ struct PEuler {
       if (s[1] >= (R)0) break;
 #pragma unroll
       for (int m = 0; m < 3; ++m) amdq[m] = amdq[m] + s[1] * w[1][m];
-      R rhoi = Rt[0];
-      R pi = g1 * (Rt[2] - ((R)0.5 * (Rt[1] * Rt[1])) / rhoi);
-      R ci = sqrt((gamma * pi) / rhoi);
-      R s3 = Rt[1] / rhoi + ci;
+      R s3 = efix_speed<true>(ph, Rt[0], Rt[1], Rt[2]);
       R rho2 = Rt[0] - w[2][0];
       R rhou2 = Rt[1] - w[2][1];
       R en2 = Rt[2] - w[2][2];
-      R p2 = g1 * (en2 - ((R)0.5 * (rhou2 * rhou2)) / rho2);
-      R c2 = sqrt((gamma * p2) / rho2);
-      R s2 = rhou2 / rho2 + c2;
+      R s2 = efix_speed<true>(ph, rho2, rhou2, en2);
       if (s2 < (R)0 && s3 > (R)0) sfract = (s2 * (s3 - s[2])) / (s3 - s2);
       else if (s[2] < (R)0) sfract = s[2];
       else break;
@@ -193,9 +205,9 @@ struct PEuler {
                               R evl[3][3], R evr[3][3]) {
 #if SCL_FAST_ROE
     if constexpr (sizeof(R) == 4) {
-      float u, h, a;
-      roe(ph, qm, q0, u, h, a);
-      const float g1 = (float)ph.gamma1, ia = __frcp_rn(a);
+      float u, h, a, ia;
+      roe(ph, qm, q0, u, h, a, &ia);
+      const float g1 = (float)ph.gamma1;
       evr[0][0] = 1.0f;      evr[0][1] = 1.0f;             evr[0][2] = 1.0f;
       evr[1][0] = u - a;     evr[1][1] = u;                evr[1][2] = u + a;
       evr[2][0] = h - u * a; evr[2][1] = 0.5f * (u * u);   evr[2][2] = h + u * a;

@@ -67,7 +67,7 @@ __device__ __forceinline__ float weno_side_scaled(float dm2, float dm1, float d0
   float s1 = tt2 * tt3;
   float s2 = (6.0f * tt1) * tt3;
   float s3 = (3.0f * tt1) * tt2;
-  float t0 = __frcp_rn((s1 + s2) + s3);
+  float t0 = rcp32((s1 + s2) + s3);
   s1 = s1 * t0;
   s3 = s3 * t0;
   return ((s1 * (t2 - t1)) + ((0.5f * s3 - 0.25f) * (t3 - t2))) * (1.0f / 3.0f);
@@ -86,19 +86,75 @@ __device__ __forceinline__ float weno_side_scaled(float dm2, float dm1, float d0
 #define SCL_FP32_FN __forceinline__
 #endif
 
+// Packed FP32 (sm_100 f32x2 arithmetic): one instruction computes both lanes,
+// each lane rounded exactly as its scalar operation would be.
+#ifndef SCL_WENO_PACKED
+#define SCL_WENO_PACKED 1
+#endif
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);  // a + (-1)b: one rounding, = a - b
+}
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 pk2(float s) { return make_float2(s, s); }
+
+// weno_side_scaled for both sides at once: lane x is side 1 on
+// (dm2, dm1, d0, dp1) = (n0, n1, n2, n3), lane y side 2 on (n4, n3, n2, n1).
+// Side 2's im = -1 negates t1, t2, t3 exactly, hence the result exactly; the
+// squares do not see it, so it is applied to the result only (`post` holds
+// the scale factor with the sign of each side).
+__device__ __forceinline__ float2 weno_sides_packed(float2 dm2, float2 dm1, float2 d0, float2 dp1,
+                                                    float2 post) {
+  const float2 t1 = psub(dm2, dm1), t2 = psub(dm1, d0), t3 = psub(d0, dp1);
+  const float2 x1 = pfma(dm1, pk2(-3.0f), dm2);
+  const float2 x2 = padd(dm1, d0);
+  const float2 x3 = pfma(d0, pk2(-3.0f), dp1);  // -(3 d0 - dp1): only its square is used
+  float2 tt1 = pfma(pmul(t1, t1), pk2(13.0f), pmul(pmul(x1, x1), pk2(3.0f)));
+  float2 tt2 = pfma(pmul(t2, t2), pk2(13.0f), pmul(pmul(x2, x2), pk2(3.0f)));
+  float2 tt3 = pfma(pmul(t3, t3), pk2(13.0f), pmul(pmul(x3, x3), pk2(3.0f)));
+  tt1 = padd(pk2(EPS_SCALED), tt1);
+  tt2 = padd(pk2(EPS_SCALED), tt2);
+  tt3 = padd(pk2(EPS_SCALED), tt3);
+  tt1 = pmul(tt1, tt1);
+  tt2 = pmul(tt2, tt2);
+  tt3 = pmul(tt3, tt3);
+  float2 s1 = pmul(tt2, tt3);
+  const float2 s2 = pmul(pmul(pk2(6.0f), tt1), tt3);
+  float2 s3 = pmul(pmul(pk2(3.0f), tt1), tt2);
+  const float2 den = padd(padd(s1, s2), s3);
+  const float2 t0 = make_float2(rcp32(den.x), rcp32(den.y));
+  s1 = pmul(s1, t0);
+  s3 = pmul(s3, t0);
+  const float2 r = pfma(s1, psub(t2, t1), pmul(pfma(s3, pk2(0.5f), pk2(-0.25f)), psub(t3, t2)));
+  return pmul(pmul(r, pk2(1.0f / 3.0f)), post);
+}
+
 // Both sides of the scaled correction for one set of five jumps h[0..4].
 static __device__ SCL_FP32_FN void weno_pair_scaled(const float h[5], float& u1, float& u2) {
   float sc = fmaxf(fmaxf(fmaxf(fabsf(h[0]), fabsf(h[1])), fmaxf(fabsf(h[2]), fabsf(h[3]))),
                    fabsf(h[4]));
-  if (!(sc > 0.0f) || !(sc < 3.0e38f)) {  // all-zero stencil (or non-finite)
+  // all-zero stencil, or non-finite / beyond 8e37 (where the reciprocal
+  // would be subnormal; FP32 states cannot carry such jumps: their squares overflow)
+  if (!(sc > 0.0f) || !(sc < 8.0e37f)) {
     u1 = (sc == 0.0f) ? 0.0f : sc;
     u2 = u1;
     return;
   }
-  float inv = __frcp_rn(sc);
+  float inv = rcp32(sc);
+#if SCL_WENO_PACKED
+  const float2 iv = pk2(inv);
+  const float2 n04 = pmul(make_float2(h[0], h[4]), iv);
+  const float2 n13 = pmul(make_float2(h[1], h[3]), iv);
+  const float n2 = h[2] * inv;
+  const float2 u = weno_sides_packed(n04, n13, pk2(n2), make_float2(n13.y, n13.x), make_float2(sc, -sc));
+  u1 = u.x;
+  u2 = u.y;
+#else
   float n0 = h[0] * inv, n1 = h[1] * inv, n2 = h[2] * inv, n3 = h[3] * inv, n4 = h[4] * inv;
   u1 = weno_side_scaled(n0, n1, n2, n3, 1.0f) * sc;
   u2 = weno_side_scaled(n4, n3, n2, n1, -1.0f) * sc;
+#endif
 }
 
 // ---------------------------------------------------------------------------
