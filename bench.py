@@ -239,7 +239,7 @@ def workloads():
                     nstep=5, cells=n * n, stages=3, bytes_cell_stage=8.0 / 3.0 * 3 * 8,
                     desc="2-D shallow water g=1, radial dam break h=2 in r<0.5 else 1 + N(0,1e-3), "
                          "4096x4096 periodic on [-2.5,2.5]^2, Roe rpn2 + tfluct, char-wise WENO5, SSPRK3, "
-                         "cfl 0.45/0.5", traffic_key=None)
+                         "cfl 0.45/0.5", traffic_key="k_stage2d_sw_charwise_mixed")
 
     def c5():
         n = 1024
@@ -559,13 +559,15 @@ def run_gpu_batch(args, rank, world, local_rank):
 
     clocks = Clocks(local_rank)
     out = {}
-    for precision in (args.precision if args.precision != "mixed" else "fp32", "fp64"):
+    head = args.precision if args.precision != "mixed" else "fp32"
+    forms = [head] + (["mixed"] if head == "fp32" else []) + ["fp64"]
+    for precision in forms:
         b = S.Batch(ps, mx, dx, precision=precision)
         for _ in range(args.warmup):
             b.set_q(qs)
             b.sharpclaw(0.0, C4_TEND, dt0, cfl_max, cfl_des)
         barrier()
-        tot_ms, tot_cells = 0.0, 0
+        tot_ms, tot_cells, tot_launch = 0.0, 0, 0
         with clocks:
             for _ in range(args.steps):
                 b.set_q(qs)
@@ -574,13 +576,13 @@ def run_gpu_batch(args, rank, world, local_rank):
                 res, ms = b.sharpclaw(0.0, C4_TEND, dt0, cfl_max, cfl_des)
                 tot_ms += ms
                 tot_cells += cell_stages(res)
+                tot_launch += b.launches()
         barrier()
         # instances the scheme cannot advance (a non-finite state: WENO5 is not
         # positivity preserving near vacuum) are flagged, not trapped
         failed = {int(k): r["info"] for k, r in enumerate(res) if r["info"] != 0}
         out[precision] = dict(batch=b, ms=max_over_ranks(tot_ms), cells=tot_cells, res=res, tune=b.tuning(),
-                              failed=failed)
-    head = args.precision if args.precision != "mixed" else "fp32"
+                              failed=failed, launches=tot_launch)
     value = world * out[head]["cells"] / (out[head]["ms"] / 1000.0)
     value64_batched = world * out["fp64"]["cells"] / (out["fp64"]["ms"] / 1000.0)
 
@@ -598,12 +600,25 @@ def run_gpu_batch(args, rank, world, local_rank):
             one_cells += int(mx[k]) * 3 * (r["steps_taken"] - r["rejected"])
     value64_one = one_cells / (one_ms / 1000.0)
 
-    # accuracy of the headline form against the FP64 batch at the window's end
-    got = out[head]["batch"].get_q()
+    # accuracy of the FP32-arithmetic forms against the FP64 batch at the
+    # window's end: per instance the largest relative L1 over the components
     ref = out["fp64"]["batch"].get_q()
-    bad = set(out[head]["failed"]) | set(out["fp64"]["failed"])
-    rel_l1 = max(float(np.abs(g[m, 3:-3] - f[m, 3:-3]).sum() / np.abs(f[m, 3:-3]).sum())
-                 for k, (g, f) in enumerate(zip(got, ref)) if k not in bad for m in range(3))
+
+    def rel_l1_of(form):
+        got = out[form]["batch"].get_q()
+        bad = set(out[form]["failed"]) | set(out["fp64"]["failed"])
+        e = [max(float(np.abs(g[m, 3:-3] - f[m, 3:-3]).sum() / np.abs(f[m, 3:-3]).sum()) for m in range(3))
+             for k, (g, f) in enumerate(zip(got, ref)) if k not in bad]
+        return float(np.max(e)), float(np.median(e))
+
+    rel_l1, rel_l1_med = rel_l1_of(head)
+    mixed = None
+    if "mixed" in out and head != "mixed":
+        mx_max, mx_med = rel_l1_of("mixed")
+        vmix = world * out["mixed"]["cells"] / (out["mixed"]["ms"] / 1000.0)
+        mixed = {"value": vmix, "unit": UNIT, "rel_l1_vs_fp64_max_over_instances": mx_max,
+                 "rel_l1_vs_fp64_median": mx_med, "failed_instances": out["mixed"]["failed"],
+                 "dtype": "f32 (f64 state/accumulation)"}
 
     # end to end through the public API: H2D of every instance, the run, D2H
     bh = out[head]["batch"]
@@ -644,12 +659,14 @@ def run_gpu_batch(args, rank, world, local_rank):
                 "fp64_batched": {"value": value64_batched, "unit": UNIT},
                 "fp64_one_at_a_time": {"value": value64_one, "unit": UNIT, "sample_instances": len(sample),
                                        "speedup_of_headline": value / value64_one},
+                "mixed_batched": mixed,
                 "accuracy": {"rel_l1_vs_fp64_batch_max_over_instances": rel_l1,
+                             "rel_l1_vs_fp64_batch_median": rel_l1_med,
                              "failed_instances": {"headline": out[head]["failed"], "fp64": out["fp64"]["failed"]}},
                 "cpu_baseline": None,
                 "e2e": {"value": world * e2e_cells / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(flat_np.nbytes),
                         "d2h_bytes_per_step": int(flat_np.nbytes), "ms_per_step": 1000.0 * e2e_s / args.steps},
-                "gpu_launches": None,
+                "gpu_launches": out[head]["launches"],
                 "clocks": ck}
         print(json.dumps(line), flush=True)
     for v in out.values():

@@ -217,6 +217,10 @@ int scl_batch_run(scl_batch* b, const scl_run* run, const double* dt_initial, sc
  * size and the trial time of each variant (2 entries). */
 int scl_batch_tuning(scl_batch* b, int* variant, int* threads, int* grid, float* trial_ms);
 
+/* Kernel launches (begin, stages, end of every captured step) of the last
+ * scl_batch_run, autotuning trials excluded. */
+long long scl_batch_launches(scl_batch* b);
+
 /* Stream of the handle (cudaStream_t as void*), for callers that overlap work. */
 void* scl_stream(scl_handle* h);
 

@@ -344,6 +344,10 @@ class Batch:
         out = [{k: getattr(r, k) for k, _ in C.scl_result._fields_} for r in res]
         return out, ms.value
 
+    def launches(self) -> int:
+        """Kernel launches of the last sharpclaw() call."""
+        return int(C.lib().scl_batch_launches(self._h))
+
     def tuning(self):
         v, nt, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         tm = (ctypes.c_float * 2)()

@@ -138,6 +138,7 @@ struct scl_batch {
   BatchLaunchers L[NBATCH_VARIANTS];
   int nvariants = 0, variant = -1, grid[NBATCH_VARIANTS] = {0, 0};
   float tune_ms[NBATCH_VARIANTS] = {0, 0};
+  long long last_launches = 0;   // kernel launches of the last scl_batch_run's replays
   StageDesc sd[MAXSTAGES];
   int nstages = 0, final_role = ROLE_A;
   cudaGraphExec_t graph = nullptr;
@@ -489,8 +490,10 @@ int scl_batch_run(scl_batch* b, const scl_run* run, const double* dt_initial, sc
   const long max_replays = (long)maxn / K + 2;
   BCK(cudaEventRecord(b->ev0, b->stream));
   b->h_nact[0] = b->h_nact[1] = 1;
+  long replays = 0;
   for (long r = 0; r < max_replays; ++r) {
     BCK(cudaGraphLaunch(b->graph, b->stream));
+    ++replays;
     BCK(cudaMemcpyAsync(&b->h_nact[r & 1], b->d_nact, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
     BCK(cudaEventRecord(b->evq[r & 1], b->stream));
     if (r > 0) {
@@ -501,6 +504,7 @@ int scl_batch_run(scl_batch* b, const scl_run* run, const double* dt_initial, sc
   BCK(cudaEventRecord(b->ev1, b->stream));
   BCK(cudaEventSynchronize(b->ev1));
   if (ms) BCK(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+  b->last_launches = (long long)replays * K * (b->nstages + 2);
   rc = download_batch_ctl(b);
   if (rc) return rc;
   for (int k = 0; k < b->ninst; ++k) {
@@ -524,6 +528,8 @@ int scl_batch_run(scl_batch* b, const scl_run* run, const double* dt_initial, sc
   }
   return SCL_OK;
 }
+
+long long scl_batch_launches(scl_batch* b) { return b ? b->last_launches : 0; }
 
 int scl_batch_tuning(scl_batch* b, int* variant, int* threads, int* grid, float* trial_ms) {
   if (!b) return bfail(SCL_E_INVALID, "null argument");

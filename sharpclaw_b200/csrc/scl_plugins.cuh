@@ -252,21 +252,47 @@ struct PShallow2D {
   static constexpr int MEQN = 3, MWAVES = 3, MAUX = 0, NDIM = 2;
   static constexpr bool HAS_TFLUCT = true;
 
+  // Roe averages of rpn2sw.f:80-88: normal and tangential velocity u, v (mu,
+  // mv the normal / tangential momentum), celerity a, and ha = 0.5/a.
+  template <class R>
+  __device__ static void roe(const Phys& ph, int mu, int mv, const R* L, const R* Rt, R& u, R& v, R& a,
+                             R& ha) {
+#if SCL_FAST_ROE
+    if constexpr (sizeof(R) == 4) {
+      // FP32 form with reciprocal square roots: sqrt(h) = h*w, m/sqrt(h) = m*w
+      // for w = 1/sqrt(h), and 0.5/a = 0.5/sqrt(g*hbar)
+      const float wl = rsqrtf(L[0]), wr = rsqrtf(Rt[0]);
+      const float inv = rcp32(L[0] * wl + Rt[0] * wr);
+      u = (L[mu] * wl + Rt[mu] * wr) * inv;
+      v = (L[mv] * wl + Rt[mv] * wr) * inv;
+      const float gh = (float)ph.grav * ((L[0] + Rt[0]) * 0.50f);
+      const float ia = rsqrtf(gh);
+      a = gh * ia;
+      ha = 0.50f * ia;
+      return;
+    }
+#endif
+    const R g = (R)ph.grav;
+    R h = (L[0] + Rt[0]) * (R)0.50;
+    R hsqrtl = sqrt(L[0]);
+    R hsqrtr = sqrt(Rt[0]);
+    R hsq2 = hsqrtl + hsqrtr;
+    u = (L[mu] / hsqrtl + Rt[mu] / hsqrtr) / hsq2;
+    v = (L[mv] / hsqrtl + Rt[mv] / hsqrtr) / hsq2;
+    a = sqrt(g * h);
+    ha = (R)0.50 / a;
+  }
+
   template <class R>
   __device__ static void solve(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl,
                                R* s, R* amdq, R* apdq) {
     const R g = (R)ph.grav;
     const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
-    R h = (L[0] + Rt[0]) * (R)0.50;                                       // rpn2sw.f:80-88
-    R hsqrtl = sqrt(L[0]);
-    R hsqrtr = sqrt(Rt[0]);
-    R hsq2 = hsqrtl + hsqrtr;
-    R u = (L[mu] / hsqrtl + Rt[mu] / hsqrtr) / hsq2;
-    R v = (L[mv] / hsqrtl + Rt[mv] / hsqrtr) / hsq2;
-    R a = sqrt(g * h);
-    R a1 = ((u + a) * dl[0] - dl[mu]) * ((R)0.50 / a);                   // :98-100
+    R u, v, a, ha;
+    roe(ph, mu, mv, L, Rt, u, v, a, ha);                                    // rpn2sw.f:80-88
+    R a1 = ((u + a) * dl[0] - dl[mu]) * ha;                                 // :98-100
     R a2 = -(v * dl[0]) + dl[mv];
-    R a3 = (-((u - a) * dl[0]) + dl[mu]) * ((R)0.50 / a);
+    R a3 = (-((u - a) * dl[0]) + dl[mu]) * ha;
     R w[3][3];
     w[0][0] = a1; w[0][mu] = a1 * (u - a); w[0][mv] = a1 * v;
     w[1][0] = (R)0; w[1][mu] = (R)0;       w[1][mv] = a2;
@@ -344,16 +370,9 @@ struct PShallow2D {
   template <class R>
   __device__ static void evec(const Phys& ph, int ixy, const R* qm, const R* q0, const R*,
                               const R*, R evl[3][3], R evr[3][3]) {
-    const R g = (R)ph.grav;
     const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
-    R h = (qm[0] + q0[0]) * (R)0.50;
-    R hsqrtl = sqrt(qm[0]);
-    R hsqrtr = sqrt(q0[0]);
-    R hsq2 = hsqrtl + hsqrtr;
-    R u = (qm[mu] / hsqrtl + q0[mu] / hsqrtr) / hsq2;
-    R v = (qm[mv] / hsqrtl + q0[mv] / hsqrtr) / hsq2;
-    R a = sqrt(g * h);
-    R ha = (R)0.50 / a;
+    R u, v, a, ha;
+    roe(ph, mu, mv, qm, q0, u, v, a, ha);
     evr[0][0] = (R)1;  evr[mu][0] = u - a; evr[mv][0] = v;
     evr[0][1] = (R)0;  evr[mu][1] = (R)0;  evr[mv][1] = (R)1;
     evr[0][2] = (R)1;  evr[mu][2] = u + a; evr[mv][2] = v;
