@@ -189,6 +189,35 @@ def run_reference(args, rank, world):
     return 0
 
 
+def max_over_ranks(x, world, device):
+    """Largest x over all ranks (an all-reduce, so every rank receives it)."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world, device):
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def job_rate(units, seconds, world, device):
+    """Whole-job throughput: the units every rank processed, summed, over the
+    slowest rank's time.  Returns (rate, slowest time).  Every rank must call
+    it, in the same order as the other collectives."""
+    tmax = max_over_ranks(seconds, world, device)
+    return sum_over_ranks(units, world, device) / tmax, tmax
+
+
 def shu_osher_params(S, mx, dx):
     return S.ClawParams(rp=S.RP_EULER, mx=mx, dx=dx, xlower=-5.0, gamma=GAMMA, mthbc=(1, 1),
                         char_decomp=2, tfluct_solver=0, time_integrator=4)
@@ -296,13 +325,6 @@ def run_gpu(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     def timed_steps(s):
         return s.time_steps(nstep, W["dt0"], cfl_max, cfl_des, tend=W["tend"], dt_variable=W["dt_variable"])
 
@@ -329,13 +351,15 @@ def run_gpu(args, rank, world, local_rank):
                 taken += res["steps_taken"] - res["rejected"]
                 rejected += res["rejected"]
         barrier()
-        return s, max_over_ranks(total_ms), res, taken, rejected
+        return s, total_ms, res, taken, rejected
 
     clocks = Clocks(local_rank)
     s_mix, ms_mix, res_mix, taken_mix, rej_mix = device_run(args.precision, clocks)
-    value = world * W["cells"] * W["stages"] * taken_mix / (ms_mix / 1000.0)
+    value, s_max = job_rate(W["cells"] * W["stages"] * taken_mix, ms_mix / 1000.0, world, dev)
+    ms_mix = 1000.0 * s_max
     s_64, ms_64, res_64, taken_64, rej_64 = device_run("fp64", clocks)
-    value64 = world * W["cells"] * W["stages"] * taken_64 / (ms_64 / 1000.0)
+    value64, s_max = job_rate(W["cells"] * W["stages"] * taken_64, ms_64 / 1000.0, world, dev)
+    ms_64 = 1000.0 * s_max
 
     # the fused stage kernels alone (roofline): the stage launches of one step
     peak, peak_kind = measured_peaks()
@@ -381,8 +405,8 @@ def run_gpu(args, rank, world, local_rank):
             r = e2e_step()
             e2e_taken += r["steps_taken"] - r["rejected"]
         barrier()
-        e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e = world * W["cells"] * W["stages"] * e2e_taken / e2e_s
+        e2e_local = time.perf_counter() - t0
+    e2e, e2e_s = job_rate(W["cells"] * W["stages"] * e2e_taken, e2e_local, world, dev)
     nbytes = q0.nbytes
 
     # accuracy: the headline form against plain FP64 after 20 fixed-dt steps
@@ -479,7 +503,7 @@ def c5_adjoint(S, ps, q0, aux0, dt, nsteps=200, ckpt=20):
             torch.cuda.synchronize()
             t2 = time.perf_counter()
             grads[precision] = g
-            out[precision] = {"forward_s": t1 - t0, "backward_s": t2 - t1, "J": float(J)}
+            out[precision] = {"forward_s": t1 - t0, "backward_s": t2 - t1, "J": float(J.detach())}
             if precision == "fp64":
                 xc = (np.arange(n) + 0.5) / n
                 X, Y = np.meshgrid(xc, xc, indexing="xy")
@@ -547,13 +571,6 @@ def run_gpu_batch(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     def cell_stages(res):
         return sum(int(mx[k]) * 3 * (r["steps_taken"] - r["rejected"]) for k, r in enumerate(res))
 
@@ -581,10 +598,11 @@ def run_gpu_batch(args, rank, world, local_rank):
         # instances the scheme cannot advance (a non-finite state: WENO5 is not
         # positivity preserving near vacuum) are flagged, not trapped
         failed = {int(k): r["info"] for k, r in enumerate(res) if r["info"] != 0}
-        out[precision] = dict(batch=b, ms=max_over_ranks(tot_ms), cells=tot_cells, res=res, tune=b.tuning(),
+        rate, s_max = job_rate(tot_cells, tot_ms / 1000.0, world, dev)
+        out[precision] = dict(batch=b, ms=1000.0 * s_max, cells=tot_cells, rate=rate, res=res, tune=b.tuning(),
                               failed=failed, launches=tot_launch)
-    value = world * out[head]["cells"] / (out[head]["ms"] / 1000.0)
-    value64_batched = world * out["fp64"]["cells"] / (out["fp64"]["ms"] / 1000.0)
+    value = out[head]["rate"]
+    value64_batched = out["fp64"]["rate"]
 
     # plain FP64 path with the instances run one at a time (a seeded sample of 48)
     rng = np.random.default_rng(44)
@@ -615,7 +633,7 @@ def run_gpu_batch(args, rank, world, local_rank):
     mixed = None
     if "mixed" in out and head != "mixed":
         mx_max, mx_med = rel_l1_of("mixed")
-        vmix = world * out["mixed"]["cells"] / (out["mixed"]["ms"] / 1000.0)
+        vmix = out["mixed"]["rate"]
         mixed = {"value": vmix, "unit": UNIT, "rel_l1_vs_fp64_max_over_instances": mx_max,
                  "rel_l1_vs_fp64_median": mx_med, "failed_instances": out["mixed"]["failed"],
                  "dtype": "f32 (f64 state/accumulation)"}
@@ -637,7 +655,7 @@ def run_gpu_batch(args, rank, world, local_rank):
             C.check(C.lib().scl_batch_get_q(bh._h, outbuf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "get_q")
             e2e_cells += cell_stages(res)
         barrier()
-        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        e2e_rate, e2e_s = job_rate(e2e_cells, time.perf_counter() - t0, world, dev)
     peak, peak_kind = measured_peaks()
     byts = 8.0 / 3.0 * 3 * (4 if head == "fp32" else 8)
     gbs = byts * out[head]["cells"] / (out[head]["ms"] / 1000.0) / 1e9
@@ -664,7 +682,7 @@ def run_gpu_batch(args, rank, world, local_rank):
                              "rel_l1_vs_fp64_batch_median": rel_l1_med,
                              "failed_instances": {"headline": out[head]["failed"], "fp64": out["fp64"]["failed"]}},
                 "cpu_baseline": None,
-                "e2e": {"value": world * e2e_cells / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(flat_np.nbytes),
+                "e2e": {"value": e2e_rate, "unit": UNIT, "h2d_bytes_per_step": int(flat_np.nbytes),
                         "d2h_bytes_per_step": int(flat_np.nbytes), "ms_per_step": 1000.0 * e2e_s / args.steps},
                 "gpu_launches": out[head]["launches"],
                 "clocks": ck}
