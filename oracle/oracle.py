@@ -170,6 +170,19 @@ def weno5(q: np.ndarray):
     return ql, qr
 
 
+def weno5_wave(q: np.ndarray, wave: np.ndarray):
+    """reconstruct.f90 weno5_wave on one line; q shape (meqn, mx2), wave shape
+    (mwaves, meqn, mx2) as returned by rp() on the cell averages."""
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    wave = np.ascontiguousarray(wave, dtype=np.float64)
+    meqn, mx2 = q.shape
+    ql = np.zeros_like(q)
+    qr = np.zeros_like(q)
+    _check(lib().ocl_weno5_wave(mx2, meqn, wave.shape[0], _ptr(q), _ptr(wave), _ptr(ql), _ptr(qr)),
+           "weno5_wave")
+    return ql, qr
+
+
 def evec(p: Params, q: np.ndarray, aux=None, ixy=1):
     """Plugin evec on one line; returns (evl, evr) shaped (meqn, meqn, mx2):
     evl[m-1, p-1, i] = evl(i,p,m) and evr[p-1, m-1, i] = evr(i,m,p)."""

@@ -210,6 +210,73 @@ int ocl_weno5(int mx2, int meqn, const double *q, double *ql, double *qr) {
   return 0;
 }
 
+/* reconstruct.f90:350-428.  wave(i,m,mw) from the rp pass on the cell
+   averages.  The reference loops i = 2..mx2 (:368) and reads wave(i-2..i+2);
+   those indices hold waves written by that rp pass (2..mx2) only for
+   4 <= i <= mx2-2, i.e. exactly the interfaces 1..mx+1 that the update
+   uses; the others (ghost interfaces, reading unset workspace there) are
+   left at zero here. */
+int ocl_weno5_wave(int mx2, int meqn, int mwaves, const double *q, const double *wave,
+                   double *ql, double *qr) {
+  const double floor14 = (double)1.0e-14f;   /* :413, a REAL(4) literal */
+#define W(k, m, mw) R3(wave, k, m, mw)
+  for (int i = 4; i <= mx2 - 2; ++i) {
+    for (int m = 1; m <= meqn; ++m) {                                         /* :370-374 */
+      R2(qr, i - 1, m) = (((-R2(q, i - 2, m)) + 7.0 * (R2(q, i - 1, m) + R2(q, i, m))) - R2(q, i + 1, m)) / 12.0;
+      R2(ql, i, m) = R2(qr, i - 1, m);
+    }
+    for (int mw = 1; mw <= mwaves; ++mw) {
+      double u[2], wnorm2 = 0.0;
+      for (int m1 = 1; m1 <= 2; ++m1) {
+        const int im = (m1 == 1) ? 1 : -1;
+        const int ione = im, inone = -im, intwo = -2 * im;
+        const double dim = (double)im;
+        wnorm2 = W(i, 1, mw) * W(i, 1, mw);                                   /* :383-392 */
+        double theta1 = W(i + intwo, 1, mw) * W(i, 1, mw);
+        double theta2 = W(i + inone, 1, mw) * W(i, 1, mw);
+        double theta3 = W(i + ione, 1, mw) * W(i, 1, mw);
+        for (int m = 2; m <= meqn; ++m) {
+          wnorm2 = wnorm2 + W(i, m, mw) * W(i, m, mw);
+          theta1 = theta1 + W(i + intwo, m, mw) * W(i, m, mw);
+          theta2 = theta2 + W(i + inone, m, mw) * W(i, m, mw);
+          theta3 = theta3 + W(i + ione, m, mw) * W(i, m, mw);
+        }
+        double t1 = dim * (theta1 - theta2);                                  /* :394-411 */
+        double t2 = dim * (theta2 - wnorm2);
+        double t3 = dim * (wnorm2 - theta3);
+        double x1 = theta1 - 3.0 * theta2;
+        double x2 = theta2 + wnorm2;
+        double x3 = 3.0 * wnorm2 - theta3;
+        double tt1 = 13.0 * (t1 * t1) + 3.0 * (x1 * x1);
+        double tt2 = 13.0 * (t2 * t2) + 3.0 * (x2 * x2);
+        double tt3 = 13.0 * (t3 * t3) + 3.0 * (x3 * x3);
+        tt1 = (EPWENO + tt1) * (EPWENO + tt1);
+        tt2 = (EPWENO + tt2) * (EPWENO + tt2);
+        tt3 = (EPWENO + tt3) * (EPWENO + tt3);
+        double s1 = tt2 * tt3;
+        double s2 = (6.0 * tt1) * tt3;
+        double s3 = (3.0 * tt1) * tt2;
+        double t0 = 1.0 / ((s1 + s2) + s3);
+        s1 = s1 * t0;
+        s3 = s3 * t0;
+        if (wnorm2 > floor14) {                                               /* :413-419 */
+          u[m1 - 1] = ((s1 * (t2 - t1)) + ((0.5 * s3 - 0.25) * (t3 - t2))) / 3.0;
+          wnorm2 = 1.0 / wnorm2;
+        } else {
+          u[m1 - 1] = 0.0;
+          wnorm2 = 0.0;
+        }
+      }
+      for (int m = 1; m <= meqn; ++m) {                                       /* :421-424 */
+        R2(qr, i - 1, m) = R2(qr, i - 1, m) + (u[0] * W(i, m, mw)) * wnorm2;
+        R2(ql, i, m) = R2(ql, i, m) + (u[1] * W(i, m, mw)) * wnorm2;
+      }
+    }
+  }
+#undef W
+  return 0;
+}
+
 /* reconstruct.f90:146-241 */
 int ocl_weno5_char(int mx2, int meqn, const double *q, const double *evl,
                    const double *evr, double *ql, double *qr) {
@@ -751,6 +818,10 @@ int ocl_flux1(const ocl_params *p, const double *q1d, double *dq1d, const double
 
   switch (p->char_decomp) {                                                   /* :92-116 */
     case 0: rc = ocl_weno5(mx2, meqn, q1d, ql, qr); break;
+    case 1:                                                                   /* :97-101 */
+      rc = ocl_rp(p, ixy, mx, q1d, q1d, aux1d, aux1d, wave, s, amdq, apdq);
+      if (!rc) rc = ocl_weno5_wave(mx2, meqn, mwaves, q1d, wave, ql, qr);
+      break;
     case 2:
       rc = ocl_evec(p, ixy, mx, q1d, aux1d, aux1d, evl, evr);
       if (!rc) rc = ocl_weno5_char(mx2, meqn, q1d, evl, evr, ql, qr);

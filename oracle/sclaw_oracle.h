@@ -71,6 +71,10 @@ int ocl_bc(const ocl_params *p, double *q);
 /* reconstruct.f90 weno5 / weno5_char on one line of mx2 = mx+2*mbc cells.
  * q, ql, qr: (mx2, meqn); evl, evr: (mx2, meqn, meqn). */
 int ocl_weno5(int mx2, int meqn, const double *q, double *ql, double *qr);
+/* reconstruct.f90:350-428; wave(mx2, meqn, mwaves) from the rp pass on the
+   cell averages (flux1.f90:99-100) */
+int ocl_weno5_wave(int mx2, int meqn, int mwaves, const double *q, const double *wave,
+                   double *ql, double *qr);
 int ocl_weno5_char(int mx2, int meqn, const double *q, const double *evl,
                    const double *evr, double *ql, double *qr);
 

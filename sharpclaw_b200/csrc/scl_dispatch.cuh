@@ -75,18 +75,22 @@ bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
   if (ndim == 1) {
     if (variant != 0) return false;
     if (cd == 0 && tf == 0) L->stage = &launch1d<P, 0, 0>;
+    if (cd == 1 && tf == 0) L->stage = &launch1d<P, 1, 0>;
     if (cd == 2 && tf == 0) L->stage = &launch1d<P, 2, 0>;
     if constexpr (P::HAS_TFLUCT) {
       if (cd == 0 && tf == 1) L->stage = &launch1d<P, 0, 1>;
+      if (cd == 1 && tf == 1) L->stage = &launch1d<P, 1, 1>;
       if (cd == 2 && tf == 1) L->stage = &launch1d<P, 2, 1>;
     }
     return L->stage != nullptr;
   }
   if constexpr (P::NDIM == 2) {
     if (cd == 0 && tf == 0) return fill2d<P, 0, 0>(variant, L);
+    if (cd == 1 && tf == 0) return fill2d<P, 1, 0>(variant, L);
     if (cd == 2 && tf == 0) return fill2d<P, 2, 0>(variant, L);
     if constexpr (P::HAS_TFLUCT) {
       if (cd == 0 && tf == 1) return fill2d<P, 0, 1>(variant, L);
+      if (cd == 1 && tf == 1) return fill2d<P, 1, 1>(variant, L);
       if (cd == 2 && tf == 1) return fill2d<P, 2, 1>(variant, L);
     }
   }
@@ -125,9 +129,11 @@ bool pick_batch_nt(int variant, BatchLaunchers* L) {
 template <class P>
 bool pick_batch(int cd, int tf, int variant, BatchLaunchers* L) {
   if (cd == 0 && tf == 0) return pick_batch_nt<P, 0, 0>(variant, L);
+  if (cd == 1 && tf == 0) return pick_batch_nt<P, 1, 0>(variant, L);
   if (cd == 2 && tf == 0) return pick_batch_nt<P, 2, 0>(variant, L);
   if constexpr (P::HAS_TFLUCT) {
     if (cd == 0 && tf == 1) return pick_batch_nt<P, 0, 1>(variant, L);
+    if (cd == 1 && tf == 1) return pick_batch_nt<P, 1, 1>(variant, L);
     if (cd == 2 && tf == 1) return pick_batch_nt<P, 2, 1>(variant, L);
   }
   return false;

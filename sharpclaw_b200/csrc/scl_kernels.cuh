@@ -117,12 +117,13 @@ __device__ SCL_FP32_FN void evec_f32(const Phys& ph, int ixy, const float* qm, c
 
 // ---------------------------------------------------------------------------
 // One interface c-1/2 (between cells c-1 and c) of a line: reconstruction,
-// Riemann solve and the CFL contribution.  `qs(k, m)` returns cell c-3+k.
+// Riemann solve and the CFL contribution.  `qs(k, m)` returns cell c-3+k,
+// `as(k, j)` aux field j of that cell (read only by the wave-based form).
 // Results: xl = qr(c-1), xr = ql(c) (states in the exact form, offsets from
 // q(c-1)/q(c) in the offset form), fluctuations amdq(c), apdq(c).
 // ---------------------------------------------------------------------------
-template <class P, int CD, int PREC, class QS>
-__device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs,
+template <class P, int CD, int PREC, class QS, class AS>
+__device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs, AS as,
                                                 const typename Prec<PREC>::R* auxm,
                                                 const typename Prec<PREC>::R* aux0,
                                                 typename Prec<PREC>::R xl[P::MEQN],
@@ -131,7 +132,7 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs,
                                                 typename Prec<PREC>::R apdq[P::MEQN],
                                                 typename Prec<PREC>::R s[P::MWAVES]) {
   using R = typename Prec<PREC>::R;
-  constexpr int M = P::MEQN;
+  constexpr int M = P::MEQN, MW = P::MWAVES, MA = P::MAUX;
   if constexpr (Prec<PREC>::EXACT) {
     double q[6][M];
 #pragma unroll
@@ -142,6 +143,21 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs,
       double evl[M][M], evr[M][M];
       P::template evec<double>(ph, ixy, q[2], q[3], auxm, aux0, evl, evr);
       weno5_char_exact<M>(q, evl, evr, xl, xr);
+    } else if constexpr (CD == 1) {
+      // waves of the cell-average Riemann problems at c-2 .. c+2 (flux1.f90:99-100)
+      double w[5][MW][M], ak[6][MA > 0 ? MA : 1];
+#pragma unroll
+      for (int k = 0; k < 6; ++k)
+#pragma unroll
+        for (int j = 0; j < MA; ++j) ak[k][j] = (double)as(k, j);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        double dk[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) dk[m] = q[k + 1][m] - q[k][m];
+        P::template waves<double>(ph, ixy, q[k], q[k + 1], dk, ak[k], ak[k + 1], w[k]);
+      }
+      weno5_wave_exact<M, MW>(q, w, xl, xr);
     } else {
       weno5_exact<M>(q, xl, xr);
     }
@@ -161,6 +177,18 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs,
       for (int m = 0; m < M; ++m) { qm[m] = (float)qs(2, m); q0[m] = (float)qs(3, m); }
       evec_f32<P>(ph, ixy, qm, q0, auxm, aux0, evl, evr);
       weno5_char_offset<M>(d, evl, evr, xl, xr);
+    } else if constexpr (CD == 1) {
+      float qf[6][M], w[5][MW][M], ak[6][MA > 0 ? MA : 1];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+#pragma unroll
+        for (int m = 0; m < M; ++m) qf[k][m] = (float)qs(k, m);
+#pragma unroll
+        for (int j = 0; j < MA; ++j) ak[k][j] = (float)as(k, j);
+      }
+#pragma unroll
+      for (int k = 0; k < 5; ++k) P::template waves<float>(ph, ixy, qf[k], qf[k + 1], d[k], ak[k], ak[k + 1], w[k]);
+      weno5_wave_offset<M, MW>(d, w, xl, xr);
     } else {
       weno5_offset<M>(d, xl, xr);
     }
@@ -281,8 +309,9 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
         aux0[k] = load_aux<S>(L.aux, (long)k * L.plane + c + 2);
       }
       auto qs = [&](int k, int m) -> S { return sm.sq[m][tid + k]; };
+      auto as = [&](int k, int j) -> R { return load_aux<S>(L.aux, (long)j * L.plane + c - 1 + k); };
       R xl[M], xr[M], am[M], ap[M], s[MW];
-      solve_interface<P, CD, PREC>(ph, L.ixy, qs, auxm, aux0, xl, xr, am, ap, s);
+      solve_interface<P, CD, PREC>(ph, L.ixy, qs, as, auxm, aux0, xl, xr, am, ap, s);
 #pragma unroll
       for (int m = 0; m < M; ++m) {
         sm.rec[0][m][tid] = xl[m]; sm.rec[1][m][tid] = xr[m];
@@ -468,8 +497,10 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
       return isx ? sq[(m * T::WY + by) * T::WX + (bx - 3 + k)]
                  : sq[(m * T::WY + (by - 3 + k)) * T::WX + bx];
     };
+    const long st = isx ? 1 : a.pitch;
+    auto as = [&](int k, int j) -> R { return load_aux<S>(a.aux, (long)j * a.plane + o0 + (long)(k - 3) * st); };
     R xl[M], xr[M], am[M], ap[M], s[MW];
-    solve_interface<P, CD, PREC>(a.ph, ixy, qs, auxm, aux0, xl, xr, am, ap, s);
+    solve_interface<P, CD, PREC>(a.ph, ixy, qs, as, auxm, aux0, xl, xr, am, ap, s);
     R* rec = isx ? recx : recy;
     const int n = isx ? T::NXI : T::NYI;
     const int slot = isx ? w : w - T::NXI;
@@ -612,8 +643,9 @@ __global__ void __launch_bounds__(128) k_ghost_cfl2d(StageArgs a) {
       aux0[k] = load_aux<S>(a.aux, (long)k * a.plane + o0);
     }
     auto qs = [&](int k, int m) -> S { return qin[(long)m * a.plane + o0 + (long)(k - 3) * st]; };
+    auto as = [&](int k, int j) -> R { return load_aux<S>(a.aux, (long)j * a.plane + o0 + (long)(k - 3) * st); };
     R xl[M], xr[M], am[M], ap[M], s[MW];
-    solve_interface<P, CD, PREC>(a.ph, ixy, qs, auxm, aux0, xl, xr, am, ap, s);
+    solve_interface<P, CD, PREC>(a.ph, ixy, qs, as, auxm, aux0, xl, xr, am, ap, s);
     double d_c = dt / (ixy == 1 ? a.dx : a.dy), d_m = d_c;
     if (a.mcapa > 0) {
       const S* cap = static_cast<const S*>(a.aux) + (long)(a.mcapa - 1) * a.plane;

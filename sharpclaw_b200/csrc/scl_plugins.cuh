@@ -41,6 +41,12 @@ struct PAdvection {
     amdq[0] = rmin(u, (R)0) * dl[0];
     apdq[0] = rmax(u, (R)0) * dl[0];
   }
+  // waves of rp1.f:35 (the jump itself), for the wave-based reconstruction
+  template <class R>
+  __device__ static void waves(const Phys&, int, const R*, const R*, const R* dl, const R*, const R*,
+                               R w[1][1]) {
+    w[0][0] = dl[0];
+  }
   template <class R>
   __device__ static void tfluct(const Phys& ph, int, const R*, const R*, const R* dl, const R*,
                                 R* adq) {
@@ -119,11 +125,12 @@ struct PEuler {
     return PLUS ? m / rho + c : m / rho - c;
   }
 
+  // Roe averages and the three waves of rp1eu.f:44-86, w[wave][component].
   template <class R>
-  __device__ static void rp(const Phys& ph, int, const R* L, const R* Rt, const R* dl, const R*,
-                            const R*, R* s, R* amdq, R* apdq) {
+  __device__ static void wave_set(const Phys& ph, const R* L, const R* Rt, const R* dl, R& u, R& enth,
+                                  R& a, R w[3][3]) {
     const R g1 = (R)ph.gamma1;
-    R u, enth, a, ia = (R)0;
+    R ia = (R)0;
     roe(ph, L, Rt, u, enth, a, &ia);                              // rp1eu.f:44-55
     R a2, a3;
 #if SCL_FAST_ROE
@@ -137,10 +144,23 @@ struct PEuler {
       a3 = ((dl[1] + (a - u) * dl[0]) - a * a2) / ((R)2 * a);                   // :67
     }
     R a1 = (dl[0] - a2) - a3;                                                   // :68
-    R w[3][3];  // w[wave][component]
     w[0][0] = a1; w[0][1] = a1 * (u - a); w[0][2] = a1 * (enth - u * a);
     w[1][0] = a2; w[1][1] = a2 * u;       w[1][2] = (a2 * (R)0.5) * (u * u);
     w[2][0] = a3; w[2][1] = a3 * (u + a); w[2][2] = a3 * (enth + u * a);
+  }
+
+  template <class R>
+  __device__ static void waves(const Phys& ph, int, const R* L, const R* Rt, const R* dl, const R*,
+                               const R*, R w[3][3]) {
+    R u, enth, a;
+    wave_set(ph, L, Rt, dl, u, enth, a, w);
+  }
+
+  template <class R>
+  __device__ static void rp(const Phys& ph, int, const R* L, const R* Rt, const R* dl, const R*,
+                            const R*, R* s, R* amdq, R* apdq) {
+    R u, enth, a, w[3][3];  // w[wave][component]
+    wave_set(ph, L, Rt, dl, u, enth, a, w);
     s[0] = u - a; s[1] = u; s[2] = u + a;
     if (!ph.efix) {                                                            // :100-111
 #pragma unroll
@@ -283,20 +303,35 @@ struct PShallow2D {
     ha = (R)0.50 / a;
   }
 
+  // Roe averages and the three waves of rpn2sw.f:80-118 along ixy.
   template <class R>
-  __device__ static void solve(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl,
-                               R* s, R* amdq, R* apdq) {
-    const R g = (R)ph.grav;
+  __device__ static void wave_set(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl, R& u,
+                                  R& a, R w[3][3]) {
     const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
-    R u, v, a, ha;
+    R v, ha;
     roe(ph, mu, mv, L, Rt, u, v, a, ha);                                    // rpn2sw.f:80-88
     R a1 = ((u + a) * dl[0] - dl[mu]) * ha;                                 // :98-100
     R a2 = -(v * dl[0]) + dl[mv];
     R a3 = (-((u - a) * dl[0]) + dl[mu]) * ha;
-    R w[3][3];
     w[0][0] = a1; w[0][mu] = a1 * (u - a); w[0][mv] = a1 * v;
     w[1][0] = (R)0; w[1][mu] = (R)0;       w[1][mv] = a2;
     w[2][0] = a3; w[2][mu] = a3 * (u + a); w[2][mv] = a3 * v;
+  }
+
+  template <class R>
+  __device__ static void waves(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl, const R*,
+                               const R*, R w[3][3]) {
+    R u, a;
+    wave_set(ph, ixy, L, Rt, dl, u, a, w);
+  }
+
+  template <class R>
+  __device__ static void solve(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl,
+                               R* s, R* amdq, R* apdq) {
+    const R g = (R)ph.grav;
+    const int mu = (ixy == 1) ? 1 : 2;
+    R u, a, w[3][3];
+    wave_set(ph, ixy, L, Rt, dl, u, a, w);
     s[0] = u - a; s[1] = u; s[2] = u + a;
     if (!ph.efix) {                                                         // :132-143
 #pragma unroll
@@ -393,26 +428,32 @@ struct PAcoustics {
   static constexpr int MEQN = NEQ, MWAVES = 2, MAUX = 2, NDIM = (NEQ == 2 ? 1 : 2);
   static constexpr bool HAS_TFLUCT = true;
   template <class R>
-  __device__ static void rp(const Phys&, int ixy, const R*, const R*, const R* dl, const R* auxl,
+  __device__ static void rp(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl, const R* auxl,
                             const R* auxr, R* s, R* amdq, R* apdq) {
     // auxl = aux of the left cell (auxr(i-1,:)), auxr = aux of the right cell (auxl(i,:))
+    R w[2][NEQ];
+    waves(ph, ixy, L, Rt, dl, auxl, auxr, w);
+    s[0] = -auxl[1];
+    s[1] = auxr[1];
+#pragma unroll
+    for (int m = 0; m < NEQ; ++m) {
+      amdq[m] = s[0] * w[0][m];
+      apdq[m] = s[1] * w[1][m];
+    }
+  }
+  // the two waves of rp1acv.f:49-60 (zero tangential component in 2-D)
+  template <class R>
+  __device__ static void waves(const Phys&, int ixy, const R*, const R*, const R* dl, const R* auxl,
+                               const R* auxr, R w[2][NEQ]) {
     const int mu = (ixy == 1) ? 1 : 2;
     R zi = auxr[0];
     R zim = auxl[0];
     R a1 = ((-dl[0]) + zi * dl[mu]) / (zim + zi);
     R a2 = (dl[0] + zim * dl[mu]) / (zim + zi);
-    s[0] = -auxl[1];
-    s[1] = auxr[1];
-    R w1[NEQ], w2[NEQ];
 #pragma unroll
-    for (int m = 0; m < NEQ; ++m) { w1[m] = (R)0; w2[m] = (R)0; }
-    w1[0] = -(a1 * zim); w1[mu] = a1;
-    w2[0] = a2 * zi;     w2[mu] = a2;
-#pragma unroll
-    for (int m = 0; m < NEQ; ++m) {
-      amdq[m] = s[0] * w1[m];
-      apdq[m] = s[1] * w2[m];
-    }
+    for (int m = 0; m < NEQ; ++m) { w[0][m] = (R)0; w[1][m] = (R)0; }
+    w[0][0] = -(a1 * zim); w[0][mu] = a1;
+    w[1][0] = a2 * zi;     w[1][mu] = a2;
   }
   template <class R>
   __device__ static void tfluct(const Phys&, int ixy, const R*, const R*, const R* dl,

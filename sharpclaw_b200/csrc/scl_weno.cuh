@@ -259,4 +259,80 @@ __device__ __forceinline__ void weno5_char_offset(const float d[5][M], const flo
   }
 }
 
+// ---------------------------------------------------------------------------
+// Wave-based form (char_decomp = 1, reconstruct.f90:350-428).  The waves W of
+// the cell-average Riemann problems at the five interfaces c-2 .. c+2 around
+// interface c-1/2 are projected on the wave of the same family at c-1/2:
+// theta_k = W(c-2+k) . W(c), theta_2 = |W(c)|^2.  The WENO algebra runs on the
+// thetas (side 1 on theta_0..3, side 2 on theta_4..1 with im = -1, exactly the
+// weno_side arguments), and the correction is u * W(c) / |W(c)|^2, dropped
+// when |W(c)|^2 <= 1e-14.  w[k][mw][m] = component m of wave mw at c-2+k.
+// ---------------------------------------------------------------------------
+// reconstruct.f90:413 `if (wnorm2.gt.1.e-14)` (a REAL(4) literal)
+__device__ __forceinline__ double wave_floor() { return (double)1.0e-14f; }
+
+template <int M, int MW>
+__device__ __forceinline__ void weno5_wave_exact(const double q[6][M], const double w[5][MW][M],
+                                                 double qrl[M], double qlr[M]) {
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    double c = ((-q[1][m]) + 7.0 * (q[2][m] + q[3][m])) - q[4][m];   // :371-372
+    qrl[m] = c / 12.0;
+    qlr[m] = qrl[m];
+  }
+#pragma unroll
+  for (int mw = 0; mw < MW; ++mw) {
+    double th[5];                                                     // :383-392
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      th[k] = w[k][mw][0] * w[2][mw][0];
+#pragma unroll
+      for (int m = 1; m < M; ++m) th[k] = th[k] + w[k][mw][m] * w[2][mw][m];
+    }
+    double u1 = 0.0, u2 = 0.0, winv = 0.0;                            // :413-419
+    if (th[2] > wave_floor()) {
+      u1 = weno_side(th[0], th[1], th[2], th[3], 1.0);
+      u2 = weno_side(th[4], th[3], th[2], th[1], -1.0);
+      winv = 1.0 / th[2];
+    }
+#pragma unroll
+    for (int m = 0; m < M; ++m) {                                     // :421-424
+      qrl[m] = qrl[m] + (u1 * w[2][mw][m]) * winv;
+      qlr[m] = qlr[m] + (u2 * w[2][mw][m]) * winv;
+    }
+  }
+}
+
+// FP32 offset form of weno5_wave_exact: jumps d (as weno5_offset), waves from
+// FP32 cell values and jumps; the thetas go through the scaled pair.
+template <int M, int MW>
+__device__ __forceinline__ void weno5_wave_offset(const float d[5][M], const float w[5][MW][M], float er[M],
+                                                  float el[M]) {
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    er[m] = (d[1][m] + 6.0f * d[2][m] - d[3][m]) * (1.0f / 12.0f);
+    el[m] = (d[1][m] - 6.0f * d[2][m] - d[3][m]) * (1.0f / 12.0f);
+  }
+#pragma unroll
+  for (int mw = 0; mw < MW; ++mw) {
+    float th[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      th[k] = w[k][mw][0] * w[2][mw][0];
+#pragma unroll
+      for (int m = 1; m < M; ++m) th[k] = th[k] + w[k][mw][m] * w[2][mw][m];
+    }
+    if (th[2] > 1.0e-14f) {
+      float u1, u2;
+      weno_pair_scaled(th, u1, u2);
+      const float winv = rcp32(th[2]);
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        er[m] = er[m] + (u1 * w[2][mw][m]) * winv;
+        el[m] = el[m] + (u2 * w[2][mw][m]) * winv;
+      }
+    }
+  }
+}
+
 }  // namespace scl
