@@ -62,7 +62,7 @@ typedef struct scl_params {
   int mx, my;           /* nx(1), nx(2)                                            */
   int meqn, mwaves, mbc, maux, mcapa;
   int lim_type;         /* 2 = WENO (reconstruct.f90)                              */
-  int char_decomp;      /* 0 weno5, 1 wave-based weno5_wave, 2 char-wise weno5_char */
+  int char_decomp;      /* 0 weno5, 1 weno5_wave, 2 weno5_char, 3 weno5_trans      */
   int tfluct_solver;    /* 1 tfluct plugin, 0 swap + second rp (flux1.f90:136-188) */
   int mthbc[4];         /* 1 extrapolation, 2 periodic, 3 solid wall               */
   double dx, dy, xlower, ylower;

@@ -277,6 +277,77 @@ int ocl_weno5_wave(int mx2, int meqn, int mwaves, const double *q, const double 
   return 0;
 }
 
+/* reconstruct.f90:244-347 (transmission-based).  The reference fills hh
+   only for i = mbc+1..mx2-2 (:282) but reconstructs i = mbc..mx2-mbc+1
+   (:300); i = mbc reads unset workspace and feeds only the ghost interface
+   2-mbc, so the loops here run over i = mbc+1..mx2-2, the interfaces 1..mx+1. */
+int ocl_weno5_trans(int mx2, int meqn, const double *q, const double *evl,
+                    const double *evr, double *ql, double *qr) {
+  const int mbc = 3;
+  double *dq = (double *)calloc((size_t)mx2 * meqn, sizeof(double));
+  double *gg = (double *)calloc((size_t)mx2 * meqn, sizeof(double));
+  double *hh = (double *)calloc((size_t)mx2 * 5, sizeof(double));
+  double *u = (double *)calloc((size_t)mx2 * meqn * 2, sizeof(double));
+  if (!dq || !gg || !hh || !u) { free(dq); free(gg); free(hh); free(u); return -3; }
+#define HH(k, o) hh[((k) - 1) + (long)((o) + 2) * mx2]
+#define U3(k, mw, s) u[((k) - 1) + (long)((mw) - 1) * mx2 + (long)((s) - 1) * mx2 * meqn]
+  for (int m = 1; m <= meqn; ++m)
+    for (int i = 2; i <= mx2; ++i) R2(dq, i, m) = R2(q, i, m) - R2(q, i - 1, m);  /* :264-269 */
+  for (int mw = 1; mw <= meqn; ++mw)                                               /* :273-280 */
+    for (int i = 2; i <= mx2; ++i) {
+      double g = 0.0;
+      for (int m = 1; m <= meqn; ++m) g = g + R3(evl, i, mw, m) * R2(dq, i, m);
+      R2(gg, i, mw) = g;
+    }
+  for (int mw = 1; mw <= meqn; ++mw) {
+    for (int m1 = -2; m1 <= 2; ++m1)                                                /* :286-294 */
+      for (int i = mbc + 1; i <= mx2 - 2; ++i) {
+        double h = 0.0;
+        for (int m = 1; m <= meqn; ++m)
+          h = h + (R3(evl, i, mw, m) * R2(gg, i + m1, mw)) * R3(evr, i + m1, m, mw);
+        HH(i, m1) = h;
+      }
+    for (int m1 = 1; m1 <= 2; ++m1) {                                               /* :298-327 */
+      const int im = (m1 == 1) ? 1 : -1;
+      const int ione = im, inone = -im, intwo = -2 * im;
+      const double dim = (double)im;
+      for (int i = mbc + 1; i <= mx2 - 2; ++i) {
+        double t1 = dim * (HH(i, intwo) - HH(i, inone));
+        double t2 = dim * (HH(i, inone) - HH(i, 0));
+        double t3 = dim * (HH(i, 0) - HH(i, ione));
+        double x1 = HH(i, intwo) - 3.0 * HH(i, inone);
+        double x2 = HH(i, inone) + HH(i, 0);
+        double x3 = 3.0 * HH(i, 0) - HH(i, ione);
+        double tt1 = 13.0 * (t1 * t1) + 3.0 * (x1 * x1);
+        double tt2 = 13.0 * (t2 * t2) + 3.0 * (x2 * x2);
+        double tt3 = 13.0 * (t3 * t3) + 3.0 * (x3 * x3);
+        tt1 = (EPWENO + tt1) * (EPWENO + tt1);
+        tt2 = (EPWENO + tt2) * (EPWENO + tt2);
+        tt3 = (EPWENO + tt3) * (EPWENO + tt3);
+        double s1 = tt2 * tt3;
+        double s2 = (6.0 * tt1) * tt3;
+        double s3 = (3.0 * tt1) * tt2;
+        double t0 = 1.0 / ((s1 + s2) + s3);
+        s1 = s1 * t0;
+        s3 = s3 * t0;
+        U3(i, mw, m1) = ((s1 * (t2 - t1)) + ((0.5 * s3 - 0.25) * (t3 - t2))) / 3.0;
+      }
+    }
+  }
+  for (int m1 = 1; m1 <= 2; ++m1)                                                   /* :332-342 */
+    for (int m = 1; m <= meqn; ++m)
+      for (int i = mbc + 1; i <= mx2 - 2; ++i) {
+        double uh = (((-R2(q, i - 2, m)) + 7.0 * (R2(q, i - 1, m) + R2(q, i, m))) - R2(q, i + 1, m)) / 12.0;
+        for (int mw = 1; mw <= meqn; ++mw) uh = uh + R3(evr, i, m, mw) * U3(i, mw, m1);
+        if (m1 == 1) R2(qr, i - 1, m) = uh;                                        /* :344-345 */
+        else R2(ql, i, m) = uh;
+      }
+#undef HH
+#undef U3
+  free(dq); free(gg); free(hh); free(u);
+  return 0;
+}
+
 /* reconstruct.f90:146-241 */
 int ocl_weno5_char(int mx2, int meqn, const double *q, const double *evl,
                    const double *evr, double *ql, double *qr) {
@@ -825,6 +896,10 @@ int ocl_flux1(const ocl_params *p, const double *q1d, double *dq1d, const double
     case 2:
       rc = ocl_evec(p, ixy, mx, q1d, aux1d, aux1d, evl, evr);
       if (!rc) rc = ocl_weno5_char(mx2, meqn, q1d, evl, evr, ql, qr);
+      break;
+    case 3:                                                                   /* :107-110 */
+      rc = ocl_evec(p, ixy, mx, q1d, aux1d, aux1d, evl, evr);
+      if (!rc) rc = ocl_weno5_trans(mx2, meqn, q1d, evl, evr, ql, qr);
       break;
     default: rc = -5;
   }

@@ -75,6 +75,9 @@ int ocl_weno5(int mx2, int meqn, const double *q, double *ql, double *qr);
    cell averages (flux1.f90:99-100) */
 int ocl_weno5_wave(int mx2, int meqn, int mwaves, const double *q, const double *wave,
                    double *ql, double *qr);
+/* reconstruct.f90:244-347 (transmission-based, char_decomp = 3) */
+int ocl_weno5_trans(int mx2, int meqn, const double *q, const double *evl,
+                    const double *evr, double *ql, double *qr);
 int ocl_weno5_char(int mx2, int meqn, const double *q, const double *evl,
                    const double *evr, double *ql, double *qr);
 

@@ -415,8 +415,8 @@ int validate(const scl_params* p) {
   if (p->mbc != 3) return fail(SCL_E_INVALID, "WENO5 requires mbc = 3 (reconstruct.f90:85)");
   if (p->mx < 3 || (p->ndim == 2 && p->my < 3)) return fail(SCL_E_INVALID, "need at least 3 cells per direction");
   if (p->lim_type != 2) return fail(SCL_E_UNSUPPORTED, "only lim_type = 2 (WENO) is built");
-  if (p->char_decomp < 0 || p->char_decomp > 2)
-    return fail(SCL_E_UNSUPPORTED, "char_decomp must be 0, 1 or 2 (3, weno5_trans, is not built)");
+  if (p->char_decomp < 0 || p->char_decomp > 3)
+    return fail(SCL_E_UNSUPPORTED, "char_decomp must be 0, 1, 2 or 3");
   if (p->tfluct_solver != 0 && p->tfluct_solver != 1) return fail(SCL_E_INVALID, "tfluct_solver must be 0 or 1");
   for (int k = 0; k < 2 * p->ndim; ++k)
     if (p->mthbc[k] < 1 || p->mthbc[k] > 3)

@@ -77,10 +77,12 @@ bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
     if (cd == 0 && tf == 0) L->stage = &launch1d<P, 0, 0>;
     if (cd == 1 && tf == 0) L->stage = &launch1d<P, 1, 0>;
     if (cd == 2 && tf == 0) L->stage = &launch1d<P, 2, 0>;
+    if (cd == 3 && tf == 0) L->stage = &launch1d<P, 3, 0>;
     if constexpr (P::HAS_TFLUCT) {
       if (cd == 0 && tf == 1) L->stage = &launch1d<P, 0, 1>;
       if (cd == 1 && tf == 1) L->stage = &launch1d<P, 1, 1>;
       if (cd == 2 && tf == 1) L->stage = &launch1d<P, 2, 1>;
+      if (cd == 3 && tf == 1) L->stage = &launch1d<P, 3, 1>;
     }
     return L->stage != nullptr;
   }
@@ -88,10 +90,12 @@ bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
     if (cd == 0 && tf == 0) return fill2d<P, 0, 0>(variant, L);
     if (cd == 1 && tf == 0) return fill2d<P, 1, 0>(variant, L);
     if (cd == 2 && tf == 0) return fill2d<P, 2, 0>(variant, L);
+    if (cd == 3 && tf == 0) return fill2d<P, 3, 0>(variant, L);
     if constexpr (P::HAS_TFLUCT) {
       if (cd == 0 && tf == 1) return fill2d<P, 0, 1>(variant, L);
       if (cd == 1 && tf == 1) return fill2d<P, 1, 1>(variant, L);
       if (cd == 2 && tf == 1) return fill2d<P, 2, 1>(variant, L);
+      if (cd == 3 && tf == 1) return fill2d<P, 3, 1>(variant, L);
     }
   }
   return false;
@@ -131,10 +135,12 @@ bool pick_batch(int cd, int tf, int variant, BatchLaunchers* L) {
   if (cd == 0 && tf == 0) return pick_batch_nt<P, 0, 0>(variant, L);
   if (cd == 1 && tf == 0) return pick_batch_nt<P, 1, 0>(variant, L);
   if (cd == 2 && tf == 0) return pick_batch_nt<P, 2, 0>(variant, L);
+  if (cd == 3 && tf == 0) return pick_batch_nt<P, 3, 0>(variant, L);
   if constexpr (P::HAS_TFLUCT) {
     if (cd == 0 && tf == 1) return pick_batch_nt<P, 0, 1>(variant, L);
     if (cd == 1 && tf == 1) return pick_batch_nt<P, 1, 1>(variant, L);
     if (cd == 2 && tf == 1) return pick_batch_nt<P, 2, 1>(variant, L);
+    if (cd == 3 && tf == 1) return pick_batch_nt<P, 3, 1>(variant, L);
   }
   return false;
 }

@@ -158,6 +158,33 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs, 
         P::template waves<double>(ph, ixy, q[k], q[k + 1], dk, ak[k], ak[k + 1], w[k]);
       }
       weno5_wave_exact<M, MW>(q, w, xl, xr);
+    } else if constexpr (CD == 3) {
+      // eigenvectors of the five interfaces c-2 .. c+2 (flux1.f90:108-110)
+      double evlc[M][M], evrc[M][M], h[5][M];
+      auto axk = [&](int k, double* out) {
+#pragma unroll
+        for (int j = 0; j < MA; ++j) out[j] = (double)as(k, j);
+      };
+      double a2[MA > 0 ? MA : 1], a3[MA > 0 ? MA : 1];
+      axk(2, a2);
+      axk(3, a3);
+      P::template evec<double>(ph, ixy, q[2], q[3], a2, a3, evlc, evrc);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        double dk[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) dk[m] = q[k + 1][m] - q[k][m];
+        if (k == 2) {
+          trans_project<double, M>(evlc, evrc, dk, evlc, h[k]);
+        } else {
+          double evl[M][M], evr[M][M], ak0[MA > 0 ? MA : 1], ak1[MA > 0 ? MA : 1];
+          axk(k, ak0);
+          axk(k + 1, ak1);
+          P::template evec<double>(ph, ixy, q[k], q[k + 1], ak0, ak1, evl, evr);
+          trans_project<double, M>(evl, evr, dk, evlc, h[k]);
+        }
+      }
+      weno5_trans_exact<M>(q, h, evrc, xl, xr);
     } else {
       weno5_exact<M>(q, xl, xr);
     }
@@ -189,6 +216,27 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs, 
 #pragma unroll
       for (int k = 0; k < 5; ++k) P::template waves<float>(ph, ixy, qf[k], qf[k + 1], d[k], ak[k], ak[k + 1], w[k]);
       weno5_wave_offset<M, MW>(d, w, xl, xr);
+    } else if constexpr (CD == 3) {
+      float qf[6][M], ak[6][MA > 0 ? MA : 1], evlc[M][M], evrc[M][M], h[5][M];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+#pragma unroll
+        for (int m = 0; m < M; ++m) qf[k][m] = (float)qs(k, m);
+#pragma unroll
+        for (int j = 0; j < MA; ++j) ak[k][j] = (float)as(k, j);
+      }
+      evec_f32<P>(ph, ixy, qf[2], qf[3], ak[2], ak[3], evlc, evrc);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        if (k == 2) {
+          trans_project<float, M>(evlc, evrc, d[k], evlc, h[k]);
+        } else {
+          float evl[M][M], evr[M][M];
+          evec_f32<P>(ph, ixy, qf[k], qf[k + 1], ak[k], ak[k + 1], evl, evr);
+          trans_project<float, M>(evl, evr, d[k], evlc, h[k]);
+        }
+      }
+      weno5_trans_offset<M>(d, h, evrc, xl, xr);
     } else {
       weno5_offset<M>(d, xl, xr);
     }

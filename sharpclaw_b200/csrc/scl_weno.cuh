@@ -335,4 +335,77 @@ __device__ __forceinline__ void weno5_wave_offset(const float d[5][M], const flo
   }
 }
 
+// ---------------------------------------------------------------------------
+// Transmission-based form (char_decomp = 3, reconstruct.f90:244-347).  Each of
+// the five interfaces c-2+k (k = 0..4) around c-1/2 has its own eigenvectors;
+// its wave strengths gg = evl_k . dq_k, carried to physical space by evr_k,
+// are projected on the left eigenvectors of c-1/2 (h_k), the WENO algebra runs
+// on h per field, and the result returns through evr of c-1/2.
+// ---------------------------------------------------------------------------
+// h_k of one neighbour interface (reconstruct.f90:273-294 for one i+m1).
+template <class T, int M>
+__device__ __forceinline__ void trans_project(const T evlk[M][M], const T evrk[M][M], const T dk[M],
+                                              const T evlc[M][M], T hk[M]) {
+  T gg[M];
+#pragma unroll
+  for (int mw = 0; mw < M; ++mw) {
+    T g = (T)0;
+#pragma unroll
+    for (int m = 0; m < M; ++m) g = g + evlk[mw][m] * dk[m];
+    gg[mw] = g;
+  }
+#pragma unroll
+  for (int mw = 0; mw < M; ++mw) {
+    T h = (T)0;
+#pragma unroll
+    for (int m = 0; m < M; ++m) h = h + (evlc[mw][m] * gg[mw]) * evrk[m][mw];
+    hk[mw] = h;
+  }
+}
+
+// reconstruct.f90:298-345 from h[k][mw]; evrc = evr of c-1/2.
+template <int M>
+__device__ __forceinline__ void weno5_trans_exact(const double q[6][M], const double h[5][M],
+                                                  const double evrc[M][M], double qrl[M], double qlr[M]) {
+  double u1[M], u2[M];
+#pragma unroll
+  for (int mw = 0; mw < M; ++mw) {
+    u1[mw] = weno_side(h[0][mw], h[1][mw], h[2][mw], h[3][mw], 1.0);
+    u2[mw] = weno_side(h[4][mw], h[3][mw], h[2][mw], h[1][mw], -1.0);
+  }
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    double c = ((-q[1][m]) + 7.0 * (q[2][m] + q[3][m])) - q[4][m];
+    double a = c / 12.0, b = c / 12.0;
+#pragma unroll
+    for (int mw = 0; mw < M; ++mw) {
+      a = a + evrc[m][mw] * u1[mw];
+      b = b + evrc[m][mw] * u2[mw];
+    }
+    qrl[m] = a;
+    qlr[m] = b;
+  }
+}
+
+template <int M>
+__device__ __forceinline__ void weno5_trans_offset(const float d[5][M], const float h[5][M],
+                                                   const float evrc[M][M], float er[M], float el[M]) {
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    er[m] = (d[1][m] + 6.0f * d[2][m] - d[3][m]) * (1.0f / 12.0f);
+    el[m] = (d[1][m] - 6.0f * d[2][m] - d[3][m]) * (1.0f / 12.0f);
+  }
+#pragma unroll
+  for (int mw = 0; mw < M; ++mw) {
+    const float hh[5] = {h[0][mw], h[1][mw], h[2][mw], h[3][mw], h[4][mw]};
+    float u1, u2;
+    weno_pair_scaled(hh, u1, u2);
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      er[m] = er[m] + evrc[m][mw] * u1;
+      el[m] = el[m] + evrc[m][mw] * u2;
+    }
+  }
+}
+
 }  // namespace scl

@@ -40,7 +40,7 @@ def test_version_string():
     (dict(mbc=2), C.SCL_E_INVALID),
     (dict(mx=2), C.SCL_E_INVALID),
     (dict(lim_type=1), C.SCL_E_UNSUPPORTED),
-    (dict(char_decomp=3), C.SCL_E_UNSUPPORTED),   # weno5_trans is not built
+    (dict(char_decomp=4), C.SCL_E_UNSUPPORTED),
     (dict(mthbc=(0, 0)), C.SCL_E_INVALID),
     (dict(mthbc=(2, 1)), C.SCL_E_INVALID),
     (dict(time_integrator=5), C.SCL_E_INVALID),

@@ -39,6 +39,13 @@ STEP_CASES = [
     ("sw2d_wave_tf1", lambda: cases.radial_dam(n=33, char_decomp=1)),
     ("sw2d_wave_wall_tf0", lambda: cases.radial_dam(n=22, char_decomp=1, tfluct_solver=0, mthbc=(3, 3, 1, 1))),
     ("acoustics2d_wave", lambda: cases.acoustics2d(n=25, char_decomp=1, background=0.05)),
+    # transmission-based WENO5 (char_decomp = 3, reconstruct.f90:244-347)
+    ("advection_trans", lambda: cases.advection(mx=120, char_decomp=3)),
+    ("euler_trans_swap", lambda: cases.shu_osher(mx=230, char_decomp=3)),
+    ("euler_riemann_trans", lambda: cases.riemann(mx=170, char_decomp=3)),
+    ("acoustics1d_trans", lambda: cases.acoustics1d(mx=150, char_decomp=3)),
+    ("sw2d_trans_tf1", lambda: cases.radial_dam(n=29, char_decomp=3)),
+    ("acoustics2d_trans_tf0", lambda: cases.acoustics2d(n=21, char_decomp=3, tfluct_solver=0)),
 ]
 
 
@@ -117,6 +124,7 @@ RUN_CASES = [
     ("euler_reject_retake", lambda: cases.shu_osher(mx=120), 3, dict(tend=0.05, dt_initial=0.05, cfl_max=0.9, cfl_desired=0.8)),
     ("sw2d_wave_ssp33", lambda: cases.radial_dam(n=26, char_decomp=1), 3, dict(tend=0.3, dt_initial=0.01, cfl_max=0.9, cfl_desired=0.8)),
     ("euler_sod_wave_ssp104", lambda: cases.riemann(mx=200, char_decomp=1), 4, dict(tend=0.1, dt_initial=0.001, cfl_max=2.5, cfl_desired=2.45)),
+    ("euler_trans_ssp104", lambda: cases.shu_osher(mx=300, char_decomp=3), 4, dict(tend=0.05, dt_initial=0.001, cfl_max=2.5, cfl_desired=2.45)),
 ]
 
 
@@ -168,7 +176,7 @@ def test_nonfinite_is_reported():
     assert r["status"] & S._capi.STATUS_NONFINITE
 
 
-@pytest.mark.parametrize("case", ["shu_osher_char", "sod_wave"])
+@pytest.mark.parametrize("case", ["shu_osher_char", "sod_wave", "shu_osher_trans"])
 @pytest.mark.parametrize("precision,tol", [("mixed", 2e-5), ("fp32", 2e-5)])
 def test_reduced_precision_error(precision, tol, case):
     """FP32 reconstruction/Riemann solves against the FP64 oracle: relative L1
@@ -178,6 +186,8 @@ def test_reduced_precision_error(precision, tol, case):
     algorithm does)."""
     if case == "shu_osher_char":
         po, ps, q, aux = cases.shu_osher(mx=400)
+    elif case == "shu_osher_trans":
+        po, ps, q, aux = cases.shu_osher(mx=400, char_decomp=3)
     else:
         po, ps, q, aux = cases.riemann(mx=400, char_decomp=1)
     ps.time_integrator = 4
