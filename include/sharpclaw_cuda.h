@@ -29,6 +29,7 @@ extern "C" {
 #define SCL_E_UNSUPPORTED (-3)  /* valid in the reference, not built here           */
 #define SCL_E_NONFINITE (-4)    /* NaN/Inf met in the CFL number                    */
 #define SCL_E_TIMEOUT (-5)      /* a bounded device wait ran out                    */
+#define SCL_E_IO (-6)           /* a frame file could not be written                */
 
 /* device status bits (scl_result.status) */
 #define SCL_STATUS_NONFINITE 1
@@ -148,6 +149,26 @@ int scl_time_stages(scl_handle* h, double dt, int reps, float* ms, long long* la
 /* Kernel launches per controller step (begin + stages + end, + 1 ghost-line
  * CFL kernel in 2-D). */
 int scl_kernels_per_step(scl_handle* h);
+
+/* Frame output in the reference's format (src/1d/out1.f90, src/2d/out2.f90):
+ * fort.qNNNN (interior cells, 4 values per record, e16.8 in 1-D and e26.16 in
+ * 2-D), fort.tNNNN, and with write_aux fort.aNNNN, in directory dir (NULL or
+ * "" = the working directory); NNNN = the last four digits of iframe.  Values
+ * below 1e-99 in magnitude are written as 0 (the reference also zeroes them in
+ * its state array; the state here is left as it is).
+ *
+ * scl_write_frame writes the handle's current state without stalling the
+ * device: it enqueues a copy into a pinned host buffer on the handle's stream
+ * and returns; a host thread formats and writes the files once the copy is
+ * done.  One frame is in flight per handle: the next scl_write_frame, and
+ * scl_wait_frames, wait for it and return its error, if any (SCL_E_IO). */
+int scl_write_frame(scl_handle* h, double t, int iframe, const char* dir, int write_aux);
+int scl_wait_frames(scl_handle* h);
+
+/* The same files from host arrays in the reference layout (synchronous; needs
+ * no GPU).  aux may be NULL when write_aux == 0 or maux == 0. */
+int scl_format_frame(const scl_params* p, const double* q, const double* aux, double t, int iframe,
+                     const char* dir, int write_aux);
 
 /* Tile shape of the fused 2-D stage kernel (no counterpart in the reference;
  * flux2.f90 sweeps whole lines).  Shapes: 0 = 16x7 cells on 128 threads,

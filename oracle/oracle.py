@@ -83,6 +83,9 @@ def lib():
         _lib.ocl_sharpclaw.argtypes = [P, ctypes.POINTER(Run), dp, dp, ctypes.POINTER(Result)]
         _lib.ocl_rp.argtypes = [P, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp, dp, dp, dp]
         _lib.ocl_evec.argtypes = [P, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp]
+        _lib.ocl_weno5_wave.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp]
+        _lib.ocl_output.argtypes = [P, dp, dp, ctypes.c_double, ctypes.c_int, ctypes.c_char_p,
+                                    ctypes.c_int]
     return _lib
 
 
@@ -212,3 +215,11 @@ def rp(p: Params, ql, qr, auxl=None, auxr=None, ixy=1):
     _check(lib().ocl_rp(ctypes.byref(p), ixy, mx, _ptr(ql), _ptr(qr), _ptr(al), _ptr(ar),
                         _ptr(wave), _ptr(s), _ptr(amdq), _ptr(apdq)), "rp")
     return wave, s, amdq, apdq
+
+
+def output(p: Params, q, aux, t: float, iframe: int, dir: str, outaux: bool):
+    """out1.f90 / out2.f90: writes fort.qNNNN, fort.tNNNN (and fort.aNNNN) in dir."""
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    a = None if aux is None else np.ascontiguousarray(aux, dtype=np.float64)
+    _check(lib().ocl_output(ctypes.byref(p), _ptr(q), _ptr(a), float(t), int(iframe), os.fsencode(dir),
+                            int(bool(outaux))), "output")

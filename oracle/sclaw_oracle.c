@@ -22,6 +22,7 @@
 #include "sclaw_oracle.h"
 
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -1153,5 +1154,99 @@ int ocl_sharpclaw(const ocl_params *p, const ocl_run *run, double *q, const doub
   res->steps_taken = steps;
   res->info = info;
   res->rejected = rejected;
+  return 0;
+}
+
+/* ======================================================================== */
+/* src/1d/out1.f90 and src/2d/out2.f90: frame files fort.qNNNN/tNNNN/aNNNN  */
+/* ======================================================================== */
+
+/* Fortran Ew.d: [-]0.<d digits>E+xx (or +xxx), right-justified in w */
+static void fmt_e(char *out, double v, int w, int d) {
+  char body[64], dig[40], raw[64];
+  int e = 0;
+  if (v != v) { snprintf(body, sizeof body, "NaN"); }
+  else if (isinf(v)) { snprintf(body, sizeof body, "%s", v < 0 ? "-Infinity" : "Infinity"); }
+  else {
+    if (v == 0.0) {
+      memset(dig, '0', (size_t)d); dig[d] = 0;
+    } else {
+      int k = 0;
+      snprintf(raw, sizeof raw, "%.*e", d - 1, fabs(v));
+      for (const char *c = raw; *c && *c != 'e'; ++c) if (*c >= '0' && *c <= '9') dig[k++] = *c;
+      dig[k] = 0;
+      e = atoi(strchr(raw, 'e') + 1) + 1;
+    }
+    int ae = e < 0 ? -e : e;
+    if (ae <= 99) snprintf(body, sizeof body, "%s0.%sE%c%02d", signbit(v) ? "-" : "", dig, e < 0 ? '-' : '+', ae);
+    else snprintf(body, sizeof body, "%s0.%s%c%03d", signbit(v) ? "-" : "", dig, e < 0 ? '-' : '+', ae);
+  }
+  int n = (int)strlen(body);
+  if (n > w) { memset(out, '*', (size_t)w); out[w] = 0; return; }
+  memset(out, ' ', (size_t)(w - n));
+  memcpy(out + (w - n), body, (size_t)n + 1);
+}
+
+static FILE *open_frame(const char *dir, char kind, int iframe) {
+  char name[16], path[4096];
+  int nstp = iframe;
+  strcpy(name, "fort.xxxxx");
+  name[5] = kind;                                   /* out1.f90:30-42 */
+  for (int ipos = 10; ipos >= 7; --ipos) { name[ipos - 1] = (char)('0' + nstp % 10); nstp /= 10; }
+  name[10] = 0;
+  if (dir && dir[0]) snprintf(path, sizeof path, "%s/%s", dir, name);
+  else snprintf(path, sizeof path, "%s", name);
+  return fopen(path, "w");
+}
+
+static void write_grid(FILE *f, const ocl_params *p, const double *a, int ncomp, int nblank1d) {
+  char b[64];
+  const int mbc = p->mbc, mx = p->mx, my = p->ndim == 2 ? p->my : 1;
+  const long ld = mx + 2 * mbc, plane = ld * (p->ndim == 2 ? my + 2 * mbc : 1);
+  fprintf(f, "%5d                 grid_number\n%5d                 AMR_level\n%5d                 mx\n", 1, 1, mx);
+  if (p->ndim == 2) {
+    fprintf(f, "%5d                 my\n", my);
+    fmt_e(b, p->xlower, 26, 16); fprintf(f, "%s    xlow\n", b);
+    fmt_e(b, p->ylower, 26, 16); fprintf(f, "%s    ylow\n", b);
+    fmt_e(b, p->dx, 26, 16); fprintf(f, "%s    dx\n", b);
+    fmt_e(b, p->dy, 26, 16); fprintf(f, "%s    dy\n\n", b);
+  } else {
+    fmt_e(b, p->xlower, 18, 8); fprintf(f, "%s    xlow\n", b);
+    fmt_e(b, p->dx, 18, 8); fprintf(f, "%s    dx\n\n", b);
+  }
+  const int w = p->ndim == 2 ? 26 : 16, d = p->ndim == 2 ? 16 : 8;
+  for (int j = 1; j <= my; ++j) {
+    for (int i = 1; i <= mx; ++i) {
+      for (int m = 1; m <= ncomp; ++m) {
+        long k = (i + mbc - 1) + (p->ndim == 2 ? (long)(j + mbc - 1) * ld : 0) + (long)(m - 1) * plane;
+        double v = a[k];
+        if (fabs(v) < 1e-99) v = 0.0;                 /* out1.f90:63-66 */
+        fmt_e(b, v, w, d);
+        fputs(b, f);
+        if (m % 4 == 0 || m == ncomp) fputc('\n', f);  /* format (4ew.d) */
+      }
+    }
+    if (p->ndim == 2) fputs("  \n", f);             /* out2.f90:68 */
+  }
+  for (int k = 0; k < (p->ndim == 2 ? 1 : nblank1d); ++k) fputs("  \n", f);
+}
+
+int ocl_output(const ocl_params *p, const double *q, const double *aux, double t, int iframe,
+               const char *dir, int outaux) {
+  FILE *fq = open_frame(dir, 'q', iframe), *ft = open_frame(dir, 't', iframe);
+  if (!fq || !ft) { if (fq) fclose(fq); if (ft) fclose(ft); return -6; }
+  write_grid(fq, p, q, p->meqn, 2);
+  if (outaux && p->maux > 0 && aux) {
+    FILE *fa = open_frame(dir, 'a', iframe);
+    if (!fa) { fclose(fq); fclose(ft); return -6; }
+    write_grid(fa, p, aux, p->maux, 1);
+    fclose(fa);
+  }
+  char b[64];
+  fmt_e(b, t, 26, 16);
+  fprintf(ft, "%s    time\n%5d                 meqn\n%5d                 ngrids\n%5d                 maux\n"
+              "%5d                 ndim\n\n\n", b, p->meqn, 1, p->maux, p->ndim);
+  fclose(fq);
+  fclose(ft);
   return 0;
 }

@@ -108,6 +108,11 @@ int ocl_rk_step(const ocl_params *p, int time_integrator, double *q, const doubl
 int ocl_sharpclaw(const ocl_params *p, const ocl_run *run, double *q, const double *aux,
                   ocl_result *res);
 
+/* src/1d/out1.f90, src/2d/out2.f90: fort.qNNNN, fort.tNNNN (and fort.aNNNN
+   with outaux) in directory dir */
+int ocl_output(const ocl_params *p, const double *q, const double *aux, double t, int iframe,
+               const char *dir, int outaux);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,6 +21,7 @@ All compute runs in the CUDA library; a missing library is an error.
 from __future__ import annotations
 
 import ctypes
+import os
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
@@ -238,6 +239,20 @@ class Solver:
     def kernels_per_step(self) -> int:
         return C.lib().scl_kernels_per_step(self._h)
 
+    def write_frame(self, t: float, iframe: int, dir: str | None = None, write_aux: bool | None = None):
+        """Write fort.qNNNN / fort.tNNNN (/ fort.aNNNN) of the current state in
+        the format of out1.f90 / out2.f90 without stalling the device; the
+        files are complete after wait_frames() (or the next write_frame).
+        write_aux defaults to the reference's choice: 1-D no, 2-D yes."""
+        if write_aux is None:
+            write_aux = self.params.ndim == 2
+        d = None if dir is None else os.fsencode(dir)
+        C.check(C.lib().scl_write_frame(self._h, float(t), int(iframe), d, int(bool(write_aux))),
+                "scl_write_frame")
+
+    def wait_frames(self):
+        C.check(C.lib().scl_wait_frames(self._h), "scl_wait_frames")
+
     TILE_SHAPES = ((16, 7, 128), (32, 7, 256), (16, 15, 256))  # (cells x, cells y, threads)
 
     def select_tiles(self, variant: int = -1):
@@ -263,6 +278,25 @@ def sharpclaw(params: ClawParams, q, aux=None, *, tstart: float, tend: float, dt
         s.set_q(q)
         res = s.sharpclaw(tstart, tend, dt_initial, cfl_max, cfl_desired, dt_max, max_steps, dt_variable)
         return s.get_q(), res
+
+
+def write_frame(params: ClawParams, q, aux=None, *, t: float, iframe: int, dir: str | None = None,
+                write_aux: bool | None = None):
+    """Frame files of out1.f90 / out2.f90 from host arrays (no GPU needed)."""
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    if q.shape != params.shape():
+        raise ValueError(f"q has shape {q.shape}, expected {params.shape()}")
+    if write_aux is None:
+        write_aux = params.ndim == 2
+    a = None
+    if write_aux and params.maux > 0:
+        if aux is None:
+            raise ValueError("write_aux needs aux")
+        a = np.ascontiguousarray(aux, dtype=np.float64)
+    cp = params.to_c(FP64)
+    d = None if dir is None else os.fsencode(dir)
+    C.check(C.lib().scl_format_frame(ctypes.byref(cp), _ptr(q), _ptr(a), float(t), int(iframe), d,
+                                     int(bool(write_aux))), "scl_format_frame")
 
 
 class Batch:

@@ -27,6 +27,7 @@ FAST32 = ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"]
 
 UNITS = {
     "scl_capi.cu": [],
+    "scl_frames.cu": [],
     "scl_noalloc.cu": [],
     "scl_batch.cu": [],
     "scl_adjoint.cu": ["--fmad=false"],

@@ -10,9 +10,11 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "scl_common.cuh"
+#include "scl_frames.h"
 #include "scl_launch.h"
 
 using namespace scl;
@@ -234,6 +236,13 @@ struct scl_handle {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t evq[2] = {nullptr, nullptr};
   double* adj = nullptr;       // adjoint work fields (5 x meqn planes), allocated on first use
+  // frame output: pinned copy of the state, the copy's event, the writer thread
+  double* fbuf = nullptr;
+  size_t fbuf_n = 0;
+  cudaEvent_t fev = nullptr;
+  std::thread fthread;
+  int frc = SCL_OK;
+  std::string ferr;
 };
 
 namespace {
@@ -514,6 +523,9 @@ int scl_create(const scl_params* p, scl_handle** out) {
 
 int scl_destroy(scl_handle* h) {
   if (!h) return SCL_OK;
+  if (h->fthread.joinable()) h->fthread.join();
+  if (h->fbuf) cudaFreeHost(h->fbuf);
+  if (h->fev) cudaEventDestroy(h->fev);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->graph) cudaGraphExecDestroy(h->graph);
   for (int r = 0; r < NROLES; ++r) if (h->buf[r]) cudaFree(h->buf[r]);
@@ -868,6 +880,75 @@ int scl_time_stages(scl_handle* h, double dt, int reps, float* ms, long long* la
 }
 
 int scl_kernels_per_step(scl_handle* h) { return h ? kernels_per_step(h) : 0; }
+
+int scl_wait_frames(scl_handle* h) {
+  if (!h) return fail(SCL_E_INVALID, "null handle");
+  if (h->fthread.joinable()) h->fthread.join();
+  const int rc = h->frc;
+  h->frc = SCL_OK;
+  if (rc) return fail(rc, h->ferr);
+  return SCL_OK;
+}
+
+int scl_write_frame(scl_handle* h, double t, int iframe, const char* dir, int write_aux) {
+  if (!h || iframe < 0) return fail(SCL_E_INVALID, "null handle or negative frame number");
+  int rc = scl_wait_frames(h);   // the pinned buffer holds one frame at a time
+  if (rc) return rc;
+  const scl_params& p = h->p;
+  const long plane_ref = h->ld * h->rows;
+  const bool aux_out = write_aux && p.maux > 0;
+  const size_t n = (size_t)plane_ref * (p.meqn + (aux_out ? p.maux : 0));
+  if (n > h->fbuf_n) {
+    if (h->fbuf) cudaFreeHost(h->fbuf);
+    h->fbuf = nullptr;
+    h->fbuf_n = 0;
+    CK(cudaMallocHost(&h->fbuf, n * sizeof(double)));
+    h->fbuf_n = n;
+  }
+  if (!h->fev) CK(cudaEventCreateWithFlags(&h->fev, cudaEventDisableTiming));
+  rc = download_field(h, h->fbuf, h->buf[h->hctl->role[ROLE_Q]], p.meqn, false);
+  if (rc) return rc;
+  const double* aq = nullptr;
+  if (aux_out) {
+    rc = download_field(h, h->fbuf + plane_ref * p.meqn, h->aux, p.maux, false);
+    if (rc) return rc;
+    aq = h->fbuf + plane_ref * p.meqn;
+  }
+  CK(cudaEventRecord(h->fev, h->stream));
+  FrameSpec f{p.ndim, p.mx, p.ndim == 2 ? p.my : 1, p.mbc, p.meqn, p.maux, p.xlower, p.ylower,
+              p.dx, p.dy, t, iframe, aux_out, dir ? std::string(dir) : std::string()};
+  const double* qq = h->fbuf;
+  h->fthread = std::thread([h, f, qq, aq]() {
+    cudaSetDevice(h->device);
+    const cudaError_t e = cudaEventSynchronize(h->fev);
+    if (e != cudaSuccess) {
+      h->frc = SCL_E_CUDA;
+      h->ferr = std::string("frame copy: ") + cudaGetErrorString(e);
+      return;
+    }
+    std::string err;
+    if (write_frame_files(f, qq, aq, &err)) {
+      h->frc = SCL_E_IO;
+      h->ferr = err;
+    }
+  });
+  return SCL_OK;
+}
+
+int scl_format_frame(const scl_params* p, const double* q, const double* aux, double t, int iframe,
+                     const char* dir, int write_aux) {
+  if (!p || !q || iframe < 0) return fail(SCL_E_INVALID, "null argument or negative frame number");
+  if ((p->ndim != 1 && p->ndim != 2) || p->mx < 1 || (p->ndim == 2 && p->my < 1) || p->mbc < 0 ||
+      p->meqn < 1 || p->maux < 0)
+    return fail(SCL_E_INVALID, "bad grid parameters");
+  const bool aux_out = write_aux && p->maux > 0;
+  if (aux_out && !aux) return fail(SCL_E_INVALID, "write_aux needs aux");
+  FrameSpec f{p->ndim, p->mx, p->ndim == 2 ? p->my : 1, p->mbc, p->meqn, p->maux, p->xlower, p->ylower,
+              p->dx, p->dy, t, iframe, aux_out, dir ? std::string(dir) : std::string()};
+  std::string err;
+  if (write_frame_files(f, q, aux_out ? aux : nullptr, &err)) return fail(SCL_E_IO, err);
+  return SCL_OK;
+}
 
 int scl_select_tiles(scl_handle* h, int variant) {
   if (!h) return fail(SCL_E_INVALID, "null handle");
