@@ -121,3 +121,15 @@ def acoustics2d(n=40, seed=5, char_decomp=0, tfluct_solver=1, mthbc=(2, 2, 2, 2)
     po = O.make_params(ndim=2, meqn=3, mwaves=2, maux=2, rp=O.RP_ACOUSTICS2D, **kw)
     ps = S.ClawParams(rp=S.RP_ACOUSTICS2D, **kw)
     return po, ps, q, aux
+
+
+def with_capacity(case, seed=11):
+    """Append a capacity field kappa in [0.7, 1.3] (seeded) to a case's aux and
+    point mcapa at it: dtdx = dt/(dx*kappa) as flux1.f90:57-58 computes it."""
+    po, ps, q, aux = case
+    kappa = 1.0 + 0.3 * np.random.default_rng(seed).uniform(-1.0, 1.0, q.shape[1:])
+    aux2 = kappa[None] if aux is None else np.concatenate([aux, kappa[None]])
+    m = aux2.shape[0]
+    po.maux, po.mcapa = m, m
+    ps.maux, ps.mcapa = m, m
+    return po, ps, q, np.ascontiguousarray(aux2)

@@ -46,6 +46,11 @@ STEP_CASES = [
     ("acoustics1d_trans", lambda: cases.acoustics1d(mx=150, char_decomp=3)),
     ("sw2d_trans_tf1", lambda: cases.radial_dam(n=29, char_decomp=3)),
     ("acoustics2d_trans_tf0", lambda: cases.acoustics2d(n=21, char_decomp=3, tfluct_solver=0)),
+    # capacity (mcapa > 0): dtdx = dt/(dx*kappa), flux1.f90:57-58
+    ("advection_capa", lambda: cases.with_capacity(cases.advection(mx=90))),
+    ("euler_capa_char", lambda: cases.with_capacity(cases.shu_osher(mx=150))),
+    ("acoustics1d_capa", lambda: cases.with_capacity(cases.acoustics1d(mx=120))),
+    ("sw2d_capa", lambda: cases.with_capacity(cases.radial_dam(n=19))),
 ]
 
 
@@ -125,6 +130,7 @@ RUN_CASES = [
     ("sw2d_wave_ssp33", lambda: cases.radial_dam(n=26, char_decomp=1), 3, dict(tend=0.3, dt_initial=0.01, cfl_max=0.9, cfl_desired=0.8)),
     ("euler_sod_wave_ssp104", lambda: cases.riemann(mx=200, char_decomp=1), 4, dict(tend=0.1, dt_initial=0.001, cfl_max=2.5, cfl_desired=2.45)),
     ("euler_trans_ssp104", lambda: cases.shu_osher(mx=300, char_decomp=3), 4, dict(tend=0.05, dt_initial=0.001, cfl_max=2.5, cfl_desired=2.45)),
+    ("sw2d_capa_ssp33", lambda: cases.with_capacity(cases.radial_dam(n=21)), 3, dict(tend=0.2, dt_initial=0.01, cfl_max=0.9, cfl_desired=0.8)),
 ]
 
 
