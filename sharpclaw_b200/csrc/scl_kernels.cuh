@@ -19,10 +19,12 @@ namespace scl {
 // contraction), SCL_MIXED (float reconstruction and Riemann solves on
 // double state), SCL_FP32 (float state).
 template <int PREC> struct Prec;
-template <> struct Prec<SCL_FP64> { using R = double; using S = double; using A = double; static constexpr bool EXACT = true; };
-template <> struct Prec<SCL_FP64_STRICT> { using R = double; using S = double; using A = double; static constexpr bool EXACT = true; };
-template <> struct Prec<SCL_MIXED> { using R = float; using S = double; using A = double; static constexpr bool EXACT = false; };
-template <> struct Prec<SCL_FP32> { using R = float; using S = float; using A = float; static constexpr bool EXACT = false; };
+// FD: the FP64 form divides through reciprocals (within a few ulp of the
+// reference's divisions); the strict form keeps the reference's operations.
+template <> struct Prec<SCL_FP64> { using R = double; using S = double; using A = double; static constexpr bool EXACT = true, FD = true; };
+template <> struct Prec<SCL_FP64_STRICT> { using R = double; using S = double; using A = double; static constexpr bool EXACT = true, FD = false; };
+template <> struct Prec<SCL_MIXED> { using R = float; using S = double; using A = double; static constexpr bool EXACT = false, FD = false; };
+template <> struct Prec<SCL_FP32> { using R = float; using S = float; using A = float; static constexpr bool EXACT = false, FD = false; };
 
 
 
@@ -133,6 +135,7 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs, 
                                                 typename Prec<PREC>::R s[P::MWAVES]) {
   using R = typename Prec<PREC>::R;
   constexpr int M = P::MEQN, MW = P::MWAVES, MA = P::MAUX;
+  constexpr bool FD = Prec<PREC>::FD;
   if constexpr (Prec<PREC>::EXACT) {
     double q[6][M];
 #pragma unroll
@@ -141,8 +144,8 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs, 
       for (int m = 0; m < M; ++m) q[k][m] = (double)qs(k, m);
     if constexpr (CD == 2) {
       double evl[M][M], evr[M][M];
-      P::template evec<double>(ph, ixy, q[2], q[3], auxm, aux0, evl, evr);
-      weno5_char_exact<M>(q, evl, evr, xl, xr);
+      P::template evec<double, FD>(ph, ixy, q[2], q[3], auxm, aux0, evl, evr);
+      weno5_char_exact<M, FD>(q, evl, evr, xl, xr);
     } else if constexpr (CD == 1) {
       // waves of the cell-average Riemann problems at c-2 .. c+2 (flux1.f90:99-100)
       double w[5][MW][M], ak[6][MA > 0 ? MA : 1];
@@ -155,9 +158,9 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs, 
         double dk[M];
 #pragma unroll
         for (int m = 0; m < M; ++m) dk[m] = q[k + 1][m] - q[k][m];
-        P::template waves<double>(ph, ixy, q[k], q[k + 1], dk, ak[k], ak[k + 1], w[k]);
+        P::template waves<double, FD>(ph, ixy, q[k], q[k + 1], dk, ak[k], ak[k + 1], w[k]);
       }
-      weno5_wave_exact<M, MW>(q, w, xl, xr);
+      weno5_wave_exact<M, MW, FD>(q, w, xl, xr);
     } else if constexpr (CD == 3) {
       // eigenvectors of the five interfaces c-2 .. c+2 (flux1.f90:108-110)
       double evlc[M][M], evrc[M][M], h[5][M];
@@ -168,7 +171,7 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs, 
       double a2[MA > 0 ? MA : 1], a3[MA > 0 ? MA : 1];
       axk(2, a2);
       axk(3, a3);
-      P::template evec<double>(ph, ixy, q[2], q[3], a2, a3, evlc, evrc);
+      P::template evec<double, FD>(ph, ixy, q[2], q[3], a2, a3, evlc, evrc);
 #pragma unroll
       for (int k = 0; k < 5; ++k) {
         double dk[M];
@@ -180,18 +183,18 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs, 
           double evl[M][M], evr[M][M], ak0[MA > 0 ? MA : 1], ak1[MA > 0 ? MA : 1];
           axk(k, ak0);
           axk(k + 1, ak1);
-          P::template evec<double>(ph, ixy, q[k], q[k + 1], ak0, ak1, evl, evr);
+          P::template evec<double, FD>(ph, ixy, q[k], q[k + 1], ak0, ak1, evl, evr);
           trans_project<double, M>(evl, evr, dk, evlc, h[k]);
         }
       }
-      weno5_trans_exact<M>(q, h, evrc, xl, xr);
+      weno5_trans_exact<M, FD>(q, h, evrc, xl, xr);
     } else {
-      weno5_exact<M>(q, xl, xr);
+      weno5_exact<M, FD>(q, xl, xr);
     }
     double dl[M];
 #pragma unroll
     for (int m = 0; m < M; ++m) dl[m] = xr[m] - xl[m];   // delta = ql(i) - qr(i-1)
-    P::template rp<double>(ph, ixy, xl, xr, dl, auxm, aux0, s, amdq, apdq);
+    P::template rp<double, FD>(ph, ixy, xl, xr, dl, auxm, aux0, s, amdq, apdq);
   } else {
     float d[5][M];
 #pragma unroll
@@ -274,13 +277,13 @@ __device__ __forceinline__ void cell_bracket(const Phys& ph, int ixy, const type
   }
   if constexpr (TF == 1) {
     R adq[M];
-    if constexpr (Prec<PREC>::EXACT) P::template tfluct<R>(ph, ixy, L, Rt, dl, auxc, adq);
+    if constexpr (Prec<PREC>::EXACT) P::template tfluct<R, Prec<PREC>::FD>(ph, ixy, L, Rt, dl, auxc, adq);
     else tfluct_f32<P>(ph, ixy, L, Rt, dl, auxc, adq);
 #pragma unroll
     for (int m = 0; m < M; ++m) br[m] = (apdq_c[m] + adq[m]) + amdq_c1[m];       // :151-152
   } else {
     R s2[P::MWAVES], am2[M], ap2[M];
-    if constexpr (Prec<PREC>::EXACT) P::template rp<R>(ph, ixy, L, Rt, dl, auxc, auxc, s2, am2, ap2);  // :181-182
+    if constexpr (Prec<PREC>::EXACT) P::template rp<R, Prec<PREC>::FD>(ph, ixy, L, Rt, dl, auxc, auxc, s2, am2, ap2);  // :181-182
     else rp_f32<P>(ph, ixy, L, Rt, dl, auxc, auxc, s2, am2, ap2);
 #pragma unroll
     for (int m = 0; m < M; ++m) br[m] = ((amdq_c1[m] + apdq_c[m]) + am2[m]) + ap2[m];  // :185-186

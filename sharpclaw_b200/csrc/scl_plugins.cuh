@@ -17,7 +17,11 @@ namespace scl {
 
 // FP32 Euler plugins use reciprocal-square-root forms of the Roe averages and
 // the entropy-fix sound speeds (algebraically the reference's, not its
-// operation order; the FP64 forms keep the reference's order).
+// operation order).  The FP64 forms keep the reference's order unless the
+// template flag FD (fast division) is set: then divisions become reciprocal
+// multiplies and square roots reciprocal square roots, as in FP32, within a
+// few ulp of the reference's values (the SCL_FP64 form; SCL_FP64_STRICT and
+// the adjoint keep FD = false).
 #ifndef SCL_FAST_ROE
 #define SCL_FAST_ROE 1
 #endif
@@ -33,7 +37,7 @@ __device__ __forceinline__ R rmax(R a, R b) { return a > b ? a : b; }
 struct PAdvection {
   static constexpr int MEQN = 1, MWAVES = 1, MAUX = 0, NDIM = 1;
   static constexpr bool HAS_TFLUCT = true;
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void rp(const Phys& ph, int, const R*, const R*, const R* dl, const R*,
                             const R*, R* s, R* amdq, R* apdq) {
     const R u = (R)ph.u;
@@ -42,12 +46,12 @@ struct PAdvection {
     apdq[0] = rmax(u, (R)0) * dl[0];
   }
   // waves of rp1.f:35 (the jump itself), for the wave-based reconstruction
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void waves(const Phys&, int, const R*, const R*, const R* dl, const R*, const R*,
                                R w[1][1]) {
     w[0][0] = dl[0];
   }
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void tfluct(const Phys& ph, int, const R*, const R*, const R* dl, const R*,
                                 R* adq) {
     const R u = (R)ph.u;
@@ -55,7 +59,7 @@ struct PAdvection {
     R ap = rmax(u, (R)0) * dl[0];
     adq[0] = am + ap;
   }
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void evec(const Phys&, int, const R*, const R*, const R*, const R*,
                               R evl[1][1], R evr[1][1]) {
     evl[0][0] = (R)1;
@@ -73,7 +77,7 @@ struct PEuler {
   static constexpr bool HAS_TFLUCT = false;
 
   // `ia` (FP32 form only) receives 1/a.
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void roe(const Phys& ph, const R* L, const R* Rt, R& u, R& enth, R& a,
                              R* ia = nullptr) {
 #if SCL_FAST_ROE
@@ -94,6 +98,20 @@ struct PEuler {
       return;
     }
 #endif
+    if constexpr (FD && sizeof(R) == 8) {
+      const double g1 = ph.gamma1;
+      const double wl = rsqrt(L[0]), wr = rsqrt(Rt[0]);
+      const double pl = g1 * (L[2] - 0.5 * (L[1] * L[1]) * (wl * wl));
+      const double pr = g1 * (Rt[2] - 0.5 * (Rt[1] * Rt[1]) * (wr * wr));
+      const double inv = 1.0 / (L[0] * wl + Rt[0] * wr);
+      u = (L[1] * wl + Rt[1] * wr) * inv;
+      enth = ((L[2] + pl) * wl + (Rt[2] + pr) * wr) * inv;
+      const double a2 = g1 * (enth - 0.5 * (u * u));
+      const double ra = rsqrt(a2);
+      a = a2 * ra;
+      if (ia) *ia = ra;
+      return;
+    }
     const R g1 = (R)ph.gamma1;
     R rhsqrtl = sqrt(L[0]);
     R rhsqrtr = sqrt(Rt[0]);
@@ -109,7 +127,7 @@ struct PEuler {
   // u - c (PLUS false) or u + c (PLUS true) of one state, the four
   // characteristic speeds of the entropy fix (rp1eu.f:132-134, 150-152,
   // 170-172, 180-182).
-  template <bool PLUS, class R>
+  template <bool PLUS, class R, bool FD = false>
   __device__ static R efix_speed(const Phys& ph, R rho, R m, R en) {
 #if SCL_FAST_ROE
     if constexpr (sizeof(R) == 4) {  // one reciprocal, one square root
@@ -119,6 +137,12 @@ struct PEuler {
       return PLUS ? u + c : u - c;
     }
 #endif
+    if constexpr (FD && sizeof(R) == 8) {
+      const double ir = 1.0 / rho, u = m * ir;
+      const double p = ph.gamma1 * (en - 0.5 * (m * u));
+      const double c = sqrt((ph.gamma * p) * ir);
+      return PLUS ? u + c : u - c;
+    }
     const R g1 = (R)ph.gamma1, gamma = (R)ph.gamma;
     R p = g1 * (en - ((R)0.5 * (m * m)) / rho);
     R c = sqrt((gamma * p) / rho);
@@ -126,20 +150,17 @@ struct PEuler {
   }
 
   // Roe averages and the three waves of rp1eu.f:44-86, w[wave][component].
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void wave_set(const Phys& ph, const R* L, const R* Rt, const R* dl, R& u, R& enth,
                                   R& a, R w[3][3]) {
     const R g1 = (R)ph.gamma1;
     R ia = (R)0;
-    roe(ph, L, Rt, u, enth, a, &ia);                              // rp1eu.f:44-55
+    roe<R, FD>(ph, L, Rt, u, enth, a, &ia);                       // rp1eu.f:44-55
     R a2, a3;
-#if SCL_FAST_ROE
-    if constexpr (sizeof(R) == 4) {
+    if constexpr ((sizeof(R) == 4 && SCL_FAST_ROE) || FD) {
       a2 = (g1 * (ia * ia)) * (((enth - u * u) * dl[0] + u * dl[1]) - dl[2]);
-      a3 = ((dl[1] + (a - u) * dl[0]) - a * a2) * (0.5f * ia);
-    } else
-#endif
-    {
+      a3 = ((dl[1] + (a - u) * dl[0]) - a * a2) * ((R)0.5 * ia);
+    } else {
       a2 = (g1 / (a * a)) * (((enth - u * u) * dl[0] + u * dl[1]) - dl[2]);   // :65-66
       a3 = ((dl[1] + (a - u) * dl[0]) - a * a2) / ((R)2 * a);                   // :67
     }
@@ -149,18 +170,18 @@ struct PEuler {
     w[2][0] = a3; w[2][1] = a3 * (u + a); w[2][2] = a3 * (enth + u * a);
   }
 
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void waves(const Phys& ph, int, const R* L, const R* Rt, const R* dl, const R*,
                                const R*, R w[3][3]) {
     R u, enth, a;
-    wave_set(ph, L, Rt, dl, u, enth, a, w);
+    wave_set<R, FD>(ph, L, Rt, dl, u, enth, a, w);
   }
 
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void rp(const Phys& ph, int, const R* L, const R* Rt, const R* dl, const R*,
                             const R*, R* s, R* amdq, R* apdq) {
     R u, enth, a, w[3][3];  // w[wave][component]
-    wave_set(ph, L, Rt, dl, u, enth, a, w);
+    wave_set<R, FD>(ph, L, Rt, dl, u, enth, a, w);
     s[0] = u - a; s[1] = u; s[2] = u + a;
     if (!ph.efix) {                                                            // :100-111
 #pragma unroll
@@ -177,7 +198,7 @@ struct PEuler {
     }
     // entropy fix, rp1eu.f:126-201
     do {
-      R s0 = efix_speed<false>(ph, L[0], L[1], L[2]);
+      R s0 = efix_speed<false, R, FD>(ph, L[0], L[1], L[2]);
       if (s0 >= (R)0 && s[0] > (R)0) {
         amdq[0] = amdq[1] = amdq[2] = (R)0;
         break;
@@ -185,7 +206,7 @@ struct PEuler {
       R rho1 = L[0] + w[0][0];
       R rhou1 = L[1] + w[0][1];
       R en1 = L[2] + w[0][2];
-      R s1 = efix_speed<false>(ph, rho1, rhou1, en1);
+      R s1 = efix_speed<false, R, FD>(ph, rho1, rhou1, en1);
       R sfract;
       if (s0 < (R)0 && s1 > (R)0) sfract = (s0 * (s1 - s[0])) / (s1 - s0);
       else if (s[0] < (R)0) sfract = s[0];
@@ -195,11 +216,11 @@ struct PEuler {
       if (s[1] >= (R)0) break;
 #pragma unroll
       for (int m = 0; m < 3; ++m) amdq[m] = amdq[m] + s[1] * w[1][m];
-      R s3 = efix_speed<true>(ph, Rt[0], Rt[1], Rt[2]);
+      R s3 = efix_speed<true, R, FD>(ph, Rt[0], Rt[1], Rt[2]);
       R rho2 = Rt[0] - w[2][0];
       R rhou2 = Rt[1] - w[2][1];
       R en2 = Rt[2] - w[2][2];
-      R s2 = efix_speed<true>(ph, rho2, rhou2, en2);
+      R s2 = efix_speed<true, R, FD>(ph, rho2, rhou2, en2);
       if (s2 < (R)0 && s3 > (R)0) sfract = (s2 * (s3 - s[2])) / (s3 - s2);
       else if (s[2] < (R)0) sfract = s[2];
       else break;
@@ -215,29 +236,27 @@ struct PEuler {
     }
   }
 
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void tfluct(const Phys&, int, const R*, const R*, const R*, const R*, R*) {}
 
   // Roe eigenvectors (new; the reference's evec1eu.f is incomplete).  Averages
   // as rp1eu.f:44-55 from the cell averages q(i-1), q(i).
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void evec(const Phys& ph, int, const R* qm, const R* q0, const R*, const R*,
                               R evl[3][3], R evr[3][3]) {
-#if SCL_FAST_ROE
-    if constexpr (sizeof(R) == 4) {
-      float u, h, a, ia;
-      roe(ph, qm, q0, u, h, a, &ia);
-      const float g1 = (float)ph.gamma1;
-      evr[0][0] = 1.0f;      evr[0][1] = 1.0f;             evr[0][2] = 1.0f;
+    if constexpr ((sizeof(R) == 4 && SCL_FAST_ROE) || FD) {
+      R u, h, a, ia;
+      roe<R, FD>(ph, qm, q0, u, h, a, &ia);
+      const R g1 = (R)ph.gamma1, h5 = (R)0.5;
+      evr[0][0] = (R)1;      evr[0][1] = (R)1;             evr[0][2] = (R)1;
       evr[1][0] = u - a;     evr[1][1] = u;                evr[1][2] = u + a;
-      evr[2][0] = h - u * a; evr[2][1] = 0.5f * (u * u);   evr[2][2] = h + u * a;
-      const float b1 = g1 * (ia * ia), b2 = 0.5f * (b1 * (u * u)), ua = u * ia, b1u = b1 * u;
-      evl[0][0] = 0.5f * (b2 + ua); evl[0][1] = -0.5f * (b1u + ia); evl[0][2] = 0.5f * b1;
-      evl[1][0] = 1.0f - b2;        evl[1][1] = b1u;                evl[1][2] = -b1;
-      evl[2][0] = 0.5f * (b2 - ua); evl[2][1] = -0.5f * (b1u - ia); evl[2][2] = 0.5f * b1;
+      evr[2][0] = h - u * a; evr[2][1] = h5 * (u * u);     evr[2][2] = h + u * a;
+      const R b1 = g1 * (ia * ia), b2 = h5 * (b1 * (u * u)), ua = u * ia, b1u = b1 * u;
+      evl[0][0] = h5 * (b2 + ua); evl[0][1] = -h5 * (b1u + ia); evl[0][2] = h5 * b1;
+      evl[1][0] = (R)1 - b2;      evl[1][1] = b1u;              evl[1][2] = -b1;
+      evl[2][0] = h5 * (b2 - ua); evl[2][1] = -h5 * (b1u - ia); evl[2][2] = h5 * b1;
       return;
     }
-#endif
     const R g1 = (R)ph.gamma1;
     R rhsqrtl = sqrt(qm[0]);
     R rhsqrtr = sqrt(q0[0]);
@@ -274,7 +293,7 @@ struct PShallow2D {
 
   // Roe averages of rpn2sw.f:80-88: normal and tangential velocity u, v (mu,
   // mv the normal / tangential momentum), celerity a, and ha = 0.5/a.
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void roe(const Phys& ph, int mu, int mv, const R* L, const R* Rt, R& u, R& v, R& a,
                              R& ha) {
 #if SCL_FAST_ROE
@@ -292,6 +311,17 @@ struct PShallow2D {
       return;
     }
 #endif
+    if constexpr (FD && sizeof(R) == 8) {
+      const double wl = rsqrt(L[0]), wr = rsqrt(Rt[0]);
+      const double inv = 1.0 / (L[0] * wl + Rt[0] * wr);
+      u = (L[mu] * wl + Rt[mu] * wr) * inv;
+      v = (L[mv] * wl + Rt[mv] * wr) * inv;
+      const double gh = ph.grav * ((L[0] + Rt[0]) * 0.50);
+      const double ia = rsqrt(gh);
+      a = gh * ia;
+      ha = 0.50 * ia;
+      return;
+    }
     const R g = (R)ph.grav;
     R h = (L[0] + Rt[0]) * (R)0.50;
     R hsqrtl = sqrt(L[0]);
@@ -304,12 +334,12 @@ struct PShallow2D {
   }
 
   // Roe averages and the three waves of rpn2sw.f:80-118 along ixy.
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void wave_set(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl, R& u,
                                   R& a, R w[3][3]) {
     const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
     R v, ha;
-    roe(ph, mu, mv, L, Rt, u, v, a, ha);                                    // rpn2sw.f:80-88
+    roe<R, FD>(ph, mu, mv, L, Rt, u, v, a, ha);                             // rpn2sw.f:80-88
     R a1 = ((u + a) * dl[0] - dl[mu]) * ha;                                 // :98-100
     R a2 = -(v * dl[0]) + dl[mv];
     R a3 = (-((u - a) * dl[0]) + dl[mu]) * ha;
@@ -318,20 +348,20 @@ struct PShallow2D {
     w[2][0] = a3; w[2][mu] = a3 * (u + a); w[2][mv] = a3 * v;
   }
 
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void waves(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl, const R*,
                                const R*, R w[3][3]) {
     R u, a;
-    wave_set(ph, ixy, L, Rt, dl, u, a, w);
+    wave_set<R, FD>(ph, ixy, L, Rt, dl, u, a, w);
   }
 
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void solve(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl,
                                R* s, R* amdq, R* apdq) {
     const R g = (R)ph.grav;
     const int mu = (ixy == 1) ? 1 : 2;
     R u, a, w[3][3];
-    wave_set(ph, ixy, L, Rt, dl, u, a, w);
+    wave_set<R, FD>(ph, ixy, L, Rt, dl, u, a, w);
     s[0] = u - a; s[1] = u; s[2] = u + a;
     if (!ph.efix) {                                                         // :132-143
 #pragma unroll
@@ -385,29 +415,29 @@ struct PShallow2D {
     }
   }
 
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void rp(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl, const R*,
                             const R*, R* s, R* amdq, R* apdq) {
-    solve(ph, ixy, L, Rt, dl, s, amdq, apdq);
+    solve<R, FD>(ph, ixy, L, Rt, dl, s, amdq, apdq);
   }
   // tfluct1sw.f: the same Roe solve with left ql(i), right qr(i); adq = amdq+apdq
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void tfluct(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl,
                                 const R*, R* adq) {
     R s[3], am[3], ap[3];
-    solve(ph, ixy, L, Rt, dl, s, am, ap);
+    solve<R, FD>(ph, ixy, L, Rt, dl, s, am, ap);
 #pragma unroll
     for (int m = 0; m < 3; ++m) adq[m] = am[m] + ap[m];
   }
   // Shallow-water Roe eigenvectors along ixy (new; the reference has none).
   // Averages as rpn2sw.f:80-88; left eigenvectors are the rows rpn2sw.f:98-100
   // uses for a1..a3.
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void evec(const Phys& ph, int ixy, const R* qm, const R* q0, const R*,
                               const R*, R evl[3][3], R evr[3][3]) {
     const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
     R u, v, a, ha;
-    roe(ph, mu, mv, qm, q0, u, v, a, ha);
+    roe<R, FD>(ph, mu, mv, qm, q0, u, v, a, ha);
     evr[0][0] = (R)1;  evr[mu][0] = u - a; evr[mv][0] = v;
     evr[0][1] = (R)0;  evr[mu][1] = (R)0;  evr[mv][1] = (R)1;
     evr[0][2] = (R)1;  evr[mu][2] = u + a; evr[mv][2] = v;
@@ -427,12 +457,12 @@ template <int NEQ>
 struct PAcoustics {
   static constexpr int MEQN = NEQ, MWAVES = 2, MAUX = 2, NDIM = (NEQ == 2 ? 1 : 2);
   static constexpr bool HAS_TFLUCT = true;
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void rp(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl, const R* auxl,
                             const R* auxr, R* s, R* amdq, R* apdq) {
     // auxl = aux of the left cell (auxr(i-1,:)), auxr = aux of the right cell (auxl(i,:))
     R w[2][NEQ];
-    waves(ph, ixy, L, Rt, dl, auxl, auxr, w);
+    waves<R, FD>(ph, ixy, L, Rt, dl, auxl, auxr, w);
     s[0] = -auxl[1];
     s[1] = auxr[1];
 #pragma unroll
@@ -442,27 +472,41 @@ struct PAcoustics {
     }
   }
   // the two waves of rp1acv.f:49-60 (zero tangential component in 2-D)
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void waves(const Phys&, int ixy, const R*, const R*, const R* dl, const R* auxl,
                                const R* auxr, R w[2][NEQ]) {
     const int mu = (ixy == 1) ? 1 : 2;
     R zi = auxr[0];
     R zim = auxl[0];
-    R a1 = ((-dl[0]) + zi * dl[mu]) / (zim + zi);
-    R a2 = (dl[0] + zim * dl[mu]) / (zim + zi);
+    R a1, a2;
+    if constexpr (FD) {
+      const R iz = (R)1 / (zim + zi);
+      a1 = ((-dl[0]) + zi * dl[mu]) * iz;
+      a2 = (dl[0] + zim * dl[mu]) * iz;
+    } else {
+      a1 = ((-dl[0]) + zi * dl[mu]) / (zim + zi);
+      a2 = (dl[0] + zim * dl[mu]) / (zim + zi);
+    }
 #pragma unroll
     for (int m = 0; m < NEQ; ++m) { w[0][m] = (R)0; w[1][m] = (R)0; }
     w[0][0] = -(a1 * zim); w[0][mu] = a1;
     w[1][0] = a2 * zi;     w[1][mu] = a2;
   }
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void tfluct(const Phys&, int ixy, const R*, const R*, const R* dl,
                                 const R* aux, R* adq) {
     const int mu = (ixy == 1) ? 1 : 2;
     R zi = aux[0];
     R zim = aux[0];
-    R a1 = ((-dl[0]) + zi * dl[mu]) / (zim + zi);
-    R a2 = (dl[0] + zim * dl[mu]) / (zim + zi);
+    R a1, a2;
+    if constexpr (FD) {
+      const R iz = (R)1 / (zim + zi);
+      a1 = ((-dl[0]) + zi * dl[mu]) * iz;
+      a2 = (dl[0] + zim * dl[mu]) * iz;
+    } else {
+      a1 = ((-dl[0]) + zi * dl[mu]) / (zim + zi);
+      a2 = (dl[0] + zim * dl[mu]) / (zim + zi);
+    }
     R s1 = -aux[1], s2 = aux[1];
     R w1[NEQ], w2[NEQ];
 #pragma unroll
@@ -476,7 +520,7 @@ struct PAcoustics {
       adq[m] = am + ap;
     }
   }
-  template <class R>
+  template <class R, bool FD = false>
   __device__ static void evec(const Phys&, int ixy, const R*, const R*, const R* auxm,
                               const R* aux0, R evl[NEQ][NEQ], R evr[NEQ][NEQ]) {
     const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;

@@ -24,7 +24,9 @@ __device__ __forceinline__ double epweno() { return (double)1.0e-36f; }
 // in [1e-16, 1e4], so every weight product stays between 1e-32 and 1e9.
 constexpr float EPS_SCALED = 1.0e-8f;
 
-// One side of the WENO5 correction, reference order (reconstruct.f90:113-132).
+// One side of the WENO5 correction, reference order (reconstruct.f90:113-132);
+// FD (fast division) multiplies by 1/3 instead of dividing by 3.
+template <bool FD = false>
 __device__ __forceinline__ double weno_side(double dm2, double dm1, double d0, double dp1,
                                             double im) {
   double t1 = im * (dm2 - dm1);
@@ -46,7 +48,15 @@ __device__ __forceinline__ double weno_side(double dm2, double dm1, double d0, d
   double t0 = 1.0 / ((s1 + s2) + s3);
   s1 = s1 * t0;
   s3 = s3 * t0;
+  if constexpr (FD) return ((s1 * (t2 - t1)) + ((0.5 * s3 - 0.25) * (t3 - t2))) * (1.0 / 3.0);
   return ((s1 * (t2 - t1)) + ((0.5 * s3 - 0.25) * (t3 - t2))) / 3.0;
+}
+
+// c/12 of the central stencil (reconstruct.f90:131-132)
+template <bool FD>
+__device__ __forceinline__ double twelfth(double c) {
+  if constexpr (FD) return c * (1.0 / 12.0);
+  return c / 12.0;
 }
 
 // Scaled FP32 form of weno_side on jumps already divided by `scale`.
@@ -161,7 +171,7 @@ static __device__ SCL_FP32_FN void weno_pair_scaled(const float h[5], float& u1,
 // Exact form (FP64): returns the reconstructed states qr(c-1) (qrl) and ql(c)
 // (qlr).  q[k][m] holds cells c-3+k, k = 0..5.
 // ---------------------------------------------------------------------------
-template <int M>
+template <int M, bool FD = false>
 __device__ __forceinline__ void weno5_exact(const double q[6][M], double qrl[M], double qlr[M]) {
 #pragma unroll
   for (int m = 0; m < M; ++m) {
@@ -169,14 +179,14 @@ __device__ __forceinline__ void weno5_exact(const double q[6][M], double qrl[M],
 #pragma unroll
     for (int k = 0; k < 5; ++k) d[k] = q[k + 1][m] - q[k][m];
     double c = ((-q[1][m]) + 7.0 * (q[2][m] + q[3][m])) - q[4][m];
-    qrl[m] = weno_side(d[0], d[1], d[2], d[3], 1.0) + c / 12.0;
-    qlr[m] = weno_side(d[4], d[3], d[2], d[1], -1.0) + c / 12.0;
+    qrl[m] = weno_side<FD>(d[0], d[1], d[2], d[3], 1.0) + twelfth<FD>(c);
+    qlr[m] = weno_side<FD>(d[4], d[3], d[2], d[1], -1.0) + twelfth<FD>(c);
   }
 }
 
 // reconstruct.f90:146-241 for one interface; evl[p][m] = evl(i,p,m),
 // evr[m][p] = evr(i,m,p).
-template <int M>
+template <int M, bool FD = false>
 __device__ __forceinline__ void weno5_char_exact(const double q[6][M], const double evl[M][M],
                                                  const double evr[M][M], double qrl[M],
                                                  double qlr[M]) {
@@ -188,7 +198,7 @@ __device__ __forceinline__ void weno5_char_exact(const double q[6][M], const dou
 #pragma unroll
   for (int m = 0; m < M; ++m) {
     double c = ((-q[1][m]) + 7.0 * (q[2][m] + q[3][m])) - q[4][m];
-    qrl[m] = c / 12.0;
+    qrl[m] = twelfth<FD>(c);
     qlr[m] = qrl[m];
   }
 #pragma unroll
@@ -201,8 +211,8 @@ __device__ __forceinline__ void weno5_char_exact(const double q[6][M], const dou
       for (int m = 0; m < M; ++m) s = s + evl[p][m] * d[k][m];
       h[k] = s;
     }
-    double u1 = weno_side(h[0], h[1], h[2], h[3], 1.0);
-    double u2 = weno_side(h[4], h[3], h[2], h[1], -1.0);
+    double u1 = weno_side<FD>(h[0], h[1], h[2], h[3], 1.0);
+    double u2 = weno_side<FD>(h[4], h[3], h[2], h[1], -1.0);
 #pragma unroll
     for (int m = 0; m < M; ++m) {
       qrl[m] = qrl[m] + evr[m][p] * u1;
@@ -271,13 +281,13 @@ __device__ __forceinline__ void weno5_char_offset(const float d[5][M], const flo
 // reconstruct.f90:413 `if (wnorm2.gt.1.e-14)` (a REAL(4) literal)
 __device__ __forceinline__ double wave_floor() { return (double)1.0e-14f; }
 
-template <int M, int MW>
+template <int M, int MW, bool FD = false>
 __device__ __forceinline__ void weno5_wave_exact(const double q[6][M], const double w[5][MW][M],
                                                  double qrl[M], double qlr[M]) {
 #pragma unroll
   for (int m = 0; m < M; ++m) {
     double c = ((-q[1][m]) + 7.0 * (q[2][m] + q[3][m])) - q[4][m];   // :371-372
-    qrl[m] = c / 12.0;
+    qrl[m] = twelfth<FD>(c);
     qlr[m] = qrl[m];
   }
 #pragma unroll
@@ -291,8 +301,8 @@ __device__ __forceinline__ void weno5_wave_exact(const double q[6][M], const dou
     }
     double u1 = 0.0, u2 = 0.0, winv = 0.0;                            // :413-419
     if (th[2] > wave_floor()) {
-      u1 = weno_side(th[0], th[1], th[2], th[3], 1.0);
-      u2 = weno_side(th[4], th[3], th[2], th[1], -1.0);
+      u1 = weno_side<FD>(th[0], th[1], th[2], th[3], 1.0);
+      u2 = weno_side<FD>(th[4], th[3], th[2], th[1], -1.0);
       winv = 1.0 / th[2];
     }
 #pragma unroll
@@ -364,19 +374,19 @@ __device__ __forceinline__ void trans_project(const T evlk[M][M], const T evrk[M
 }
 
 // reconstruct.f90:298-345 from h[k][mw]; evrc = evr of c-1/2.
-template <int M>
+template <int M, bool FD = false>
 __device__ __forceinline__ void weno5_trans_exact(const double q[6][M], const double h[5][M],
                                                   const double evrc[M][M], double qrl[M], double qlr[M]) {
   double u1[M], u2[M];
 #pragma unroll
   for (int mw = 0; mw < M; ++mw) {
-    u1[mw] = weno_side(h[0][mw], h[1][mw], h[2][mw], h[3][mw], 1.0);
-    u2[mw] = weno_side(h[4][mw], h[3][mw], h[2][mw], h[1][mw], -1.0);
+    u1[mw] = weno_side<FD>(h[0][mw], h[1][mw], h[2][mw], h[3][mw], 1.0);
+    u2[mw] = weno_side<FD>(h[4][mw], h[3][mw], h[2][mw], h[1][mw], -1.0);
   }
 #pragma unroll
   for (int m = 0; m < M; ++m) {
     double c = ((-q[1][m]) + 7.0 * (q[2][m] + q[3][m])) - q[4][m];
-    double a = c / 12.0, b = c / 12.0;
+    double a = twelfth<FD>(c), b = twelfth<FD>(c);
 #pragma unroll
     for (int mw = 0; mw < M; ++mw) {
       a = a + evrc[m][mw] * u1[mw];
