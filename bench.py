@@ -409,12 +409,13 @@ def run_gpu(args, rank, world, local_rank):
     e2e, e2e_s = job_rate(W["cells"] * W["stages"] * e2e_taken, e2e_local, world, dev)
     nbytes = q0.nbytes
 
-    # accuracy: the headline form against plain FP64 after 20 fixed-dt steps
+    # accuracy: the headline form against FP64 in the reference's operation
+    # order (fp64_strict) after 20 fixed-dt steps
     acc = {}
     if rank == 0:
         outs = {}
         dt = W["dt0"]
-        for name in ("fp64", args.precision):
+        for name in ("fp64_strict", args.precision, "fp64"):
             with S.Solver(ps, name) as s:
                 if aux0 is not None:
                     s.set_aux(aux0)
@@ -422,11 +423,12 @@ def run_gpu(args, rank, world, local_rank):
                 s.sharpclaw(0.0, 20 * dt, dt, 1e9, 0.5, dt_variable=0)
                 q = s.get_q()
                 outs[name] = q[:, 3:-3] if ps.ndim == 1 else q[:, 3:-3, 3:-3]
-        a, b = outs[args.precision], outs["fp64"]
+        a, b = outs[args.precision], outs["fp64_strict"]
         nc = a.shape[0]
-        acc = {"rel_l1_vs_fp64": max(float(np.abs(a[m] - b[m]).sum() / max(np.abs(b[m]).sum(), 1e-300))
+        acc = {"rel_l1_vs_fp64_strict": max(float(np.abs(a[m] - b[m]).sum() / max(np.abs(b[m]).sum(), 1e-300))
                                      for m in range(nc)),
-               "rel_linf_vs_fp64": float(np.abs(a - b).max() / np.abs(b).max()),
+               "rel_linf_vs_fp64_strict": float(np.abs(a - b).max() / np.abs(b).max()),
+               "fp64_rel_linf_vs_fp64_strict": float(np.abs(outs["fp64"] - b).max() / np.abs(b).max()),
                "steps": 20, "dt": dt}
 
     # CPU baseline: the oracle on a bounded sample, one core (C2 only)
@@ -577,7 +579,8 @@ def run_gpu_batch(args, rank, world, local_rank):
     clocks = Clocks(local_rank)
     out = {}
     head = args.precision if args.precision != "mixed" else "fp32"
-    forms = [head] + (["mixed"] if head == "fp32" else []) + ["fp64"]
+    # fp64_strict (the reference's operation order) is the accuracy reference
+    forms = [head] + (["mixed"] if head == "fp32" else []) + ["fp64", "fp64_strict"]
     for precision in forms:
         b = S.Batch(ps, mx, dx, precision=precision)
         for _ in range(args.warmup):
@@ -618,13 +621,14 @@ def run_gpu_batch(args, rank, world, local_rank):
             one_cells += int(mx[k]) * 3 * (r["steps_taken"] - r["rejected"])
     value64_one = one_cells / (one_ms / 1000.0)
 
-    # accuracy of the FP32-arithmetic forms against the FP64 batch at the
-    # window's end: per instance the largest relative L1 over the components
-    ref = out["fp64"]["batch"].get_q()
+    # accuracy of the FP32-arithmetic forms against the FP64 batch in the
+    # reference's operation order at the window's end: per instance the
+    # largest relative L1 over the components
+    ref = out["fp64_strict"]["batch"].get_q()
 
     def rel_l1_of(form):
         got = out[form]["batch"].get_q()
-        bad = set(out[form]["failed"]) | set(out["fp64"]["failed"])
+        bad = set(out[form]["failed"]) | set(out["fp64_strict"]["failed"])
         e = [max(float(np.abs(g[m, 3:-3] - f[m, 3:-3]).sum() / np.abs(f[m, 3:-3]).sum()) for m in range(3))
              for k, (g, f) in enumerate(zip(got, ref)) if k not in bad]
         return float(np.max(e)), float(np.median(e))
@@ -634,8 +638,8 @@ def run_gpu_batch(args, rank, world, local_rank):
     if "mixed" in out and head != "mixed":
         mx_max, mx_med = rel_l1_of("mixed")
         vmix = out["mixed"]["rate"]
-        mixed = {"value": vmix, "unit": UNIT, "rel_l1_vs_fp64_max_over_instances": mx_max,
-                 "rel_l1_vs_fp64_median": mx_med, "failed_instances": out["mixed"]["failed"],
+        mixed = {"value": vmix, "unit": UNIT, "rel_l1_vs_fp64_strict_max_over_instances": mx_max,
+                 "rel_l1_vs_fp64_strict_median": mx_med, "failed_instances": out["mixed"]["failed"],
                  "dtype": "f32 (f64 state/accumulation)"}
 
     # end to end through the public API: H2D of every instance, the run, D2H
@@ -675,11 +679,12 @@ def run_gpu_batch(args, rank, world, local_rank):
                              "traffic": None, "note": "whole batch step time (stage + controller kernels)",
                              "algorithmic_bytes_per_cell_stage": byts, "peak_source": peak_kind},
                 "fp64_batched": {"value": value64_batched, "unit": UNIT},
+                "fp64_strict_batched": {"value": out["fp64_strict"]["rate"], "unit": UNIT},
                 "fp64_one_at_a_time": {"value": value64_one, "unit": UNIT, "sample_instances": len(sample),
                                        "speedup_of_headline": value / value64_one},
                 "mixed_batched": mixed,
-                "accuracy": {"rel_l1_vs_fp64_batch_max_over_instances": rel_l1,
-                             "rel_l1_vs_fp64_batch_median": rel_l1_med,
+                "accuracy": {"rel_l1_vs_fp64_strict_batch_max_over_instances": rel_l1,
+                             "rel_l1_vs_fp64_strict_batch_median": rel_l1_med,
                              "failed_instances": {"headline": out[head]["failed"], "fp64": out["fp64"]["failed"]}},
                 "cpu_baseline": None,
                 "e2e": {"value": e2e_rate, "unit": UNIT, "h2d_bytes_per_step": int(flat_np.nbytes),

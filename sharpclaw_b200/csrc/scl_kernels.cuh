@@ -30,13 +30,18 @@ template <> struct Prec<SCL_FP32> { using R = float; using S = float; using A = 
 
 // ---------------------------------------------------------------------------
 // Shu-Osher stage combinations (src/sharpclaw.f90), evaluated in A precision.
+// DIV3: divide by 3 as the reference does (strict form); otherwise multiply
+// by 1/3 (within an ulp).
 // ---------------------------------------------------------------------------
-template <class A>
+template <class A, bool DIV3 = true>
 __device__ __forceinline__ void combine(int kind, A q, A qo, A dq, A& out, A& out2) {
   switch (kind) {
     case SK_ADD: out = q + dq; break;                                            // :264,:356
     case SK_SSP33_2: out = (A)0.75 * qo + (A)0.25 * (q + dq); break;             // :365
-    case SK_SSP33_3: out = (qo + (A)2.0 * (q + dq)) / (A)3.0; break;             // :374
+    case SK_SSP33_3:                                                             // :374
+      if constexpr (DIV3) out = (qo + (A)2.0 * (q + dq)) / (A)3.0;
+      else out = (qo + (A)2.0 * (q + dq)) * (A)(1.0 / 3.0);
+      break;
     case SK_ADD_SIXTH: out = q + (A)(1.0 / 6.0) * dq; break;                     // :396..455
     case SK_SSP104_5: {                                                          // :424-426
       A r2 = q + (A)(1.0 / 6.0) * dq;
@@ -320,6 +325,7 @@ struct Tile1DSmem {
   typename Prec<PREC>::S sq[P::MEQN][NT + 8];
   typename Prec<PREC>::R rec[4][P::MEQN][NT];   // 0: qr(c-1)  1: ql(c)  2: amdq(c)  3: apdq(c)
   typename Prec<PREC>::R sred[NT / 32];
+  double dtdx;   // dt/dx, one division per tile
 };
 
 // One tile of a 1-D stage: the CTA solves interfaces c = c0 .. c0+NT-1 and
@@ -336,7 +342,7 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
   const int tid = threadIdx.x;
   const int mx = L.mx;
   const double dt = L.ctl->dt;
-  const double dtdx0 = dt / L.dx;
+  if (tid == 0) sm.dtdx = dt / L.dx;
 
   // stage cells c0-3 .. c0+NT+1 (global offset c+2)
   for (int k = tid; k < NT + 5; k += NT) {
@@ -346,6 +352,7 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
     for (int m = 0; m < M; ++m) sm.sq[m][k] = ok ? L.qin[(long)m * L.plane + g] : (S)1;
   }
   __syncthreads();
+  const double dtdx0 = sm.dtdx;
 
   // ---- interface phase ----
   R cflmax = (R)0;
@@ -420,7 +427,7 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
           Ac qv = (Ac)sm.sq[m][tid + 3];
           Ac qov = L.qo ? (Ac)L.qo[(long)m * L.plane + c + 2] : (Ac)0;
           Ac o1, o2 = (Ac)0;
-          combine<Ac>(kind, qv, qov, dqv, o1, o2);
+          combine<Ac, PREC == SCL_FP64_STRICT>(kind, qv, qov, dqv, o1, o2);
           bad |= !isfinite(o1);
           if (edge) put_1d<S, Ac>(L.out, L.plane, m, c, images_1d(c, mx, L.bl, L.br), o1);
           else L.out[(long)m * L.plane + c + 2] = (S)o1;
@@ -506,7 +513,8 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
   const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
   const S* qin = static_cast<const S*>(a.buf[ctl->role[a.sd.in]]);
   const double dt = ctl->dt;
-  const double dtdx0 = dt / a.dx, dtdy0 = dt / a.dy;
+  __shared__ double s_dtd[2];   // dt/dx, dt/dy: two divisions per CTA
+  if (tid == 0) { s_dtd[0] = dt / a.dx; s_dtd[1] = dt / a.dy; }
 
   // stage the block: cells (i0-3 .. i0+TX+2, j0-3 .. j0+TY+2)
   for (int k = tid; k < T::WX * T::WY; k += NT) {
@@ -518,6 +526,7 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
     for (int m = 0; m < M; ++m) sq[(m * T::WY + ky) * T::WX + kx] = ok ? qin[(long)m * a.plane + off] : (S)1;
   }
   __syncthreads();
+  const double dtdx0 = s_dtd[0], dtdy0 = s_dtd[1];
 
   R cflmax = (R)0;
   int bad = 0;
@@ -638,7 +647,7 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
         Ac qv = (Ac)sq[(m * T::WY + lj + 3) * T::WX + li + 3];
         Ac qov = qo ? (Ac)qo[(long)m * a.plane + o0] : (Ac)0;
         Ac o1, o2 = (Ac)0;
-        combine<Ac>(kind, qv, qov, (Ac)dqs[m], o1, o2);
+        combine<Ac, PREC == SCL_FP64_STRICT>(kind, qv, qov, (Ac)dqs[m], o1, o2);
         bad |= !isfinite(o1);
         if (edge)
           put_2d<S, Ac>(out, a.plane, a.pitch, m, gi, gj, images_1d(gi, nx, a.mthbc[0], a.mthbc[1]),
