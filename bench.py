@@ -631,15 +631,17 @@ def run_gpu_batch(args, rank, world, local_rank):
         bad = set(out[form]["failed"]) | set(out["fp64_strict"]["failed"])
         e = [max(float(np.abs(g[m, 3:-3] - f[m, 3:-3]).sum() / np.abs(f[m, 3:-3]).sum()) for m in range(3))
              for k, (g, f) in enumerate(zip(got, ref)) if k not in bad]
-        return float(np.max(e)), float(np.median(e))
+        e = np.asarray(e)
+        return float(np.max(e)), float(np.median(e)), int((e > 1e-5).sum()), len(e)
 
-    rel_l1, rel_l1_med = rel_l1_of(head)
+    rel_l1, rel_l1_med, n_over, n_cmp = rel_l1_of(head)
     mixed = None
     if "mixed" in out and head != "mixed":
-        mx_max, mx_med = rel_l1_of("mixed")
+        mx_max, mx_med, mx_over, _ = rel_l1_of("mixed")
         vmix = out["mixed"]["rate"]
         mixed = {"value": vmix, "unit": UNIT, "rel_l1_vs_fp64_strict_max_over_instances": mx_max,
-                 "rel_l1_vs_fp64_strict_median": mx_med, "failed_instances": out["mixed"]["failed"],
+                 "rel_l1_vs_fp64_strict_median": mx_med, "instances_above_1e-5": mx_over,
+                 "failed_instances": out["mixed"]["failed"],
                  "dtype": "f32 (f64 state/accumulation)"}
 
     # end to end through the public API: H2D of every instance, the run, D2H
@@ -685,6 +687,7 @@ def run_gpu_batch(args, rank, world, local_rank):
                 "mixed_batched": mixed,
                 "accuracy": {"rel_l1_vs_fp64_strict_batch_max_over_instances": rel_l1,
                              "rel_l1_vs_fp64_strict_batch_median": rel_l1_med,
+                             "instances_compared": n_cmp, "instances_above_1e-5": n_over,
                              "failed_instances": {"headline": out[head]["failed"], "fp64": out["fp64"]["failed"]}},
                 "cpu_baseline": None,
                 "e2e": {"value": e2e_rate, "unit": UNIT, "h2d_bytes_per_step": int(flat_np.nbytes),
