@@ -3,9 +3,12 @@
 // SCL_PREC_VALUE defined; the FP64_STRICT unit is compiled without FMA
 // contraction so its arithmetic follows the reference's evaluation order.
 #pragma once
+#include <type_traits>
+
 #include "scl_batch.cuh"
 #include "scl_kernels.cuh"
 #include "scl_launch.h"
+#include "scl_pair.cuh"
 
 #ifndef SCL_PREC_VALUE
 #error "SCL_PREC_VALUE must be defined"
@@ -24,6 +27,23 @@ template <class P, int CD, int TF>
 void launch1d(const StageArgs& a, cudaStream_t st) {
   const int nb = (a.mx + NT1 - 2) / (NT1 - 1);
   k_stage1d<P, CD, TF, PREC, NT1><<<nb, NT1, 0, st>>>(a);
+}
+
+// 1-D Euler in the FP32 forms: two interfaces per thread in packed FP32
+// (scl_pair.cuh); capacity grids take the one-interface kernel.
+#ifndef SCL_PAIR
+#define SCL_PAIR 1
+#endif
+constexpr int NTP = 128;
+
+template <int CD>
+void launch1d_pair(const StageArgs& a, cudaStream_t st) {
+  if (a.mcapa > 0) {
+    launch1d<PEuler, CD, 0>(a, st);
+    return;
+  }
+  const int nb = (a.mx + 2 * NTP - 2) / (2 * NTP - 1);
+  k_stage1d_pair<CD, PREC, NTP><<<nb, NTP, 0, st>>>(a);
 }
 
 template <class P, int CD, int TF, int TX, int TY, int NT>
@@ -74,6 +94,10 @@ bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
   L->ghost = nullptr;
   if (ndim == 1) {
     if (variant != 0) return false;
+    if constexpr (SCL_PAIR && std::is_same_v<P, PEuler> && !Prec<PREC>::EXACT) {
+      if (cd == 0 && tf == 0) { L->stage = &launch1d_pair<0>; return true; }
+      if (cd == 2 && tf == 0) { L->stage = &launch1d_pair<2>; return true; }
+    }
     if (cd == 0 && tf == 0) L->stage = &launch1d<P, 0, 0>;
     if (cd == 1 && tf == 0) L->stage = &launch1d<P, 1, 0>;
     if (cd == 2 && tf == 0) L->stage = &launch1d<P, 2, 0>;
