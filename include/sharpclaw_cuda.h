@@ -235,12 +235,19 @@ int scl_batch_set_aux(scl_batch* b, const double* aux);
  * the same start state (autotuning), then restores that state. */
 int scl_batch_run(scl_batch* b, const scl_run* run, const double* dt_initial, scl_result* res, float* ms);
 /* The autotuner's choice: variant index, threads per CTA, persistent grid
- * size and the trial time of each variant (2 entries). */
+ * size and the trial time of each variant (3 entries: tile widths 128 and 256,
+ * and the paired two-interfaces-per-thread tile of 1-D Euler in the FP32
+ * forms; 0 for variants a plugin does not have). */
 int scl_batch_tuning(scl_batch* b, int* variant, int* threads, int* grid, float* trial_ms);
 
 /* Kernel launches (begin, stages, end of every captured step) of the last
  * scl_batch_run, autotuning trials excluded. */
 long long scl_batch_launches(scl_batch* b);
+
+/* Fix the batched tile variant (0, 1 or 2, as scl_batch_tuning reports them), or
+ * with -1 let the next scl_batch_run time both and keep the faster (the
+ * default).  No counterpart in the reference. */
+int scl_batch_select(scl_batch* b, int variant);
 
 /* Stream of the handle (cudaStream_t as void*), for callers that overlap work. */
 void* scl_stream(scl_handle* h);

@@ -378,13 +378,17 @@ class Batch:
         out = [{k: getattr(r, k) for k, _ in C.scl_result._fields_} for r in res]
         return out, ms.value
 
+    def select(self, variant: int = -1):
+        """Fix the tile variant (0, 1) or let the next run choose (-1)."""
+        C.check(C.lib().scl_batch_select(self._h, int(variant)), "scl_batch_select")
+
     def launches(self) -> int:
         """Kernel launches of the last sharpclaw() call."""
         return int(C.lib().scl_batch_launches(self._h))
 
     def tuning(self):
         v, nt, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        tm = (ctypes.c_float * 2)()
+        tm = (ctypes.c_float * 3)()
         C.check(C.lib().scl_batch_tuning(self._h, ctypes.byref(v), ctypes.byref(nt), ctypes.byref(g), tm),
                 "scl_batch_tuning")
         return {"variant": v.value, "threads": nt.value, "grid": g.value, "trial_ms": list(tm)}

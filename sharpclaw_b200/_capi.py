@@ -93,6 +93,7 @@ SIGNATURES = [
     ("scl_batch_run", ctypes.c_int, [_h, ctypes.POINTER(scl_run), ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.POINTER(ctypes.c_float)]),
     ("scl_batch_launches", ctypes.c_longlong, [_h]),
+    ("scl_batch_select", ctypes.c_int, [_h, ctypes.c_int]),
     ("scl_batch_tuning", ctypes.c_int, [_h, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]),
     ("scl_adjoint_step", ctypes.c_int, [_h, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

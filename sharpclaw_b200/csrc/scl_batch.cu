@@ -136,8 +136,8 @@ struct scl_batch {
   double* d_dx = nullptr;
   int *d_active = nullptr, *d_prefix = nullptr, *d_nact = nullptr, *h_nact = nullptr;
   BatchLaunchers L[NBATCH_VARIANTS];
-  int nvariants = 0, variant = -1, grid[NBATCH_VARIANTS] = {0, 0};
-  float tune_ms[NBATCH_VARIANTS] = {0, 0};
+  int nvariants = 0, variant = -1, grid[NBATCH_VARIANTS] = {};
+  float tune_ms[NBATCH_VARIANTS] = {};
   long long last_launches = 0;   // kernel launches of the last scl_batch_run's replays
   StageDesc sd[MAXSTAGES];
   int nstages = 0, final_role = ROLE_A;
@@ -530,6 +530,16 @@ int scl_batch_run(scl_batch* b, const scl_run* run, const double* dt_initial, sc
 }
 
 long long scl_batch_launches(scl_batch* b) { return b ? b->last_launches : 0; }
+
+int scl_batch_select(scl_batch* b, int variant) {
+  if (!b) return bfail(SCL_E_INVALID, "null argument");
+  if (variant < -1 || variant >= b->nvariants) return bfail(SCL_E_UNSUPPORTED, "no such tile variant");
+  BCK(cudaStreamSynchronize(b->stream));
+  b->variant = variant;
+  for (int v = 0; v < NBATCH_VARIANTS; ++v) b->tune_ms[v] = 0.0f;
+  if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  return SCL_OK;
+}
 
 int scl_batch_tuning(scl_batch* b, int* variant, int* threads, int* grid, float* trial_ms) {
   if (!b) return bfail(SCL_E_INVALID, "null argument");

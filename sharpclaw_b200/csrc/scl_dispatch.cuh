@@ -148,8 +148,34 @@ void fill_batch(BatchLaunchers* L) {
   L->blocks_per_sm = &batch_blocks_per_sm<P, CD, TF, NT>;
   L->nt = NT;
 }
+template <int CD>
+void launch_batch_stage_pair(const BatchArgs& a, int grid, cudaStream_t st) {
+  if (a.mcapa > 0) {   // capacity: the one-interface tile of the same width (255 cells)
+    k_batch_stage<PEuler, CD, 0, PREC, 2 * NTP><<<grid, 2 * NTP, 0, st>>>(a);
+    return;
+  }
+  k_batch_stage_pair<CD, PREC, NTP><<<grid, NTP, 0, st>>>(a);
+}
+template <int CD>
+int batch_blocks_per_sm_pair() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage_pair<CD, PREC, NTP>, NTP, 0);
+  return n;
+}
+
 template <class P, int CD, int TF>
 bool pick_batch_nt(int variant, BatchLaunchers* L) {
+  // variants 0 and 1: one interface per thread, tiles of 127 / 255 cells;
+  // variant 2 (1-D Euler in the FP32 forms): the paired tile of 255 cells
+  if constexpr (SCL_PAIR && std::is_same_v<P, PEuler> && !Prec<PREC>::EXACT && TF == 0 && (CD == 0 || CD == 2)) {
+    if (variant == 2) {
+      L->stage = &launch_batch_stage_pair<CD>;
+      L->begin = &launch_batch_begin<2 * NTP>;
+      L->blocks_per_sm = &batch_blocks_per_sm_pair<CD>;
+      L->nt = NTP;
+      return true;
+    }
+  }
   if (variant == 0) { fill_batch<P, CD, TF, 128>(L); return true; }
   if (variant == 1) { fill_batch<P, CD, TF, 256>(L); return true; }
   return false;

@@ -35,7 +35,7 @@ struct BatchLaunchers {
   int nt;   // threads per CTA = interfaces per tile
 };
 
-constexpr int NBATCH_VARIANTS = 2;   // tile width 128 or 256
+constexpr int NBATCH_VARIANTS = 3;   // tile width 128 or 256; 2: paired 1-D Euler tile (FP32 forms)
 
 bool get_batch_launchers_fp64(int rp, int cd, int tf, int variant, BatchLaunchers* L);
 bool get_batch_launchers_fp64s(int rp, int cd, int tf, int variant, BatchLaunchers* L);

@@ -7,6 +7,7 @@
 // the entropy fix become per-lane selects, entered when either lane needs
 // them.  Used for PEuler, char_decomp 0 or 2, tfluct_solver 0, mixed / FP32.
 #pragma once
+#include "scl_batch.cuh"
 #include "scl_kernels.cuh"
 
 namespace scl {
@@ -410,6 +411,69 @@ __global__ void __launch_bounds__(NT, SCL_PAIR_MINB) k_stage1d_pair(StageArgs a)
     if (tid == 0) {
       atomic_max_nonneg(&ctl->stage_cfl[a.stage], (double)v);
       if (anybad) atomicOr(&ctl->status, SCL_STATUS_NONFINITE);
+    }
+  }
+}
+
+// Batched form: the persistent walk over the active instances' tiles of
+// k_batch_stage, with the paired tile (2NT-1 cells) and one CFL atomic per
+// tile into the tile's own controller.
+template <int CD, int PREC, int NT>
+__global__ void __launch_bounds__(NT, SCL_PAIR_MINB) k_batch_stage_pair(BatchArgs a) {
+  using S = typename Prec<PREC>::S;
+  __shared__ PairSmem<PREC, NT> sm;
+  const int na = *a.nact;
+  if (na == 0) return;
+  const int ntiles = a.prefix[na];
+  const int tid = threadIdx.x;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int lo = 0, hi = na - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (a.prefix[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    const int k = a.active[lo];
+    Ctl* ctl = &a.ctl[k];
+    const long off = a.off[k];
+    Line<S> L;
+    L.ctl = ctl;
+    L.qin = static_cast<const S*>(a.arena[ctl->role[a.sd.in]]) + off;
+    L.qo = a.sd.aux_in >= 0 ? static_cast<const S*>(a.arena[ctl->role[a.sd.aux_in]]) + off : nullptr;
+    L.out = static_cast<S*>(a.arena[ctl->role[a.sd.out]]) + off;
+    L.out2 = a.sd.out2 >= 0 ? static_cast<S*>(a.arena[ctl->role[a.sd.out2]]) + off : nullptr;
+    L.dq_out = nullptr;
+    L.aux = a.aux ? static_cast<const void*>(static_cast<const S*>(a.aux) + a.aoff[k]) : nullptr;
+    L.mx = a.mx[k];
+    L.plane = a.plane[k];
+    L.dx = a.dx[k];
+    L.bl = a.mthbc[0];
+    L.br = a.mthbc[1];
+    L.mcapa = a.mcapa;
+    L.kind = a.sd.kind;
+    L.stage = a.stage;
+    L.ixy = 1;
+    const int c0 = 1 + (t - a.prefix[lo]) * (2 * NT - 1);
+    if (tid == 0) sm.dtdx = ctl->dt / L.dx;
+    for (int j = tid; j < 2 * NT + 5; j += NT) {
+      const long g = (long)c0 - 1 + j;
+      const bool ok = g < (long)L.mx + 6;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) sm.sq[m][j] = ok ? L.qin[(long)m * L.plane + g] : (S)1;
+    }
+    __syncthreads();
+    float cflmax = 0.0f;
+    int bad = 0;
+    pair_compute<CD, PREC, NT>(L, a.ph, c0, &sm.sq[0][0], sm, sm.dtdx, cflmax, bad);
+    cflmax = warp_max(cflmax);
+    if ((tid & 31) == 0) sm.sred[tid >> 5] = cflmax;
+    const int anybad = __syncthreads_or(bad);
+    if (tid < 32) {
+      float v = (tid < NT / 32) ? sm.sred[tid] : 0.0f;
+      v = warp_max(v);
+      if (tid == 0) {
+        atomic_max_nonneg(&ctl->stage_cfl[a.stage], (double)v);
+        if (anybad) atomicOr(&ctl->status, SCL_STATUS_NONFINITE);
+      }
     }
   }
 }

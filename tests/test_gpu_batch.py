@@ -75,19 +75,22 @@ def test_batch_advection_tfluct_strict_and_rerun():
         assert np.array_equal(got[k][:, 3:-3], q2[:, 3:-3])
 
 
+@pytest.mark.parametrize("variant", [-1, 0, 1, 2])
 @pytest.mark.parametrize("precision,tol", [("fp32", 2e-5), ("mixed", 2e-5)])
-def test_batch_euler_reduced_precision(precision, tol):
+def test_batch_euler_reduced_precision(precision, tol, variant):
     mxs = [100, 400, 250]
     probs = _euler_batch(9, mxs)
     ps = S.ClawParams(rp=S.RP_EULER, mx=10, dx=0.1, mthbc=(1, 1), char_decomp=0, tfluct_solver=0,
                       time_integrator=3)
     dt0 = [0.5 * dx / sm for (_, _, dx, sm) in probs]
     with S.Batch(ps, mxs, [p[2] for p in probs], precision=precision) as b:
+        b.select(variant)      # 0, 1: one interface per thread; 2: two (Euler FP32 forms)
         b.set_q([p[1] for p in probs])
         res, _ = b.sharpclaw(0.0, 0.05, dt0, 0.9, 0.8)
         got = b.get_q()
         tune = b.tuning()
     assert tune["threads"] in (128, 256) and tune["grid"] > 0
+    assert variant < 0 or tune["variant"] == variant
     for k, (po, q, dx, sm) in enumerate(probs):
         qo, ro = O.sharpclaw(po, q, None, tstart=0.0, tend=0.05, dt_initial=dt0[k], cfl_max=0.9, cfl_desired=0.8,
                              time_integrator=3)
