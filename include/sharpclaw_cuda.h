@@ -62,7 +62,7 @@ typedef struct scl_params {
   int ndim;             /* 1 or 2                                                  */
   int mx, my;           /* nx(1), nx(2)                                            */
   int meqn, mwaves, mbc, maux, mcapa;
-  int lim_type;         /* 2 = WENO (reconstruct.f90)                              */
+  int lim_type;         /* 2 = WENO5, 1 = second-order TVD (reconstruct.f90)       */
   int char_decomp;      /* 0 weno5, 1 weno5_wave, 2 weno5_char, 3 weno5_trans      */
   int tfluct_solver;    /* 1 tfluct plugin, 0 swap + second rp (flux1.f90:136-188) */
   int mthbc[4];         /* 1 extrapolation, 2 periodic, 3 solid wall               */
@@ -72,6 +72,9 @@ typedef struct scl_params {
   double u, gamma, grav;
   int time_integrator;  /* 1 SSP22, 2 SSP42, 3 SSP33, 4 SSP104 (sharpclaw.f90:159) */
   int precision;        /* SCL_FP64, SCL_FP64_STRICT, SCL_MIXED, SCL_FP32          */
+  int mthlim[4];        /* TVD limiter per component / field / wave (lim_type = 1):
+                           1 minmod, 2 superbee, 3 van Leer, 4 MC, 5 Cada-Torrilhon
+                           (ClawParams%mthlim, reconstruct.f90:551-571)          */
 } scl_params;
 
 /* Arguments of sharpclaw() (src/sharpclaw.f90:2-5). */

@@ -34,6 +34,7 @@ class Params(ctypes.Structure):
         ("xlower", ctypes.c_double), ("ylower", ctypes.c_double),
         ("rp", ctypes.c_int), ("efix", ctypes.c_int),
         ("u", ctypes.c_double), ("gamma", ctypes.c_double), ("grav", ctypes.c_double),
+        ("mthlim", ctypes.c_int * 4),
     ]
 
 
@@ -98,7 +99,7 @@ def _ptr(a):
 
 def make_params(*, ndim=1, mx, my=1, meqn, mwaves, mbc=3, maux=0, mcapa=0, char_decomp=0,
                 tfluct_solver=1, mthbc=(2, 2, 2, 2), dx, dy=1.0, xlower=0.0, ylower=0.0,
-                rp, efix=None, u=1.0, gamma=1.4, grav=1.0, lim_type=2) -> Params:
+                rp, efix=None, u=1.0, gamma=1.4, grav=1.0, lim_type=2, mthlim=(1, 1, 1, 1)) -> Params:
     p = Params()
     p.ndim, p.mx, p.my = ndim, mx, (my if ndim == 2 else 1)
     p.meqn, p.mwaves, p.mbc, p.maux, p.mcapa = meqn, mwaves, mbc, maux, mcapa
@@ -109,6 +110,8 @@ def make_params(*, ndim=1, mx, my=1, meqn, mwaves, mbc=3, maux=0, mcapa=0, char_
     p.rp = rp
     p.efix = (1 if rp == RP_EULER else 0) if efix is None else int(efix)
     p.u, p.gamma, p.grav = u, gamma, grav
+    for k in range(4):
+        p.mthlim[k] = int(mthlim[k]) if k < len(mthlim) else 1
     return p
 
 

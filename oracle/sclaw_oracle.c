@@ -349,6 +349,109 @@ int ocl_weno5_trans(int mx2, int meqn, const double *q, const double *evl,
   return 0;
 }
 
+/* reconstruct.f90:551-571 (the same five limiters at :610-630, :699-719):
+   mthlim 1 minmod, 2 superbee, 3 van Leer, 4 MC, 5 Cada-Torrilhon */
+static double tvd_limiter(int t, double r) {
+  switch (t) {
+    case 1: return dmax1(0.0, dmin1(1.0, r));
+    case 2: return dmax1(dmax1(0.0, dmin1(1.0, 2.0 * r)), dmin1(2.0, r));
+    case 3: return (r + fabs(r)) / (1.0 + fabs(r));
+    case 4: { double c = (1.0 + r) / 2.0; return dmax1(0.0, dmin1(dmin1(c, 2.0), 2.0 * r)); }
+    case 5: {
+      const double beta = 2.0, xgamma = 2.0, alpha = 1.0 / 3.0;
+      double pp = (2.0 + r) / 3.0;
+      double amax = dmax1(dmax1(-alpha * r, 0.0), dmin1(dmin1(beta * r, pp), xgamma));
+      return dmax1(0.0, dmin1(pp, amax));
+    }
+  }
+  return 0.0;
+}
+
+/* reconstruct.f90:525-577, componentwise.  The reference's loop starts with
+   dqm left over from the previous component (unset for the first), which
+   feeds the left state of interface 1; here every cell's dqm is
+   q(i)-q(i-1).  A cell with dqm = 0 gets no slope (the reference's
+   r = dqp/dqm is undefined there). */
+int ocl_tvd2(int mx2, int meqn, const double *q, const int *mthlim, double *ql, double *qr) {
+  for (int m = 1; m <= meqn; ++m)
+    for (int i = 3; i <= mx2 - 2; ++i) {                      /* i = mbc+1 .. mx2-mbc, mbc = 2 */
+      double dqm = R2(q, i, m) - R2(q, i - 1, m);
+      double dqp = R2(q, i + 1, m) - R2(q, i, m);
+      double phi = (dqm != 0.0) ? tvd_limiter(mthlim[m - 1], dqp / dqm) : 0.0;
+      R2(qr, i, m) = R2(q, i, m) + (0.5 * phi) * dqm;
+      R2(ql, i, m) = R2(q, i, m) - (0.5 * phi) * dqm;
+    }
+  return 0;
+}
+
+/* reconstruct.f90:580-651, characteristic-wise */
+int ocl_tvd2_char(int mx2, int meqn, const double *q, const int *mthlim, const double *evl,
+                  const double *evr, double *ql, double *qr) {
+  const double floor14 = (double)1.0e-14f;                    /* :609, a REAL(4) literal */
+  double *dq = (double *)calloc((size_t)mx2 * meqn, sizeof(double));
+  double *u = (double *)calloc((size_t)mx2 * meqn * 2, sizeof(double));
+  if (!dq || !u) { free(dq); free(u); return -3; }
+#define U3(k, mw, sd) u[((k) - 1) + (long)((mw) - 1) * mx2 + (long)((sd) - 1) * mx2 * meqn]
+  for (int m = 1; m <= meqn; ++m)
+    for (int i = 2; i <= mx2; ++i) R2(dq, i, m) = R2(q, i, m) - R2(q, i - 1, m);
+  for (int m = 1; m <= meqn; ++m)
+    for (int m1 = 1; m1 <= 2; ++m1) {
+      const double dim = (m1 == 1) ? 1.0 : -1.0;
+      for (int i = 3; i <= mx2 - 1; ++i) {                     /* :594-603 hh(i, m1-2), hh(i, m1-1) */
+        double ha = 0.0, hb = 0.0;
+        for (int mm = 1; mm <= meqn; ++mm) ha = ha + R3(evl, i, m, mm) * R2(dq, i + m1 - 2, mm);
+        for (int mm = 1; mm <= meqn; ++mm) hb = hb + R3(evl, i, m, mm) * R2(dq, i + m1 - 1, mm);
+        double r = (fabs(ha) > floor14) ? hb / ha : 0.0;
+        U3(i, m, m1) = ((dim * 0.5) * tvd_limiter(mthlim[m - 1], r)) * ha;
+      }
+    }
+  for (int m = 1; m <= meqn; ++m)                              /* :637-646 */
+    for (int i = 3; i <= mx2 - 1; ++i) {
+      R2(qr, i - 1, m) = R2(q, i - 1, m);
+      R2(ql, i, m) = R2(q, i, m);
+      for (int mm = 1; mm <= meqn; ++mm) {
+        R2(qr, i - 1, m) = R2(qr, i - 1, m) + R3(evr, i, m, mm) * U3(i, mm, 1);
+        R2(ql, i, m) = R2(ql, i, m) + R3(evr, i, m, mm) * U3(i, mm, 2);
+      }
+    }
+#undef U3
+  free(dq);
+  free(u);
+  return 0;
+}
+
+/* reconstruct.f90:654-761, wave-based: wave and s from the rp pass on the
+   cell averages (flux1.f90:84-86) */
+int ocl_tvd2_wave(int mx2, int meqn, int mwaves, const double *q, const int *mthlim, const double *wave,
+                  const double *s, double *ql, double *qr) {
+#define W(k, m, mw) R3(wave, k, m, mw)
+  for (int m = 1; m <= meqn; ++m)
+    for (int i = 2; i <= mx2; ++i) {                           /* :673-676 */
+      R2(qr, i - 1, m) = R2(q, i - 1, m);
+      R2(ql, i, m) = R2(q, i, m);
+    }
+  for (int mw = 1; mw <= mwaves; ++mw) {
+    double dotr = 0.0;
+    for (int i = 2; i <= mx2 - 2; ++i) {                       /* i = mbc .. mx2-mbc, mbc = 2 */
+      double wnorm2 = 0.0, dotl = dotr;
+      dotr = 0.0;
+      for (int m = 1; m <= meqn; ++m) {
+        wnorm2 = wnorm2 + W(i, m, mw) * W(i, m, mw);
+        dotr = dotr + W(i, m, mw) * W(i + 1, m, mw);
+      }
+      if (wnorm2 == 0.0) continue;
+      double r = (s[(i - 1) + (long)(mw - 1) * mx2] > 0.0) ? dotl / wnorm2 : dotr / wnorm2;
+      double uu = 0.5 * tvd_limiter(mthlim[mw - 1], r);
+      for (int m = 1; m <= meqn; ++m) {
+        R2(qr, i - 1, m) = R2(qr, i - 1, m) + W(i, m, mw) * uu;
+        R2(ql, i, m) = R2(ql, i, m) - W(i, m, mw) * uu;
+      }
+    }
+  }
+#undef W
+  return 0;
+}
+
 /* reconstruct.f90:146-241 */
 int ocl_weno5_char(int mx2, int meqn, const double *q, const double *evl,
                    const double *evr, double *ql, double *qr) {
@@ -863,7 +966,7 @@ int ocl_flux1(const ocl_params *p, const double *q1d, double *dq1d, const double
   const long ld = mx + 2 * mbc;
   const int mx2 = (int)ld;
   int rc = 0;
-  if (p->lim_type != 2) return -5;
+  if (p->lim_type != 1 && p->lim_type != 2) return -5;
   double dx = (ixy == 1) ? p->dx : p->dy;
   double *dtdx = (double *)calloc((size_t)ld, sizeof(double));
   double *ql = (double *)calloc((size_t)ld * meqn, sizeof(double));
@@ -888,6 +991,20 @@ int ocl_flux1(const ocl_params *p, const double *q1d, double *dq1d, const double
   if (p->ndim > 1)                                                            /* :62 */
     for (long k = 0; k < ld * meqn; ++k) dq1d[k] = 0.0;
 
+  if (p->lim_type == 1) {                                                    /* :78-91 */
+    switch (p->char_decomp) {
+      case 0: rc = ocl_tvd2(mx2, meqn, q1d, p->mthlim, ql, qr); break;
+      case 1:
+        rc = ocl_rp(p, ixy, mx, q1d, q1d, aux1d, aux1d, wave, s, amdq, apdq);
+        if (!rc) rc = ocl_tvd2_wave(mx2, meqn, mwaves, q1d, p->mthlim, wave, s, ql, qr);
+        break;
+      case 2:
+        rc = ocl_evec(p, ixy, mx, q1d, aux1d, aux1d, evl, evr);
+        if (!rc) rc = ocl_tvd2_char(mx2, meqn, q1d, p->mthlim, evl, evr, ql, qr);
+        break;
+      default: rc = -5;
+    }
+  } else
   switch (p->char_decomp) {                                                   /* :92-116 */
     case 0: rc = ocl_weno5(mx2, meqn, q1d, ql, qr); break;
     case 1:                                                                   /* :97-101 */

@@ -39,7 +39,7 @@ typedef struct {
   int ndim;             /* 1 or 2                                  ClawParams%ndim  */
   int mx, my;           /* interior cells                          ClawParams%nx    */
   int meqn, mwaves, mbc, maux, mcapa;
-  int lim_type;         /* only 2 (WENO) is on the path                              */
+  int lim_type;         /* 2 WENO5, 1 TVD (reconstruct.f90:525-763)                  */
   int char_decomp;      /* 0 componentwise, 2 characteristic-wise                   */
   int tfluct_solver;    /* 1: tfluct plugin, 0: swap + second rp                    */
   int mthbc[4];         /* 1 extrap, 2 periodic, 3 wall                              */
@@ -49,6 +49,7 @@ typedef struct {
   double u;             /* advection speed        common /comrp/ u                  */
   double gamma;         /* ratio of specific heats common /param/ gamma,gamma1       */
   double grav;          /* gravity                 common /comrp/ g                  */
+  int mthlim[4];        /* TVD limiter per component/field/wave (lim_type = 1)       */
 } ocl_params;
 
 typedef struct {
@@ -75,6 +76,12 @@ int ocl_weno5(int mx2, int meqn, const double *q, double *ql, double *qr);
    cell averages (flux1.f90:99-100) */
 int ocl_weno5_wave(int mx2, int meqn, int mwaves, const double *q, const double *wave,
                    double *ql, double *qr);
+/* reconstruct.f90:525-761: second-order TVD reconstructions (lim_type = 1) */
+int ocl_tvd2(int mx2, int meqn, const double *q, const int *mthlim, double *ql, double *qr);
+int ocl_tvd2_char(int mx2, int meqn, const double *q, const int *mthlim, const double *evl,
+                  const double *evr, double *ql, double *qr);
+int ocl_tvd2_wave(int mx2, int meqn, int mwaves, const double *q, const int *mthlim, const double *wave,
+                  const double *s, double *ql, double *qr);
 /* reconstruct.f90:244-347 (transmission-based, char_decomp = 3) */
 int ocl_weno5_trans(int mx2, int meqn, const double *q, const double *evl,
                     const double *evr, double *ql, double *qr);

@@ -70,6 +70,7 @@ class ClawParams:
     gamma: float = 1.4
     grav: float = 1.0
     time_integrator: int = 3
+    mthlim: Sequence[int] = field(default_factory=lambda: (1, 1, 1, 1))
 
     def __post_init__(self):
         meqn, mwaves, maux, ndim = PLUGINS.get(self.rp, (None, None, 0, None))
@@ -103,6 +104,8 @@ class ClawParams:
         p.rp, p.efix = self.rp, int(self.efix)
         p.u, p.gamma, p.grav = self.u, self.gamma, self.grav
         p.time_integrator, p.precision = self.time_integrator, precision
+        for k in range(4):
+            p.mthlim[k] = int(self.mthlim[k]) if k < len(self.mthlim) else 1
         return p
 
 

@@ -33,6 +33,7 @@ class scl_params(ctypes.Structure):
         ("rp", ctypes.c_int), ("efix", ctypes.c_int),
         ("u", ctypes.c_double), ("gamma", ctypes.c_double), ("grav", ctypes.c_double),
         ("time_integrator", ctypes.c_int), ("precision", ctypes.c_int),
+        ("mthlim", ctypes.c_int * 4),
     ]
 
 

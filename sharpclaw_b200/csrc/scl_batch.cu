@@ -171,6 +171,7 @@ BatchArgs make_bargs(const scl_batch* b, int s) {
   a.ph.gamma1 = b->p.gamma - 1.0;
   a.ph.grav = b->p.grav;
   a.ph.efix = b->p.efix;
+  for (int k = 0; k < 4; ++k) a.ph.mthlim[k] = b->p.mthlim[k];
   return a;
 }
 
@@ -339,7 +340,8 @@ int scl_batch_create(const scl_params* p, int ninst, const int* mx, const double
   if (!p || !mx || !dx || !out || ninst < 1) return bfail(SCL_E_INVALID, "bad argument");
   *out = nullptr;
   if (p->ndim != 1) return bfail(SCL_E_INVALID, "batched solver takes 1-D problems");
-  if (p->mbc != 3 || p->lim_type != 2) return bfail(SCL_E_INVALID, "need mbc = 3 and lim_type = 2");
+  if (p->mbc != 3 || (p->lim_type != 1 && p->lim_type != 2)) return bfail(SCL_E_INVALID, "need mbc = 3 and lim_type 1 or 2");
+  if (p->char_decomp < 0 || p->char_decomp > (p->lim_type == 2 ? 3 : 2)) return bfail(SCL_E_UNSUPPORTED, "char_decomp out of range");
   if (p->precision < SCL_FP64 || p->precision > SCL_FP32) return bfail(SCL_E_INVALID, "bad precision");
   for (int k = 0; k < 2; ++k)
     if (p->mthbc[k] < 1 || p->mthbc[k] > 3 || (p->mthbc[k] == 3 && p->meqn < 2))
@@ -366,7 +368,9 @@ int scl_batch_create(const scl_params* p, int ninst, const int* mx, const double
   b->nstages = batch_stage_table(p->time_integrator, b->sd, &b->final_role);
   if (!b->nstages) { delete b; return bfail(SCL_E_INVALID, "time_integrator should be between 1 and 4"); }
   for (int v = 0; v < NBATCH_VARIANTS; ++v)
-    if (batch_launchers(p->precision, p->rp, p->char_decomp, p->tfluct_solver, v, &b->L[v])) b->nvariants = v + 1;
+    if (batch_launchers(p->precision, p->rp, p->lim_type == 1 ? 10 + p->char_decomp : p->char_decomp,
+                        p->tfluct_solver, v, &b->L[v]))
+      b->nvariants = v + 1;
   if (b->nvariants == 0) { delete b; return bfail(SCL_E_UNSUPPORTED, "no batched kernel for this plugin / options"); }
   b->mx.assign(mx, mx + ninst);
   b->dx.assign(dx, dx + ninst);

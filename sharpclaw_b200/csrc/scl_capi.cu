@@ -150,6 +150,10 @@ __global__ void k_f32_to_f64(const float* a, double* b, long n) {
     b[k] = (double)a[k];
 }
 
+// Reconstruction code of the stage kernels' CD parameter: char_decomp for
+// WENO5 (lim_type 2), 10 + char_decomp for TVD (lim_type 1).
+int recon_code(const scl_params& p) { return p.lim_type == 1 ? 10 + p.char_decomp : p.char_decomp; }
+
 bool get_launchers(int prec, int rp, int ndim, int cd, int tf, int variant, Launchers* L) {
   switch (prec) {
     case SCL_FP64: return get_launchers_fp64(rp, ndim, cd, tf, variant, L);
@@ -269,6 +273,7 @@ StageArgs make_args(const scl_handle* h, int s) {
   a.ph.gamma1 = h->p.gamma - 1.0;
   a.ph.grav = h->p.grav;
   a.ph.efix = h->p.efix;
+  for (int k = 0; k < 4; ++k) a.ph.mthlim[k] = h->p.mthlim[k];
   return a;
 }
 
@@ -423,9 +428,13 @@ int validate(const scl_params* p) {
   if (p->ndim != 1 && p->ndim != 2) return fail(SCL_E_INVALID, "ndim must be 1 or 2");
   if (p->mbc != 3) return fail(SCL_E_INVALID, "WENO5 requires mbc = 3 (reconstruct.f90:85)");
   if (p->mx < 3 || (p->ndim == 2 && p->my < 3)) return fail(SCL_E_INVALID, "need at least 3 cells per direction");
-  if (p->lim_type != 2) return fail(SCL_E_UNSUPPORTED, "only lim_type = 2 (WENO) is built");
-  if (p->char_decomp < 0 || p->char_decomp > 3)
-    return fail(SCL_E_UNSUPPORTED, "char_decomp must be 0, 1, 2 or 3");
+  if (p->lim_type != 1 && p->lim_type != 2)
+    return fail(SCL_E_UNSUPPORTED, "lim_type must be 1 (TVD) or 2 (WENO5); 0 (polynomial) is not built");
+  if (p->char_decomp < 0 || p->char_decomp > (p->lim_type == 2 ? 3 : 2))
+    return fail(SCL_E_UNSUPPORTED, "char_decomp must be 0..3 with WENO5, 0..2 with TVD (flux1.f90:78-116)");
+  if (p->lim_type == 1)
+    for (int k = 0; k < std::max(p->meqn, p->mwaves) && k < 4; ++k)
+      if (p->mthlim[k] < 1 || p->mthlim[k] > 5) return fail(SCL_E_INVALID, "mthlim must be 1..5 (reconstruct.f90:551-571)");
   if (p->tfluct_solver != 0 && p->tfluct_solver != 1) return fail(SCL_E_INVALID, "tfluct_solver must be 0 or 1");
   for (int k = 0; k < 2 * p->ndim; ++k)
     if (p->mthbc[k] < 1 || p->mthbc[k] > 3)
@@ -478,14 +487,14 @@ int scl_create(const scl_params* p, scl_handle** out) {
   h->rows = p->ndim == 2 ? p->my + 2 * p->mbc : 1;
   h->pitch = (h->ld + 31) / 32 * 32;
   h->plane = h->pitch * h->rows;
-  if (!get_launchers(p->precision, p->rp, p->ndim, p->char_decomp, p->tfluct_solver, 0, &h->LV[0])) {
+  if (!get_launchers(p->precision, p->rp, p->ndim, recon_code(*p), p->tfluct_solver, 0, &h->LV[0])) {
     delete h;
     return fail(SCL_E_UNSUPPORTED, "no kernel for this plugin / char_decomp / tfluct_solver");
   }
   h->L = h->LV[0];
   if (p->ndim == 2)
     while (h->nvariants < N2D_VARIANTS &&
-           get_launchers(p->precision, p->rp, p->ndim, p->char_decomp, p->tfluct_solver, h->nvariants,
+           get_launchers(p->precision, p->rp, p->ndim, recon_code(*p), p->tfluct_solver, h->nvariants,
                          &h->LV[h->nvariants]))
       h->nvariants += 1;
   h->nstages = stage_table(p->time_integrator, h->sd, &h->final_role);
@@ -614,7 +623,7 @@ int scl_flux1(scl_handle* h, const double* q1d, const double* aux1d, double* dq1
   p1.dx = (ixy == 1) ? h->p.dx : h->p.dy;
   p1.mthbc[0] = p1.mthbc[1] = 1;
   Launchers L1{};
-  if (!get_launchers(p1.precision, p1.rp, 1, p1.char_decomp, p1.tfluct_solver, 0, &L1))
+  if (!get_launchers(p1.precision, p1.rp, 1, recon_code(p1), p1.tfluct_solver, 0, &L1))
     return fail(SCL_E_UNSUPPORTED, "no 1-D kernel for this plugin");
   const long ld = mx + 2 * p1.mbc, pitch = (ld + 31) / 32 * 32;
   const size_t ss = h->ssize;
@@ -671,6 +680,7 @@ int scl_flux1(scl_handle* h, const double* q1d, const double* aux1d, double* dq1
     a.mcapa = p1.mcapa;
     a.ph.u = p1.u; a.ph.gamma = p1.gamma; a.ph.gamma1 = p1.gamma - 1.0; a.ph.grav = p1.grav;
     a.ph.efix = p1.efix;
+    for (int k = 0; k < 4; ++k) a.ph.mthlim[k] = p1.mthlim[k];
     L1.stage(a, h->stream);
     if (cudaGetLastError() != cudaSuccess) rc = fail(SCL_E_CUDA, "flux1 launch");
   }
@@ -982,7 +992,7 @@ extern "C" int scl_adjoint_step(scl_handle* h, const double* q_dev, const double
                                 double* lam_out_dev, double dt) {
   if (!h || !q_dev || !lam_in_dev || !lam_out_dev) return fail(SCL_E_INVALID, "null argument");
   const scl_params& p = h->p;
-  if (!adjoint_supported(p.rp, p.ndim, p.char_decomp, p.time_integrator, p.mthbc))
+  if (p.lim_type != 2 || !adjoint_supported(p.rp, p.ndim, p.char_decomp, p.time_integrator, p.mthbc))
     return fail(SCL_E_UNSUPPORTED,
                 "the adjoint covers 2-D acoustics, componentwise WENO5, SSPRK(3,3), periodic bc");
   if (h->ssize != sizeof(double)) return fail(SCL_E_UNSUPPORTED, "the adjoint needs double state");

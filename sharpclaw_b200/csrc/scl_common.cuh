@@ -68,6 +68,7 @@ struct Phys {
   double gamma1;  // gamma - 1
   double grav;    // gravity                apps/shallowWater/2dRadialDam/setprob.f90
   int efix;
+  int mthlim[4];  // TVD limiters (ClawParams%mthlim)
 };
 
 // Arguments of one stage launch (all by value; pointers are device pointers).

@@ -102,11 +102,17 @@ bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
     if (cd == 1 && tf == 0) L->stage = &launch1d<P, 1, 0>;
     if (cd == 2 && tf == 0) L->stage = &launch1d<P, 2, 0>;
     if (cd == 3 && tf == 0) L->stage = &launch1d<P, 3, 0>;
+    if (cd == 10 && tf == 0) L->stage = &launch1d<P, 10, 0>;
+    if (cd == 11 && tf == 0) L->stage = &launch1d<P, 11, 0>;
+    if (cd == 12 && tf == 0) L->stage = &launch1d<P, 12, 0>;
     if constexpr (P::HAS_TFLUCT) {
       if (cd == 0 && tf == 1) L->stage = &launch1d<P, 0, 1>;
       if (cd == 1 && tf == 1) L->stage = &launch1d<P, 1, 1>;
       if (cd == 2 && tf == 1) L->stage = &launch1d<P, 2, 1>;
       if (cd == 3 && tf == 1) L->stage = &launch1d<P, 3, 1>;
+      if (cd == 10 && tf == 1) L->stage = &launch1d<P, 10, 1>;
+      if (cd == 11 && tf == 1) L->stage = &launch1d<P, 11, 1>;
+      if (cd == 12 && tf == 1) L->stage = &launch1d<P, 12, 1>;
     }
     return L->stage != nullptr;
   }
@@ -115,11 +121,17 @@ bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
     if (cd == 1 && tf == 0) return fill2d<P, 1, 0>(variant, L);
     if (cd == 2 && tf == 0) return fill2d<P, 2, 0>(variant, L);
     if (cd == 3 && tf == 0) return fill2d<P, 3, 0>(variant, L);
+    if (cd == 10 && tf == 0) return fill2d<P, 10, 0>(variant, L);
+    if (cd == 11 && tf == 0) return fill2d<P, 11, 0>(variant, L);
+    if (cd == 12 && tf == 0) return fill2d<P, 12, 0>(variant, L);
     if constexpr (P::HAS_TFLUCT) {
       if (cd == 0 && tf == 1) return fill2d<P, 0, 1>(variant, L);
       if (cd == 1 && tf == 1) return fill2d<P, 1, 1>(variant, L);
       if (cd == 2 && tf == 1) return fill2d<P, 2, 1>(variant, L);
       if (cd == 3 && tf == 1) return fill2d<P, 3, 1>(variant, L);
+      if (cd == 10 && tf == 1) return fill2d<P, 10, 1>(variant, L);
+      if (cd == 11 && tf == 1) return fill2d<P, 11, 1>(variant, L);
+      if (cd == 12 && tf == 1) return fill2d<P, 12, 1>(variant, L);
     }
   }
   return false;
@@ -186,11 +198,17 @@ bool pick_batch(int cd, int tf, int variant, BatchLaunchers* L) {
   if (cd == 1 && tf == 0) return pick_batch_nt<P, 1, 0>(variant, L);
   if (cd == 2 && tf == 0) return pick_batch_nt<P, 2, 0>(variant, L);
   if (cd == 3 && tf == 0) return pick_batch_nt<P, 3, 0>(variant, L);
+  if (cd == 10 && tf == 0) return pick_batch_nt<P, 10, 0>(variant, L);
+  if (cd == 11 && tf == 0) return pick_batch_nt<P, 11, 0>(variant, L);
+  if (cd == 12 && tf == 0) return pick_batch_nt<P, 12, 0>(variant, L);
   if constexpr (P::HAS_TFLUCT) {
     if (cd == 0 && tf == 1) return pick_batch_nt<P, 0, 1>(variant, L);
     if (cd == 1 && tf == 1) return pick_batch_nt<P, 1, 1>(variant, L);
     if (cd == 2 && tf == 1) return pick_batch_nt<P, 2, 1>(variant, L);
     if (cd == 3 && tf == 1) return pick_batch_nt<P, 3, 1>(variant, L);
+    if (cd == 10 && tf == 1) return pick_batch_nt<P, 10, 1>(variant, L);
+    if (cd == 11 && tf == 1) return pick_batch_nt<P, 11, 1>(variant, L);
+    if (cd == 12 && tf == 1) return pick_batch_nt<P, 12, 1>(variant, L);
   }
   return false;
 }

@@ -193,6 +193,31 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs, 
         }
       }
       weno5_trans_exact<M, FD>(q, h, evrc, xl, xr);
+    } else if constexpr (CD == 10) {                      // lim_type 1: tvd2
+      tvd2_exact<M>(q, ph.mthlim, xl, xr);
+    } else if constexpr (CD == 11) {                      // lim_type 1: tvd2_wave
+      double w[3][MW][M], sc[MW], ak[4][MA > 0 ? MA : 1];
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int i = 0; i < MA; ++i) ak[j][i] = (double)as(j + 1, i);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {                       // interfaces c-1, c, c+1
+        double dk[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) dk[m] = q[j + 2][m] - q[j + 1][m];
+        P::template waves<double, FD>(ph, ixy, q[j + 1], q[j + 2], dk, ak[j], ak[j + 1], w[j],
+                                      j == 1 ? sc : (double*)nullptr);
+      }
+      tvd2_wave_core<double, M, MW>(w, sc, ph.mthlim, q[2], q[3], xl, xr);
+    } else if constexpr (CD == 12) {                      // lim_type 1: tvd2_char
+      double evl[M][M], evr[M][M], d3[3][M];
+      P::template evec<double, FD>(ph, ixy, q[2], q[3], auxm, aux0, evl, evr);
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int m = 0; m < M; ++m) d3[j][m] = q[j + 2][m] - q[j + 1][m];
+      tvd2_char_core<double, M>(d3, evl, evr, ph.mthlim, q[2], q[3], xl, xr);
     } else {
       weno5_exact<M, FD>(q, xl, xr);
     }
@@ -245,6 +270,36 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs, 
         }
       }
       weno5_trans_offset<M>(d, h, evrc, xl, xr);
+    } else if constexpr (CD == 10) {
+      tvd2_offset<M>(d, ph.mthlim, xl, xr);
+    } else if constexpr (CD == 11) {
+      float qf[4][M], ak[4][MA > 0 ? MA : 1], w[3][MW][M], sc[MW], z[M];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+#pragma unroll
+        for (int m = 0; m < M; ++m) qf[j][m] = (float)qs(j + 1, m);
+#pragma unroll
+        for (int i = 0; i < MA; ++i) ak[j][i] = (float)as(j + 1, i);
+      }
+#pragma unroll
+      for (int m = 0; m < M; ++m) z[m] = 0.0f;
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        P::template waves<float>(ph, ixy, qf[j], qf[j + 1], d[j + 1], ak[j], ak[j + 1], w[j],
+                                 j == 1 ? sc : (float*)nullptr);
+      tvd2_wave_core<float, M, MW>(w, sc, ph.mthlim, z, z, xl, xr);
+    } else if constexpr (CD == 12) {
+      float qm[M], q0[M], evl[M][M], evr[M][M], d3[3][M], z[M];
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        qm[m] = (float)qs(2, m);
+        q0[m] = (float)qs(3, m);
+        z[m] = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) d3[j][m] = d[j + 1][m];
+      }
+      evec_f32<P>(ph, ixy, qm, q0, auxm, aux0, evl, evr);
+      tvd2_char_core<float, M>(d3, evl, evr, ph.mthlim, z, z, xl, xr);
     } else {
       weno5_offset<M>(d, xl, xr);
     }

@@ -47,9 +47,10 @@ struct PAdvection {
   }
   // waves of rp1.f:35 (the jump itself), for the wave-based reconstruction
   template <class R, bool FD = false>
-  __device__ static void waves(const Phys&, int, const R*, const R*, const R* dl, const R*, const R*,
-                               R w[1][1]) {
+  __device__ static void waves(const Phys& ph, int, const R*, const R*, const R* dl, const R*, const R*,
+                               R w[1][1], R* s = nullptr) {
     w[0][0] = dl[0];
+    if (s) s[0] = (R)ph.u;
   }
   template <class R, bool FD = false>
   __device__ static void tfluct(const Phys& ph, int, const R*, const R*, const R* dl, const R*,
@@ -172,9 +173,10 @@ struct PEuler {
 
   template <class R, bool FD = false>
   __device__ static void waves(const Phys& ph, int, const R* L, const R* Rt, const R* dl, const R*,
-                               const R*, R w[3][3]) {
+                               const R*, R w[3][3], R* s = nullptr) {
     R u, enth, a;
     wave_set<R, FD>(ph, L, Rt, dl, u, enth, a, w);
+    if (s) { s[0] = u - a; s[1] = u; s[2] = u + a; }
   }
 
   template <class R, bool FD = false>
@@ -350,9 +352,10 @@ struct PShallow2D {
 
   template <class R, bool FD = false>
   __device__ static void waves(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl, const R*,
-                               const R*, R w[3][3]) {
+                               const R*, R w[3][3], R* s = nullptr) {
     R u, a;
     wave_set<R, FD>(ph, ixy, L, Rt, dl, u, a, w);
+    if (s) { s[0] = u - a; s[1] = u; s[2] = u + a; }
   }
 
   template <class R, bool FD = false>
@@ -474,8 +477,9 @@ struct PAcoustics {
   // the two waves of rp1acv.f:49-60 (zero tangential component in 2-D)
   template <class R, bool FD = false>
   __device__ static void waves(const Phys&, int ixy, const R*, const R*, const R* dl, const R* auxl,
-                               const R* auxr, R w[2][NEQ]) {
+                               const R* auxr, R w[2][NEQ], R* s = nullptr) {
     const int mu = (ixy == 1) ? 1 : 2;
+    if (s) { s[0] = -auxl[1]; s[1] = auxr[1]; }
     R zi = auxr[0];
     R zim = auxl[0];
     R a1, a2;

@@ -418,4 +418,124 @@ __device__ __forceinline__ void weno5_trans_offset(const float d[5][M], const fl
   }
 }
 
+// ---------------------------------------------------------------------------
+// Second-order TVD reconstructions (lim_type = 1, reconstruct.f90:525-761).
+// q[k][m] holds cells c-3+k (only c-2 .. c+1 are read).
+// ---------------------------------------------------------------------------
+// reconstruct.f90:551-571: limiter mthlim = 1 minmod, 2 superbee, 3 van Leer,
+// 4 monotonized centered, 5 Cada & Torrilhon
+template <class T>
+__device__ __forceinline__ T tvd_limiter(int t, T r) {
+  auto mn = [](T a, T b) { return a < b ? a : b; };
+  auto mx = [](T a, T b) { return a > b ? a : b; };
+  switch (t) {
+    case 1: return mx((T)0, mn((T)1, r));
+    case 2: return mx(mx((T)0, mn((T)1, (T)2 * r)), mn((T)2, r));
+    case 3: return (r + fabs(r)) / ((T)1 + fabs(r));
+    case 4: {
+      const T c = ((T)1 + r) / (T)2;
+      return mx((T)0, mn(mn(c, (T)2), (T)2 * r));
+    }
+    case 5: {
+      const T beta = (T)2, xgamma = (T)2, alpha = (T)(1.0 / 3.0);
+      const T pp = ((T)2 + r) / (T)3;
+      const T amax = mx(mx(-alpha * r, (T)0), mn(mn(beta * r, pp), xgamma));
+      return mx((T)0, mn(pp, amax));
+    }
+  }
+  return (T)0;
+}
+
+// tvd2, componentwise (reconstruct.f90:543-574): qr(c-1) from cell c-1,
+// ql(c) from cell c; a cell whose backward jump is 0 gets no slope.
+template <int M>
+__device__ __forceinline__ void tvd2_exact(const double q[6][M], const int* mthlim, double qrl[M], double qlr[M]) {
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    double dqm = q[2][m] - q[1][m], dqp = q[3][m] - q[2][m];
+    double phi = dqm != 0.0 ? tvd_limiter(mthlim[m], dqp / dqm) : 0.0;
+    qrl[m] = q[2][m] + (0.5 * phi) * dqm;
+    dqm = q[3][m] - q[2][m];
+    dqp = q[4][m] - q[3][m];
+    phi = dqm != 0.0 ? tvd_limiter(mthlim[m], dqp / dqm) : 0.0;
+    qlr[m] = q[3][m] - (0.5 * phi) * dqm;
+  }
+}
+
+// offsets er = qr(c-1)-q(c-1), el = ql(c)-q(c) from the jumps d[k] (FP32 forms)
+template <int M>
+__device__ __forceinline__ void tvd2_offset(const float d[5][M], const int* mthlim, float er[M], float el[M]) {
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    float phi = d[1][m] != 0.0f ? tvd_limiter(mthlim[m], d[2][m] / d[1][m]) : 0.0f;
+    er[m] = (0.5f * phi) * d[1][m];
+    phi = d[2][m] != 0.0f ? tvd_limiter(mthlim[m], d[3][m] / d[2][m]) : 0.0f;
+    el[m] = -((0.5f * phi) * d[2][m]);
+  }
+}
+
+// tvd2_char (reconstruct.f90:580-651): jumps at interfaces c-1, c, c+1
+// (d[0..2]) projected on the left eigenvectors of c-1/2; with base = the
+// cell values (exact form) or 0 (offset form).
+template <class T, int M>
+__device__ __forceinline__ void tvd2_char_core(const T d[3][M], const T evl[M][M], const T evr[M][M],
+                                               const int* mthlim, const T* base_r, const T* base_l, T xr[M],
+                                               T xl[M]) {
+  const T floor14 = (T)(double)1.0e-14f;                       // :609, a REAL(4) literal
+  T u1[M], u2[M];
+#pragma unroll
+  for (int p = 0; p < M; ++p) {
+    T h[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      T t = (T)0;
+#pragma unroll
+      for (int m = 0; m < M; ++m) t = t + evl[p][m] * d[k][m];
+      h[k] = t;
+    }
+    T r = fabs(h[0]) > floor14 ? h[1] / h[0] : (T)0;
+    u1[p] = ((T)0.5 * tvd_limiter(mthlim[p], r)) * h[0];
+    r = fabs(h[1]) > floor14 ? h[2] / h[1] : (T)0;
+    u2[p] = ((T)(-0.5) * tvd_limiter(mthlim[p], r)) * h[1];
+  }
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    T a = base_r[m], b = base_l[m];
+#pragma unroll
+    for (int p = 0; p < M; ++p) {
+      a = a + evr[m][p] * u1[p];
+      b = b + evr[m][p] * u2[p];
+    }
+    xr[m] = a;
+    xl[m] = b;
+  }
+}
+
+// tvd2_wave (reconstruct.f90:654-761): waves w[k] at interfaces c-1, c, c+1,
+// speeds s of c-1/2; the same base convention as tvd2_char_core.
+template <class T, int M, int MW>
+__device__ __forceinline__ void tvd2_wave_core(const T w[3][MW][M], const T s[MW], const int* mthlim,
+                                               const T* base_r, const T* base_l, T xr[M], T xl[M]) {
+#pragma unroll
+  for (int m = 0; m < M; ++m) { xr[m] = base_r[m]; xl[m] = base_l[m]; }
+#pragma unroll
+  for (int mw = 0; mw < MW; ++mw) {
+    T wnorm2 = (T)0, dotl = (T)0, dotr = (T)0;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      wnorm2 = wnorm2 + w[1][mw][m] * w[1][mw][m];
+      dotl = dotl + w[0][mw][m] * w[1][mw][m];
+      dotr = dotr + w[1][mw][m] * w[2][mw][m];
+    }
+    if (wnorm2 == (T)0) continue;
+    const T r = s[mw] > (T)0 ? dotl / wnorm2 : dotr / wnorm2;
+    const T uu = (T)0.5 * tvd_limiter(mthlim[mw], r);
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      xr[m] = xr[m] + w[1][mw][m] * uu;
+      xl[m] = xl[m] - w[1][mw][m] * uu;
+    }
+  }
+}
+
 }  // namespace scl

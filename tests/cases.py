@@ -133,3 +133,16 @@ def with_capacity(case, seed=11):
     po.maux, po.mcapa = m, m
     ps.maux, ps.mcapa = m, m
     return po, ps, q, np.ascontiguousarray(aux2)
+
+
+def with_tvd(case, mthlim=(1, 1, 1, 1), char_decomp=0):
+    """Switch a case to the second-order TVD reconstructions (lim_type = 1,
+    reconstruct.f90:525-761) with the given limiters per component / field /
+    wave and char_decomp (0 tvd2, 1 tvd2_wave, 2 tvd2_char)."""
+    po, ps, q, aux = case
+    po.lim_type = ps.lim_type = 1
+    po.char_decomp = ps.char_decomp = char_decomp
+    for k in range(4):
+        po.mthlim[k] = int(mthlim[k])
+    ps.mthlim = tuple(int(v) for v in mthlim)
+    return po, ps, q, aux

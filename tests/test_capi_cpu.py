@@ -39,7 +39,9 @@ def test_version_string():
 @pytest.mark.parametrize("change,code", [
     (dict(mbc=2), C.SCL_E_INVALID),
     (dict(mx=2), C.SCL_E_INVALID),
-    (dict(lim_type=1), C.SCL_E_UNSUPPORTED),
+    (dict(lim_type=0), C.SCL_E_UNSUPPORTED),
+    (dict(lim_type=1, char_decomp=3), C.SCL_E_UNSUPPORTED),
+    (dict(lim_type=1, mthlim=(1, 6, 1, 1)), C.SCL_E_INVALID),
     (dict(char_decomp=4), C.SCL_E_UNSUPPORTED),
     (dict(mthbc=(0, 0)), C.SCL_E_INVALID),
     (dict(mthbc=(2, 1)), C.SCL_E_INVALID),

@@ -51,6 +51,14 @@ STEP_CASES = [
     ("euler_capa_char", lambda: cases.with_capacity(cases.shu_osher(mx=150))),
     ("acoustics1d_capa", lambda: cases.with_capacity(cases.acoustics1d(mx=120))),
     ("sw2d_capa", lambda: cases.with_capacity(cases.radial_dam(n=19))),
+    # second-order TVD reconstructions (lim_type = 1), all five limiters
+    ("advection_tvd2_vanleer", lambda: cases.with_tvd(cases.advection(mx=90), (3, 1, 1, 1), 0)),
+    ("euler_tvd2", lambda: cases.with_tvd(cases.shu_osher(mx=150), (1, 2, 3, 1), 0)),
+    ("euler_tvd2_wave", lambda: cases.with_tvd(cases.riemann(mx=120), (4, 4, 5, 1), 1)),
+    ("euler_tvd2_char", lambda: cases.with_tvd(cases.shu_osher(mx=150), (5, 3, 2, 1), 2)),
+    ("acoustics1d_tvd2_wave", lambda: cases.with_tvd(cases.acoustics1d(mx=100), (2, 4, 1, 1), 1)),
+    ("sw2d_tvd2_char", lambda: cases.with_tvd(cases.radial_dam(n=19), (1, 2, 4, 1), 2)),
+    ("acoustics2d_tvd2", lambda: cases.with_tvd(cases.acoustics2d(n=17, background=0.05), (3, 5, 2, 1), 0)),
 ]
 
 
@@ -131,6 +139,7 @@ RUN_CASES = [
     ("euler_sod_wave_ssp104", lambda: cases.riemann(mx=200, char_decomp=1), 4, dict(tend=0.1, dt_initial=0.001, cfl_max=2.5, cfl_desired=2.45)),
     ("euler_trans_ssp104", lambda: cases.shu_osher(mx=300, char_decomp=3), 4, dict(tend=0.05, dt_initial=0.001, cfl_max=2.5, cfl_desired=2.45)),
     ("sw2d_capa_ssp33", lambda: cases.with_capacity(cases.radial_dam(n=21)), 3, dict(tend=0.2, dt_initial=0.01, cfl_max=0.9, cfl_desired=0.8)),
+    ("euler_tvd2_char_ssp33", lambda: cases.with_tvd(cases.shu_osher(mx=160), (4, 4, 4, 1), 2), 3, dict(tend=0.05, dt_initial=0.002, cfl_max=0.9, cfl_desired=0.8)),
 ]
 
 
@@ -182,7 +191,7 @@ def test_nonfinite_is_reported():
     assert r["status"] & S._capi.STATUS_NONFINITE
 
 
-@pytest.mark.parametrize("case", ["shu_osher_char", "sod_wave", "shu_osher_trans"])
+@pytest.mark.parametrize("case", ["shu_osher_char", "sod_wave", "shu_osher_trans", "shu_osher_tvd2_char"])
 @pytest.mark.parametrize("precision,tol", [("mixed", 2e-5), ("fp32", 2e-5)])
 def test_reduced_precision_error(precision, tol, case):
     """FP32 reconstruction/Riemann solves against the FP64 oracle: relative L1
@@ -194,6 +203,8 @@ def test_reduced_precision_error(precision, tol, case):
         po, ps, q, aux = cases.shu_osher(mx=400)
     elif case == "shu_osher_trans":
         po, ps, q, aux = cases.shu_osher(mx=400, char_decomp=3)
+    elif case == "shu_osher_tvd2_char":
+        po, ps, q, aux = cases.with_tvd(cases.shu_osher(mx=400), (4, 4, 4, 1), 2)
     else:
         po, ps, q, aux = cases.riemann(mx=400, char_decomp=1)
     ps.time_integrator = 4
