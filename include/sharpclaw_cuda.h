@@ -49,6 +49,12 @@ extern "C" {
 #define SCL_RP_SW2D 3         /* apps/shallowWater/2dRadialDam/{rpn2sw.f,tfluct1sw.f} (+evec) */
 #define SCL_RP_ACOUSTICS1D 4  /* apps/acoustics/1d/interface/{rp1acv.f,tfluct1acv.f,evec.f90} */
 #define SCL_RP_ACOUSTICS2D 5  /* 2-D variable-coefficient acoustics rpn2/tfluct/evec (new)    */
+#define SCL_RP_ADVECTION2D 6  /* apps/advection/2d/swirl/rpn2ad1.f: edge velocities in aux      */
+
+/* ---- b4step hooks (src/b4step.f90 and the apps' own, run on the device) - */
+#define SCL_B4STEP_NONE 0     /* src/b4step.f90: no-op                                      */
+#define SCL_B4STEP_SWIRL 1    /* apps/advection/2d/swirl/b4step.f90: aux = aux0 *
+                                 cos(2 pi (t + dt/2) / tperiod); no-op for tperiod = 0     */
 
 /* ---- arithmetic ---------------------------------------------------------- */
 #define SCL_FP64 0         /* plain FP64 (FMA contraction allowed)                       */
@@ -172,6 +178,12 @@ int scl_wait_frames(scl_handle* h);
  * no GPU).  aux may be NULL when write_aux == 0 or maux == 0. */
 int scl_format_frame(const scl_params* p, const double* q, const double* aux, double t, int iframe,
                      const char* dir, int write_aux);
+
+/* Select the b4step hook that scl_sharpclaw / scl_time_steps run on the
+ * device before every new (not retaken) time step, as sharpclaw.f90:129 calls
+ * b4step; param is the hook's constant (SCL_B4STEP_SWIRL: tperiod).  The aux
+ * set by scl_set_aux (now or later) is the hook's base field aux0. */
+int scl_set_b4step(scl_handle* h, int kind, double param);
 
 /* Tile shape of the fused 2-D stage kernel (no counterpart in the reference;
  * flux2.f90 sweeps whole lines).  Shapes: 0 = 16x7 cells on 128 threads,

@@ -20,7 +20,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "libsclaw_oracle.so")
 
-RP_ADVECTION, RP_EULER, RP_SW2D, RP_ACOUSTICS1D, RP_ACOUSTICS2D = 1, 2, 3, 4, 5
+RP_ADVECTION, RP_EULER, RP_SW2D, RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION2D = 1, 2, 3, 4, 5, 6
 
 
 class Params(ctypes.Structure):
@@ -35,6 +35,7 @@ class Params(ctypes.Structure):
         ("rp", ctypes.c_int), ("efix", ctypes.c_int),
         ("u", ctypes.c_double), ("gamma", ctypes.c_double), ("grav", ctypes.c_double),
         ("mthlim", ctypes.c_int * 4),
+        ("b4step", ctypes.c_int), ("tperiod", ctypes.c_double),
     ]
 
 

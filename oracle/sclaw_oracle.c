@@ -536,6 +536,20 @@ static void rp_advection(const ocl_params *p, int mx, const double *ql, const do
   }
 }
 
+/* apps/advection/2d/swirl/rpn2ad1.f:39-45: speed auxl(i,ixy), the edge
+   velocity stored with the right cell of interface i-1/2 */
+static void rp_advedge(const ocl_params *p, int ixy, int mx, const double *ql, const double *qr,
+                       const double *auxl, double *wave, double *s, double *amdq, double *apdq) {
+  const int mbc = p->mbc, meqn = p->meqn;
+  const long ld = mx + 2 * mbc;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    L3(wave, i, 1, 1) = L2(ql, i, 1) - L2(qr, i - 1, 1);
+    L2(s, i, 1) = L2(auxl, i, ixy);
+    L2(amdq, i, 1) = dmin1(L2(auxl, i, ixy), 0.0) * L3(wave, i, 1, 1);
+    L2(apdq, i, 1) = dmax1(L2(auxl, i, ixy), 0.0) * L3(wave, i, 1, 1);
+  }
+}
+
 /* apps/advection/1d/tfluct1.f:78-87 */
 static void tfluct_advection(const ocl_params *p, int mx, const double *ql, const double *qr,
                              double *s, double *adq) {
@@ -912,6 +926,7 @@ int ocl_rp(const ocl_params *p, int ixy, int mx, const double *ql, const double 
            double *amdq, double *apdq) {
   switch (p->rp) {
     case OCL_RP_ADVECTION: rp_advection(p, mx, ql, qr, wave, s, amdq, apdq); return 0;
+    case OCL_RP_ADVECTION2D: rp_advedge(p, ixy, mx, ql, qr, auxl, wave, s, amdq, apdq); return 0;
     case OCL_RP_EULER: rp_euler(p, mx, ql, qr, wave, s, amdq, apdq); return 0;
     case OCL_RP_SW2D: rp_sw(p, ixy, mx, ql, qr, wave, s, amdq, apdq, 0); return 0;
     case OCL_RP_ACOUSTICS1D:
@@ -948,7 +963,8 @@ int ocl_evec(const ocl_params *p, int ixy, int mx, const double *q, const double
              const double *auxr, double *evl, double *evr) {
   (void)auxr;
   switch (p->rp) {
-    case OCL_RP_ADVECTION: evec_advection(p, mx, evl, evr); return 0;
+    case OCL_RP_ADVECTION:
+    case OCL_RP_ADVECTION2D: evec_advection(p, mx, evl, evr); return 0;
     case OCL_RP_EULER: evec_euler(p, mx, q, evl, evr); return 0;
     case OCL_RP_SW2D: evec_sw(p, ixy, mx, q, evl, evr); return 0;
     case OCL_RP_ACOUSTICS1D:
@@ -1207,9 +1223,28 @@ out:
 /* ======================================================================== */
 /* src/sharpclaw.f90:2-243 driver                                            */
 /* ======================================================================== */
-int ocl_sharpclaw(const ocl_params *p, const ocl_run *run, double *q, const double *aux,
+/* apps/advection/2d/swirl/b4step.f90: aux = aux0 * cos(pi2 (time + dt/2) / tperiod),
+   aux0 the stream-function velocities setaux.f computes (the app recomputes
+   them each call; identical values) */
+static void b4step_swirl(const ocl_params *p, const double *aux0, double *aux, long n, double time, double dt) {
+  if (p->tperiod == 0.0) return;
+  const double pi2 = 2.0 * (4.0 * atan(1.0));
+  const double vt = cos(pi2 * (time + dt / 2.0) / p->tperiod);
+  for (long k = 0; k < n; ++k) aux[k] = vt * aux0[k];
+}
+
+int ocl_sharpclaw(const ocl_params *p, const ocl_run *run, double *q, const double *aux_in,
                   ocl_result *res) {
   const long n = ocl_plane(p) * p->meqn;
+  const long na = ocl_plane(p) * (p->maux > 0 ? p->maux : 1);
+  double *auxw = NULL;          /* the hook's working aux */
+  const double *aux = aux_in;
+  if (p->b4step == 1 && aux_in) {
+    auxw = (double *)malloc(sizeof(double) * (size_t)na);
+    if (!auxw) return -3;
+    memcpy(auxw, aux_in, sizeof(double) * (size_t)na);
+    aux = auxw;
+  }
   double tstart = run->tstart, tend = run->tend;
   double t = tstart, told = tstart, dt = run->dt_initial, cfl = 0.0, cflmax = 0.0;
   double dtmin = dt, dtmax = dt;
@@ -1219,17 +1254,17 @@ int ocl_sharpclaw(const ocl_params *p, const ocl_run *run, double *q, const doub
     if (tend < tstart) maxn = 1;
     else {
       maxn = (int)((tend - tstart + 1e-10) / dt);
-      if (fabs(maxn * dt - (tend - tstart)) > 1e-5 * (tend - tstart)) { res->info = 2; return 0; }
+      if (fabs(maxn * dt - (tend - tstart)) > 1e-5 * (tend - tstart)) { res->info = 2; free(auxw); return 0; }
     }
   }
-  if (run->dt_variable == 1 && run->cfl_desired > run->cfl_max) { res->info = 3; return 0; }
+  if (run->dt_variable == 1 && run->cfl_desired > run->cfl_max) { res->info = 3; free(auxw); return 0; }
   double *qold = (double *)malloc(sizeof(double) * (size_t)n);
-  if (!qold) return -3;
+  if (!qold) { free(auxw); return -3; }
   for (int it = 1; it <= maxn; ++it) {                                          /* :118-222 */
     if (!retake) {
       told = t;
       if (told + dt > tend && tstart < tend) dt = tend - told;
-      /* b4step: default no-op (src/b4step.f90) */
+      if (auxw) b4step_swirl(p, aux_in, auxw, na, told, dt);                 /* :129 */
       memcpy(qold, q, sizeof(double) * (size_t)n);
     }
     retake = 0;
@@ -1259,6 +1294,7 @@ int ocl_sharpclaw(const ocl_params *p, const ocl_run *run, double *q, const doub
     if (t >= tend) break;
   }
   free(qold);
+  free(auxw);
   if (rc) return rc;
   if (run->dt_variable == 1 && t < tend && steps == maxn) info = 11;           /* :225 */
   if (run->dt_variable == 0 && cflmax > run->cfl_max) info = 12;               /* :228 */

@@ -32,7 +32,8 @@ enum {
   OCL_RP_EULER = 2,         /* apps/euler/shockentropy/rp1eu.f + new Roe evec          */
   OCL_RP_SW2D = 3,          /* apps/shallowWater/2dRadialDam/{rpn2sw.f,tfluct1sw.f}   */
   OCL_RP_ACOUSTICS1D = 4,   /* apps/acoustics/1d/interface/{rp1acv,tfluct1acv,evec}   */
-  OCL_RP_ACOUSTICS2D = 5    /* new 2-D variable-coefficient acoustics rpn2/tfluct/evec */
+  OCL_RP_ACOUSTICS2D = 5,   /* new 2-D variable-coefficient acoustics rpn2/tfluct/evec */
+  OCL_RP_ADVECTION2D = 6    /* apps/advection/2d/swirl/rpn2ad1.f (edge velocities)     */
 };
 
 typedef struct {
@@ -50,6 +51,8 @@ typedef struct {
   double gamma;         /* ratio of specific heats common /param/ gamma,gamma1       */
   double grav;          /* gravity                 common /comrp/ g                  */
   int mthlim[4];        /* TVD limiter per component/field/wave (lim_type = 1)       */
+  int b4step;           /* 0 src/b4step.f90 (no-op), 1 apps/advection/2d/swirl        */
+  double tperiod;       /* swirl: common /comvt/ tperiod                              */
 } ocl_params;
 
 typedef struct {

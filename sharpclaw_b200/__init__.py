@@ -28,11 +28,12 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _capi as C
-from ._capi import (FP32, FP64, FP64_STRICT, MIXED, RP_ACOUSTICS1D, RP_ACOUSTICS2D,  # noqa: F401
-                    RP_ADVECTION, RP_EULER, RP_SW2D, SharpClawError)
+from ._capi import (B4STEP_NONE, B4STEP_SWIRL, FP32, FP64, FP64_STRICT, MIXED,  # noqa: F401
+                    RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION, RP_ADVECTION2D, RP_EULER, RP_SW2D,
+                    SharpClawError)
 
 __all__ = ["ClawParams", "Solver", "Batch", "sharpclaw", "SharpClawError", "RP_ADVECTION", "RP_EULER",
-           "RP_SW2D", "RP_ACOUSTICS1D", "RP_ACOUSTICS2D"]
+           "RP_SW2D", "RP_ACOUSTICS1D", "RP_ACOUSTICS2D", "RP_ADVECTION2D", "B4STEP_NONE", "B4STEP_SWIRL"]
 
 # plugin id -> (meqn, mwaves, maux, ndim)
 PLUGINS = {
@@ -41,6 +42,7 @@ PLUGINS = {
     RP_SW2D: (3, 3, 0, 2),
     RP_ACOUSTICS1D: (2, 2, 2, 1),
     RP_ACOUSTICS2D: (3, 2, 2, 2),
+    RP_ADVECTION2D: (1, 1, 2, 2),
 }
 
 
@@ -252,6 +254,12 @@ class Solver:
         d = None if dir is None else os.fsencode(dir)
         C.check(C.lib().scl_write_frame(self._h, float(t), int(iframe), d, int(bool(write_aux))),
                 "scl_write_frame")
+
+    def set_b4step(self, kind: int, param: float = 0.0):
+        """Run a b4step hook on the device before every new time step of
+        sharpclaw() (B4STEP_SWIRL: param = tperiod); the aux set with set_aux
+        is the hook's base field."""
+        C.check(C.lib().scl_set_b4step(self._h, int(kind), float(param)), "scl_set_b4step")
 
     def wait_frames(self):
         C.check(C.lib().scl_wait_frames(self._h), "scl_wait_frames")

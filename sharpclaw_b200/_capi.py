@@ -13,7 +13,8 @@ LIB_PATH = os.path.join(HERE, "libsharpclaw_b200.so")
 
 SCL_OK, SCL_E_INVALID, SCL_E_CUDA, SCL_E_UNSUPPORTED, SCL_E_NONFINITE, SCL_E_TIMEOUT, SCL_E_IO = \
     0, -1, -2, -3, -4, -5, -6
-RP_ADVECTION, RP_EULER, RP_SW2D, RP_ACOUSTICS1D, RP_ACOUSTICS2D = 1, 2, 3, 4, 5
+RP_ADVECTION, RP_EULER, RP_SW2D, RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION2D = 1, 2, 3, 4, 5, 6
+B4STEP_NONE, B4STEP_SWIRL = 0, 1
 FP64, FP64_STRICT, MIXED, FP32 = 0, 1, 2, 3
 INFO_DT_NOT_DIVIDING, INFO_CFL_DESIRED_GT_MAX, INFO_TOO_MANY_STEPS, INFO_CFL_FIXED_DT, INFO_NONFINITE = 2, 3, 11, 12, 20
 STATUS_NONFINITE, STATUS_TIMEOUT, STATUS_BOUNDS = 1, 2, 4
@@ -77,6 +78,7 @@ SIGNATURES = [
                                         ctypes.POINTER(ctypes.c_longlong)]),
     ("scl_kernels_per_step", ctypes.c_int, [_h]),
     ("scl_select_tiles", ctypes.c_int, [_h, ctypes.c_int]),
+    ("scl_set_b4step", ctypes.c_int, [_h, ctypes.c_int, ctypes.c_double]),
     ("scl_write_frame", ctypes.c_int, [_h, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
     ("scl_wait_frames", ctypes.c_int, [_h]),
     ("scl_format_frame", ctypes.c_int, [ctypes.POINTER(scl_params), _dp, _dp, ctypes.c_double, ctypes.c_int,

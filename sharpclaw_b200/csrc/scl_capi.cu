@@ -42,6 +42,7 @@ __global__ void k_begin_step(Ctl* c) {
   if (c->done) return;
   if (c->n_iter >= c->maxn) { c->done = 1; return; }   // do n=1,maxn exhausted
   c->n_iter += 1;
+  c->fresh = !c->retake;                                             // b4step runs on new steps only
   if (!c->retake) {
     c->told = c->t;                                                  // :120
     if (c->told + c->dt > c->tend && c->tstart < c->tend) c->dt = c->tend - c->told;  // :124
@@ -101,6 +102,18 @@ __global__ void k_end_step(Ctl* c, int last_stage, int final_role) {
   }
   c->steps_taken += 1;                                              // :219
   if (c->t >= c->tend) c->done = 1;                                 // :220
+}
+
+// b4step of apps/advection/2d/swirl/b4step.f90 on the device: before a new
+// step, aux = aux0 * cos(2 pi (told + dt/2) / tperiod) over every cell,
+// ghost cells included (the app rebuilds aux0 from its stream function).
+template <class S>
+__global__ void k_b4step_swirl(const Ctl* c, S* aux, const S* aux0, long n, double tperiod) {
+  if (c->done || !c->fresh || tperiod == 0.0) return;
+  const double pi2 = 2.0 * 3.141592653589793;                       // setprob.f: 2*(4*datan(1))
+  const double vt = cos(pi2 * (c->told + c->dt / 2.0) / tperiod);
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
+    aux[k] = (S)(vt * (double)aux0[k]);
 }
 
 // bc1.f90 on device (initial fill after an upload); one thread per (m, ibc)
@@ -247,6 +260,10 @@ struct scl_handle {
   std::thread fthread;
   int frc = SCL_OK;
   std::string ferr;
+  // b4step hook: kind, its constant, the base aux field it scales
+  int b4kind = SCL_B4STEP_NONE;
+  double b4param = 0.0;
+  void* aux0 = nullptr;
 };
 
 namespace {
@@ -300,6 +317,15 @@ int enqueue_stages(scl_handle* h) {
 
 int enqueue_step(scl_handle* h) {
   k_begin_step<<<1, 1, 0, h->stream>>>(h->ctl);
+  if (h->b4kind == SCL_B4STEP_SWIRL) {
+    const long n = h->plane * h->p.maux;
+    if (h->ssize == sizeof(double))
+      k_b4step_swirl<double><<<148, 256, 0, h->stream>>>(h->ctl, static_cast<double*>(h->aux),
+                                                         static_cast<const double*>(h->aux0), n, h->b4param);
+    else
+      k_b4step_swirl<float><<<148, 256, 0, h->stream>>>(h->ctl, static_cast<float*>(h->aux),
+                                                        static_cast<const float*>(h->aux0), n, h->b4param);
+  }
   int rc = enqueue_stages(h);
   if (rc) return rc;
   k_end_step<<<1, 1, 0, h->stream>>>(h->ctl, h->nstages - 1, h->final_role);
@@ -307,7 +333,9 @@ int enqueue_step(scl_handle* h) {
   return SCL_OK;
 }
 
-int kernels_per_step(const scl_handle* h) { return h->nstages + 2 + (h->L.ghost ? 1 : 0); }
+int kernels_per_step(const scl_handle* h) {
+  return h->nstages + 2 + (h->L.ghost ? 1 : 0) + (h->b4kind != SCL_B4STEP_NONE ? 1 : 0);
+}
 
 // Capture `steps` controller steps (begin, stages, end) into one executable
 // graph; rebuilt only when a different step count is asked for.
@@ -451,7 +479,8 @@ int validate(const scl_params* p) {
   if (!(p->dx > 0) || (p->ndim == 2 && !(p->dy > 0))) return fail(SCL_E_INVALID, "dx, dy must be > 0");
   struct { int rp, meqn, mwaves, maux, ndim; } tab[] = {
       {SCL_RP_ADVECTION, 1, 1, 0, 1}, {SCL_RP_EULER, 3, 3, 0, 1}, {SCL_RP_SW2D, 3, 3, 0, 2},
-      {SCL_RP_ACOUSTICS1D, 2, 2, 2, 1}, {SCL_RP_ACOUSTICS2D, 3, 2, 2, 2}};
+      {SCL_RP_ACOUSTICS1D, 2, 2, 2, 1}, {SCL_RP_ACOUSTICS2D, 3, 2, 2, 2},
+      {SCL_RP_ADVECTION2D, 1, 1, 2, 2}};
   for (auto& t : tab)
     if (t.rp == p->rp) {
       if (p->meqn != t.meqn || p->mwaves != t.mwaves)
@@ -541,6 +570,7 @@ int scl_destroy(scl_handle* h) {
   if (h->aux) cudaFree(h->aux);
   if (h->stage64) cudaFree(h->stage64);
   if (h->adj) cudaFree(h->adj);
+  if (h->aux0) cudaFree(h->aux0);
   if (h->ctl) cudaFree(h->ctl);
   if (h->hctl) cudaFreeHost(h->hctl);
   if (h->hdone) cudaFreeHost(h->hdone);
@@ -577,7 +607,27 @@ int scl_set_aux(scl_handle* h, const double* aux) {
   if (h->p.maux == 0) return SCL_OK;
   int rc = upload_field(h, h->aux, aux, h->p.maux, false);
   if (rc) return rc;
+  if (h->aux0)   // the b4step hook's base field follows the aux the caller sets
+    CK(cudaMemcpyAsync(h->aux0, h->aux, h->ssize * h->plane * h->p.maux, cudaMemcpyDeviceToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  return SCL_OK;
+}
+
+int scl_set_b4step(scl_handle* h, int kind, double param) {
+  if (!h) return fail(SCL_E_INVALID, "null handle");
+  if (kind != SCL_B4STEP_NONE && kind != SCL_B4STEP_SWIRL) return fail(SCL_E_UNSUPPORTED, "unknown b4step hook");
+  if (kind == SCL_B4STEP_SWIRL && (h->p.rp != SCL_RP_ADVECTION2D || h->p.maux < 2))
+    return fail(SCL_E_INVALID, "the swirl b4step scales the edge velocities of SCL_RP_ADVECTION2D");
+  CK(cudaStreamSynchronize(h->stream));
+  if (kind != SCL_B4STEP_NONE && !h->aux0) {
+    const size_t bytes = h->ssize * h->plane * h->p.maux;
+    CK(cudaMalloc(&h->aux0, bytes));
+    CK(cudaMemcpyAsync(h->aux0, h->aux, bytes, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  h->b4kind = kind;
+  h->b4param = param;
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }   // captured steps change
   return SCL_OK;
 }
 

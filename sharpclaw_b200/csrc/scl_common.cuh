@@ -58,7 +58,8 @@ struct __align__(16) Ctl {
   int retake, done, info, dt_variable;
   int status;                   // OR of SCL_STATUS_* raised by kernels
   int accept_always;            // single-step mode (scl_rk_step): no dt update, always accept
-  int pad[2];
+  int fresh;                    // 1: the current step is a new one (b4step runs), 0: a retake
+  int pad;
 };
 
 // Physics constants of the plugins (COMMON blocks /comrp/, /param/).

@@ -451,6 +451,39 @@ struct PShallow2D {
 };
 
 // ------------------------------------------------------------------------
+// 2-D advection with edge velocities (apps/advection/2d/swirl/rpn2ad1.f:
+// 39-45): aux(i,j,1) = u on the left edge, aux(i,j,2) = v on the bottom edge
+// of cell (i,j); the speed at interface i-1/2 along ixy is aux(i,ixy) of the
+// right cell.  No tfluct exists (the app runs the swapped second solve).
+// ------------------------------------------------------------------------
+struct PAdvEdge2D {
+  static constexpr int MEQN = 1, MWAVES = 1, MAUX = 2, NDIM = 2;
+  static constexpr bool HAS_TFLUCT = false;
+  template <class R, bool FD = false>
+  __device__ static void rp(const Phys&, int ixy, const R*, const R*, const R* dl, const R*,
+                            const R* auxr, R* s, R* amdq, R* apdq) {
+    const R u = auxr[ixy - 1];
+    s[0] = u;
+    amdq[0] = rmin(u, (R)0) * dl[0];
+    apdq[0] = rmax(u, (R)0) * dl[0];
+  }
+  template <class R, bool FD = false>
+  __device__ static void waves(const Phys&, int ixy, const R*, const R*, const R* dl, const R*,
+                               const R* auxr, R w[1][1], R* s = nullptr) {
+    w[0][0] = dl[0];
+    if (s) s[0] = auxr[ixy - 1];
+  }
+  template <class R, bool FD = false>
+  __device__ static void tfluct(const Phys&, int, const R*, const R*, const R*, const R*, R*) {}
+  template <class R, bool FD = false>
+  __device__ static void evec(const Phys&, int, const R*, const R*, const R*, const R*,
+                              R evl[1][1], R evr[1][1]) {
+    evl[0][0] = (R)1;
+    evr[0][0] = (R)1;
+  }
+};
+
+// ------------------------------------------------------------------------
 // Variable-coefficient acoustics, aux(:,1) = impedance Z, aux(:,2) = c.
 // 1-D: apps/acoustics/1d/interface/rp1acv.f:49-80, tfluct1acv.f:134-166,
 // evec.f90:196-206.  2-D (new): the same solve normal to the slice

@@ -146,3 +146,26 @@ def with_tvd(case, mthlim=(1, 1, 1, 1), char_decomp=0):
         po.mthlim[k] = int(mthlim[k])
     ps.mthlim = tuple(int(v) for v in mthlim)
     return po, ps, q, aux
+
+
+def swirl(n=40, tperiod=0.0, char_decomp=0):
+    """apps/advection/2d/swirl: [0,1]^2, extrapolation bc, edge velocities
+    from the stream function psi = sin^2(pi x) sin^2(pi y)/pi (setaux.f,
+    ghost cells included), q = 1 for x < 0.5 else 0 (qinit.f90), WENO5, the
+    swapped second solve (tfluct_solver 0); b4step scales the velocities by
+    cos(2 pi (t + dt/2)/tperiod) when tperiod > 0."""
+    d = 1.0 / n
+    pi = 4.0 * np.arctan(1.0)
+    psi = lambda x, y: (np.sin(pi * x) * np.sin(pi * x)) * (np.sin(pi * y) * np.sin(pi * y)) / pi
+    idx = np.arange(-2, n + 4)                       # cells 1-mbc .. n+mbc
+    XL, YL = np.meshgrid((idx - 1) * d, (idx - 1) * d, indexing="xy")
+    aux = np.stack([-(psi(XL, YL + d) - psi(XL, YL)) / d, (psi(XL + d, YL) - psi(XL, YL)) / d])
+    q = np.zeros((1, n + 6, n + 6))
+    xc = (np.arange(1, n + 1) - 0.5) * d
+    q[0, 3:-3, 3:-3] = np.where(xc[None, :] < 0.5, 1.0, 0.0) * np.ones((n, 1))
+    kw = dict(mx=n, my=n, dx=d, dy=d, mthbc=(1, 1, 1, 1), char_decomp=char_decomp, tfluct_solver=0)
+    po = O.make_params(ndim=2, meqn=1, mwaves=1, maux=2, rp=O.RP_ADVECTION2D, **kw)
+    po.b4step = 1 if tperiod > 0 else 0
+    po.tperiod = tperiod
+    ps = S.ClawParams(rp=S.RP_ADVECTION2D, **kw)
+    return po, ps, q, np.ascontiguousarray(aux)

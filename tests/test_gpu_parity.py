@@ -59,6 +59,9 @@ STEP_CASES = [
     ("acoustics1d_tvd2_wave", lambda: cases.with_tvd(cases.acoustics1d(mx=100), (2, 4, 1, 1), 1)),
     ("sw2d_tvd2_char", lambda: cases.with_tvd(cases.radial_dam(n=19), (1, 2, 4, 1), 2)),
     ("acoustics2d_tvd2", lambda: cases.with_tvd(cases.acoustics2d(n=17, background=0.05), (3, 5, 2, 1), 0)),
+    # apps/advection/2d/swirl: edge-velocity advection (rpn2ad1.f)
+    ("swirl", lambda: cases.swirl(n=27)),
+    ("swirl_tvd2_wave", lambda: cases.with_tvd(cases.swirl(n=21), (5, 1, 1, 1), 1)),
 ]
 
 
@@ -139,6 +142,7 @@ RUN_CASES = [
     ("euler_sod_wave_ssp104", lambda: cases.riemann(mx=200, char_decomp=1), 4, dict(tend=0.1, dt_initial=0.001, cfl_max=2.5, cfl_desired=2.45)),
     ("euler_trans_ssp104", lambda: cases.shu_osher(mx=300, char_decomp=3), 4, dict(tend=0.05, dt_initial=0.001, cfl_max=2.5, cfl_desired=2.45)),
     ("sw2d_capa_ssp33", lambda: cases.with_capacity(cases.radial_dam(n=21)), 3, dict(tend=0.2, dt_initial=0.01, cfl_max=0.9, cfl_desired=0.8)),
+    ("swirl_ssp104", lambda: cases.swirl(n=32), 4, dict(tend=0.6, dt_initial=0.01, cfl_max=2.5, cfl_desired=2.45)),
     ("euler_tvd2_char_ssp33", lambda: cases.with_tvd(cases.shu_osher(mx=160), (4, 4, 4, 1), 2), 3, dict(tend=0.05, dt_initial=0.002, cfl_max=0.9, cfl_desired=0.8)),
 ]
 
@@ -217,3 +221,28 @@ def test_reduced_precision_error(precision, tol, case):
     for m in range(3):
         rel = np.abs(qg[m, 3:-3] - qo[m, 3:-3]).sum() / np.abs(qo[m, 3:-3]).sum()
         assert rel <= tol, (m, rel)
+
+
+def test_swirl_b4step_run():
+    """apps/advection/2d/swirl with its b4step (time-periodic velocities), run
+    on the device: agrees with the oracle to the last few bits (the device
+    cosine and the host libm cosine may differ by an ulp), and differs from
+    the run without the hook."""
+    po, ps, q, aux = cases.swirl(n=32, tperiod=0.5)
+    ps.time_integrator = 4
+    run = dict(tend=0.6, dt_initial=0.01, cfl_max=2.5, cfl_desired=2.45)
+    qo, ro = O.sharpclaw(po, q, aux, tstart=0.0, time_integrator=4, **run)
+    with S.Solver(ps, "fp64_strict") as s:
+        s.set_aux(aux)
+        s.set_b4step(S.B4STEP_SWIRL, 0.5)
+        s.set_q(q)
+        res = s.sharpclaw(0.0, run["tend"], run["dt_initial"], run["cfl_max"], run["cfl_desired"])
+        qg = s.get_q()
+        s.set_b4step(S.B4STEP_NONE)
+        s.set_aux(aux)
+        s.set_q(q)
+        s.sharpclaw(0.0, run["tend"], run["dt_initial"], run["cfl_max"], run["cfl_desired"])
+        qn = s.get_q()
+    assert res["steps_taken"] == ro.steps_taken and res["rejected"] == ro.rejected
+    assert _rel_inf(_interior(qg, 2), _interior(qo, 2)) <= 1e-13
+    assert _rel_inf(_interior(qn, 2), _interior(qo, 2)) > 1e-3
