@@ -155,8 +155,10 @@ int scl_time_steps(scl_handle* h, const scl_run* run, int nsteps, float* ms, scl
  * state is not advanced (every pass restarts from q^n). */
 int scl_time_stages(scl_handle* h, double dt, int reps, float* ms, long long* launches);
 
-/* Kernel launches per controller step (begin + stages + end, + 1 ghost-line
- * CFL kernel in 2-D). */
+/* Kernel launches per controller step inside a step graph (stages + one
+ * controller kernel that ends the step and begins the next, + 1 ghost-line
+ * CFL kernel in 2-D, + 1 b4step kernel when set); each graph replay adds
+ * one begin kernel. */
 int scl_kernels_per_step(scl_handle* h);
 
 /* Frame output in the reference's format (src/1d/out1.f90, src/2d/out2.f90):

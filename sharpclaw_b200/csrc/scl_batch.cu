@@ -175,11 +175,16 @@ BatchArgs make_bargs(const scl_batch* b, int s) {
   return a;
 }
 
-int enqueue_batch_step(scl_batch* b, int v) {
+// One batch step.  Inside a graph of several steps, a step after the first
+// ends its predecessor in its begin kernel (first = false) and only the last
+// step launches k_batch_end.
+int enqueue_batch_step(scl_batch* b, int v, bool first = true, bool last = true) {
   const BatchLaunchers& L = b->L[v];
-  L.begin(b->ctl, b->d_mx, b->ninst, b->d_active, b->d_prefix, b->d_nact, b->stream);
+  L.begin(b->ctl, b->d_mx, b->ninst, b->d_active, b->d_prefix, b->d_nact, first ? -1 : b->nstages - 1,
+          b->final_role, b->stream);
   for (int s = 0; s < b->nstages; ++s) L.stage(make_bargs(b, s), b->grid[v], b->stream);
-  k_batch_end<<<(b->ninst + 255) / 256, 256, 0, b->stream>>>(b->ctl, b->ninst, b->nstages - 1, b->final_role);
+  if (last)
+    k_batch_end<<<(b->ninst + 255) / 256, 256, 0, b->stream>>>(b->ctl, b->ninst, b->nstages - 1, b->final_role);
   BCK(cudaGetLastError());
   return SCL_OK;
 }
@@ -270,7 +275,7 @@ int build_batch_graph(scl_batch* b, int steps) {
   cudaGraph_t g = nullptr;
   BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   int rc = SCL_OK;
-  for (int k = 0; k < steps && rc == SCL_OK; ++k) rc = enqueue_batch_step(b, b->variant);
+  for (int k = 0; k < steps && rc == SCL_OK; ++k) rc = enqueue_batch_step(b, b->variant, k == 0, k == steps - 1);
   cudaError_t e = cudaStreamEndCapture(b->stream, &g);
   if (rc) { if (g) cudaGraphDestroy(g); return rc; }
   if (e != cudaSuccess) return bfail(SCL_E_CUDA, std::string("capture: ") + cudaGetErrorString(e));
@@ -486,7 +491,7 @@ int scl_batch_run(scl_batch* b, const scl_run* run, const double* dt_initial, sc
     rc = upload_batch_ctl(b);
     if (rc) return rc;
   }
-  const int K = std::max(1, 160 / (b->nstages + 2));
+  const int K = std::max(1, 160 / (b->nstages + 1));
   rc = build_batch_graph(b, K);
   if (rc) return rc;
   int maxn = 0;
@@ -508,7 +513,8 @@ int scl_batch_run(scl_batch* b, const scl_run* run, const double* dt_initial, sc
   BCK(cudaEventRecord(b->ev1, b->stream));
   BCK(cudaEventSynchronize(b->ev1));
   if (ms) BCK(cudaEventElapsedTime(ms, b->ev0, b->ev1));
-  b->last_launches = (long long)replays * K * (b->nstages + 2);
+  // per replay: K begins (each but the first also ends a step), K * nstages stages, one end
+  b->last_launches = (long long)replays * (K * (b->nstages + 1) + 1);
   rc = download_batch_ctl(b);
   if (rc) return rc;
   for (int k = 0; k < b->ninst; ++k) {

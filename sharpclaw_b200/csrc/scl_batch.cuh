@@ -10,7 +10,8 @@
 //   active tiles of all instances: tile -> instance by binary search),
 //   end (one thread per instance: k_end_step logic).
 // The host captures K such steps in a CUDA graph and replays it until no
-// instance is active.
+// instance is active; inside the graph the end of step k runs in the begin
+// kernel of step k+1 (same thread per instance, end logic first).
 #pragma once
 #include "scl_kernels.cuh"
 
@@ -98,11 +99,12 @@ __device__ __forceinline__ void end_one(Ctl* c, int last_stage, int final_role) 
 }
 
 // Begin of a batch step on one CTA of 1024 threads: controller begin for every
-// instance, then the ordered list of active instances with the exclusive
+// instance (after the end of the previous step when end_stage >= 0: its last
+// stage index), then the ordered list of active instances with the exclusive
 // prefix sum of their tile counts (a block-wide scan in chunks of 1024).
 template <int NT>
 __global__ void __launch_bounds__(1024) k_batch_begin(Ctl* ctl, const int* mx, int ninst, int* active,
-                                                      int* prefix, int* nact) {
+                                                      int* prefix, int* nact, int end_stage, int final_role) {
   __shared__ int wact[32], wtiles[32];
   __shared__ int base_tiles, base_act;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -112,6 +114,7 @@ __global__ void __launch_bounds__(1024) k_batch_begin(Ctl* ctl, const int* mx, i
     const int k = k0 + tid;
     int act = 0, tiles = 0;
     if (k < ninst) {
+      if (end_stage >= 0) end_one(&ctl[k], end_stage, final_role);
       begin_one(&ctl[k]);
       act = ctl[k].done ? 0 : 1;
       tiles = act ? (mx[k] + NT - 2) / (NT - 1) : 0;

@@ -38,7 +38,7 @@ int fail(int code, const std::string& msg) {
 // ---------------------------------------------------------------------------
 // Controller kernels: one thread each, src/sharpclaw.f90:118-221.
 // ---------------------------------------------------------------------------
-__global__ void k_begin_step(Ctl* c) {
+__device__ __forceinline__ void ctl_begin(Ctl* c) {
   if (c->done) return;
   if (c->n_iter >= c->maxn) { c->done = 1; return; }   // do n=1,maxn exhausted
   c->n_iter += 1;
@@ -53,7 +53,7 @@ __global__ void k_begin_step(Ctl* c) {
   for (int s = 0; s < MAXSTAGES; ++s) c->stage_cfl[s] = 0.0;
 }
 
-__global__ void k_end_step(Ctl* c, int last_stage, int final_role) {
+__device__ __forceinline__ void ctl_end(Ctl* c, int last_stage, int final_role) {
   if (c->done) return;
   const double cfl = c->stage_cfl[last_stage];   // the last stage's CFL (:184, A2)
   c->cfl_last = cfl;
@@ -102,6 +102,14 @@ __global__ void k_end_step(Ctl* c, int last_stage, int final_role) {
   }
   c->steps_taken += 1;                                              // :219
   if (c->t >= c->tend) c->done = 1;                                 // :220
+}
+
+__global__ void k_begin_step(Ctl* c) { ctl_begin(c); }
+__global__ void k_end_step(Ctl* c, int last_stage, int final_role) { ctl_end(c, last_stage, final_role); }
+// the end of one step and the begin of the next in one launch (inside a graph)
+__global__ void k_end_begin(Ctl* c, int last_stage, int final_role) {
+  ctl_end(c, last_stage, final_role);
+  ctl_begin(c);
 }
 
 // b4step of apps/advection/2d/swirl/b4step.f90 on the device: before a new
@@ -315,8 +323,11 @@ int enqueue_stages(scl_handle* h) {
   return SCL_OK;
 }
 
-int enqueue_step(scl_handle* h) {
-  k_begin_step<<<1, 1, 0, h->stream>>>(h->ctl);
+// One controller step: begin (only for the first step of a sequence; later
+// steps are begun by the previous step's k_end_begin), the b4step hook, the
+// stages, end (last step) or end + the next begin.
+int enqueue_step(scl_handle* h, bool first = true, bool last = true) {
+  if (first) k_begin_step<<<1, 1, 0, h->stream>>>(h->ctl);
   if (h->b4kind == SCL_B4STEP_SWIRL) {
     const long n = h->plane * h->p.maux;
     if (h->ssize == sizeof(double))
@@ -328,13 +339,15 @@ int enqueue_step(scl_handle* h) {
   }
   int rc = enqueue_stages(h);
   if (rc) return rc;
-  k_end_step<<<1, 1, 0, h->stream>>>(h->ctl, h->nstages - 1, h->final_role);
+  if (last) k_end_step<<<1, 1, 0, h->stream>>>(h->ctl, h->nstages - 1, h->final_role);
+  else k_end_begin<<<1, 1, 0, h->stream>>>(h->ctl, h->nstages - 1, h->final_role);
   CK(cudaGetLastError());
   return SCL_OK;
 }
 
+// launches per step inside a graph (plus one begin per graph replay)
 int kernels_per_step(const scl_handle* h) {
-  return h->nstages + 2 + (h->L.ghost ? 1 : 0) + (h->b4kind != SCL_B4STEP_NONE ? 1 : 0);
+  return h->nstages + 1 + (h->L.ghost ? 1 : 0) + (h->b4kind != SCL_B4STEP_NONE ? 1 : 0);
 }
 
 // Capture `steps` controller steps (begin, stages, end) into one executable
@@ -346,7 +359,7 @@ int build_graph(scl_handle* h, int steps) {
   cudaGraph_t g = nullptr;
   CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   int rc = SCL_OK;
-  for (int k = 0; k < steps && rc == SCL_OK; ++k) rc = enqueue_step(h);
+  for (int k = 0; k < steps && rc == SCL_OK; ++k) rc = enqueue_step(h, k == 0, k == steps - 1);
   cudaError_t e = cudaStreamEndCapture(h->stream, &g);
   if (rc) { if (g) cudaGraphDestroy(g); return rc; }
   if (e != cudaSuccess) return fail(SCL_E_CUDA, std::string("capture: ") + cudaGetErrorString(e));

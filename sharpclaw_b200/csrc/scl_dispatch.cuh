@@ -144,8 +144,8 @@ void launch_batch_stage(const BatchArgs& a, int grid, cudaStream_t st) {
 }
 template <int NT>
 void launch_batch_begin(Ctl* ctl, const int* mx, int ninst, int* active, int* prefix, int* nact,
-                        cudaStream_t st) {
-  k_batch_begin<NT><<<1, 1024, 0, st>>>(ctl, mx, ninst, active, prefix, nact);
+                        int end_stage, int final_role, cudaStream_t st) {
+  k_batch_begin<NT><<<1, 1024, 0, st>>>(ctl, mx, ninst, active, prefix, nact, end_stage, final_role);
 }
 template <class P, int CD, int TF, int NT>
 int batch_blocks_per_sm() {

@@ -30,7 +30,9 @@ struct BatchArgs;
 // Batched persistent launchers of one plugin / precision / tile width.
 struct BatchLaunchers {
   void (*stage)(const BatchArgs&, int grid, cudaStream_t);
-  void (*begin)(Ctl* ctl, const int* mx, int ninst, int* active, int* prefix, int* nact, cudaStream_t);
+  // end_stage >= 0: run the previous step's end (that last stage, final_role) first
+  void (*begin)(Ctl* ctl, const int* mx, int ninst, int* active, int* prefix, int* nact, int end_stage,
+                int final_role, cudaStream_t);
   int (*blocks_per_sm)();
   int nt;   // threads per CTA = interfaces per tile
 };
