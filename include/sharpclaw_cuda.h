@@ -161,6 +161,27 @@ int scl_time_stages(scl_handle* h, double dt, int reps, float* ms, long long* la
  * one begin kernel. */
 int scl_kernels_per_step(scl_handle* h);
 
+/* How scl_sharpclaw and scl_time_steps run the controller loop (no
+ * counterpart in the reference, whose loop is sharpclaw.f90:118-221 on the
+ * host).  SCL_RUN_GRAPH: CUDA graphs of stage and controller kernels, any
+ * grid.  SCL_RUN_RESIDENT: one thread-block cluster of up to 8 CTAs keeps the
+ * whole loop in one launch (per 4096 iterations), for 1-D grids of at most
+ * 64 tiles of 127 cells (8128 cells) without a b4step hook; SCL_E_UNSUPPORTED
+ * otherwise.  SCL_RUN_AUTO (the default): resident for 1-D grids of at most
+ * 16 tiles (2032 cells), graphs for the rest.  Both modes run the same tile
+ * arithmetic and controller, so their results are identical, except in the
+ * FP32 forms of 1-D Euler (char_decomp 0/2, tfluct_solver 0), whose graph
+ * path uses a paired kernel with a different FP32 contraction order. */
+#define SCL_RUN_AUTO 0
+#define SCL_RUN_GRAPH 1
+#define SCL_RUN_RESIDENT 2
+int scl_set_run_mode(scl_handle* h, int mode);
+
+/* The mode the last scl_sharpclaw / scl_time_steps ran in (SCL_RUN_GRAPH or
+ * SCL_RUN_RESIDENT) and the kernels it launched (graph nodes counted one by
+ * one); either out pointer may be NULL. */
+int scl_last_run(scl_handle* h, int* mode, long long* launches);
+
 /* Frame output in the reference's format (src/1d/out1.f90, src/2d/out2.f90):
  * fort.qNNNN (interior cells, 4 values per record, e16.8 in 1-D and e26.16 in
  * 2-D), fort.tNNNN, and with write_aux fort.aNNNN, in directory dir (NULL or

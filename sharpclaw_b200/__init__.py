@@ -30,10 +30,11 @@ import numpy as np
 from . import _capi as C
 from ._capi import (B4STEP_NONE, B4STEP_SWIRL, FP32, FP64, FP64_STRICT, MIXED,  # noqa: F401
                     RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION, RP_ADVECTION2D, RP_EULER, RP_SW2D,
-                    SharpClawError)
+                    RUN_AUTO, RUN_GRAPH, RUN_RESIDENT, SharpClawError)
 
 __all__ = ["ClawParams", "Solver", "Batch", "sharpclaw", "SharpClawError", "RP_ADVECTION", "RP_EULER",
-           "RP_SW2D", "RP_ACOUSTICS1D", "RP_ACOUSTICS2D", "RP_ADVECTION2D", "B4STEP_NONE", "B4STEP_SWIRL"]
+           "RP_SW2D", "RP_ACOUSTICS1D", "RP_ACOUSTICS2D", "RP_ADVECTION2D", "B4STEP_NONE", "B4STEP_SWIRL",
+           "RUN_AUTO", "RUN_GRAPH", "RUN_RESIDENT"]
 
 # plugin id -> (meqn, mwaves, maux, ndim)
 PLUGINS = {
@@ -243,6 +244,18 @@ class Solver:
     @property
     def kernels_per_step(self) -> int:
         return C.lib().scl_kernels_per_step(self._h)
+
+    def set_run_mode(self, mode: int):
+        """RUN_GRAPH: step graphs; RUN_RESIDENT: the whole controller loop in
+        one thread-block cluster (1-D grids of at most 8128 cells); RUN_AUTO
+        (default): resident up to 2032 cells."""
+        C.check(C.lib().scl_set_run_mode(self._h, int(mode)), "scl_set_run_mode")
+
+    def last_run(self):
+        """(mode, kernel launches) of the last sharpclaw() / time_steps()."""
+        m, n = ctypes.c_int(), ctypes.c_longlong()
+        C.check(C.lib().scl_last_run(self._h, ctypes.byref(m), ctypes.byref(n)), "scl_last_run")
+        return m.value, n.value
 
     def write_frame(self, t: float, iframe: int, dir: str | None = None, write_aux: bool | None = None):
         """Write fort.qNNNN / fort.tNNNN (/ fort.aNNNN) of the current state in

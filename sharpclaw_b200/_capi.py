@@ -15,6 +15,7 @@ SCL_OK, SCL_E_INVALID, SCL_E_CUDA, SCL_E_UNSUPPORTED, SCL_E_NONFINITE, SCL_E_TIM
     0, -1, -2, -3, -4, -5, -6
 RP_ADVECTION, RP_EULER, RP_SW2D, RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION2D = 1, 2, 3, 4, 5, 6
 B4STEP_NONE, B4STEP_SWIRL = 0, 1
+RUN_AUTO, RUN_GRAPH, RUN_RESIDENT = 0, 1, 2
 FP64, FP64_STRICT, MIXED, FP32 = 0, 1, 2, 3
 INFO_DT_NOT_DIVIDING, INFO_CFL_DESIRED_GT_MAX, INFO_TOO_MANY_STEPS, INFO_CFL_FIXED_DT, INFO_NONFINITE = 2, 3, 11, 12, 20
 STATUS_NONFINITE, STATUS_TIMEOUT, STATUS_BOUNDS = 1, 2, 4
@@ -77,6 +78,8 @@ SIGNATURES = [
     ("scl_time_stages", ctypes.c_int, [_h, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
                                         ctypes.POINTER(ctypes.c_longlong)]),
     ("scl_kernels_per_step", ctypes.c_int, [_h]),
+    ("scl_set_run_mode", ctypes.c_int, [_h, ctypes.c_int]),
+    ("scl_last_run", ctypes.c_int, [_h, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)]),
     ("scl_select_tiles", ctypes.c_int, [_h, ctypes.c_int]),
     ("scl_set_b4step", ctypes.c_int, [_h, ctypes.c_int, ctypes.c_double]),
     ("scl_write_frame", ctypes.c_int, [_h, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),

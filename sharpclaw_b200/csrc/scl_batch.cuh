@@ -4,15 +4,16 @@
 // Every instance k keeps its own controller (t, dt, CFL, roles, status: the
 // scalars of src/sharpclaw.f90) in ctl[k], so instances take their own
 // adaptive steps, rejections and final times.  A step of the batch is
-//   begin (one CTA: per-instance k_begin_step logic, then the list of active
+//   begin (one CTA: ctl_begin for every instance, then the list of active
 //   instances and the prefix sum of their tiles),
 //   one persistent stage kernel per RK stage (a fixed grid of CTAs walks the
 //   active tiles of all instances: tile -> instance by binary search),
-//   end (one thread per instance: k_end_step logic).
+//   end (one thread per instance: ctl_end).
 // The host captures K such steps in a CUDA graph and replays it until no
 // instance is active; inside the graph the end of step k runs in the begin
 // kernel of step k+1 (same thread per instance, end logic first).
 #pragma once
+#include "scl_ctl.cuh"
 #include "scl_kernels.cuh"
 
 namespace scl {
@@ -36,68 +37,6 @@ struct BatchArgs {
   Phys ph;
 };
 
-// The per-instance controller logic is the single-grid controller's
-// (src/sharpclaw.f90:118-221) applied to ctl[k].
-__device__ __forceinline__ void begin_one(Ctl* c) {
-  if (c->done) return;
-  if (c->n_iter >= c->maxn) { c->done = 1; return; }
-  c->n_iter += 1;
-  if (!c->retake) {
-    c->told = c->t;
-    if (c->told + c->dt > c->tend && c->tstart < c->tend) c->dt = c->tend - c->told;
-  }
-  c->retake = 0;
-  c->t = c->told + c->dt;
-  for (int s = 0; s < MAXSTAGES; ++s) c->stage_cfl[s] = 0.0;
-}
-
-__device__ __forceinline__ void end_one(Ctl* c, int last_stage, int final_role) {
-  if (c->done) return;
-  const double cfl = c->stage_cfl[last_stage];
-  c->cfl_last = cfl;
-  if (cfl != cfl) {
-    c->status |= SCL_STATUS_NONFINITE;
-    c->info = SCL_INFO_NONFINITE;
-    c->t = c->told;
-    c->done = 1;
-    return;
-  }
-  if (cfl <= c->cfl_max && (c->status & SCL_STATUS_NONFINITE)) {
-    c->info = SCL_INFO_NONFINITE;
-    c->t = c->told;
-    c->done = 1;
-    return;
-  }
-  c->status &= ~SCL_STATUS_NONFINITE;
-  if (c->dt_variable == 1) {
-    if (cfl > 0.0) {
-      c->dt = fmin(c->dt_max, c->dt * c->cfl_desired / cfl);
-      c->dtmin = fmin(c->dt, c->dtmin);
-      c->dtmax = fmax(c->dt, c->dtmax);
-    } else {
-      c->dt = c->dt_max;
-    }
-  }
-  if (cfl <= c->cfl_max) {
-    c->cflmax = fmax(cfl, c->cflmax);
-    const int tmp = c->role[ROLE_Q];
-    c->role[ROLE_Q] = c->role[final_role];
-    c->role[final_role] = tmp;
-  } else {
-    c->t = c->told;
-    c->rejected += 1;
-    if (c->dt_variable == 1) {
-      c->retake = 1;
-    } else {
-      c->cflmax = fmax(cfl, c->cflmax);
-      c->done = 1;
-      return;
-    }
-  }
-  c->steps_taken += 1;
-  if (c->t >= c->tend) c->done = 1;
-}
-
 // Begin of a batch step on one CTA of 1024 threads: controller begin for every
 // instance (after the end of the previous step when end_stage >= 0: its last
 // stage index), then the ordered list of active instances with the exclusive
@@ -114,8 +53,8 @@ __global__ void __launch_bounds__(1024) k_batch_begin(Ctl* ctl, const int* mx, i
     const int k = k0 + tid;
     int act = 0, tiles = 0;
     if (k < ninst) {
-      if (end_stage >= 0) end_one(&ctl[k], end_stage, final_role);
-      begin_one(&ctl[k]);
+      if (end_stage >= 0) ctl_end(&ctl[k], end_stage, final_role);
+      ctl_begin(&ctl[k]);
       act = ctl[k].done ? 0 : 1;
       tiles = act ? (mx[k] + NT - 2) / (NT - 1) : 0;
     }
@@ -157,7 +96,7 @@ __global__ void __launch_bounds__(1024) k_batch_begin(Ctl* ctl, const int* mx, i
 
 static __global__ void k_batch_end(Ctl* ctl, int ninst, int last_stage, int final_role) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < ninst) end_one(&ctl[k], last_stage, final_role);
+  if (k < ninst) ctl_end(&ctl[k], last_stage, final_role);
 }
 
 // Persistent stage kernel: a fixed grid walks the active tiles.

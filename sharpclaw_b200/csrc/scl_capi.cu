@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "scl_common.cuh"
+#include "scl_ctl.cuh"
 #include "scl_frames.h"
 #include "scl_launch.h"
 
@@ -35,75 +36,7 @@ int fail(int code, const std::string& msg) {
       return fail(SCL_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
   } while (0)
 
-// ---------------------------------------------------------------------------
-// Controller kernels: one thread each, src/sharpclaw.f90:118-221.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void ctl_begin(Ctl* c) {
-  if (c->done) return;
-  if (c->n_iter >= c->maxn) { c->done = 1; return; }   // do n=1,maxn exhausted
-  c->n_iter += 1;
-  c->fresh = !c->retake;                                             // b4step runs on new steps only
-  if (!c->retake) {
-    c->told = c->t;                                                  // :120
-    if (c->told + c->dt > c->tend && c->tstart < c->tend) c->dt = c->tend - c->told;  // :124
-    // b4step: default no-op (src/b4step.f90); qold = q is the Q role (:132-135)
-  }
-  c->retake = 0;
-  c->t = c->told + c->dt;                                            // :139
-  for (int s = 0; s < MAXSTAGES; ++s) c->stage_cfl[s] = 0.0;
-}
-
-__device__ __forceinline__ void ctl_end(Ctl* c, int last_stage, int final_role) {
-  if (c->done) return;
-  const double cfl = c->stage_cfl[last_stage];   // the last stage's CFL (:184, A2)
-  c->cfl_last = cfl;
-  // A NaN CFL number cannot drive dt control (the reference would reject and
-  // retake with a NaN or dt_max step forever): stop with q = qold.
-  if (cfl != cfl) {
-    c->status |= SCL_STATUS_NONFINITE;
-    c->info = SCL_INFO_NONFINITE;
-    c->t = c->told;
-    c->done = 1;
-    return;
-  }
-  // Non-finite stage outputs matter only if the step is accepted; a rejected
-  // step's stages are discarded (q = qold) as in the reference.
-  if (cfl <= c->cfl_max && (c->status & SCL_STATUS_NONFINITE)) {
-    c->info = SCL_INFO_NONFINITE;
-    c->t = c->told;
-    c->done = 1;
-    return;
-  }
-  c->status &= ~SCL_STATUS_NONFINITE;
-  if (c->dt_variable == 1) {                                        // :184-192
-    if (cfl > 0.0) {
-      c->dt = fmin(c->dt_max, c->dt * c->cfl_desired / cfl);
-      c->dtmin = fmin(c->dt, c->dtmin);
-      c->dtmax = fmax(c->dt, c->dtmax);
-    } else {
-      c->dt = c->dt_max;
-    }
-  }
-  if (cfl <= c->cfl_max) {                                          // :195-197 accept
-    c->cflmax = fmax(cfl, c->cflmax);
-    const int tmp = c->role[ROLE_Q];
-    c->role[ROLE_Q] = c->role[final_role];
-    c->role[final_role] = tmp;
-  } else {                                                          // :198-216 reject
-    c->t = c->told;
-    c->rejected += 1;
-    if (c->dt_variable == 1) {
-      c->retake = 1;
-    } else {
-      c->cflmax = fmax(cfl, c->cflmax);
-      c->done = 1;
-      return;
-    }
-  }
-  c->steps_taken += 1;                                              // :219
-  if (c->t >= c->tend) c->done = 1;                                 // :220
-}
-
+// Controller kernels: one thread each (the logic is in scl_ctl.cuh).
 __global__ void k_begin_step(Ctl* c) { ctl_begin(c); }
 __global__ void k_end_step(Ctl* c, int last_stage, int final_role) { ctl_end(c, last_stage, final_role); }
 // the end of one step and the begin of the next in one launch (inside a graph)
@@ -272,6 +205,10 @@ struct scl_handle {
   int b4kind = SCL_B4STEP_NONE;
   double b4param = 0.0;
   void* aux0 = nullptr;
+  // time-loop mode (SCL_RUN_*) and what the last run used
+  int run_mode = SCL_RUN_AUTO;
+  int last_mode = SCL_RUN_AUTO;
+  long long last_launches = 0;
 };
 
 namespace {
@@ -863,8 +800,11 @@ int run_loop(scl_handle* h, int graph_steps, long max_replays, float* ms) {
   if (rc) return rc;
   if (ms) CK(cudaEventRecord(h->ev0, h->stream));
   h->hdone[0] = h->hdone[1] = 0;
+  h->last_mode = SCL_RUN_GRAPH;
+  h->last_launches = 0;
   for (long r = 0; r < max_replays; ++r) {
     CK(cudaGraphLaunch(h->graph, h->stream));
+    h->last_launches += (long long)graph_steps * kernels_per_step(h) + 1;
     if (max_replays == 1) break;
     CK(cudaMemcpyAsync(&h->hdone[r & 1], &h->ctl->done, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaEventRecord(h->evq[r & 1], h->stream));
@@ -881,20 +821,79 @@ int run_loop(scl_handle* h, int graph_steps, long max_replays, float* ms) {
   return download_ctl(h);
 }
 
+int resident_tiles(const scl_handle* h) { return (h->p.mx + RES_NT - 2) / (RES_NT - 1); }
+
+// A resident run needs a 1-D grid of at most RES_MAX_TILES tiles and no
+// b4step hook (the hooks run as kernels of the step graph).
+bool resident_possible(const scl_handle* h) {
+  return h->p.ndim == 1 && h->L.run != nullptr && h->b4kind == SCL_B4STEP_NONE &&
+         resident_tiles(h) <= RES_MAX_TILES;
+}
+
+int use_resident(const scl_handle* h, bool* yes) {
+  *yes = false;
+  if (h->run_mode == SCL_RUN_GRAPH) return SCL_OK;
+  if (h->run_mode == SCL_RUN_RESIDENT) {
+    if (!resident_possible(h))
+      return fail(SCL_E_UNSUPPORTED, "resident run: needs a 1-D grid of at most 64 tiles and no b4step hook");
+    *yes = true;
+    return SCL_OK;
+  }
+  *yes = resident_possible(h) && resident_tiles(h) <= RES_AUTO_TILES;
+  return SCL_OK;
+}
+
+// The controller loop as cluster-resident launches of RES_ITERS iterations
+// each, relaunched until the controller is done (after maxn iterations at
+// the latest).
+int run_resident(scl_handle* h, float* ms) {
+  RunArgs ra{};
+  ra.st = make_args(h, 0);
+  for (int s = 0; s < h->nstages; ++s) ra.sd[s] = h->sd[s];
+  ra.nstages = h->nstages;
+  ra.final_role = h->final_role;
+  ra.max_iters = RES_ITERS;
+  const long max_launches = (long)h->hctl->maxn / RES_ITERS + 1;
+  if (ms) CK(cudaEventRecord(h->ev0, h->stream));
+  h->last_mode = SCL_RUN_RESIDENT;
+  h->last_launches = 0;
+  for (long r = 0; r < max_launches; ++r) {
+    CK(h->L.run(ra, h->stream));
+    h->last_launches += 1;
+    if (r + 1 == max_launches) break;
+    CK(cudaMemcpyAsync(&h->hdone[0], &h->ctl->done, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->hdone[0]) break;
+  }
+  if (ms) {
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    CK(cudaEventElapsedTime(ms, h->ev0, h->ev1));
+  }
+  return download_ctl(h);
+}
+
 }  // namespace
 
 extern "C" {
 
 int scl_sharpclaw(scl_handle* h, const scl_run* run, scl_result* res) {
   if (!h || !run || !res) return fail(SCL_E_INVALID, "null argument");
+  bool resident = false;
+  int rc = use_resident(h, &resident);
+  if (rc) return rc;
   bool early = false;
-  int rc = init_run(h, run, run->max_steps, res, &early);
+  rc = init_run(h, run, run->max_steps, res, &early);
   if (rc || early) return rc;
-  // a graph replay runs gs controller steps; after maxn iterations the
-  // controller is done, so no more than ceil(maxn/gs) replays are launched
-  const int gs = std::min(std::max(1, h->hctl->maxn), default_graph_steps(h));
-  const long replays = ((long)h->hctl->maxn + gs - 1) / gs;
-  rc = run_loop(h, gs, replays, nullptr);
+  if (resident) {
+    rc = run_resident(h, nullptr);
+  } else {
+    // a graph replay runs gs controller steps; after maxn iterations the
+    // controller is done, so no more than ceil(maxn/gs) replays are launched
+    const int gs = std::min(std::max(1, h->hctl->maxn), default_graph_steps(h));
+    const long replays = ((long)h->hctl->maxn + gs - 1) / gs;
+    rc = run_loop(h, gs, replays, nullptr);
+  }
   if (rc) return rc;
   finish_run(h, res);
   if (res->status & SCL_STATUS_NONFINITE) return fail(SCL_E_NONFINITE, "non-finite CFL number");
@@ -918,12 +917,19 @@ int scl_sharpclaw_device(scl_handle* h, const scl_run* run, double* q_dev, scl_r
 
 int scl_time_steps(scl_handle* h, const scl_run* run, int nsteps, float* ms, scl_result* res) {
   if (!h || !run || !ms || !res || nsteps < 1) return fail(SCL_E_INVALID, "bad argument");
+  bool resident = false;
+  int rc = use_resident(h, &resident);
+  if (rc) return rc;
   bool early = false;
-  int rc = init_run(h, run, nsteps, res, &early);
+  rc = init_run(h, run, nsteps, res, &early);
   if (rc || early) return rc ? rc : fail(SCL_E_INVALID, "run parameters rejected (info set)");
-  const int gs = nsteps <= 64 ? nsteps : default_graph_steps(h);
-  const long replays = (nsteps + gs - 1) / gs;
-  rc = run_loop(h, gs, replays, ms);
+  if (resident) {
+    rc = run_resident(h, ms);
+  } else {
+    const int gs = nsteps <= 64 ? nsteps : default_graph_steps(h);
+    const long replays = (nsteps + gs - 1) / gs;
+    rc = run_loop(h, gs, replays, ms);
+  }
   if (rc) return rc;
   finish_run(h, res);
   return SCL_OK;
@@ -953,6 +959,23 @@ int scl_time_stages(scl_handle* h, double dt, int reps, float* ms, long long* la
 }
 
 int scl_kernels_per_step(scl_handle* h) { return h ? kernels_per_step(h) : 0; }
+
+int scl_set_run_mode(scl_handle* h, int mode) {
+  if (!h) return fail(SCL_E_INVALID, "null handle");
+  if (mode != SCL_RUN_AUTO && mode != SCL_RUN_GRAPH && mode != SCL_RUN_RESIDENT)
+    return fail(SCL_E_INVALID, "run mode must be SCL_RUN_AUTO, SCL_RUN_GRAPH or SCL_RUN_RESIDENT");
+  if (mode == SCL_RUN_RESIDENT && !resident_possible(h))
+    return fail(SCL_E_UNSUPPORTED, "resident run: needs a 1-D grid of at most 64 tiles and no b4step hook");
+  h->run_mode = mode;
+  return SCL_OK;
+}
+
+int scl_last_run(scl_handle* h, int* mode, long long* launches) {
+  if (!h) return fail(SCL_E_INVALID, "null handle");
+  if (mode) *mode = h->last_mode;
+  if (launches) *launches = h->last_launches;
+  return SCL_OK;
+}
 
 int scl_wait_frames(scl_handle* h) {
   if (!h) return fail(SCL_E_INVALID, "null handle");

@@ -90,6 +90,16 @@ struct StageArgs {
   Phys ph;
 };
 
+// Arguments of a cluster-resident run of a 1-D grid (the whole controller
+// loop in one launch): the stage arguments of stage 0 plus every stage's
+// descriptor.
+struct RunArgs {
+  StageArgs st;
+  StageDesc sd[MAXSTAGES];
+  int nstages, final_role;
+  int max_iters;            // controller iterations of one launch
+};
+
 // NaN-propagating maximum used for the CFL number: a NaN anywhere makes the
 // block result NaN so the controller can flag a non-finite state.
 template <class R>

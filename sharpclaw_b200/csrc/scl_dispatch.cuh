@@ -3,12 +3,14 @@
 // SCL_PREC_VALUE defined; the FP64_STRICT unit is compiled without FMA
 // contraction so its arithmetic follows the reference's evaluation order.
 #pragma once
+#include <algorithm>
 #include <type_traits>
 
 #include "scl_batch.cuh"
 #include "scl_kernels.cuh"
 #include "scl_launch.h"
 #include "scl_pair.cuh"
+#include "scl_resident.cuh"
 
 #ifndef SCL_PREC_VALUE
 #error "SCL_PREC_VALUE must be defined"
@@ -27,6 +29,26 @@ template <class P, int CD, int TF>
 void launch1d(const StageArgs& a, cudaStream_t st) {
   const int nb = (a.mx + NT1 - 2) / (NT1 - 1);
   k_stage1d<P, CD, TF, PREC, NT1><<<nb, NT1, 0, st>>>(a);
+}
+
+// One cluster of min(tiles, RES_CLUSTER) CTAs runs the controller loop.
+template <class P, int CD, int TF>
+cudaError_t launch_run1d(const RunArgs& a, cudaStream_t st) {
+  const int ntiles = (a.st.mx + RES_NT - 2) / (RES_NT - 1);
+  const int nc = std::min(ntiles, RES_CLUSTER);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nc, 1, 1);
+  cfg.blockDim = dim3(RES_NT, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = nc;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_run1d<P, CD, TF, PREC, RES_NT>, a);
 }
 
 // 1-D Euler in the FP32 forms: two interfaces per thread in packed FP32
@@ -88,31 +110,40 @@ bool fill2d(int variant, Launchers* L) {
   return true;
 }
 
+template <class P, int CD, int TF>
+void fill1d(Launchers* L) {
+  L->stage = &launch1d<P, CD, TF>;
+  L->run = &launch_run1d<P, CD, TF>;
+}
+
 template <class P>
 bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
   L->stage = nullptr;
   L->ghost = nullptr;
+  L->run = nullptr;
   if (ndim == 1) {
     if (variant != 0) return false;
-    if constexpr (SCL_PAIR && std::is_same_v<P, PEuler> && !Prec<PREC>::EXACT) {
-      if (cd == 0 && tf == 0) { L->stage = &launch1d_pair<0>; return true; }
-      if (cd == 2 && tf == 0) { L->stage = &launch1d_pair<2>; return true; }
-    }
-    if (cd == 0 && tf == 0) L->stage = &launch1d<P, 0, 0>;
-    if (cd == 1 && tf == 0) L->stage = &launch1d<P, 1, 0>;
-    if (cd == 2 && tf == 0) L->stage = &launch1d<P, 2, 0>;
-    if (cd == 3 && tf == 0) L->stage = &launch1d<P, 3, 0>;
-    if (cd == 10 && tf == 0) L->stage = &launch1d<P, 10, 0>;
-    if (cd == 11 && tf == 0) L->stage = &launch1d<P, 11, 0>;
-    if (cd == 12 && tf == 0) L->stage = &launch1d<P, 12, 0>;
+    if (cd == 0 && tf == 0) fill1d<P, 0, 0>(L);
+    if (cd == 1 && tf == 0) fill1d<P, 1, 0>(L);
+    if (cd == 2 && tf == 0) fill1d<P, 2, 0>(L);
+    if (cd == 3 && tf == 0) fill1d<P, 3, 0>(L);
+    if (cd == 10 && tf == 0) fill1d<P, 10, 0>(L);
+    if (cd == 11 && tf == 0) fill1d<P, 11, 0>(L);
+    if (cd == 12 && tf == 0) fill1d<P, 12, 0>(L);
     if constexpr (P::HAS_TFLUCT) {
-      if (cd == 0 && tf == 1) L->stage = &launch1d<P, 0, 1>;
-      if (cd == 1 && tf == 1) L->stage = &launch1d<P, 1, 1>;
-      if (cd == 2 && tf == 1) L->stage = &launch1d<P, 2, 1>;
-      if (cd == 3 && tf == 1) L->stage = &launch1d<P, 3, 1>;
-      if (cd == 10 && tf == 1) L->stage = &launch1d<P, 10, 1>;
-      if (cd == 11 && tf == 1) L->stage = &launch1d<P, 11, 1>;
-      if (cd == 12 && tf == 1) L->stage = &launch1d<P, 12, 1>;
+      if (cd == 0 && tf == 1) fill1d<P, 0, 1>(L);
+      if (cd == 1 && tf == 1) fill1d<P, 1, 1>(L);
+      if (cd == 2 && tf == 1) fill1d<P, 2, 1>(L);
+      if (cd == 3 && tf == 1) fill1d<P, 3, 1>(L);
+      if (cd == 10 && tf == 1) fill1d<P, 10, 1>(L);
+      if (cd == 11 && tf == 1) fill1d<P, 11, 1>(L);
+      if (cd == 12 && tf == 1) fill1d<P, 12, 1>(L);
+    }
+    // the FP32 forms of 1-D Euler step large grids with the paired kernel;
+    // a resident run keeps the one-interface tile code
+    if constexpr (SCL_PAIR && std::is_same_v<P, PEuler> && !Prec<PREC>::EXACT) {
+      if (cd == 0 && tf == 0) L->stage = &launch1d_pair<0>;
+      if (cd == 2 && tf == 0) L->stage = &launch1d_pair<2>;
     }
     return L->stage != nullptr;
   }

@@ -509,18 +509,17 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
 // ---------------------------------------------------------------------------
 // 1-D stage kernel: one tile per CTA over a single grid.
 // ---------------------------------------------------------------------------
-template <class P, int CD, int TF, int PREC, int NT>
-__global__ void __launch_bounds__(NT) k_stage1d(StageArgs a) {
-  using S = typename Prec<PREC>::S;
-  __shared__ Tile1DSmem<P, PREC, NT> sm;
+// The line of stage `stage` (descriptor sd) of a single 1-D grid: its
+// buffers resolved through the controller's current roles.
+template <class S>
+__device__ __forceinline__ Line<S> line1d(const StageArgs& a, const StageDesc& sd, int stage) {
   Ctl* ctl = a.ctl;
-  if (ctl->done) return;
   Line<S> L;
   L.ctl = ctl;
-  L.qin = static_cast<const S*>(a.buf[ctl->role[a.sd.in]]);
-  L.qo = a.sd.aux_in >= 0 ? static_cast<const S*>(a.buf[ctl->role[a.sd.aux_in]]) : nullptr;
-  L.out = a.sd.kind == SK_DQ ? nullptr : static_cast<S*>(a.buf[ctl->role[a.sd.out]]);
-  L.out2 = a.sd.out2 >= 0 ? static_cast<S*>(a.buf[ctl->role[a.sd.out2]]) : nullptr;
+  L.qin = static_cast<const S*>(a.buf[ctl->role[sd.in]]);
+  L.qo = sd.aux_in >= 0 ? static_cast<const S*>(a.buf[ctl->role[sd.aux_in]]) : nullptr;
+  L.out = sd.kind == SK_DQ ? nullptr : static_cast<S*>(a.buf[ctl->role[sd.out]]);
+  L.out2 = sd.out2 >= 0 ? static_cast<S*>(a.buf[ctl->role[sd.out2]]) : nullptr;
   L.dq_out = a.dq_out;
   L.aux = a.aux;
   L.mx = a.mx;
@@ -529,10 +528,18 @@ __global__ void __launch_bounds__(NT) k_stage1d(StageArgs a) {
   L.bl = a.mthbc[0];
   L.br = a.mthbc[1];
   L.mcapa = a.mcapa;
-  L.kind = a.sd.kind;
-  L.stage = a.stage;
+  L.kind = sd.kind;
+  L.stage = stage;
   L.ixy = a.ixy;
-  stage1d_tile<P, CD, TF, PREC, NT>(L, a.ph, 1 + blockIdx.x * (NT - 1), sm);
+  return L;
+}
+
+template <class P, int CD, int TF, int PREC, int NT>
+__global__ void __launch_bounds__(NT) k_stage1d(StageArgs a) {
+  using S = typename Prec<PREC>::S;
+  __shared__ Tile1DSmem<P, PREC, NT> sm;
+  if (a.ctl->done) return;
+  stage1d_tile<P, CD, TF, PREC, NT>(line1d<S>(a, a.sd, a.stage), a.ph, 1 + blockIdx.x * (NT - 1), sm);
 }
 
 // ---------------------------------------------------------------------------

@@ -8,7 +8,17 @@ namespace scl {
 struct Launchers {
   void (*stage)(const StageArgs&, cudaStream_t);  // one fused RK stage over the grid
   void (*ghost)(const StageArgs&, cudaStream_t);  // 2-D ghost-line CFL (nullptr in 1-D)
+  cudaError_t (*run)(const RunArgs&, cudaStream_t);  // cluster-resident run (1-D), or nullptr
 };
+
+// Cluster-resident runs: tile width, largest cluster (portable size), the
+// tile counts up to which the automatic mode picks them and up to which they
+// are allowed, and controller iterations per launch.
+constexpr int RES_NT = 128;
+constexpr int RES_CLUSTER = 8;
+constexpr int RES_AUTO_TILES = 16;
+constexpr int RES_MAX_TILES = 64;
+constexpr int RES_ITERS = 4096;
 
 // One getter per arithmetic form; `variant` selects a tile shape (2-D).
 bool get_launchers_fp64(int rp, int ndim, int cd, int tf, int variant, Launchers* L);

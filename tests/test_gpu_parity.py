@@ -147,16 +147,23 @@ RUN_CASES = [
 ]
 
 
+@pytest.mark.parametrize("mode", ["graph", "resident"])
 @pytest.mark.parametrize("name,make,ti,run", RUN_CASES, ids=[c[0] for c in RUN_CASES])
-def test_sharpclaw_run_strict(name, make, ti, run):
+def test_sharpclaw_run_strict(name, make, ti, run, mode):
+    """Full runs, bit-identical to the oracle, with the controller loop in
+    step graphs and (1-D) in one cluster-resident launch."""
     po, ps, q, aux = make()
+    if mode == "resident" and ps.ndim != 1:
+        pytest.skip("resident runs are 1-D")
     ps.time_integrator = ti
     qo, ro = O.sharpclaw(po, q, aux, tstart=0.0, time_integrator=ti, **run)
     with S.Solver(ps, "fp64_strict") as s:
+        s.set_run_mode(S.RUN_GRAPH if mode == "graph" else S.RUN_RESIDENT)
         s.set_aux(aux) if aux is not None else None
         s.set_q(q)
         res = s.sharpclaw(0.0, run["tend"], run["dt_initial"], run["cfl_max"], run["cfl_desired"])
         qg = s.get_q()
+        assert s.last_run()[0] == (S.RUN_GRAPH if mode == "graph" else S.RUN_RESIDENT)
     assert res["steps_taken"] == ro.steps_taken
     assert res["rejected"] == ro.rejected
     assert res["info"] == ro.info
