@@ -50,6 +50,17 @@ extern "C" {
 #define SCL_RP_ACOUSTICS1D 4  /* apps/acoustics/1d/interface/{rp1acv.f,tfluct1acv.f,evec.f90} */
 #define SCL_RP_ACOUSTICS2D 5  /* 2-D variable-coefficient acoustics rpn2/tfluct/evec (new)    */
 #define SCL_RP_ADVECTION2D 6  /* apps/advection/2d/swirl/rpn2ad1.f: edge velocities in aux      */
+#define SCL_RP_SW1D 7         /* apps/shallowWater/2dRadialDam/1dRadialSymm-qwave/{rp1sw.f,
+                                 tfluct1sw.f}, entropy fix on by default (+ Roe evec, new)  */
+
+/* ---- source terms: the src(q,dq,aux,t,dt) an app links (src/1d/step1d.f90:23),
+ * evaluated in the stage kernel before the fluctuations are subtracted;
+ * 1-D, SCL_RP_SW1D only ---------------------------------------------------- */
+#define SCL_SRC_NONE 0           /* src/1d/src1.f90: dq = 0                                */
+#define SCL_SRC_RADIAL_SW 1      /* apps/shallowWater/2dRadialDam/1dRadialSymm-qwave/src1.f90:
+                                    dq = -dt (hu, hu^2/h) / r, r = xlower + (i-1/2) dx     */
+#define SCL_SRC_BATHYMETRY_SW 2  /* apps/shallowWater/1dPerturbSteady/src1.f90:
+                                    dq(2) = -g h (b(i) - b(i-1)) / dx * dt, b = aux(:,1)   */
 
 /* ---- b4step hooks (src/b4step.f90 and the apps' own, run on the device) - */
 #define SCL_B4STEP_NONE 0     /* src/b4step.f90: no-op                                      */
@@ -81,6 +92,8 @@ typedef struct scl_params {
   int mthlim[4];        /* TVD limiter per component / field / wave (lim_type = 1):
                            1 minmod, 2 superbee, 3 van Leer, 4 MC, 5 Cada-Torrilhon
                            (ClawParams%mthlim, reconstruct.f90:551-571)          */
+  int src_term;         /* SCL_SRC_* (ClawParams%src_term; the reference links the
+                           app's src1.f90 instead)                                */
 } scl_params;
 
 /* Arguments of sharpclaw() (src/sharpclaw.f90:2-5). */

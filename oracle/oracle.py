@@ -20,7 +20,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "libsclaw_oracle.so")
 
-RP_ADVECTION, RP_EULER, RP_SW2D, RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION2D = 1, 2, 3, 4, 5, 6
+RP_ADVECTION, RP_EULER, RP_SW2D, RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION2D, RP_SW1D = 1, 2, 3, 4, 5, 6, 7
+SRC_NONE, SRC_RADIAL_SW, SRC_BATHYMETRY_SW = 0, 1, 2
 
 
 class Params(ctypes.Structure):
@@ -36,6 +37,7 @@ class Params(ctypes.Structure):
         ("u", ctypes.c_double), ("gamma", ctypes.c_double), ("grav", ctypes.c_double),
         ("mthlim", ctypes.c_int * 4),
         ("b4step", ctypes.c_int), ("tperiod", ctypes.c_double),
+        ("src_term", ctypes.c_int),
     ]
 
 
@@ -100,7 +102,8 @@ def _ptr(a):
 
 def make_params(*, ndim=1, mx, my=1, meqn, mwaves, mbc=3, maux=0, mcapa=0, char_decomp=0,
                 tfluct_solver=1, mthbc=(2, 2, 2, 2), dx, dy=1.0, xlower=0.0, ylower=0.0,
-                rp, efix=None, u=1.0, gamma=1.4, grav=1.0, lim_type=2, mthlim=(1, 1, 1, 1)) -> Params:
+                rp, efix=None, u=1.0, gamma=1.4, grav=1.0, lim_type=2, mthlim=(1, 1, 1, 1),
+                src_term=SRC_NONE) -> Params:
     p = Params()
     p.ndim, p.mx, p.my = ndim, mx, (my if ndim == 2 else 1)
     p.meqn, p.mwaves, p.mbc, p.maux, p.mcapa = meqn, mwaves, mbc, maux, mcapa
@@ -109,10 +112,12 @@ def make_params(*, ndim=1, mx, my=1, meqn, mwaves, mbc=3, maux=0, mcapa=0, char_
         p.mthbc[k] = int(mthbc[k]) if k < len(mthbc) else 2
     p.dx, p.dy, p.xlower, p.ylower = dx, dy, xlower, ylower
     p.rp = rp
-    p.efix = (1 if rp == RP_EULER else 0) if efix is None else int(efix)
+    # rp1eu.f:40 and 1dRadialSymm-qwave/rp1sw.f data efix /.true./; rpn2sw.f:48 .false.
+    p.efix = (1 if rp in (RP_EULER, RP_SW1D) else 0) if efix is None else int(efix)
     p.u, p.gamma, p.grav = u, gamma, grav
     for k in range(4):
         p.mthlim[k] = int(mthlim[k]) if k < len(mthlim) else 1
+    p.src_term = int(src_term)
     return p
 
 

@@ -827,6 +827,103 @@ static void evec_sw(const ocl_params *p, int ixy, int mx, const double *q, doubl
   }
 }
 
+/* apps/shallowWater/2dRadialDam/1dRadialSymm-qwave/rp1sw.f:46-183: 1-D
+ * shallow water Roe solver, Harten-Hyman entropy fix when p->efix (the app's
+ * data efix /.true./).  cell_internal: the same solve with left ql(i) and
+ * right qr(i) (tfluct1sw.f of that app, which returns adq = amdq + apdq). */
+static void rp_sw1d(const ocl_params *p, int mx, const double *ql, const double *qr,
+                    double *wave, double *s, double *amdq, double *apdq, int cell_internal) {
+  const int mbc = p->mbc, meqn = 2, mwaves = 2;
+  const long ld = mx + 2 * mbc;
+  const double grav = p->grav;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {                                  /* :46-67 */
+    const double *L = cell_internal ? ql : qr;
+    const double *R = cell_internal ? qr : ql;
+    const int il = cell_internal ? i : i - 1;
+#define QLT(m) L2(L, il, m)
+#define QRT(m) L2(R, i, m)
+    double ubar = (QLT(2) / sqrt(QLT(1)) + QRT(2) / sqrt(QRT(1))) / (sqrt(QLT(1)) + sqrt(QRT(1)));
+    double cbar = sqrt((0.5 * grav) * (QLT(1) + QRT(1)));
+    double d1 = QRT(1) - QLT(1);
+    double d2 = QRT(2) - QLT(2);
+    double a1 = (0.5 * (-d2 + (ubar + cbar) * d1)) / cbar;
+    double a2 = (0.5 * (d2 - (ubar - cbar) * d1)) / cbar;
+    L3(wave, i, 1, 1) = a1;
+    L3(wave, i, 2, 1) = a1 * (ubar - cbar);
+    L2(s, i, 1) = ubar - cbar;
+    L3(wave, i, 1, 2) = a2;
+    L3(wave, i, 2, 2) = a2 * (ubar + cbar);
+    L2(s, i, 2) = ubar + cbar;
+  }
+  if (!p->efix) {                                                              /* :80-92 */
+    for (int m = 1; m <= 2; ++m)
+      for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double am = 0.0, ap = 0.0;
+        for (int mw = 1; mw <= mwaves; ++mw) {
+          if (L2(s, i, mw) < 0.0) am = am + L2(s, i, mw) * L3(wave, i, m, mw);
+          else ap = ap + L2(s, i, mw) * L3(wave, i, m, mw);
+        }
+        L2(amdq, i, m) = am;
+        L2(apdq, i, m) = ap;
+      }
+    return;
+  }
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {                                  /* :113-173 */
+    const double *L = cell_internal ? ql : qr;
+    const double *R = cell_internal ? qr : ql;
+    const int il = cell_internal ? i : i - 1;
+    double s0 = QLT(2) / QLT(1) - sqrt(grav * QLT(1));
+    if (s0 >= 0.0 && L2(s, i, 1) > 0.0) {
+      for (int m = 1; m <= 2; ++m) L2(amdq, i, m) = 0.0;
+      continue;
+    }
+    double hr1 = QLT(1) + L3(wave, i, 1, 1);
+    double uhr1 = QLT(2) + L3(wave, i, 2, 1);
+    double s1 = uhr1 / hr1 - sqrt(grav * hr1);
+    double sfract;
+    if (s0 < 0.0 && s1 > 0.0) sfract = (s0 * (s1 - L2(s, i, 1))) / (s1 - s0);
+    else if (L2(s, i, 1) < 0.0) sfract = L2(s, i, 1);
+    else sfract = 0.0;
+    for (int m = 1; m <= 2; ++m) L2(amdq, i, m) = sfract * L3(wave, i, m, 1);
+    double s3 = QRT(2) / QRT(1) + sqrt(grav * QRT(1));
+    double hl2 = QRT(1) - L3(wave, i, 1, 2);
+    double uhl2 = QRT(2) - L3(wave, i, 2, 2);
+    double s2 = uhl2 / hl2 + sqrt(grav * hl2);
+    if (s2 < 0.0 && s3 > 0.0) sfract = (s2 * (s3 - L2(s, i, 2))) / (s3 - s2);
+    else if (L2(s, i, 2) < 0.0) sfract = L2(s, i, 2);
+    else continue;
+    for (int m = 1; m <= 2; ++m) L2(amdq, i, m) = L2(amdq, i, m) + sfract * L3(wave, i, m, 2);
+  }
+#undef QLT
+#undef QRT
+  for (int m = 1; m <= 2; ++m)                                                 /* :176-183 */
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+      double df = 0.0;
+      for (int mw = 1; mw <= mwaves; ++mw) df = df + L2(s, i, mw) * L3(wave, i, m, mw);
+      L2(apdq, i, m) = df - L2(amdq, i, m);
+    }
+  (void)meqn;
+}
+
+/* 1-D shallow-water Roe eigenvectors at interface i-1/2 (new; the reference
+ * has none): averages as rp1sw.f:47-49 from q(i-1), q(i); the left
+ * eigenvectors are the rows rp1sw.f:56-57 uses for a1, a2. */
+static void evec_sw1d(const ocl_params *p, int mx, const double *q, double *evl, double *evr) {
+  const int mbc = p->mbc, meqn = 2;
+  const long ld = mx + 2 * mbc;
+  const double grav = p->grav;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    double ubar = (L2(q, i - 1, 2) / sqrt(L2(q, i - 1, 1)) + L2(q, i, 2) / sqrt(L2(q, i, 1))) /
+                  (sqrt(L2(q, i - 1, 1)) + sqrt(L2(q, i, 1)));
+    double cbar = sqrt((0.5 * grav) * (L2(q, i - 1, 1) + L2(q, i, 1)));
+    double ha = 0.5 / cbar;
+    L3(evr, i, 1, 1) = 1.0;          L3(evr, i, 1, 2) = 1.0;
+    L3(evr, i, 2, 1) = ubar - cbar;  L3(evr, i, 2, 2) = ubar + cbar;
+    L3(evl, i, 1, 1) = (ubar + cbar) * ha;     L3(evl, i, 1, 2) = -ha;
+    L3(evl, i, 2, 1) = -((ubar - cbar) * ha);  L3(evl, i, 2, 2) = ha;
+  }
+}
+
 /* apps/acoustics/1d/interface/rp1acv.f:49-80; with ixy it is also the new 2-D
  * normal solver (mu = normal velocity, tangential components carry 0). */
 static void rp_acoustics(const ocl_params *p, int ixy, int mx, const double *ql, const double *qr,
@@ -929,6 +1026,7 @@ int ocl_rp(const ocl_params *p, int ixy, int mx, const double *ql, const double 
     case OCL_RP_ADVECTION2D: rp_advedge(p, ixy, mx, ql, qr, auxl, wave, s, amdq, apdq); return 0;
     case OCL_RP_EULER: rp_euler(p, mx, ql, qr, wave, s, amdq, apdq); return 0;
     case OCL_RP_SW2D: rp_sw(p, ixy, mx, ql, qr, wave, s, amdq, apdq, 0); return 0;
+    case OCL_RP_SW1D: rp_sw1d(p, mx, ql, qr, wave, s, amdq, apdq, 0); return 0;
     case OCL_RP_ACOUSTICS1D:
     case OCL_RP_ACOUSTICS2D:
       rp_acoustics(p, ixy, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq); return 0;
@@ -952,6 +1050,17 @@ int ocl_tfluct(const ocl_params *p, int ixy, int mx, const double *ql, const dou
       free(wave); free(am); free(ap);
       return 0;
     }
+    case OCL_RP_SW1D: {
+      /* 1dRadialSymm-qwave/tfluct1sw.f:44-186: left ql(i), right qr(i) */
+      const long ld = mx + 2L * p->mbc;
+      double *wave = (double *)calloc((size_t)ld * 4, sizeof(double));
+      double *am = (double *)calloc((size_t)ld * 2, sizeof(double));
+      double *ap = (double *)calloc((size_t)ld * 2, sizeof(double));
+      rp_sw1d(p, mx, ql, qr, wave, s, am, ap, 1);
+      for (long k = 0; k < ld * 2; ++k) adq[k] = am[k] + ap[k];
+      free(wave); free(am); free(ap);
+      return 0;
+    }
     case OCL_RP_ACOUSTICS1D:
     case OCL_RP_ACOUSTICS2D:
       tfluct_acoustics(p, ixy, mx, ql, qr, auxl, s, adq); return 0;
@@ -967,6 +1076,7 @@ int ocl_evec(const ocl_params *p, int ixy, int mx, const double *q, const double
     case OCL_RP_ADVECTION2D: evec_advection(p, mx, evl, evr); return 0;
     case OCL_RP_EULER: evec_euler(p, mx, q, evl, evr); return 0;
     case OCL_RP_SW2D: evec_sw(p, ixy, mx, q, evl, evr); return 0;
+    case OCL_RP_SW1D: evec_sw1d(p, mx, q, evl, evr); return 0;
     case OCL_RP_ACOUSTICS1D:
     case OCL_RP_ACOUSTICS2D: evec_acoustics(p, ixy, mx, auxl, evl, evr); return 0;
   }
@@ -1128,7 +1238,26 @@ out:
   return rc;
 }
 
-/* src/1d/step1d.f90:2-31, src/2d/step2d.f90:2-41 (with src1/src2 zeroing) */
+/* The app's src(q,dq,aux,t,dt) on a 1-D grid: dq(i,:) for i = 1..mx.
+ *   OCL_SRC_RADIAL_SW     apps/shallowWater/2dRadialDam/1dRadialSymm-qwave/src1.f90:24-28
+ *   OCL_SRC_BATHYMETRY_SW apps/shallowWater/1dPerturbSteady/src1.f90:31-34 */
+static void src1(const ocl_params *p, const double *q, double *dq, const double *aux, double dt) {
+  const int mbc = p->mbc, mx = p->mx;
+  const long ld = mx + 2 * mbc;
+  for (int i = 1; i <= mx; ++i) {
+    if (p->src_term == OCL_SRC_RADIAL_SW) {
+      double rad_pos = p->xlower + ((double)i - 0.5) * p->dx;
+      L2(dq, i, 1) = -(((1.0 * dt) * L2(q, i, 2)) / rad_pos);
+      L2(dq, i, 2) = -((((1.0 * dt) * (L2(q, i, 2) * L2(q, i, 2))) / L2(q, i, 1)) / rad_pos);
+    } else if (p->src_term == OCL_SRC_BATHYMETRY_SW) {
+      L2(dq, i, 1) = 0.0;
+      L2(dq, i, 2) = -(((((1.0 * p->grav) * L2(q, i, 1)) * (L2(aux, i, 1) - L2(aux, i - 1, 1))) / p->dx) * dt);
+    }
+  }
+}
+
+/* src/1d/step1d.f90:2-31, src/2d/step2d.f90:2-41 (with src1/src2 zeroing,
+ * or the app's 1-D source hook) */
 int ocl_step(const ocl_params *p, double *q, double *dq, const double *aux, double dt,
              double t, double *cfl) {
   (void)t;
@@ -1136,6 +1265,12 @@ int ocl_step(const ocl_params *p, double *q, double *dq, const double *aux, doub
   if (rc) return rc;
   const long n = ocl_plane(p) * p->meqn;
   for (long k = 0; k < n; ++k) dq[k] = 0.0;   /* src: interior zeroed; ghosts unused */
+  if (p->ndim == 1 && p->src_term != OCL_SRC_NONE) {
+    if (p->meqn != 2) return -5;
+    if (p->src_term == OCL_SRC_BATHYMETRY_SW && p->maux < 1) return -5;
+    if (p->src_term != OCL_SRC_RADIAL_SW && p->src_term != OCL_SRC_BATHYMETRY_SW) return -5;
+    src1(p, q, dq, aux, dt);
+  }
   if (p->ndim == 1) return ocl_flux1(p, q, dq, aux, dt, cfl, 1, p->mx);
   return flux2(p, q, dq, aux, dt, cfl);
 }

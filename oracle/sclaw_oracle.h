@@ -33,7 +33,16 @@ enum {
   OCL_RP_SW2D = 3,          /* apps/shallowWater/2dRadialDam/{rpn2sw.f,tfluct1sw.f}   */
   OCL_RP_ACOUSTICS1D = 4,   /* apps/acoustics/1d/interface/{rp1acv,tfluct1acv,evec}   */
   OCL_RP_ACOUSTICS2D = 5,   /* new 2-D variable-coefficient acoustics rpn2/tfluct/evec */
-  OCL_RP_ADVECTION2D = 6    /* apps/advection/2d/swirl/rpn2ad1.f (edge velocities)     */
+  OCL_RP_ADVECTION2D = 6,   /* apps/advection/2d/swirl/rpn2ad1.f (edge velocities)     */
+  OCL_RP_SW1D = 7           /* apps/shallowWater/2dRadialDam/1dRadialSymm-qwave/
+                               {rp1sw.f,tfluct1sw.f} + new Roe evec                    */
+};
+
+/* Source-term hooks: the src(q,dq,aux,t,dt) an app links (src/1d/step1d.f90:23). */
+enum {
+  OCL_SRC_NONE = 0,         /* src/1d/src1.f90: dq = 0                                 */
+  OCL_SRC_RADIAL_SW = 1,    /* 1dRadialSymm-qwave/src1.f90: radial shallow water        */
+  OCL_SRC_BATHYMETRY_SW = 2 /* 1dPerturbSteady/src1.f90: -g h b_x, b = aux(:,1)         */
 };
 
 typedef struct {
@@ -53,6 +62,7 @@ typedef struct {
   int mthlim[4];        /* TVD limiter per component/field/wave (lim_type = 1)       */
   int b4step;           /* 0 src/b4step.f90 (no-op), 1 apps/advection/2d/swirl        */
   double tperiod;       /* swirl: common /comvt/ tperiod                              */
+  int src_term;         /* OCL_SRC_* (1-D)                                            */
 } ocl_params;
 
 typedef struct {

@@ -29,11 +29,13 @@ import numpy as np
 
 from . import _capi as C
 from ._capi import (B4STEP_NONE, B4STEP_SWIRL, FP32, FP64, FP64_STRICT, MIXED,  # noqa: F401
-                    RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION, RP_ADVECTION2D, RP_EULER, RP_SW2D,
+                    RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION, RP_ADVECTION2D, RP_EULER, RP_SW1D, RP_SW2D,
+                    SRC_BATHYMETRY_SW, SRC_NONE, SRC_RADIAL_SW,
                     RUN_AUTO, RUN_GRAPH, RUN_RESIDENT, SharpClawError)
 
 __all__ = ["ClawParams", "Solver", "Batch", "sharpclaw", "SharpClawError", "RP_ADVECTION", "RP_EULER",
-           "RP_SW2D", "RP_ACOUSTICS1D", "RP_ACOUSTICS2D", "RP_ADVECTION2D", "B4STEP_NONE", "B4STEP_SWIRL",
+           "RP_SW2D", "RP_ACOUSTICS1D", "RP_ACOUSTICS2D", "RP_ADVECTION2D", "RP_SW1D", "SRC_NONE", "SRC_RADIAL_SW",
+           "SRC_BATHYMETRY_SW", "B4STEP_NONE", "B4STEP_SWIRL",
            "RUN_AUTO", "RUN_GRAPH", "RUN_RESIDENT"]
 
 # plugin id -> (meqn, mwaves, maux, ndim)
@@ -44,6 +46,7 @@ PLUGINS = {
     RP_ACOUSTICS1D: (2, 2, 2, 1),
     RP_ACOUSTICS2D: (3, 2, 2, 2),
     RP_ADVECTION2D: (1, 1, 2, 2),
+    RP_SW1D: (2, 2, 0, 1),
 }
 
 
@@ -74,6 +77,7 @@ class ClawParams:
     grav: float = 1.0
     time_integrator: int = 3
     mthlim: Sequence[int] = field(default_factory=lambda: (1, 1, 1, 1))
+    src_term: int = 0
 
     def __post_init__(self):
         meqn, mwaves, maux, ndim = PLUGINS.get(self.rp, (None, None, 0, None))
@@ -86,7 +90,8 @@ class ClawParams:
         if self.ndim is None:
             self.ndim = ndim
         if self.efix is None:
-            self.efix = 1 if self.rp == RP_EULER else 0
+            # rp1eu.f:40 and 1dRadialSymm-qwave/rp1sw.f: efix .true.; rpn2sw.f:48 .false.
+            self.efix = 1 if self.rp in (RP_EULER, RP_SW1D) else 0
         if self.ndim == 1:
             self.my = 1
 
@@ -109,6 +114,7 @@ class ClawParams:
         p.time_integrator, p.precision = self.time_integrator, precision
         for k in range(4):
             p.mthlim[k] = int(self.mthlim[k]) if k < len(self.mthlim) else 1
+        p.src_term = int(self.src_term)
         return p
 
 

@@ -13,7 +13,8 @@ LIB_PATH = os.path.join(HERE, "libsharpclaw_b200.so")
 
 SCL_OK, SCL_E_INVALID, SCL_E_CUDA, SCL_E_UNSUPPORTED, SCL_E_NONFINITE, SCL_E_TIMEOUT, SCL_E_IO = \
     0, -1, -2, -3, -4, -5, -6
-RP_ADVECTION, RP_EULER, RP_SW2D, RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION2D = 1, 2, 3, 4, 5, 6
+RP_ADVECTION, RP_EULER, RP_SW2D, RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION2D, RP_SW1D = 1, 2, 3, 4, 5, 6, 7
+SRC_NONE, SRC_RADIAL_SW, SRC_BATHYMETRY_SW = 0, 1, 2
 B4STEP_NONE, B4STEP_SWIRL = 0, 1
 RUN_AUTO, RUN_GRAPH, RUN_RESIDENT = 0, 1, 2
 FP64, FP64_STRICT, MIXED, FP32 = 0, 1, 2, 3
@@ -36,6 +37,7 @@ class scl_params(ctypes.Structure):
         ("u", ctypes.c_double), ("gamma", ctypes.c_double), ("grav", ctypes.c_double),
         ("time_integrator", ctypes.c_int), ("precision", ctypes.c_int),
         ("mthlim", ctypes.c_int * 4),
+        ("src_term", ctypes.c_int),
     ]
 
 

@@ -230,6 +230,8 @@ StageArgs make_args(const scl_handle* h, int s) {
   a.dy = h->p.dy;
   for (int k = 0; k < 4; ++k) a.mthbc[k] = h->p.mthbc[k];
   a.mcapa = h->p.mcapa;
+  a.src_term = h->p.src_term;
+  a.xlower = h->p.xlower;
   a.ph.u = h->p.u;
   a.ph.gamma = h->p.gamma;
   a.ph.gamma1 = h->p.gamma - 1.0;
@@ -430,7 +432,15 @@ int validate(const scl_params* p) {
   struct { int rp, meqn, mwaves, maux, ndim; } tab[] = {
       {SCL_RP_ADVECTION, 1, 1, 0, 1}, {SCL_RP_EULER, 3, 3, 0, 1}, {SCL_RP_SW2D, 3, 3, 0, 2},
       {SCL_RP_ACOUSTICS1D, 2, 2, 2, 1}, {SCL_RP_ACOUSTICS2D, 3, 2, 2, 2},
-      {SCL_RP_ADVECTION2D, 1, 1, 2, 2}};
+      {SCL_RP_ADVECTION2D, 1, 1, 2, 2}, {SCL_RP_SW1D, 2, 2, 0, 1}};
+  if (p->src_term != SCL_SRC_NONE) {
+    if (p->src_term != SCL_SRC_RADIAL_SW && p->src_term != SCL_SRC_BATHYMETRY_SW)
+      return fail(SCL_E_INVALID, "src_term must be SCL_SRC_NONE, SCL_SRC_RADIAL_SW or SCL_SRC_BATHYMETRY_SW");
+    if (p->rp != SCL_RP_SW1D || p->ndim != 1)
+      return fail(SCL_E_UNSUPPORTED, "the source-term hooks are the 1-D shallow-water apps' (SCL_RP_SW1D)");
+    if (p->src_term == SCL_SRC_BATHYMETRY_SW && p->maux < 1)
+      return fail(SCL_E_INVALID, "the bathymetry source reads b from aux(:,1): maux >= 1");
+  }
   for (auto& t : tab)
     if (t.rp == p->rp) {
       if (p->meqn != t.meqn || p->mwaves != t.mwaves)

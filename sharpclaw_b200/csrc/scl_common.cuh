@@ -88,6 +88,8 @@ struct StageArgs {
   int mthbc[4];
   int mcapa;                // 1-based aux index of capacity, 0 if none
   Phys ph;
+  int src_term;             // SCL_SRC_* (1-D single grids)
+  double xlower;
 };
 
 // Arguments of a cluster-resident run of a 1-D grid (the whole controller

@@ -8,6 +8,8 @@
 // stages its cells plus ghosts in shared memory, solves one interface per
 // thread into shared memory, then updates one cell per thread.
 #pragma once
+#include <type_traits>
+
 #include "scl_common.cuh"
 #include "scl_plugins.cuh"
 #include "scl_weno.cuh"
@@ -373,7 +375,29 @@ struct Line {
   double dx;
   int bl, br;          // mthbc of the two ends
   int mcapa, kind, stage, ixy;
+  int src = SCL_SRC_NONE;  // source-term hook and the grid's lower edge (radial hook)
+  double xlower = 0.0;
 };
+
+// The source-term hooks, src(q,dq,aux,t,dt) of the app (src/1d/step1d.f90:23):
+// dq of cell c (1-based) from the stage input (h, hu) and the step's dt, in
+// the written evaluation order.
+//   SCL_SRC_RADIAL_SW      1dRadialSymm-qwave/src1.f90:24-28
+//   SCL_SRC_BATHYMETRY_SW  1dPerturbSteady/src1.f90:31-34, b = aux(:,1)
+template <class A, class S>
+__device__ __forceinline__ void source_1d(int kind, const Phys& ph, double xlower, double dx, double dt,
+                                          int c, A h, A hu, const void* aux, A* out) {
+  if (kind == SCL_SRC_RADIAL_SW) {
+    const A rad = (A)(xlower + ((double)c - 0.5) * dx);
+    out[0] = -(((A)dt * hu) / rad);
+    out[1] = -((((A)dt * (hu * hu)) / h) / rad);
+  } else {
+    const S* b = static_cast<const S*>(aux);
+    const A db = (A)b[c + 2] - (A)b[c + 1];
+    out[0] = (A)0;
+    out[1] = -(((((A)ph.grav * h) * db) / (A)dx) * (A)dt);
+  }
+}
 
 template <class P, int PREC, int NT>
 struct Tile1DSmem {
@@ -469,16 +493,33 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
         const S* cap = static_cast<const S*>(L.aux) + (long)(L.mcapa - 1) * L.plane;
         dtdx_c = dt / (L.dx * (double)cap[c + 2]);
       }
+      // dq starts from the source term (zero without one) and loses the
+      // fluctuations, flux1.f90:150-152 / 184-187
+      Ac srcv[M];
+      const bool has_src = L.src != SCL_SRC_NONE;
+      if constexpr (M == 2) {
+        if (has_src)
+          source_1d<Ac, S>(L.src, ph, L.xlower, L.dx, dt, c, (Ac)sm.sq[0][tid + 3], (Ac)sm.sq[1][tid + 3],
+                           L.aux, srcv);
+      }
+      auto dq_of = [&](int m) -> Ac {
+        if constexpr (M == 2) {
+          if (has_src) {
+            if constexpr (std::is_same_v<R, Ac>) return srcv[m] - (R)dtdx_c * br[m];
+            else return srcv[m] + (Ac)((R)0 - (R)dtdx_c * br[m]);
+          }
+        }
+        return (Ac)((R)0 - (R)dtdx_c * br[m]);
+      };
       const int kind = L.kind;
       if (kind == SK_DQ) {
 #pragma unroll
-        for (int m = 0; m < M; ++m)
-          L.dq_out[(long)m * L.plane + c + 2] = (double)((R)0 - (R)dtdx_c * br[m]);
+        for (int m = 0; m < M; ++m) L.dq_out[(long)m * L.plane + c + 2] = (double)dq_of(m);
       } else {
         const bool edge = c <= 3 || c >= mx - 2;   // only these cells have ghost images
 #pragma unroll
         for (int m = 0; m < M; ++m) {
-          Ac dqv = (Ac)((R)0 - (R)dtdx_c * br[m]);
+          Ac dqv = dq_of(m);
           Ac qv = (Ac)sm.sq[m][tid + 3];
           Ac qov = L.qo ? (Ac)L.qo[(long)m * L.plane + c + 2] : (Ac)0;
           Ac o1, o2 = (Ac)0;
@@ -531,6 +572,8 @@ __device__ __forceinline__ Line<S> line1d(const StageArgs& a, const StageDesc& s
   L.kind = sd.kind;
   L.stage = stage;
   L.ixy = a.ixy;
+  L.src = a.src_term;
+  L.xlower = a.xlower;
   return L;
 }
 

@@ -451,6 +451,150 @@ struct PShallow2D {
 };
 
 // ------------------------------------------------------------------------
+// 1-D shallow water: apps/shallowWater/2dRadialDam/1dRadialSymm-qwave/
+// rp1sw.f:46-183 (Roe solver, Harten-Hyman entropy fix when ph.efix, the
+// app's data efix /.true./) and tfluct1sw.f:44-186 of the same app (the same
+// solve with left ql(i), right qr(i); adq = amdq + apdq).
+// ------------------------------------------------------------------------
+struct PShallow1D {
+  static constexpr int MEQN = 2, MWAVES = 2, MAUX = 0, NDIM = 1;
+  static constexpr bool HAS_TFLUCT = true;
+
+  // Roe averages of rp1sw.f:47-49: velocity u, celerity c, ha = 0.5/c (ha
+  // only in the forms that multiply by it).
+  template <class R, bool FD = false>
+  __device__ static void roe(const Phys& ph, const R* L, const R* Rt, R& u, R& c, R& ha) {
+#if SCL_FAST_ROE
+    if constexpr (sizeof(R) == 4) {
+      const float wl = rsqrtf(L[0]), wr = rsqrtf(Rt[0]);
+      u = (L[1] * wl + Rt[1] * wr) * rcp32(L[0] * wl + Rt[0] * wr);
+      const float gh = (0.5f * (float)ph.grav) * (L[0] + Rt[0]);
+      const float ia = rsqrtf(gh);
+      c = gh * ia;
+      ha = 0.5f * ia;
+      return;
+    }
+#endif
+    if constexpr (FD && sizeof(R) == 8) {
+      const double wl = rsqrt(L[0]), wr = rsqrt(Rt[0]);
+      u = (L[1] * wl + Rt[1] * wr) * (1.0 / (L[0] * wl + Rt[0] * wr));
+      const double gh = (0.5 * ph.grav) * (L[0] + Rt[0]);
+      const double ia = rsqrt(gh);
+      c = gh * ia;
+      ha = 0.5 * ia;
+      return;
+    }
+    u = (L[1] / sqrt(L[0]) + Rt[1] / sqrt(Rt[0])) / (sqrt(L[0]) + sqrt(Rt[0]));
+    c = sqrt(((R)0.5 * (R)ph.grav) * (L[0] + Rt[0]));
+    ha = (R)0.5 / c;
+  }
+
+  // The two waves and speeds of rp1sw.f:52-66 (dl = right - left state).
+  template <class R, bool FD = false>
+  __device__ static void wave_set(const Phys& ph, const R* L, const R* Rt, const R* dl, R w[2][2], R* s) {
+    R u, c, ha;
+    roe<R, FD>(ph, L, Rt, u, c, ha);
+    R a1, a2;
+    if constexpr (sizeof(R) == 4 || FD) {
+      a1 = ((u + c) * dl[0] - dl[1]) * ha;
+      a2 = (dl[1] - (u - c) * dl[0]) * ha;
+    } else {
+      a1 = ((R)0.5 * ((u + c) * dl[0] - dl[1])) / c;    // :56, -d2 + x == x - d2
+      a2 = ((R)0.5 * (dl[1] - (u - c) * dl[0])) / c;    // :57
+    }
+    w[0][0] = a1; w[0][1] = a1 * (u - c); s[0] = u - c;
+    w[1][0] = a2; w[1][1] = a2 * (u + c); s[1] = u + c;
+  }
+
+  template <class R, bool FD = false>
+  __device__ static void waves(const Phys& ph, int, const R* L, const R* Rt, const R* dl, const R*,
+                               const R*, R w[2][2], R* s = nullptr) {
+    R sp[2];
+    wave_set<R, FD>(ph, L, Rt, dl, w, sp);
+    if (s) { s[0] = sp[0]; s[1] = sp[1]; }
+  }
+
+  template <class R, bool FD = false>
+  __device__ static void solve(const Phys& ph, const R* L, const R* Rt, const R* dl, R* s, R* amdq,
+                               R* apdq) {
+    R w[2][2];
+    wave_set<R, FD>(ph, L, Rt, dl, w, s);
+    if (!ph.efix) {                                                         // :80-92
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        R am = (R)0, ap = (R)0;
+#pragma unroll
+        for (int mw = 0; mw < 2; ++mw) {
+          if (s[mw] < (R)0) am = am + s[mw] * w[mw][m];
+          else ap = ap + s[mw] * w[mw][m];
+        }
+        amdq[m] = am; apdq[m] = ap;
+      }
+      return;
+    }
+    const R g = (R)ph.grav;
+    do {                                                                    // :113-173
+      R s0 = L[1] / L[0] - sqrt(g * L[0]);
+      if (s0 >= (R)0 && s[0] > (R)0) {
+        amdq[0] = amdq[1] = (R)0;
+        break;
+      }
+      R hr1 = L[0] + w[0][0];
+      R uhr1 = L[1] + w[0][1];
+      R s1 = uhr1 / hr1 - sqrt(g * hr1);
+      R sfract;
+      if (s0 < (R)0 && s1 > (R)0) sfract = (s0 * (s1 - s[0])) / (s1 - s0);
+      else if (s[0] < (R)0) sfract = s[0];
+      else sfract = (R)0;
+      amdq[0] = sfract * w[0][0];
+      amdq[1] = sfract * w[0][1];
+      R s3 = Rt[1] / Rt[0] + sqrt(g * Rt[0]);
+      R hl2 = Rt[0] - w[1][0];
+      R uhl2 = Rt[1] - w[1][1];
+      R s2 = uhl2 / hl2 + sqrt(g * hl2);
+      if (s2 < (R)0 && s3 > (R)0) sfract = (s2 * (s3 - s[1])) / (s3 - s2);
+      else if (s[1] < (R)0) sfract = s[1];
+      else break;
+      amdq[0] = amdq[0] + sfract * w[1][0];
+      amdq[1] = amdq[1] + sfract * w[1][1];
+    } while (0);
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {                                           // :176-183
+      R df = (R)0;
+#pragma unroll
+      for (int mw = 0; mw < 2; ++mw) df = df + s[mw] * w[mw][m];
+      apdq[m] = df - amdq[m];
+    }
+  }
+
+  template <class R, bool FD = false>
+  __device__ static void rp(const Phys& ph, int, const R* L, const R* Rt, const R* dl, const R*,
+                            const R*, R* s, R* amdq, R* apdq) {
+    solve<R, FD>(ph, L, Rt, dl, s, amdq, apdq);
+  }
+  template <class R, bool FD = false>
+  __device__ static void tfluct(const Phys& ph, int, const R* L, const R* Rt, const R* dl, const R*,
+                                R* adq) {
+    R s[2], am[2], ap[2];
+    solve<R, FD>(ph, L, Rt, dl, s, am, ap);
+    adq[0] = am[0] + ap[0];
+    adq[1] = am[1] + ap[1];
+  }
+  // Roe eigenvectors (new; the reference has none): averages of rp1sw.f:47-49,
+  // left eigenvectors the rows rp1sw.f:56-57 uses for a1, a2.
+  template <class R, bool FD = false>
+  __device__ static void evec(const Phys& ph, int, const R* qm, const R* q0, const R*, const R*,
+                              R evl[2][2], R evr[2][2]) {
+    R u, c, ha;
+    roe<R, FD>(ph, qm, q0, u, c, ha);
+    evr[0][0] = (R)1;  evr[0][1] = (R)1;
+    evr[1][0] = u - c; evr[1][1] = u + c;
+    evl[0][0] = (u + c) * ha;    evl[0][1] = -ha;
+    evl[1][0] = -((u - c) * ha); evl[1][1] = ha;
+  }
+};
+
+// ------------------------------------------------------------------------
 // 2-D advection with edge velocities (apps/advection/2d/swirl/rpn2ad1.f:
 // 39-45): aux(i,j,1) = u on the left edge, aux(i,j,2) = v on the bottom edge
 // of cell (i,j); the speed at interface i-1/2 along ixy is aux(i,ixy) of the

@@ -169,3 +169,38 @@ def swirl(n=40, tperiod=0.0, char_decomp=0):
     po.tperiod = tperiod
     ps = S.ClawParams(rp=S.RP_ADVECTION2D, **kw)
     return po, ps, q, np.ascontiguousarray(aux)
+
+
+def radial_sw(mx=200, char_decomp=0, tfluct_solver=0, src=True, efix=1):
+    """Radially symmetric dam break, apps/shallowWater/2dRadialDam/
+    1dRadialSymm-qwave: r in [0, 2.5], h = 2 for r < 0.5 else 1, hu = 0,
+    g = 1, wall at r = 0 and extrapolation outside, rp1sw.f + the radial
+    source term of its src1.f90."""
+    dx = 2.5 / mx
+    xc = (np.arange(mx) + 0.5) * dx
+    q = np.zeros((2, mx + 6))
+    q[0, 3:-3] = np.where(xc < 0.5, 2.0, 1.0)
+    kw = dict(mx=mx, dx=dx, xlower=0.0, mthbc=(3, 1), char_decomp=char_decomp, tfluct_solver=tfluct_solver,
+              grav=1.0, efix=efix)
+    po = O.make_params(meqn=2, mwaves=2, rp=O.RP_SW1D, src_term=O.SRC_RADIAL_SW if src else O.SRC_NONE, **kw)
+    ps = S.ClawParams(rp=S.RP_SW1D, src_term=S.SRC_RADIAL_SW if src else S.SRC_NONE, **kw)
+    return po, ps, q, None
+
+
+def bathymetry_sw(mx=200, eps=0.2, char_decomp=0, tfluct_solver=1):
+    """Perturbation of a lake at rest over a bump, apps/shallowWater/
+    1dPerturbSteady (setaux.f90, qinit.f90, setprob g = 9.81, eps = 0.2) on
+    [0, 2] with extrapolation bc, solved with rp1sw.f and the bathymetry
+    source of that app's src1.f90 (b in aux(:,1))."""
+    dx = 2.0 / mx
+    xa = (np.arange(-3, mx + 3) + 0.5) * dx
+    b = np.where((xa >= 1.4) & (xa <= 1.6), 0.25 * (np.cos(10 * np.pi * (xa - 1.5)) + 1.0), 0.0)
+    aux = b[None, :].copy()
+    q = np.zeros((2, mx + 6))
+    xc = xa[3:-3]
+    q[0, 3:-3] = 1.0 - b[3:-3] + np.where((xc >= 1.1) & (xc <= 1.2), eps, 0.0)
+    kw = dict(mx=mx, dx=dx, xlower=0.0, mthbc=(1, 1), char_decomp=char_decomp, tfluct_solver=tfluct_solver,
+              grav=9.81, maux=1)
+    po = O.make_params(meqn=2, mwaves=2, rp=O.RP_SW1D, src_term=O.SRC_BATHYMETRY_SW, **kw)
+    ps = S.ClawParams(rp=S.RP_SW1D, src_term=S.SRC_BATHYMETRY_SW, **kw)
+    return po, ps, q, aux

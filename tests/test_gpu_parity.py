@@ -62,6 +62,16 @@ STEP_CASES = [
     # apps/advection/2d/swirl: edge-velocity advection (rpn2ad1.f)
     ("swirl", lambda: cases.swirl(n=27)),
     ("swirl_tvd2_wave", lambda: cases.with_tvd(cases.swirl(n=21), (5, 1, 1, 1), 1)),
+    # 1-D shallow water (1dRadialSymm-qwave rp1sw.f / tfluct1sw.f) with the
+    # apps' source terms (src1.f90): radial geometry, bathymetry
+    ("sw1d_radial_src_tf0", lambda: cases.radial_sw(mx=150)),
+    ("sw1d_radial_char_tf1", lambda: cases.radial_sw(mx=120, char_decomp=2, tfluct_solver=1)),
+    ("sw1d_radial_wave", lambda: cases.radial_sw(mx=100, char_decomp=1)),
+    ("sw1d_radial_trans_tf1", lambda: cases.radial_sw(mx=110, char_decomp=3, tfluct_solver=1)),
+    ("sw1d_noefix_nosrc", lambda: cases.radial_sw(mx=90, src=False, efix=0)),
+    ("sw1d_bathymetry_src", lambda: cases.bathymetry_sw(mx=160)),
+    ("sw1d_bathymetry_char_tf0", lambda: cases.bathymetry_sw(mx=140, char_decomp=2, tfluct_solver=0)),
+    ("sw1d_radial_tvd2_char", lambda: cases.with_tvd(cases.radial_sw(mx=100), (2, 3, 1, 1), 2)),
 ]
 
 
@@ -144,6 +154,8 @@ RUN_CASES = [
     ("sw2d_capa_ssp33", lambda: cases.with_capacity(cases.radial_dam(n=21)), 3, dict(tend=0.2, dt_initial=0.01, cfl_max=0.9, cfl_desired=0.8)),
     ("swirl_ssp104", lambda: cases.swirl(n=32), 4, dict(tend=0.6, dt_initial=0.01, cfl_max=2.5, cfl_desired=2.45)),
     ("euler_tvd2_char_ssp33", lambda: cases.with_tvd(cases.shu_osher(mx=160), (4, 4, 4, 1), 2), 3, dict(tend=0.05, dt_initial=0.002, cfl_max=0.9, cfl_desired=0.8)),
+    ("sw1d_radial_ssp104", lambda: cases.radial_sw(mx=200), 4, dict(tend=0.3, dt_initial=0.002, cfl_max=1.0, cfl_desired=0.9)),
+    ("sw1d_bathymetry_ssp104", lambda: cases.bathymetry_sw(mx=200), 4, dict(tend=0.05, dt_initial=0.0005, cfl_max=0.5, cfl_desired=0.2)),
 ]
 
 
@@ -253,3 +265,27 @@ def test_swirl_b4step_run():
     assert res["steps_taken"] == ro.steps_taken and res["rejected"] == ro.rejected
     assert _rel_inf(_interior(qg, 2), _interior(qo, 2)) <= 1e-13
     assert _rel_inf(_interior(qn, 2), _interior(qo, 2)) > 1e-3
+
+
+@pytest.mark.parametrize("case", ["radial", "bathymetry"])
+@pytest.mark.parametrize("precision,tol", [("mixed", 2e-6), ("fp32", 2e-5)])
+def test_reduced_precision_sw1d_source(precision, tol, case):
+    """The FP32 forms with a source term against the FP64 oracle (relative L1
+    of each component): the source is evaluated in the state's type (FP64 in
+    the mixed form)."""
+    if case == "radial":
+        po, ps, q, aux = cases.radial_sw(mx=400)
+        run = dict(tend=0.3, dt_initial=0.001, cfl_max=1.0, cfl_desired=0.9)
+    else:
+        po, ps, q, aux = cases.bathymetry_sw(mx=400)
+        run = dict(tend=0.05, dt_initial=0.0005, cfl_max=0.5, cfl_desired=0.2)
+    ps.time_integrator = 4
+    qo, ro = O.sharpclaw(po, q, aux, tstart=0.0, time_integrator=4, **run)
+    with S.Solver(ps, precision) as s:
+        s.set_aux(aux) if aux is not None else None
+        s.set_q(q)
+        s.sharpclaw(0.0, run["tend"], run["dt_initial"], run["cfl_max"], run["cfl_desired"])
+        qg = s.get_q()
+    for m in range(2):
+        rel = np.abs(qg[m, 3:-3] - qo[m, 3:-3]).sum() / np.abs(qo[m, 3:-3]).sum()
+        assert rel <= tol, (m, rel)

@@ -28,6 +28,8 @@ CASES = [
     # several tiles per CTA (40 tiles on a cluster of 8)
     ("advection_5000_ssp42", lambda: cases.advection(mx=5000), 2, dict(tend=0.02, dt_initial=0.0001, cfl_max=1.9, cfl_desired=1.8)),
     ("euler_5000", lambda: cases.shu_osher(mx=5000), 3, dict(tend=0.01, dt_initial=0.0001, cfl_max=0.9, cfl_desired=0.8)),
+    # 1-D shallow water with the radial source term (src1.f90 of 1dRadialSymm-qwave)
+    ("sw1d_radial_src", lambda: cases.radial_sw(mx=300), 4, dict(tend=0.2, dt_initial=0.002, cfl_max=1.0, cfl_desired=0.9)),
     # first step rejected and retaken
     ("euler_reject", lambda: cases.shu_osher(mx=120), 3, dict(tend=0.05, dt_initial=0.05, cfl_max=0.9, cfl_desired=0.8)),
 ]

@@ -125,3 +125,72 @@ def test_roe_property_euler_and_sw():
         for i in range(1, n):
             df = flux(ql[:, i]) - flux(qr[:, i - 1])
             assert np.allclose(am[:, i] + ap[:, i], df, rtol=1e-10, atol=1e-10)
+
+
+def test_sw1d_roe_property_and_eigenvectors():
+    """rp1sw.f (with and without its entropy fix): amdq + apdq = f(right) -
+    f(left); the new 1-D shallow-water eigenvectors are inverse pairs."""
+    rng = np.random.default_rng(13)
+    n = 20
+    h = rng.uniform(0.5, 2.0, n)
+    hu = h * rng.uniform(-2, 2, n)
+    q = np.stack([h, hu])
+
+    def flux(s):
+        return np.array([s[1], s[1] * s[1] / s[0] + 0.5 * s[0] * s[0]])
+    for efix in (0, 1):
+        p = O.make_params(mx=n - 6, meqn=2, mwaves=2, dx=0.1, rp=O.RP_SW1D, efix=efix, mthbc=(1, 1))
+        wave, s, am, ap = O.rp(p, q.copy(), q.copy())
+        for i in range(1, n):
+            df = flux(q[:, i]) - flux(q[:, i - 1])
+            assert np.allclose(am[:, i] + ap[:, i], df, rtol=1e-10, atol=1e-10)
+    evl, evr = O.evec(p, q, ixy=1)
+    for i in range(1, n):
+        assert np.allclose(evl[:, :, i].T @ evr[:, :, i].T, np.eye(2), atol=1e-12)
+
+
+@pytest.mark.parametrize("src", ["radial", "bathymetry"])
+@pytest.mark.parametrize("tfluct_solver", [0, 1])
+def test_source_term_known_answer(src, tfluct_solver):
+    """On a uniform state every fluctuation is exactly zero, so the step's dq
+    is the app's src1.f90 formula, evaluated here in numpy in the same order."""
+    if src == "radial":
+        po, _, q, aux = cases.radial_sw(mx=40, tfluct_solver=tfluct_solver)
+        po.mthbc[0] = 1
+    else:
+        po, _, q, aux = cases.bathymetry_sw(mx=40, tfluct_solver=tfluct_solver)
+    q[0, :], q[1, :] = 1.3, 0.4
+    dt = 0.01
+    _, dq, _ = O.step(po, q, aux, dt)
+    i = np.arange(1, po.mx + 1)
+    want = np.zeros((2, po.mx))
+    if src == "radial":
+        rad = po.xlower + (i - 0.5) * po.dx
+        want[0] = -((dt * q[1, i + 2]) / rad)
+        want[1] = -(((dt * (q[1, i + 2] * q[1, i + 2])) / q[0, i + 2]) / rad)
+    else:
+        want[1] = -((((po.grav * q[0, i + 2]) * (aux[0, i + 2] - aux[0, i + 1])) / po.dx) * dt)
+    assert np.array_equal(dq[:, 3:-3], want)
+
+
+def test_radial_sw_reproduces_2d_radial_dam():
+    """The purpose of 1dRadialSymm-qwave: with its radial source term the 1-D
+    solver reproduces the 2-D radial dam break (2dRadialDam, same data) along
+    a ray; without the source term the 1-D (planar) dam break is ten times
+    further off."""
+    n = 100
+    po, _, q, aux = cases.radial_dam(n=n, noise=0.0, char_decomp=0, tfluct_solver=1, mthbc=(1, 1, 1, 1))
+    run = dict(tstart=0.0, tend=0.25, dt_initial=0.005, cfl_max=1.0, cfl_desired=0.9, time_integrator=4)
+    q2, r2 = O.sharpclaw(po, q, aux, **run)
+    xs = po.xlower + (np.arange(n) + 0.5) * po.dx
+    j = n // 2
+    h2 = q2[0, 3 + j, 3:-3]
+    errs = {}
+    for src in (True, False):
+        p1, _, q1, _ = cases.radial_sw(mx=50, src=src)
+        q1f, r1 = O.sharpclaw(p1, q1, None, **run)
+        assert r1.info == 0 and r1.tend == 0.25
+        xc = (np.arange(p1.mx) + 0.5) * p1.dx
+        h1 = np.interp(np.sqrt(xs ** 2 + xs[j] ** 2), xc, q1f[0, 3:-3])
+        errs[src] = np.abs(h2 - h1).sum() / np.abs(h2).sum()
+    assert errs[True] < 0.005 and errs[False] > 0.03, errs
