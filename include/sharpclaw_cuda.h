@@ -79,8 +79,11 @@ typedef struct scl_params {
   int ndim;             /* 1 or 2                                                  */
   int mx, my;           /* nx(1), nx(2)                                            */
   int meqn, mwaves, mbc, maux, mcapa;
-  int lim_type;         /* 2 = WENO5, 1 = second-order TVD (reconstruct.f90)       */
-  int char_decomp;      /* 0 weno5, 1 weno5_wave, 2 weno5_char, 3 weno5_trans      */
+  int lim_type;         /* 2 = WENO5, 1 = second-order TVD (reconstruct.f90),
+                           0 = unlimited polynomial of order mthlim(1) = 3
+                           (polyrecon.f90; single grids, not the batched solver)  */
+  int char_decomp;      /* 0 weno5, 1 weno5_wave, 2 weno5_char, 3 weno5_trans
+                           (TVD: 0..2, polynomial: 0 q2qlqr_poly, 1 _poly_wave)   */
   int tfluct_solver;    /* 1 tfluct plugin, 0 swap + second rp (flux1.f90:136-188) */
   int mthbc[4];         /* 1 extrapolation, 2 periodic, 3 solid wall               */
   double dx, dy, xlower, ylower;
@@ -91,7 +94,8 @@ typedef struct scl_params {
   int precision;        /* SCL_FP64, SCL_FP64_STRICT, SCL_MIXED, SCL_FP32          */
   int mthlim[4];        /* TVD limiter per component / field / wave (lim_type = 1):
                            1 minmod, 2 superbee, 3 van Leer, 4 MC, 5 Cada-Torrilhon
-                           (ClawParams%mthlim, reconstruct.f90:551-571)          */
+                           (ClawParams%mthlim, reconstruct.f90:551-571); with
+                           lim_type = 0, mthlim[0] is the order (3)              */
   int src_term;         /* SCL_SRC_* (ClawParams%src_term; the reference links the
                            app's src1.f90 instead)                                */
 } scl_params;
@@ -181,7 +185,7 @@ int scl_kernels_per_step(scl_handle* h);
  * whole loop in one launch (per 4096 iterations), for 1-D grids of at most
  * 64 tiles of 127 cells (8128 cells) without a b4step hook; SCL_E_UNSUPPORTED
  * otherwise.  SCL_RUN_AUTO (the default): resident for 1-D grids of at most
- * 16 tiles (2032 cells), graphs for the rest.  Both modes run the same tile
+ * 8 tiles (1016 cells: one tile per CTA), graphs for the rest.  Both modes run the same tile
  * arithmetic and controller, so their results are identical, except in the
  * FP32 forms of 1-D Euler (char_decomp 0/2, tfluct_solver 0), whose graph
  * path uses a paired kernel with a different FP32 contraction order. */

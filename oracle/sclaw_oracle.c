@@ -452,6 +452,67 @@ int ocl_tvd2_wave(int mx2, int meqn, int mwaves, const double *q, const int *mth
   return 0;
 }
 
+/* polyrecon.f90:5-79 (q2qlqr_poly, lim_type 0, char_decomp 0): unlimited
+ * upwind-centred reconstruction of order mthlim(1) = 3 (c(-1) = 1/6,
+ * c(0) = 2/6).  The reference loops over interfaces i = k+1 .. mx-k-1 only
+ * and leaves ql/qr of interfaces 1, mx-1, mx, mx+1 as the workspace held them
+ * (undefined); here every interface whose stencil lies in the ghost cells gets
+ * the same formula, a documented deviation.  Order 7 needs four ghost cells
+ * and is rejected (mbc = 3). */
+int ocl_poly(int mx2, int meqn, const double *q, int order, double *ql, double *qr) {
+  if (order != 3) return -5;
+  const int k = (order - 1) / 2;
+  const double cm1 = 1.0 / 6.0, c0 = 2.0 / 6.0;                               /* :27-29 */
+  for (int m = 1; m <= meqn; ++m)
+    for (int i = 1 + k + 1; i <= mx2 - k; ++i) {                               /* 1-based line index */
+      double tm1 = R2(q, i - 1, m) - R2(q, i - 2, m);                          /* theta(j) = du(i+j) */
+      double t0 = R2(q, i, m) - R2(q, i - 1, m);
+      double tp1 = R2(q, i + 1, m) - R2(q, i, m);
+      double ur = (0.0 + cm1 * tm1) + c0 * t0;                                 /* :66-69 */
+      double ul = (0.0 + cm1 * tp1) + c0 * t0;
+      R2(qr, i - 1, m) = R2(q, i - 1, m) + ur;                                 /* :56-57, 73-75 */
+      R2(ql, i, m) = R2(q, i, m) - ul;
+    }
+  return 0;
+}
+
+/* polyrecon.f90:176-253 (q2qlqr_poly_wave, lim_type 0, char_decomp 1): the
+ * same stencil on the projections theta(j) = wave(i+j).wave(i) of each wave
+ * family, skipped when theta(0) <= 1e-14 (a REAL(4) literal), order 3. */
+int ocl_poly_wave(int mx2, int meqn, int mwaves, const double *q, int order, const double *wave,
+                  double *ql, double *qr) {
+  if (order != 3) return -5;
+  const int k = (order - 1) / 2;
+  const double cm1 = 1.0 / 6.0, c0 = 2.0 / 6.0;
+  const double floor14 = (double)1.0e-14f;
+#define W(i, m, mw) R3(wave, i, m, mw)
+  for (int i = 1 + k + 1; i <= mx2 - k; ++i) {
+    for (int m = 1; m <= meqn; ++m) {                                          /* :218-222 */
+      R2(qr, i - 1, m) = R2(q, i - 1, m);
+      R2(ql, i, m) = R2(q, i, m);
+    }
+    for (int mw = 1; mw <= mwaves; ++mw) {
+      double theta[3];
+      for (int j = -1; j <= 1; ++j) {                                          /* :226-231 */
+        double t = W(i + j, 1, mw) * W(i, 1, mw);
+        for (int m = 2; m <= meqn; ++m) t = t + W(i + j, m, mw) * W(i, m, mw);
+        theta[j + 1] = t;
+      }
+      if (theta[1] > floor14) {                                                /* :233-247 */
+        double wavenormed = 1.0 / theta[1];
+        double ur = (0.0 + cm1 * theta[0]) + c0 * theta[1];
+        double ul = (0.0 + cm1 * theta[2]) + c0 * theta[1];
+        for (int m = 1; m <= meqn; ++m) {
+          R2(qr, i - 1, m) = R2(qr, i - 1, m) + (ur * wavenormed) * W(i, m, mw);
+          R2(ql, i, m) = R2(ql, i, m) - (ul * wavenormed) * W(i, m, mw);
+        }
+      }
+    }
+  }
+#undef W
+  return 0;
+}
+
 /* reconstruct.f90:146-241 */
 int ocl_weno5_char(int mx2, int meqn, const double *q, const double *evl,
                    const double *evr, double *ql, double *qr) {
@@ -1092,7 +1153,7 @@ int ocl_flux1(const ocl_params *p, const double *q1d, double *dq1d, const double
   const long ld = mx + 2 * mbc;
   const int mx2 = (int)ld;
   int rc = 0;
-  if (p->lim_type != 1 && p->lim_type != 2) return -5;
+  if (p->lim_type < 0 || p->lim_type > 2) return -5;
   double dx = (ixy == 1) ? p->dx : p->dy;
   double *dtdx = (double *)calloc((size_t)ld, sizeof(double));
   double *ql = (double *)calloc((size_t)ld * meqn, sizeof(double));
@@ -1117,7 +1178,16 @@ int ocl_flux1(const ocl_params *p, const double *q1d, double *dq1d, const double
   if (p->ndim > 1)                                                            /* :62 */
     for (long k = 0; k < ld * meqn; ++k) dq1d[k] = 0.0;
 
-  if (p->lim_type == 1) {                                                    /* :78-91 */
+  if (p->lim_type == 0) {                                                    /* :65-76 */
+    switch (p->char_decomp) {
+      case 0: rc = ocl_poly(mx2, meqn, q1d, p->mthlim[0], ql, qr); break;
+      case 1:
+        rc = ocl_rp(p, ixy, mx, q1d, q1d, aux1d, aux1d, wave, s, amdq, apdq);
+        if (!rc) rc = ocl_poly_wave(mx2, meqn, mwaves, q1d, p->mthlim[0], wave, ql, qr);
+        break;
+      default: rc = -5;
+    }
+  } else if (p->lim_type == 1) {                                             /* :78-91 */
     switch (p->char_decomp) {
       case 0: rc = ocl_tvd2(mx2, meqn, q1d, p->mthlim, ql, qr); break;
       case 1:

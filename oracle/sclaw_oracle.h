@@ -49,7 +49,8 @@ typedef struct {
   int ndim;             /* 1 or 2                                  ClawParams%ndim  */
   int mx, my;           /* interior cells                          ClawParams%nx    */
   int meqn, mwaves, mbc, maux, mcapa;
-  int lim_type;         /* 2 WENO5, 1 TVD (reconstruct.f90:525-763)                  */
+  int lim_type;         /* 2 WENO5, 1 TVD (reconstruct.f90:525-763), 0 unlimited
+                           polynomial (polyrecon.f90, order mthlim(1) = 3)          */
   int char_decomp;      /* 0 componentwise, 2 characteristic-wise                   */
   int tfluct_solver;    /* 1: tfluct plugin, 0: swap + second rp                    */
   int mthbc[4];         /* 1 extrap, 2 periodic, 3 wall                              */
@@ -91,6 +92,9 @@ int ocl_weno5_wave(int mx2, int meqn, int mwaves, const double *q, const double 
                    double *ql, double *qr);
 /* reconstruct.f90:525-761: second-order TVD reconstructions (lim_type = 1) */
 int ocl_tvd2(int mx2, int meqn, const double *q, const int *mthlim, double *ql, double *qr);
+int ocl_poly(int mx2, int meqn, const double *q, int order, double *ql, double *qr);
+int ocl_poly_wave(int mx2, int meqn, int mwaves, const double *q, int order, const double *wave,
+                  double *ql, double *qr);
 int ocl_tvd2_char(int mx2, int meqn, const double *q, const int *mthlim, const double *evl,
                   const double *evr, double *ql, double *qr);
 int ocl_tvd2_wave(int mx2, int meqn, int mwaves, const double *q, const int *mthlim, const double *wave,

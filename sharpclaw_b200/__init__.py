@@ -254,7 +254,7 @@ class Solver:
     def set_run_mode(self, mode: int):
         """RUN_GRAPH: step graphs; RUN_RESIDENT: the whole controller loop in
         one thread-block cluster (1-D grids of at most 8128 cells); RUN_AUTO
-        (default): resident up to 2032 cells."""
+        (default): resident up to 1016 cells."""
         C.check(C.lib().scl_set_run_mode(self._h, int(mode)), "scl_set_run_mode")
 
     def last_run(self):

@@ -345,6 +345,7 @@ int scl_batch_create(const scl_params* p, int ninst, const int* mx, const double
   if (!p || !mx || !dx || !out || ninst < 1) return bfail(SCL_E_INVALID, "bad argument");
   *out = nullptr;
   if (p->ndim != 1) return bfail(SCL_E_INVALID, "batched solver takes 1-D problems");
+  if (p->lim_type == 0) return bfail(SCL_E_UNSUPPORTED, "no polynomial reconstruction (lim_type 0) in the batched solver");
   if (p->mbc != 3 || (p->lim_type != 1 && p->lim_type != 2)) return bfail(SCL_E_INVALID, "need mbc = 3 and lim_type 1 or 2");
   if (p->char_decomp < 0 || p->char_decomp > (p->lim_type == 2 ? 3 : 2)) return bfail(SCL_E_UNSUPPORTED, "char_decomp out of range");
   if (p->precision < SCL_FP64 || p->precision > SCL_FP32) return bfail(SCL_E_INVALID, "bad precision");

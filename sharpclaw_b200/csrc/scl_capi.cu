@@ -105,8 +105,11 @@ __global__ void k_f32_to_f64(const float* a, double* b, long n) {
 }
 
 // Reconstruction code of the stage kernels' CD parameter: char_decomp for
-// WENO5 (lim_type 2), 10 + char_decomp for TVD (lim_type 1).
-int recon_code(const scl_params& p) { return p.lim_type == 1 ? 10 + p.char_decomp : p.char_decomp; }
+// WENO5 (lim_type 2), 10 + char_decomp for TVD (lim_type 1), 20 +
+// char_decomp for the unlimited polynomial (lim_type 0).
+int recon_code(const scl_params& p) {
+  return p.lim_type == 1 ? 10 + p.char_decomp : p.lim_type == 0 ? 20 + p.char_decomp : p.char_decomp;
+}
 
 bool get_launchers(int prec, int rp, int ndim, int cd, int tf, int variant, Launchers* L) {
   switch (prec) {
@@ -408,10 +411,16 @@ int validate(const scl_params* p) {
   if (p->ndim != 1 && p->ndim != 2) return fail(SCL_E_INVALID, "ndim must be 1 or 2");
   if (p->mbc != 3) return fail(SCL_E_INVALID, "WENO5 requires mbc = 3 (reconstruct.f90:85)");
   if (p->mx < 3 || (p->ndim == 2 && p->my < 3)) return fail(SCL_E_INVALID, "need at least 3 cells per direction");
-  if (p->lim_type != 1 && p->lim_type != 2)
-    return fail(SCL_E_UNSUPPORTED, "lim_type must be 1 (TVD) or 2 (WENO5); 0 (polynomial) is not built");
-  if (p->char_decomp < 0 || p->char_decomp > (p->lim_type == 2 ? 3 : 2))
-    return fail(SCL_E_UNSUPPORTED, "char_decomp must be 0..3 with WENO5, 0..2 with TVD (flux1.f90:78-116)");
+  if (p->lim_type < 0 || p->lim_type > 2)
+    return fail(SCL_E_INVALID, "lim_type must be 0 (polynomial), 1 (TVD) or 2 (WENO5)");
+  if (p->char_decomp < 0 || p->char_decomp > (p->lim_type == 2 ? 3 : p->lim_type == 1 ? 2 : 1))
+    return fail(SCL_E_UNSUPPORTED,
+                "char_decomp must be 0..3 with WENO5, 0..2 with TVD, 0..1 with the polynomial (flux1.f90:65-116)");
+  if (p->lim_type == 0 && p->mthlim[0] != 3) {
+    if (p->mthlim[0] == 7)
+      return fail(SCL_E_UNSUPPORTED, "polynomial order 7 needs four ghost cells (mbc = 3 here)");
+    return fail(SCL_E_INVALID, "Invalid reconstruction order: mthlim(1) must be 3 (polyrecon.f90:23-39)");
+  }
   if (p->lim_type == 1)
     for (int k = 0; k < std::max(p->meqn, p->mwaves) && k < 4; ++k)
       if (p->mthlim[k] < 1 || p->mthlim[k] > 5) return fail(SCL_E_INVALID, "mthlim must be 1..5 (reconstruct.f90:551-571)");

@@ -130,6 +130,8 @@ bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
     if (cd == 10 && tf == 0) fill1d<P, 10, 0>(L);
     if (cd == 11 && tf == 0) fill1d<P, 11, 0>(L);
     if (cd == 12 && tf == 0) fill1d<P, 12, 0>(L);
+    if (cd == 20 && tf == 0) fill1d<P, 20, 0>(L);
+    if (cd == 21 && tf == 0) fill1d<P, 21, 0>(L);
     if constexpr (P::HAS_TFLUCT) {
       if (cd == 0 && tf == 1) fill1d<P, 0, 1>(L);
       if (cd == 1 && tf == 1) fill1d<P, 1, 1>(L);
@@ -138,6 +140,8 @@ bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
       if (cd == 10 && tf == 1) fill1d<P, 10, 1>(L);
       if (cd == 11 && tf == 1) fill1d<P, 11, 1>(L);
       if (cd == 12 && tf == 1) fill1d<P, 12, 1>(L);
+      if (cd == 20 && tf == 1) fill1d<P, 20, 1>(L);
+      if (cd == 21 && tf == 1) fill1d<P, 21, 1>(L);
     }
     // the FP32 forms of 1-D Euler step large grids with the paired kernel;
     // a resident run keeps the one-interface tile code
@@ -155,6 +159,8 @@ bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
     if (cd == 10 && tf == 0) return fill2d<P, 10, 0>(variant, L);
     if (cd == 11 && tf == 0) return fill2d<P, 11, 0>(variant, L);
     if (cd == 12 && tf == 0) return fill2d<P, 12, 0>(variant, L);
+    if (cd == 20 && tf == 0) return fill2d<P, 20, 0>(variant, L);
+    if (cd == 21 && tf == 0) return fill2d<P, 21, 0>(variant, L);
     if constexpr (P::HAS_TFLUCT) {
       if (cd == 0 && tf == 1) return fill2d<P, 0, 1>(variant, L);
       if (cd == 1 && tf == 1) return fill2d<P, 1, 1>(variant, L);
@@ -163,6 +169,8 @@ bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
       if (cd == 10 && tf == 1) return fill2d<P, 10, 1>(variant, L);
       if (cd == 11 && tf == 1) return fill2d<P, 11, 1>(variant, L);
       if (cd == 12 && tf == 1) return fill2d<P, 12, 1>(variant, L);
+      if (cd == 20 && tf == 1) return fill2d<P, 20, 1>(variant, L);
+      if (cd == 21 && tf == 1) return fill2d<P, 21, 1>(variant, L);
     }
   }
   return false;

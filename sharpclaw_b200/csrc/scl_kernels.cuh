@@ -220,6 +220,22 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs, 
 #pragma unroll
         for (int m = 0; m < M; ++m) d3[j][m] = q[j + 2][m] - q[j + 1][m];
       tvd2_char_core<double, M>(d3, evl, evr, ph.mthlim, q[2], q[3], xl, xr);
+    } else if constexpr (CD == 20) {                      // lim_type 0: q2qlqr_poly
+      poly3_exact<M>(q, xl, xr);
+    } else if constexpr (CD == 21) {                      // lim_type 0: q2qlqr_poly_wave
+      double w[3][MW][M], ak[4][MA > 0 ? MA : 1];
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int i = 0; i < MA; ++i) ak[j][i] = (double)as(j + 1, i);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {                       // interfaces c-1, c, c+1 (flux1.f90:73-75)
+        double dk[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) dk[m] = q[j + 2][m] - q[j + 1][m];
+        P::template waves<double, FD>(ph, ixy, q[j + 1], q[j + 2], dk, ak[j], ak[j + 1], w[j]);
+      }
+      poly3_wave_core<double, M, MW>(w, q[2], q[3], xl, xr);
     } else {
       weno5_exact<M, FD>(q, xl, xr);
     }
@@ -302,6 +318,22 @@ __device__ __forceinline__ void solve_interface(const Phys& ph, int ixy, QS qs, 
       }
       evec_f32<P>(ph, ixy, qm, q0, auxm, aux0, evl, evr);
       tvd2_char_core<float, M>(d3, evl, evr, ph.mthlim, z, z, xl, xr);
+    } else if constexpr (CD == 20) {
+      poly3_offset<M>(d, xl, xr);
+    } else if constexpr (CD == 21) {
+      float qf[4][M], ak[4][MA > 0 ? MA : 1], w[3][MW][M], z[M];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+#pragma unroll
+        for (int m = 0; m < M; ++m) qf[j][m] = (float)qs(j + 1, m);
+#pragma unroll
+        for (int i = 0; i < MA; ++i) ak[j][i] = (float)as(j + 1, i);
+      }
+#pragma unroll
+      for (int m = 0; m < M; ++m) z[m] = 0.0f;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) P::template waves<float>(ph, ixy, qf[j], qf[j + 1], d[j + 1], ak[j], ak[j + 1], w[j]);
+      poly3_wave_core<float, M, MW>(w, z, z, xl, xr);
     } else {
       weno5_offset<M>(d, xl, xr);
     }

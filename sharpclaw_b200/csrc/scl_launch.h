@@ -16,7 +16,7 @@ struct Launchers {
 // are allowed, and controller iterations per launch.
 constexpr int RES_NT = 128;
 constexpr int RES_CLUSTER = 8;
-constexpr int RES_AUTO_TILES = 16;
+constexpr int RES_AUTO_TILES = 8;   // one tile per CTA: beyond it the graphs are faster
 constexpr int RES_MAX_TILES = 64;
 constexpr int RES_ITERS = 4096;
 

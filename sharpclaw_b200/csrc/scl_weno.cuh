@@ -538,4 +538,70 @@ __device__ __forceinline__ void tvd2_wave_core(const T w[3][MW][M], const T s[MW
   }
 }
 
+// ---------------------------------------------------------------------------
+// Unlimited polynomial reconstruction of order 3 (lim_type 0, polyrecon.f90):
+// c(-1) = 1/6, c(0) = 2/6 (:27-29); ur and ul accumulate from 0 in the
+// reference's order (:66-69); qr(c-1) = q(c-1) + ur, ql(c) = q(c) - ul.
+// ---------------------------------------------------------------------------
+template <int M>
+__device__ __forceinline__ void poly3_exact(const double q[6][M], double qrl[M], double qlr[M]) {
+  const double cm1 = 1.0 / 6.0, c0 = 2.0 / 6.0;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const double tm1 = q[2][m] - q[1][m], t0 = q[3][m] - q[2][m], tp1 = q[4][m] - q[3][m];
+    const double ur = (0.0 + cm1 * tm1) + c0 * t0;
+    const double ul = (0.0 + cm1 * tp1) + c0 * t0;
+    qrl[m] = q[2][m] + ur;
+    qlr[m] = q[3][m] - ul;
+  }
+}
+
+// offsets er = qr(c-1)-q(c-1), el = ql(c)-q(c) from the jumps d[k] (FP32 forms)
+template <int M>
+__device__ __forceinline__ void poly3_offset(const float d[5][M], float er[M], float el[M]) {
+  const float cm1 = (float)(1.0 / 6.0), c0 = (float)(2.0 / 6.0);
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    er[m] = (0.0f + cm1 * d[1][m]) + c0 * d[2][m];
+    el[m] = -((0.0f + cm1 * d[3][m]) + c0 * d[2][m]);
+  }
+}
+
+// q2qlqr_poly_wave (polyrecon.f90:214-251), order 3: per wave family the
+// projections theta(j) = wave(c+j).wave(c), j = -1..1 (w[0..2] = waves of
+// interfaces c-1, c, c+1), skipped when theta(0) <= 1e-14 (a REAL(4) literal);
+// base = the cell values (exact form) or 0 (offset form).
+template <class T, int M, int MW>
+__device__ __forceinline__ void poly3_wave_core(const T w[3][MW][M], const T* base_r, const T* base_l, T xr[M],
+                                                T xl[M]) {
+  const T floor14 = (T)(double)1.0e-14f;
+  const T cm1 = (T)(1.0 / 6.0), c0 = (T)(2.0 / 6.0);
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    xr[m] = base_r[m];
+    xl[m] = base_l[m];
+  }
+#pragma unroll
+  for (int mw = 0; mw < MW; ++mw) {
+    T th[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      T t = w[j][mw][0] * w[1][mw][0];
+#pragma unroll
+      for (int m = 1; m < M; ++m) t = t + w[j][mw][m] * w[1][mw][m];
+      th[j] = t;
+    }
+    if (th[1] > floor14) {
+      const T wn = (T)1 / th[1];
+      const T ur = ((T)0 + cm1 * th[0]) + c0 * th[1];
+      const T ul = ((T)0 + cm1 * th[2]) + c0 * th[1];
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        xr[m] = xr[m] + (ur * wn) * w[1][mw][m];
+        xl[m] = xl[m] - (ul * wn) * w[1][mw][m];
+      }
+    }
+  }
+}
+
 }  // namespace scl

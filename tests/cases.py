@@ -148,6 +148,17 @@ def with_tvd(case, mthlim=(1, 1, 1, 1), char_decomp=0):
     return po, ps, q, aux
 
 
+def with_poly(case, char_decomp=0):
+    """Switch a case to the unlimited polynomial reconstruction of order 3
+    (lim_type = 0, polyrecon.f90: 0 q2qlqr_poly, 1 q2qlqr_poly_wave)."""
+    po, ps, q, aux = case
+    po.lim_type = ps.lim_type = 0
+    po.char_decomp = ps.char_decomp = char_decomp
+    po.mthlim[0] = 3
+    ps.mthlim = (3,) + tuple(ps.mthlim[1:])
+    return po, ps, q, aux
+
+
 def swirl(n=40, tperiod=0.0, char_decomp=0):
     """apps/advection/2d/swirl: [0,1]^2, extrapolation bc, edge velocities
     from the stream function psi = sin^2(pi x) sin^2(pi y)/pi (setaux.f,

@@ -39,7 +39,13 @@ def test_version_string():
 @pytest.mark.parametrize("change,code", [
     (dict(mbc=2), C.SCL_E_INVALID),
     (dict(mx=2), C.SCL_E_INVALID),
-    (dict(lim_type=0), C.SCL_E_UNSUPPORTED),
+    (dict(lim_type=0), C.SCL_E_UNSUPPORTED),                                   # char_decomp 2
+    (dict(lim_type=0, char_decomp=0, mthlim=(7, 1, 1, 1)), C.SCL_E_UNSUPPORTED),  # needs mbc = 4
+    (dict(lim_type=0, char_decomp=0, mthlim=(5, 1, 1, 1)), C.SCL_E_INVALID),      # polyrecon.f90 stops
+    (dict(lim_type=3), C.SCL_E_INVALID),
+    (dict(src_term=1), C.SCL_E_UNSUPPORTED),                                    # SW1D hooks only
+    (dict(src_term=5), C.SCL_E_INVALID),
+    (dict(rp=S.RP_SW1D, meqn=None, mwaves=None, char_decomp=0, src_term=2), C.SCL_E_INVALID),  # maux 0
     (dict(lim_type=1, char_decomp=3), C.SCL_E_UNSUPPORTED),
     (dict(lim_type=1, mthlim=(1, 6, 1, 1)), C.SCL_E_INVALID),
     (dict(char_decomp=4), C.SCL_E_UNSUPPORTED),

@@ -72,6 +72,15 @@ STEP_CASES = [
     ("sw1d_bathymetry_src", lambda: cases.bathymetry_sw(mx=160)),
     ("sw1d_bathymetry_char_tf0", lambda: cases.bathymetry_sw(mx=140, char_decomp=2, tfluct_solver=0)),
     ("sw1d_radial_tvd2_char", lambda: cases.with_tvd(cases.radial_sw(mx=100), (2, 3, 1, 1), 2)),
+    # unlimited polynomial reconstruction of order 3 (lim_type = 0, polyrecon.f90)
+    ("advection_poly3", lambda: cases.with_poly(cases.advection(mx=100), 0)),
+    ("advection_poly3_wave", lambda: cases.with_poly(cases.advection(mx=90), 1)),
+    ("euler_poly3_wave", lambda: cases.with_poly(cases.riemann(mx=120), 1)),
+    ("acoustics1d_poly3", lambda: cases.with_poly(cases.acoustics1d(mx=100), 0)),
+    ("acoustics1d_poly3_wave", lambda: cases.with_poly(cases.acoustics1d(mx=110), 1)),
+    ("sw1d_poly3_src", lambda: cases.with_poly(cases.radial_sw(mx=90), 0)),
+    ("sw2d_poly3_wave", lambda: cases.with_poly(cases.radial_dam(n=20), 1)),
+    ("acoustics2d_poly3", lambda: cases.with_poly(cases.acoustics2d(n=17, background=0.05), 0)),
 ]
 
 
@@ -156,6 +165,8 @@ RUN_CASES = [
     ("euler_tvd2_char_ssp33", lambda: cases.with_tvd(cases.shu_osher(mx=160), (4, 4, 4, 1), 2), 3, dict(tend=0.05, dt_initial=0.002, cfl_max=0.9, cfl_desired=0.8)),
     ("sw1d_radial_ssp104", lambda: cases.radial_sw(mx=200), 4, dict(tend=0.3, dt_initial=0.002, cfl_max=1.0, cfl_desired=0.9)),
     ("sw1d_bathymetry_ssp104", lambda: cases.bathymetry_sw(mx=200), 4, dict(tend=0.05, dt_initial=0.0005, cfl_max=0.5, cfl_desired=0.2)),
+    ("acoustics_poly3_wave_ssp104", lambda: cases.with_poly(cases.acoustics1d(mx=100), 1), 4, dict(tend=1.0, dt_initial=0.025, cfl_max=2.9, cfl_desired=2.85)),
+    ("sw2d_poly3_ssp33", lambda: cases.with_poly(cases.radial_dam(n=24), 0), 3, dict(tend=0.1, dt_initial=0.01, cfl_max=0.9, cfl_desired=0.8)),
 ]
 
 
@@ -267,12 +278,14 @@ def test_swirl_b4step_run():
     assert _rel_inf(_interior(qn, 2), _interior(qo, 2)) > 1e-3
 
 
-@pytest.mark.parametrize("case", ["radial", "bathymetry"])
-@pytest.mark.parametrize("precision,tol", [("mixed", 2e-6), ("fp32", 2e-5)])
+@pytest.mark.parametrize("case,precision,tol", [("radial", "mixed", 2e-6), ("radial", "fp32", 2e-5),
+                                               ("bathymetry", "mixed", 2e-6), ("bathymetry", "fp32", 2e-4)])
 def test_reduced_precision_sw1d_source(precision, tol, case):
     """The FP32 forms with a source term against the FP64 oracle (relative L1
     of each component): the source is evaluated in the state's type (FP64 in
-    the mixed form)."""
+    the mixed form).  Over the bump the momentum balance is a small difference
+    of two O(g h^2) terms, so with FP32 state the momentum (itself small: only
+    the perturbation moves) carries a larger relative error."""
     if case == "radial":
         po, ps, q, aux = cases.radial_sw(mx=400)
         run = dict(tend=0.3, dt_initial=0.001, cfl_max=1.0, cfl_desired=0.9)

@@ -102,10 +102,10 @@ def test_resident_max_steps():
 
 
 def test_auto_mode():
-    """RUN_AUTO: resident for 1-D grids of at most 16 tiles of 127 cells,
-    graphs for larger grids, 2-D grids and runs with a b4step hook."""
+    """RUN_AUTO: resident for 1-D grids of at most 8 tiles of 127 cells (one
+    per CTA), graphs for larger grids and for 2-D grids."""
     run = dict(tend=0.001, dt_initial=0.0001, cfl_max=0.85, cfl_desired=0.8)
-    for mx, want in ((2032, S.RUN_RESIDENT), (2033, S.RUN_GRAPH)):
+    for mx, want in ((1016, S.RUN_RESIDENT), (1017, S.RUN_GRAPH)):
         _, ps, q, aux = cases.advection(mx=mx)
         assert _run(ps, q, aux, "fp64", S.RUN_AUTO, run)[2][0] == want
     _, ps, q, aux = cases.radial_dam(n=24)
