@@ -443,17 +443,17 @@ def run_gpu(args, rank, world, local_rank):
     if args.workload == "c5" and rank == 0:
         adj = c5_adjoint(S, ps, q0, aux0, W["dt0"])
 
-    kps = s_mix.kernels_per_step
-    # scl_time_steps replays a graph of gs time steps (all nstep when nstep <= 64,
-    # else 160 launches' worth); each replay launches gs * kps kernels plus one begin
-    gs = nstep if nstep <= 64 else max(1, 160 // kps)
-    launches = -(-nstep // gs) * (gs * kps + 1) * args.steps
+    # kernels the library launched in one timed sharpclaw loop (graph nodes
+    # counted one by one; one launch per 4096 steps for a cluster-resident run)
+    run_mode, run_launches = s_mix.last_run()
+    launches = run_launches * args.steps
     ck = clocks.summary()
     if rank == 0:
         cfg = {"workload": W["desc"], "cells": W["cells"], "time_steps_per_step": nstep,
                "stages_per_time_step": W["stages"], "precision": args.precision,
                "l2": "flushed (256 MiB write) between timed steps",
-               "parallelism": "replicas (one independent grid per GPU)"}
+               "parallelism": "replicas (one independent grid per GPU)",
+               "time_loop": "cluster-resident launch" if run_mode == S.RUN_RESIDENT else "CUDA graphs"}
         if ps.ndim == 2:
             cfg["tiles"] = {"headline": s_mix.tiles(), "fp64": s_64.tiles()}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
