@@ -350,7 +350,9 @@ def run_gpu(args, rank, world, local_rank):
                 total_ms += ms
                 taken += res["steps_taken"] - res["rejected"]
                 rejected += res["rejected"]
+                run_record = s.last_run()
         barrier()
+        s.timed_run_record = run_record
         return s, total_ms, res, taken, rejected
 
     clocks = Clocks(local_rank)
@@ -445,7 +447,7 @@ def run_gpu(args, rank, world, local_rank):
 
     # kernels the library launched in one timed sharpclaw loop (graph nodes
     # counted one by one; one launch per 4096 steps for a cluster-resident run)
-    run_mode, run_launches = s_mix.last_run()
+    run_mode, run_launches = s_mix.timed_run_record
     launches = run_launches * args.steps
     ck = clocks.summary()
     if rank == 0:
