@@ -134,6 +134,7 @@ __global__ void __launch_bounds__(NT) k_batch_stage(BatchArgs a) {
     L.kind = a.sd.kind;
     L.stage = a.stage;
     L.ixy = 1;
+    L.dt = ctl->dt;
     stage1d_tile<P, CD, TF, PREC, NT>(L, a.ph, 1 + (t - a.prefix[lo]) * (NT - 1), sm);
   }
 }

@@ -409,6 +409,7 @@ struct Line {
   int mcapa, kind, stage, ixy;
   int src = SCL_SRC_NONE;  // source-term hook and the grid's lower edge (radial hook)
   double xlower = 0.0;
+  double dt = 0.0;         // the controller's dt for this step (read with the roles)
 };
 
 // The source-term hooks, src(q,dq,aux,t,dt) of the app (src/1d/step1d.f90:23):
@@ -452,7 +453,7 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
   constexpr int M = P::MEQN, MW = P::MWAVES, MA = P::MAUX;
   const int tid = threadIdx.x;
   const int mx = L.mx;
-  const double dt = L.ctl->dt;
+  const double dt = L.dt;
   if (tid == 0) sm.dtdx = dt / L.dx;
 
   // stage cells c0-3 .. c0+NT+1 (global offset c+2)
@@ -606,6 +607,7 @@ __device__ __forceinline__ Line<S> line1d(const StageArgs& a, const StageDesc& s
   L.ixy = a.ixy;
   L.src = a.src_term;
   L.xlower = a.xlower;
+  L.dt = ctl->dt;
   return L;
 }
 

@@ -29,6 +29,10 @@ __global__ void __launch_bounds__(NT) k_run1d(RunArgs a) {
   namespace cg = cooperative_groups;
   using S = typename Prec<PREC>::S;
   __shared__ Tile1DSmem<P, PREC, NT> sm;
+  // this step's stage lines (roles and dt are fixed within a step); raw
+  // storage, as shared variables take no constructors
+  __shared__ __align__(16) unsigned char lines_raw[sizeof(Line<S>) * MAXSTAGES];
+  Line<S>* lines = reinterpret_cast<Line<S>*>(lines_raw);
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank(), nc = (int)cl.num_blocks();
   const bool leader = rank == 0 && threadIdx.x == 0;
@@ -43,9 +47,13 @@ __global__ void __launch_bounds__(NT) k_run1d(RunArgs a) {
     // The same value in every thread: the controller writes ctl only before
     // the barrier that follows the last stage of this iteration.
     if (it == a.max_iters || ctl->done) break;
+    // one read of the controller's roles and dt per step, all stages at once
+    if (threadIdx.x < a.nstages) lines[threadIdx.x] = line1d<S>(a.st, a.sd[threadIdx.x], threadIdx.x);
+    __syncthreads();
     for (int s = 0; s < a.nstages; ++s) {
-      const Line<S> L = line1d<S>(a.st, a.sd[s], s);
-      for (int t = rank; t < ntiles; t += nc) stage1d_tile<P, CD, TF, PREC, NT>(L, a.st.ph, 1 + t * (NT - 1), sm);
+      const Line<S> L = lines[s];
+      for (int t = rank; t < ntiles; t += nc)
+        stage1d_tile<P, CD, TF, PREC, NT>(L, a.st.ph, 1 + t * (NT - 1), sm);
       cl.sync();
     }
   }
