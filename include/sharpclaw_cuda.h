@@ -52,6 +52,13 @@ extern "C" {
 #define SCL_RP_ADVECTION2D 6  /* apps/advection/2d/swirl/rpn2ad1.f: edge velocities in aux      */
 #define SCL_RP_SW1D 7         /* apps/shallowWater/2dRadialDam/1dRadialSymm-qwave/{rp1sw.f,
                                  tfluct1sw.f}, entropy fix on by default (+ Roe evec, new)  */
+/* f-wave shallow water (rpf-wave.f90, tfluctf-wave.f90 of each app):        */
+#define SCL_RP_SWF_BATHY 8    /* apps/shallowWater/1dPerturbSteady: bathymetry b = aux(:,1),
+                                 its source in the cell's total fluctuation (maux >= 1)     */
+#define SCL_RP_SWF_RADIAL 9   /* 2dRadialDam/1dRadialSymm-fwave: aux = (r, dx), the radial
+                                 source in the interface flux difference (maux >= 2)       */
+#define SCL_RP_SWF_KAPPA 10   /* 2dRadialDam/1dRadialSymm-fwave-kappa: aux = (r(i-1/2), r, r,
+                                 dx), area-weighted fluxes, capacity aux(:,2) (maux >= 4)  */
 
 /* ---- source terms: the src(q,dq,aux,t,dt) an app links (src/1d/step1d.f90:23),
  * evaluated in the stage kernel before the fluctuations are subtracted;

@@ -985,6 +985,103 @@ static void evec_sw1d(const ocl_params *p, int mx, const double *q, double *evl,
   }
 }
 
+/* The f-wave shallow-water solvers of apps/shallowWater/1dPerturbSteady and
+ * 2dRadialDam/1dRadialSymm-fwave{,-kappa} (rpf-wave.f90:55-122,
+ * tfluctf-wave.f90:55-126 of each): Roe averages, the flux difference of the
+ * app (with its source or area terms) split on the Roe eigenvectors into two
+ * f-waves, amdq/apdq by the sign of the speeds (half each for a NaN speed).
+ * cell_internal: the tfluct variant, left ql(i), right qr(i), which returns
+ * the total fluctuation in amdq (adq = amdq + apdq). */
+static void rp_swf(const ocl_params *p, int mx, const double *ql, const double *qr, const double *auxl,
+                   const double *auxr, double *wave, double *s, double *amdq, double *apdq,
+                   int cell_internal) {
+  const int mbc = p->mbc, meqn = 2;
+  const long ld = mx + 2 * mbc;
+  const double grav = p->grav;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    double hl, ul, hr, ur;
+    if (cell_internal) {
+      hl = L2(ql, i, 1); ul = L2(ql, i, 2) / hl;
+      hr = L2(qr, i, 1); ur = L2(qr, i, 2) / hr;
+    } else {
+      hl = L2(qr, i - 1, 1); ul = L2(qr, i - 1, 2) / hl;
+      hr = L2(ql, i, 1); ur = L2(ql, i, 2) / hr;
+    }
+    double hbar = 0.5 * (hr + hl);
+    double uhat = (sqrt(hl) * ul + sqrt(hr) * ur) / (sqrt(hl) + sqrt(hr));
+    double chat = sqrt(grav * hbar);
+    double f1, f2;
+    if (p->rp == OCL_RP_SWF_BATHY && !cell_internal) {            /* 1dPerturbSteady/rpf-wave.f90:67-68 */
+      f1 = (hr * ur) - (hl * ul);
+      f2 = ((hr * ur) * ur + (0.5 * grav) * (hr * hr)) - ((hl * ul) * ul + (0.5 * grav) * (hl * hl));
+    } else if (p->rp == OCL_RP_SWF_BATHY) {                       /* tfluctf-wave.f90:56-70 */
+      double bl = L2(auxl, i - 1, 1), br = L2(auxr, i + 1, 1);
+      f1 = (hr * ur) - (hl * ul);
+      f2 = (((hr * ur) * ur + ((0.5 * grav) * hr) * hr) - ((hl * ul) * ul + ((0.5 * grav) * hl) * hl)) +
+           ((grav * hbar) * (br - bl)) / 2.0;
+    } else if (p->rp == OCL_RP_SWF_RADIAL && !cell_internal) {    /* 1dRadialSymm-fwave/rpf-wave.f90:69-70 */
+      f1 = ((hr * ur) - (hl * ul)) + ((hbar * uhat) / L2(auxl, i, 1)) * L2(auxl, i, 2);
+      f2 = (((hr * ur) * ur + (0.5 * grav) * (hr * hr)) - ((hl * ul) * ul + (0.5 * grav) * (hl * hl))) +
+           ((hbar * (uhat * uhat)) / L2(auxl, i, 1)) * L2(auxl, i, 2);
+    } else if (p->rp == OCL_RP_SWF_RADIAL) {                      /* tfluctf-wave.f90:68-69 */
+      f1 = (hr * ur) - (hl * ul);
+      f2 = ((hr * ur) * ur + ((0.5 * grav) * hr) * hr) - ((hl * ul) * ul + ((0.5 * grav) * hl) * hl);
+    } else if (!cell_internal) {                                  /* -kappa/rpf-wave.f90:69-70 */
+      f1 = L2(auxl, i, 1) * (hr * ur) - L2(auxr, i - 1, 1) * (hl * ul);
+      f2 = (L2(auxl, i, 1) * ((hr * ur) * ur + ((0.5 * grav) * hr) * hr) -
+            L2(auxr, i - 1, 1) * ((hl * ul) * ul + ((0.5 * grav) * hl) * hl)) -
+           (((0.5 * grav) * hbar) * hbar) * L2(auxl, i, 4);
+    } else {                                                      /* -kappa/tfluctf-wave.f90:68-69 */
+      f1 = L2(auxr, i, 2) * (hr * ur) - L2(auxl, i, 2) * (hl * ul);
+      f2 = L2(auxr, i, 2) * ((hr * ur) * ur + ((0.5 * grav) * hr) * hr) -
+           L2(auxl, i, 3) * ((hl * ul) * ul + ((0.5 * grav) * hl) * hl);
+    }
+    double sp[2] = {uhat - chat, uhat + chat};
+    double R[2][2] = {{1.0, 1.0}, {uhat - chat, uhat + chat}};          /* R(j,k) */
+    double Lm[2][2] = {{(chat + uhat) / (2.0 * chat), -(1.0 / (2.0 * chat))},
+                       {(chat - uhat) / (2.0 * chat), 1.0 / (2.0 * chat)}};   /* L(j,k) */
+    double fd[2] = {f1, f2}, beta[2];
+    for (int j = 0; j < 2; ++j) {
+      double b = 0.0;
+      for (int k = 0; k < 2; ++k) b = b + Lm[j][k] * fd[k];
+      beta[j] = b;
+    }
+    L2(s, i, 1) = sp[0];
+    L2(s, i, 2) = sp[1];
+    for (int j = 0; j < 2; ++j) {
+      double am = 0.0, ap = 0.0;
+      for (int k = 0; k < 2; ++k) {
+        double fw = beta[k] * R[j][k];
+        L3(wave, i, j + 1, k + 1) = fw;
+        if (sp[k] < 0.0) am = am + fw;
+        else if (sp[k] >= 0.0) ap = ap + fw;
+        else { am = am + 0.5 * fw; ap = ap + 0.5 * fw; }
+      }
+      L2(amdq, i, j + 1) = am;
+      L2(apdq, i, j + 1) = ap;
+    }
+  }
+}
+
+/* Roe eigenvectors of the f-wave solvers from q(i-1), q(i) (their R and L,
+ * rpf-wave.f90:71-88). */
+static void evec_swf(const ocl_params *p, int mx, const double *q, double *evl, double *evr) {
+  const int mbc = p->mbc, meqn = 2;
+  const long ld = mx + 2 * mbc;
+  const double grav = p->grav;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    double hl = L2(q, i - 1, 1), ul = L2(q, i - 1, 2) / hl;
+    double hr = L2(q, i, 1), ur = L2(q, i, 2) / hr;
+    double hbar = 0.5 * (hr + hl);
+    double uhat = (sqrt(hl) * ul + sqrt(hr) * ur) / (sqrt(hl) + sqrt(hr));
+    double chat = sqrt(grav * hbar);
+    L3(evr, i, 1, 1) = 1.0;          L3(evr, i, 1, 2) = 1.0;
+    L3(evr, i, 2, 1) = uhat - chat;  L3(evr, i, 2, 2) = uhat + chat;
+    L3(evl, i, 1, 1) = (chat + uhat) / (2.0 * chat);  L3(evl, i, 1, 2) = -(1.0 / (2.0 * chat));
+    L3(evl, i, 2, 1) = (chat - uhat) / (2.0 * chat);  L3(evl, i, 2, 2) = 1.0 / (2.0 * chat);
+  }
+}
+
 /* apps/acoustics/1d/interface/rp1acv.f:49-80; with ixy it is also the new 2-D
  * normal solver (mu = normal velocity, tangential components carry 0). */
 static void rp_acoustics(const ocl_params *p, int ixy, int mx, const double *ql, const double *qr,
@@ -1088,6 +1185,9 @@ int ocl_rp(const ocl_params *p, int ixy, int mx, const double *ql, const double 
     case OCL_RP_EULER: rp_euler(p, mx, ql, qr, wave, s, amdq, apdq); return 0;
     case OCL_RP_SW2D: rp_sw(p, ixy, mx, ql, qr, wave, s, amdq, apdq, 0); return 0;
     case OCL_RP_SW1D: rp_sw1d(p, mx, ql, qr, wave, s, amdq, apdq, 0); return 0;
+    case OCL_RP_SWF_BATHY:
+    case OCL_RP_SWF_RADIAL:
+    case OCL_RP_SWF_KAPPA: rp_swf(p, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq, 0); return 0;
     case OCL_RP_ACOUSTICS1D:
     case OCL_RP_ACOUSTICS2D:
       rp_acoustics(p, ixy, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq); return 0;
@@ -1122,6 +1222,18 @@ int ocl_tfluct(const ocl_params *p, int ixy, int mx, const double *ql, const dou
       free(wave); free(am); free(ap);
       return 0;
     }
+    case OCL_RP_SWF_BATHY:
+    case OCL_RP_SWF_RADIAL:
+    case OCL_RP_SWF_KAPPA: {
+      const long ld = mx + 2L * p->mbc;
+      double *wave = (double *)calloc((size_t)ld * 4, sizeof(double));
+      double *am = (double *)calloc((size_t)ld * 2, sizeof(double));
+      double *ap = (double *)calloc((size_t)ld * 2, sizeof(double));
+      rp_swf(p, mx, ql, qr, auxl, auxr, wave, s, am, ap, 1);
+      for (long k = 0; k < ld * 2; ++k) adq[k] = am[k] + ap[k];     /* tfluctf-wave.f90:121-123 */
+      free(wave); free(am); free(ap);
+      return 0;
+    }
     case OCL_RP_ACOUSTICS1D:
     case OCL_RP_ACOUSTICS2D:
       tfluct_acoustics(p, ixy, mx, ql, qr, auxl, s, adq); return 0;
@@ -1138,6 +1250,9 @@ int ocl_evec(const ocl_params *p, int ixy, int mx, const double *q, const double
     case OCL_RP_EULER: evec_euler(p, mx, q, evl, evr); return 0;
     case OCL_RP_SW2D: evec_sw(p, ixy, mx, q, evl, evr); return 0;
     case OCL_RP_SW1D: evec_sw1d(p, mx, q, evl, evr); return 0;
+    case OCL_RP_SWF_BATHY:
+    case OCL_RP_SWF_RADIAL:
+    case OCL_RP_SWF_KAPPA: evec_swf(p, mx, q, evl, evr); return 0;
     case OCL_RP_ACOUSTICS1D:
     case OCL_RP_ACOUSTICS2D: evec_acoustics(p, ixy, mx, auxl, evl, evr); return 0;
   }

@@ -34,8 +34,13 @@ enum {
   OCL_RP_ACOUSTICS1D = 4,   /* apps/acoustics/1d/interface/{rp1acv,tfluct1acv,evec}   */
   OCL_RP_ACOUSTICS2D = 5,   /* new 2-D variable-coefficient acoustics rpn2/tfluct/evec */
   OCL_RP_ADVECTION2D = 6,   /* apps/advection/2d/swirl/rpn2ad1.f (edge velocities)     */
-  OCL_RP_SW1D = 7           /* apps/shallowWater/2dRadialDam/1dRadialSymm-qwave/
+  OCL_RP_SW1D = 7,          /* apps/shallowWater/2dRadialDam/1dRadialSymm-qwave/
                                {rp1sw.f,tfluct1sw.f} + new Roe evec                    */
+  OCL_RP_SWF_BATHY = 8,     /* apps/shallowWater/1dPerturbSteady/{rpf-wave.f90,
+                               tfluctf-wave.f90}: f-waves, bathymetry b = aux(:,1)     */
+  OCL_RP_SWF_RADIAL = 9,    /* 2dRadialDam/1dRadialSymm-fwave: aux = (r, dx)            */
+  OCL_RP_SWF_KAPPA = 10     /* 2dRadialDam/1dRadialSymm-fwave-kappa: aux = (r(i-1/2),
+                               r(i), r(i), dx), capacity aux(:,2)                      */
 };
 
 /* Source-term hooks: the src(q,dq,aux,t,dt) an app links (src/1d/step1d.f90:23). */

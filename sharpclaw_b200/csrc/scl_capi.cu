@@ -441,7 +441,8 @@ int validate(const scl_params* p) {
   struct { int rp, meqn, mwaves, maux, ndim; } tab[] = {
       {SCL_RP_ADVECTION, 1, 1, 0, 1}, {SCL_RP_EULER, 3, 3, 0, 1}, {SCL_RP_SW2D, 3, 3, 0, 2},
       {SCL_RP_ACOUSTICS1D, 2, 2, 2, 1}, {SCL_RP_ACOUSTICS2D, 3, 2, 2, 2},
-      {SCL_RP_ADVECTION2D, 1, 1, 2, 2}, {SCL_RP_SW1D, 2, 2, 0, 1}};
+      {SCL_RP_ADVECTION2D, 1, 1, 2, 2}, {SCL_RP_SW1D, 2, 2, 0, 1}, {SCL_RP_SWF_BATHY, 2, 2, 1, 1},
+      {SCL_RP_SWF_RADIAL, 2, 2, 2, 1}, {SCL_RP_SWF_KAPPA, 2, 2, 4, 1}};
   if (p->src_term != SCL_SRC_NONE) {
     if (p->src_term != SCL_SRC_RADIAL_SW && p->src_term != SCL_SRC_BATHYMETRY_SW)
       return fail(SCL_E_INVALID, "src_term must be SCL_SRC_NONE, SCL_SRC_RADIAL_SW or SCL_SRC_BATHYMETRY_SW");

@@ -274,6 +274,9 @@ bool SCL_PREC_GETTER(int rp, int ndim, int cd, int tf, int variant, Launchers* L
     case SCL_RP_ACOUSTICS2D: return pick<PAcoustics<3>>(ndim, cd, tf, variant, L);
     case SCL_RP_ADVECTION2D: return pick<PAdvEdge2D>(ndim, cd, tf, variant, L);
     case SCL_RP_SW1D: return ndim == 1 && pick<PShallow1D>(ndim, cd, tf, variant, L);
+    case SCL_RP_SWF_BATHY: return ndim == 1 && pick<PShallowF1D<0>>(ndim, cd, tf, variant, L);
+    case SCL_RP_SWF_RADIAL: return ndim == 1 && pick<PShallowF1D<1>>(ndim, cd, tf, variant, L);
+    case SCL_RP_SWF_KAPPA: return ndim == 1 && pick<PShallowF1D<2>>(ndim, cd, tf, variant, L);
   }
   return false;
 }

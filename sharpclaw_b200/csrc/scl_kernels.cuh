@@ -377,8 +377,9 @@ __device__ __forceinline__ void cell_bracket(const Phys& ph, int ixy, const type
     for (int m = 0; m < M; ++m) br[m] = (apdq_c[m] + adq[m]) + amdq_c1[m];       // :151-152
   } else {
     R s2[P::MWAVES], am2[M], ap2[M];
-    if constexpr (Prec<PREC>::EXACT) P::template rp<R, Prec<PREC>::FD>(ph, ixy, L, Rt, dl, auxc, auxc, s2, am2, ap2);  // :181-182
-    else rp_f32<P>(ph, ixy, L, Rt, dl, auxc, auxc, s2, am2, ap2);
+    const R* a0 = auxc + (tfluct_nb<P>::value ? P::MAUX : 0);   // the cell's own aux
+    if constexpr (Prec<PREC>::EXACT) P::template rp<R, Prec<PREC>::FD>(ph, ixy, L, Rt, dl, a0, a0, s2, am2, ap2);  // :181-182
+    else rp_f32<P>(ph, ixy, L, Rt, dl, a0, a0, s2, am2, ap2);
 #pragma unroll
     for (int m = 0; m < M; ++m) br[m] = ((amdq_c1[m] + apdq_c[m]) + am2[m]) + ap2[m];  // :185-186
   }
@@ -517,9 +518,14 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
         qrc[m] = sm.rec[0][m][tid + 1];
         amc1[m] = sm.rec[2][m][tid + 1];
       }
-      R auxc[MA > 0 ? MA : 1];
+      // the cell's aux (and, for TFLUCT_NB plugins, its neighbours' on both sides)
+      constexpr int NB = tfluct_nb<P>::value ? 3 : 1;
+      R auxc[NB * (MA > 0 ? MA : 1)];
 #pragma unroll
-      for (int k = 0; k < MA; ++k) auxc[k] = load_aux<S>(L.aux, (long)k * L.plane + c + 2);
+      for (int j = 0; j < NB; ++j)
+#pragma unroll
+        for (int k = 0; k < MA; ++k)
+          auxc[j * MA + k] = load_aux<S>(L.aux, (long)k * L.plane + c + 2 + j - (NB - 1) / 2);
       cell_bracket<P, TF, PREC>(ph, L.ixy, qc, auxc, qlc, qrc, apc, amc1, br);
       double dtdx_c = dtdx0;
       if (L.mcapa > 0) {

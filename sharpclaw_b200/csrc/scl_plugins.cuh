@@ -11,6 +11,7 @@
 // is computed from FP64 cell-average jumps, so it keeps the precision of the
 // jump rather than of the states.
 #pragma once
+#include <type_traits>
 #include "scl_common.cuh"
 
 namespace scl {
@@ -593,6 +594,174 @@ struct PShallow1D {
     evl[1][0] = -((u - c) * ha); evl[1][1] = ha;
   }
 };
+
+// ------------------------------------------------------------------------
+// f-wave shallow water, the solvers of three apps (rpf-wave.f90:55-122 and
+// tfluctf-wave.f90:55-126 of each): Roe averages, the app's flux difference
+// split on the Roe eigenvectors into two f-waves, amdq / apdq by the sign of
+// the speeds (half each for a NaN speed).  V selects the app:
+//   0  apps/shallowWater/1dPerturbSteady: bathymetry b = aux(:,1); its source
+//      g hbar (b(i+1) - b(i-1))/2 enters the cell's total fluctuation, which
+//      therefore reads the aux of both neighbours (TFLUCT_NB)
+//   1  2dRadialDam/1dRadialSymm-fwave: aux = (r, dx); the geometric source
+//      hbar (uhat, uhat^2) dx / r enters the interface flux difference
+//   2  2dRadialDam/1dRadialSymm-fwave-kappa: aux = (r(i-1/2), r, r, dx),
+//      area-weighted fluxes (capacity aux(:,2)).
+// ------------------------------------------------------------------------
+template <int V>
+struct PShallowF1D {
+  static constexpr int MEQN = 2, MWAVES = 2, MAUX = V == 0 ? 1 : (V == 1 ? 2 : 4), NDIM = 1;
+  static constexpr bool HAS_TFLUCT = true;
+  static constexpr bool TFLUCT_NB = V == 0;
+
+  // states, velocities and Roe averages (rpf-wave.f90:55-65)
+  template <class R, bool FD>
+  __device__ static void roe(const Phys& ph, const R* L, const R* Rt, R& ul, R& ur, R& hbar, R& uhat, R& chat) {
+    const R hl = L[0], hr = Rt[0];
+    if constexpr (sizeof(R) == 4 || FD) {
+      // sqrt(h) u = m / sqrt(h) = m w for w = 1/sqrt(h)
+      R wl, wr, inv;
+      if constexpr (sizeof(R) == 4) {
+        wl = rsqrtf(hl); wr = rsqrtf(hr);
+        inv = rcp32(hl * wl + hr * wr);
+      } else {
+        wl = rsqrt(hl); wr = rsqrt(hr);
+        inv = (R)1 / (hl * wl + hr * wr);
+      }
+      ul = L[1] * (wl * wl);
+      ur = Rt[1] * (wr * wr);
+      uhat = (L[1] * wl + Rt[1] * wr) * inv;
+    } else {
+      ul = L[1] / hl;
+      ur = Rt[1] / hr;
+      uhat = (sqrt(hl) * ul + sqrt(hr) * ur) / (sqrt(hl) + sqrt(hr));
+    }
+    hbar = (R)0.5 * (hr + hl);
+    chat = sqrt((R)ph.grav * hbar);
+  }
+
+  // the app's flux difference at an interface (CELL false: left qr(i-1),
+  // right ql(i), am = aux(i-1), a0 = aux(i)) or inside a cell (CELL true:
+  // left ql(i), right qr(i); a0 = aux(i), for V = 0 a0 points at aux(i-1..i+1))
+  template <bool CELL, class R>
+  __device__ static void flux_diff(const Phys& ph, const R* L, const R* Rt, R ul, R ur, R hbar, R uhat,
+                                   const R* am, const R* a0, R& f1, R& f2) {
+    const R hl = L[0], hr = Rt[0], g = (R)ph.grav, hg = (R)0.5 * g;
+    if constexpr (V == 0 && !CELL) {                           // 1dPerturbSteady/rpf-wave.f90:67-68
+      f1 = (hr * ur) - (hl * ul);
+      f2 = ((hr * ur) * ur + hg * (hr * hr)) - ((hl * ul) * ul + hg * (hl * hl));
+    } else if constexpr (V == 0) {                             // tfluctf-wave.f90:56-70
+      const R bl = a0[0], br = a0[2];
+      f1 = (hr * ur) - (hl * ul);
+      f2 = (((hr * ur) * ur + (hg * hr) * hr) - ((hl * ul) * ul + (hg * hl) * hl)) + ((g * hbar) * (br - bl)) / (R)2;
+    } else if constexpr (V == 1 && !CELL) {                    // 1dRadialSymm-fwave/rpf-wave.f90:69-70
+      f1 = ((hr * ur) - (hl * ul)) + ((hbar * uhat) / a0[0]) * a0[1];
+      f2 = (((hr * ur) * ur + hg * (hr * hr)) - ((hl * ul) * ul + hg * (hl * hl))) +
+           ((hbar * (uhat * uhat)) / a0[0]) * a0[1];
+    } else if constexpr (V == 1) {                             // tfluctf-wave.f90:68-69
+      f1 = (hr * ur) - (hl * ul);
+      f2 = ((hr * ur) * ur + (hg * hr) * hr) - ((hl * ul) * ul + (hg * hl) * hl);
+    } else if constexpr (!CELL) {                              // -kappa/rpf-wave.f90:69-70
+      f1 = a0[0] * (hr * ur) - am[0] * (hl * ul);
+      f2 = (a0[0] * ((hr * ur) * ur + (hg * hr) * hr) - am[0] * ((hl * ul) * ul + (hg * hl) * hl)) -
+           ((hg * hbar) * hbar) * a0[3];
+    } else {                                                   // -kappa/tfluctf-wave.f90:68-69
+      f1 = a0[1] * (hr * ur) - a0[1] * (hl * ul);
+      f2 = a0[1] * ((hr * ur) * ur + (hg * hr) * hr) - a0[2] * ((hl * ul) * ul + (hg * hl) * hl);
+    }
+  }
+
+  // f-waves fw[k][j] and speeds (rpf-wave.f90:72-103)
+  template <bool CELL, class R, bool FD>
+  __device__ static void fwaves(const Phys& ph, const R* L, const R* Rt, const R* am, const R* a0, R fw[2][2],
+                                R* s) {
+    R ul, ur, hbar, uhat, chat, f1, f2;
+    roe<R, FD>(ph, L, Rt, ul, ur, hbar, uhat, chat);
+    flux_diff<CELL, R>(ph, L, Rt, ul, ur, hbar, uhat, am, a0, f1, f2);
+    s[0] = uhat - chat;
+    s[1] = uhat + chat;
+    R l11, l12, l21, l22;
+    if constexpr (sizeof(R) == 4 || FD) {
+      R i2c;
+      if constexpr (sizeof(R) == 4) i2c = rcp32((R)2 * chat);
+      else i2c = (R)1 / ((R)2 * chat);
+      l11 = (chat + uhat) * i2c; l12 = -i2c;
+      l21 = (chat - uhat) * i2c; l22 = i2c;
+    } else {
+      l11 = (chat + uhat) / ((R)2 * chat); l12 = -((R)1 / ((R)2 * chat));
+      l21 = (chat - uhat) / ((R)2 * chat); l22 = (R)1 / ((R)2 * chat);
+    }
+    const R b1 = ((R)0 + l11 * f1) + l12 * f2;
+    const R b2 = ((R)0 + l21 * f1) + l22 * f2;
+    fw[0][0] = b1 * (R)1; fw[0][1] = b1 * s[0];
+    fw[1][0] = b2 * (R)1; fw[1][1] = b2 * s[1];
+  }
+
+  template <class R>
+  __device__ static void split(const R fw[2][2], const R* s, R* amdq, R* apdq) {   // rpf-wave.f90:106-119
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      R am = (R)0, ap = (R)0;
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        if (s[k] < (R)0) am = am + fw[k][j];
+        else if (s[k] >= (R)0) ap = ap + fw[k][j];
+        else { am = am + (R)0.5 * fw[k][j]; ap = ap + (R)0.5 * fw[k][j]; }
+      }
+      amdq[j] = am; apdq[j] = ap;
+    }
+  }
+
+  template <class R, bool FD = false>
+  __device__ static void rp(const Phys& ph, int, const R* L, const R* Rt, const R*, const R* auxm,
+                            const R* aux0, R* s, R* amdq, R* apdq) {
+    R fw[2][2];
+    fwaves<false, R, FD>(ph, L, Rt, auxm, aux0, fw, s);
+    split<R>(fw, s, amdq, apdq);
+  }
+  template <class R, bool FD = false>
+  __device__ static void waves(const Phys& ph, int, const R* L, const R* Rt, const R*, const R* auxm,
+                               const R* aux0, R w[2][2], R* s = nullptr) {
+    R sp[2];
+    fwaves<false, R, FD>(ph, L, Rt, auxm, aux0, w, sp);
+    if (s) { s[0] = sp[0]; s[1] = sp[1]; }
+  }
+  template <class R, bool FD = false>
+  __device__ static void tfluct(const Phys& ph, int, const R* L, const R* Rt, const R*, const R* aux,
+                                R* adq) {
+    R fw[2][2], s[2], am[2], ap[2];
+    fwaves<true, R, FD>(ph, L, Rt, aux, aux, fw, s);
+    split<R>(fw, s, am, ap);
+    adq[0] = am[0] + ap[0];                                  // tfluctf-wave.f90:121-123
+    adq[1] = am[1] + ap[1];
+  }
+  // Roe eigenvectors R and L of rpf-wave.f90:71-88 from q(i-1), q(i)
+  template <class R, bool FD = false>
+  __device__ static void evec(const Phys& ph, int, const R* qm, const R* q0, const R*, const R*,
+                              R evl[2][2], R evr[2][2]) {
+    R ul, ur, hbar, uhat, chat;
+    roe<R, FD>(ph, qm, q0, ul, ur, hbar, uhat, chat);
+    evr[0][0] = (R)1; evr[0][1] = (R)1;
+    evr[1][0] = uhat - chat; evr[1][1] = uhat + chat;
+    if constexpr (sizeof(R) == 4 || FD) {
+      R i2c;
+      if constexpr (sizeof(R) == 4) i2c = rcp32((R)2 * chat);
+      else i2c = (R)1 / ((R)2 * chat);
+      evl[0][0] = (chat + uhat) * i2c; evl[0][1] = -i2c;
+      evl[1][0] = (chat - uhat) * i2c; evl[1][1] = i2c;
+    } else {
+      evl[0][0] = (chat + uhat) / ((R)2 * chat); evl[0][1] = -((R)1 / ((R)2 * chat));
+      evl[1][0] = (chat - uhat) / ((R)2 * chat); evl[1][1] = (R)1 / ((R)2 * chat);
+    }
+  }
+};
+
+// Plugins whose total fluctuation reads the aux of cells c-1, c, c+1 (three
+// MAUX groups, centre in the middle) declare TFLUCT_NB = true.
+template <class P, class = void>
+struct tfluct_nb : std::false_type {};
+template <class P>
+struct tfluct_nb<P, std::void_t<decltype(P::TFLUCT_NB)>> : std::bool_constant<P::TFLUCT_NB> {};
 
 // ------------------------------------------------------------------------
 // 2-D advection with edge velocities (apps/advection/2d/swirl/rpn2ad1.f:

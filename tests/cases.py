@@ -215,3 +215,36 @@ def bathymetry_sw(mx=200, eps=0.2, char_decomp=0, tfluct_solver=1):
     po = O.make_params(meqn=2, mwaves=2, rp=O.RP_SW1D, src_term=O.SRC_BATHYMETRY_SW, **kw)
     ps = S.ClawParams(rp=S.RP_SW1D, src_term=S.SRC_BATHYMETRY_SW, **kw)
     return po, ps, q, aux
+
+
+def fwave_bathymetry(mx=200, eps=0.2, char_decomp=0, tfluct_solver=1):
+    """apps/shallowWater/1dPerturbSteady as the app runs it: the f-wave solver
+    (rpf-wave.f90) with the bathymetry source inside its tfluct
+    (tfluctf-wave.f90), the library's zero src; data as bathymetry_sw."""
+    po, ps, q, aux = bathymetry_sw(mx=mx, eps=eps, char_decomp=char_decomp, tfluct_solver=tfluct_solver)
+    po.rp, po.src_term = O.RP_SWF_BATHY, O.SRC_NONE
+    ps.rp, ps.src_term = S.RP_SWF_BATHY, S.SRC_NONE
+    return po, ps, q, aux
+
+
+def fwave_radial(mx=200, kappa=False, char_decomp=0, tfluct_solver=1):
+    """The radial dam break of radial_sw with the f-wave solvers of
+    2dRadialDam/1dRadialSymm-fwave (aux = (r, dx), setaux.f90) or, with
+    kappa, 1dRadialSymm-fwave-kappa (aux = (r(i-1/2), r, r, dx), capacity
+    aux(:,2))."""
+    dx = 2.5 / mx
+    xa = (np.arange(-3, mx + 3) + 0.5) * dx
+    if kappa:
+        xi = np.arange(-3, mx + 3) * dx
+        aux = np.ascontiguousarray(np.stack([xi, xa, xa, np.full_like(xa, dx)]))
+        rp_o, rp_s, mcapa = O.RP_SWF_KAPPA, S.RP_SWF_KAPPA, 2
+    else:
+        aux = np.ascontiguousarray(np.stack([xa, np.full_like(xa, dx)]))
+        rp_o, rp_s, mcapa = O.RP_SWF_RADIAL, S.RP_SWF_RADIAL, 0
+    q = np.zeros((2, mx + 6))
+    q[0, 3:-3] = np.where(xa[3:-3] < 0.5, 2.0, 1.0)
+    kw = dict(mx=mx, dx=dx, xlower=0.0, mthbc=(3, 1), char_decomp=char_decomp, tfluct_solver=tfluct_solver,
+              grav=1.0, maux=aux.shape[0], mcapa=mcapa)
+    po = O.make_params(meqn=2, mwaves=2, rp=rp_o, **kw)
+    ps = S.ClawParams(rp=rp_s, **kw)
+    return po, ps, q, aux

@@ -81,6 +81,15 @@ STEP_CASES = [
     ("sw1d_poly3_src", lambda: cases.with_poly(cases.radial_sw(mx=90), 0)),
     ("sw2d_poly3_wave", lambda: cases.with_poly(cases.radial_dam(n=20), 1)),
     ("acoustics2d_poly3", lambda: cases.with_poly(cases.acoustics2d(n=17, background=0.05), 0)),
+    # f-wave shallow water: 1dPerturbSteady, 1dRadialSymm-fwave, -fwave-kappa
+    ("swf_bathy_tf1", lambda: cases.fwave_bathymetry(mx=160)),
+    ("swf_bathy_char_tf0", lambda: cases.fwave_bathymetry(mx=120, char_decomp=2, tfluct_solver=0)),
+    ("swf_bathy_wave", lambda: cases.fwave_bathymetry(mx=110, char_decomp=1)),
+    ("swf_radial_tf1", lambda: cases.fwave_radial(mx=130)),
+    ("swf_radial_trans_tf0", lambda: cases.fwave_radial(mx=100, char_decomp=3, tfluct_solver=0)),
+    ("swf_kappa_tf1", lambda: cases.fwave_radial(mx=120, kappa=True)),
+    ("swf_kappa_char", lambda: cases.fwave_radial(mx=90, kappa=True, char_decomp=2)),
+    ("swf_kappa_tvd2_tf0", lambda: cases.with_tvd(cases.fwave_radial(mx=100, kappa=True, tfluct_solver=0), (4, 2, 1, 1), 0)),
 ]
 
 
@@ -167,6 +176,9 @@ RUN_CASES = [
     ("sw1d_bathymetry_ssp104", lambda: cases.bathymetry_sw(mx=200), 4, dict(tend=0.05, dt_initial=0.0005, cfl_max=0.5, cfl_desired=0.2)),
     ("acoustics_poly3_wave_ssp104", lambda: cases.with_poly(cases.acoustics1d(mx=100), 1), 4, dict(tend=1.0, dt_initial=0.025, cfl_max=2.9, cfl_desired=2.85)),
     ("sw2d_poly3_ssp33", lambda: cases.with_poly(cases.radial_dam(n=24), 0), 3, dict(tend=0.1, dt_initial=0.01, cfl_max=0.9, cfl_desired=0.8)),
+    ("swf_bathy_ssp104", lambda: cases.fwave_bathymetry(mx=200), 4, dict(tend=0.05, dt_initial=0.0005, cfl_max=0.5, cfl_desired=0.2)),
+    ("swf_radial_ssp104", lambda: cases.fwave_radial(mx=200), 4, dict(tend=0.2, dt_initial=0.002, cfl_max=0.3, cfl_desired=0.2)),
+    ("swf_kappa_ssp104", lambda: cases.fwave_radial(mx=100, kappa=True), 4, dict(tend=0.1, dt_initial=0.001, cfl_max=0.3, cfl_desired=0.2)),
 ]
 
 

@@ -30,6 +30,9 @@ CASES = [
     ("euler_5000", lambda: cases.shu_osher(mx=5000), 3, dict(tend=0.01, dt_initial=0.0001, cfl_max=0.9, cfl_desired=0.8)),
     # 1-D shallow water with the radial source term (src1.f90 of 1dRadialSymm-qwave)
     ("sw1d_radial_src", lambda: cases.radial_sw(mx=300), 4, dict(tend=0.2, dt_initial=0.002, cfl_max=1.0, cfl_desired=0.9)),
+    # f-wave shallow water with neighbour aux in tfluct (1dPerturbSteady) and capacity (-kappa)
+    ("swf_bathy", lambda: cases.fwave_bathymetry(mx=400), 4, dict(tend=0.02, dt_initial=0.0005, cfl_max=0.5, cfl_desired=0.2)),
+    ("swf_kappa", lambda: cases.fwave_radial(mx=200, kappa=True), 4, dict(tend=0.01, dt_initial=0.001, cfl_max=0.3, cfl_desired=0.2)),
     # first step rejected and retaken
     ("euler_reject", lambda: cases.shu_osher(mx=120), 3, dict(tend=0.05, dt_initial=0.05, cfl_max=0.9, cfl_desired=0.8)),
 ]

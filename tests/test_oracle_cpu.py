@@ -174,10 +174,10 @@ def test_source_term_known_answer(src, tfluct_solver):
 
 
 def test_radial_sw_reproduces_2d_radial_dam():
-    """The purpose of 1dRadialSymm-qwave: with its radial source term the 1-D
-    solver reproduces the 2-D radial dam break (2dRadialDam, same data) along
-    a ray; without the source term the 1-D (planar) dam break is ten times
-    further off."""
+    """The purpose of the 1dRadialSymm apps: with its radial source term the
+    1-D q-wave solver reproduces the 2-D radial dam break (2dRadialDam, same
+    data) along a ray, as do the two f-wave apps; without the source term the
+    1-D (planar) dam break is ten times further off."""
     n = 100
     po, _, q, aux = cases.radial_dam(n=n, noise=0.0, char_decomp=0, tfluct_solver=1, mthbc=(1, 1, 1, 1))
     run = dict(tstart=0.0, tend=0.25, dt_initial=0.005, cfl_max=1.0, cfl_desired=0.9, time_integrator=4)
@@ -186,14 +186,19 @@ def test_radial_sw_reproduces_2d_radial_dam():
     j = n // 2
     h2 = q2[0, 3 + j, 3:-3]
     errs = {}
-    for src in (True, False):
-        p1, _, q1, _ = cases.radial_sw(mx=50, src=src)
-        q1f, r1 = O.sharpclaw(p1, q1, None, **run)
+    for name, make in (("qwave_src", lambda: cases.radial_sw(mx=50)),
+                       ("planar", lambda: cases.radial_sw(mx=50, src=False)),
+                       ("fwave", lambda: cases.fwave_radial(mx=50)),
+                       ("fwave_kappa", lambda: cases.fwave_radial(mx=50, kappa=True))):
+        p1, _, q1, a1 = make()
+        q1f, r1 = O.sharpclaw(p1, q1, a1, **run)
         assert r1.info == 0 and r1.tend == 0.25
         xc = (np.arange(p1.mx) + 0.5) * p1.dx
         h1 = np.interp(np.sqrt(xs ** 2 + xs[j] ** 2), xc, q1f[0, 3:-3])
-        errs[src] = np.abs(h2 - h1).sum() / np.abs(h2).sum()
-    assert errs[True] < 0.005 and errs[False] > 0.03, errs
+        errs[name] = np.abs(h2 - h1).sum() / np.abs(h2).sum()
+    assert errs["qwave_src"] < 0.005 and errs["planar"] > 0.03, errs
+    # the f-wave apps carry the radial terms in their Riemann solvers instead
+    assert errs["fwave"] < 0.008 and errs["fwave_kappa"] < 0.008, errs
 
 
 @pytest.mark.parametrize("char_decomp", [0, 1])
@@ -216,3 +221,23 @@ def test_polynomial_reconstruction_third_order(char_decomp):
         errs.append(np.abs(qf[0, 3:-3] - q[0, 3:-3]).sum() * dx)
     orders = [np.log2(errs[k] / errs[k + 1]) for k in range(2)]
     assert min(orders) > 2.9, orders
+
+
+def test_fwave_flat_bottom_equals_roe():
+    """With a flat bottom the f-wave splitting of 1dPerturbSteady/rpf-wave.f90
+    gives the Roe fluctuations of rp1sw.f without its entropy fix: the
+    f-waves are s_k times the waves when the Roe matrix maps the jump in q to
+    the jump in the flux."""
+    rng = np.random.default_rng(3)
+    n = 30
+    h = rng.uniform(0.5, 2.0, n)
+    q = np.stack([h, h * rng.uniform(-1, 1, n)])
+    pf = O.make_params(mx=n - 6, meqn=2, mwaves=2, maux=1, dx=0.1, rp=O.RP_SWF_BATHY, grav=9.81, mthbc=(1, 1))
+    pq = O.make_params(mx=n - 6, meqn=2, mwaves=2, dx=0.1, rp=O.RP_SW1D, grav=9.81, efix=0, mthbc=(1, 1))
+    flat = np.zeros((1, n))
+    _, sf, amf, apf = O.rp(pf, q.copy(), q.copy(), flat, flat)
+    _, sq, amq, apq = O.rp(pq, q.copy(), q.copy())
+    scale = np.abs(amq).max() + np.abs(apq).max()
+    assert np.abs(sf[:, 1:] - sq[:, 1:]).max() <= 1e-14 * np.abs(sq).max()
+    assert np.abs(amf[:, 1:] - amq[:, 1:]).max() <= 1e-13 * scale
+    assert np.abs(apf[:, 1:] - apq[:, 1:]).max() <= 1e-13 * scale
