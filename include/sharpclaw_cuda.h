@@ -59,6 +59,10 @@ extern "C" {
                                  source in the interface flux difference (maux >= 2)       */
 #define SCL_RP_SWF_KAPPA 10   /* 2dRadialDam/1dRadialSymm-fwave-kappa: aux = (r(i-1/2), r, r,
                                  dx), area-weighted fluxes, capacity aux(:,2) (maux >= 4)  */
+#define SCL_RP_ACOUSTICS_CONST 11  /* apps/acoustics/1d/homogeneous/{rp1.f,tfluct.f,evec.f}:
+                                      constant rho, bulk (scl_params.rho, .bulk)          */
+#define SCL_RP_ACOUSTICS_FWAVE 12  /* apps/acoustics/1d/fwave/{rp1acfw.f,tfluct1.f,evec.f}:
+                                      q = (strain, momentum), aux = (rho, bulk)          */
 
 /* ---- source terms: the src(q,dq,aux,t,dt) an app links (src/1d/step1d.f90:23),
  * evaluated in the stage kernel before the fluctuations are subtracted;
@@ -105,6 +109,7 @@ typedef struct scl_params {
                            lim_type = 0, mthlim[0] is the order (3)              */
   int src_term;         /* SCL_SRC_* (ClawParams%src_term; the reference links the
                            app's src1.f90 instead)                                */
+  double rho, bulk;     /* SCL_RP_ACOUSTICS_CONST: common /cparam/ rho, bulk       */
 } scl_params;
 
 /* Arguments of sharpclaw() (src/sharpclaw.f90:2-5). */

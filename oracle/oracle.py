@@ -22,6 +22,7 @@ _LIB = os.path.join(_HERE, "libsclaw_oracle.so")
 
 RP_ADVECTION, RP_EULER, RP_SW2D, RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION2D, RP_SW1D = 1, 2, 3, 4, 5, 6, 7
 RP_SWF_BATHY, RP_SWF_RADIAL, RP_SWF_KAPPA = 8, 9, 10
+RP_ACOUSTICS_CONST, RP_ACOUSTICS_FWAVE = 11, 12
 SRC_NONE, SRC_RADIAL_SW, SRC_BATHYMETRY_SW = 0, 1, 2
 
 
@@ -39,6 +40,7 @@ class Params(ctypes.Structure):
         ("mthlim", ctypes.c_int * 4),
         ("b4step", ctypes.c_int), ("tperiod", ctypes.c_double),
         ("src_term", ctypes.c_int),
+        ("rho", ctypes.c_double), ("bulk", ctypes.c_double),
     ]
 
 
@@ -104,7 +106,7 @@ def _ptr(a):
 def make_params(*, ndim=1, mx, my=1, meqn, mwaves, mbc=3, maux=0, mcapa=0, char_decomp=0,
                 tfluct_solver=1, mthbc=(2, 2, 2, 2), dx, dy=1.0, xlower=0.0, ylower=0.0,
                 rp, efix=None, u=1.0, gamma=1.4, grav=1.0, lim_type=2, mthlim=(1, 1, 1, 1),
-                src_term=SRC_NONE) -> Params:
+                src_term=SRC_NONE, rho=1.0, bulk=1.0) -> Params:
     p = Params()
     p.ndim, p.mx, p.my = ndim, mx, (my if ndim == 2 else 1)
     p.meqn, p.mwaves, p.mbc, p.maux, p.mcapa = meqn, mwaves, mbc, maux, mcapa
@@ -119,6 +121,7 @@ def make_params(*, ndim=1, mx, my=1, meqn, mwaves, mbc=3, maux=0, mcapa=0, char_
     for k in range(4):
         p.mthlim[k] = int(mthlim[k]) if k < len(mthlim) else 1
     p.src_term = int(src_term)
+    p.rho, p.bulk = rho, bulk
     return p
 
 

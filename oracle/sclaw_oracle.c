@@ -1082,6 +1082,118 @@ static void evec_swf(const ocl_params *p, int mx, const double *q, double *evl, 
   }
 }
 
+/* apps/acoustics/1d/homogeneous: rp1.f:33-53 and tfluct.f (cell_internal:
+ * left ql(i), right qr(i), adq = amdq + apdq), cc = sqrt(bulk/rho), zz =
+ * cc*rho as setprob.f computes them. */
+static void rp_acconst(const ocl_params *p, int mx, const double *ql, const double *qr, double *wave,
+                       double *s, double *amdq, double *apdq, int cell_internal) {
+  const int mbc = p->mbc, meqn = 2;
+  const long ld = mx + 2 * mbc;
+  const double cc = sqrt(p->bulk / p->rho), zz = cc * p->rho;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    double d1, d2;
+    if (cell_internal) { d1 = L2(qr, i, 1) - L2(ql, i, 1); d2 = L2(qr, i, 2) - L2(ql, i, 2); }
+    else { d1 = L2(ql, i, 1) - L2(qr, i - 1, 1); d2 = L2(ql, i, 2) - L2(qr, i - 1, 2); }
+    double a1 = ((-d1) + zz * d2) / (2.0 * zz);
+    double a2 = (d1 + zz * d2) / (2.0 * zz);
+    L3(wave, i, 1, 1) = -(a1 * zz);
+    L3(wave, i, 2, 1) = a1;
+    L2(s, i, 1) = -cc;
+    L3(wave, i, 1, 2) = a2 * zz;
+    L3(wave, i, 2, 2) = a2;
+    L2(s, i, 2) = cc;
+  }
+  for (int m = 1; m <= 2; ++m)
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+      L2(amdq, i, m) = L2(s, i, 1) * L3(wave, i, m, 1);
+      L2(apdq, i, m) = L2(s, i, 2) * L3(wave, i, m, 2);
+    }
+}
+
+/* apps/acoustics/1d/homogeneous/evec.f */
+static void evec_acconst(const ocl_params *p, int mx, double *evl, double *evr) {
+  const int mbc = p->mbc, meqn = 2;
+  const long ld = mx + 2 * mbc;
+  const double cc = sqrt(p->bulk / p->rho), zz = cc * p->rho;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    L3(evr, i, 1, 1) = -zz;
+    L3(evr, i, 1, 2) = zz;
+    L3(evr, i, 2, 1) = 1.0;
+    L3(evr, i, 2, 2) = 1.0;
+    double z = 1.0 / (zz + zz);
+    L3(evl, i, 1, 1) = -z;
+    L3(evl, i, 1, 2) = zz * z;
+    L3(evl, i, 2, 1) = 1.0 * z;
+    L3(evl, i, 2, 2) = zz * z;
+  }
+}
+
+/* apps/acoustics/1d/fwave: rp1acfw.f:40-78 (linear stress sigma = bulk*eps,
+ * sigmap = bulk, :85-100) and tfluct1.f (cell_internal: both sides use
+ * aux(i), left ql(i), right qr(i)). */
+static void rp_acfwave(const ocl_params *p, int mx, const double *ql, const double *qr, const double *auxl,
+                       const double *auxr, double *wave, double *s, double *amdq, double *apdq,
+                       int cell_internal) {
+  const int mbc = p->mbc, meqn = 2;
+  const long ld = mx + 2 * mbc;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    double rhoi, rhoim, epsi, epsim, urhoi, urhoim, ki, kim;
+    if (cell_internal) {
+      rhoi = L2(auxr, i, 1); rhoim = L2(auxl, i, 1);
+      epsi = L2(qr, i, 1); epsim = L2(ql, i, 1);
+      urhoi = L2(qr, i, 2); urhoim = L2(ql, i, 2);
+      ki = L2(auxr, i, 2); kim = L2(auxl, i, 2);
+    } else {
+      rhoi = L2(auxl, i, 1); rhoim = L2(auxr, i - 1, 1);
+      epsi = L2(ql, i, 1); epsim = L2(qr, i - 1, 1);
+      urhoi = L2(ql, i, 2); urhoim = L2(qr, i - 1, 2);
+      ki = L2(auxl, i, 2); kim = L2(auxr, i - 1, 2);
+    }
+    double ci = sqrt(ki / rhoi);
+    double cim = sqrt(kim / rhoim);
+    double zi = ci * rhoi;
+    double zim = cim * rhoim;
+    double du = urhoi / rhoi - urhoim / rhoim;
+    double dsig = ki * epsi - kim * epsim;
+    double b1 = -((zi * du + dsig) / (zim + zi));
+    double b2 = -((zim * du - dsig) / (zim + zi));
+    L3(wave, i, 1, 1) = b1;
+    L3(wave, i, 2, 1) = b1 * zim;
+    L2(s, i, 1) = -cim;
+    L3(wave, i, 1, 2) = b2;
+    L3(wave, i, 2, 2) = b2 * (-zi);
+    L2(s, i, 2) = ci;
+  }
+  for (int m = 1; m <= 2; ++m)
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+      L2(amdq, i, m) = L3(wave, i, m, 1);
+      L2(apdq, i, m) = L3(wave, i, m, 2);
+    }
+}
+
+/* apps/acoustics/1d/fwave/evec.f:40-63 (as the app writes it: evl holds the
+ * rows (1, 1) and (zim, -zi), evr their inverse) */
+static void evec_acfwave(const ocl_params *p, int mx, const double *auxl, const double *auxr, double *evl,
+                         double *evr) {
+  const int mbc = p->mbc, meqn = 2;
+  const long ld = mx + 2 * mbc;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    double ci = sqrt(L2(auxl, i, 2) / L2(auxl, i, 1));
+    double cim = sqrt(L2(auxr, i - 1, 2) / L2(auxr, i - 1, 1));
+    double zi = ci * L2(auxl, i, 1);
+    double zim = cim * L2(auxr, i - 1, 1);
+    L3(evl, i, 1, 1) = 1.0;
+    L3(evl, i, 1, 2) = 1.0;
+    L3(evl, i, 2, 1) = zim;
+    L3(evl, i, 2, 2) = -zi;
+    double zh = 1.0 / (zim + zi);
+    L3(evr, i, 1, 1) = zi * zh;
+    L3(evr, i, 1, 2) = zh;
+    L3(evr, i, 2, 1) = zim * zh;
+    L3(evr, i, 2, 2) = -zh;
+  }
+}
+
 /* apps/acoustics/1d/interface/rp1acv.f:49-80; with ixy it is also the new 2-D
  * normal solver (mu = normal velocity, tangential components carry 0). */
 static void rp_acoustics(const ocl_params *p, int ixy, int mx, const double *ql, const double *qr,
@@ -1188,6 +1300,8 @@ int ocl_rp(const ocl_params *p, int ixy, int mx, const double *ql, const double 
     case OCL_RP_SWF_BATHY:
     case OCL_RP_SWF_RADIAL:
     case OCL_RP_SWF_KAPPA: rp_swf(p, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq, 0); return 0;
+    case OCL_RP_ACOUSTICS_CONST: rp_acconst(p, mx, ql, qr, wave, s, amdq, apdq, 0); return 0;
+    case OCL_RP_ACOUSTICS_FWAVE: rp_acfwave(p, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq, 0); return 0;
     case OCL_RP_ACOUSTICS1D:
     case OCL_RP_ACOUSTICS2D:
       rp_acoustics(p, ixy, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq); return 0;
@@ -1234,6 +1348,18 @@ int ocl_tfluct(const ocl_params *p, int ixy, int mx, const double *ql, const dou
       free(wave); free(am); free(ap);
       return 0;
     }
+    case OCL_RP_ACOUSTICS_CONST:
+    case OCL_RP_ACOUSTICS_FWAVE: {
+      const long ld = mx + 2L * p->mbc;
+      double *wave = (double *)calloc((size_t)ld * 4, sizeof(double));
+      double *am = (double *)calloc((size_t)ld * 2, sizeof(double));
+      double *ap = (double *)calloc((size_t)ld * 2, sizeof(double));
+      if (p->rp == OCL_RP_ACOUSTICS_CONST) rp_acconst(p, mx, ql, qr, wave, s, am, ap, 1);
+      else rp_acfwave(p, mx, ql, qr, auxl, auxr, wave, s, am, ap, 1);
+      for (long k = 0; k < ld * 2; ++k) adq[k] = am[k] + ap[k];
+      free(wave); free(am); free(ap);
+      return 0;
+    }
     case OCL_RP_ACOUSTICS1D:
     case OCL_RP_ACOUSTICS2D:
       tfluct_acoustics(p, ixy, mx, ql, qr, auxl, s, adq); return 0;
@@ -1253,6 +1379,8 @@ int ocl_evec(const ocl_params *p, int ixy, int mx, const double *q, const double
     case OCL_RP_SWF_BATHY:
     case OCL_RP_SWF_RADIAL:
     case OCL_RP_SWF_KAPPA: evec_swf(p, mx, q, evl, evr); return 0;
+    case OCL_RP_ACOUSTICS_CONST: evec_acconst(p, mx, evl, evr); return 0;
+    case OCL_RP_ACOUSTICS_FWAVE: evec_acfwave(p, mx, auxl, auxr, evl, evr); return 0;
     case OCL_RP_ACOUSTICS1D:
     case OCL_RP_ACOUSTICS2D: evec_acoustics(p, ixy, mx, auxl, evl, evr); return 0;
   }

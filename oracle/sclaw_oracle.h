@@ -39,8 +39,12 @@ enum {
   OCL_RP_SWF_BATHY = 8,     /* apps/shallowWater/1dPerturbSteady/{rpf-wave.f90,
                                tfluctf-wave.f90}: f-waves, bathymetry b = aux(:,1)     */
   OCL_RP_SWF_RADIAL = 9,    /* 2dRadialDam/1dRadialSymm-fwave: aux = (r, dx)            */
-  OCL_RP_SWF_KAPPA = 10     /* 2dRadialDam/1dRadialSymm-fwave-kappa: aux = (r(i-1/2),
+  OCL_RP_SWF_KAPPA = 10,    /* 2dRadialDam/1dRadialSymm-fwave-kappa: aux = (r(i-1/2),
                                r(i), r(i), dx), capacity aux(:,2)                      */
+  OCL_RP_ACOUSTICS_CONST = 11,  /* apps/acoustics/1d/homogeneous/{rp1.f,tfluct.f,evec.f},
+                                   common /cparam/ rho, bulk                           */
+  OCL_RP_ACOUSTICS_FWAVE = 12   /* apps/acoustics/1d/fwave/{rp1acfw.f,tfluct1.f,evec.f}:
+                                   q = (strain, momentum), aux = (rho, bulk)           */
 };
 
 /* Source-term hooks: the src(q,dq,aux,t,dt) an app links (src/1d/step1d.f90:23). */
@@ -69,6 +73,7 @@ typedef struct {
   int b4step;           /* 0 src/b4step.f90 (no-op), 1 apps/advection/2d/swirl        */
   double tperiod;       /* swirl: common /comvt/ tperiod                              */
   int src_term;         /* OCL_SRC_* (1-D)                                            */
+  double rho, bulk;     /* homogeneous acoustics: common /cparam/ rho, bulk           */
 } ocl_params;
 
 typedef struct {

@@ -29,12 +29,14 @@ import numpy as np
 
 from . import _capi as C
 from ._capi import (B4STEP_NONE, B4STEP_SWIRL, FP32, FP64, FP64_STRICT, MIXED,  # noqa: F401
+                    RP_ACOUSTICS_CONST, RP_ACOUSTICS_FWAVE,
                     RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION, RP_ADVECTION2D, RP_EULER, RP_SW1D, RP_SW2D,
                     RP_SWF_BATHY, RP_SWF_KAPPA, RP_SWF_RADIAL, SRC_BATHYMETRY_SW, SRC_NONE, SRC_RADIAL_SW,
                     RUN_AUTO, RUN_GRAPH, RUN_RESIDENT, SharpClawError)
 
 __all__ = ["ClawParams", "Solver", "Batch", "sharpclaw", "SharpClawError", "RP_ADVECTION", "RP_EULER",
            "RP_SW2D", "RP_ACOUSTICS1D", "RP_ACOUSTICS2D", "RP_ADVECTION2D", "RP_SW1D", "RP_SWF_BATHY", "RP_SWF_RADIAL", "RP_SWF_KAPPA",
+           "RP_ACOUSTICS_CONST", "RP_ACOUSTICS_FWAVE",
            "SRC_NONE", "SRC_RADIAL_SW",
            "SRC_BATHYMETRY_SW", "B4STEP_NONE", "B4STEP_SWIRL",
            "RUN_AUTO", "RUN_GRAPH", "RUN_RESIDENT"]
@@ -51,6 +53,8 @@ PLUGINS = {
     RP_SWF_BATHY: (2, 2, 1, 1),
     RP_SWF_RADIAL: (2, 2, 2, 1),
     RP_SWF_KAPPA: (2, 2, 4, 1),
+    RP_ACOUSTICS_CONST: (2, 2, 0, 1),
+    RP_ACOUSTICS_FWAVE: (2, 2, 2, 1),
 }
 
 
@@ -82,6 +86,8 @@ class ClawParams:
     time_integrator: int = 3
     mthlim: Sequence[int] = field(default_factory=lambda: (1, 1, 1, 1))
     src_term: int = 0
+    rho: float = 1.0      # homogeneous acoustics (common /cparam/)
+    bulk: float = 1.0
 
     def __post_init__(self):
         meqn, mwaves, maux, ndim = PLUGINS.get(self.rp, (None, None, 0, None))
@@ -119,6 +125,7 @@ class ClawParams:
         for k in range(4):
             p.mthlim[k] = int(self.mthlim[k]) if k < len(self.mthlim) else 1
         p.src_term = int(self.src_term)
+        p.rho, p.bulk = float(self.rho), float(self.bulk)
         return p
 
 

@@ -16,6 +16,7 @@ SCL_OK, SCL_E_INVALID, SCL_E_CUDA, SCL_E_UNSUPPORTED, SCL_E_NONFINITE, SCL_E_TIM
 RP_ADVECTION, RP_EULER, RP_SW2D, RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION2D, RP_SW1D = 1, 2, 3, 4, 5, 6, 7
 SRC_NONE, SRC_RADIAL_SW, SRC_BATHYMETRY_SW = 0, 1, 2
 RP_SWF_BATHY, RP_SWF_RADIAL, RP_SWF_KAPPA = 8, 9, 10
+RP_ACOUSTICS_CONST, RP_ACOUSTICS_FWAVE = 11, 12
 B4STEP_NONE, B4STEP_SWIRL = 0, 1
 RUN_AUTO, RUN_GRAPH, RUN_RESIDENT = 0, 1, 2
 FP64, FP64_STRICT, MIXED, FP32 = 0, 1, 2, 3
@@ -39,6 +40,7 @@ class scl_params(ctypes.Structure):
         ("time_integrator", ctypes.c_int), ("precision", ctypes.c_int),
         ("mthlim", ctypes.c_int * 4),
         ("src_term", ctypes.c_int),
+        ("rho", ctypes.c_double), ("bulk", ctypes.c_double),
     ]
 
 

@@ -241,6 +241,7 @@ StageArgs make_args(const scl_handle* h, int s) {
   a.ph.grav = h->p.grav;
   a.ph.efix = h->p.efix;
   for (int k = 0; k < 4; ++k) a.ph.mthlim[k] = h->p.mthlim[k];
+  set_acoustics_consts(h->p, &a.ph);
   return a;
 }
 
@@ -442,7 +443,10 @@ int validate(const scl_params* p) {
       {SCL_RP_ADVECTION, 1, 1, 0, 1}, {SCL_RP_EULER, 3, 3, 0, 1}, {SCL_RP_SW2D, 3, 3, 0, 2},
       {SCL_RP_ACOUSTICS1D, 2, 2, 2, 1}, {SCL_RP_ACOUSTICS2D, 3, 2, 2, 2},
       {SCL_RP_ADVECTION2D, 1, 1, 2, 2}, {SCL_RP_SW1D, 2, 2, 0, 1}, {SCL_RP_SWF_BATHY, 2, 2, 1, 1},
-      {SCL_RP_SWF_RADIAL, 2, 2, 2, 1}, {SCL_RP_SWF_KAPPA, 2, 2, 4, 1}};
+      {SCL_RP_SWF_RADIAL, 2, 2, 2, 1}, {SCL_RP_SWF_KAPPA, 2, 2, 4, 1}, {SCL_RP_ACOUSTICS_CONST, 2, 2, 0, 1},
+      {SCL_RP_ACOUSTICS_FWAVE, 2, 2, 2, 1}};
+  if (p->rp == SCL_RP_ACOUSTICS_CONST && !(p->rho > 0 && p->bulk > 0))
+    return fail(SCL_E_INVALID, "homogeneous acoustics needs rho > 0 and bulk > 0 (setprob.f)");
   if (p->src_term != SCL_SRC_NONE) {
     if (p->src_term != SCL_SRC_RADIAL_SW && p->src_term != SCL_SRC_BATHYMETRY_SW)
       return fail(SCL_E_INVALID, "src_term must be SCL_SRC_NONE, SCL_SRC_RADIAL_SW or SCL_SRC_BATHYMETRY_SW");
@@ -701,6 +705,7 @@ int scl_flux1(scl_handle* h, const double* q1d, const double* aux1d, double* dq1
     a.ph.u = p1.u; a.ph.gamma = p1.gamma; a.ph.gamma1 = p1.gamma - 1.0; a.ph.grav = p1.grav;
     a.ph.efix = p1.efix;
     for (int k = 0; k < 4; ++k) a.ph.mthlim[k] = p1.mthlim[k];
+    set_acoustics_consts(p1, &a.ph);
     L1.stage(a, h->stream);
     if (cudaGetLastError() != cudaSuccess) rc = fail(SCL_E_CUDA, "flux1 launch");
   }

@@ -6,6 +6,7 @@
 // mapped to offset 0.  Rows are padded to `pitch` elements (a multiple of 32)
 // so every row start is 256-byte aligned; a 2-D plane holds (my+2*mbc) rows.
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -70,7 +71,19 @@ struct Phys {
   double grav;    // gravity                apps/shallowWater/2dRadialDam/setprob.f90
   int efix;
   int mthlim[4];  // TVD limiters (ClawParams%mthlim)
+  double cc, zz;  // homogeneous acoustics: sqrt(bulk/rho), cc*rho (apps/acoustics/1d/homogeneous/setprob.f)
 };
+
+// Host side: the constants setprob.f of apps/acoustics/1d/homogeneous derives
+// from rho and bulk (cc = sqrt(bulk/rho), zz = cc*rho).
+inline void set_acoustics_consts(const scl_params& p, Phys* ph) {
+  ph->cc = 0.0;
+  ph->zz = 0.0;
+  if (p.rp == SCL_RP_ACOUSTICS_CONST && p.rho > 0 && p.bulk > 0) {
+    ph->cc = std::sqrt(p.bulk / p.rho);
+    ph->zz = ph->cc * p.rho;
+  }
+}
 
 // Arguments of one stage launch (all by value; pointers are device pointers).
 struct StageArgs {

@@ -756,6 +756,145 @@ struct PShallowF1D {
   }
 };
 
+// ------------------------------------------------------------------------
+// Constant-coefficient acoustics, apps/acoustics/1d/homogeneous (rp1.f:33-53,
+// tfluct.f, evec.f): cc = sqrt(bulk/rho), zz = cc*rho (setprob.f), passed in
+// Phys as cc, zz.
+// ------------------------------------------------------------------------
+struct PAcousticsConst {
+  static constexpr int MEQN = 2, MWAVES = 2, MAUX = 0, NDIM = 1;
+  static constexpr bool HAS_TFLUCT = true;
+
+  template <class R, bool FD = false>
+  __device__ static void waves(const Phys& ph, int, const R*, const R*, const R* dl, const R*, const R*,
+                               R w[2][2], R* s = nullptr) {
+    const R zz = (R)ph.zz, cc = (R)ph.cc;
+    R a1, a2;
+    if constexpr (sizeof(R) == 4 || FD) {
+      const R i2z = (R)1 / ((R)2 * zz);
+      a1 = ((-dl[0]) + zz * dl[1]) * i2z;
+      a2 = (dl[0] + zz * dl[1]) * i2z;
+    } else {
+      a1 = ((-dl[0]) + zz * dl[1]) / ((R)2 * zz);
+      a2 = (dl[0] + zz * dl[1]) / ((R)2 * zz);
+    }
+    w[0][0] = -(a1 * zz); w[0][1] = a1;
+    w[1][0] = a2 * zz;    w[1][1] = a2;
+    if (s) { s[0] = -cc; s[1] = cc; }
+  }
+  template <class R, bool FD = false>
+  __device__ static void rp(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl, const R* am,
+                            const R* a0, R* s, R* amdq, R* apdq) {
+    R w[2][2];
+    waves<R, FD>(ph, ixy, L, Rt, dl, am, a0, w, s);
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      amdq[m] = s[0] * w[0][m];
+      apdq[m] = s[1] * w[1][m];
+    }
+  }
+  template <class R, bool FD = false>
+  __device__ static void tfluct(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl, const R* aux,
+                                R* adq) {
+    R w[2][2], s[2];
+    waves<R, FD>(ph, ixy, L, Rt, dl, aux, aux, w, s);
+#pragma unroll
+    for (int m = 0; m < 2; ++m) adq[m] = s[0] * w[0][m] + s[1] * w[1][m];
+  }
+  template <class R, bool FD = false>
+  __device__ static void evec(const Phys& ph, int, const R*, const R*, const R*, const R*, R evl[2][2],
+                              R evr[2][2]) {
+    const R zz = (R)ph.zz;
+    evr[0][0] = -zz;   evr[0][1] = zz;
+    evr[1][0] = (R)1;  evr[1][1] = (R)1;
+    const R z = (R)1 / (zz + zz);
+    evl[0][0] = -z;        evl[0][1] = zz * z;
+    evl[1][0] = (R)1 * z;  evl[1][1] = zz * z;
+  }
+};
+
+// ------------------------------------------------------------------------
+// Acoustics in strain / momentum form with f-waves, apps/acoustics/1d/fwave
+// (rp1acfw.f:40-78 with the linear sigma = bulk*eps of :85-100, tfluct1.f,
+// evec.f): q = (eps, rho u), aux = (rho, bulk).  The app's evec puts the
+// rows (1, 1) and (zim, -zi) in evl and their inverse in evr; kept as written.
+// ------------------------------------------------------------------------
+struct PAcousticsFwave {
+  static constexpr int MEQN = 2, MWAVES = 2, MAUX = 2, NDIM = 1;
+  static constexpr bool HAS_TFLUCT = true;
+
+  // f-waves between the left state L (material am) and the right state Rt
+  // (material a0)
+  template <class R, bool FD = false>
+  __device__ static void fwaves(const R* L, const R* Rt, const R* am, const R* a0, R w[2][2], R* s) {
+    const R rhoi = a0[0], rhoim = am[0], ki = a0[1], kim = am[1];
+    R ci, cim, du, inv;
+    if constexpr (sizeof(R) == 4 || FD) {
+      const R iri = (R)1 / rhoi, irim = (R)1 / rhoim;
+      ci = sqrt(ki * iri);
+      cim = sqrt(kim * irim);
+      du = Rt[1] * iri - L[1] * irim;
+    } else {
+      ci = sqrt(ki / rhoi);
+      cim = sqrt(kim / rhoim);
+      du = Rt[1] / rhoi - L[1] / rhoim;
+    }
+    const R zi = ci * rhoi, zim = cim * rhoim;
+    const R dsig = ki * Rt[0] - kim * L[0];
+    R b1, b2;
+    if constexpr (sizeof(R) == 4 || FD) {
+      inv = (R)1 / (zim + zi);
+      b1 = -((zi * du + dsig) * inv);
+      b2 = -((zim * du - dsig) * inv);
+    } else {
+      b1 = -((zi * du + dsig) / (zim + zi));
+      b2 = -((zim * du - dsig) / (zim + zi));
+    }
+    w[0][0] = b1; w[0][1] = b1 * zim;    s[0] = -cim;
+    w[1][0] = b2; w[1][1] = b2 * (-zi);  s[1] = ci;
+  }
+  template <class R, bool FD = false>
+  __device__ static void waves(const Phys&, int, const R* L, const R* Rt, const R*, const R* am,
+                               const R* a0, R w[2][2], R* s = nullptr) {
+    R sp[2];
+    fwaves<R, FD>(L, Rt, am, a0, w, sp);
+    if (s) { s[0] = sp[0]; s[1] = sp[1]; }
+  }
+  template <class R, bool FD = false>
+  __device__ static void rp(const Phys&, int, const R* L, const R* Rt, const R*, const R* am, const R* a0,
+                            R* s, R* amdq, R* apdq) {
+    R w[2][2];
+    fwaves<R, FD>(L, Rt, am, a0, w, s);
+#pragma unroll
+    for (int m = 0; m < 2; ++m) { amdq[m] = w[0][m]; apdq[m] = w[1][m]; }
+  }
+  template <class R, bool FD = false>
+  __device__ static void tfluct(const Phys&, int, const R* L, const R* Rt, const R*, const R* aux, R* adq) {
+    R w[2][2], s[2];
+    fwaves<R, FD>(L, Rt, aux, aux, w, s);
+#pragma unroll
+    for (int m = 0; m < 2; ++m) adq[m] = w[0][m] + w[1][m];
+  }
+  template <class R, bool FD = false>
+  __device__ static void evec(const Phys&, int, const R*, const R*, const R* am, const R* a0, R evl[2][2],
+                              R evr[2][2]) {
+    R ci, cim;
+    if constexpr (sizeof(R) == 4 || FD) {
+      ci = sqrt(a0[1] * ((R)1 / a0[0]));
+      cim = sqrt(am[1] * ((R)1 / am[0]));
+    } else {
+      ci = sqrt(a0[1] / a0[0]);
+      cim = sqrt(am[1] / am[0]);
+    }
+    const R zi = ci * a0[0], zim = cim * am[0];
+    evl[0][0] = (R)1; evl[0][1] = (R)1;
+    evl[1][0] = zim;  evl[1][1] = -zi;
+    const R zh = (R)1 / (zim + zi);
+    evr[0][0] = zi * zh;  evr[0][1] = zh;
+    evr[1][0] = zim * zh; evr[1][1] = -zh;
+  }
+};
+
 // Plugins whose total fluctuation reads the aux of cells c-1, c, c+1 (three
 // MAUX groups, centre in the middle) declare TFLUCT_NB = true.
 template <class P, class = void>

@@ -248,3 +248,38 @@ def fwave_radial(mx=200, kappa=False, char_decomp=0, tfluct_solver=1):
     po = O.make_params(meqn=2, mwaves=2, rp=rp_o, **kw)
     ps = S.ClawParams(rp=rp_s, **kw)
     return po, ps, q, aux
+
+
+def acoustics_const(mx=200, rho=1.0, bulk=4.0, mthbc=(3, 3), char_decomp=0, tfluct_solver=0, smooth=False):
+    """apps/acoustics/1d/homogeneous (setrun.py: [-1, 1], walls, rho 1, bulk
+    4): p0 = exp(-50 (x-0.3)^2) cos(20 (x-0.3)) for x <= 0.3 (qinit.f), u0 = 0;
+    smooth: the Gaussian alone, for the exact-solution check."""
+    dx = 2.0 / mx
+    xc = -1.0 + (np.arange(mx) + 0.5) * dx
+    p0 = np.exp(-50.0 * (xc - 0.3) ** 2)
+    if not smooth:
+        p0 = np.where(xc > 0.3, 0.0, p0 * np.cos(20.0 * (xc - 0.3)))
+    q = np.zeros((2, mx + 6))
+    q[0, 3:-3] = p0
+    kw = dict(mx=mx, dx=dx, xlower=-1.0, mthbc=mthbc, char_decomp=char_decomp, tfluct_solver=tfluct_solver,
+              rho=rho, bulk=bulk)
+    po = O.make_params(meqn=2, mwaves=2, rp=O.RP_ACOUSTICS_CONST, **kw)
+    ps = S.ClawParams(rp=S.RP_ACOUSTICS_CONST, **kw)
+    return po, ps, q, None
+
+
+def acoustics_fwave(mx=200, char_decomp=2, tfluct_solver=1, mthbc=(1, 1)):
+    """apps/acoustics/1d/fwave: the interface problem of acoustics1d in strain
+    / momentum form, q = (eps, rho u) with eps = -p/bulk, aux = (rho, bulk)."""
+    from acoustics_exact import InterfaceProblem
+    ap = InterfaceProblem()
+    dx = 20.0 / mx
+    za = ap.setaux(mx)                      # (Z, c)
+    rho, bulk = za[0] / za[1], za[0] * za[1]
+    aux = np.ascontiguousarray(np.stack([rho, bulk]))
+    qp = ap.qinit(mx, za)                   # (p, u)
+    q = np.stack([-qp[0] / bulk, rho * qp[1]])
+    kw = dict(mx=mx, dx=dx, xlower=-10.0, mthbc=mthbc, char_decomp=char_decomp, tfluct_solver=tfluct_solver)
+    po = O.make_params(meqn=2, mwaves=2, maux=2, rp=O.RP_ACOUSTICS_FWAVE, **kw)
+    ps = S.ClawParams(rp=S.RP_ACOUSTICS_FWAVE, **kw)
+    return po, ps, q, aux

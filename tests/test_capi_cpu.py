@@ -46,6 +46,7 @@ def test_version_string():
     (dict(src_term=1), C.SCL_E_UNSUPPORTED),                                    # SW1D hooks only
     (dict(src_term=5), C.SCL_E_INVALID),
     (dict(rp=S.RP_SW1D, meqn=None, mwaves=None, char_decomp=0, src_term=2), C.SCL_E_INVALID),  # maux 0
+    (dict(rp=S.RP_ACOUSTICS_CONST, meqn=None, mwaves=None, char_decomp=0, rho=0.0), C.SCL_E_INVALID),
     (dict(lim_type=1, char_decomp=3), C.SCL_E_UNSUPPORTED),
     (dict(lim_type=1, mthlim=(1, 6, 1, 1)), C.SCL_E_INVALID),
     (dict(char_decomp=4), C.SCL_E_UNSUPPORTED),

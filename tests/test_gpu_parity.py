@@ -90,6 +90,15 @@ STEP_CASES = [
     ("swf_kappa_tf1", lambda: cases.fwave_radial(mx=120, kappa=True)),
     ("swf_kappa_char", lambda: cases.fwave_radial(mx=90, kappa=True, char_decomp=2)),
     ("swf_kappa_tvd2_tf0", lambda: cases.with_tvd(cases.fwave_radial(mx=100, kappa=True, tfluct_solver=0), (4, 2, 1, 1), 0)),
+    # apps/acoustics/1d/homogeneous and apps/acoustics/1d/fwave
+    ("acconst_wall_tf0", lambda: cases.acoustics_const(mx=150)),
+    ("acconst_char_tf1", lambda: cases.acoustics_const(mx=120, char_decomp=2, tfluct_solver=1)),
+    ("acconst_wave", lambda: cases.acoustics_const(mx=100, char_decomp=1, mthbc=(2, 2))),
+    ("acconst_trans", lambda: cases.acoustics_const(mx=110, char_decomp=3, mthbc=(1, 1))),
+    ("acfwave_char_tf1", lambda: cases.acoustics_fwave(mx=160)),
+    ("acfwave_comp_tf0", lambda: cases.acoustics_fwave(mx=140, char_decomp=0, tfluct_solver=0)),
+    ("acfwave_wave", lambda: cases.acoustics_fwave(mx=120, char_decomp=1)),
+    ("acfwave_tvd2_wave", lambda: cases.with_tvd(cases.acoustics_fwave(mx=100), (3, 4, 1, 1), 1)),
 ]
 
 
@@ -179,6 +188,8 @@ RUN_CASES = [
     ("swf_bathy_ssp104", lambda: cases.fwave_bathymetry(mx=200), 4, dict(tend=0.05, dt_initial=0.0005, cfl_max=0.5, cfl_desired=0.2)),
     ("swf_radial_ssp104", lambda: cases.fwave_radial(mx=200), 4, dict(tend=0.2, dt_initial=0.002, cfl_max=0.3, cfl_desired=0.2)),
     ("swf_kappa_ssp104", lambda: cases.fwave_radial(mx=100, kappa=True), 4, dict(tend=0.1, dt_initial=0.001, cfl_max=0.3, cfl_desired=0.2)),
+    ("acconst_ssp104", lambda: cases.acoustics_const(mx=200), 4, dict(tend=0.5, dt_initial=0.001, cfl_max=0.25, cfl_desired=0.25)),
+    ("acfwave_ssp104", lambda: cases.acoustics_fwave(mx=200), 4, dict(tend=2.0, dt_initial=0.025, cfl_max=2.5, cfl_desired=2.45)),
 ]
 
 

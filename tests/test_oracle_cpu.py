@@ -241,3 +241,64 @@ def test_fwave_flat_bottom_equals_roe():
     assert np.abs(sf[:, 1:] - sq[:, 1:]).max() <= 1e-14 * np.abs(sq).max()
     assert np.abs(amf[:, 1:] - amq[:, 1:]).max() <= 1e-13 * scale
     assert np.abs(apf[:, 1:] - apq[:, 1:]).max() <= 1e-13 * scale
+
+
+def test_acoustics_fwave_interface_known_answer():
+    """apps/acoustics/1d/fwave solves the interface problem of sharpclawtest.py
+    in strain / momentum form (WENO5 char-wise, SSPRK(10,4), t = 8): the
+    pressure -bulk*eps and velocity (rho u)/rho meet the same exact solution
+    as the interface app, with the same error bounds."""
+    from acoustics_exact import InterfaceProblem
+    ap = InterfaceProblem()
+    errs = []
+    for mx in (400, 800):
+        po, _, q, aux = cases.acoustics_fwave(mx=mx)
+        qf, r = O.sharpclaw(po, q, aux, tstart=0.0, tend=8.0, dt_initial=0.025, cfl_max=2.5,
+                            cfl_desired=2.45, time_integrator=4)
+        assert r.info == 0 and r.tend == 8.0
+        pe, ue = ap.cell_averages(mx, r.tend)
+        dx = 20.0 / mx
+        errs.append((np.abs(pe + aux[1, 3:-3] * qf[0, 3:-3]).sum() * dx,
+                     np.abs(ue - qf[1, 3:-3] / aux[0, 3:-3]).sum() * dx))
+    assert errs[0][0] < 0.06 and errs[1][0] < 0.013, errs
+    assert np.log2(errs[0][0] / errs[1][0]) > 2.0 and np.log2(errs[0][1] / errs[1][1]) > 2.0
+
+
+def test_acoustics_homogeneous_dalembert():
+    """apps/acoustics/1d/homogeneous on a periodic domain: the Gaussian pulse
+    splits into two waves moving at +-c (d'Alembert); cell averages of the
+    exact solution at t = 0.5, errors falling with mx."""
+    errs = []
+    for mx in (100, 200):
+        po, _, q, aux = cases.acoustics_const(mx=mx, mthbc=(2, 2), smooth=True)
+        T = 0.5
+        qf, r = O.sharpclaw(po, q, aux, tstart=0.0, tend=T, dt_initial=0.001, cfl_max=2.5, cfl_desired=2.4,
+                            time_integrator=4)
+        assert r.info == 0
+        c = np.sqrt(po.bulk / po.rho)
+        z = c * po.rho
+        dx = 2.0 / mx
+        xe = -1.0 + dx * np.arange(mx + 1)
+        g, w = np.polynomial.legendre.leggauss(10)
+        pts = 0.5 * (xe[:-1, None] + xe[1:, None]) + 0.5 * dx * g[None, :]
+
+        def p0(x):
+            y = (x + 1.0) % 2.0 - 1.0
+            return np.exp(-50.0 * (y - 0.3) ** 2)
+        pe = (0.5 * (p0(pts - c * T) + p0(pts + c * T)) * w).sum(1) * 0.5
+        ue = ((p0(pts - c * T) - p0(pts + c * T)) / (2 * z) * w).sum(1) * 0.5
+        errs.append((np.abs(pe - qf[0, 3:-3]).sum() * dx, np.abs(ue - qf[1, 3:-3]).sum() * dx))
+    assert errs[1][0] < 2e-4 and errs[1][1] < 5e-5, errs
+    assert np.log2(errs[0][0] / errs[1][0]) > 3.0, errs
+
+
+def test_acoustics_app_eigenvectors_are_inverse_pairs():
+    rng = np.random.default_rng(9)
+    n = 16
+    q = rng.uniform(-1, 1, (2, n))
+    aux = np.stack([rng.uniform(0.5, 2, n), rng.uniform(0.5, 4, n)])
+    for rp, kw in ((O.RP_ACOUSTICS_CONST, dict(rho=1.3, bulk=3.1)), (O.RP_ACOUSTICS_FWAVE, dict(maux=2))):
+        p = O.make_params(mx=n - 6, meqn=2, mwaves=2, dx=0.1, rp=rp, mthbc=(1, 1), char_decomp=2, **kw)
+        evl, evr = O.evec(p, q, aux if rp == O.RP_ACOUSTICS_FWAVE else None)
+        for i in range(1, n):
+            assert np.allclose(evl[:, :, i].T @ evr[:, :, i].T, np.eye(2), atol=1e-12)
