@@ -63,6 +63,10 @@ extern "C" {
                                       constant rho, bulk (scl_params.rho, .bulk)          */
 #define SCL_RP_ACOUSTICS_FWAVE 12  /* apps/acoustics/1d/fwave/{rp1acfw.f,tfluct1.f,evec.f}:
                                       q = (strain, momentum), aux = (rho, bulk)          */
+#define SCL_RP_TRAFFIC 13          /* apps/traffic/congTraffic/{rpf-wave.f90,tfluct1.f90}:
+                                      flux umax(x) q (1-q), aux = umax                   */
+#define SCL_RP_ADVECTION_CONS 14   /* apps/traffic/flux-uq/rpf-wave.f90: (u(x) q)_x with
+                                      cell velocities aux = u; no tfluct                 */
 
 /* ---- source terms: the src(q,dq,aux,t,dt) an app links (src/1d/step1d.f90:23),
  * evaluated in the stage kernel before the fluctuations are subtracted;

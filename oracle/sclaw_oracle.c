@@ -1194,6 +1194,64 @@ static void evec_acfwave(const ocl_params *p, int mx, const double *auxl, const 
   }
 }
 
+/* apps/traffic/congTraffic/rpf-wave.f90:30-72: f-wave for the flux
+ * umax(x) q (1-q) with the entropy-satisfying split of its four sign cases;
+ * tfluct1.f90:27-33: the cell's flux difference (both sides aux(i)). */
+static void rp_traffic(const ocl_params *p, int mx, const double *ql, const double *qr, const double *auxl,
+                       const double *auxr, double *wave, double *s, double *amdq, double *apdq) {
+  const int mbc = p->mbc, meqn = 1;
+  const long ld = mx + 2 * mbc;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    double fim1 = (L2(auxr, i - 1, 1) * L2(qr, i - 1, 1)) * (1.0 - L2(qr, i - 1, 1));
+    double fi = (L2(auxl, i, 1) * L2(ql, i, 1)) * (1.0 - L2(ql, i, 1));
+    L3(wave, i, 1, 1) = fi - fim1;
+    double sim1 = L2(auxr, i - 1, 1) * (1.0 - 2.0 * L2(qr, i - 1, 1));
+    double si = L2(auxl, i, 1) * (1.0 - 2.0 * L2(ql, i, 1));
+    if (sim1 < 0.0 && si <= 0.0) {
+      L2(s, i, 1) = sim1; L2(amdq, i, 1) = L3(wave, i, 1, 1); L2(apdq, i, 1) = 0.0;
+    } else if (sim1 >= 0.0 && si > 0.0) {
+      L2(s, i, 1) = si; L2(amdq, i, 1) = 0.0; L2(apdq, i, 1) = L3(wave, i, 1, 1);
+    } else if (sim1 < 0.0 && si > 0.0) {                      /* transonic rarefaction */
+      L2(s, i, 1) = 0.5 * (sim1 + si);
+      double f0 = dmin1(L2(auxr, i - 1, 1), L2(auxl, i, 1)) * 0.25;
+      L2(amdq, i, 1) = f0 - fim1;
+      L2(apdq, i, 1) = fi - f0;
+    } else {
+      L2(s, i, 1) = 0.5 * (sim1 + si);
+      if (L2(s, i, 1) < 0.0) { L2(amdq, i, 1) = L3(wave, i, 1, 1); L2(apdq, i, 1) = 0.0; }
+      else if (L2(s, i, 1) > 0.0) { L2(amdq, i, 1) = 0.0; L2(apdq, i, 1) = L3(wave, i, 1, 1); }
+      else { L2(amdq, i, 1) = 0.5 * L3(wave, i, 1, 1); L2(apdq, i, 1) = 0.5 * L3(wave, i, 1, 1); }
+    }
+  }
+}
+
+static void tfluct_traffic(const ocl_params *p, int mx, const double *ql, const double *qr, const double *auxl,
+                           const double *auxr, double *adq) {
+  const int mbc = p->mbc;
+  const long ld = mx + 2 * mbc;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    double fim1 = (L2(auxl, i, 1) * L2(ql, i, 1)) * (1.0 - L2(ql, i, 1));
+    double fi = (L2(auxr, i, 1) * L2(qr, i, 1)) * (1.0 - L2(qr, i, 1));
+    L2(adq, i, 1) = fi - fim1;
+  }
+}
+
+/* apps/traffic/flux-uq/rpf-wave.f90:34-52: conservative advection with cell
+ * velocities, f-wave u(i) q(i) - u(i-1) q(i-1) to the side of u(i)'s sign. */
+static void rp_advcons(const ocl_params *p, int mx, const double *ql, const double *qr, const double *auxl,
+                       const double *auxr, double *wave, double *s, double *amdq, double *apdq) {
+  const int mbc = p->mbc, meqn = 1;
+  const long ld = mx + 2 * mbc;
+  for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+    double ui = L2(auxl, i, 1), uim = L2(auxr, i - 1, 1);
+    double fim = uim * L2(qr, i - 1, 1);
+    double fi = ui * L2(ql, i, 1);
+    L3(wave, i, 1, 1) = fi - fim;
+    if (ui > 0.0) { L2(s, i, 1) = ui; L2(amdq, i, 1) = 0.0; L2(apdq, i, 1) = L3(wave, i, 1, 1); }
+    else { L2(s, i, 1) = uim; L2(amdq, i, 1) = L3(wave, i, 1, 1); L2(apdq, i, 1) = 0.0; }
+  }
+}
+
 /* apps/acoustics/1d/interface/rp1acv.f:49-80; with ixy it is also the new 2-D
  * normal solver (mu = normal velocity, tangential components carry 0). */
 static void rp_acoustics(const ocl_params *p, int ixy, int mx, const double *ql, const double *qr,
@@ -1302,6 +1360,8 @@ int ocl_rp(const ocl_params *p, int ixy, int mx, const double *ql, const double 
     case OCL_RP_SWF_KAPPA: rp_swf(p, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq, 0); return 0;
     case OCL_RP_ACOUSTICS_CONST: rp_acconst(p, mx, ql, qr, wave, s, amdq, apdq, 0); return 0;
     case OCL_RP_ACOUSTICS_FWAVE: rp_acfwave(p, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq, 0); return 0;
+    case OCL_RP_TRAFFIC: rp_traffic(p, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq); return 0;
+    case OCL_RP_ADVECTION_CONS: rp_advcons(p, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq); return 0;
     case OCL_RP_ACOUSTICS1D:
     case OCL_RP_ACOUSTICS2D:
       rp_acoustics(p, ixy, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq); return 0;
@@ -1348,6 +1408,7 @@ int ocl_tfluct(const ocl_params *p, int ixy, int mx, const double *ql, const dou
       free(wave); free(am); free(ap);
       return 0;
     }
+    case OCL_RP_TRAFFIC: tfluct_traffic(p, mx, ql, qr, auxl, auxr, adq); return 0;
     case OCL_RP_ACOUSTICS_CONST:
     case OCL_RP_ACOUSTICS_FWAVE: {
       const long ld = mx + 2L * p->mbc;
@@ -1372,7 +1433,9 @@ int ocl_evec(const ocl_params *p, int ixy, int mx, const double *q, const double
   (void)auxr;
   switch (p->rp) {
     case OCL_RP_ADVECTION:
-    case OCL_RP_ADVECTION2D: evec_advection(p, mx, evl, evr); return 0;
+    case OCL_RP_ADVECTION2D:
+    case OCL_RP_TRAFFIC:
+    case OCL_RP_ADVECTION_CONS: evec_advection(p, mx, evl, evr); return 0;
     case OCL_RP_EULER: evec_euler(p, mx, q, evl, evr); return 0;
     case OCL_RP_SW2D: evec_sw(p, ixy, mx, q, evl, evr); return 0;
     case OCL_RP_SW1D: evec_sw1d(p, mx, q, evl, evr); return 0;

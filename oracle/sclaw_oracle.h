@@ -43,8 +43,11 @@ enum {
                                r(i), r(i), dx), capacity aux(:,2)                      */
   OCL_RP_ACOUSTICS_CONST = 11,  /* apps/acoustics/1d/homogeneous/{rp1.f,tfluct.f,evec.f},
                                    common /cparam/ rho, bulk                           */
-  OCL_RP_ACOUSTICS_FWAVE = 12   /* apps/acoustics/1d/fwave/{rp1acfw.f,tfluct1.f,evec.f}:
+  OCL_RP_ACOUSTICS_FWAVE = 12,  /* apps/acoustics/1d/fwave/{rp1acfw.f,tfluct1.f,evec.f}:
                                    q = (strain, momentum), aux = (rho, bulk)           */
+  OCL_RP_TRAFFIC = 13,      /* apps/traffic/congTraffic/{rpf-wave.f90,tfluct1.f90}:
+                               flux umax(x) q (1-q), aux = umax                        */
+  OCL_RP_ADVECTION_CONS = 14 /* apps/traffic/flux-uq/rpf-wave.f90: (u(x) q)_x, aux = u  */
 };
 
 /* Source-term hooks: the src(q,dq,aux,t,dt) an app links (src/1d/step1d.f90:23). */

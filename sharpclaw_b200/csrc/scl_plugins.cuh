@@ -895,6 +895,92 @@ struct PAcousticsFwave {
   }
 };
 
+// ------------------------------------------------------------------------
+// Traffic flow with a variable speed limit, apps/traffic/congTraffic
+// (rpf-wave.f90:30-72, tfluct1.f90:27-33): flux umax(x) q (1-q), aux = umax;
+// the f-wave goes left, right, or (transonic rarefaction) splits at the
+// sonic flux min(umax) / 4.
+// ------------------------------------------------------------------------
+struct PTraffic {
+  static constexpr int MEQN = 1, MWAVES = 1, MAUX = 1, NDIM = 1;
+  static constexpr bool HAS_TFLUCT = true;
+  template <class R, bool FD = false>
+  __device__ static void rp(const Phys&, int, const R* L, const R* Rt, const R*, const R* am, const R* a0,
+                            R* s, R* amdq, R* apdq) {
+    const R fim1 = (am[0] * L[0]) * ((R)1 - L[0]);
+    const R fi = (a0[0] * Rt[0]) * ((R)1 - Rt[0]);
+    const R fw = fi - fim1;
+    const R sim1 = am[0] * ((R)1 - (R)2 * L[0]);
+    const R si = a0[0] * ((R)1 - (R)2 * Rt[0]);
+    if (sim1 < (R)0 && si <= (R)0) {
+      s[0] = sim1; amdq[0] = fw; apdq[0] = (R)0;
+    } else if (sim1 >= (R)0 && si > (R)0) {
+      s[0] = si; amdq[0] = (R)0; apdq[0] = fw;
+    } else if (sim1 < (R)0 && si > (R)0) {
+      s[0] = (R)0.5 * (sim1 + si);
+      const R f0 = rmin(am[0], a0[0]) * (R)0.25;
+      amdq[0] = f0 - fim1;
+      apdq[0] = fi - f0;
+    } else {
+      s[0] = (R)0.5 * (sim1 + si);
+      if (s[0] < (R)0) { amdq[0] = fw; apdq[0] = (R)0; }
+      else if (s[0] > (R)0) { amdq[0] = (R)0; apdq[0] = fw; }
+      else { amdq[0] = (R)0.5 * fw; apdq[0] = (R)0.5 * fw; }
+    }
+  }
+  template <class R, bool FD = false>
+  __device__ static void waves(const Phys& ph, int ixy, const R* L, const R* Rt, const R* dl, const R* am,
+                               const R* a0, R w[1][1], R* s = nullptr) {
+    w[0][0] = (a0[0] * Rt[0]) * ((R)1 - Rt[0]) - (am[0] * L[0]) * ((R)1 - L[0]);
+    if (s) {
+      R sp[1], m1[1], p1[1];
+      rp<R, FD>(ph, ixy, L, Rt, dl, am, a0, sp, m1, p1);
+      s[0] = sp[0];
+    }
+  }
+  template <class R, bool FD = false>
+  __device__ static void tfluct(const Phys&, int, const R* L, const R* Rt, const R*, const R* aux, R* adq) {
+    adq[0] = (aux[0] * Rt[0]) * ((R)1 - Rt[0]) - (aux[0] * L[0]) * ((R)1 - L[0]);
+  }
+  template <class R, bool FD = false>
+  __device__ static void evec(const Phys&, int, const R*, const R*, const R*, const R*, R evl[1][1],
+                              R evr[1][1]) {
+    evl[0][0] = (R)1;
+    evr[0][0] = (R)1;
+  }
+};
+
+// ------------------------------------------------------------------------
+// Conservative advection with cell velocities, apps/traffic/flux-uq
+// (rpf-wave.f90:34-52): f-wave u(i) q(i) - u(i-1) q(i-1), to the right when
+// u(i) > 0, aux = u.  The app has no tfluct (tfluct_solver 0).
+// ------------------------------------------------------------------------
+struct PAdvCons {
+  static constexpr int MEQN = 1, MWAVES = 1, MAUX = 1, NDIM = 1;
+  static constexpr bool HAS_TFLUCT = false;
+  template <class R, bool FD = false>
+  __device__ static void rp(const Phys&, int, const R* L, const R* Rt, const R*, const R* am, const R* a0,
+                            R* s, R* amdq, R* apdq) {
+    const R fw = a0[0] * Rt[0] - am[0] * L[0];
+    if (a0[0] > (R)0) { s[0] = a0[0]; amdq[0] = (R)0; apdq[0] = fw; }
+    else { s[0] = am[0]; amdq[0] = fw; apdq[0] = (R)0; }
+  }
+  template <class R, bool FD = false>
+  __device__ static void waves(const Phys&, int, const R* L, const R* Rt, const R*, const R* am, const R* a0,
+                               R w[1][1], R* s = nullptr) {
+    w[0][0] = a0[0] * Rt[0] - am[0] * L[0];
+    if (s) s[0] = a0[0] > (R)0 ? a0[0] : am[0];
+  }
+  template <class R, bool FD = false>
+  __device__ static void tfluct(const Phys&, int, const R*, const R*, const R*, const R*, R*) {}
+  template <class R, bool FD = false>
+  __device__ static void evec(const Phys&, int, const R*, const R*, const R*, const R*, R evl[1][1],
+                              R evr[1][1]) {
+    evl[0][0] = (R)1;
+    evr[0][0] = (R)1;
+  }
+};
+
 // Plugins whose total fluctuation reads the aux of cells c-1, c, c+1 (three
 // MAUX groups, centre in the middle) declare TFLUCT_NB = true.
 template <class P, class = void>

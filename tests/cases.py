@@ -283,3 +283,36 @@ def acoustics_fwave(mx=200, char_decomp=2, tfluct_solver=1, mthbc=(1, 1)):
     po = O.make_params(meqn=2, mwaves=2, maux=2, rp=O.RP_ACOUSTICS_FWAVE, **kw)
     ps = S.ClawParams(rp=S.RP_ACOUSTICS_FWAVE, **kw)
     return po, ps, q, aux
+
+
+def traffic(mx=300, rho=(0.13, 0.1), umax=(2.0, 1.0), lower=-20.0, upper=40.0, mthbc=(1, 1), char_decomp=0,
+            tfluct_solver=1):
+    """apps/traffic/congTraffic (setrun.py: [-20, 40], densities 0.13 / 0.1,
+    speed limits 2 / 1 on either side of x = 0, extrapolation bc): q = density,
+    aux = umax per cell (the app's setaux.f90 leaves aux unset; the limits of
+    its setprob data are used, split at x = 0 like its qinit)."""
+    dx = (upper - lower) / mx
+    xa = lower + (np.arange(-3, mx + 3) + 0.5) * dx
+    aux = np.ascontiguousarray(np.where(xa < 0.0, umax[0], umax[1])[None, :])
+    q = np.zeros((1, mx + 6))
+    q[0, 3:-3] = np.where(xa[3:-3] < 0.0, rho[0], rho[1])
+    kw = dict(mx=mx, dx=dx, xlower=lower, mthbc=mthbc, char_decomp=char_decomp, tfluct_solver=tfluct_solver)
+    po = O.make_params(meqn=1, mwaves=1, maux=1, rp=O.RP_TRAFFIC, **kw)
+    ps = S.ClawParams(rp=S.RP_TRAFFIC, **kw)
+    return po, ps, q, aux
+
+
+def advection_cons(mx=300, u=(2.0, 1.0), rho=(0.3333, 0.1), lower=-45.0, upper=45.0, mthbc=(1, 1),
+                   char_decomp=0):
+    """apps/traffic/flux-uq: (u(x) q)_x = 0 with cell velocities u1 / u2 and
+    densities rho1 / rho2 on either side of x = 0 (setaux.f90, qinit.f90),
+    [-45, 45], extrapolation bc, the swapped second solve."""
+    dx = (upper - lower) / mx
+    xa = lower + (np.arange(-3, mx + 3) + 0.5) * dx
+    aux = np.ascontiguousarray(np.where(xa < 0.0, u[0], u[1])[None, :])
+    q = np.zeros((1, mx + 6))
+    q[0, 3:-3] = np.where(xa[3:-3] < 0.0, rho[0], rho[1])
+    kw = dict(mx=mx, dx=dx, xlower=lower, mthbc=mthbc, char_decomp=char_decomp, tfluct_solver=0)
+    po = O.make_params(meqn=1, mwaves=1, maux=1, rp=O.RP_ADVECTION_CONS, **kw)
+    ps = S.ClawParams(rp=S.RP_ADVECTION_CONS, **kw)
+    return po, ps, q, aux

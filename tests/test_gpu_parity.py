@@ -99,6 +99,13 @@ STEP_CASES = [
     ("acfwave_comp_tf0", lambda: cases.acoustics_fwave(mx=140, char_decomp=0, tfluct_solver=0)),
     ("acfwave_wave", lambda: cases.acoustics_fwave(mx=120, char_decomp=1)),
     ("acfwave_tvd2_wave", lambda: cases.with_tvd(cases.acoustics_fwave(mx=100), (3, 4, 1, 1), 1)),
+    # apps/traffic/congTraffic and apps/traffic/flux-uq
+    ("traffic_tf1", lambda: cases.traffic(mx=150)),
+    ("traffic_transonic_tf0", lambda: cases.traffic(mx=120, rho=(0.8, 0.2), umax=(1.0, 1.5), tfluct_solver=0)),
+    ("traffic_wave", lambda: cases.traffic(mx=110, rho=(0.3, 0.7), char_decomp=1)),
+    ("traffic_poly3", lambda: cases.with_poly(cases.traffic(mx=100), 0)),
+    ("advcons", lambda: cases.advection_cons(mx=140)),
+    ("advcons_trans", lambda: cases.advection_cons(mx=100, u=(-1.0, 2.0), char_decomp=3)),
 ]
 
 
@@ -190,6 +197,8 @@ RUN_CASES = [
     ("swf_kappa_ssp104", lambda: cases.fwave_radial(mx=100, kappa=True), 4, dict(tend=0.1, dt_initial=0.001, cfl_max=0.3, cfl_desired=0.2)),
     ("acconst_ssp104", lambda: cases.acoustics_const(mx=200), 4, dict(tend=0.5, dt_initial=0.001, cfl_max=0.25, cfl_desired=0.25)),
     ("acfwave_ssp104", lambda: cases.acoustics_fwave(mx=200), 4, dict(tend=2.0, dt_initial=0.025, cfl_max=2.5, cfl_desired=2.45)),
+    ("traffic_ssp104", lambda: cases.traffic(mx=300), 4, dict(tend=10.0, dt_initial=0.01, cfl_max=0.3, cfl_desired=0.2)),
+    ("advcons_ssp22", lambda: cases.advection_cons(mx=300), 1, dict(tend=10.0, dt_initial=0.01, cfl_max=0.5, cfl_desired=0.45)),
 ]
 
 

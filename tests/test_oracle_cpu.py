@@ -302,3 +302,43 @@ def test_acoustics_app_eigenvectors_are_inverse_pairs():
         evl, evr = O.evec(p, q, aux if rp == O.RP_ACOUSTICS_FWAVE else None)
         for i in range(1, n):
             assert np.allclose(evl[:, :, i].T @ evr[:, :, i].T, np.eye(2), atol=1e-12)
+
+
+@pytest.mark.parametrize("rho", [(0.2, 0.6), (0.8, 0.2)], ids=["shock", "transonic_rarefaction"])
+def test_traffic_riemann_exact(rho):
+    """apps/traffic/congTraffic's f-wave solver with a uniform speed limit 1:
+    the LWR Riemann problem has a shock of speed 1 - rho_l - rho_r, or a fan
+    rho = (1 - x/t)/2 through the sonic point (the solver's transonic split);
+    L1 error of the cell averages at t = 0.5 halves with dx."""
+    rl, rr = rho
+    errs = []
+    for mx in (200, 400):
+        po, _, q, aux = cases.traffic(mx=mx, rho=rho, umax=(1.0, 1.0), lower=-1.0, upper=1.0)
+        T = 0.5
+        qf, r = O.sharpclaw(po, q, aux, tstart=0.0, tend=T, dt_initial=0.001, cfl_max=0.5, cfl_desired=0.45,
+                            time_integrator=4)
+        assert r.info == 0
+        dx = 2.0 / mx
+        xc = -1.0 + (np.arange(mx) + 0.5) * dx
+        if rl < rr:
+            ex = np.where(xc < (1.0 - rl - rr) * T, rl, rr)
+        else:
+            xi = xc / T
+            ex = np.where(xi < 1 - 2 * rl, rl, np.where(xi > 1 - 2 * rr, rr, 0.5 * (1 - xi)))
+        errs.append(np.abs(qf[0, 3:-3] - ex).sum() * dx)
+    assert errs[0] < 2e-3 and errs[1] < 0.6 * errs[0], errs
+
+
+def test_conservative_advection_uniform_velocity():
+    """apps/traffic/flux-uq's solver with a uniform velocity is upwind
+    advection: one period on a periodic domain returns the data to within the
+    WENO5 error, and the total is conserved to rounding."""
+    mx = 200
+    po, _, q, aux = cases.advection_cons(mx=mx, u=(1.0, 1.0), lower=0.0, upper=1.0, mthbc=(2, 2))
+    xc = (np.arange(mx) + 0.5) / mx
+    q[0, 3:-3] = 1.0 + 0.5 * np.sin(2 * np.pi * xc)
+    qf, r = O.sharpclaw(po, q, aux, tstart=0.0, tend=1.0, dt_initial=0.002, cfl_max=0.5, cfl_desired=0.45,
+                        time_integrator=3)
+    assert r.info == 0
+    assert np.abs(qf[0, 3:-3] - q[0, 3:-3]).max() < 1e-6
+    assert abs(qf[0, 3:-3].sum() - q[0, 3:-3].sum()) <= 1e-12 * q[0, 3:-3].sum()
