@@ -67,6 +67,9 @@ extern "C" {
                                       flux umax(x) q (1-q), aux = umax                   */
 #define SCL_RP_ADVECTION_CONS 14   /* apps/traffic/flux-uq/rpf-wave.f90: (u(x) q)_x with
                                       cell velocities aux = u; no tfluct                 */
+#define SCL_RP_STEGOTON 15         /* apps/elasticity/stegoton/{rp1nel.f,tfluct1.f}: stress
+                                      exp(A eps) - 1 (A > 0) or B eps, aux = (rho, A, B)
+                                      (+ evec of the form of acoustics/1d/fwave, new)    */
 
 /* ---- source terms: the src(q,dq,aux,t,dt) an app links (src/1d/step1d.f90:23),
  * evaluated in the stage kernel before the fluctuations are subtracted;

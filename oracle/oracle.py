@@ -23,7 +23,7 @@ _LIB = os.path.join(_HERE, "libsclaw_oracle.so")
 RP_ADVECTION, RP_EULER, RP_SW2D, RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION2D, RP_SW1D = 1, 2, 3, 4, 5, 6, 7
 RP_SWF_BATHY, RP_SWF_RADIAL, RP_SWF_KAPPA = 8, 9, 10
 RP_ACOUSTICS_CONST, RP_ACOUSTICS_FWAVE = 11, 12
-RP_TRAFFIC, RP_ADVECTION_CONS = 13, 14
+RP_TRAFFIC, RP_ADVECTION_CONS, RP_STEGOTON = 13, 14, 15
 SRC_NONE, SRC_RADIAL_SW, SRC_BATHYMETRY_SW = 0, 1, 2
 
 

@@ -888,7 +888,7 @@ static void evec_sw(const ocl_params *p, int ixy, int mx, const double *q, doubl
   }
 }
 
-/* apps/shallowWater/2dRadialDam/1dRadialSymm-qwave/rp1sw.f:46-183: 1-D
+/* apps/shallowWater/2dRadialDam/1dRadialSymm-qwave/rp1sw.f:43-185: 1-D
  * shallow water Roe solver, Harten-Hyman entropy fix when p->efix (the app's
  * data efix /.true./).  cell_internal: the same solve with left ql(i) and
  * right qr(i) (tfluct1sw.f of that app, which returns adq = amdq + apdq). */
@@ -1082,7 +1082,7 @@ static void evec_swf(const ocl_params *p, int mx, const double *q, double *evl, 
   }
 }
 
-/* apps/acoustics/1d/homogeneous: rp1.f:33-53 and tfluct.f (cell_internal:
+/* apps/acoustics/1d/homogeneous: rp1.f:50-76 and tfluct.f (cell_internal:
  * left ql(i), right qr(i), adq = amdq + apdq), cc = sqrt(bulk/rho), zz =
  * cc*rho as setprob.f computes them. */
 static void rp_acconst(const ocl_params *p, int mx, const double *ql, const double *qr, double *wave,
@@ -1128,33 +1128,51 @@ static void evec_acconst(const ocl_params *p, int mx, double *evl, double *evr) 
   }
 }
 
-/* apps/acoustics/1d/fwave: rp1acfw.f:40-78 (linear stress sigma = bulk*eps,
- * sigmap = bulk, :85-100) and tfluct1.f (cell_internal: both sides use
- * aux(i), left ql(i), right qr(i)). */
+/* Stress laws: apps/acoustics/1d/fwave/rp1acfw.f:116-140 (sigma = bulk*eps)
+ * and apps/elasticity/stegoton/rp1nel.f:116-175 (exp(A eps) - 1 for A > 0,
+ * else B eps), with their derivatives. */
+static double sigma_el(const ocl_params *p, double eps, double a, double b) {
+  if (p->rp == OCL_RP_STEGOTON) return a > 0.0 ? exp(a * eps) - 1.0 : b * eps;
+  return a * eps;
+}
+static double sigmap_el(const ocl_params *p, double eps, double a, double b) {
+  if (p->rp == OCL_RP_STEGOTON) return a > 0.0 ? a * exp(a * eps) : b;
+  (void)eps;
+  return a;
+}
+
+/* apps/acoustics/1d/fwave: rp1acfw.f:53-109 and tfluct1.f (cell_internal:
+ * both sides use aux(i), left ql(i), right qr(i)); the same for
+ * apps/elasticity/stegoton (rp1nel.f:53-109, tfluct1.f:56-113) with its stress law. */
 static void rp_acfwave(const ocl_params *p, int mx, const double *ql, const double *qr, const double *auxl,
                        const double *auxr, double *wave, double *s, double *amdq, double *apdq,
                        int cell_internal) {
   const int mbc = p->mbc, meqn = 2;
   const long ld = mx + 2 * mbc;
   for (int i = 2 - mbc; i <= mx + mbc; ++i) {
-    double rhoi, rhoim, epsi, epsim, urhoi, urhoim, ki, kim;
+    double rhoi, rhoim, epsi, epsim, urhoi, urhoim, ai, aim, bi = 0.0, bim = 0.0;
+    const int nl = p->rp == OCL_RP_STEGOTON;
     if (cell_internal) {
       rhoi = L2(auxr, i, 1); rhoim = L2(auxl, i, 1);
       epsi = L2(qr, i, 1); epsim = L2(ql, i, 1);
       urhoi = L2(qr, i, 2); urhoim = L2(ql, i, 2);
-      ki = L2(auxr, i, 2); kim = L2(auxl, i, 2);
+      ai = L2(auxr, i, 2); aim = L2(auxl, i, 2);
+      if (nl) { bi = L2(auxr, i, 3); bim = L2(auxl, i, 3); }
     } else {
       rhoi = L2(auxl, i, 1); rhoim = L2(auxr, i - 1, 1);
       epsi = L2(ql, i, 1); epsim = L2(qr, i - 1, 1);
       urhoi = L2(ql, i, 2); urhoim = L2(qr, i - 1, 2);
-      ki = L2(auxl, i, 2); kim = L2(auxr, i - 1, 2);
+      ai = L2(auxl, i, 2); aim = L2(auxr, i - 1, 2);
+      if (nl) { bi = L2(auxl, i, 3); bim = L2(auxr, i - 1, 3); }
     }
+    double ki = sigmap_el(p, epsi, ai, bi);
+    double kim = sigmap_el(p, epsim, aim, bim);
     double ci = sqrt(ki / rhoi);
     double cim = sqrt(kim / rhoim);
     double zi = ci * rhoi;
     double zim = cim * rhoim;
     double du = urhoi / rhoi - urhoim / rhoim;
-    double dsig = ki * epsi - kim * epsim;
+    double dsig = sigma_el(p, epsi, ai, bi) - sigma_el(p, epsim, aim, bim);
     double b1 = -((zi * du + dsig) / (zim + zi));
     double b2 = -((zim * du - dsig) / (zim + zi));
     L3(wave, i, 1, 1) = b1;
@@ -1173,13 +1191,16 @@ static void rp_acfwave(const ocl_params *p, int mx, const double *ql, const doub
 
 /* apps/acoustics/1d/fwave/evec.f:40-63 (as the app writes it: evl holds the
  * rows (1, 1) and (zim, -zi), evr their inverse) */
-static void evec_acfwave(const ocl_params *p, int mx, const double *auxl, const double *auxr, double *evl,
-                         double *evr) {
+static void evec_acfwave(const ocl_params *p, int mx, const double *q, const double *auxl, const double *auxr,
+                         double *evl, double *evr) {
   const int mbc = p->mbc, meqn = 2;
   const long ld = mx + 2 * mbc;
+  const int nl = p->rp == OCL_RP_STEGOTON;
   for (int i = 2 - mbc; i <= mx + mbc; ++i) {
-    double ci = sqrt(L2(auxl, i, 2) / L2(auxl, i, 1));
-    double cim = sqrt(L2(auxr, i - 1, 2) / L2(auxr, i - 1, 1));
+    double ki = sigmap_el(p, L2(q, i, 1), L2(auxl, i, 2), nl ? L2(auxl, i, 3) : 0.0);
+    double kim = sigmap_el(p, L2(q, i - 1, 1), L2(auxr, i - 1, 2), nl ? L2(auxr, i - 1, 3) : 0.0);
+    double ci = sqrt(ki / L2(auxl, i, 1));
+    double cim = sqrt(kim / L2(auxr, i - 1, 1));
     double zi = ci * L2(auxl, i, 1);
     double zim = cim * L2(auxr, i - 1, 1);
     L3(evl, i, 1, 1) = 1.0;
@@ -1194,9 +1215,9 @@ static void evec_acfwave(const ocl_params *p, int mx, const double *auxl, const 
   }
 }
 
-/* apps/traffic/congTraffic/rpf-wave.f90:30-72: f-wave for the flux
+/* apps/traffic/congTraffic/rpf-wave.f90:42-90: f-wave for the flux
  * umax(x) q (1-q) with the entropy-satisfying split of its four sign cases;
- * tfluct1.f90:27-33: the cell's flux difference (both sides aux(i)). */
+ * tfluct1.f90:39-49: the cell's flux difference (both sides aux(i)). */
 static void rp_traffic(const ocl_params *p, int mx, const double *ql, const double *qr, const double *auxl,
                        const double *auxr, double *wave, double *s, double *amdq, double *apdq) {
   const int mbc = p->mbc, meqn = 1;
@@ -1236,7 +1257,7 @@ static void tfluct_traffic(const ocl_params *p, int mx, const double *ql, const 
   }
 }
 
-/* apps/traffic/flux-uq/rpf-wave.f90:34-52: conservative advection with cell
+/* apps/traffic/flux-uq/rpf-wave.f90:43-64: conservative advection with cell
  * velocities, f-wave u(i) q(i) - u(i-1) q(i-1) to the side of u(i)'s sign. */
 static void rp_advcons(const ocl_params *p, int mx, const double *ql, const double *qr, const double *auxl,
                        const double *auxr, double *wave, double *s, double *amdq, double *apdq) {
@@ -1359,7 +1380,8 @@ int ocl_rp(const ocl_params *p, int ixy, int mx, const double *ql, const double 
     case OCL_RP_SWF_RADIAL:
     case OCL_RP_SWF_KAPPA: rp_swf(p, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq, 0); return 0;
     case OCL_RP_ACOUSTICS_CONST: rp_acconst(p, mx, ql, qr, wave, s, amdq, apdq, 0); return 0;
-    case OCL_RP_ACOUSTICS_FWAVE: rp_acfwave(p, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq, 0); return 0;
+    case OCL_RP_ACOUSTICS_FWAVE:
+    case OCL_RP_STEGOTON: rp_acfwave(p, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq, 0); return 0;
     case OCL_RP_TRAFFIC: rp_traffic(p, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq); return 0;
     case OCL_RP_ADVECTION_CONS: rp_advcons(p, mx, ql, qr, auxl, auxr, wave, s, amdq, apdq); return 0;
     case OCL_RP_ACOUSTICS1D:
@@ -1410,7 +1432,8 @@ int ocl_tfluct(const ocl_params *p, int ixy, int mx, const double *ql, const dou
     }
     case OCL_RP_TRAFFIC: tfluct_traffic(p, mx, ql, qr, auxl, auxr, adq); return 0;
     case OCL_RP_ACOUSTICS_CONST:
-    case OCL_RP_ACOUSTICS_FWAVE: {
+    case OCL_RP_ACOUSTICS_FWAVE:
+    case OCL_RP_STEGOTON: {
       const long ld = mx + 2L * p->mbc;
       double *wave = (double *)calloc((size_t)ld * 4, sizeof(double));
       double *am = (double *)calloc((size_t)ld * 2, sizeof(double));
@@ -1443,7 +1466,8 @@ int ocl_evec(const ocl_params *p, int ixy, int mx, const double *q, const double
     case OCL_RP_SWF_RADIAL:
     case OCL_RP_SWF_KAPPA: evec_swf(p, mx, q, evl, evr); return 0;
     case OCL_RP_ACOUSTICS_CONST: evec_acconst(p, mx, evl, evr); return 0;
-    case OCL_RP_ACOUSTICS_FWAVE: evec_acfwave(p, mx, auxl, auxr, evl, evr); return 0;
+    case OCL_RP_ACOUSTICS_FWAVE:
+    case OCL_RP_STEGOTON: evec_acfwave(p, mx, q, auxl, auxr, evl, evr); return 0;
     case OCL_RP_ACOUSTICS1D:
     case OCL_RP_ACOUSTICS2D: evec_acoustics(p, ixy, mx, auxl, evl, evr); return 0;
   }

@@ -47,7 +47,9 @@ enum {
                                    q = (strain, momentum), aux = (rho, bulk)           */
   OCL_RP_TRAFFIC = 13,      /* apps/traffic/congTraffic/{rpf-wave.f90,tfluct1.f90}:
                                flux umax(x) q (1-q), aux = umax                        */
-  OCL_RP_ADVECTION_CONS = 14 /* apps/traffic/flux-uq/rpf-wave.f90: (u(x) q)_x, aux = u  */
+  OCL_RP_ADVECTION_CONS = 14, /* apps/traffic/flux-uq/rpf-wave.f90: (u(x) q)_x, aux = u */
+  OCL_RP_STEGOTON = 15      /* apps/elasticity/stegoton/{rp1nel.f,tfluct1.f}: sigma =
+                               exp(A eps) - 1 (A > 0) or B eps, aux = (rho, A, B)      */
 };
 
 /* Source-term hooks: the src(q,dq,aux,t,dt) an app links (src/1d/step1d.f90:23). */

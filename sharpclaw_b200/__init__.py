@@ -29,7 +29,7 @@ import numpy as np
 
 from . import _capi as C
 from ._capi import (B4STEP_NONE, B4STEP_SWIRL, FP32, FP64, FP64_STRICT, MIXED,  # noqa: F401
-                    RP_ACOUSTICS_CONST, RP_ACOUSTICS_FWAVE, RP_ADVECTION_CONS, RP_TRAFFIC,
+                    RP_ACOUSTICS_CONST, RP_ACOUSTICS_FWAVE, RP_ADVECTION_CONS, RP_STEGOTON, RP_TRAFFIC,
                     RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION, RP_ADVECTION2D, RP_EULER, RP_SW1D, RP_SW2D,
                     RP_SWF_BATHY, RP_SWF_KAPPA, RP_SWF_RADIAL, SRC_BATHYMETRY_SW, SRC_NONE, SRC_RADIAL_SW,
                     RUN_AUTO, RUN_GRAPH, RUN_RESIDENT, SharpClawError)
@@ -37,6 +37,7 @@ from ._capi import (B4STEP_NONE, B4STEP_SWIRL, FP32, FP64, FP64_STRICT, MIXED,  
 __all__ = ["ClawParams", "Solver", "Batch", "sharpclaw", "SharpClawError", "RP_ADVECTION", "RP_EULER",
            "RP_SW2D", "RP_ACOUSTICS1D", "RP_ACOUSTICS2D", "RP_ADVECTION2D", "RP_SW1D", "RP_SWF_BATHY", "RP_SWF_RADIAL", "RP_SWF_KAPPA",
            "RP_ACOUSTICS_CONST", "RP_ACOUSTICS_FWAVE", "RP_TRAFFIC", "RP_ADVECTION_CONS",
+           "RP_STEGOTON",
            "SRC_NONE", "SRC_RADIAL_SW",
            "SRC_BATHYMETRY_SW", "B4STEP_NONE", "B4STEP_SWIRL",
            "RUN_AUTO", "RUN_GRAPH", "RUN_RESIDENT"]
@@ -57,6 +58,7 @@ PLUGINS = {
     RP_ACOUSTICS_FWAVE: (2, 2, 2, 1),
     RP_TRAFFIC: (1, 1, 1, 1),
     RP_ADVECTION_CONS: (1, 1, 1, 1),
+    RP_STEGOTON: (2, 2, 3, 1),
 }
 
 

@@ -444,7 +444,8 @@ int validate(const scl_params* p) {
       {SCL_RP_ACOUSTICS1D, 2, 2, 2, 1}, {SCL_RP_ACOUSTICS2D, 3, 2, 2, 2},
       {SCL_RP_ADVECTION2D, 1, 1, 2, 2}, {SCL_RP_SW1D, 2, 2, 0, 1}, {SCL_RP_SWF_BATHY, 2, 2, 1, 1},
       {SCL_RP_SWF_RADIAL, 2, 2, 2, 1}, {SCL_RP_SWF_KAPPA, 2, 2, 4, 1}, {SCL_RP_ACOUSTICS_CONST, 2, 2, 0, 1},
-      {SCL_RP_ACOUSTICS_FWAVE, 2, 2, 2, 1}, {SCL_RP_TRAFFIC, 1, 1, 1, 1}, {SCL_RP_ADVECTION_CONS, 1, 1, 1, 1}};
+      {SCL_RP_ACOUSTICS_FWAVE, 2, 2, 2, 1}, {SCL_RP_TRAFFIC, 1, 1, 1, 1}, {SCL_RP_ADVECTION_CONS, 1, 1, 1, 1},
+      {SCL_RP_STEGOTON, 2, 2, 3, 1}};
   if (p->rp == SCL_RP_ADVECTION_CONS && p->tfluct_solver == 1)
     return fail(SCL_E_INVALID, "the flux-uq app has no tfluct: use tfluct_solver 0");
   if (p->rp == SCL_RP_ACOUSTICS_CONST && !(p->rho > 0 && p->bulk > 0))

@@ -278,7 +278,8 @@ bool SCL_PREC_GETTER(int rp, int ndim, int cd, int tf, int variant, Launchers* L
     case SCL_RP_SWF_RADIAL: return ndim == 1 && pick<PShallowF1D<1>>(ndim, cd, tf, variant, L);
     case SCL_RP_SWF_KAPPA: return ndim == 1 && pick<PShallowF1D<2>>(ndim, cd, tf, variant, L);
     case SCL_RP_ACOUSTICS_CONST: return ndim == 1 && pick<PAcousticsConst>(ndim, cd, tf, variant, L);
-    case SCL_RP_ACOUSTICS_FWAVE: return ndim == 1 && pick<PAcousticsFwave>(ndim, cd, tf, variant, L);
+    case SCL_RP_ACOUSTICS_FWAVE: return ndim == 1 && pick<PElasticFwave<0>>(ndim, cd, tf, variant, L);
+    case SCL_RP_STEGOTON: return ndim == 1 && pick<PElasticFwave<1>>(ndim, cd, tf, variant, L);
     case SCL_RP_TRAFFIC: return ndim == 1 && pick<PTraffic>(ndim, cd, tf, variant, L);
     case SCL_RP_ADVECTION_CONS: return ndim == 1 && pick<PAdvCons>(ndim, cd, tf, variant, L);
   }

@@ -453,7 +453,7 @@ struct PShallow2D {
 
 // ------------------------------------------------------------------------
 // 1-D shallow water: apps/shallowWater/2dRadialDam/1dRadialSymm-qwave/
-// rp1sw.f:46-183 (Roe solver, Harten-Hyman entropy fix when ph.efix, the
+// rp1sw.f:43-185 (Roe solver, Harten-Hyman entropy fix when ph.efix, the
 // app's data efix /.true./) and tfluct1sw.f:44-186 of the same app (the same
 // solve with left ql(i), right qr(i); adq = amdq + apdq).
 // ------------------------------------------------------------------------
@@ -757,7 +757,7 @@ struct PShallowF1D {
 };
 
 // ------------------------------------------------------------------------
-// Constant-coefficient acoustics, apps/acoustics/1d/homogeneous (rp1.f:33-53,
+// Constant-coefficient acoustics, apps/acoustics/1d/homogeneous (rp1.f:50-76,
 // tfluct.f, evec.f): cc = sqrt(bulk/rho), zz = cc*rho (setprob.f), passed in
 // Phys as cc, zz.
 // ------------------------------------------------------------------------
@@ -814,20 +814,45 @@ struct PAcousticsConst {
 };
 
 // ------------------------------------------------------------------------
-// Acoustics in strain / momentum form with f-waves, apps/acoustics/1d/fwave
-// (rp1acfw.f:40-78 with the linear sigma = bulk*eps of :85-100, tfluct1.f,
-// evec.f): q = (eps, rho u), aux = (rho, bulk).  The app's evec puts the
-// rows (1, 1) and (zim, -zi) in evl and their inverse in evr; kept as written.
+// Elasticity in strain / momentum form with f-waves, q = (eps, rho u):
+//   NL = 0  apps/acoustics/1d/fwave (rp1acfw.f:53-109, tfluct1.f, evec.f):
+//           linear stress sigma = bulk*eps (rp1acfw.f:116-140), aux = (rho, bulk)
+//   NL = 1  apps/elasticity/stegoton (rp1nel.f:53-175, tfluct1.f): sigma =
+//           exp(A eps) - 1 where A > 0, else B eps; aux = (rho, A, B)
+// The acoustics app's evec puts the rows (1, 1) and (zim, -zi) in evl and
+// their inverse in evr; kept as written, and used with the stegoton's
+// stress law too (that app builds no evec; new).
 // ------------------------------------------------------------------------
-struct PAcousticsFwave {
-  static constexpr int MEQN = 2, MWAVES = 2, MAUX = 2, NDIM = 1;
+template <int NL>
+struct PElasticFwave {
+  static constexpr int MEQN = 2, MWAVES = 2, MAUX = NL ? 3 : 2, NDIM = 1;
   static constexpr bool HAS_TFLUCT = true;
+
+  // stress and its derivative of the material a at strain eps
+  template <class R>
+  __device__ static R sigma(R eps, const R* a) {
+    if constexpr (NL) {
+      if (a[1] > (R)0) return exp(a[1] * eps) - (R)1;
+      return a[2] * eps;
+    } else {
+      return a[1] * eps;
+    }
+  }
+  template <class R>
+  __device__ static R sigmap(R eps, const R* a) {
+    if constexpr (NL) {
+      if (a[1] > (R)0) return a[1] * exp(a[1] * eps);
+      return a[2];
+    } else {
+      return a[1];
+    }
+  }
 
   // f-waves between the left state L (material am) and the right state Rt
   // (material a0)
   template <class R, bool FD = false>
   __device__ static void fwaves(const R* L, const R* Rt, const R* am, const R* a0, R w[2][2], R* s) {
-    const R rhoi = a0[0], rhoim = am[0], ki = a0[1], kim = am[1];
+    const R rhoi = a0[0], rhoim = am[0], ki = sigmap<R>(Rt[0], a0), kim = sigmap<R>(L[0], am);
     R ci, cim, du, inv;
     if constexpr (sizeof(R) == 4 || FD) {
       const R iri = (R)1 / rhoi, irim = (R)1 / rhoim;
@@ -840,7 +865,7 @@ struct PAcousticsFwave {
       du = Rt[1] / rhoi - L[1] / rhoim;
     }
     const R zi = ci * rhoi, zim = cim * rhoim;
-    const R dsig = ki * Rt[0] - kim * L[0];
+    const R dsig = sigma<R>(Rt[0], a0) - sigma<R>(L[0], am);
     R b1, b2;
     if constexpr (sizeof(R) == 4 || FD) {
       inv = (R)1 / (zim + zi);
@@ -876,15 +901,16 @@ struct PAcousticsFwave {
     for (int m = 0; m < 2; ++m) adq[m] = w[0][m] + w[1][m];
   }
   template <class R, bool FD = false>
-  __device__ static void evec(const Phys&, int, const R*, const R*, const R* am, const R* a0, R evl[2][2],
+  __device__ static void evec(const Phys&, int, const R* qm, const R* q0, const R* am, const R* a0, R evl[2][2],
                               R evr[2][2]) {
+    const R ki = sigmap<R>(q0[0], a0), kim = sigmap<R>(qm[0], am);
     R ci, cim;
     if constexpr (sizeof(R) == 4 || FD) {
-      ci = sqrt(a0[1] * ((R)1 / a0[0]));
-      cim = sqrt(am[1] * ((R)1 / am[0]));
+      ci = sqrt(ki * ((R)1 / a0[0]));
+      cim = sqrt(kim * ((R)1 / am[0]));
     } else {
-      ci = sqrt(a0[1] / a0[0]);
-      cim = sqrt(am[1] / am[0]);
+      ci = sqrt(ki / a0[0]);
+      cim = sqrt(kim / am[0]);
     }
     const R zi = ci * a0[0], zim = cim * am[0];
     evl[0][0] = (R)1; evl[0][1] = (R)1;
@@ -897,7 +923,7 @@ struct PAcousticsFwave {
 
 // ------------------------------------------------------------------------
 // Traffic flow with a variable speed limit, apps/traffic/congTraffic
-// (rpf-wave.f90:30-72, tfluct1.f90:27-33): flux umax(x) q (1-q), aux = umax;
+// (rpf-wave.f90:42-90, tfluct1.f90:39-49): flux umax(x) q (1-q), aux = umax;
 // the f-wave goes left, right, or (transonic rarefaction) splits at the
 // sonic flux min(umax) / 4.
 // ------------------------------------------------------------------------
@@ -952,7 +978,7 @@ struct PTraffic {
 
 // ------------------------------------------------------------------------
 // Conservative advection with cell velocities, apps/traffic/flux-uq
-// (rpf-wave.f90:34-52): f-wave u(i) q(i) - u(i-1) q(i-1), to the right when
+// (rpf-wave.f90:43-64): f-wave u(i) q(i) - u(i-1) q(i-1), to the right when
 // u(i) > 0, aux = u.  The app has no tfluct (tfluct_solver 0).
 // ------------------------------------------------------------------------
 struct PAdvCons {

@@ -316,3 +316,24 @@ def advection_cons(mx=300, u=(2.0, 1.0), rho=(0.3333, 0.1), lower=-45.0, upper=4
     po = O.make_params(meqn=1, mwaves=1, maux=1, rp=O.RP_ADVECTION_CONS, **kw)
     ps = S.ClawParams(rp=S.RP_ADVECTION_CONS, **kw)
     return po, ps, q, aux
+
+
+def stegoton(mx=200, char_decomp=0, tfluct_solver=1, mthbc=(1, 1), amp=0.05):
+    """apps/elasticity/stegoton: layered medium (setaux.f: rho, K = 1, 1 in
+    the first half of each unit cell, 4, 4 in the second; aux(:,3) = 0, so the
+    stress is exp(K eps) - 1), strain eps and momentum rho u; a smooth strain
+    pulse stands in for the app's moving-wall boundary condition (mthbc 0,
+    user code that the device path does not run)."""
+    lower, upper = 0.0, 30.0
+    dx = (upper - lower) / mx
+    xa = lower + (np.arange(-3, mx + 3) + 0.5) * dx
+    frac = xa - np.floor(xa)
+    rho = np.where(frac < 0.5, 1.0, 4.0)
+    K = np.where(frac < 0.5, 1.0, 4.0)
+    aux = np.ascontiguousarray(np.stack([rho, K, np.zeros_like(xa)]))
+    q = np.zeros((2, mx + 6))
+    q[0, 3:-3] = amp * np.exp(-((xa[3:-3] - 8.0) / 2.0) ** 2)
+    kw = dict(mx=mx, dx=dx, xlower=lower, mthbc=mthbc, char_decomp=char_decomp, tfluct_solver=tfluct_solver)
+    po = O.make_params(meqn=2, mwaves=2, maux=3, rp=O.RP_STEGOTON, **kw)
+    ps = S.ClawParams(rp=S.RP_STEGOTON, **kw)
+    return po, ps, q, aux

@@ -342,3 +342,19 @@ def test_conservative_advection_uniform_velocity():
     assert r.info == 0
     assert np.abs(qf[0, 3:-3] - q[0, 3:-3]).max() < 1e-6
     assert abs(qf[0, 3:-3].sum() - q[0, 3:-3].sum()) <= 1e-12 * q[0, 3:-3].sum()
+
+
+def test_stegoton_small_strain_is_linear_acoustics():
+    """apps/elasticity/stegoton's stress exp(K eps) - 1 linearises to K eps:
+    for a strain pulse of amplitude 1e-6 one step of the stegoton solver
+    equals, to the relative size of the neglected K eps^2 / 2 term, the step of
+    the linear f-wave acoustics app on the same (rho, K) medium."""
+    po, _, q, aux = cases.stegoton(mx=150, amp=1e-6)
+    pl = O.make_params(meqn=2, mwaves=2, maux=2, rp=O.RP_ACOUSTICS_FWAVE, mx=po.mx, dx=po.dx, xlower=po.xlower,
+                       mthbc=(1, 1), char_decomp=0, tfluct_solver=1)
+    _, dqn, cfln = O.step(po, q, aux, 0.05)
+    _, dql, cfll = O.step(pl, q, np.ascontiguousarray(aux[:2]), 0.05)
+    scale = np.abs(dql[:, 3:-3]).max()
+    assert scale > 0
+    assert np.abs(dqn[:, 3:-3] - dql[:, 3:-3]).max() <= 1e-5 * scale
+    assert abs(cfln - cfll) <= 1e-5 * cfll
