@@ -592,8 +592,9 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
 // The line of stage `stage` (descriptor sd) of a single 1-D grid: its
 // buffers resolved through the controller's current roles.
 template <class S>
-__device__ __forceinline__ Line<S> line1d(const StageArgs& a, const StageDesc& sd, int stage) {
-  Ctl* ctl = a.ctl;
+__device__ __forceinline__ Line<S> line1d(const StageArgs& a, const StageDesc& sd, int stage,
+                                          Ctl* ctl_override = nullptr) {
+  Ctl* ctl = ctl_override ? ctl_override : a.ctl;
   Line<S> L;
   L.ctl = ctl;
   L.qin = static_cast<const S*>(a.buf[ctl->role[sd.in]]);
