@@ -76,3 +76,44 @@ def test_params_shapes():
     assert p.meqn == 3 and p.mwaves == 3 and p.ndim == 2 and p.efix == 0
     p = S.ClawParams(rp=S.RP_EULER, mx=10, dx=0.1)
     assert p.shape() == (3, 16) and p.efix == 1
+
+
+def test_header_is_plain_c_and_links(tmp_path):
+    """include/sharpclaw_cuda.h is the boundary a C, C++ or Fortran caller
+    binds: it compiles as C99, every declared function links against the
+    library, and a C program calls it (scl_version, scl_create rejecting bad
+    parameters, scl_format_frame writing a frame: no GPU involved)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    names = declared_functions()
+    src = tmp_path / "caller.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <string.h>\n#include "sharpclaw_cuda.h"\n'
+        "int main(void) {\n"
+        "  void* fns[] = {" + ", ".join("(void*)&" + n for n in names) + "};\n"
+        '  printf("%s %d\\n", scl_version(), (int)(sizeof(fns) / sizeof(fns[0])));\n'
+        "  scl_params p; memset(&p, 0, sizeof(p));\n"
+        "  scl_handle* h = 0;\n"
+        "  int rc = scl_create(&p, &h);\n"
+        '  printf("%d %s\\n", rc, scl_last_error());\n'
+        "  p.ndim = 1; p.mx = 4; p.meqn = 1; p.mwaves = 1; p.mbc = 3; p.dx = 0.25; p.rp = SCL_RP_ADVECTION;\n"
+        "  p.lim_type = 2; p.tfluct_solver = 1; p.mthbc[0] = p.mthbc[1] = 2; p.time_integrator = 3;\n"
+        "  double q[10] = {0, 0, 0, 1, 2, 3, 4, 0, 0, 0};\n"
+        '  int rf = scl_format_frame(&p, q, 0, 0.5, 7, "' + str(tmp_path) + '", 0);\n'
+        '  printf("%d\\n", rf);\n'
+        "  return (rc == SCL_E_INVALID && h == 0 && rf == SCL_OK) ? 0 : 1;\n}\n")
+    libdir = os.path.dirname(C.LIB_PATH)
+    exe = tmp_path / "caller"
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src),
+                        "-o", str(exe), "-L", libdir, "-lsharpclaw_b200", "-Wl,-rpath," + libdir],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    first = r.stdout.splitlines()[0]
+    assert "sm_100a" in first and first.endswith(" %d" % len(names))
+    frame = (tmp_path / "fort.q0007").read_text()
+    assert "0.10000000E+01" in frame and "0.40000000E+01" in frame
