@@ -298,6 +298,40 @@ class Solver:
     def wait_frames(self):
         C.check(C.lib().scl_wait_frames(self._h), "scl_wait_frames")
 
+    def run_frames(self, t0: float, dt_initial: float, cfl_max: float, cfl_desired: float, *,
+                   nout: int = 0, tfinal: float | None = None, tout=None, outdir: str | None = None,
+                   dt_max: float = 1e99, max_steps: int = 50000, dt_variable: int = 1,
+                   write_aux: bool | None = None) -> list:
+        """The output loop of src/main.f90:170-245 on the device-resident
+        state: frame 0 at t0, then for each output time a sharpclaw() call
+        from the previous one (outstyle 1: nout equal intervals to tfinal;
+        outstyle 2: the times in tout), dt_initial carried over as the last
+        dt (main.f90:220), and frame n written from the device without
+        stalling it.  Returns the result dict of every interval; a non-zero
+        info is returned, not raised, as main.f90 reports it and goes on."""
+        if tout is None:
+            if nout < 1 or tfinal is None:
+                raise ValueError("give nout and tfinal (outstyle 1) or tout (outstyle 2)")
+            dtout = (tfinal - t0) / nout
+            times = None
+        else:
+            times = [float(x) for x in tout]
+            nout = len(times)
+        self.write_frame(t0, 0, outdir, write_aux)
+        results = []
+        tend = t0
+        dt = dt_initial
+        for n in range(1, nout + 1):
+            tstart = tend
+            tend = tstart + dtout if times is None else times[n - 1]        # main.f90:180-186
+            res = self.sharpclaw(tstart, tend, dt, cfl_max, cfl_desired, dt_max=dt_max, max_steps=max_steps,
+                                 dt_variable=dt_variable)
+            results.append(res)
+            dt = res["dt_last"]                                              # :220
+            self.write_frame(tend, n, outdir, write_aux)                     # :230-233
+        self.wait_frames()
+        return results
+
     TILE_SHAPES = ((16, 7, 128), (32, 7, 256), (16, 15, 256))  # (cells x, cells y, threads)
 
     def select_tiles(self, variant: int = -1):

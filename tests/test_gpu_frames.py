@@ -52,3 +52,41 @@ def test_write_error_is_reported_on_wait(tmp_path):
         s.write_frame(0.0, 1, dir=str(tmp_path))     # the handle stays usable
         s.wait_frames()
     assert (tmp_path / "fort.q0001").exists()
+
+
+@pytest.mark.parametrize("make,ti,run", [
+    (lambda: cases.acoustics1d(mx=100), 4, dict(dt_initial=0.025, cfl_max=2.9, cfl_desired=2.85, tfinal=2.0, nout=4)),
+    (lambda: cases.radial_dam(n=24), 3, dict(dt_initial=0.01, cfl_max=0.9, cfl_desired=0.8, tfinal=0.3, nout=3)),
+])
+def test_run_frames_matches_the_reference_driver(tmp_path, make, ti, run):
+    """Solver.run_frames follows main.f90's output loop: the frames it writes
+    from the device (FP64_STRICT) are byte-identical to the oracle run through
+    the same loop (sharpclaw per interval, dt_initial = dt_last, out1/out2)."""
+    from oracle import oracle as O
+    po, ps, q, aux = make()
+    ps.time_integrator = ti
+    gdir, odir = tmp_path / "gpu", tmp_path / "oracle"
+    gdir.mkdir()
+    odir.mkdir()
+    with S.Solver(ps, "fp64_strict") as s:
+        s.set_aux(aux) if aux is not None else None
+        s.set_q(q)
+        res = s.run_frames(0.0, run["dt_initial"], run["cfl_max"], run["cfl_desired"], nout=run["nout"],
+                           tfinal=run["tfinal"], outdir=str(gdir))
+    outaux = ps.ndim == 2
+    qo = O.bc(po, q)
+    O.output(po, qo, aux, 0.0, 0, str(odir), outaux)
+    dt, tend = run["dt_initial"], 0.0
+    dtout = run["tfinal"] / run["nout"]
+    for n in range(1, run["nout"] + 1):
+        tstart, tend = tend, tend + dtout
+        qo, ro = O.sharpclaw(po, qo, aux, tstart=tstart, tend=tend, dt_initial=dt, cfl_max=run["cfl_max"],
+                             cfl_desired=run["cfl_desired"], time_integrator=ti)
+        assert res[n - 1]["steps_taken"] == ro.steps_taken and res[n - 1]["info"] == ro.info
+        dt = ro.dt_last
+        O.output(po, qo, aux, tend, n, str(odir), outaux)
+    names = sorted(p.name for p in odir.iterdir())
+    assert names == sorted(p.name for p in gdir.iterdir())
+    assert len(names) == (run["nout"] + 1) * (3 if outaux and ps.maux > 0 else 2)
+    for name in names:
+        assert _read(gdir / name) == _read(odir / name), name
