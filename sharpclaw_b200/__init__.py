@@ -34,7 +34,10 @@ from ._capi import (B4STEP_NONE, B4STEP_SWIRL, FP32, FP64, FP64_STRICT, MIXED,  
                     RP_SWF_BATHY, RP_SWF_KAPPA, RP_SWF_RADIAL, SRC_BATHYMETRY_SW, SRC_NONE, SRC_RADIAL_SW,
                     RUN_AUTO, RUN_GRAPH, RUN_RESIDENT, SharpClawError)
 
-__all__ = ["ClawParams", "Solver", "Batch", "sharpclaw", "SharpClawError", "RP_ADVECTION", "RP_EULER",
+from .datafile import claw_params, read_sharpclaw_data, run_settings  # noqa: E402,F401
+
+__all__ = ["ClawParams", "Solver", "Batch", "sharpclaw", "SharpClawError", "read_sharpclaw_data",
+           "claw_params", "run_settings", "RP_ADVECTION", "RP_EULER",
            "RP_SW2D", "RP_ACOUSTICS1D", "RP_ACOUSTICS2D", "RP_ADVECTION2D", "RP_SW1D", "RP_SWF_BATHY", "RP_SWF_RADIAL", "RP_SWF_KAPPA",
            "RP_ACOUSTICS_CONST", "RP_ACOUSTICS_FWAVE", "RP_TRAFFIC", "RP_ADVECTION_CONS",
            "RP_STEGOTON",
