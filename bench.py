@@ -224,7 +224,9 @@ def shu_osher_params(S, mx, dx):
 
 
 def workloads():
-    """Benchmark workloads (BASELINE configurations).  Each returns the solver
+    """Benchmark workloads c1..c5 (1-D advection 1000 cells, 1-D Euler 2^20,
+    2-D shallow water 4096^2, batched Riemann problems, 2-D acoustics 1024^2
+    with its adjoint).  Each returns the solver
     parameters, initial data, aux, run settings and the bytes one cell-stage
     must move (k_I * meqn * 8 + maux * 8, double state)."""
     import numpy as np
