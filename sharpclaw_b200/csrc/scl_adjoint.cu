@@ -214,12 +214,18 @@ __global__ void k_adj_final(double* l0, const double* l3, const double* l2, cons
     l0[k] = (1.0 / 3.0) * l3[k] + 0.75 * l2[k] + l1[k] + t[k];
 }
 
+// out = a x + b y (SSPRK(10,4) forward states and adjoint combinations)
+__global__ void k_axpby(double* out, double a, const double* x, double b, const double* y, long n) {
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
+    out[k] = a * x[k] + b * y[k];
+}
+
 }  // namespace
 
 namespace scl {
 
 bool adjoint_supported(int rp, int ndim, int cd, int ti, const int* mthbc) {
-  if (rp != SCL_RP_ACOUSTICS2D || ndim != 2 || cd != 0 || ti != 3) return false;
+  if (rp != SCL_RP_ACOUSTICS2D || ndim != 2 || cd != 0 || (ti != 3 && ti != 4)) return false;
   for (int k = 0; k < 4; ++k) if (mthbc[k] != 2) return false;
   return true;
 }
@@ -240,6 +246,10 @@ void launch_adj_combine(int mode, double* a, const double* b, const double* c, l
 void launch_adj_final(double* l0, const double* l3, const double* l2, const double* l1, const double* t, long n,
                       cudaStream_t st) {
   k_adj_final<<<592, 256, 0, st>>>(l0, l3, l2, l1, t, n);
+}
+
+void launch_axpby(double* out, double a, const double* x, double b, const double* y, long n, cudaStream_t st) {
+  k_axpby<<<592, 256, 0, st>>>(out, a, x, b, y, n);
 }
 
 }  // namespace scl

@@ -1102,20 +1102,115 @@ namespace scl {
 void set_last_error(const char* msg) { g_err = msg ? msg : ""; }
 }  // namespace scl
 
+namespace {
+
+// Discrete adjoint of one SSPRK(10,4) step (src/sharpclaw.f90:380-464) with
+// D(q) = dt L(q):
+//   s_{k+1} = s_k + D(s_k)/6 (k = 0..3), s5 = s4 + D(s4)/6,
+//   r1 = 0.04 s0 + 0.36 s5, s5' = 0.6 s0 + 0.4 s5,
+//   s6..s9 from s5' as s1..s4 from s0, q_new = (r1 + 0.6 s9) + 0.1 D(s9).
+// The forward keeps the ten states at which D is evaluated (SK_DQ launches of
+// the handle's stage kernel, so in FP64_STRICT they equal the solver's states
+// bit for bit); the backward applies D'(s)^T in reverse:
+//   l9 = 0.6 l + 0.1 D'(s9)^T l,   l_k = l_{k+1} + D'(s_k)^T l_{k+1} / 6,
+//   l5 = 0.4 l5' + 0.36 l,   acc = 0.6 l5' + 0.04 l,
+//   l0 = acc + l1 + D'(s0)^T l1 / 6.
+int adjoint_ssp104(scl_handle* h, const double* q_dev, const double* lam_in_dev, double* lam_out_dev, double dt) {
+  const scl_params& p = h->p;
+  const long nfield = h->plane * p.meqn;
+  double* S[10];
+  for (int k = 0; k < 10; ++k) S[k] = h->adj + k * nfield;    // s0..s4, s5', s6..s9
+  double* DQ = h->adj + 10 * nfield;
+  double* LIN = h->adj + 11 * nfield;
+  double* LA = h->adj + 12 * nfield;
+  double* LB = h->adj + 13 * nfield;
+  double* T = h->adj + 14 * nfield;
+  double* ACC = h->adj + 15 * nfield;
+  // a controller with identity roles and this dt for the SK_DQ evaluations
+  Ctl c{};
+  c.dt = dt;
+  for (int r = 0; r < NROLES; ++r) c.role[r] = r;
+  Ctl* dctl = h->ctl + 1;
+  CK(cudaMemcpyAsync(dctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream));
+  auto evalD = [&](double* s) {
+    launch_bc<double>(h, s);
+    StageArgs a = make_args(h, 0);
+    a.ctl = dctl;
+    for (int r = 0; r < NROLES; ++r) a.buf[r] = s;
+    a.dq_out = DQ;
+    a.sd = StageDesc{SK_DQ, ROLE_Q, -1, -1, -1};
+    a.stage = 0;
+    h->L.stage(a, h->stream);
+  };
+  const double sixth = 1.0 / 6.0;
+  int rc = upload_field(h, S[0], q_dev, p.meqn, true);
+  if (rc) return rc;
+  for (int k = 0; k < 4; ++k) {                                  // stages 1-4 (:396-419)
+    evalD(S[k]);
+    launch_axpby(S[k + 1], 1.0, S[k], sixth, DQ, nfield, h->stream);
+  }
+  evalD(S[4]);                                                   // stage 5 (:421-429)
+  launch_axpby(T, 1.0, S[4], sixth, DQ, nfield, h->stream);      // s5 (r2)
+  launch_axpby(S[5], 0.6, S[0], 0.4, T, nfield, h->stream);      // s5'
+  for (int k = 5; k < 9; ++k) {                                  // stages 6-9 (:431-455)
+    evalD(S[k]);
+    launch_axpby(S[k + 1], 1.0, S[k], sixth, DQ, nfield, h->stream);
+  }
+  launch_bc<double>(h, S[9]);   // the VJP reads the periodic images of s9 too
+  CK(cudaGetLastError());
+  const size_t w = sizeof(double) * h->ld;
+  CK(cudaMemcpy2DAsync(LIN, sizeof(double) * h->pitch, lam_in_dev, w, w, (size_t)h->rows * p.meqn,
+                       cudaMemcpyDeviceToDevice, h->stream));
+  Phys ph{};
+  ph.u = p.u; ph.gamma = p.gamma; ph.gamma1 = p.gamma - 1.0; ph.grav = p.grav; ph.efix = p.efix;
+  const double* aux = static_cast<const double*>(h->aux);
+  auto vjp = [&](const double* s, const double* lam) {
+    launch_vjp2d(s, lam, aux, T, h->pitch, h->plane, p.mx, p.my, p.dx, p.dy, dt, ph, h->stream);
+  };
+  vjp(S[9], LIN);                                                // stage 10 (:457-462)
+  launch_axpby(LA, 0.6, LIN, 0.1, T, nfield, h->stream);         // l9
+  double *cur = LA, *nxt = LB;
+  for (int k = 8; k >= 5; --k) {                                 // s8, s7, s6, s5'
+    vjp(S[k], cur);
+    launch_axpby(nxt, 1.0, cur, sixth, T, nfield, h->stream);
+    std::swap(cur, nxt);
+  }
+  launch_axpby(ACC, 0.6, cur, 0.04, LIN, nfield, h->stream);     // the s0 share of s5' and r1
+  launch_axpby(nxt, 0.4, cur, 0.36, LIN, nfield, h->stream);     // l5
+  std::swap(cur, nxt);
+  for (int k = 4; k >= 1; --k) {                                 // s4 .. s1
+    vjp(S[k], cur);
+    launch_axpby(nxt, 1.0, cur, sixth, T, nfield, h->stream);
+    std::swap(cur, nxt);
+  }
+  vjp(S[0], cur);
+  launch_axpby(nxt, 1.0, ACC, 1.0, cur, nfield, h->stream);
+  launch_axpby(cur, 1.0, nxt, sixth, T, nfield, h->stream);      // l0
+  CK(cudaGetLastError());
+  CK(cudaMemcpy2DAsync(lam_out_dev, w, cur, sizeof(double) * h->pitch, w, (size_t)h->rows * p.meqn,
+                       cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return SCL_OK;
+}
+
+}  // namespace
+
 extern "C" int scl_adjoint_step(scl_handle* h, const double* q_dev, const double* lam_in_dev,
                                 double* lam_out_dev, double dt) {
   if (!h || !q_dev || !lam_in_dev || !lam_out_dev) return fail(SCL_E_INVALID, "null argument");
   const scl_params& p = h->p;
   if (p.lim_type != 2 || !adjoint_supported(p.rp, p.ndim, p.char_decomp, p.time_integrator, p.mthbc))
     return fail(SCL_E_UNSUPPORTED,
-                "the adjoint covers 2-D acoustics, componentwise WENO5, SSPRK(3,3), periodic bc");
+                "the adjoint covers 2-D acoustics, componentwise WENO5, SSPRK(3,3) or SSPRK(10,4), periodic bc");
   if (h->ssize != sizeof(double)) return fail(SCL_E_UNSUPPORTED, "the adjoint needs double state");
   const long nfield = h->plane * p.meqn;
+  const int nf = p.time_integrator == 4 ? 16 : 5;   // work fields
   if (!h->adj) {
-    if (cudaMalloc(&h->adj, sizeof(double) * nfield * 5) != cudaSuccess)
+    if (cudaMalloc(&h->adj, sizeof(double) * nfield * nf) != cudaSuccess)
       return fail(SCL_E_CUDA, "cudaMalloc adjoint fields");
-    CK(cudaMemsetAsync(h->adj, 0, sizeof(double) * nfield * 5, h->stream));
+    CK(cudaMemsetAsync(h->adj, 0, sizeof(double) * nfield * nf, h->stream));
   }
+  if (p.time_integrator == 4) return adjoint_ssp104(h, q_dev, lam_in_dev, lam_out_dev, dt);
   double* L3 = h->adj;
   double* L2 = L3 + nfield;
   double* L1 = L2 + nfield;

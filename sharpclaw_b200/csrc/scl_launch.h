@@ -64,4 +64,5 @@ void launch_vjp2d(const double* q, const double* lam, const double* aux, double*
 void launch_adj_combine(int mode, double* a, const double* b, const double* c, long n, cudaStream_t st);
 void launch_adj_final(double* l0, const double* l3, const double* l2, const double* l1, const double* t, long n,
                       cudaStream_t st);
+void launch_axpby(double* out, double a, const double* x, double b, const double* y, long n, cudaStream_t st);
 }  // namespace scl

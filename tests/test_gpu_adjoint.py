@@ -1,6 +1,7 @@
-"""The hand-written adjoint (scl_adjoint_step, sharpclaw_b200.adjoint) on a GPU.
+"""The hand-written adjoint (scl_adjoint_step, sharpclaw_b200.adjoint) on a GPU,
+for SSPRK(3,3) and SSPRK(10,4):
 
-* one SSPRK(3,3) step: the forward step of the FP64_STRICT solver equals the
+* one step: the forward step of the FP64_STRICT solver equals the
   FP64 PyTorch restatement (tests/torch_ref.py, same evaluation order) bit for
   bit, and the vector-Jacobian product equals torch.autograd through that
   restatement to 1e-11 relative;
@@ -28,13 +29,13 @@ from sharpclaw_b200 import adjoint as A
 pytestmark = pytest.mark.gpu
 
 
-def _problem(n=24, seed=5, background=0.0):
+def _problem(n=24, seed=5, background=0.0, ti=3):
     po, ps, q, aux = cases.acoustics2d(n=n, seed=seed, background=background)
     # periodic aux: ghost cells are the images of interior cells
     inner = aux[:, 3:-3, 3:-3]
     aux = np.ascontiguousarray(np.pad(inner, ((0, 0), (3, 3), (3, 3)), mode="wrap"))
-    ps.time_integrator = 3
-    dt = 0.4 * ps.dx / float(aux[1].max())
+    ps.time_integrator = ti
+    dt = (0.4 if ti == 3 else 1.2) * ps.dx / float(aux[1].max())
     return ps, q, aux, dt
 
 
@@ -48,20 +49,22 @@ def _cpu(a):
     return torch.from_numpy(np.ascontiguousarray(a))
 
 
-def test_forward_step_matches_torch_restatement():
-    ps, q, aux, dt = _problem()
+@pytest.mark.parametrize("ti", [3, 4])
+def test_forward_step_matches_torch_restatement(ti):
+    ps, q, aux, dt = _problem(ti=ti)
     with S.Solver(ps, "fp64_strict") as s:
         s.set_aux(aux)
         s.set_q(q)
         s.rk_step(dt)
         got = s.get_q()[:, 3:-3, 3:-3]
     Z, c = _cpu(aux[0, 3:-3, 3:-3]), _cpu(aux[1, 3:-3, 3:-3])
-    ref = torch_ref.ssprk3(_cpu(q[:, 3:-3, 3:-3]), Z, c, dt, ps.dx, ps.dy).numpy()
+    ref = torch_ref.rk(ti)(_cpu(q[:, 3:-3, 3:-3]), Z, c, dt, ps.dx, ps.dy).numpy()
     assert np.array_equal(got, ref)
 
 
-def test_adjoint_step_matches_autograd():
-    ps, q, aux, dt = _problem()
+@pytest.mark.parametrize("ti", [3, 4])
+def test_adjoint_step_matches_autograd(ti):
+    ps, q, aux, dt = _problem(ti=ti)
     rng = np.random.default_rng(1)
     lam = np.zeros_like(q)
     lam[:, 3:-3, 3:-3] = rng.standard_normal(lam[:, 3:-3, 3:-3].shape)
@@ -70,21 +73,22 @@ def test_adjoint_step_matches_autograd():
         got = A.adjoint_step(s, _dev(q), _dev(lam), dt).cpu().numpy()[:, 3:-3, 3:-3]
     Z, c = _cpu(aux[0, 3:-3, 3:-3]), _cpu(aux[1, 3:-3, 3:-3])
     x = _cpu(q[:, 3:-3, 3:-3]).requires_grad_(True)
-    y = torch_ref.ssprk3(x, Z, c, dt, ps.dx, ps.dy)
+    y = torch_ref.rk(ti)(x, Z, c, dt, ps.dx, ps.dy)
     (g,) = torch.autograd.grad(y, x, _cpu(lam[:, 3:-3, 3:-3]))
     ref = g.numpy()
     assert np.abs(got - ref).max() <= 1e-11 * np.abs(ref).max()
 
 
-def test_adjoint_dot_product_identity():
-    ps, q, aux, dt = _problem(n=20, seed=8)
+@pytest.mark.parametrize("ti", [3, 4])
+def test_adjoint_dot_product_identity(ti):
+    ps, q, aux, dt = _problem(n=20, seed=8, ti=ti)
     rng = np.random.default_rng(2)
     w = np.zeros_like(q)
     w[:, 3:-3, 3:-3] = rng.standard_normal(w[:, 3:-3, 3:-3].shape)
     v = rng.standard_normal(q[:, 3:-3, 3:-3].shape)
     Z, c = _cpu(aux[0, 3:-3, 3:-3]), _cpu(aux[1, 3:-3, 3:-3])
     x = _cpu(q[:, 3:-3, 3:-3])
-    _, jv = torch.func.jvp(lambda t: torch_ref.ssprk3(t, Z, c, dt, ps.dx, ps.dy), (x,), (_cpu(v),))
+    _, jv = torch.func.jvp(lambda t: torch_ref.rk(ti)(t, Z, c, dt, ps.dx, ps.dy), (x,), (_cpu(v),))
     with S.Solver(ps, "fp64_strict") as s:
         s.set_aux(aux)
         jtw = A.adjoint_step(s, _dev(q), _dev(w), dt).cpu().numpy()[:, 3:-3, 3:-3]
@@ -93,9 +97,10 @@ def test_adjoint_dot_product_identity():
     assert abs(lhs - rhs) <= 1e-11 * max(abs(lhs), 1.0)
 
 
-def test_misfit_gradient_against_finite_differences():
-    ps, q, aux, dt = _problem(n=32, seed=3, background=0.05)
-    nsteps = 60
+@pytest.mark.parametrize("ti", [3, 4])
+def test_misfit_gradient_against_finite_differences(ti):
+    ps, q, aux, dt = _problem(n=32, seed=3, background=0.05, ti=ti)
+    nsteps = 60 if ti == 3 else 20
     rng = np.random.default_rng(4)
     p_obs = _dev(q[0, 3:-3, 3:-3] * 0.9 + 0.01 * rng.standard_normal(q[0, 3:-3, 3:-3].shape))
     with S.Solver(ps, "fp64") as s:

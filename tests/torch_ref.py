@@ -70,3 +70,22 @@ def ssprk3(q, Z, c, dt, dx, dy):
     q1 = q + D(q, Z, c, dt, dx, dy)
     q2 = 0.75 * q + 0.25 * (q1 + D(q1, Z, c, dt, dx, dy))
     return (q + 2.0 * (q2 + D(q2, Z, c, dt, dx, dy))) / 3.0
+
+
+def ssp104(q, Z, c, dt, dx, dy):
+    """ts_ssp104 (sharpclaw.f90:380-464) in the stage kernels' order."""
+    def Dq(x):
+        return D(x, Z, c, dt, dx, dy)
+    s = q
+    for _ in range(4):
+        s = s + (1.0 / 6.0) * Dq(s)
+    r2 = s + (1.0 / 6.0) * Dq(s)
+    r1 = 0.04 * q + 0.36 * r2
+    s = 0.6 * q + 0.4 * r2
+    for _ in range(4):
+        s = s + (1.0 / 6.0) * Dq(s)
+    return (r1 + 0.6 * s) + 0.1 * Dq(s)
+
+
+def rk(ti):
+    return {3: ssprk3, 4: ssp104}[ti]
