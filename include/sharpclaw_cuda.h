@@ -277,8 +277,8 @@ int scl_tiles(scl_handle* h, int* variant, int* tuned, float* trial_ms);
 int scl_rk_step_noalloc(const scl_params* p, double* q_dev, const double* aux_dev, double dt,
                         double* cfl, void* stream);
 
-/* Discrete adjoint of one SSPRK(3,3) step (ts_ssp33, sharpclaw.f90:337-376),
- * or of one SSPRK(10,4) step (ts_ssp104, :380-464) when time_integrator = 4,
+/* Discrete adjoint of one step of the handle's integrator (ts_ssp22, ts_ssp42,
+ * ts_ssp33, ts_ssp104: sharpclaw.f90:247-464)
  * of dq = dt*L(q) (flux2 with componentwise WENO5 and a Riemann solver that
  * is linear in the jumps): given q^n and lam_in = dJ/dq^{n+1}, returns
  * lam_out = dJ/dq^n.  Device arrays in the reference layout (interior cells

@@ -225,7 +225,7 @@ __global__ void k_axpby(double* out, double a, const double* x, double b, const 
 namespace scl {
 
 bool adjoint_supported(int rp, int ndim, int cd, int ti, const int* mthbc) {
-  if (rp != SCL_RP_ACOUSTICS2D || ndim != 2 || cd != 0 || (ti != 3 && ti != 4)) return false;
+  if (rp != SCL_RP_ACOUSTICS2D || ndim != 2 || cd != 0 || ti < 1 || ti > 4) return false;
   for (int k = 0; k < 4; ++k) if (mthbc[k] != 2) return false;
   return true;
 }

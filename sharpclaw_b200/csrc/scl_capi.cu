@@ -1104,22 +1104,28 @@ void set_last_error(const char* msg) { g_err = msg ? msg : ""; }
 
 namespace {
 
-// Discrete adjoint of one SSPRK(10,4) step (src/sharpclaw.f90:380-464) with
-// D(q) = dt L(q):
-//   s_{k+1} = s_k + D(s_k)/6 (k = 0..3), s5 = s4 + D(s4)/6,
-//   r1 = 0.04 s0 + 0.36 s5, s5' = 0.6 s0 + 0.4 s5,
-//   s6..s9 from s5' as s1..s4 from s0, q_new = (r1 + 0.6 s9) + 0.1 D(s9).
-// The forward keeps the ten states at which D is evaluated (SK_DQ launches of
-// the handle's stage kernel, so in FP64_STRICT they equal the solver's states
-// bit for bit); the backward applies D'(s)^T in reverse:
-//   l9 = 0.6 l + 0.1 D'(s9)^T l,   l_k = l_{k+1} + D'(s_k)^T l_{k+1} / 6,
-//   l5 = 0.4 l5' + 0.36 l,   acc = 0.6 l5' + 0.04 l,
-//   l0 = acc + l1 + D'(s0)^T l1 / 6.
-int adjoint_ssp104(scl_handle* h, const double* q_dev, const double* lam_in_dev, double* lam_out_dev, double dt) {
+// Discrete adjoint of one SSPRK(10,4), SSPRK(2,2) or SSPRK(4,2) step
+// (src/sharpclaw.f90:380-464, 247-276, 280-333) with D(q) = dt L(q).  The
+// forward evaluates D at the stage states with SK_DQ launches of the
+// handle's own stage kernel (in FP64_STRICT these are the solver's states
+// bit for bit) and keeps them; the backward applies D'(s)^T in reverse:
+//   SSPRK(10,4): s_{k+1} = s_k + D(s_k)/6 (k = 0..4, s5 = r2),
+//     r1 = 0.04 s0 + 0.36 s5, s5' = 0.6 s0 + 0.4 s5, s6..s9 from s5',
+//     q_new = (r1 + 0.6 s9) + 0.1 D(s9);
+//     l9 = 0.6 l + 0.1 D'(s9)^T l, l_k = l_{k+1} + D'(s_k)^T l_{k+1} / 6,
+//     l5 = 0.4 l5' + 0.36 l, acc = 0.6 l5' + 0.04 l, l0 = acc + l1 + D'(s0)^T l1 / 6;
+//   SSPRK(2,2): s1 = s0 + D(s0), q_new = 0.5 ((s0 + s1) + D(s1));
+//     l1 = 0.5 l + 0.5 D'(s1)^T l, l0 = 0.5 l + l1 + D'(s0)^T l1;
+//   SSPRK(4,2): s_{k+1} = s_k + D(s_k)/3 (k = 0..2),
+//     q_new = (0.25 s0 + 0.75 s3) + 0.25 D(s3);
+//     l3 = 0.75 l + 0.25 D'(s3)^T l, l_k = l_{k+1} + D'(s_k)^T l_{k+1} / 3,
+//     l0 = 0.25 l + l1 + D'(s0)^T l1 / 3.
+int adjoint_rk(scl_handle* h, const double* q_dev, const double* lam_in_dev, double* lam_out_dev, double dt) {
   const scl_params& p = h->p;
+  const int ti = p.time_integrator;
   const long nfield = h->plane * p.meqn;
   double* S[10];
-  for (int k = 0; k < 10; ++k) S[k] = h->adj + k * nfield;    // s0..s4, s5', s6..s9
+  for (int k = 0; k < 10; ++k) S[k] = h->adj + k * nfield;    // stage states
   double* DQ = h->adj + 10 * nfield;
   double* LIN = h->adj + 11 * nfield;
   double* LA = h->adj + 12 * nfield;
@@ -1142,21 +1148,35 @@ int adjoint_ssp104(scl_handle* h, const double* q_dev, const double* lam_in_dev,
     a.stage = 0;
     h->L.stage(a, h->stream);
   };
-  const double sixth = 1.0 / 6.0;
+  const double sixth = 1.0 / 6.0, third = 1.0 / 3.0;
   int rc = upload_field(h, S[0], q_dev, p.meqn, true);
   if (rc) return rc;
-  for (int k = 0; k < 4; ++k) {                                  // stages 1-4 (:396-419)
-    evalD(S[k]);
-    launch_axpby(S[k + 1], 1.0, S[k], sixth, DQ, nfield, h->stream);
+  int last = 0;   // index of the last stage state
+  if (ti == 4) {
+    for (int k = 0; k < 4; ++k) {                                // stages 1-4 (:396-419)
+      evalD(S[k]);
+      launch_axpby(S[k + 1], 1.0, S[k], sixth, DQ, nfield, h->stream);
+    }
+    evalD(S[4]);                                                 // stage 5 (:421-429)
+    launch_axpby(T, 1.0, S[4], sixth, DQ, nfield, h->stream);    // s5 (r2)
+    launch_axpby(S[5], 0.6, S[0], 0.4, T, nfield, h->stream);    // s5'
+    for (int k = 5; k < 9; ++k) {                                // stages 6-9 (:431-455)
+      evalD(S[k]);
+      launch_axpby(S[k + 1], 1.0, S[k], sixth, DQ, nfield, h->stream);
+    }
+    last = 9;
+  } else if (ti == 1) {
+    evalD(S[0]);                                                 // :262-264
+    launch_axpby(S[1], 1.0, S[0], 1.0, DQ, nfield, h->stream);
+    last = 1;
+  } else {
+    for (int k = 0; k < 3; ++k) {                                // :296-322
+      evalD(S[k]);
+      launch_axpby(S[k + 1], 1.0, S[k], third, DQ, nfield, h->stream);
+    }
+    last = 3;
   }
-  evalD(S[4]);                                                   // stage 5 (:421-429)
-  launch_axpby(T, 1.0, S[4], sixth, DQ, nfield, h->stream);      // s5 (r2)
-  launch_axpby(S[5], 0.6, S[0], 0.4, T, nfield, h->stream);      // s5'
-  for (int k = 5; k < 9; ++k) {                                  // stages 6-9 (:431-455)
-    evalD(S[k]);
-    launch_axpby(S[k + 1], 1.0, S[k], sixth, DQ, nfield, h->stream);
-  }
-  launch_bc<double>(h, S[9]);   // the VJP reads the periodic images of s9 too
+  launch_bc<double>(h, S[last]);   // the VJP reads the periodic images of the last state too
   CK(cudaGetLastError());
   const size_t w = sizeof(double) * h->ld;
   CK(cudaMemcpy2DAsync(LIN, sizeof(double) * h->pitch, lam_in_dev, w, w, (size_t)h->rows * p.meqn,
@@ -1167,25 +1187,44 @@ int adjoint_ssp104(scl_handle* h, const double* q_dev, const double* lam_in_dev,
   auto vjp = [&](const double* s, const double* lam) {
     launch_vjp2d(s, lam, aux, T, h->pitch, h->plane, p.mx, p.my, p.dx, p.dy, dt, ph, h->stream);
   };
-  vjp(S[9], LIN);                                                // stage 10 (:457-462)
-  launch_axpby(LA, 0.6, LIN, 0.1, T, nfield, h->stream);         // l9
   double *cur = LA, *nxt = LB;
-  for (int k = 8; k >= 5; --k) {                                 // s8, s7, s6, s5'
-    vjp(S[k], cur);
-    launch_axpby(nxt, 1.0, cur, sixth, T, nfield, h->stream);
+  if (ti == 4) {
+    vjp(S[9], LIN);                                              // stage 10 (:457-462)
+    launch_axpby(cur, 0.6, LIN, 0.1, T, nfield, h->stream);      // l9
+    for (int k = 8; k >= 5; --k) {                               // s8, s7, s6, s5'
+      vjp(S[k], cur);
+      launch_axpby(nxt, 1.0, cur, sixth, T, nfield, h->stream);
+      std::swap(cur, nxt);
+    }
+    launch_axpby(ACC, 0.6, cur, 0.04, LIN, nfield, h->stream);   // the s0 share of s5' and r1
+    launch_axpby(nxt, 0.4, cur, 0.36, LIN, nfield, h->stream);   // l5
     std::swap(cur, nxt);
+    for (int k = 4; k >= 1; --k) {                               // s4 .. s1
+      vjp(S[k], cur);
+      launch_axpby(nxt, 1.0, cur, sixth, T, nfield, h->stream);
+      std::swap(cur, nxt);
+    }
+    vjp(S[0], cur);
+    launch_axpby(nxt, 1.0, ACC, 1.0, cur, nfield, h->stream);
+    launch_axpby(cur, 1.0, nxt, sixth, T, nfield, h->stream);    // l0
+  } else if (ti == 1) {
+    vjp(S[1], LIN);
+    launch_axpby(cur, 0.5, LIN, 0.5, T, nfield, h->stream);      // l1
+    vjp(S[0], cur);
+    launch_axpby(nxt, 0.5, LIN, 1.0, cur, nfield, h->stream);
+    launch_axpby(cur, 1.0, nxt, 1.0, T, nfield, h->stream);      // l0
+  } else {
+    vjp(S[3], LIN);
+    launch_axpby(cur, 0.75, LIN, 0.25, T, nfield, h->stream);    // l3
+    for (int k = 2; k >= 1; --k) {                               // s2, s1
+      vjp(S[k], cur);
+      launch_axpby(nxt, 1.0, cur, third, T, nfield, h->stream);
+      std::swap(cur, nxt);
+    }
+    vjp(S[0], cur);
+    launch_axpby(nxt, 0.25, LIN, 1.0, cur, nfield, h->stream);
+    launch_axpby(cur, 1.0, nxt, third, T, nfield, h->stream);    // l0
   }
-  launch_axpby(ACC, 0.6, cur, 0.04, LIN, nfield, h->stream);     // the s0 share of s5' and r1
-  launch_axpby(nxt, 0.4, cur, 0.36, LIN, nfield, h->stream);     // l5
-  std::swap(cur, nxt);
-  for (int k = 4; k >= 1; --k) {                                 // s4 .. s1
-    vjp(S[k], cur);
-    launch_axpby(nxt, 1.0, cur, sixth, T, nfield, h->stream);
-    std::swap(cur, nxt);
-  }
-  vjp(S[0], cur);
-  launch_axpby(nxt, 1.0, ACC, 1.0, cur, nfield, h->stream);
-  launch_axpby(cur, 1.0, nxt, sixth, T, nfield, h->stream);      // l0
   CK(cudaGetLastError());
   CK(cudaMemcpy2DAsync(lam_out_dev, w, cur, sizeof(double) * h->pitch, w, (size_t)h->rows * p.meqn,
                        cudaMemcpyDeviceToDevice, h->stream));
@@ -1201,16 +1240,16 @@ extern "C" int scl_adjoint_step(scl_handle* h, const double* q_dev, const double
   const scl_params& p = h->p;
   if (p.lim_type != 2 || !adjoint_supported(p.rp, p.ndim, p.char_decomp, p.time_integrator, p.mthbc))
     return fail(SCL_E_UNSUPPORTED,
-                "the adjoint covers 2-D acoustics, componentwise WENO5, SSPRK(3,3) or SSPRK(10,4), periodic bc");
+                "the adjoint covers 2-D acoustics, componentwise WENO5, periodic bc");
   if (h->ssize != sizeof(double)) return fail(SCL_E_UNSUPPORTED, "the adjoint needs double state");
   const long nfield = h->plane * p.meqn;
-  const int nf = p.time_integrator == 4 ? 16 : 5;   // work fields
+  const int nf = p.time_integrator == 3 ? 5 : 16;   // work fields
   if (!h->adj) {
     if (cudaMalloc(&h->adj, sizeof(double) * nfield * nf) != cudaSuccess)
       return fail(SCL_E_CUDA, "cudaMalloc adjoint fields");
     CK(cudaMemsetAsync(h->adj, 0, sizeof(double) * nfield * nf, h->stream));
   }
-  if (p.time_integrator == 4) return adjoint_ssp104(h, q_dev, lam_in_dev, lam_out_dev, dt);
+  if (p.time_integrator != 3) return adjoint_rk(h, q_dev, lam_in_dev, lam_out_dev, dt);
   double* L3 = h->adj;
   double* L2 = L3 + nfield;
   double* L1 = L2 + nfield;

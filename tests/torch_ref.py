@@ -87,5 +87,19 @@ def ssp104(q, Z, c, dt, dx, dy):
     return (r1 + 0.6 * s) + 0.1 * Dq(s)
 
 
+def ssp22(q, Z, c, dt, dx, dy):
+    """ts_ssp22 (sharpclaw.f90:247-276)."""
+    q1 = q + D(q, Z, c, dt, dx, dy)
+    return 0.5 * ((q + q1) + D(q1, Z, c, dt, dx, dy))
+
+
+def ssp42(q, Z, c, dt, dx, dy):
+    """ts_ssp42 (sharpclaw.f90:280-333)."""
+    s = q
+    for _ in range(3):
+        s = s + (1.0 / 3.0) * D(s, Z, c, dt, dx, dy)
+    return (0.25 * q + 0.75 * s) + 0.25 * D(s, Z, c, dt, dx, dy)
+
+
 def rk(ti):
-    return {3: ssprk3, 4: ssp104}[ti]
+    return {1: ssp22, 2: ssp42, 3: ssprk3, 4: ssp104}[ti]
