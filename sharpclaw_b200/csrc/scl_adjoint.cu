@@ -1,5 +1,7 @@
-// scl_adjoint.cu -- discrete adjoint of the SSPRK(3,3) WENO step for the
-// linear-Riemann plugins (2-D variable-coefficient acoustics), periodic bc.
+// scl_adjoint.cu -- discrete adjoint of the WENO step for the linear-Riemann
+// plugins (2-D variable-coefficient acoustics), periodic bc: the VJP of one
+// stage operator (componentwise or characteristic-wise WENO5) and the
+// SSPRK(3,3) combinations (the other integrators' are in scl_capi.cu).
 //
 // The forward operator of one stage is D(q) = dt*L(q) of flux2
 // (src/2d/flux2.f90): per line, WENO5 edge values (reconstruct.f90:77-143),
@@ -77,8 +79,13 @@ constexpr int TA = 128;   // cells per adjoint tile
 
 // VJP of one sweep direction of D over tiles of lines.  q, lam, out: pitched
 // planes (double); periodic wrap is applied to every index, so ghost cells of
-// q are not read.  out (+)= D_dir'(q)^T lam on interior cells.
-template <class P>
+// q are not read.  out (+)= D_dir'(q)^T lam on interior cells.  CD 0:
+// componentwise weno5; CD 2: weno5_char, whose eigenvectors depend on aux
+// only for these plugins (so the projection is linear): the adjoint of an
+// edge value is taken to the fields with evr^T, through weno_side's reverse
+// mode, and back to the component jumps with evl^T, with the eigenvectors of
+// the interface that reconstructs it (c+1 for qr(c), c for ql(c)).
+template <class P, int CD>
 __global__ void __launch_bounds__(TA) k_vjp_sweep(const double* q, const double* lam, const double* aux,
                                                    double* out, long pitch, long plane, int nx, int ny,
                                                    int dir, double dtdx, Phys ph, int accumulate) {
@@ -153,6 +160,59 @@ __global__ void __launch_bounds__(TA) k_vjp_sweep(const double* q, const double*
       nu[e] = acc;
     }
     const int kq = k + 2;    // sq index of cell c
+    if constexpr (CD == 2) {
+      double Gr[M], Gl[M], D[M][4], gD[M][4];
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        Gr[m] = -mu[m][k + 1] + nu[m];
+        Gl[m] = mu[m][k] - nu[m];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) { D[m][j] = sq[m][kq - 1 + j] - sq[m][kq - 2 + j]; gD[m][j] = 0.0; }
+      }
+      // eigenvectors of interface c (cells c-1, c) and c+1 (cells c, c+1)
+      double am1[MA > 0 ? MA : 1], a0[MA > 0 ? MA : 1], ap1[MA > 0 ? MA : 1], z[M];
+#pragma unroll
+      for (int a = 0; a < MA; ++a) { am1[a] = sa[a][kl - 1]; a0[a] = sa[a][kl]; ap1[a] = sa[a][kl + 1]; }
+#pragma unroll
+      for (int m = 0; m < M; ++m) z[m] = 0.0;
+      double evlL[M][M], evrL[M][M], evlR[M][M], evrR[M][M];
+      P::template evec<double>(ph, dir, z, z, am1, a0, evlL, evrL);
+      P::template evec<double>(ph, dir, z, z, a0, ap1, evlR, evrR);
+#pragma unroll
+      for (int pf = 0; pf < M; ++pf) {
+        double g1 = 0.0, g2 = 0.0, h1[4], h2[4], gh1[4] = {0.0, 0.0, 0.0, 0.0}, gh2[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int m = 0; m < M; ++m) { g1 += evrR[m][pf] * Gr[m]; g2 += evrL[m][pf] * Gl[m]; }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+          for (int m = 0; m < M; ++m) { s1 = s1 + evlR[pf][m] * D[m][j]; s2 = s2 + evlL[pf][m] * D[m][j]; }
+          h1[j] = s1;
+          h2[j] = s2;
+        }
+        weno_side_vjp(h1[0], h1[1], h1[2], h1[3], 1.0, g1, gh1[0], gh1[1], gh1[2], gh1[3]);
+        weno_side_vjp(h2[3], h2[2], h2[1], h2[0], -1.0, g2, gh2[3], gh2[2], gh2[1], gh2[0]);
+#pragma unroll
+        for (int m = 0; m < M; ++m)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) gD[m][j] += evlR[pf][m] * gh1[j] + evlL[pf][m] * gh2[j];
+      }
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        double v[5];
+        v[0] = -Gl[m] / 12.0;
+        v[1] = -Gr[m] / 12.0 + 7.0 * Gl[m] / 12.0;
+        v[2] = 7.0 * Gr[m] / 12.0 + 7.0 * Gl[m] / 12.0;
+        v[3] = 7.0 * Gr[m] / 12.0 - Gl[m] / 12.0;
+        v[4] = -Gr[m] / 12.0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) { v[j + 1] += gD[m][j]; v[j] -= gD[m][j]; }
+#pragma unroll
+        for (int j = 0; j < 5; ++j) vc[m][j][k] = v[j];
+      }
+      continue;
+    }
 #pragma unroll
     for (int m = 0; m < M; ++m) {
       const double Gr = -mu[m][k + 1] + nu[m];   // interface c+1 is mu index k+1
@@ -225,18 +285,23 @@ __global__ void k_axpby(double* out, double a, const double* x, double b, const 
 namespace scl {
 
 bool adjoint_supported(int rp, int ndim, int cd, int ti, const int* mthbc) {
-  if (rp != SCL_RP_ACOUSTICS2D || ndim != 2 || cd != 0 || ti < 1 || ti > 4) return false;
+  if (rp != SCL_RP_ACOUSTICS2D || ndim != 2 || (cd != 0 && cd != 2) || ti < 1 || ti > 4) return false;
   for (int k = 0; k < 4; ++k) if (mthbc[k] != 2) return false;
   return true;
 }
 
 // out = D'(q)^T lam summed over both sweeps (q, lam, out pitched planes)
 void launch_vjp2d(const double* q, const double* lam, const double* aux, double* out, long pitch, long plane,
-                  int nx, int ny, double dx, double dy, double dt, const Phys& ph, cudaStream_t st) {
+                  int nx, int ny, double dx, double dy, double dt, const Phys& ph, int cd, cudaStream_t st) {
   using P = PAcoustics<3>;
   dim3 gx((nx + TA - 1) / TA, ny), gy((ny + TA - 1) / TA, nx);
-  k_vjp_sweep<P><<<gx, TA, 0, st>>>(q, lam, aux, out, pitch, plane, nx, ny, 1, dt / dx, ph, 0);
-  k_vjp_sweep<P><<<gy, TA, 0, st>>>(q, lam, aux, out, pitch, plane, nx, ny, 2, dt / dy, ph, 1);
+  if (cd == 2) {
+    k_vjp_sweep<P, 2><<<gx, TA, 0, st>>>(q, lam, aux, out, pitch, plane, nx, ny, 1, dt / dx, ph, 0);
+    k_vjp_sweep<P, 2><<<gy, TA, 0, st>>>(q, lam, aux, out, pitch, plane, nx, ny, 2, dt / dy, ph, 1);
+  } else {
+    k_vjp_sweep<P, 0><<<gx, TA, 0, st>>>(q, lam, aux, out, pitch, plane, nx, ny, 1, dt / dx, ph, 0);
+    k_vjp_sweep<P, 0><<<gy, TA, 0, st>>>(q, lam, aux, out, pitch, plane, nx, ny, 2, dt / dy, ph, 1);
+  }
 }
 
 void launch_adj_combine(int mode, double* a, const double* b, const double* c, long n, cudaStream_t st) {

@@ -1,5 +1,6 @@
 """The hand-written adjoint (scl_adjoint_step, sharpclaw_b200.adjoint) on a GPU,
-for each integrator (SSPRK(2,2), (4,2), (3,3), (10,4)):
+for each integrator (SSPRK(2,2), (4,2), (3,3), (10,4)) with componentwise
+WENO5 and, for SSPRK(3,3) and (10,4), characteristic-wise WENO5:
 
 * one step: the forward step of the FP64_STRICT solver equals the
   FP64 PyTorch restatement (tests/torch_ref.py, same evaluation order) bit for
@@ -29,8 +30,8 @@ from sharpclaw_b200 import adjoint as A
 pytestmark = pytest.mark.gpu
 
 
-def _problem(n=24, seed=5, background=0.0, ti=3):
-    po, ps, q, aux = cases.acoustics2d(n=n, seed=seed, background=background)
+def _problem(n=24, seed=5, background=0.0, ti=3, cd=0):
+    po, ps, q, aux = cases.acoustics2d(n=n, seed=seed, background=background, char_decomp=cd)
     # periodic aux: ghost cells are the images of interior cells
     inner = aux[:, 3:-3, 3:-3]
     aux = np.ascontiguousarray(np.pad(inner, ((0, 0), (3, 3), (3, 3)), mode="wrap"))
@@ -49,22 +50,22 @@ def _cpu(a):
     return torch.from_numpy(np.ascontiguousarray(a))
 
 
-@pytest.mark.parametrize("ti", [1, 2, 3, 4])
-def test_forward_step_matches_torch_restatement(ti):
-    ps, q, aux, dt = _problem(ti=ti)
+@pytest.mark.parametrize("ti,cd", [(1, 0), (2, 0), (3, 0), (4, 0), (3, 2), (4, 2)])
+def test_forward_step_matches_torch_restatement(ti, cd):
+    ps, q, aux, dt = _problem(ti=ti, cd=cd)
     with S.Solver(ps, "fp64_strict") as s:
         s.set_aux(aux)
         s.set_q(q)
         s.rk_step(dt)
         got = s.get_q()[:, 3:-3, 3:-3]
     Z, c = _cpu(aux[0, 3:-3, 3:-3]), _cpu(aux[1, 3:-3, 3:-3])
-    ref = torch_ref.rk(ti)(_cpu(q[:, 3:-3, 3:-3]), Z, c, dt, ps.dx, ps.dy).numpy()
+    ref = torch_ref.rk(ti)(_cpu(q[:, 3:-3, 3:-3]), Z, c, dt, ps.dx, ps.dy, cd).numpy()
     assert np.array_equal(got, ref)
 
 
-@pytest.mark.parametrize("ti", [1, 2, 3, 4])
-def test_adjoint_step_matches_autograd(ti):
-    ps, q, aux, dt = _problem(ti=ti)
+@pytest.mark.parametrize("ti,cd", [(1, 0), (2, 0), (3, 0), (4, 0), (3, 2), (4, 2)])
+def test_adjoint_step_matches_autograd(ti, cd):
+    ps, q, aux, dt = _problem(ti=ti, cd=cd)
     rng = np.random.default_rng(1)
     lam = np.zeros_like(q)
     lam[:, 3:-3, 3:-3] = rng.standard_normal(lam[:, 3:-3, 3:-3].shape)
@@ -73,22 +74,22 @@ def test_adjoint_step_matches_autograd(ti):
         got = A.adjoint_step(s, _dev(q), _dev(lam), dt).cpu().numpy()[:, 3:-3, 3:-3]
     Z, c = _cpu(aux[0, 3:-3, 3:-3]), _cpu(aux[1, 3:-3, 3:-3])
     x = _cpu(q[:, 3:-3, 3:-3]).requires_grad_(True)
-    y = torch_ref.rk(ti)(x, Z, c, dt, ps.dx, ps.dy)
+    y = torch_ref.rk(ti)(x, Z, c, dt, ps.dx, ps.dy, cd)
     (g,) = torch.autograd.grad(y, x, _cpu(lam[:, 3:-3, 3:-3]))
     ref = g.numpy()
     assert np.abs(got - ref).max() <= 1e-11 * np.abs(ref).max()
 
 
-@pytest.mark.parametrize("ti", [1, 2, 3, 4])
-def test_adjoint_dot_product_identity(ti):
-    ps, q, aux, dt = _problem(n=20, seed=8, ti=ti)
+@pytest.mark.parametrize("ti,cd", [(1, 0), (2, 0), (3, 0), (4, 0), (3, 2), (4, 2)])
+def test_adjoint_dot_product_identity(ti, cd):
+    ps, q, aux, dt = _problem(n=20, seed=8, ti=ti, cd=cd)
     rng = np.random.default_rng(2)
     w = np.zeros_like(q)
     w[:, 3:-3, 3:-3] = rng.standard_normal(w[:, 3:-3, 3:-3].shape)
     v = rng.standard_normal(q[:, 3:-3, 3:-3].shape)
     Z, c = _cpu(aux[0, 3:-3, 3:-3]), _cpu(aux[1, 3:-3, 3:-3])
     x = _cpu(q[:, 3:-3, 3:-3])
-    _, jv = torch.func.jvp(lambda t: torch_ref.rk(ti)(t, Z, c, dt, ps.dx, ps.dy), (x,), (_cpu(v),))
+    _, jv = torch.func.jvp(lambda t: torch_ref.rk(ti)(t, Z, c, dt, ps.dx, ps.dy, cd), (x,), (_cpu(v),))
     with S.Solver(ps, "fp64_strict") as s:
         s.set_aux(aux)
         jtw = A.adjoint_step(s, _dev(q), _dev(w), dt).cpu().numpy()[:, 3:-3, 3:-3]
@@ -97,9 +98,9 @@ def test_adjoint_dot_product_identity(ti):
     assert abs(lhs - rhs) <= 1e-11 * max(abs(lhs), 1.0)
 
 
-@pytest.mark.parametrize("ti", [1, 2, 3, 4])
-def test_misfit_gradient_against_finite_differences(ti):
-    ps, q, aux, dt = _problem(n=32, seed=3, background=0.05, ti=ti)
+@pytest.mark.parametrize("ti,cd", [(1, 0), (2, 0), (3, 0), (4, 0), (3, 2), (4, 2)])
+def test_misfit_gradient_against_finite_differences(ti, cd):
+    ps, q, aux, dt = _problem(n=32, seed=3, background=0.05, ti=ti, cd=cd)
     nsteps = {1: 60, 2: 30, 3: 60, 4: 20}[ti]
     rng = np.random.default_rng(4)
     p_obs = _dev(q[0, 3:-3, 3:-3] * 0.9 + 0.01 * rng.standard_normal(q[0, 3:-3, 3:-3].shape))

@@ -32,12 +32,15 @@ def weno_side(dm2, dm1, d0, dp1, im):
     return ((s1 * (t2 - t1)) + ((0.5 * s3 - 0.25) * (t3 - t2))) / 3.0
 
 
-def sweep(q, Z, c, dtdx, axis, mu):
+def sweep(q, Z, c, dtdx, axis, mu, cd=0):
     r = lambda a, s: torch.roll(a, s, dims=axis)   # r(a, 1)[i] = a[i-1]
-    d = q - r(q, 1)
-    D0, D1, D2, D3 = r(d, 1), d, r(d, -1), r(d, -2)
-    qr = weno_side(D0, D1, D2, D3, 1.0) + (-r(q, 1) + 7.0 * (q + r(q, -1)) - r(q, -2)) / 12.0
-    ql = weno_side(D3, D2, D1, D0, -1.0) + (-r(q, 2) + 7.0 * (r(q, 1) + q) - r(q, -1)) / 12.0
+    if cd == 2:
+        qr, ql = char_edges(q, Z, axis, mu)
+    else:
+        d = q - r(q, 1)
+        D0, D1, D2, D3 = r(d, 1), d, r(d, -1), r(d, -2)
+        qr = weno_side(D0, D1, D2, D3, 1.0) + (-r(q, 1) + 7.0 * (q + r(q, -1)) - r(q, -2)) / 12.0
+        ql = weno_side(D3, D2, D1, D0, -1.0) + (-r(q, 2) + 7.0 * (r(q, 1) + q) - r(q, -1)) / 12.0
     dl = ql - r(qr, 1)                      # interface i: ql(i) - qr(i-1)
     zi, zim = Z, r(Z, 1)
     a1 = (-dl[0] + zi * dl[mu]) / (zim + zi)
@@ -62,20 +65,54 @@ def sweep(q, Z, c, dtdx, axis, mu):
     return -dtdx * (apdq + adq + amdq_next)
 
 
-def D(q, Z, c, dt, dx, dy):
-    return sweep(q, Z, c, dt / dx, -1, 1) + sweep(q, Z, c, dt / dy, -2, 2)
+def char_edges(q, Z, axis, mu):
+    """weno5_char (reconstruct.f90:146-241) with the acoustics eigenvectors of
+    each interface (evec.f90:196-206 with the tangential velocity as a third,
+    zero-speed field): returns qr(c) and ql(c) of every cell, accumulated in
+    the kernel's order (full 3x3 sums, zero entries included)."""
+    r = lambda a, s: torch.roll(a, s, dims=axis)
+    mv = 3 - mu
+    zim, zi = r(Z, 1), Z                    # interface i between cells i-1 and i
+    z = 1.0 / (zim + zi)
+    zero, one = torch.zeros_like(Z), torch.ones_like(Z)
+    evl = [[zero] * 3 for _ in range(3)]
+    evr = [[zero] * 3 for _ in range(3)]
+    evr[0][0], evr[0][1], evr[mu][0], evr[mu][1], evr[mv][2] = -zim, zi, one, one, one
+    evl[0][0], evl[0][mu], evl[1][0], evl[1][mu], evl[2][mv] = -1.0 * z, zi * z, 1.0 * z, zim * z, one
+    d = q - r(q, 1)                          # d(j) = q(j) - q(j-1)
+    dk = [r(d, 2 - k) for k in range(5)]     # at interface i: d(i-2+k)
+    cen = ((-r(q, 2)) + 7.0 * (r(q, 1) + q)) - r(q, -1)
+    QR = [cen[m] / 12.0 for m in range(3)]   # qr(i-1)
+    QL = [cen[m] / 12.0 for m in range(3)]   # ql(i)
+    for p in range(3):
+        h = []
+        for k in range(5):
+            s = torch.zeros_like(Z)
+            for m in range(3):
+                s = s + evl[p][m] * dk[k][m]
+            h.append(s)
+        u1 = weno_side(h[0], h[1], h[2], h[3], 1.0)
+        u2 = weno_side(h[4], h[3], h[2], h[1], -1.0)
+        for m in range(3):
+            QR[m] = QR[m] + evr[m][p] * u1
+            QL[m] = QL[m] + evr[m][p] * u2
+    return r(torch.stack(QR), -1), torch.stack(QL)
 
 
-def ssprk3(q, Z, c, dt, dx, dy):
-    q1 = q + D(q, Z, c, dt, dx, dy)
-    q2 = 0.75 * q + 0.25 * (q1 + D(q1, Z, c, dt, dx, dy))
-    return (q + 2.0 * (q2 + D(q2, Z, c, dt, dx, dy))) / 3.0
+def D(q, Z, c, dt, dx, dy, cd=0):
+    return sweep(q, Z, c, dt / dx, -1, 1, cd) + sweep(q, Z, c, dt / dy, -2, 2, cd)
 
 
-def ssp104(q, Z, c, dt, dx, dy):
+def ssprk3(q, Z, c, dt, dx, dy, cd=0):
+    q1 = q + D(q, Z, c, dt, dx, dy, cd)
+    q2 = 0.75 * q + 0.25 * (q1 + D(q1, Z, c, dt, dx, dy, cd))
+    return (q + 2.0 * (q2 + D(q2, Z, c, dt, dx, dy, cd))) / 3.0
+
+
+def ssp104(q, Z, c, dt, dx, dy, cd=0):
     """ts_ssp104 (sharpclaw.f90:380-464) in the stage kernels' order."""
     def Dq(x):
-        return D(x, Z, c, dt, dx, dy)
+        return D(x, Z, c, dt, dx, dy, cd)
     s = q
     for _ in range(4):
         s = s + (1.0 / 6.0) * Dq(s)
@@ -87,18 +124,18 @@ def ssp104(q, Z, c, dt, dx, dy):
     return (r1 + 0.6 * s) + 0.1 * Dq(s)
 
 
-def ssp22(q, Z, c, dt, dx, dy):
+def ssp22(q, Z, c, dt, dx, dy, cd=0):
     """ts_ssp22 (sharpclaw.f90:247-276)."""
-    q1 = q + D(q, Z, c, dt, dx, dy)
-    return 0.5 * ((q + q1) + D(q1, Z, c, dt, dx, dy))
+    q1 = q + D(q, Z, c, dt, dx, dy, cd)
+    return 0.5 * ((q + q1) + D(q1, Z, c, dt, dx, dy, cd))
 
 
-def ssp42(q, Z, c, dt, dx, dy):
+def ssp42(q, Z, c, dt, dx, dy, cd=0):
     """ts_ssp42 (sharpclaw.f90:280-333)."""
     s = q
     for _ in range(3):
-        s = s + (1.0 / 3.0) * D(s, Z, c, dt, dx, dy)
-    return (0.25 * q + 0.75 * s) + 0.25 * D(s, Z, c, dt, dx, dy)
+        s = s + (1.0 / 3.0) * D(s, Z, c, dt, dx, dy, cd)
+    return (0.25 * q + 0.75 * s) + 0.25 * D(s, Z, c, dt, dx, dy, cd)
 
 
 def rk(ti):
