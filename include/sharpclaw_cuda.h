@@ -279,11 +279,13 @@ int scl_rk_step_noalloc(const scl_params* p, double* q_dev, const double* aux_de
 
 /* Discrete adjoint of one step of the handle's integrator (ts_ssp22, ts_ssp42,
  * ts_ssp33, ts_ssp104: sharpclaw.f90:247-464)
- * of dq = dt*L(q) (flux2 with componentwise WENO5 and a Riemann solver that
- * is linear in the jumps): given q^n and lam_in = dJ/dq^{n+1}, returns
- * lam_out = dJ/dq^n.  Device arrays in the reference layout (interior cells
- * are meaningful).  Built for the 2-D acoustics plugin with periodic bc and
- * double state; computed in FP64.  No reference counterpart (the reference
+ * of dq = dt*L(q) (flux1/flux2 with componentwise or characteristic-wise
+ * WENO5 and a Riemann solver that is linear in the jumps): given q^n and
+ * lam_in = dJ/dq^{n+1}, returns lam_out = dJ/dq^n.  Device arrays in the
+ * reference layout (interior cells are meaningful).  Built for the 2-D
+ * acoustics plugin and the 1-D interface acoustics plugin
+ * (apps/acoustics/1d/interface), with periodic bc and double state;
+ * computed in FP64.  No reference counterpart (the reference
  * has no adjoint). */
 int scl_adjoint_step(scl_handle* h, const double* q_dev, const double* lam_in_dev, double* lam_out_dev,
                      double dt);

@@ -1,9 +1,9 @@
 """Adjoint of the WENO / Riemann / SSP-RK step behind torch.autograd.
 
-``WaveMisfit`` maps the initial pressure p0 of a 2-D variable-coefficient
-acoustics problem (q = (p, u, v), u = v = 0 initially, periodic) to the
-misfit J = 1/2 ||p(T) - p_obs||^2 after `nsteps` fixed-dt SSPRK(3,3) steps of
-the device solver.  Its backward pass is the hand-written discrete adjoint of
+``WaveMisfit`` maps the initial pressure p0 of a variable-coefficient
+acoustics problem (2-D q = (p, u, v) or 1-D q = (p, u), velocities zero
+initially, periodic) to the misfit J = 1/2 ||p(T) - p_obs||^2 after `nsteps`
+fixed-dt steps of the device solver's SSP Runge-Kutta integrator.  Its backward pass is the hand-written discrete adjoint of
 the library (``scl_adjoint_step``, FP64): the forward keeps a checkpoint of q
 every `checkpoint_every` steps; the backward recomputes each segment from
 its checkpoint and runs the adjoint steps through it in reverse, so memory is
@@ -17,6 +17,11 @@ import torch
 
 from . import _capi as C
 from . import ClawParams, Solver
+
+
+def _interior(P: ClawParams, m: int):
+    """Index of component m's interior cells (three ghost cells per side)."""
+    return (m,) + (slice(3, -3),) * P.ndim
 
 
 def _advance(solver: Solver, q: torch.Tensor, dt: float, nsteps: int) -> None:
@@ -45,7 +50,7 @@ class WaveMisfit(torch.autograd.Function):
     def forward(ctx, p0, solver: Solver, dt: float, nsteps: int, p_obs, checkpoint_every: int = 20):
         P: ClawParams = solver.params
         q = torch.zeros(P.shape(), dtype=torch.float64, device=p0.device)
-        q[0, 3:-3, 3:-3] = p0.detach().to(torch.float64)
+        q[_interior(P, 0)] = p0.detach().to(torch.float64)
         ckpts, lens = [], []
         done = 0
         while done < nsteps:
@@ -54,7 +59,7 @@ class WaveMisfit(torch.autograd.Function):
             lens.append(k)
             _advance(solver, q, dt, k)
             done += k
-        r = q[0, 3:-3, 3:-3] - p_obs
+        r = q[_interior(P, 0)] - p_obs
         ctx.solver, ctx.dt, ctx.lens = solver, dt, lens
         ctx.save_for_backward(r, *ckpts)
         return 0.5 * (r * r).sum()
@@ -64,7 +69,7 @@ class WaveMisfit(torch.autograd.Function):
         r, *ckpts = ctx.saved_tensors
         solver, dt = ctx.solver, ctx.dt
         lam = torch.zeros_like(ckpts[0])
-        lam[0, 3:-3, 3:-3] = gJ * r
+        lam[_interior(solver.params, 0)] = gJ * r
         for q0, k in zip(reversed(ckpts), reversed(ctx.lens)):
             states = [q0.clone()]
             for _ in range(k - 1):                    # recompute the segment
@@ -73,7 +78,7 @@ class WaveMisfit(torch.autograd.Function):
                 states.append(q)
             for q in reversed(states):
                 lam = adjoint_step(solver, q, lam, dt)
-        return lam[0, 3:-3, 3:-3].clone(), None, None, None, None, None
+        return lam[_interior(solver.params, 0)].clone(), None, None, None, None, None
 
 
 def wave_misfit(p0, solver: Solver, dt: float, nsteps: int, p_obs, checkpoint_every: int = 20):

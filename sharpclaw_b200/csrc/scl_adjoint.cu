@@ -285,14 +285,25 @@ __global__ void k_axpby(double* out, double a, const double* x, double b, const 
 namespace scl {
 
 bool adjoint_supported(int rp, int ndim, int cd, int ti, const int* mthbc) {
-  if (rp != SCL_RP_ACOUSTICS2D || ndim != 2 || (cd != 0 && cd != 2) || ti < 1 || ti > 4) return false;
+  if ((cd != 0 && cd != 2) || ti < 1 || ti > 4) return false;
+  if (rp == SCL_RP_ACOUSTICS1D && ndim == 1) return mthbc[0] == 2 && mthbc[1] == 2;
+  if (rp != SCL_RP_ACOUSTICS2D || ndim != 2) return false;
   for (int k = 0; k < 4; ++k) if (mthbc[k] != 2) return false;
   return true;
 }
 
 // out = D'(q)^T lam summed over both sweeps (q, lam, out pitched planes)
 void launch_vjp2d(const double* q, const double* lam, const double* aux, double* out, long pitch, long plane,
-                  int nx, int ny, double dx, double dy, double dt, const Phys& ph, int cd, cudaStream_t st) {
+                  int nx, int ny, double dx, double dy, double dt, const Phys& ph, int cd, cudaStream_t st,
+                  int ndim) {
+  if (ndim == 1) {
+    // one line (apps/acoustics/1d/interface): row offset 0, so pitch 0
+    using P1 = PAcoustics<2>;
+    dim3 g((nx + TA - 1) / TA, 1);
+    if (cd == 2) k_vjp_sweep<P1, 2><<<g, TA, 0, st>>>(q, lam, aux, out, 0, plane, nx, 1, 1, dt / dx, ph, 0);
+    else k_vjp_sweep<P1, 0><<<g, TA, 0, st>>>(q, lam, aux, out, 0, plane, nx, 1, 1, dt / dx, ph, 0);
+    return;
+  }
   using P = PAcoustics<3>;
   dim3 gx((nx + TA - 1) / TA, ny), gy((ny + TA - 1) / TA, nx);
   if (cd == 2) {

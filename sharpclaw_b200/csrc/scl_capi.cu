@@ -1185,7 +1185,7 @@ int adjoint_rk(scl_handle* h, const double* q_dev, const double* lam_in_dev, dou
   ph.u = p.u; ph.gamma = p.gamma; ph.gamma1 = p.gamma - 1.0; ph.grav = p.grav; ph.efix = p.efix;
   const double* aux = static_cast<const double*>(h->aux);
   auto vjp = [&](const double* s, const double* lam) {
-    launch_vjp2d(s, lam, aux, T, h->pitch, h->plane, p.mx, p.my, p.dx, p.dy, dt, ph, p.char_decomp, h->stream);
+    launch_vjp2d(s, lam, aux, T, h->pitch, h->plane, p.mx, p.my, p.dx, p.dy, dt, ph, p.char_decomp, h->stream, p.ndim);
   };
   double *cur = LA, *nxt = LB;
   if (ti == 4) {
@@ -1240,7 +1240,7 @@ extern "C" int scl_adjoint_step(scl_handle* h, const double* q_dev, const double
   const scl_params& p = h->p;
   if (p.lim_type != 2 || !adjoint_supported(p.rp, p.ndim, p.char_decomp, p.time_integrator, p.mthbc))
     return fail(SCL_E_UNSUPPORTED,
-                "the adjoint covers 2-D acoustics, WENO5 componentwise or char-wise, periodic bc");
+                "the adjoint covers the acoustics plugins (1-D interface, 2-D), WENO5 componentwise or char-wise, periodic bc");
   if (h->ssize != sizeof(double)) return fail(SCL_E_UNSUPPORTED, "the adjoint needs double state");
   const long nfield = h->plane * p.meqn;
   const int nf = p.time_integrator == 3 ? 5 : 16;   // work fields
@@ -1278,11 +1278,11 @@ extern "C" int scl_adjoint_step(scl_handle* h, const double* q_dev, const double
   Phys ph{};
   ph.u = p.u; ph.gamma = p.gamma; ph.gamma1 = p.gamma - 1.0; ph.grav = p.grav; ph.efix = p.efix;
   const double* aux = static_cast<const double*>(h->aux);
-  launch_vjp2d(B, L3, aux, T, h->pitch, h->plane, p.mx, p.my, p.dx, p.dy, dt, ph, p.char_decomp, h->stream);
+  launch_vjp2d(B, L3, aux, T, h->pitch, h->plane, p.mx, p.my, p.dx, p.dy, dt, ph, p.char_decomp, h->stream, p.ndim);
   launch_adj_combine(0, L2, L3, T, nfield, h->stream);          // l2 = 2/3 (l3 + D'(q2) l3)
-  launch_vjp2d(A, L2, aux, T, h->pitch, h->plane, p.mx, p.my, p.dx, p.dy, dt, ph, p.char_decomp, h->stream);
+  launch_vjp2d(A, L2, aux, T, h->pitch, h->plane, p.mx, p.my, p.dx, p.dy, dt, ph, p.char_decomp, h->stream, p.ndim);
   launch_adj_combine(1, L1, L2, T, nfield, h->stream);          // l1 = 1/4 (l2 + D'(q1) l2)
-  launch_vjp2d(Q, L1, aux, T, h->pitch, h->plane, p.mx, p.my, p.dx, p.dy, dt, ph, p.char_decomp, h->stream);
+  launch_vjp2d(Q, L1, aux, T, h->pitch, h->plane, p.mx, p.my, p.dx, p.dy, dt, ph, p.char_decomp, h->stream, p.ndim);
   launch_adj_final(L0, L3, L2, L1, T, nfield, h->stream);       // l0 = l3/3 + 3/4 l2 + l1 + D'(q0) l1
   CK(cudaGetLastError());
   CK(cudaMemcpy2DAsync(lam_out_dev, w, L0, sizeof(double) * h->pitch, w, (size_t)h->rows * p.meqn,

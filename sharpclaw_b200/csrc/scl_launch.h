@@ -60,7 +60,8 @@ namespace scl {
 // Discrete adjoint pieces (FP64, 2-D acoustics, periodic bc).
 bool adjoint_supported(int rp, int ndim, int cd, int ti, const int* mthbc);
 void launch_vjp2d(const double* q, const double* lam, const double* aux, double* out, long pitch, long plane,
-                  int nx, int ny, double dx, double dy, double dt, const Phys& ph, int cd, cudaStream_t st);
+                  int nx, int ny, double dx, double dy, double dt, const Phys& ph, int cd, cudaStream_t st,
+                  int ndim = 2);
 void launch_adj_combine(int mode, double* a, const double* b, const double* c, long n, cudaStream_t st);
 void launch_adj_final(double* l0, const double* l3, const double* l2, const double* l1, const double* t, long n,
                       cudaStream_t st);

@@ -1,6 +1,8 @@
 """The hand-written adjoint (scl_adjoint_step, sharpclaw_b200.adjoint) on a GPU,
 for each integrator (SSPRK(2,2), (4,2), (3,3), (10,4)) with componentwise
-WENO5 and, for SSPRK(3,3) and (10,4), characteristic-wise WENO5:
+WENO5 and, for SSPRK(3,3) and (10,4), characteristic-wise WENO5, on 2-D
+variable-coefficient acoustics and on the 1-D interface app
+(apps/acoustics/1d/interface, periodic):
 
 * one step: the forward step of the FP64_STRICT solver equals the
   FP64 PyTorch restatement (tests/torch_ref.py, same evaluation order) bit for
@@ -117,6 +119,96 @@ def test_misfit_gradient_against_finite_differences(ti, cd):
             h = 1e-7
             Jp = A.wave_misfit(p0.detach() + h * d, s, dt, nsteps, p_obs)
             Jm = A.wave_misfit(p0.detach() - h * d, s, dt, nsteps, p_obs)
+            fd = float((Jp - Jm) / (2 * h))
+            ad = float((g * d).sum())
+            assert abs(fd - ad) <= 1e-4 * abs(fd), (k, fd, ad)
+
+
+# ---- 1-D: the acoustics interface app (apps/acoustics/1d/interface), periodic ----
+
+def _problem1d(mx=120, ti=3, cd=0, background=0.0):
+    po, ps, q, aux = cases.acoustics1d(mx=mx, char_decomp=cd, mthbc=(2, 2))
+    aux = np.ascontiguousarray(np.pad(aux[:, 3:-3], ((0, 0), (3, 3)), mode="wrap"))
+    # a smooth periodic background keeps every cell difference well above
+    # rounding, out of the epsilon regime of the smoothness indicators
+    q = q.copy()
+    x = ps.xlower + (np.arange(mx) + 0.5) * ps.dx
+    q[0, 3:-3] += background * np.cos(2 * np.pi * (x - ps.xlower) / (mx * ps.dx) + 0.3)
+    ps.time_integrator = ti
+    dt = {1: 0.4, 2: 0.8, 3: 0.4, 4: 1.2}[ti] * ps.dx / float(aux[1].max())
+    return ps, q, aux, dt
+
+
+CASES_1D = [(1, 0), (3, 0), (4, 0), (3, 2), (4, 2)]
+
+
+@pytest.mark.parametrize("ti,cd", CASES_1D)
+def test_1d_forward_step_matches_torch_restatement(ti, cd):
+    ps, q, aux, dt = _problem1d(ti=ti, cd=cd)
+    with S.Solver(ps, "fp64_strict") as s:
+        s.set_aux(aux)
+        s.set_q(q)
+        s.rk_step(dt)
+        got = s.get_q()[:, 3:-3]
+    Z, c = _cpu(aux[0, 3:-3]), _cpu(aux[1, 3:-3])
+    ref = torch_ref.rk(ti)(_cpu(q[:, 3:-3]), Z, c, dt, ps.dx, ps.dx, cd).numpy()
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("ti,cd", CASES_1D)
+def test_1d_adjoint_step_matches_autograd_and_dot_product(ti, cd):
+    ps, q, aux, dt = _problem1d(ti=ti, cd=cd)
+    rng = np.random.default_rng(6)
+    lam = np.zeros_like(q)
+    lam[:, 3:-3] = rng.standard_normal(lam[:, 3:-3].shape)
+    v = rng.standard_normal(q[:, 3:-3].shape)
+    with S.Solver(ps, "fp64_strict") as s:
+        s.set_aux(aux)
+        got = A.adjoint_step(s, _dev(q), _dev(lam), dt).cpu().numpy()[:, 3:-3]
+    Z, c = _cpu(aux[0, 3:-3]), _cpu(aux[1, 3:-3])
+    f = lambda t: torch_ref.rk(ti)(t, Z, c, dt, ps.dx, ps.dx, cd)
+    x = _cpu(q[:, 3:-3]).requires_grad_(True)
+    (g,) = torch.autograd.grad(f(x), x, _cpu(lam[:, 3:-3]))
+    ref = g.numpy()
+    assert np.abs(got - ref).max() <= 1e-11 * np.abs(ref).max()
+    _, jv = torch.func.jvp(f, (_cpu(q[:, 3:-3]),), (_cpu(v),))
+    lhs = float((jv.numpy() * lam[:, 3:-3]).sum())
+    rhs = float((v * got).sum())
+    assert abs(lhs - rhs) <= 1e-11 * max(abs(lhs), 1.0)
+
+
+@pytest.mark.parametrize("ti,cd", [(3, 0), (4, 2)])
+def test_1d_misfit_gradient_against_autograd_and_finite_differences(ti, cd):
+    ps, q, aux, dt = _problem1d(mx=200, ti=ti, cd=cd, background=0.05)
+    nsteps = 40
+    rng = np.random.default_rng(7)
+    p_obs = q[0, 3:-3] * 0.9 + 0.01 * rng.standard_normal(q[0, 3:-3].shape)
+    Z, c = _cpu(aux[0, 3:-3]), _cpu(aux[1, 3:-3])
+
+    def J_ref(p0):
+        y = torch.stack([p0, torch.zeros_like(p0)])
+        for _ in range(nsteps):
+            y = torch_ref.rk(ti)(y, Z, c, dt, ps.dx, ps.dx, cd)
+        return 0.5 * ((y[0] - _cpu(p_obs)) ** 2).sum()
+
+    x = _cpu(q[0, 3:-3]).requires_grad_(True)
+    (g_ref,) = torch.autograd.grad(J_ref(x), x)
+    with S.Solver(ps, "fp64") as s:
+        s.set_aux(aux)
+        p0 = _dev(q[0, 3:-3]).requires_grad_(True)
+        J = A.wave_misfit(p0, s, dt, nsteps, _dev(p_obs), checkpoint_every=15)
+        (g,) = torch.autograd.grad(J, p0)
+        g_cpu = g.cpu().numpy()
+        assert np.abs(g_cpu - g_ref.numpy()).max() <= 1e-9 * np.abs(g_ref.numpy()).max()
+        for k in range(3):
+            d = _dev(rng.standard_normal(q[0, 3:-3].shape))
+            # the pulse crossing the impedance jump keeps the WENO weights
+            # switching: central differences of this misfit converge slowly in
+            # h (3e-4 at h = 1e-7, 4e-6 at h = 1e-8 along a white-noise
+            # direction), so h = 1e-8, where rounding (1e-16 J / h) is still small
+            h = 1e-8
+            Jp = A.wave_misfit(p0.detach() + h * d, s, dt, nsteps, _dev(p_obs))
+            Jm = A.wave_misfit(p0.detach() - h * d, s, dt, nsteps, _dev(p_obs))
             fd = float((Jp - Jm) / (2 * h))
             ad = float((g * d).sum())
             assert abs(fd - ad) <= 1e-4 * abs(fd), (k, fd, ad)

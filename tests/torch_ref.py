@@ -47,18 +47,19 @@ def sweep(q, Z, c, dtdx, axis, mu, cd=0):
     a2 = (dl[0] + zim * dl[mu]) / (zim + zi)
     s1, s2 = -r(c, 1), c
     zero = torch.zeros_like(a1)
-    w1 = [-a1 * zim, zero, zero]
+    M = q.shape[0]
+    w1 = [-a1 * zim] + [zero] * (M - 1)
     w1[mu] = a1
-    w2 = [a2 * zi, zero, zero]
+    w2 = [a2 * zi] + [zero] * (M - 1)
     w2[mu] = a2
     amdq = torch.stack([s1 * w for w in w1])
     apdq = torch.stack([s2 * w for w in w2])
     dt_ = qr - ql                           # tfluct: left ql(i), right qr(i), aux of cell i
     b1 = (-dt_[0] + Z * dt_[mu]) / (2.0 * Z)
     b2 = (dt_[0] + Z * dt_[mu]) / (2.0 * Z)
-    v1 = [-b1 * Z, zero, zero]
+    v1 = [-b1 * Z] + [zero] * (M - 1)
     v1[mu] = b1
-    v2 = [b2 * Z, zero, zero]
+    v2 = [b2 * Z] + [zero] * (M - 1)
     v2[mu] = b2
     adq = torch.stack([-c * a + c * b for a, b in zip(v1, v2)])
     amdq_next = torch.roll(amdq, -1, dims=axis)
@@ -71,35 +72,40 @@ def char_edges(q, Z, axis, mu):
     zero-speed field): returns qr(c) and ql(c) of every cell, accumulated in
     the kernel's order (full 3x3 sums, zero entries included)."""
     r = lambda a, s: torch.roll(a, s, dims=axis)
-    mv = 3 - mu
+    M = q.shape[0]
     zim, zi = r(Z, 1), Z                    # interface i between cells i-1 and i
     z = 1.0 / (zim + zi)
     zero, one = torch.zeros_like(Z), torch.ones_like(Z)
-    evl = [[zero] * 3 for _ in range(3)]
-    evr = [[zero] * 3 for _ in range(3)]
-    evr[0][0], evr[0][1], evr[mu][0], evr[mu][1], evr[mv][2] = -zim, zi, one, one, one
-    evl[0][0], evl[0][mu], evl[1][0], evl[1][mu], evl[2][mv] = -1.0 * z, zi * z, 1.0 * z, zim * z, one
+    evl = [[zero] * M for _ in range(M)]
+    evr = [[zero] * M for _ in range(M)]
+    evr[0][0], evr[0][1], evr[mu][0], evr[mu][1] = -zim, zi, one, one
+    evl[0][0], evl[0][mu], evl[1][0], evl[1][mu] = -1.0 * z, zi * z, 1.0 * z, zim * z
+    if M == 3:
+        mv = 3 - mu
+        evr[mv][2], evl[2][mv] = one, one
     d = q - r(q, 1)                          # d(j) = q(j) - q(j-1)
     dk = [r(d, 2 - k) for k in range(5)]     # at interface i: d(i-2+k)
     cen = ((-r(q, 2)) + 7.0 * (r(q, 1) + q)) - r(q, -1)
-    QR = [cen[m] / 12.0 for m in range(3)]   # qr(i-1)
-    QL = [cen[m] / 12.0 for m in range(3)]   # ql(i)
-    for p in range(3):
+    QR = [cen[m] / 12.0 for m in range(M)]   # qr(i-1)
+    QL = [cen[m] / 12.0 for m in range(M)]   # ql(i)
+    for p in range(M):
         h = []
         for k in range(5):
             s = torch.zeros_like(Z)
-            for m in range(3):
+            for m in range(M):
                 s = s + evl[p][m] * dk[k][m]
             h.append(s)
         u1 = weno_side(h[0], h[1], h[2], h[3], 1.0)
         u2 = weno_side(h[4], h[3], h[2], h[1], -1.0)
-        for m in range(3):
+        for m in range(M):
             QR[m] = QR[m] + evr[m][p] * u1
             QL[m] = QL[m] + evr[m][p] * u2
     return r(torch.stack(QR), -1), torch.stack(QL)
 
 
 def D(q, Z, c, dt, dx, dy, cd=0):
+    if q.dim() == 2:                         # 1-D: (p, u) on one line
+        return sweep(q, Z, c, dt / dx, -1, 1, cd)
     return sweep(q, Z, c, dt / dx, -1, 1, cd) + sweep(q, Z, c, dt / dy, -2, 2, cd)
 
 
