@@ -85,6 +85,16 @@ extern "C" {
 #define SCL_B4STEP_SWIRL 1    /* apps/advection/2d/swirl/b4step.f90: aux = aux0 *
                                  cos(2 pi (t + dt/2) / tperiod); no-op for tperiod = 0     */
 
+/* ---- user boundary conditions (mthbc = 0: the app's own bc1.f, run on the
+ * device before every stage, with the stage time) -------------------------- */
+#define SCL_BC_USER_NONE 0              /* src/1d/bc1.f90: mthbc = 0 stops      */
+#define SCL_BC_USER_OSCILLATING_WALL 1  /* apps/elasticity/stegoton/bc1.f: a wall
+   at x = xlower (mthbc[0] = 0) moving with v = -a1 g0((t - t1)/tw1), at
+   x = xupper (mthbc[1] = 0) with v = a2 g0((t - t2)/tw2), g0(s) = 1 + cos(pi s)
+   for |s| < 1, else 0; ghost momentum 2 v rho - q2 of the mirror cell.  Once
+   a stage time lies in (5 tw1, 5 tw1 + 1) both sides become periodic (q and
+   aux ghosts) for the rest of the handle's life, as bc1.f rewrites mthbc.   */
+
 /* ---- arithmetic ---------------------------------------------------------- */
 #define SCL_FP64 0         /* plain FP64 (FMA contraction allowed)                       */
 #define SCL_FP64_STRICT 1  /* FP64, no FMA contraction: the reference's evaluation order */
@@ -103,7 +113,8 @@ typedef struct scl_params {
   int char_decomp;      /* 0 weno5, 1 weno5_wave, 2 weno5_char, 3 weno5_trans
                            (TVD: 0..2, polynomial: 0 q2qlqr_poly, 1 _poly_wave)   */
   int tfluct_solver;    /* 1 tfluct plugin, 0 swap + second rp (flux1.f90:136-188) */
-  int mthbc[4];         /* 1 extrapolation, 2 periodic, 3 solid wall               */
+  int mthbc[4];         /* 1 extrapolation, 2 periodic, 3 solid wall,
+                           0 the user bc named by bc_user (1-D)                   */
   double dx, dy, xlower, ylower;
   int rp;               /* SCL_RP_*                                                */
   int efix;             /* entropy fix (rp1eu.f:40 .true., rpn2sw.f:48 .false.)    */
@@ -117,6 +128,10 @@ typedef struct scl_params {
   int src_term;         /* SCL_SRC_* (ClawParams%src_term; the reference links the
                            app's src1.f90 instead)                                */
   double rho, bulk;     /* SCL_RP_ACOUSTICS_CONST: common /cparam/ rho, bulk       */
+  int bc_user;          /* SCL_BC_USER_* for the sides with mthbc = 0              */
+  double wall[6];       /* SCL_BC_USER_OSCILLATING_WALL: t1, a1, tw1 (common
+                           /comwall/, setprob.data) and t2, a2, tw2 of the right
+                           wall                                                    */
 } scl_params;
 
 /* Arguments of sharpclaw() (src/sharpclaw.f90:2-5). */

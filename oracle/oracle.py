@@ -42,6 +42,7 @@ class Params(ctypes.Structure):
         ("b4step", ctypes.c_int), ("tperiod", ctypes.c_double),
         ("src_term", ctypes.c_int),
         ("rho", ctypes.c_double), ("bulk", ctypes.c_double),
+        ("bc_user", ctypes.c_int), ("wall", ctypes.c_double * 6), ("bc_switched", ctypes.c_int),
     ]
 
 
@@ -61,6 +62,7 @@ class Result(ctypes.Structure):
         ("cfl_last", ctypes.c_double), ("dt_minused", ctypes.c_double),
         ("dt_maxused", ctypes.c_double), ("dt_last", ctypes.c_double),
         ("steps_taken", ctypes.c_int), ("info", ctypes.c_int), ("rejected", ctypes.c_int),
+        ("bc_switched", ctypes.c_int),
     ]
 
 
@@ -107,7 +109,8 @@ def _ptr(a):
 def make_params(*, ndim=1, mx, my=1, meqn, mwaves, mbc=3, maux=0, mcapa=0, char_decomp=0,
                 tfluct_solver=1, mthbc=(2, 2, 2, 2), dx, dy=1.0, xlower=0.0, ylower=0.0,
                 rp, efix=None, u=1.0, gamma=1.4, grav=1.0, lim_type=2, mthlim=(1, 1, 1, 1),
-                src_term=SRC_NONE, rho=1.0, bulk=1.0) -> Params:
+                src_term=SRC_NONE, rho=1.0, bulk=1.0, bc_user=0,
+                wall=(0.0, 0.0, 1.0, 0.0, 0.0, 1.0)) -> Params:
     p = Params()
     p.ndim, p.mx, p.my = ndim, mx, (my if ndim == 2 else 1)
     p.meqn, p.mwaves, p.mbc, p.maux, p.mcapa = meqn, mwaves, mbc, maux, mcapa
@@ -123,6 +126,9 @@ def make_params(*, ndim=1, mx, my=1, meqn, mwaves, mbc=3, maux=0, mcapa=0, char_
         p.mthlim[k] = int(mthlim[k]) if k < len(mthlim) else 1
     p.src_term = int(src_term)
     p.rho, p.bulk = rho, bulk
+    p.bc_user = int(bc_user)
+    for k in range(6):
+        p.wall[k] = float(wall[k])
     return p
 
 

@@ -153,6 +153,51 @@ int ocl_bc(const ocl_params *p, double *q) {
   return p->ndim == 1 ? bc1(p, q) : bc2(p, q);
 }
 
+/* g0 of apps/elasticity/stegoton/bc1.f:152-166 (pi = 4 datan(1), setprob.f:20) */
+static double wall_g0(double s) {
+  const double pi = 4.0 * atan(1.0);
+  return fabs(s) < 1.0 ? 1.0 + cos(pi * s) : 0.0;
+}
+
+/* apps/elasticity/stegoton/bc1.f:1-150 at time t, replacing bc1.f90: the
+ * switch of both sides to periodic while 5 tw1 < t < 5 tw1 + 1 (:31-35; it
+ * rewrites mthbc, so it stays: p->bc_switched), periodic aux ghosts of aux
+ * fields 1..3 when the left side is periodic (:36-45), then each side; an
+ * oscillating wall on mthbc = 0 sides (:100-106, :200-206).  bc1.f:62 reads
+ * aux(i,1) with i never set; the mirror cell's aux(ibc,1) is used here, as
+ * the right wall does (:206). */
+static int bc1_user(ocl_params *p, double *q, double *aux, double t) {
+  const int mbc = p->mbc, mx = p->mx;
+  const long ld = mx + 2 * mbc;
+  const double t1 = p->wall[0], a1 = p->wall[1], tw1 = p->wall[2];
+  const double t2 = p->wall[3], a2 = p->wall[4], tw2 = p->wall[5];
+  if (mbc != 3 || p->meqn < 2 || !aux || p->maux < 1) return -2;
+  if (t > 5.0 * tw1 && t < 5.0 * tw1 + 1.0) p->bc_switched = 1;
+  const int bl = p->bc_switched ? 2 : p->mthbc[0], br = p->bc_switched ? 2 : p->mthbc[1];
+  if (bl == 2)
+    for (int j = 1; j <= (p->maux < 3 ? p->maux : 3); ++j)
+      for (int ibc = 1; ibc <= mbc; ++ibc) {
+        L2(aux, 1 - ibc, j) = L2(aux, mx + 1 - ibc, j);
+        L2(aux, mx + ibc, j) = L2(aux, ibc, j);
+      }
+  /* the standard sides as bc1.f90; a moving wall starts as a solid wall */
+  ocl_params pc = *p;
+  pc.mthbc[0] = bl == 0 ? 3 : bl;
+  pc.mthbc[1] = br == 0 ? 3 : br;
+  int rc = bc1(&pc, q);
+  if (rc) return rc;
+  if (bl == 0) {
+    const double vwall = -(a1 * wall_g0((t - t1) / tw1));
+    for (int ibc = 1; ibc <= mbc; ++ibc) L2(q, 1 - ibc, 2) = 2.0 * vwall * L2(aux, ibc, 1) - L2(q, ibc, 2);
+  }
+  if (br == 0) {
+    const double vwall = a2 * wall_g0((t - t2) / tw2);
+    for (int ibc = 1; ibc <= mbc; ++ibc)
+      L2(q, mx + ibc, 2) = 2.0 * vwall * L2(aux, mx + 1 - ibc, 1) - L2(q, mx + 1 - ibc, 2);
+  }
+  return 0;
+}
+
 /* ======================================================================== */
 /* WENO5 reconstructions, src/reconstruct.f90.  Indices are the rebased      */
 /* (1-based, assumed-shape) array indices of the reference: array index k    */
@@ -1658,10 +1703,9 @@ static void src1(const ocl_params *p, const double *q, double *dq, const double 
 
 /* src/1d/step1d.f90:2-31, src/2d/step2d.f90:2-41 (with src1/src2 zeroing,
  * or the app's 1-D source hook) */
-int ocl_step(const ocl_params *p, double *q, double *dq, const double *aux, double dt,
-             double t, double *cfl) {
-  (void)t;
-  int rc = ocl_bc(p, q);
+static int step_st(ocl_params *p, double *q, double *dq, double *aux, double dt, double t,
+                   double *cfl) {
+  int rc = (p->ndim == 1 && p->bc_user) ? bc1_user(p, q, aux, t) : ocl_bc(p, q);
   if (rc) return rc;
   const long n = ocl_plane(p) * p->meqn;
   for (long k = 0; k < n; ++k) dq[k] = 0.0;   /* src: interior zeroed; ghosts unused */
@@ -1675,17 +1719,36 @@ int ocl_step(const ocl_params *p, double *q, double *dq, const double *aux, doub
   return flux2(p, q, dq, aux, dt, cfl);
 }
 
+/* a working copy of aux for the user bc, which rewrites aux ghost cells */
+static double *aux_copy(const ocl_params *p, const double *aux) {
+  if (!p->bc_user || !aux) return NULL;
+  const size_t na = (size_t)ocl_plane(p) * (size_t)(p->maux > 0 ? p->maux : 1);
+  double *w = (double *)malloc(sizeof(double) * na);
+  if (w) memcpy(w, aux, sizeof(double) * na);
+  return w;
+}
+
+int ocl_step(const ocl_params *p, double *q, double *dq, const double *aux, double dt,
+             double t, double *cfl) {
+  ocl_params pl = *p;
+  double *auxw = aux_copy(p, aux);
+  if (p->bc_user && aux && !auxw) return -3;
+  int rc = step_st(&pl, q, dq, auxw ? auxw : (double *)aux, dt, t, cfl);
+  free(auxw);
+  return rc;
+}
+
 /* ======================================================================== */
 /* SSP-RK stages, src/sharpclaw.f90:247-464 (whole-array updates).           */
 /* ======================================================================== */
-int ocl_rk_step(const ocl_params *p, int ti, double *q, const double *qold,
-                const double *aux, double dt, double told, double *cfl) {
+static int rk_step_st(ocl_params *p, int ti, double *q, const double *qold, double *aux, double dt,
+                      double told, double *cfl) {
   const long n = ocl_plane(p) * p->meqn;
   double *r1 = (double *)calloc((size_t)n, sizeof(double));
   double *r2 = (ti == 4) ? (double *)calloc((size_t)n, sizeof(double)) : NULL;
   int rc = 0;
   if (!r1 || (ti == 4 && !r2)) { free(r1); free(r2); return -3; }
-#define STEP(dst, tt) do { rc = ocl_step(p, q, (dst), aux, dt, (tt), cfl); if (rc) goto out; } while (0)
+#define STEP(dst, tt) do { rc = step_st(p, q, (dst), aux, dt, (tt), cfl); if (rc) goto out; } while (0)
   if (ti == 1) {                                           /* ts_ssp22 :247-276 */
     const double c2 = 1.0;
     STEP(r1, told);
@@ -1755,6 +1818,16 @@ out:
   return rc;
 }
 
+int ocl_rk_step(const ocl_params *p, int ti, double *q, const double *qold,
+                const double *aux, double dt, double told, double *cfl) {
+  ocl_params pl = *p;
+  double *auxw = aux_copy(p, aux);
+  if (p->bc_user && aux && !auxw) return -3;
+  int rc = rk_step_st(&pl, ti, q, qold, auxw ? auxw : (double *)aux, dt, told, cfl);
+  free(auxw);
+  return rc;
+}
+
 /* ======================================================================== */
 /* src/sharpclaw.f90:2-243 driver                                            */
 /* ======================================================================== */
@@ -1772,9 +1845,10 @@ int ocl_sharpclaw(const ocl_params *p, const ocl_run *run, double *q, const doub
                   ocl_result *res) {
   const long n = ocl_plane(p) * p->meqn;
   const long na = ocl_plane(p) * (p->maux > 0 ? p->maux : 1);
-  double *auxw = NULL;          /* the hook's working aux */
+  double *auxw = NULL;          /* the hooks' working aux */
   const double *aux = aux_in;
-  if (p->b4step == 1 && aux_in) {
+  ocl_params pl = *p;           /* the user bc's switch state evolves */
+  if ((p->b4step == 1 || p->bc_user) && aux_in) {
     auxw = (double *)malloc(sizeof(double) * (size_t)na);
     if (!auxw) return -3;
     memcpy(auxw, aux_in, sizeof(double) * (size_t)na);
@@ -1799,13 +1873,16 @@ int ocl_sharpclaw(const ocl_params *p, const ocl_run *run, double *q, const doub
     if (!retake) {
       told = t;
       if (told + dt > tend && tstart < tend) dt = tend - told;
-      if (auxw) b4step_swirl(p, aux_in, auxw, na, told, dt);                 /* :129 */
+      if (auxw && p->b4step == 1) b4step_swirl(p, aux_in, auxw, na, told, dt);                 /* :129 */
       memcpy(qold, q, sizeof(double) * (size_t)n);
     }
     retake = 0;
     t = told + dt;
-    if (p->ndim == 1) { rc = ocl_bc(p, q); if (rc) break; }
-    rc = ocl_rk_step(p, run->time_integrator, q, qold, aux, dt, told, &cfl);
+    if (p->ndim == 1) {                                                        /* :153 */
+      rc = pl.bc_user ? bc1_user(&pl, q, auxw, told) : ocl_bc(p, q);
+      if (rc) break;
+    }
+    rc = rk_step_st(&pl, run->time_integrator, q, qold, (double *)aux, dt, told, &cfl);
     if (rc) break;
     if (run->dt_variable == 1) {                                               /* :184-192 */
       if (cfl > 0.0) {
@@ -1842,6 +1919,7 @@ int ocl_sharpclaw(const ocl_params *p, const ocl_run *run, double *q, const doub
   res->steps_taken = steps;
   res->info = info;
   res->rejected = rejected;
+  res->bc_switched = pl.bc_switched;
   return 0;
 }
 

@@ -67,7 +67,7 @@ typedef struct {
                            polynomial (polyrecon.f90, order mthlim(1) = 3)          */
   int char_decomp;      /* 0 componentwise, 2 characteristic-wise                   */
   int tfluct_solver;    /* 1: tfluct plugin, 0: swap + second rp                    */
-  int mthbc[4];         /* 1 extrap, 2 periodic, 3 wall                              */
+  int mthbc[4];         /* 1 extrap, 2 periodic, 3 wall, 0 user bc (bc_user)         */
   double dx, dy, xlower, ylower;
   int rp;               /* OCL_RP_* */
   int efix;             /* entropy fix flag (Euler default 1, SW default 0)          */
@@ -79,6 +79,9 @@ typedef struct {
   double tperiod;       /* swirl: common /comvt/ tperiod                              */
   int src_term;         /* OCL_SRC_* (1-D)                                            */
   double rho, bulk;     /* homogeneous acoustics: common /cparam/ rho, bulk           */
+  int bc_user;          /* 1: apps/elasticity/stegoton/bc1.f replaces src/1d/bc1.f90  */
+  double wall[6];       /* t1, a1, tw1 (common /comwall/), t2, a2, tw2                 */
+  int bc_switched;      /* the switch to periodic of bc1.f:31-35 has happened         */
 } ocl_params;
 
 typedef struct {
@@ -91,6 +94,7 @@ typedef struct {
   double tend;          /* time reached */
   double cfl_maxused, cfl_last, dt_minused, dt_maxused, dt_last;
   int steps_taken, info, rejected;
+  int bc_switched;      /* state of the user bc's switch after the run                */
 } ocl_result;
 
 /* size of a field with ghost cells (number of doubles per component) */

@@ -28,7 +28,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _capi as C
-from ._capi import (B4STEP_NONE, B4STEP_SWIRL, FP32, FP64, FP64_STRICT, MIXED,  # noqa: F401
+from ._capi import (B4STEP_NONE, B4STEP_SWIRL, BC_USER_NONE, BC_USER_OSCILLATING_WALL, FP32, FP64, FP64_STRICT, MIXED,  # noqa: F401
                     RP_ACOUSTICS_CONST, RP_ACOUSTICS_FWAVE, RP_ADVECTION_CONS, RP_STEGOTON, RP_TRAFFIC,
                     RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION, RP_ADVECTION2D, RP_EULER, RP_SW1D, RP_SW2D,
                     RP_SWF_BATHY, RP_SWF_KAPPA, RP_SWF_RADIAL, SRC_BATHYMETRY_SW, SRC_NONE, SRC_RADIAL_SW,
@@ -43,7 +43,7 @@ __all__ = ["ClawParams", "Solver", "Batch", "sharpclaw", "SharpClawError", "read
            "RP_STEGOTON",
            "SRC_NONE", "SRC_RADIAL_SW",
            "SRC_BATHYMETRY_SW", "B4STEP_NONE", "B4STEP_SWIRL",
-           "RUN_AUTO", "RUN_GRAPH", "RUN_RESIDENT"]
+           "RUN_AUTO", "RUN_GRAPH", "RUN_RESIDENT", "BC_USER_NONE", "BC_USER_OSCILLATING_WALL"]
 
 # plugin id -> (meqn, mwaves, maux, ndim)
 PLUGINS = {
@@ -95,6 +95,10 @@ class ClawParams:
     src_term: int = 0
     rho: float = 1.0      # homogeneous acoustics (common /cparam/)
     bulk: float = 1.0
+    # mthbc = 0 sides: the app's bc1.f on the device (BC_USER_OSCILLATING_WALL:
+    # apps/elasticity/stegoton/bc1.f with wall = (t1, a1, tw1, t2, a2, tw2))
+    bc_user: int = 0
+    wall: Sequence[float] = (0.0, 0.0, 1.0, 0.0, 0.0, 1.0)
 
     def __post_init__(self):
         meqn, mwaves, maux, ndim = PLUGINS.get(self.rp, (None, None, 0, None))
@@ -133,6 +137,9 @@ class ClawParams:
             p.mthlim[k] = int(self.mthlim[k]) if k < len(self.mthlim) else 1
         p.src_term = int(self.src_term)
         p.rho, p.bulk = float(self.rho), float(self.bulk)
+        p.bc_user = int(self.bc_user)
+        for k in range(6):
+            p.wall[k] = float(self.wall[k])
         return p
 
 

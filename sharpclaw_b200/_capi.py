@@ -19,6 +19,7 @@ RP_SWF_BATHY, RP_SWF_RADIAL, RP_SWF_KAPPA = 8, 9, 10
 RP_ACOUSTICS_CONST, RP_ACOUSTICS_FWAVE = 11, 12
 RP_TRAFFIC, RP_ADVECTION_CONS, RP_STEGOTON = 13, 14, 15
 B4STEP_NONE, B4STEP_SWIRL = 0, 1
+BC_USER_NONE, BC_USER_OSCILLATING_WALL = 0, 1
 RUN_AUTO, RUN_GRAPH, RUN_RESIDENT = 0, 1, 2
 FP64, FP64_STRICT, MIXED, FP32 = 0, 1, 2, 3
 INFO_DT_NOT_DIVIDING, INFO_CFL_DESIRED_GT_MAX, INFO_TOO_MANY_STEPS, INFO_CFL_FIXED_DT, INFO_NONFINITE = 2, 3, 11, 12, 20
@@ -42,6 +43,7 @@ class scl_params(ctypes.Structure):
         ("mthlim", ctypes.c_int * 4),
         ("src_term", ctypes.c_int),
         ("rho", ctypes.c_double), ("bulk", ctypes.c_double),
+        ("bc_user", ctypes.c_int), ("wall", ctypes.c_double * 6),
     ]
 
 

@@ -364,6 +364,7 @@ int scl_batch_create(const scl_params* p, int ninst, const int* mx, const double
   if (!ok) return bfail(SCL_E_INVALID, "batched solver takes the 1-D plugins");
   if (p->mcapa < 0 || p->mcapa > p->maux) return bfail(SCL_E_INVALID, "mcapa out of range");
   if (p->src_term != SCL_SRC_NONE) return bfail(SCL_E_UNSUPPORTED, "no source-term hooks in the batched solver");
+  if (p->bc_user != SCL_BC_USER_NONE) return bfail(SCL_E_UNSUPPORTED, "no user bc in the batched solver");
   for (int k = 0; k < ninst; ++k) {
     if (mx[k] < 3) return bfail(SCL_E_INVALID, "every instance needs mx >= 3");
     if (!(dx[k] > 0)) return bfail(SCL_E_INVALID, "every instance needs dx > 0");

@@ -73,6 +73,61 @@ __global__ void k_bc1(S* q, long plane, int mx, int meqn, int bl, int br) {
   else if (br == 3) at(mx + ibc) = (m == 1) ? -at(mx + 1 - ibc) : at(mx + 1 - ibc);
 }
 
+// apps/elasticity/stegoton/bc1.f, g0: 1 + cos(pi s) on |s| < 1 (pi = 4 atan(1))
+__device__ __forceinline__ double wall_g0(double s) {
+  return fabs(s) < 1.0 ? 1.0 + cos(3.141592653589793 * s) : 0.0;
+}
+
+// The user bc of apps/elasticity/stegoton/bc1.f on the input of one stage, at
+// the stage's time (step1d.f90:20 calls bc with it): the switch to periodic
+// (bc1.f:31-35, remembered in ctl->bc_switched as bc1.f rewrites mthbc), the
+// periodic ghosts of aux fields 1..3 when the left side is periodic
+// (bc1.f:36-45), then each side.  One CTA; thread 0
+// decides, then one thread per (m, ibc) writes q ghosts and one per (j, ibc)
+// aux ghosts.  The moving wall's ghost momentum uses the density of the mirror
+// cell, aux(ibc,1) (bc1.f:62 indexes aux with the unset loop variable i).
+template <class S>
+__global__ void k_bc_user1d(StageArgs a, int meqn, int maux) {
+  Ctl* c = a.ctl;
+  __shared__ int sw;
+  __shared__ double vl, vr;
+  if (c->done) return;
+  if (threadIdx.x == 0) {
+    const double told = c->told, dt = c->dt;
+    const double t = a.tform == 0 ? told + a.tc * dt : a.tform == 1 ? told + dt / a.tc : a.tc;
+    const double t1 = a.wall[0], a1 = a.wall[1], tw1 = a.wall[2];
+    const double t2 = a.wall[3], a2 = a.wall[4], tw2 = a.wall[5];
+    if (t > 5.0 * tw1 && t < 5.0 * tw1 + 1.0) c->bc_switched = 1;
+    sw = c->bc_switched;
+    vl = -(a1 * wall_g0((t - t1) / tw1));
+    vr = a2 * wall_g0((t - t2) / tw2);
+  }
+  __syncthreads();
+  S* q = static_cast<S*>(a.buf[c->role[a.sd.in]]);
+  S* aux = static_cast<S*>(const_cast<void*>(a.aux));
+  const int mx = a.mx, k = threadIdx.x;
+  const int bl = sw ? 2 : a.mthbc[0], br = sw ? 2 : a.mthbc[1];
+  if (bl == 2 && k < 3 * (maux < 3 ? maux : 3)) {
+    const int j = k / 3, ibc = k % 3 + 1;
+    S* p = aux + (long)j * a.plane;
+    p[1 - ibc + 2] = p[mx + 1 - ibc + 2];
+    p[mx + ibc + 2] = p[ibc + 2];
+  }
+  if (k >= 3 * meqn) return;
+  const int m = k / 3, ibc = k % 3 + 1;
+  S* p = q + (long)m * a.plane;
+  auto at = [&](int i) -> S& { return p[i + 2]; };
+  auto rho = [&](int i) -> double { return (double)aux[i + 2]; };
+  if (bl == 0) at(1 - ibc) = m == 1 ? (S)(2.0 * vl * rho(ibc) - (double)at(ibc)) : at(ibc);
+  else if (bl == 1) at(1 - ibc) = at(1);
+  else if (bl == 2) at(1 - ibc) = at(mx + 1 - ibc);
+  else at(1 - ibc) = (m == 1) ? -at(ibc) : at(ibc);
+  if (br == 0) at(mx + ibc) = m == 1 ? (S)(2.0 * vr * rho(mx + 1 - ibc) - (double)at(mx + 1 - ibc)) : at(mx + 1 - ibc);
+  else if (br == 1) at(mx + ibc) = at(mx);
+  else if (br == 2) at(mx + ibc) = at(ibc);
+  else at(mx + ibc) = (m == 1) ? -at(mx + 1 - ibc) : at(mx + 1 - ibc);
+}
+
 // bc2.f90 x-sides (all rows j = 1-mbc..ny+mbc), then y-sides (all columns)
 template <class S>
 __global__ void k_bc2(S* q, long plane, long pitch, int nx, int ny, int meqn, int b0, int b1,
@@ -216,6 +271,24 @@ struct scl_handle {
 
 namespace {
 
+// The time of stage s of integrator ti, `that` of sharpclaw.f90 in its
+// written form: told + tc*dt (form 0) or told + dt/tc (form 1).
+void stage_time_form(int ti, int s, int* form, double* tc) {
+  *form = 0;
+  *tc = 0.0;                                               // stage 1: told
+  if (s == 0) return;
+  if (ti == 1) { *tc = 1.0; return; }                      // :268 c2 = 1
+  if (ti == 2) {                                           // :307-325
+    const double third = 1.0 / 3.0;
+    *tc = s == 1 ? third : s == 2 ? 2.0 * third : 1.0;
+    return;
+  }
+  if (ti == 3) { *tc = s == 1 ? 1.0 : 0.5; return; }       // :359, :368
+  static const double c104[10] = {0.0, 6.0, 3.0, 0.5, 2.0 / 3.0, 1.0 / 3.0, 0.5, 2.0 / 3.0, 5.0 / 6.0, 1.0};
+  *tc = c104[s];                                           // :397-456
+  *form = (s == 1 || s == 2) ? 1 : 0;                      // dt/6.d0, dt/3.d0
+}
+
 StageArgs make_args(const scl_handle* h, int s) {
   StageArgs a{};
   a.ctl = h->ctl;
@@ -242,7 +315,16 @@ StageArgs make_args(const scl_handle* h, int s) {
   a.ph.efix = h->p.efix;
   for (int k = 0; k < 4; ++k) a.ph.mthlim[k] = h->p.mthlim[k];
   set_acoustics_consts(h->p, &a.ph);
+  a.bc_user = h->p.bc_user;
+  for (int k = 0; k < 6; ++k) a.wall[k] = h->p.wall[k];
+  stage_time_form(h->p.time_integrator, s, &a.tform, &a.tc);
   return a;
+}
+
+// the user bc hook on the input of the stage `a` describes
+void launch_bc_user(scl_handle* h, const StageArgs& a) {
+  if (h->ssize == sizeof(double)) k_bc_user1d<double><<<1, 32, 0, h->stream>>>(a, h->p.meqn, h->p.maux);
+  else k_bc_user1d<float><<<1, 32, 0, h->stream>>>(a, h->p.meqn, h->p.maux);
 }
 
 int upload_ctl(scl_handle* h) {
@@ -259,6 +341,7 @@ int download_ctl(scl_handle* h) {
 int enqueue_stages(scl_handle* h) {
   for (int s = 0; s < h->nstages; ++s) {
     StageArgs a = make_args(h, s);
+    if (h->p.bc_user) launch_bc_user(h, a);
     h->L.stage(a, h->stream);
     if (h->L.ghost && s == h->nstages - 1) h->L.ghost(a, h->stream);
   }
@@ -290,7 +373,7 @@ int enqueue_step(scl_handle* h, bool first = true, bool last = true) {
 
 // launches per step inside a graph (plus one begin per graph replay)
 int kernels_per_step(const scl_handle* h) {
-  return h->nstages + 1 + (h->L.ghost ? 1 : 0) + (h->b4kind != SCL_B4STEP_NONE ? 1 : 0);
+  return h->nstages * (h->p.bc_user ? 2 : 1) + 1 + (h->L.ghost ? 1 : 0) + (h->b4kind != SCL_B4STEP_NONE ? 1 : 0);
 }
 
 // Capture `steps` controller steps (begin, stages, end) into one executable
@@ -426,9 +509,16 @@ int validate(const scl_params* p) {
     for (int k = 0; k < std::max(p->meqn, p->mwaves) && k < 4; ++k)
       if (p->mthlim[k] < 1 || p->mthlim[k] > 5) return fail(SCL_E_INVALID, "mthlim must be 1..5 (reconstruct.f90:551-571)");
   if (p->tfluct_solver != 0 && p->tfluct_solver != 1) return fail(SCL_E_INVALID, "tfluct_solver must be 0 or 1");
-  for (int k = 0; k < 2 * p->ndim; ++k)
-    if (p->mthbc[k] < 1 || p->mthbc[k] > 3)
-      return fail(SCL_E_INVALID, "mthbc must be 1, 2 or 3 (0 = user bc is not built)");
+  if (p->bc_user < SCL_BC_USER_NONE || p->bc_user > SCL_BC_USER_OSCILLATING_WALL)
+    return fail(SCL_E_INVALID, "bc_user must be SCL_BC_USER_NONE or SCL_BC_USER_OSCILLATING_WALL");
+  if (p->bc_user && (p->ndim != 1 || p->meqn < 2 || p->meqn > 10 || p->maux < 1 || p->maux > 10))
+    return fail(SCL_E_UNSUPPORTED, "the oscillating-wall bc is 1-D with 2..10 components and 1..10 aux fields");
+  for (int k = 0; k < 2 * p->ndim; ++k) {
+    if (p->mthbc[k] == 0 && !p->bc_user)
+      return fail(SCL_E_INVALID, "mthbc(k)=0 and no BCs specified in bc1 (set bc_user)");
+    if (p->mthbc[k] < 0 || p->mthbc[k] > 3)
+      return fail(SCL_E_INVALID, "mthbc must be 0 (user bc), 1, 2 or 3");
+  }
   for (int k = 0; k < 2 * p->ndim; ++k)
     if (p->mthbc[k] == 3 && p->meqn < (k < 2 ? 2 : 3))
       return fail(SCL_E_INVALID, "solid wall bc negates component 2 (x) / 3 (y): meqn too small");
@@ -609,7 +699,6 @@ int scl_set_b4step(scl_handle* h, int kind, double param) {
 }
 
 int scl_step_dq(scl_handle* h, double* q, double* dq, double dt, double t, double* cfl) {
-  (void)t;
   if (!h || !q || !dq) return fail(SCL_E_INVALID, "null argument");
   int rc = scl_set_q(h, q);   // upload + bc
   if (rc) return rc;
@@ -621,6 +710,13 @@ int scl_step_dq(scl_handle* h, double* q, double* dq, double dt, double t, doubl
   CK(cudaMemsetAsync(h->stage64, 0, sizeof(double) * h->plane * h->p.meqn, h->stream));
   StageArgs a = make_args(h, 0);
   a.sd = StageDesc{SK_DQ, ROLE_Q, -1, -1, -1};
+  if (h->p.bc_user) {   // step1d.f90:20: bc at the step's time t
+    a.tform = 2;
+    a.tc = t;
+    launch_bc_user(h, a);
+    CK(cudaMemcpyAsync(&h->hctl->bc_switched, &h->ctl->bc_switched, sizeof(int), cudaMemcpyDeviceToHost,
+                       h->stream));
+  }
   h->L.stage(a, h->stream);
   if (h->L.ghost) h->L.ghost(a, h->stream);
   CK(cudaGetLastError());
@@ -854,7 +950,7 @@ int resident_tiles(const scl_handle* h) { return (h->p.mx + RES_NT - 2) / (RES_N
 // A resident run needs a 1-D grid of at most RES_MAX_TILES tiles and no
 // b4step hook (the hooks run as kernels of the step graph).
 bool resident_possible(const scl_handle* h) {
-  return h->p.ndim == 1 && h->L.run != nullptr && h->b4kind == SCL_B4STEP_NONE &&
+  return h->p.ndim == 1 && h->L.run != nullptr && h->b4kind == SCL_B4STEP_NONE && !h->p.bc_user &&
          resident_tiles(h) <= RES_MAX_TILES;
 }
 
@@ -863,7 +959,7 @@ int use_resident(const scl_handle* h, bool* yes) {
   if (h->run_mode == SCL_RUN_GRAPH) return SCL_OK;
   if (h->run_mode == SCL_RUN_RESIDENT) {
     if (!resident_possible(h))
-      return fail(SCL_E_UNSUPPORTED, "resident run: needs a 1-D grid of at most 64 tiles and no b4step hook");
+      return fail(SCL_E_UNSUPPORTED, "resident run: needs a 1-D grid of at most 64 tiles, no b4step hook and no user bc");
     *yes = true;
     return SCL_OK;
   }
@@ -976,7 +1072,11 @@ int scl_time_stages(scl_handle* h, double dt, int reps, float* ms, long long* la
   if (rc) return rc;
   CK(cudaEventRecord(h->ev0, h->stream));
   for (int r = 0; r < reps; ++r) {
-    for (int s = 0; s < h->nstages; ++s) h->L.stage(make_args(h, s), h->stream);
+    for (int s = 0; s < h->nstages; ++s) {
+      const StageArgs a = make_args(h, s);
+      if (h->p.bc_user) launch_bc_user(h, a);
+      h->L.stage(a, h->stream);
+    }
   }
   CK(cudaGetLastError());
   CK(cudaEventRecord(h->ev1, h->stream));

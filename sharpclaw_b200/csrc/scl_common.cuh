@@ -60,7 +60,7 @@ struct __align__(16) Ctl {
   int status;                   // OR of SCL_STATUS_* raised by kernels
   int accept_always;            // single-step mode (scl_rk_step): no dt update, always accept
   int fresh;                    // 1: the current step is a new one (b4step runs), 0: a retake
-  int pad;
+  int bc_switched;              // the user bc switched both sides to periodic (persistent)
 };
 
 // Physics constants of the plugins (COMMON blocks /comrp/, /param/).
@@ -103,6 +103,11 @@ struct StageArgs {
   Phys ph;
   int src_term;             // SCL_SRC_* (1-D single grids)
   double xlower;
+  // user bc hook (SCL_BC_USER_*) and this stage's time: told + tc*dt (tform
+  // 0), told + dt/tc (1), or tc itself (2), as sharpclaw.f90 writes `that`
+  int bc_user, tform;
+  double tc;
+  double wall[6];
 };
 
 // Arguments of a cluster-resident run of a 1-D grid (the whole controller

@@ -162,6 +162,7 @@ extern "C" int scl_rk_step_noalloc(const scl_params* p, double* q_dev, const dou
   if (p->maux > 0 && !aux_dev) return fail_na(SCL_E_INVALID, "aux_dev required when maux > 0");
   if (p->mcapa < 0 || p->mcapa > p->maux) return fail_na(SCL_E_INVALID, "mcapa out of range");
   if (p->src_term != SCL_SRC_NONE) return fail_na(SCL_E_UNSUPPORTED, "no source-term hooks in scl_rk_step_noalloc");
+  if (p->bc_user != SCL_BC_USER_NONE) return fail_na(SCL_E_UNSUPPORTED, "no user bc in scl_rk_step_noalloc");
   const long ld = (long)p->mx + 2 * p->mbc;
   // the kernels read exactly the plugin's number of components and aux fields
   struct { int rp, meqn, mwaves, maux; } tab[] = {

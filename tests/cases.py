@@ -74,6 +74,29 @@ def acoustics1d(mx=200, rho=(1.0, 4.0), c=(1.0, 0.5), char_decomp=0, tfluct_solv
     return po, ps, q, aux
 
 
+def stegoton_wall(mx=288, upper=6.0, wall=(1.0, 0.01, 1.0, 0.0, 0.0, 1.0), mthbc=(0, 1), char_decomp=0):
+    """apps/elasticity/stegoton as its sharpclaw.data runs it: q = 0, the
+    oscillating wall of bc1.f at xlower (mthbc 0) and extrapolation at xupper,
+    the switch to periodic when a stage time enters (5 tw1, 5 tw1 + 1).  The
+    app's wall (t1 = 10, a1 = 0.1, tw1 = 10 on [0, 150]) is scaled to
+    t1 = tw1 = 1 on [0, upper] so the pulse, its travel and the switch fit a
+    short run, with a1 = 0.01: the ten times faster ramp at a1 = 0.1 drives
+    the exponential stress law into blow-up; 48 cells per layer period as the
+    app's mx = 7200.  Layers as setaux.f: ix = xcell truncates toward zero,
+    so the ghost cells left of x = 0 are layer A."""
+    po, ps, q, aux = stegoton(mx=mx, char_decomp=char_decomp, mthbc=mthbc, amp=0.0)
+    dx = upper / mx
+    xa = (np.arange(-3, mx + 3) + 0.5) * dx
+    frac = xa - np.trunc(xa)
+    rho = np.where(frac < 0.5, 1.0, 4.0)
+    aux = np.ascontiguousarray(np.stack([rho, rho.copy(), np.zeros_like(xa)]))
+    po = O.make_params(meqn=2, mwaves=2, maux=3, rp=O.RP_STEGOTON, mx=mx, dx=dx, xlower=0.0, mthbc=mthbc,
+                       char_decomp=char_decomp, tfluct_solver=1, bc_user=1, wall=wall)
+    ps = S.ClawParams(rp=S.RP_STEGOTON, mx=mx, dx=dx, xlower=0.0, mthbc=mthbc, char_decomp=char_decomp,
+                      tfluct_solver=1, bc_user=S.BC_USER_OSCILLATING_WALL, wall=wall)
+    return po, ps, np.zeros((2, mx + 6)), aux
+
+
 def radial_dam(n=48, noise=1e-3, seed=3, char_decomp=2, tfluct_solver=1, mthbc=(2, 2, 2, 2), efix=0):
     """2-D shallow-water radial dam break on [-2.5,2.5]^2: h = 2 inside r < 0.5,
     1 outside (cell-centre test), hu = hv = 0, seeded N(0, noise) on h."""

@@ -50,7 +50,10 @@ def test_version_string():
     (dict(lim_type=1, char_decomp=3), C.SCL_E_UNSUPPORTED),
     (dict(lim_type=1, mthlim=(1, 6, 1, 1)), C.SCL_E_INVALID),
     (dict(char_decomp=4), C.SCL_E_UNSUPPORTED),
-    (dict(mthbc=(0, 0)), C.SCL_E_INVALID),
+    (dict(mthbc=(0, 0)), C.SCL_E_INVALID),                                      # user bc without bc_user
+    (dict(bc_user=2), C.SCL_E_INVALID),
+    (dict(bc_user=1, mthbc=(0, 1)), C.SCL_E_UNSUPPORTED),                        # the wall needs aux rho
+    (dict(rp=S.RP_SW2D, meqn=None, mwaves=None, my=8, dy=0.1, mthbc=(0, 1, 1, 1), bc_user=1), C.SCL_E_UNSUPPORTED),
     (dict(mthbc=(2, 1)), C.SCL_E_INVALID),
     (dict(time_integrator=5), C.SCL_E_INVALID),
     (dict(tfluct_solver=1), C.SCL_E_INVALID),   # Euler has no tfluct plugin

@@ -358,3 +358,65 @@ def test_stegoton_small_strain_is_linear_acoustics():
     assert scale > 0
     assert np.abs(dqn[:, 3:-3] - dql[:, 3:-3]).max() <= 1e-5 * scale
     assert abs(cfln - cfll) <= 1e-5 * cfll
+
+
+# ---- user bc: apps/elasticity/stegoton/bc1.f (oscillating wall, switch to periodic) ----
+
+def test_oscillating_wall_ghosts_known_answer():
+    """bc1.f:100-106 at t: ghost cells mirror cells 1..3, with ghost momentum
+    2 v rho(ibc) - q2(ibc), v = -a1 (1 + cos(pi (t - t1)/tw1)); extrapolation
+    on the right (bc1.f:210-215)."""
+    po, _, q, aux = cases.stegoton_wall(mx=48, wall=(1.0, 0.1, 1.0, 0.0, 0.0, 1.0))
+    q = np.random.default_rng(3).standard_normal(q.shape)
+    t = 1.3
+    qg, _, _ = O.step(po, q, aux, 0.01, t)
+    v = -(0.1 * (1.0 + np.cos(np.pi * (t - 1.0) / 1.0)))
+    for ibc in (1, 2, 3):
+        assert qg[0, 3 - ibc] == q[0, 2 + ibc]
+        assert qg[1, 3 - ibc] == 2.0 * v * aux[0, 2 + ibc] - q[1, 2 + ibc]
+        assert qg[0, 48 + 2 + ibc] == q[0, 48 + 2] and qg[1, 48 + 2 + ibc] == q[1, 48 + 2]
+    # |t - t1| >= tw1: the wall is at rest, a solid wall (bc1.f:130-136)
+    qs, dqs, cs = O.step(po, q, aux, 0.01, 2.5)
+    pw = cases.stegoton_wall(mx=48, mthbc=(3, 1))[0]
+    pw.bc_user = 0
+    qw, dqw, cw = O.step(pw, q, aux, 0.01, 2.5)
+    assert np.array_equal(qs, qw) and np.array_equal(dqs, dqw) and cs == cw
+
+
+def test_user_bc_switch_to_periodic():
+    """bc1.f:31-45: a stage time in (5 tw1, 5 tw1 + 1) makes both sides
+    periodic, q and aux ghosts alike; outside the window nothing changes."""
+    po, _, q, aux = cases.stegoton_wall(mx=48)
+    rng = np.random.default_rng(4)
+    q = rng.standard_normal(q.shape)
+    aux = aux.copy()
+    aux[:, :3] = rng.uniform(1.0, 4.0, (3, 3))   # ghost aux that differs from the periodic image
+    aux[:, -3:] = rng.uniform(1.0, 4.0, (3, 3))
+    aux[2] = 0.0
+    qg, dq, _ = O.step(po, q, aux, 0.01, 5.5)
+    pp = cases.stegoton_wall(mx=48, mthbc=(2, 2))[0]
+    pp.bc_user = 0
+    auxp = aux.copy()
+    auxp[:, :3], auxp[:, -3:] = aux[:, -6:-3], aux[:, 3:6]
+    qp, dqp, _ = O.step(pp, q, auxp, 0.01, 5.5)
+    assert np.array_equal(qg, qp) and np.array_equal(dq, dqp)
+    # a run across the window ends switched; one that stops before does not
+    run = dict(tstart=0.0, dt_initial=0.02, cfl_max=2.5, cfl_desired=2.45, time_integrator=4)
+    _, r1 = O.sharpclaw(po, np.zeros_like(q), cases.stegoton_wall(mx=48)[3], tend=4.0, **run)
+    _, r2 = O.sharpclaw(po, np.zeros_like(q), cases.stegoton_wall(mx=48)[3], tend=5.6, **run)
+    assert r1.bc_switched == 0 and r2.bc_switched == 1
+
+
+def test_oscillating_wall_launches_a_pulse():
+    """From rest, the wall motion of 0 < t < 2 puts a pulse into the medium;
+    vwall = -a1 g0 < 0 pulls the wall away (bc1.f:59, "negative for
+    expansion"), so the strain is mostly positive; by t = 3 the front has travelled
+    about 3 (c = 1 in both layers) and the right part is still at rest."""
+    po, _, q, aux = cases.stegoton_wall(mx=288)
+    qf, res = O.sharpclaw(po, q, aux, tstart=0.0, tend=3.0, dt_initial=0.01, cfl_max=2.5,
+                          cfl_desired=2.45, time_integrator=4)
+    assert res.info == 0 and res.rejected == 0 and res.bc_switched == 0
+    x = (np.arange(288) + 0.5) * po.dx
+    eps = qf[0, 3:-3]
+    assert eps.max() > 0.005 and eps.max() > 10 * -eps.min()
+    assert np.abs(eps[x > 4.5]).max() < 1e-5 * eps.max()
