@@ -84,6 +84,10 @@ extern "C" {
 #define SCL_B4STEP_NONE 0     /* src/b4step.f90: no-op                                      */
 #define SCL_B4STEP_SWIRL 1    /* apps/advection/2d/swirl/b4step.f90: aux = aux0 *
                                  cos(2 pi (t + dt/2) / tperiod); no-op for tperiod = 0     */
+#define SCL_B4STEP_TIME_REVERSAL 2  /* apps/elasticity/stegoton/b4step1.f: once, at the
+                                 first step with told + 1e-10 >= trtime (param), q(:,2) =
+                                 -q(:,2) over every cell; 1-D.  Its time traces
+                                 (fort.17/18/28) are host I/O and are not written      */
 
 /* ---- user boundary conditions (mthbc = 0: the app's own bc1.f, run on the
  * device before every stage, with the stage time) -------------------------- */
@@ -255,8 +259,10 @@ int scl_format_frame(const scl_params* p, const double* q, const double* aux, do
 
 /* Select the b4step hook that scl_sharpclaw / scl_time_steps run on the
  * device before every new (not retaken) time step, as sharpclaw.f90:129 calls
- * b4step; param is the hook's constant (SCL_B4STEP_SWIRL: tperiod).  The aux
- * set by scl_set_aux (now or later) is the hook's base field aux0. */
+ * b4step; param is the hook's constant (SCL_B4STEP_SWIRL: tperiod, and the
+ * aux set by scl_set_aux, now or later, is the hook's base field aux0;
+ * SCL_B4STEP_TIME_REVERSAL: trtime, and the handle remembers that the flip
+ * has happened, as the app's itrdone). */
 int scl_set_b4step(scl_handle* h, int kind, double param);
 
 /* Tile shape of the fused 2-D stage kernel (no counterpart in the reference;

@@ -43,6 +43,7 @@ class Params(ctypes.Structure):
         ("src_term", ctypes.c_int),
         ("rho", ctypes.c_double), ("bulk", ctypes.c_double),
         ("bc_user", ctypes.c_int), ("wall", ctypes.c_double * 6), ("bc_switched", ctypes.c_int),
+        ("trtime", ctypes.c_double), ("b4_done", ctypes.c_int),
     ]
 
 

@@ -1874,6 +1874,12 @@ int ocl_sharpclaw(const ocl_params *p, const ocl_run *run, double *q, const doub
       told = t;
       if (told + dt > tend && tstart < tend) dt = tend - told;
       if (auxw && p->b4step == 1) b4step_swirl(p, aux_in, auxw, na, told, dt);                 /* :129 */
+      /* apps/elasticity/stegoton/b4step1.f:15-21 (1.e-10 is REAL(4)) */
+      if (p->b4step == 2 && p->ndim == 1 && !pl.b4_done && told + (double)1.0e-10f >= p->trtime) {
+        const long ld = p->mx + 2 * p->mbc;
+        for (long i = 0; i < ld; ++i) q[ld + i] = -q[ld + i];
+        pl.b4_done = 1;
+      }
       memcpy(qold, q, sizeof(double) * (size_t)n);
     }
     retake = 0;

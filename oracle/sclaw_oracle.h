@@ -75,13 +75,16 @@ typedef struct {
   double gamma;         /* ratio of specific heats common /param/ gamma,gamma1       */
   double grav;          /* gravity                 common /comrp/ g                  */
   int mthlim[4];        /* TVD limiter per component/field/wave (lim_type = 1)       */
-  int b4step;           /* 0 src/b4step.f90 (no-op), 1 apps/advection/2d/swirl        */
+  int b4step;           /* 0 src/b4step.f90 (no-op), 1 apps/advection/2d/swirl,
+                           2 apps/elasticity/stegoton/b4step1.f (time reversal)       */
   double tperiod;       /* swirl: common /comvt/ tperiod                              */
   int src_term;         /* OCL_SRC_* (1-D)                                            */
   double rho, bulk;     /* homogeneous acoustics: common /cparam/ rho, bulk           */
   int bc_user;          /* 1: apps/elasticity/stegoton/bc1.f replaces src/1d/bc1.f90  */
   double wall[6];       /* t1, a1, tw1 (common /comwall/), t2, a2, tw2                 */
   int bc_switched;      /* the switch to periodic of bc1.f:31-35 has happened         */
+  double trtime;        /* stegoton b4step: common /comtimereverse/ trtime             */
+  int b4_done;          /* ... and its itrdone                                         */
 } ocl_params;
 
 typedef struct {

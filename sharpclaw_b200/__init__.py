@@ -28,7 +28,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _capi as C
-from ._capi import (B4STEP_NONE, B4STEP_SWIRL, BC_USER_NONE, BC_USER_OSCILLATING_WALL, FP32, FP64, FP64_STRICT, MIXED,  # noqa: F401
+from ._capi import (B4STEP_NONE, B4STEP_SWIRL, B4STEP_TIME_REVERSAL, BC_USER_NONE, BC_USER_OSCILLATING_WALL, FP32, FP64, FP64_STRICT, MIXED,  # noqa: F401
                     RP_ACOUSTICS_CONST, RP_ACOUSTICS_FWAVE, RP_ADVECTION_CONS, RP_STEGOTON, RP_TRAFFIC,
                     RP_ACOUSTICS1D, RP_ACOUSTICS2D, RP_ADVECTION, RP_ADVECTION2D, RP_EULER, RP_SW1D, RP_SW2D,
                     RP_SWF_BATHY, RP_SWF_KAPPA, RP_SWF_RADIAL, SRC_BATHYMETRY_SW, SRC_NONE, SRC_RADIAL_SW,
@@ -43,7 +43,8 @@ __all__ = ["ClawParams", "Solver", "Batch", "sharpclaw", "SharpClawError", "read
            "RP_STEGOTON",
            "SRC_NONE", "SRC_RADIAL_SW",
            "SRC_BATHYMETRY_SW", "B4STEP_NONE", "B4STEP_SWIRL",
-           "RUN_AUTO", "RUN_GRAPH", "RUN_RESIDENT", "BC_USER_NONE", "BC_USER_OSCILLATING_WALL"]
+           "RUN_AUTO", "RUN_GRAPH", "RUN_RESIDENT", "BC_USER_NONE", "BC_USER_OSCILLATING_WALL",
+           "B4STEP_TIME_REVERSAL"]
 
 # plugin id -> (meqn, mwaves, maux, ndim)
 PLUGINS = {
@@ -301,8 +302,9 @@ class Solver:
 
     def set_b4step(self, kind: int, param: float = 0.0):
         """Run a b4step hook on the device before every new time step of
-        sharpclaw() (B4STEP_SWIRL: param = tperiod); the aux set with set_aux
-        is the hook's base field."""
+        sharpclaw() (B4STEP_SWIRL: param = tperiod, and the aux set with
+        set_aux is the hook's base field; B4STEP_TIME_REVERSAL: param =
+        trtime, apps/elasticity/stegoton/b4step1.f)."""
         C.check(C.lib().scl_set_b4step(self._h, int(kind), float(param)), "scl_set_b4step")
 
     def wait_frames(self):

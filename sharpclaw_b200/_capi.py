@@ -18,7 +18,7 @@ SRC_NONE, SRC_RADIAL_SW, SRC_BATHYMETRY_SW = 0, 1, 2
 RP_SWF_BATHY, RP_SWF_RADIAL, RP_SWF_KAPPA = 8, 9, 10
 RP_ACOUSTICS_CONST, RP_ACOUSTICS_FWAVE = 11, 12
 RP_TRAFFIC, RP_ADVECTION_CONS, RP_STEGOTON = 13, 14, 15
-B4STEP_NONE, B4STEP_SWIRL = 0, 1
+B4STEP_NONE, B4STEP_SWIRL, B4STEP_TIME_REVERSAL = 0, 1, 2
 BC_USER_NONE, BC_USER_OSCILLATING_WALL = 0, 1
 RUN_AUTO, RUN_GRAPH, RUN_RESIDENT = 0, 1, 2
 FP64, FP64_STRICT, MIXED, FP32 = 0, 1, 2, 3

@@ -73,6 +73,23 @@ __global__ void k_bc1(S* q, long plane, int mx, int meqn, int bl, int br) {
   else if (br == 3) at(mx + ibc) = (m == 1) ? -at(mx + 1 - ibc) : at(mx + 1 - ibc);
 }
 
+// apps/elasticity/stegoton/b4step1.f: on a new step with told + 1e-10 >=
+// trtime (1.e-10 is a REAL(4) literal), and only once (itrdone of
+// /comtimereverse/), negate the momentum over every cell, ghosts included.
+// One CTA: thread 0 decides, all flip, thread 0 records it.
+template <class S>
+__global__ void k_b4step_reverse(StageArgs a, int ld, double trtime) {
+  Ctl* c = a.ctl;
+  __shared__ int go;
+  if (threadIdx.x == 0)
+    go = !c->done && c->fresh && !c->b4_done && c->told + (double)1.0e-10f >= trtime;
+  __syncthreads();
+  if (!go) return;
+  S* q = static_cast<S*>(a.buf[c->role[ROLE_Q]]) + a.plane;   // component 2
+  for (int i = threadIdx.x; i < ld; i += blockDim.x) q[i] = -q[i];
+  if (threadIdx.x == 0) c->b4_done = 1;
+}
+
 // apps/elasticity/stegoton/bc1.f, g0: 1 + cos(pi s) on |s| < 1 (pi = 4 atan(1))
 __device__ __forceinline__ double wall_g0(double s) {
   return fabs(s) < 1.0 ? 1.0 + cos(3.141592653589793 * s) : 0.0;
@@ -362,6 +379,10 @@ int enqueue_step(scl_handle* h, bool first = true, bool last = true) {
     else
       k_b4step_swirl<float><<<148, 256, 0, h->stream>>>(h->ctl, static_cast<float*>(h->aux),
                                                         static_cast<const float*>(h->aux0), n, h->b4param);
+  } else if (h->b4kind == SCL_B4STEP_TIME_REVERSAL) {
+    const StageArgs a = make_args(h, 0);
+    if (h->ssize == sizeof(double)) k_b4step_reverse<double><<<1, 256, 0, h->stream>>>(a, (int)h->ld, h->b4param);
+    else k_b4step_reverse<float><<<1, 256, 0, h->stream>>>(a, (int)h->ld, h->b4param);
   }
   int rc = enqueue_stages(h);
   if (rc) return rc;
@@ -682,11 +703,14 @@ int scl_set_aux(scl_handle* h, const double* aux) {
 
 int scl_set_b4step(scl_handle* h, int kind, double param) {
   if (!h) return fail(SCL_E_INVALID, "null handle");
-  if (kind != SCL_B4STEP_NONE && kind != SCL_B4STEP_SWIRL) return fail(SCL_E_UNSUPPORTED, "unknown b4step hook");
+  if (kind != SCL_B4STEP_NONE && kind != SCL_B4STEP_SWIRL && kind != SCL_B4STEP_TIME_REVERSAL)
+    return fail(SCL_E_UNSUPPORTED, "unknown b4step hook");
   if (kind == SCL_B4STEP_SWIRL && (h->p.rp != SCL_RP_ADVECTION2D || h->p.maux < 2))
     return fail(SCL_E_INVALID, "the swirl b4step scales the edge velocities of SCL_RP_ADVECTION2D");
+  if (kind == SCL_B4STEP_TIME_REVERSAL && (h->p.ndim != 1 || h->p.meqn < 2))
+    return fail(SCL_E_INVALID, "the time-reversal b4step negates component 2 of a 1-D grid");
   CK(cudaStreamSynchronize(h->stream));
-  if (kind != SCL_B4STEP_NONE && !h->aux0) {
+  if (kind == SCL_B4STEP_SWIRL && !h->aux0) {
     const size_t bytes = h->ssize * h->plane * h->p.maux;
     CK(cudaMalloc(&h->aux0, bytes));
     CK(cudaMemcpyAsync(h->aux0, h->aux, bytes, cudaMemcpyDeviceToDevice, h->stream));

@@ -61,6 +61,7 @@ struct __align__(16) Ctl {
   int accept_always;            // single-step mode (scl_rk_step): no dt update, always accept
   int fresh;                    // 1: the current step is a new one (b4step runs), 0: a retake
   int bc_switched;              // the user bc switched both sides to periodic (persistent)
+  int b4_done;                  // the time-reversal b4step has fired (persistent)
 };
 
 // Physics constants of the plugins (COMMON blocks /comrp/, /param/).

@@ -74,16 +74,17 @@ def acoustics1d(mx=200, rho=(1.0, 4.0), c=(1.0, 0.5), char_decomp=0, tfluct_solv
     return po, ps, q, aux
 
 
-def stegoton_wall(mx=288, upper=6.0, wall=(1.0, 0.01, 1.0, 0.0, 0.0, 1.0), mthbc=(0, 1), char_decomp=0):
+def stegoton_wall(mx=288, upper=6.0, wall=(1.0, 0.1, 1.0, 0.0, 0.0, 1.0), mthbc=(0, 1), char_decomp=0):
     """apps/elasticity/stegoton as its sharpclaw.data runs it: q = 0, the
     oscillating wall of bc1.f at xlower (mthbc 0) and extrapolation at xupper,
     the switch to periodic when a stage time enters (5 tw1, 5 tw1 + 1).  The
     app's wall (t1 = 10, a1 = 0.1, tw1 = 10 on [0, 150]) is scaled to
     t1 = tw1 = 1 on [0, upper] so the pulse, its travel and the switch fit a
-    short run, with a1 = 0.01: the ten times faster ramp at a1 = 0.1 drives
-    the exponential stress law into blow-up; 48 cells per layer period as the
-    app's mx = 7200.  Layers as setaux.f: ix = xcell truncates toward zero,
-    so the ghost cells left of x = 0 are layer A."""
+    short run; a1 = 0.1 as the app; 48 cells per layer period as the app's
+    mx = 7200.  Layers as setaux.f: ix = xcell truncates toward zero, so the
+    ghost cells left of x = 0 are layer A, the mirror image of cells 1..3 --
+    a wall between unlike materials (floor instead of truncation) feeds
+    energy into the reflected wave and the run blows up."""
     po, ps, q, aux = stegoton(mx=mx, char_decomp=char_decomp, mthbc=mthbc, amp=0.0)
     dx = upper / mx
     xa = (np.arange(-3, mx + 3) + 0.5) * dx
@@ -350,7 +351,7 @@ def stegoton(mx=200, char_decomp=0, tfluct_solver=1, mthbc=(1, 1), amp=0.05):
     lower, upper = 0.0, 30.0
     dx = (upper - lower) / mx
     xa = lower + (np.arange(-3, mx + 3) + 0.5) * dx
-    frac = xa - np.floor(xa)
+    frac = xa - np.trunc(xa)     # setaux.f: ix = xcell truncates toward zero
     rho = np.where(frac < 0.5, 1.0, 4.0)
     K = np.where(frac < 0.5, 1.0, 4.0)
     aux = np.ascontiguousarray(np.stack([rho, K, np.zeros_like(xa)]))

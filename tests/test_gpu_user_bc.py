@@ -1,4 +1,6 @@
-"""The user boundary condition of apps/elasticity/stegoton/bc1.f on a GPU
+"""The stegoton's hooks on a GPU: its b4step1.f time reversal
+(SCL_B4STEP_TIME_REVERSAL) and the user boundary condition of
+apps/elasticity/stegoton/bc1.f
 (SCL_BC_USER_OSCILLATING_WALL): an oscillating wall at xlower (mthbc 0)
 driven at each stage's time, extrapolation at xupper, and the switch of both
 sides to periodic once a stage time enters (5 tw1, 5 tw1 + 1).  Compared with
@@ -83,3 +85,47 @@ def test_user_bc_refused_where_not_built():
             s.set_aux(aux)
             s.set_q(q)
             s.sharpclaw(0.0, 0.1, 0.01, 2.5, 2.45)
+
+
+@pytest.mark.parametrize("precision", ["fp64_strict", "fp64"])
+def test_time_reversal_run_parity(precision):
+    """Layered medium, strain 0.02 (nonlinear), periodic, variable dt: the flip
+    at the first step from t = 2.5 on, then a second call that must not flip
+    again (itrdone of /comtimereverse/ is kept by the handle)."""
+    po, ps, q, aux = cases.stegoton(mx=400, amp=0.02, mthbc=(2, 2))
+    ps.time_integrator = 4
+    run = dict(dt_initial=0.01, cfl_max=2.5, cfl_desired=2.45)
+    po.b4step, po.trtime = 2, 2.5
+    qo, ro = O.sharpclaw(po, q, aux, tstart=0.0, tend=5.0, time_integrator=4, **run)
+    po.b4_done = 1
+    qo2, ro2 = O.sharpclaw(po, qo, aux, tstart=5.0, tend=6.0, time_integrator=4, **run)
+    with S.Solver(ps, precision) as s:
+        s.set_aux(aux)
+        s.set_b4step(S.B4STEP_TIME_REVERSAL, 2.5)
+        s.set_q(q)
+        res = s.sharpclaw(0.0, 5.0, run["dt_initial"], run["cfl_max"], run["cfl_desired"])
+        q1 = s.get_q()
+        res2 = s.sharpclaw(5.0, 6.0, run["dt_initial"], run["cfl_max"], run["cfl_desired"])
+        q2 = s.get_q()
+    assert res["steps_taken"] == ro.steps_taken and res2["steps_taken"] == ro2.steps_taken
+    assert _rel(q1[:, 3:-3], qo[:, 3:-3]) <= 10 * TOL[precision]
+    assert _rel(q2[:, 3:-3], qo2[:, 3:-3]) <= 10 * TOL[precision]
+
+
+def test_time_reversal_restores_the_pulse():
+    """The known answer of the oracle test on the device, in the FMA form.  (The
+    mixed form evaluates exp(K eps) - 1 in FP32, which at strain 1e-4 cancels
+    to ~6e-8 absolute error, a 1 % offset of this pulse: a limit of that form
+    for the stegoton law at small strain, not of the hook.)"""
+    _, ps, q, _ = cases.stegoton(mx=600, amp=1e-4, mthbc=(2, 2))
+    aux = np.ascontiguousarray(np.stack([np.ones(606), np.ones(606), np.zeros(606)]))
+    ps.time_integrator = 4
+    with S.Solver(ps, "fp64") as s:
+        s.set_aux(aux)
+        s.set_b4step(S.B4STEP_TIME_REVERSAL, 5.0)
+        s.set_q(q)
+        r = s.sharpclaw(0.0, 10.0, 1 / 32, 2.5, 2.45, dt_variable=0)
+        qf = s.get_q()
+    scale = np.abs(q[0, 3:-3]).max()
+    assert r["info"] == 0
+    assert np.abs(qf[0, 3:-3] - q[0, 3:-3]).max() <= 2e-6 * scale

@@ -420,3 +420,24 @@ def test_oscillating_wall_launches_a_pulse():
     eps = qf[0, 3:-3]
     assert eps.max() > 0.005 and eps.max() > 10 * -eps.min()
     assert np.abs(eps[x > 4.5]).max() < 1e-5 * eps.max()
+
+
+def test_time_reversal_returns_the_pulse():
+    """apps/elasticity/stegoton/b4step1.f negates the momentum once, at the
+    first step with t + 1e-10 >= trtime.  In a homogeneous medium at strain
+    1e-4 (linear), periodic, with dt = 1/32 so a step starts exactly at
+    trtime = 5, the wave runs back and at t = 10 the initial pulse is
+    restored to 5e-7 (without the flip it has moved away: error 1)."""
+    po, _, q, _ = cases.stegoton(mx=600, amp=1e-4, mthbc=(2, 2))
+    aux = np.ascontiguousarray(np.stack([np.ones(606), np.ones(606), np.zeros(606)]))
+    run = dict(tstart=0.0, tend=10.0, dt_initial=1 / 32, cfl_max=2.5, cfl_desired=2.45, dt_variable=0,
+               time_integrator=4)
+    po.b4step, po.trtime = 2, 5.0
+    qf, r = O.sharpclaw(po, q, aux, **run)
+    scale = np.abs(q[0, 3:-3]).max()
+    assert r.info == 0
+    assert np.abs(qf[0, 3:-3] - q[0, 3:-3]).max() <= 2e-6 * scale
+    assert np.abs(qf[1, 3:-3]).max() <= 2e-7 * scale
+    po.b4step = 0
+    qn, _ = O.sharpclaw(po, q, aux, **run)
+    assert np.abs(qn[0, 3:-3] - q[0, 3:-3]).max() >= 0.5 * scale
