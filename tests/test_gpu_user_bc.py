@@ -113,14 +113,29 @@ def test_time_reversal_run_parity(precision):
 
 
 def test_time_reversal_restores_the_pulse():
-    """The known answer of the oracle test on the device, in the FMA form.  (The
-    mixed form evaluates exp(K eps) - 1 in FP32, which at strain 1e-4 cancels
-    to ~6e-8 absolute error, a 1 % offset of this pulse: a limit of that form
-    for the stegoton law at small strain, not of the hook.)"""
+    """The known answer of the oracle test on the device, in the FMA form."""
     _, ps, q, _ = cases.stegoton(mx=600, amp=1e-4, mthbc=(2, 2))
     aux = np.ascontiguousarray(np.stack([np.ones(606), np.ones(606), np.zeros(606)]))
     ps.time_integrator = 4
     with S.Solver(ps, "fp64") as s:
+        s.set_aux(aux)
+        s.set_b4step(S.B4STEP_TIME_REVERSAL, 5.0)
+        s.set_q(q)
+        r = s.sharpclaw(0.0, 10.0, 1 / 32, 2.5, 2.45, dt_variable=0)
+        qf = s.get_q()
+    scale = np.abs(q[0, 3:-3]).max()
+    assert r["info"] == 0
+    assert np.abs(qf[0, 3:-3] - q[0, 3:-3]).max() <= 2e-6 * scale
+
+
+def test_time_reversal_restores_the_pulse_mixed():
+    """The same in the mixed form, whose FP32 stress is expm1f(K eps): no
+    cancellation at strain 1e-4 (exp(K eps) - 1 in FP32 left a 1.1e-2 error;
+    expm1f gives 5.0e-7, as FP64)."""
+    _, ps, q, _ = cases.stegoton(mx=600, amp=1e-4, mthbc=(2, 2))
+    aux = np.ascontiguousarray(np.stack([np.ones(606), np.ones(606), np.zeros(606)]))
+    ps.time_integrator = 4
+    with S.Solver(ps, "mixed") as s:
         s.set_aux(aux)
         s.set_b4step(S.B4STEP_TIME_REVERSAL, 5.0)
         s.set_q(q)
