@@ -134,7 +134,14 @@ __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
   if (!(v > 0.0) && v == v) return;  // +0/-0 never raise the max
   unsigned long long bits = __double_as_longlong(v);
   if (v != v) bits = 0x7ff8000000000000ULL;
-  atomicMax(reinterpret_cast<unsigned long long*>(addr), bits);
+  unsigned long long* p = reinterpret_cast<unsigned long long*>(addr);
+  // Every tile of a smooth field carries nearly the same maximum, and one
+  // atomic per tile on a single word serialises a large grid.  The slot only
+  // grows during a launch, so a read that already shows >= bits makes the
+  // atomic redundant; a stale read can only cost a redundant atomic.  A
+  // volatile generic load (global or shared slot) bypasses L1.
+  if (*reinterpret_cast<volatile unsigned long long*>(p) >= bits) return;
+  atomicMax(p, bits);
 }
 
 template <class T>

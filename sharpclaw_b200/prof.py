@@ -44,7 +44,19 @@ def sw2d(n):
     return p, q, None, 0.4 * d
 
 
-WORKLOADS = {"euler1d": euler1d, "sw2d": sw2d}
+def advection1d(mx):
+    """Scalar advection on [0,1], periodic, u = 1 (apps/advection/1d): the
+    lightest physics -- componentwise WENO5, Godunov rp, tfluct, SSPRK(3,3)."""
+    dx = 1.0 / mx
+    xc = (np.arange(mx) + 0.5) * dx
+    q = np.zeros((1, mx + 6))
+    q[0, 3:-3] = np.exp(-200.0 * (xc - 0.3) ** 2) + ((xc > 0.6) & (xc < 0.8))
+    p = S.ClawParams(rp=S.RP_ADVECTION, mx=mx, dx=dx, mthbc=(2, 2), char_decomp=0, tfluct_solver=1,
+                     time_integrator=3)
+    return p, q, None, 0.8 * dx
+
+
+WORKLOADS = {"euler1d": euler1d, "sw2d": sw2d, "advection1d": advection1d}
 
 
 def main():
