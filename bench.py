@@ -99,6 +99,17 @@ def cpu_cores():
         return os.cpu_count() or 1
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
 # --------------------------------------------------------------------------
 # clocks sampler (nvidia-smi during the timed region)
 # --------------------------------------------------------------------------
@@ -161,7 +172,7 @@ def run_reference(args, rank, world):
         return 0
     import multiprocessing as mp
     cores = cpu_cores()
-    sample_mx = 1 << 17
+    sample_mx = MX                      # the headline grid itself
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
         pool.map(_oracle_one, [(1024, 1)] * cores)  # import + warm the workers
@@ -176,14 +187,15 @@ def run_reference(args, rank, world):
             rates.append(sum(n for n, _ in out) / wall)
     value = sum(rates) / len(rates)
     ms = 1000.0 * sum(walls) / len(walls)
-    sample = (f"{cores} independent processes, each one SSPRK(10,4) time step of the same "
-              f"Shu-Osher problem at mx=2^17 (C restatement of the reference, gcc -O2, no FMA)")
+    sample = (f"{cores} independent processes on {cores} host cores ({cpu_model()}), each one "
+              f"SSPRK(10,4) time step of the headline Shu-Osher grid, mx=2^20 (C restatement of the "
+              f"reference, gcc -O2, no FMA)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config({"sample_mx": sample_mx}),
+            "config": config({"sample_mx": sample_mx, "host_cpu": cpu_model()}),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": sample},
+                             "sample": sample, "cpu_model": cpu_model()},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -218,6 +230,16 @@ def job_rate(units, seconds, world, device):
     return sum_over_ranks(units, world, device) / tmax, tmax
 
 
+def oracle_params(ps):
+    """The oracle's parameter struct for the same run as ClawParams ps."""
+    from oracle import oracle as O
+    return O.make_params(ndim=ps.ndim, mx=ps.mx, my=ps.my, meqn=ps.meqn, mwaves=ps.mwaves, mbc=ps.mbc,
+                         maux=ps.maux, mcapa=ps.mcapa, char_decomp=ps.char_decomp, tfluct_solver=ps.tfluct_solver,
+                         mthbc=tuple(ps.mthbc), dx=ps.dx, dy=ps.dy, xlower=ps.xlower, ylower=ps.ylower, rp=ps.rp,
+                         efix=ps.efix, u=ps.u, gamma=ps.gamma, grav=ps.grav, lim_type=ps.lim_type,
+                         mthlim=tuple(ps.mthlim), src_term=ps.src_term, rho=ps.rho, bulk=ps.bulk)
+
+
 def shu_osher_params(S, mx, dx):
     return S.ClawParams(rp=S.RP_EULER, mx=mx, dx=dx, xlower=-5.0, gamma=GAMMA, mthbc=(1, 1),
                         char_decomp=2, tfluct_solver=0, time_integrator=4)
@@ -236,7 +258,7 @@ def workloads():
         q, dx = shu_osher(MX)
         return dict(params=shu_osher_params(S, MX, dx), q=q, aux=None, dt0=DT0, cfl=(CFL_MAX, CFL_DESIRED),
                     dt_variable=1, tend=1e30, nstep=NSTEP, cells=MX, stages=10, bytes_cell_stage=2.3 * 3 * 8,
-                    desc=WORKLOAD, traffic_key="k_stage1d_euler_charwise_mixed")
+                    desc=WORKLOAD, traffic_key="k_stage1d_euler_charwise_mixed", oracle_steps=2)
 
     def c1():
         mx = 1000
@@ -254,7 +276,8 @@ def workloads():
         return dict(params=p, q=q, aux=None, dt0=0.8 * dx, cfl=(0.85, 0.8), dt_variable=1, tend=1.0,
                     nstep=2000, cells=mx, stages=3, bytes_cell_stage=8.0 / 3.0 * 8,
                     desc="1-D advection a=1, periodic [0,1], mx=1000, WENO5 componentwise + Godunov rp, "
-                         "tfluct, SSPRK3, cfl 0.8/0.85, full run to t=1 per step", traffic_key=None)
+                         "tfluct, SSPRK3, cfl 0.8/0.85, full run to t=1 per step", traffic_key=None,
+                    oracle_steps=20)
 
     def c3():
         n = 4096
@@ -270,7 +293,7 @@ def workloads():
                     nstep=5, cells=n * n, stages=3, bytes_cell_stage=8.0 / 3.0 * 3 * 8,
                     desc="2-D shallow water g=1, radial dam break h=2 in r<0.5 else 1 + N(0,1e-3), "
                          "4096x4096 periodic on [-2.5,2.5]^2, Roe rpn2 + tfluct, char-wise WENO5, SSPRK3, "
-                         "cfl 0.45/0.5", traffic_key="k_stage2d_sw_charwise_mixed")
+                         "cfl 0.45/0.5", traffic_key="k_stage2d_sw_charwise_mixed", oracle_steps=1)
 
     def c5():
         n = 1024
@@ -301,7 +324,8 @@ def workloads():
                     nstep=20, cells=n * n, stages=3, bytes_cell_stage=8.0 / 3.0 * 3 * 8 + 2 * 8,
                     desc="2-D variable-coefficient acoustics 1024x1024 periodic, rho,K log-normal(0,0.3) "
                          "smoothed (periodic), p0 = 4 Gaussian bumps + 0.05 cos cos, WENO5 componentwise + "
-                         "rpn2/tfluct, SSPRK3, fixed dt, 20 steps per step", traffic_key=None)
+                         "rpn2/tfluct, SSPRK3, fixed dt, 20 steps per step", traffic_key=None,
+                    oracle_steps=2)
 
     return {"c2": c2, "c1": c1, "c3": c3, "c5": c5}
 
@@ -374,6 +398,13 @@ def run_gpu(args, rank, world, local_rank):
                 traffic_per_cell = json.load(f)[W["traffic_key"]]["dram_bytes_per_cell"]
         except Exception:
             traffic_per_cell = None
+    counters = {}
+    if W["traffic_key"]:
+        try:
+            with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+                counters = json.load(f)
+        except Exception:
+            counters = {}
     roof = {}
     for name, s in (("headline", s_mix), ("fp64", s_64)):
         st_ms, n_launch = s.time_stages(res_mix["dt_last"], 20)
@@ -385,6 +416,13 @@ def run_gpu(args, rank, world, local_rank):
                       "traffic": (traffic_per_cell * W["cells"]) if traffic_per_cell else None,
                       "avg_launch_us": avg_ms * 1000.0, "algorithmic_bytes_per_launch": bytes_per_launch,
                       "peak_source": peak_kind}
+        # the issue-slot ceiling of the same kernel: warp instructions per
+        # cell-stage (ncu capture of the kernel, profiles/) at the measured
+        # launch rate, against 4 schedulers x SMs x the SM clock under load
+        key = W["traffic_key"] and W["traffic_key"].replace("_mixed", "_" + ("fp64" if name == "fp64" else args.precision))
+        wi = counters.get(key, {}).get("warp_inst_per_cell") if key else None
+        roof[name]["compute_key"] = key
+        roof[name]["warp_inst_per_cell_stage"] = wi
 
     # end to end through the public API with host buffers
     qh = torch.from_numpy(q0.copy()).pin_memory()
@@ -413,35 +451,65 @@ def run_gpu(args, rank, world, local_rank):
     e2e, e2e_s = job_rate(W["cells"] * W["stages"] * e2e_taken, e2e_local, world, dev)
     nbytes = q0.nbytes
 
-    # accuracy: the headline form against FP64 in the reference's operation
-    # order (fp64_strict) after 20 fixed-dt steps
+    # accuracy against the oracle (the C restatement of the reference, run
+    # here on one host core) over a short fixed-dt window of the same grid,
+    # and against the GPU's FP64_STRICT form (bit for bit the oracle, by the
+    # GPU tests) over a longer one
     acc = {}
     if rank == 0:
-        outs = {}
-        dt = W["dt0"]
-        for name in ("fp64_strict", args.precision, "fp64"):
+        from oracle import oracle as O
+
+        def inner(q):
+            return q[:, 3:-3] if ps.ndim == 1 else q[:, 3:-3, 3:-3]
+
+        def rel_l1(a, b):
+            return max(float(np.abs(a[m] - b[m]).sum() / max(np.abs(b[m]).sum(), 1e-300)) for m in range(a.shape[0]))
+
+        def rel_linf(a, b):
+            return float(np.abs(a - b).max() / np.abs(b).max())
+
+        def gpu_run(name, nsteps):
             with S.Solver(ps, name) as s:
                 if aux0 is not None:
                     s.set_aux(aux0)
                 s.set_q(q0)
-                s.sharpclaw(0.0, 20 * dt, dt, 1e9, 0.5, dt_variable=0)
-                q = s.get_q()
-                outs[name] = q[:, 3:-3] if ps.ndim == 1 else q[:, 3:-3, 3:-3]
+                s.sharpclaw(0.0, nsteps * dt, dt, 1e9, 0.5, dt_variable=0)
+                return inner(s.get_q())
+
+        dt = W["dt0"]
+        n_or = W["oracle_steps"]
+        t0 = time.perf_counter()
+        qo, _ = O.sharpclaw(oracle_params(ps), q0, aux0, tstart=0.0, tend=n_or * dt, dt_initial=dt, cfl_max=1e9,
+                            cfl_desired=0.5, dt_variable=0, time_integrator=ps.time_integrator)
+        oracle_s = time.perf_counter() - t0
+        b = inner(qo)
+        vs_oracle = {"steps": n_or, "dt": dt, "oracle_seconds": oracle_s}
+        for name in (args.precision, "fp64", "fp64_strict"):
+            a = gpu_run(name, n_or)
+            vs_oracle[name] = {"rel_l1": rel_l1(a, b), "rel_linf": rel_linf(a, b),
+                               "bitwise_equal": bool(np.array_equal(a, b))}
+        outs = {name: gpu_run(name, 20) for name in ("fp64_strict", args.precision, "fp64")}
         a, b = outs[args.precision], outs["fp64_strict"]
-        nc = a.shape[0]
-        acc = {"rel_l1_vs_fp64_strict": max(float(np.abs(a[m] - b[m]).sum() / max(np.abs(b[m]).sum(), 1e-300))
-                                     for m in range(nc)),
-               "rel_linf_vs_fp64_strict": float(np.abs(a - b).max() / np.abs(b).max()),
-               "fp64_rel_linf_vs_fp64_strict": float(np.abs(outs["fp64"] - b).max() / np.abs(b).max()),
-               "steps": 20, "dt": dt}
+        acc = {"vs_oracle": vs_oracle,
+               "rel_l1_vs_fp64_strict": rel_l1(a, b), "rel_linf_vs_fp64_strict": rel_linf(a, b),
+               "fp64_rel_linf_vs_fp64_strict": rel_linf(outs["fp64"], b), "steps": 20, "dt": dt}
 
     # CPU baseline: the oracle on a bounded sample, one core (C2 only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and args.workload == "c2":
-        n, t = _oracle_one((1 << 18, 2))
-        cpu = {"value": n / t, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": "mx=2^18 Shu-Osher, 2 SSPRK(10,4) time steps, C restatement of the reference "
-                         "(gcc -O2, no FMA), single thread"}
+        n, t = _oracle_one((MX, 1))
+        cpu = {"value": n / t, "unit": UNIT, "cores": 1, "kind": "port", "cpu_model": cpu_model(),
+               "sample": "the headline grid, mx=2^20 Shu-Osher, 1 SSPRK(10,4) time step, C restatement of the "
+                         "reference (gcc -O2, no FMA), single thread"}
+
+    # the batched workload (2048 Riemann problems), a short window, in the
+    # same process: FP32 batch against plain FP64 run one grid at a time
+    batched = None
+    if args.workload == "c2" and not args.no_batched:
+        batched, bout = batch_measure(args, world, dev, C4_BLOCK_TEND, 3, 1, clocks, flush, e2e=False,
+                                      one_at_a_time=24)
+        for v in bout.values():
+            v["batch"].close()
 
     adj = None
     if args.workload == "c5" and rank == 0:
@@ -452,6 +520,17 @@ def run_gpu(args, rank, world, local_rank):
     run_mode, run_launches = s_mix.timed_run_record
     launches = run_launches * args.steps
     ck = clocks.summary()
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    for name, r in roof.items():
+        wi = r.pop("warp_inst_per_cell_stage")
+        key = r.pop("compute_key")
+        if wi and ck.get("sm_mhz"):
+            rate = W["cells"] / (r["avg_launch_us"] * 1e-6)     # cell-stages per second of the kernel
+            ach = wi * rate
+            pk = nsm * 4 * ck["sm_mhz"] * 1e6
+            r["compute"] = {"bound": "issue", "unit": "warp-instructions/s", "achieved": ach, "peak": pk,
+                            "frac": ach / pk, "warp_inst_per_cell_stage": wi, "counters": key,
+                            "peak_is": f"{nsm} SMs x 4 schedulers x median SM clock under load"}
     if rank == 0:
         cfg = {"workload": W["desc"], "cells": W["cells"], "time_steps_per_step": nstep,
                "stages_per_time_step": W["stages"], "precision": args.precision,
@@ -478,6 +557,8 @@ def run_gpu(args, rank, world, local_rank):
                 "clocks": ck}
         if adj is not None:
             line["adjoint"] = adj
+        if batched is not None:
+            line["batched"] = batched
         print(json.dumps(line), flush=True)
     s_mix.close()
     s_64.close()
@@ -559,48 +640,50 @@ def c4_instances(n=2048, seed=4):
     return mx, 1.0 / mx.astype(np.float64), qs, np.array(dt0)
 
 
-def run_gpu_batch(args, rank, world, local_rank):
-    """C4: the batched FP32 solver against plain FP64 grids run one at a time."""
+C4_BLOCK_TEND = 0.001   # window of the batched block inside the default (headline) run
+
+
+def batch_measure(args, world, dev, tend, steps, warmup, clocks, flush, e2e=True, one_at_a_time=48):
+    """The batched workload (2048 Riemann problems) over t in [0, tend]: the
+    batched solver in the FP32 form (the headline of this workload), the mixed
+    form, FP64 and FP64_STRICT (the oracle's operation order: bit for bit the
+    oracle's sharpclaw() per instance, by the GPU tests), plus FP64 run one
+    grid at a time on a seeded sample.  Device time with CUDA events, L2
+    flushed between timed runs.  Returns a dict of rates, accuracy (per
+    instance, largest relative L1 over the components against the FP64_STRICT
+    batch) and the batches (open; the caller closes them)."""
     import numpy as np
     import torch
-    import torch.distributed as dist
     import sharpclaw_b200 as S
-
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
     mx, dx, qs, dt0 = c4_instances()
     ps = S.ClawParams(rp=S.RP_EULER, mx=10, dx=0.1, mthbc=(1, 1), char_decomp=0, tfluct_solver=0,
                       time_integrator=3, gamma=GAMMA)
     cfl_max, cfl_des = 0.9, 0.8
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def barrier():
         torch.cuda.synchronize()
         if world > 1:
+            import torch.distributed as dist
             dist.barrier()
         torch.cuda.synchronize()
 
     def cell_stages(res):
         return sum(int(mx[k]) * 3 * (r["steps_taken"] - r["rejected"]) for k, r in enumerate(res))
 
-    clocks = Clocks(local_rank)
     out = {}
-    head = args.precision if args.precision != "mixed" else "fp32"
-    # fp64_strict (the reference's operation order) is the accuracy reference
-    forms = [head] + (["mixed"] if head == "fp32" else []) + ["fp64", "fp64_strict"]
-    for precision in forms:
+    for precision in ("fp32", "mixed", "fp64", "fp64_strict"):
         b = S.Batch(ps, mx, dx, precision=precision)
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             b.set_q(qs)
-            b.sharpclaw(0.0, C4_TEND, dt0, cfl_max, cfl_des)
+            b.sharpclaw(0.0, tend, dt0, cfl_max, cfl_des)
         barrier()
         tot_ms, tot_cells, tot_launch = 0.0, 0, 0
         with clocks:
-            for _ in range(args.steps):
+            for _ in range(steps):
                 b.set_q(qs)
                 flush.zero_()
                 torch.cuda.synchronize()
-                res, ms = b.sharpclaw(0.0, C4_TEND, dt0, cfl_max, cfl_des)
+                res, ms = b.sharpclaw(0.0, tend, dt0, cfl_max, cfl_des)
                 tot_ms += ms
                 tot_cells += cell_stages(res)
                 tot_launch += b.launches()
@@ -611,96 +694,106 @@ def run_gpu_batch(args, rank, world, local_rank):
         rate, s_max = job_rate(tot_cells, tot_ms / 1000.0, world, dev)
         out[precision] = dict(batch=b, ms=1000.0 * s_max, cells=tot_cells, rate=rate, res=res, tune=b.tuning(),
                               failed=failed, launches=tot_launch)
-    value = out[head]["rate"]
-    value64_batched = out["fp64"]["rate"]
 
-    # plain FP64 path with the instances run one at a time (a seeded sample of 48)
+    # plain FP64 path with the instances run one at a time (a seeded sample)
     rng = np.random.default_rng(44)
-    sample = rng.choice(len(mx), 48, replace=False)
+    sample = rng.choice(len(mx), one_at_a_time, replace=False)
     one_ms, one_cells = 0.0, 0
     for k in sample:
         p1 = S.ClawParams(rp=S.RP_EULER, mx=int(mx[k]), dx=float(dx[k]), mthbc=(1, 1), char_decomp=0,
                           tfluct_solver=0, time_integrator=3, gamma=GAMMA)
         with S.Solver(p1, "fp64") as s:
             s.set_q(qs[k])
-            ms, r = s.time_steps(200000, float(dt0[k]), cfl_max, cfl_des, tend=C4_TEND)
+            ms, r = s.time_steps(200000, float(dt0[k]), cfl_max, cfl_des, tend=tend)
             one_ms += ms
             one_cells += int(mx[k]) * 3 * (r["steps_taken"] - r["rejected"])
-    value64_one = one_cells / (one_ms / 1000.0)
+    one_rate, _ = job_rate(one_cells, one_ms / 1000.0, world, dev)
 
-    # accuracy of the FP32-arithmetic forms against the FP64 batch in the
-    # reference's operation order at the window's end: per instance the
-    # largest relative L1 over the components
     ref = out["fp64_strict"]["batch"].get_q()
 
-    def rel_l1_of(form):
+    def accuracy(form):
         got = out[form]["batch"].get_q()
         bad = set(out[form]["failed"]) | set(out["fp64_strict"]["failed"])
-        e = [max(float(np.abs(g[m, 3:-3] - f[m, 3:-3]).sum() / np.abs(f[m, 3:-3]).sum()) for m in range(3))
-             for k, (g, f) in enumerate(zip(got, ref)) if k not in bad]
-        e = np.asarray(e)
-        return float(np.max(e)), float(np.median(e)), int((e > 1e-5).sum()), len(e)
+        e = np.asarray([max(float(np.abs(g[m, 3:-3] - f[m, 3:-3]).sum() / np.abs(f[m, 3:-3]).sum())
+                            for m in range(3)) for k, (g, f) in enumerate(zip(got, ref)) if k not in bad])
+        return {"rel_l1_vs_fp64_strict_max_over_instances": float(e.max()),
+                "rel_l1_vs_fp64_strict_median": float(np.median(e)),
+                "instances_compared": int(e.size), "instances_above_1e-5": int((e > 1e-5).sum()),
+                "nonfinite_instances": len(out[form]["failed"])}
 
-    rel_l1, rel_l1_med, n_over, n_cmp = rel_l1_of(head)
-    mixed = None
-    if "mixed" in out and head != "mixed":
-        mx_max, mx_med, mx_over, _ = rel_l1_of("mixed")
-        vmix = out["mixed"]["rate"]
-        mixed = {"value": vmix, "unit": UNIT, "rel_l1_vs_fp64_strict_max_over_instances": mx_max,
-                 "rel_l1_vs_fp64_strict_median": mx_med, "instances_above_1e-5": mx_over,
-                 "failed_instances": out["mixed"]["failed"],
-                 "dtype": "f32 (f64 state/accumulation)"}
-
-    # end to end through the public API: H2D of every instance, the run, D2H
-    bh = out[head]["batch"]
-    flat = torch.from_numpy(bh.pack(qs)).pin_memory()
-    flat_np = flat.numpy()
-    outbuf = torch.empty_like(flat).pin_memory().numpy()
-    import ctypes
-    from sharpclaw_b200 import _capi as C
-    barrier()
-    with clocks:
-        t0 = time.perf_counter()
-        e2e_cells = 0
-        for _ in range(args.steps):
-            C.check(C.lib().scl_batch_set_q(bh._h, flat_np.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "set_q")
-            res, _ = bh.sharpclaw(0.0, C4_TEND, dt0, cfl_max, cfl_des)
-            C.check(C.lib().scl_batch_get_q(bh._h, outbuf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "get_q")
-            e2e_cells += cell_stages(res)
+    e2e_rate = None
+    nbytes = 0
+    if e2e:
+        import ctypes
+        from sharpclaw_b200 import _capi as C
+        bh = out["fp32"]["batch"]
+        flat = torch.from_numpy(bh.pack(qs)).pin_memory()
+        flat_np = flat.numpy()
+        outbuf = torch.empty_like(flat).pin_memory().numpy()
+        nbytes = int(flat_np.nbytes)
         barrier()
-        e2e_rate, e2e_s = job_rate(e2e_cells, time.perf_counter() - t0, world, dev)
+        with clocks:
+            t0 = time.perf_counter()
+            e2e_cells = 0
+            for _ in range(steps):
+                C.check(C.lib().scl_batch_set_q(bh._h, flat_np.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                        "set_q")
+                res, _ = bh.sharpclaw(0.0, tend, dt0, cfl_max, cfl_des)
+                C.check(C.lib().scl_batch_get_q(bh._h, outbuf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                        "get_q")
+                e2e_cells += cell_stages(res)
+            barrier()
+            e2e_rate, e2e_s = job_rate(e2e_cells, time.perf_counter() - t0, world, dev)
+    r32, r64, r64s = out["fp32"]["rate"], out["fp64"]["rate"], out["fp64_strict"]["rate"]
+    summary = {
+        "workload": ("2048 batched 1-D Euler Riemann problems, mx~log-uniform[256,65536] (seed 4), rho,p U[0.1,1], "
+                     f"u U[-1,1], WENO5 componentwise + Roe/efix, SSPRK3, cfl 0.8/0.9, window t in [0,{tend}]"),
+        "cells_total": int(mx.sum()), "instances": len(mx), "window": tend, "timed_runs": steps,
+        "fp32_batched": {"value": r32, "unit": UNIT, **accuracy("fp32"), "tuning": out["fp32"]["tune"]},
+        "mixed_batched": {"value": out["mixed"]["rate"], "unit": UNIT, **accuracy("mixed")},
+        "fp64_batched": {"value": r64, "unit": UNIT},
+        "fp64_strict_batched": {"value": r64s, "unit": UNIT},
+        "fp64_one_at_a_time": {"value": one_rate, "unit": UNIT, "sample_instances": int(len(sample))},
+        "fp32_batched_over_fp64_one_at_a_time": r32 / one_rate,
+        "fp32_batched_over_fp64_batched": r32 / r64,
+        "fp32_batched_over_fp64_strict_batched": r32 / r64s,
+        "mixed_batched_over_fp64_one_at_a_time": out["mixed"]["rate"] / one_rate,
+    }
+    if e2e_rate is not None:
+        summary["fp32_batched_e2e"] = {"value": e2e_rate, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                                       "d2h_bytes_per_step": nbytes, "ms_per_step": 1000.0 * e2e_s / steps}
+    return summary, out
+
+
+def run_gpu_batch(args, rank, world, local_rank):
+    """The batched workload as the bench line: the FP32 batch over the window
+    t in [0, C4_TEND] per step, against plain FP64 grids run one at a time."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    clocks = Clocks(local_rank)
+    summary, out = batch_measure(args, world, dev, C4_TEND, args.steps, args.warmup, clocks, flush)
+    head = out["fp32"]
     peak, peak_kind = measured_peaks()
-    byts = 8.0 / 3.0 * 3 * (4 if head == "fp32" else 8)
-    gbs = byts * out[head]["cells"] / (out[head]["ms"] / 1000.0) / 1e9
+    byts = 8.0 / 3.0 * 3 * 4
+    gbs = byts * head["cells"] / (head["ms"] / 1000.0) / 1e9
     ck = clocks.summary()
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": out[head]["ms"] / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if head == "fp32" else "f64",
+        e2e = summary.pop("fp32_batched_e2e")
+        line = {"metric": METRIC, "value": summary["fp32_batched"]["value"], "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic",
-                "config": {"workload": "2048 batched 1-D Euler Riemann problems, mx~log-uniform[256,65536] "
-                                       "(seed 4), rho,p U[0.1,1], u U[-1,1], WENO5 componentwise + Roe/efix, "
-                                       f"SSPRK3, cfl 0.8/0.9, window t in [0,{C4_TEND}] per step",
-                           "cells_total": int(mx.sum()), "instances": len(mx), "precision": head,
-                           "tuning": out[head]["tune"], "l2": "flushed (256 MiB write) between timed steps",
+                "config": {"workload": summary["workload"], "cells_total": summary["cells_total"],
+                           "instances": summary["instances"], "precision": "fp32", "tuning": head["tune"],
+                           "l2": "flushed (256 MiB write) between timed steps",
                            "parallelism": "replicas (one independent batch per GPU)"},
                 "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
                              "traffic": None, "note": "whole batch step time (stage + controller kernels)",
                              "algorithmic_bytes_per_cell_stage": byts, "peak_source": peak_kind},
-                "fp64_batched": {"value": value64_batched, "unit": UNIT},
-                "fp64_strict_batched": {"value": out["fp64_strict"]["rate"], "unit": UNIT},
-                "fp64_one_at_a_time": {"value": value64_one, "unit": UNIT, "sample_instances": len(sample),
-                                       "speedup_of_headline": value / value64_one},
-                "mixed_batched": mixed,
-                "accuracy": {"rel_l1_vs_fp64_strict_batch_max_over_instances": rel_l1,
-                             "rel_l1_vs_fp64_strict_batch_median": rel_l1_med,
-                             "instances_compared": n_cmp, "instances_above_1e-5": n_over,
-                             "failed_instances": {"headline": out[head]["failed"], "fp64": out["fp64"]["failed"]}},
-                "cpu_baseline": None,
-                "e2e": {"value": e2e_rate, "unit": UNIT, "h2d_bytes_per_step": int(flat_np.nbytes),
-                        "d2h_bytes_per_step": int(flat_np.nbytes), "ms_per_step": 1000.0 * e2e_s / args.steps},
-                "gpu_launches": out[head]["launches"],
-                "clocks": ck}
+                "batched": summary, "cpu_baseline": None, "e2e": e2e,
+                "gpu_launches": head["launches"], "clocks": ck}
         print(json.dumps(line), flush=True)
     for v in out.values():
         v["batch"].close()
@@ -730,6 +823,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp64", "fp64_strict"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-workload block of the default (c2) run")
     ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4", "c5"],
                     help="c2 (default, the headline): 1-D Euler mx=2^20; c1 advection; c3 2-D shallow "
                          "water 4096^2; c4 2048 batched Euler Riemann problems; c5 2-D acoustics 1024^2")

@@ -3,8 +3,9 @@
  *
  * Drop-in boundary for the reference's hot path.  The reference binds these
  * operations as Fortran subroutines; a Fortran host replaces them with
- * bind(C) shims that forward here (see INTEGRATION.md for the
- * iso_c_binding module).  Every entry point returns an int status (0 = ok,
+ * bind(C) shims that forward here (the iso_c_binding module and the shims
+ * flux1, flux2, step and sharpclaw are in fortran/sharpclaw_cuda.f90).
+ * Every entry point returns an int status (0 = ok,
  * negative = SCL_E_*) and never calls exit/abort, replacing the reference's
  * `stop` statements.
  *
@@ -290,9 +291,15 @@ int scl_tiles(scl_handle* h, int* variant, int* tuned, float* trial_ms);
  * library is loaded).  Grids with meqn*(mx+2*mbc) > SCL_NOALLOC_MAX_VALUES are
  * rejected (SCL_E_INVALID).  Calls on one GPU share that array: calls whose
  * work overlaps on the same GPU race, so serialise them.  The first call on a
- * device resolves the array's address; make it before any stream capture.
+ * device resolves the array's address; make it before any stream capture, and
+ * do not reset the device afterwards (the address is kept for the process).
+ * q_dev and aux_dev must be device or managed allocations of the current
+ * device (anything else: SCL_E_INVALID, nothing launched); a CUDA error the
+ * caller left pending is reported as SCL_E_CUDA and left in place.
  * stream is a cudaStream_t (NULL = default stream); when cfl is not NULL the
- * call waits for the step and returns the last stage's CFL number.  Double
+ * call waits for the step, returns the last stage's CFL number and reports a
+ * non-finite state (SCL_E_NONFINITE) or a kernel error (SCL_E_CUDA); with cfl
+ * NULL it returns once the step is enqueued and reports neither.  Double
  * state only (FP64, FP64_STRICT, MIXED). */
 #define SCL_NOALLOC_MAX_VALUES 196608
 int scl_rk_step_noalloc(const scl_params* p, double* q_dev, const double* aux_dev, double dt,

@@ -376,7 +376,8 @@ int scl_batch_create(const scl_params* p, int ninst, const int* mx, const double
   b->nstages = batch_stage_table(p->time_integrator, b->sd, &b->final_role);
   if (!b->nstages) { delete b; return bfail(SCL_E_INVALID, "time_integrator should be between 1 and 4"); }
   for (int v = 0; v < NBATCH_VARIANTS; ++v)
-    if (batch_launchers(p->precision, p->rp, p->lim_type == 1 ? 10 + p->char_decomp : p->char_decomp,
+    if ((v < 2 || p->mcapa == 0) &&   // the paired tile (variant 2) has no capacity form
+        batch_launchers(p->precision, p->rp, p->lim_type == 1 ? 10 + p->char_decomp : p->char_decomp,
                         p->tfluct_solver, v, &b->L[v]))
       b->nvariants = v + 1;
   if (b->nvariants == 0) { delete b; return bfail(SCL_E_UNSUPPORTED, "no batched kernel for this plugin / options"); }

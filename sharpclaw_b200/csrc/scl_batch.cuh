@@ -41,7 +41,9 @@ struct BatchArgs {
 // instance (after the end of the previous step when end_stage >= 0: its last
 // stage index), then the ordered list of active instances with the exclusive
 // prefix sum of their tile counts (a block-wide scan in chunks of 1024).
-template <int NT>
+// Tile j of an instance updates the STRIDE cells from FIRST + j*STRIDE, so
+// an instance of mx cells has (mx - FIRST)/STRIDE + 1 tiles.
+template <int STRIDE, int FIRST>
 __global__ void __launch_bounds__(1024) k_batch_begin(Ctl* ctl, const int* mx, int ninst, int* active,
                                                       int* prefix, int* nact, int end_stage, int final_role) {
   __shared__ int wact[32], wtiles[32];
@@ -56,7 +58,7 @@ __global__ void __launch_bounds__(1024) k_batch_begin(Ctl* ctl, const int* mx, i
       if (end_stage >= 0) ctl_end(&ctl[k], end_stage, final_role);
       ctl_begin(&ctl[k]);
       act = ctl[k].done ? 0 : 1;
-      tiles = act ? (mx[k] + NT - 2) / (NT - 1) : 0;
+      tiles = act ? (mx[k] - FIRST) / STRIDE + 1 : 0;
     }
     // inclusive warp scans of (act, tiles)
     int a = act, t = tiles;

@@ -58,14 +58,26 @@ cudaError_t launch_run1d(const RunArgs& a, cudaStream_t st) {
 #endif
 constexpr int NTP = 128;
 
+// Bulk-copy staging needs every role buffer on a 16-byte boundary and a
+// component stride that keeps the planes there (handles pad it to 32
+// elements; caller-owned arrays may not).
+inline bool pair_tma_ok(const StageArgs& a) {
+  constexpr long AL = 16 / (long)sizeof(S);
+  if (a.plane % AL != 0) return false;
+  for (int r = 0; r < NROLES; ++r)
+    if (reinterpret_cast<uintptr_t>(a.buf[r]) % 16 != 0) return false;
+  return true;
+}
+
 template <int CD>
 void launch1d_pair(const StageArgs& a, cudaStream_t st) {
   if (a.mcapa > 0) {
     launch1d<PEuler, CD, 0>(a, st);
     return;
   }
-  const int nb = (a.mx + 2 * NTP - 2) / (2 * NTP - 1);
-  k_stage1d_pair<CD, PREC, NTP><<<nb, NTP, 0, st>>>(a);
+  const int nb = a.mx / PairGeom<PREC, NTP>::STRIDE + 1;
+  if (pair_tma_ok(a)) k_stage1d_pair<CD, PREC, NTP, true><<<nb, NTP, 0, st>>>(a);
+  else k_stage1d_pair<CD, PREC, NTP, false><<<nb, NTP, 0, st>>>(a);
 }
 
 template <class P, int CD, int TF, int TX, int TY, int NT>
@@ -181,10 +193,10 @@ template <class P, int CD, int TF, int NT>
 void launch_batch_stage(const BatchArgs& a, int grid, cudaStream_t st) {
   k_batch_stage<P, CD, TF, PREC, NT><<<grid, NT, 0, st>>>(a);
 }
-template <int NT>
+template <int STRIDE, int FIRST>
 void launch_batch_begin(Ctl* ctl, const int* mx, int ninst, int* active, int* prefix, int* nact,
                         int end_stage, int final_role, cudaStream_t st) {
-  k_batch_begin<NT><<<1, 1024, 0, st>>>(ctl, mx, ninst, active, prefix, nact, end_stage, final_role);
+  k_batch_begin<STRIDE, FIRST><<<1, 1024, 0, st>>>(ctl, mx, ninst, active, prefix, nact, end_stage, final_role);
 }
 template <class P, int CD, int TF, int NT>
 int batch_blocks_per_sm() {
@@ -195,16 +207,13 @@ int batch_blocks_per_sm() {
 template <class P, int CD, int TF, int NT>
 void fill_batch(BatchLaunchers* L) {
   L->stage = &launch_batch_stage<P, CD, TF, NT>;
-  L->begin = &launch_batch_begin<NT>;
+  L->begin = &launch_batch_begin<NT - 1, 1>;
   L->blocks_per_sm = &batch_blocks_per_sm<P, CD, TF, NT>;
   L->nt = NT;
 }
+// (capacity batches do not get this variant: scl_batch_create skips it)
 template <int CD>
 void launch_batch_stage_pair(const BatchArgs& a, int grid, cudaStream_t st) {
-  if (a.mcapa > 0) {   // capacity: the one-interface tile of the same width (255 cells)
-    k_batch_stage<PEuler, CD, 0, PREC, 2 * NTP><<<grid, 2 * NTP, 0, st>>>(a);
-    return;
-  }
   k_batch_stage_pair<CD, PREC, NTP><<<grid, NTP, 0, st>>>(a);
 }
 template <int CD>
@@ -217,11 +226,11 @@ int batch_blocks_per_sm_pair() {
 template <class P, int CD, int TF>
 bool pick_batch_nt(int variant, BatchLaunchers* L) {
   // variants 0 and 1: one interface per thread, tiles of 127 / 255 cells;
-  // variant 2 (1-D Euler in the FP32 forms): the paired tile of 255 cells
+  // variant 2 (1-D Euler in the FP32 forms): the paired tile of 254 cells
   if constexpr (SCL_PAIR && std::is_same_v<P, PEuler> && !Prec<PREC>::EXACT && TF == 0 && (CD == 0 || CD == 2)) {
     if (variant == 2) {
       L->stage = &launch_batch_stage_pair<CD>;
-      L->begin = &launch_batch_begin<2 * NTP>;
+      L->begin = &launch_batch_begin<PairGeom<PREC, NTP>::STRIDE, 0>;
       L->blocks_per_sm = &batch_blocks_per_sm_pair<CD>;
       L->nt = NTP;
       return true;

@@ -390,6 +390,45 @@ __device__ __forceinline__ R load_aux(const void* aux, long off) {
   return (R)static_cast<const R*>(aux)[off];
 }
 
+// Running CFL maximum of flux1.f90:126-133 (max over waves of
+// max(dtdx(i)*s, -dtdx(i-1)*s)) and flux2.f90:47,80, kept in FP64 in every
+// arithmetic form.  The exact forms form the reference's products in double.
+// The FP32 forms keep the largest |s| per direction in R (exact) and
+// multiply it by dt/dx or dt/dy once, in double: with one dtdx per direction
+// max(dtdx s, -dtdx s) = dtdx |s|, and since rounding is monotonic that
+// product equals the maximum of the per-interface FP64 products.  Capacity
+// grids (a dtdx per cell) form each product in double.  NaN propagates.
+template <class R>
+struct CflMax {
+  double v = 0.0;
+  R sx = (R)0, sy = (R)0;
+  template <int MW>
+  __device__ __forceinline__ void add(const R* s, double d_c, double d_m, bool per_cell, bool isx) {
+    if constexpr (std::is_same_v<R, double>) {
+#pragma unroll
+      for (int w = 0; w < MW; ++w) v = nanmax(v, nanmax(d_c * s[w], -d_m * s[w]));
+    } else {
+      if (per_cell) {
+#pragma unroll
+        for (int w = 0; w < MW; ++w) {
+          const double sw = (double)s[w];
+          v = nanmax(v, nanmax(d_c * sw, -d_m * sw));
+        }
+      } else {
+        R m = isx ? sx : sy;
+#pragma unroll
+        for (int w = 0; w < MW; ++w) m = nanmax(m, fabsf(s[w]));
+        if (isx) sx = m; else sy = m;
+      }
+    }
+  }
+  // the thread's value, given the grid's dt/dx and dt/dy
+  __device__ __forceinline__ double value(double dtdx, double dtdy) const {
+    if constexpr (std::is_same_v<R, double>) return v;
+    else return nanmax(v, nanmax(dtdx * (double)sx, dtdy * (double)sy));
+  }
+};
+
 // ---------------------------------------------------------------------------
 // One line (a 1-D grid, a batched instance, or a line of a 2-D plugin) as a
 // stage sees it: buffers already resolved through the controller's roles.
@@ -437,7 +476,7 @@ template <class P, int PREC, int NT>
 struct Tile1DSmem {
   typename Prec<PREC>::S sq[P::MEQN][NT + 8];
   typename Prec<PREC>::R rec[4][P::MEQN][NT];   // 0: qr(c-1)  1: ql(c)  2: amdq(c)  3: apdq(c)
-  typename Prec<PREC>::R sred[NT / 32];
+  double sred[NT / 32];
   double dtdx;   // dt/dx, one division per tile
 };
 
@@ -468,7 +507,7 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
   const double dtdx0 = sm.dtdx;
 
   // ---- interface phase ----
-  R cflmax = (R)0;
+  CflMax<R> cfl;
   int bad = 0;   // a non-finite stage output (reported through ctl->status)
   {
     const int c = c0 + tid;
@@ -495,12 +534,7 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
         dtdx_c = dt / (L.dx * (double)cap[c + 2]);
         dtdx_m = dt / (L.dx * (double)cap[c + 1]);
       }
-#pragma unroll
-      for (int w = 0; w < MW; ++w) {
-        R v1 = (R)dtdx_c * s[w];
-        R v2 = -(R)dtdx_m * s[w];
-        cflmax = nanmax(cflmax, nanmax(v1, v2));
-      }
+      cfl.template add<MW>(s, dtdx_c, dtdx_m, L.mcapa > 0, true);
     }
   }
   __syncthreads();
@@ -573,11 +607,11 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
   }
 
   // ---- CFL reduction: warp max, block max, one atomic per tile ----
-  cflmax = warp_max(cflmax);
+  double cflmax = warp_max(cfl.value(dtdx0, dtdx0));
   if ((tid & 31) == 0) sm.sred[tid >> 5] = cflmax;
   const int anybad = __syncthreads_or(bad);
   if (tid < 32) {
-    R v = (tid < NT / 32) ? sm.sred[tid] : (R)0;
+    double v = (tid < NT / 32) ? sm.sred[tid] : 0.0;
     v = warp_max(v);
     if (tid == 0) {
       atomic_max_nonneg(&L.ctl->stage_cfl[L.stage], (double)v);
@@ -650,7 +684,7 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
   S* sq = reinterpret_cast<S*>(smem_raw);                                  // [M][WY][WX]
   R* recx = reinterpret_cast<R*>(sq + M * T::WX * T::WY);                  // [4][M][NXI]
   R* recy = recx + 4 * M * T::NXI;                                         // [4][M][NYI]
-  __shared__ R sred[NT / 32];
+  __shared__ double sred[NT / 32];
 
   const Ctl* ctl = a.ctl;
   if (ctl->done) return;
@@ -674,7 +708,7 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
   __syncthreads();
   const double dtdx0 = s_dtd[0], dtdy0 = s_dtd[1];
 
-  R cflmax = (R)0;
+  CflMax<R> cfl;
   int bad = 0;
   for (int w = tid; w < T::NXI + T::NYI; w += NT) {
     const bool isx = w < T::NXI;
@@ -726,8 +760,7 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
     }
     // interior lines only; flux2.f90 also scans the ghost lines j=0,ny+1 /
     // i=0,nx+1, which the ghost-line kernel covers.
-#pragma unroll
-    for (int k = 0; k < MW; ++k) cflmax = nanmax(cflmax, nanmax((R)d_c * s[k], -(R)d_m * s[k]));
+    cfl.template add<MW>(s, d_c, d_m, a.mcapa > 0, isx);
   }
   __syncthreads();
 
@@ -805,11 +838,11 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
     }
   }
 
-  cflmax = warp_max(cflmax);
+  const double cflmax = warp_max(cfl.value(dtdx0, dtdy0));
   if ((tid & 31) == 0) sred[tid >> 5] = cflmax;
   const int anybad = __syncthreads_or(bad);
   if (tid < 32) {
-    R v = (tid < NT / 32) ? sred[tid] : (R)0;
+    double v = (tid < NT / 32) ? sred[tid] : 0.0;
     v = warp_max(v);
     if (tid == 0) {
       atomic_max_nonneg(&a.ctl->stage_cfl[a.stage], (double)v);
@@ -826,7 +859,7 @@ __global__ void __launch_bounds__(128) k_ghost_cfl2d(StageArgs a) {
   using R = typename Prec<PREC>::R;
   using S = typename Prec<PREC>::S;
   constexpr int M = P::MEQN, MW = P::MWAVES, MA = P::MAUX;
-  __shared__ R sred[4];
+  __shared__ double sred[4];
   const Ctl* ctl = a.ctl;
   if (ctl->done) return;
   const int nx = a.mx, ny = a.my;
@@ -834,7 +867,7 @@ __global__ void __launch_bounds__(128) k_ghost_cfl2d(StageArgs a) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   const S* qin = static_cast<const S*>(a.buf[ctl->role[a.sd.in]]);
   const double dt = ctl->dt;
-  R cflmax = (R)0;
+  CflMax<R> cfl;
   if (w < 2 * nxl + 2 * nyl) {
     int ixy, gi, gj;
     if (w < 2 * nxl) { ixy = 1; gi = 1 + (w % nxl); gj = (w < nxl) ? 0 : ny + 1; }
@@ -859,14 +892,13 @@ __global__ void __launch_bounds__(128) k_ghost_cfl2d(StageArgs a) {
       d_c = dt / (h * (double)cap[o0]);
       d_m = dt / (h * (double)cap[om]);
     }
-#pragma unroll
-    for (int k = 0; k < MW; ++k) cflmax = nanmax(cflmax, nanmax((R)d_c * s[k], -(R)d_m * s[k]));
+    cfl.template add<MW>(s, d_c, d_m, a.mcapa > 0, ixy == 1);
   }
-  cflmax = warp_max(cflmax);
+  const double cflmax = warp_max(cfl.value(dt / a.dx, dt / a.dy));
   if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = cflmax;
   __syncthreads();
   if (threadIdx.x < 32) {
-    R v = (threadIdx.x < 4) ? sred[threadIdx.x] : (R)0;
+    double v = (threadIdx.x < 4) ? sred[threadIdx.x] : 0.0;
     v = warp_max(v);
     if (threadIdx.x == 0) atomic_max_nonneg(&a.ctl->stage_cfl[a.stage], (double)v);
   }

@@ -19,7 +19,16 @@
 //    each other: serialise them;
 //  * the first call on each device looks up the scratch array's device
 //    address with cudaGetSymbolAddress (with that device current); make this
-//    first call before any stream capture is started on that thread.
+//    first call before any stream capture is started on that thread.  The
+//    address is kept for the life of the process: a device reset
+//    (cudaDeviceReset) after the first call invalidates it, so do not reset
+//    a device this library has stepped on;
+//  * q_dev and aux_dev must be device (or managed) allocations of the current
+//    device; any other pointer is refused before anything is launched;
+//  * a CUDA error left pending by the caller's earlier work is reported (and
+//    left in place) instead of being taken for a failure of this call;
+//  * with cfl == NULL the call returns once the step is enqueued: it then
+//    reports neither a non-finite state nor an asynchronous kernel error.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -135,6 +144,29 @@ int noalloc_table(int ti, StageDesc* sd) {
   return n;
 }
 
+// A caller pointer the stage kernels may dereference: a device or managed
+// allocation of the current device.  Host memory (pageable or pinned) and
+// other devices' memory are refused with SCL_E_INVALID before any launch.
+int check_device_pointer(const void* p, const char* name) {
+  cudaPointerAttributes at{};
+  cudaError_t e = cudaPointerGetAttributes(&at, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();   // the query's own error (none was pending before it)
+    return fail_na(SCL_E_INVALID, std::string(name) + " is not a device allocation (cudaPointerGetAttributes: " +
+                                      cudaGetErrorString(e) + ")");
+  }
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return fail_na(SCL_E_INVALID, "no current CUDA device");
+  }
+  if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+    return fail_na(SCL_E_INVALID, std::string(name) + " is not device or managed memory");
+  if (at.type == cudaMemoryTypeDevice && at.device != dev)
+    return fail_na(SCL_E_INVALID, std::string(name) + " belongs to another device");
+  return SCL_OK;
+}
+
 bool launchers_for(int prec, int rp, int cd, int tf, Launchers* L) {
   switch (prec) {
     case SCL_FP64: return get_launchers_fp64(rp, 1, cd, tf, 0, L);
@@ -187,6 +219,17 @@ extern "C" int scl_rk_step_noalloc(const scl_params* p, double* q_dev, const dou
   StageDesc sd[MAXSTAGES];
   const int ns = noalloc_table(p->time_integrator, sd);
   if (ns == 0) return fail_na(SCL_E_INVALID, "time_integrator should be between 1 and 4");
+
+  // an error left by the caller's earlier work stays the caller's
+  cudaError_t pend = cudaPeekAtLastError();
+  if (pend == cudaErrorNoDevice || pend == cudaErrorInsufficientDriver)
+    return fail_na(SCL_E_CUDA, std::string("no usable CUDA device: ") + cudaGetErrorString(pend));
+  if (pend != cudaSuccess)
+    return fail_na(SCL_E_CUDA, std::string("a CUDA error was pending before this call (left in place): ") +
+                                   cudaGetErrorString(pend));
+  int rc0 = check_device_pointer(q_dev, "q_dev");
+  if (rc0 == SCL_OK && p->maux > 0) rc0 = check_device_pointer(aux_dev, "aux_dev");
+  if (rc0) return rc0;
 
   void* base = nullptr;
   int rc = scratch_for_current_device(&base);

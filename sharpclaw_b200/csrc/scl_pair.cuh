@@ -9,6 +9,7 @@
 #pragma once
 #include "scl_batch.cuh"
 #include "scl_kernels.cuh"
+#include "scl_tma.cuh"
 
 namespace scl {
 
@@ -229,55 +230,185 @@ __device__ __forceinline__ void weno5_offset2(const f2 d[5][3], const f2 evl[3][
     }
   }
 }
-
 // ---- the tile ---------------------------------------------------------------
 #ifndef SCL_PAIR_MINB
 #define SCL_PAIR_MINB 6
 #endif
 
+// Tile geometry.  Thread t owns interfaces and cells c = c0 + 2t (lane x) and
+// c + 1 (lane y) with c0 = (2NT-2) b even, so a thread's two cells sit at the
+// even element offset c+2 (offset = cell + 2 in the reference layout) and its
+// stencil window starts at the even offset c-2: 16-byte vector accesses in
+// double planes.  A tile updates the 2NT-2 cells c0 .. c0+2NT-3 (cell 0 of
+// tile 0 is a ghost cell and is not written) from interfaces c0 .. c0+2NT-2;
+// the last thread's second interface is not needed.
+template <int PREC, int NT>
+struct PairGeom {
+  using S = typename Prec<PREC>::S;
+  static constexpr int AL = 16 / (int)sizeof(S);                 // elements per 16 bytes
+  static constexpr int STRIDE = 2 * NT - 2;                       // cells per tile
+  static constexpr int SQW = (2 * NT + 8 + AL - 1) / AL * AL;     // staged offsets per component
+};
+
+// One staged window: offsets a0 .. a0+SQW-1 of the three component planes.
+template <int PREC, int NT>
+struct PairWin {
+  __align__(16) typename Prec<PREC>::S v[3][PairGeom<PREC, NT>::SQW];
+};
+
+// Interface records of a tile: 0: qr(c-1)  1: ql(c)  2: amdq(c)  3: apdq(c).
+template <int NT>
+struct PairRec {
+  __align__(16) float r[4][3][2 * NT + 2];
+};
+
 template <int PREC, int NT>
 struct PairSmem {
-  using S = typename Prec<PREC>::S;
-  static constexpr int SQW = 2 * NT + 8;           // staged cells per component
-  __align__(16) S sq[3][SQW];
-  __align__(16) float rec[4][3][2 * NT + 2];       // 0: qr(c-1)  1: ql(c)  2: amdq(c)  3: apdq(c)
+  PairWin<PREC, NT> sq;    // stage input
+  PairWin<PREC, NT> so;    // the stage's pointwise input (qold or r1), same window
+  PairRec<NT> rec;
   float sred[NT / 32];
   double dtdx;
+  uint64_t bar;            // completion of the bulk copies of the tile
 };
 
 __device__ __forceinline__ f2 ld2(const float* p) { return *reinterpret_cast<const float2*>(p); }
 __device__ __forceinline__ void st2(float* p, f2 v) { *reinterpret_cast<float2*>(p) = v; }
 
-// One tile from staged cells sq[m*SQW + k] (k = 0 .. 2NT+4 <-> cells
-// c0-3 .. c0+2NT+1): interfaces c0 .. c0+2NT-1 and cells c0 .. c0+2NT-2;
-// thread t owns interfaces and cells c0+2t (lane x) and c0+2t+1 (lane y); the
-// last cell of the tile is the next tile's first.
-template <int CD, int PREC, int NT>
+// two consecutive elements at an even offset (one 16- or 8-byte access)
+template <class S>
+struct Pair2;
+template <>
+struct Pair2<double> {
+  using V = double2;
+};
+template <>
+struct Pair2<float> {
+  using V = float2;
+};
+template <class S>
+__device__ __forceinline__ typename Pair2<S>::V ldp(const S* p) {
+  return *reinterpret_cast<const typename Pair2<S>::V*>(p);
+}
+template <class S>
+__device__ __forceinline__ void stp(S* p, S x, S y) {
+  typename Pair2<S>::V v;
+  v.x = x;
+  v.y = y;
+  *reinterpret_cast<typename Pair2<S>::V*>(p) = v;
+}
+
+// Window of a tile: first staged offset a0 (a multiple of AL, so that the
+// bulk copies start on 16 bytes) and the shift sh = (c0-2) - a0 of the
+// stencil windows inside it.
+template <int PREC, int NT>
+__device__ __forceinline__ int pair_window(int c0, int& sh) {
+  constexpr int AL = PairGeom<PREC, NT>::AL;
+  const int a0 = (c0 - 2 + AL) / AL * AL - AL;   // floor to a multiple of AL (c0 - 2 >= -2)
+  sh = c0 - 2 - a0;
+  return a0;
+}
+
+// Issue (thread 0 only) the bulk copies of the tile at c0: the component
+// planes of the stage input into wq and, when wo is given, of the pointwise
+// input qo into wo, all completed on bar.  Offsets below 0 (tile 0 only) are
+// filled with 1 before the arrival, so the waiting threads see them.
+template <int PREC, int NT>
+__device__ __forceinline__ void pair_issue(const Line<typename Prec<PREC>::S>& L, int c0, PairWin<PREC, NT>& wq,
+                                           PairWin<PREC, NT>* wo, uint64_t* bar) {
+  using S = typename Prec<PREC>::S;
+  constexpr int AL = PairGeom<PREC, NT>::AL, SQW = PairGeom<PREC, NT>::SQW;
+  int sh;
+  const int a0 = pair_window<PREC, NT>(c0, sh);
+  const int hend = (L.mx + 6 + AL - 1) / AL * AL;   // round_up(mx+6, AL) <= plane (host-checked)
+  const int lo = a0 > 0 ? a0 : 0;
+  const int hi = a0 + SQW < hend ? a0 + SQW : hend;
+  for (int k = 0; k < lo - a0; ++k)
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      wq.v[m][k] = (S)1;
+      if (wo) wo->v[m][k] = (S)1;
+    }
+  const uint32_t bytes = (uint32_t)(hi - lo) * (uint32_t)sizeof(S);
+  fence_proxy_async_smem();   // earlier accesses of these buffers come before the copies' writes
+  mbar_arrive_expect_tx(bar, bytes * (wo ? 6u : 3u));
+#pragma unroll
+  for (int m = 0; m < 3; ++m) bulk_g2s(&wq.v[m][lo - a0], L.qin + (long)m * L.plane + lo, bytes, bar);
+  if (wo)
+#pragma unroll
+    for (int m = 0; m < 3; ++m) bulk_g2s(&wo->v[m][lo - a0], L.qo + (long)m * L.plane + lo, bytes, bar);
+}
+
+// Every thread waits for phase `parity` of bar; false on every thread when
+// the bounded wait ran out (SCL_STATUS_TIMEOUT is raised and the copies
+// still in flight are given a second bounded wait to land).
+__device__ __forceinline__ bool pair_wait(Ctl* ctl, uint64_t* bar, uint32_t parity) {
+  const bool ok = mbar_wait_bounded(bar, parity);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicOr(&ctl->status, SCL_STATUS_TIMEOUT);
+    mbar_wait_bounded(bar, parity);
+    return false;
+  }
+  return true;
+}
+
+// The threads stage the window themselves (planes not on 16 bytes).
+template <int PREC, int NT>
+__device__ __forceinline__ void pair_load(const Line<typename Prec<PREC>::S>& L, int c0, PairWin<PREC, NT>& wq,
+                                          PairWin<PREC, NT>* wo) {
+  using S = typename Prec<PREC>::S;
+  constexpr int SQW = PairGeom<PREC, NT>::SQW;
+  int sh;
+  const int a0 = pair_window<PREC, NT>(c0, sh);
+  for (int k = threadIdx.x; k < SQW; k += NT) {
+    const long g = (long)a0 + k;
+    const bool in = g >= 0 && g < (long)L.mx + 6;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      wq.v[m][k] = in ? L.qin[(long)m * L.plane + g] : (S)1;
+      if (wo) wo->v[m][k] = in ? L.qo[(long)m * L.plane + g] : (S)1;
+    }
+  }
+}
+
+// One staged tile: interfaces c (lane x) and c+1 (lane y) of thread t, then
+// its cells c and c+1.  smax collects the largest |s| over the tile's
+// interfaces of the grid (1 .. mx+1).  wo: the staged pointwise input, or
+// nullptr to read it (when the stage has one) from global memory.  VEC: the
+// planes' alignment allows 16-byte accesses of a thread's two cells.
+template <int CD, int PREC, int NT, bool VEC>
 __device__ __forceinline__ void pair_compute(const Line<typename Prec<PREC>::S>& L, const Phys& ph, int c0,
-                                             const typename Prec<PREC>::S* sq, PairSmem<PREC, NT>& sm,
-                                             double dtdx0, float& cflmax, int& bad) {
+                                             const PairWin<PREC, NT>& wq, const PairWin<PREC, NT>* wo,
+                                             PairRec<NT>& rec, double dtdx0, float& smax, int& bad) {
   using S = typename Prec<PREC>::S;
   using Ac = typename Prec<PREC>::A;
-  constexpr int SQW = PairSmem<PREC, NT>::SQW;
   const int tid = threadIdx.x;
   const int mx = L.mx;
   const float dtdx = (float)dtdx0;
   const int c = c0 + 2 * tid;
-  auto Q = [&](int m, int k) -> S { return sq[m * SQW + k]; };
+  int sh;
+  pair_window<PREC, NT>(c0, sh);
+  const int b = sh + 2 * tid;   // staged index of offset c-2 (cell c-4)
 
   // ---- interface phase: interfaces c (lane x) and c+1 (lane y) ----
   {
-    const int b = 2 * tid;   // index of cell c-3
     f2 d[5][3], qm[3], q0[3];
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
+      S e[8];   // cells c-4 .. c+3
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const auto v = ldp(&wq.v[m][b + 2 * k]);
+        e[2 * k] = v.x;
+        e[2 * k + 1] = v.y;
+      }
       float dj[6];
 #pragma unroll
-      for (int k = 0; k < 6; ++k) dj[k] = (float)(Q(m, b + k + 1) - Q(m, b + k));
+      for (int k = 0; k < 6; ++k) dj[k] = (float)(e[k + 2] - e[k + 1]);
 #pragma unroll
       for (int k = 0; k < 5; ++k) d[k][m] = F2(dj[k], dj[k + 1]);
-      qm[m] = F2((float)Q(m, b + 2), (float)Q(m, b + 3));
-      q0[m] = F2((float)Q(m, b + 3), (float)Q(m, b + 4));
+      qm[m] = F2((float)e[3], (float)e[4]);
+      q0[m] = F2((float)e[4], (float)e[5]);
     }
     f2 evl[3][3], evr[3][3];
     if constexpr (CD == 2) EulerPair::evec(ph, qm, q0, evl, evr);
@@ -293,31 +424,36 @@ __device__ __forceinline__ void pair_compute(const Line<typename Prec<PREC>::S>&
     EulerPair::rp(ph, Lq, Rq, dl, s, am, ap);
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
-      st2(&sm.rec[0][m][2 * tid], er[m]);
-      st2(&sm.rec[1][m][2 * tid], el[m]);
-      st2(&sm.rec[2][m][2 * tid], am[m]);
-      st2(&sm.rec[3][m][2 * tid], ap[m]);
+      st2(&rec.r[0][m][2 * tid], er[m]);
+      st2(&rec.r[1][m][2 * tid], el[m]);
+      st2(&rec.r[2][m][2 * tid], am[m]);
+      st2(&rec.r[3][m][2 * tid], ap[m]);
     }
-    // flux1.f90:126-133 for the interfaces of the grid
+    // flux1.f90:126-133 over the interfaces 1 .. mx+1 of the grid: with one
+    // dtdx, max(dtdx s, -dtdx s) = dtdx |s|, and the largest |s| is
+    // multiplied by dtdx once, in FP64 (the same value as the maximum of the
+    // FP64 products, since rounding is monotonic)
+    const bool ix = c >= 1 && c <= mx + 1, iy = c + 1 <= mx + 1;
 #pragma unroll
     for (int w = 0; w < 3; ++w) {
-      if (c <= mx + 1) cflmax = nanmax(cflmax, nanmax(dtdx * s[w].x, -dtdx * s[w].x));
-      if (c + 1 <= mx + 1) cflmax = nanmax(cflmax, nanmax(dtdx * s[w].y, -dtdx * s[w].y));
+      if (ix) smax = nanmax(smax, fabsf(s[w].x));
+      if (iy) smax = nanmax(smax, fabsf(s[w].y));
     }
   }
   __syncthreads();
 
   // ---- cell phase: cells c (lane x) and c+1 (lane y) ----
-  if (c <= mx) {
+  if (tid < NT - 1 && c <= mx) {
     const int i = 2 * tid;
     f2 qc[3], qlc[3], qrc[3], apc[3], amc1[3];
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
-      qc[m] = F2((float)Q(m, i + 3), (float)Q(m, i + 4));
-      qlc[m] = ld2(&sm.rec[1][m][i]);
-      apc[m] = ld2(&sm.rec[3][m][i]);
-      qrc[m] = F2(sm.rec[0][m][i + 1], sm.rec[0][m][i + 2]);
-      amc1[m] = F2(sm.rec[2][m][i + 1], sm.rec[2][m][i + 2]);
+      const auto v = ldp(&wq.v[m][b + 4]);
+      qc[m] = F2((float)v.x, (float)v.y);
+      qlc[m] = ld2(&rec.r[1][m][i]);
+      apc[m] = ld2(&rec.r[3][m][i]);
+      qrc[m] = F2(rec.r[0][m][i + 1], rec.r[0][m][i + 2]);
+      amc1[m] = F2(rec.r[2][m][i + 1], rec.r[2][m][i + 2]);
     }
     f2 Lq[3], Rq[3], dl[3], s2[3], am2[3], ap2[3];
 #pragma unroll
@@ -327,33 +463,77 @@ __device__ __forceinline__ void pair_compute(const Line<typename Prec<PREC>::S>&
       dl[m] = sub(qrc[m], qlc[m]);
     }
     EulerPair::rp(ph, Lq, Rq, dl, s2, am2, ap2);   // flux1.f90:181-182
-    const bool second = (tid < NT - 1) && (c + 1 <= mx);   // lane y is a cell of this tile
+    const bool vx = c >= 1;              // cell 0 of tile 0 is a ghost cell
+    const bool vy = c + 1 <= mx;
+    const bool edge = c <= 3 || c + 1 >= mx - 2;   // a lane has ghost images
     const int kind = L.kind;
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
       const f2 br = add(add(add(amc1[m], apc[m]), am2[m]), ap2[m]);   // :185-186
       const f2 dq = mul(F2(-dtdx), br);
-#pragma unroll
-      for (int lane = 0; lane < 2; ++lane) {
-        if (lane == 1 && !second) continue;
-        const int cc = c + lane;
-        const float dqf = lane ? dq.y : dq.x;
-        if (kind == SK_DQ) {
-          L.dq_out[(long)m * L.plane + cc + 2] = (double)dqf;
-          continue;
+      if (kind == SK_DQ) {
+        if (vx) L.dq_out[(long)m * L.plane + c + 2] = (double)dq.x;
+        if (vy) L.dq_out[(long)m * L.plane + c + 3] = (double)dq.y;
+        continue;
+      }
+      const auto qv = ldp(&wq.v[m][b + 4]);
+      typename Pair2<S>::V qov;
+      qov.x = (S)0;
+      qov.y = (S)0;
+      if (L.qo) {
+        if (wo) {
+          qov = ldp(&wo->v[m][b + 4]);
+        } else {
+          const S* pq = L.qo + (long)m * L.plane + c + 2;
+          if (VEC && vx && vy) qov = ldp(pq);
+          else {
+            if (vx) qov.x = pq[0];
+            if (vy) qov.y = pq[1];
+          }
         }
-        const Ac qv = (Ac)Q(m, i + 3 + lane);
-        const Ac qov = L.qo ? (Ac)L.qo[(long)m * L.plane + cc + 2] : (Ac)0;
-        Ac o1, o2 = (Ac)0;
-        combine<Ac, false>(kind, qv, qov, (Ac)dqf, o1, o2);
-        bad |= !isfinite(o1);
-        const bool edge = cc <= 3 || cc >= mx - 2;
-        if (edge) put_1d<S, Ac>(L.out, L.plane, m, cc, images_1d(cc, mx, L.bl, L.br), o1);
-        else L.out[(long)m * L.plane + cc + 2] = (S)o1;
-        if (L.out2) L.out2[(long)m * L.plane + cc + 2] = (S)o2;
+      }
+      Ac ox, oy, o2x = (Ac)0, o2y = (Ac)0;
+      combine<Ac, false>(kind, (Ac)qv.x, (Ac)qov.x, (Ac)dq.x, ox, o2x);
+      combine<Ac, false>(kind, (Ac)qv.y, (Ac)qov.y, (Ac)dq.y, oy, o2y);
+      bad |= (vx && !isfinite(ox)) || (vy && !isfinite(oy));
+      S* po = L.out + (long)m * L.plane + c + 2;
+      if (VEC && vx && vy && !edge) {
+        stp<S>(po, (S)ox, (S)oy);
+        if (L.out2) stp<S>(L.out2 + (long)m * L.plane + c + 2, (S)o2x, (S)o2y);
+      } else {
+        if (vx) {
+          if (c <= 3 || c >= mx - 2) put_1d<S, Ac>(L.out, L.plane, m, c, images_1d(c, mx, L.bl, L.br), ox);
+          else po[0] = (S)ox;
+          if (L.out2) L.out2[(long)m * L.plane + c + 2] = (S)o2x;
+        }
+        if (vy) {
+          if (c + 1 <= 3 || c + 1 >= mx - 2)
+            put_1d<S, Ac>(L.out, L.plane, m, c + 1, images_1d(c + 1, mx, L.bl, L.br), oy);
+          else po[1] = (S)oy;
+          if (L.out2) L.out2[(long)m * L.plane + c + 3] = (S)o2y;
+        }
       }
     }
   }
+}
+
+// CTA maximum of smax, times dtdx in FP64, into the stage's CFL slot; the
+// non-finite flag into the status word.  Ends with a CTA-wide barrier.
+template <int NT>
+__device__ __forceinline__ void pair_reduce(Ctl* ctl, int stage, float* sred, double dtdx, float smax, int bad) {
+  const int tid = threadIdx.x;
+  smax = warp_max(smax);
+  if ((tid & 31) == 0) sred[tid >> 5] = smax;
+  const int anybad = __syncthreads_or(bad);
+  if (tid < 32) {
+    float v = (tid < NT / 32) ? sred[tid] : 0.0f;
+    v = warp_max(v);
+    if (tid == 0) {
+      atomic_max_nonneg(&ctl->stage_cfl[stage], dtdx * (double)v);
+      if (anybad) atomicOr(&ctl->status, SCL_STATUS_NONFINITE);
+    }
+  }
+  __syncthreads();   // sred and the staged windows are reused by the next tile
 }
 
 template <class S>
@@ -362,7 +542,7 @@ __device__ __forceinline__ Line<S> line_of(const StageArgs& a, Ctl* ctl) {
   L.ctl = ctl;
   L.qin = static_cast<const S*>(a.buf[ctl->role[a.sd.in]]);
   L.qo = a.sd.aux_in >= 0 ? static_cast<const S*>(a.buf[ctl->role[a.sd.aux_in]]) : nullptr;
-  L.out = static_cast<S*>(a.buf[ctl->role[a.sd.out]]);
+  L.out = a.sd.kind == SK_DQ ? nullptr : static_cast<S*>(a.buf[ctl->role[a.sd.out]]);
   L.out2 = a.sd.out2 >= 0 ? static_cast<S*>(a.buf[ctl->role[a.sd.out2]]) : nullptr;
   L.dq_out = a.dq_out;
   L.aux = a.aux;
@@ -375,49 +555,46 @@ __device__ __forceinline__ Line<S> line_of(const StageArgs& a, Ctl* ctl) {
   L.kind = a.sd.kind;
   L.stage = a.stage;
   L.ixy = a.ixy;
+  L.dt = ctl->dt;
   return L;
 }
 
-// One tile per CTA (k_stage1d's geometry with 2NT interfaces per tile).
-template <int CD, int PREC, int NT>
-__global__ void __launch_bounds__(NT, SCL_PAIR_MINB) k_stage1d_pair(StageArgs a) {
+// One tile per CTA.  TMA: the planes are 16-byte aligned with an even (double)
+// or multiple-of-4 (float) component stride, checked by the launcher, and the
+// tile is staged by bulk copies; otherwise by the threads.
+template <int CD, int PREC, int NT, bool TMA, int MINB = SCL_PAIR_MINB>
+__global__ void __launch_bounds__(NT, MINB) k_stage1d_pair(StageArgs a) {
   using S = typename Prec<PREC>::S;
-  using Sm = PairSmem<PREC, NT>;
-  __shared__ Sm sm;
+  __shared__ PairSmem<PREC, NT> sm;
   Ctl* ctl = a.ctl;
   if (ctl->done) return;
   const Line<S> L = line_of<S>(a, ctl);
-  const int tid = threadIdx.x;
-  const int c0 = 1 + blockIdx.x * (2 * NT - 1);
-  if (tid == 0) sm.dtdx = ctl->dt / a.dx;
-  // stage cells c0-3 .. c0+2NT+1 (global offset c+2)
-  for (int k = tid; k < 2 * NT + 5; k += NT) {
-    const long g = (long)c0 - 1 + k;
-    const bool ok = g < (long)L.mx + 6;
-#pragma unroll
-    for (int m = 0; m < 3; ++m) sm.sq[m][k] = ok ? L.qin[(long)m * L.plane + g] : (S)1;
-  }
-  __syncthreads();
-  float cflmax = 0.0f;
-  int bad = 0;
-  pair_compute<CD, PREC, NT>(L, a.ph, c0, &sm.sq[0][0], sm, sm.dtdx, cflmax, bad);
-
-  cflmax = warp_max(cflmax);
-  if ((tid & 31) == 0) sm.sred[tid >> 5] = cflmax;
-  const int anybad = __syncthreads_or(bad);
-  if (tid < 32) {
-    float v = (tid < NT / 32) ? sm.sred[tid] : 0.0f;
-    v = warp_max(v);
-    if (tid == 0) {
-      atomic_max_nonneg(&ctl->stage_cfl[a.stage], (double)v);
-      if (anybad) atomicOr(&ctl->status, SCL_STATUS_NONFINITE);
+  const int c0 = (int)blockIdx.x * PairGeom<PREC, NT>::STRIDE;
+  PairWin<PREC, NT>* wo = L.qo ? &sm.so : nullptr;
+  if constexpr (TMA) {
+    if (threadIdx.x == 0) {
+      mbar_init(&sm.bar, 1);
+      fence_mbar_init();
+      sm.dtdx = L.dt / L.dx;
+      pair_issue<PREC, NT>(L, c0, sm.sq, wo, &sm.bar);
     }
+    __syncthreads();   // the barrier is initialised before any thread waits on it
+    if (!pair_wait(ctl, &sm.bar, 0)) return;
+  } else {
+    if (threadIdx.x == 0) sm.dtdx = L.dt / L.dx;
+    pair_load<PREC, NT>(L, c0, sm.sq, wo);
+    __syncthreads();
   }
+  float smax = 0.0f;
+  int bad = 0;
+  pair_compute<CD, PREC, NT, TMA>(L, a.ph, c0, sm.sq, wo, sm.rec, sm.dtdx, smax, bad);
+  pair_reduce<NT>(ctl, a.stage, sm.sred, sm.dtdx, smax, bad);
 }
 
 // Batched form: the persistent walk over the active instances' tiles of
-// k_batch_stage, with the paired tile (2NT-1 cells) and one CFL atomic per
-// tile into the tile's own controller.
+// k_batch_stage with the paired tile (instances are 16-byte aligned with
+// planes padded to 32 elements, so the tiles are staged by bulk copies) and
+// one CFL atomic per tile into the tile's own controller.
 template <int CD, int PREC, int NT>
 __global__ void __launch_bounds__(NT, SCL_PAIR_MINB) k_batch_stage_pair(BatchArgs a) {
   using S = typename Prec<PREC>::S;
@@ -426,7 +603,13 @@ __global__ void __launch_bounds__(NT, SCL_PAIR_MINB) k_batch_stage_pair(BatchArg
   if (na == 0) return;
   const int ntiles = a.prefix[na];
   const int tid = threadIdx.x;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  if (tid == 0) {
+    mbar_init(&sm.bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  uint32_t parity = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, parity ^= 1u) {
     int lo = 0, hi = na - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
@@ -442,39 +625,28 @@ __global__ void __launch_bounds__(NT, SCL_PAIR_MINB) k_batch_stage_pair(BatchArg
     L.out = static_cast<S*>(a.arena[ctl->role[a.sd.out]]) + off;
     L.out2 = a.sd.out2 >= 0 ? static_cast<S*>(a.arena[ctl->role[a.sd.out2]]) + off : nullptr;
     L.dq_out = nullptr;
-    L.aux = a.aux ? static_cast<const void*>(static_cast<const S*>(a.aux) + a.aoff[k]) : nullptr;
+    L.aux = nullptr;
     L.mx = a.mx[k];
     L.plane = a.plane[k];
     L.dx = a.dx[k];
     L.bl = a.mthbc[0];
     L.br = a.mthbc[1];
-    L.mcapa = a.mcapa;
+    L.mcapa = 0;
     L.kind = a.sd.kind;
     L.stage = a.stage;
     L.ixy = 1;
-    const int c0 = 1 + (t - a.prefix[lo]) * (2 * NT - 1);
-    if (tid == 0) sm.dtdx = ctl->dt / L.dx;
-    for (int j = tid; j < 2 * NT + 5; j += NT) {
-      const long g = (long)c0 - 1 + j;
-      const bool ok = g < (long)L.mx + 6;
-#pragma unroll
-      for (int m = 0; m < 3; ++m) sm.sq[m][j] = ok ? L.qin[(long)m * L.plane + g] : (S)1;
+    L.dt = ctl->dt;
+    const int c0 = (t - a.prefix[lo]) * PairGeom<PREC, NT>::STRIDE;
+    PairWin<PREC, NT>* wo = L.qo ? &sm.so : nullptr;
+    if (tid == 0) {
+      sm.dtdx = L.dt / L.dx;
+      pair_issue<PREC, NT>(L, c0, sm.sq, wo, &sm.bar);
     }
-    __syncthreads();
-    float cflmax = 0.0f;
+    if (!pair_wait(ctl, &sm.bar, parity)) return;
+    float smax = 0.0f;
     int bad = 0;
-    pair_compute<CD, PREC, NT>(L, a.ph, c0, &sm.sq[0][0], sm, sm.dtdx, cflmax, bad);
-    cflmax = warp_max(cflmax);
-    if ((tid & 31) == 0) sm.sred[tid >> 5] = cflmax;
-    const int anybad = __syncthreads_or(bad);
-    if (tid < 32) {
-      float v = (tid < NT / 32) ? sm.sred[tid] : 0.0f;
-      v = warp_max(v);
-      if (tid == 0) {
-        atomic_max_nonneg(&ctl->stage_cfl[a.stage], (double)v);
-        if (anybad) atomicOr(&ctl->status, SCL_STATUS_NONFINITE);
-      }
-    }
+    pair_compute<CD, PREC, NT, true>(L, a.ph, c0, sm.sq, wo, sm.rec, sm.dtdx, smax, bad);
+    pair_reduce<NT>(ctl, a.stage, sm.sred, sm.dtdx, smax, bad);
   }
 }
 

@@ -4,8 +4,10 @@ setrun.py) can be started here from the same file.
 
 The file is what setrun.py writes: a comment header, then one record per
 item, `value(s) =: name (description)`.  As the Fortran list-directed reads
-do, each read takes the leading values of the next non-blank record; blank
-records and `#` lines are skipped.  The plugin id and its physical constants
+do, each read starts at the next non-blank record and takes as many values
+as it asks for, continuing onto the following records when one record holds
+fewer (the rest of its last record is skipped); blank records and `#` lines
+are skipped.  The plugin id and its physical constants
 (the app's setprob.data) are not in this file: pass them to `claw_params`.
 """
 from __future__ import annotations
@@ -25,11 +27,19 @@ def read_sharpclaw_data(path: str) -> dict:
     with open(path) as f:
         recs = _records(f.read())
 
+    def nvals(n, conv=float):
+        # one list-directed read of n values (main.f90:78 tout(1:nout),
+        # :106 mthlim(1:mwaves)): records are consumed until n values are read
+        vals = []
+        while len(vals) < n:
+            try:
+                vals += next(recs)
+            except StopIteration:
+                raise ValueError(f"{path}: end of file after {len(vals)} of {n} values") from None
+        return [conv(v) for v in vals[:n]]
+
     def nxt(n=1, conv=float):
-        vals = next(recs)
-        if len(vals) < n:
-            raise ValueError(f"{path}: expected {n} values, got {vals}")
-        out = [conv(v) for v in vals[:n]]
+        out = nvals(n, conv)
         return out if n > 1 else out[0]
 
     def ival(v):
@@ -43,7 +53,7 @@ def read_sharpclaw_data(path: str) -> dict:
     if d["outstyle"] == 1:                                              # :72-84
         d["tfinal"] = nxt()
     elif d["outstyle"] == 2:
-        d["tout"] = [float(v) for v in next(recs)[:d["nout"]]]
+        d["tout"] = nvals(d["nout"])
     elif d["outstyle"] == 3:
         d["nstepout"], d["nstop"] = nxt(2, ival)
         d["nout"] = d["nstop"]
@@ -55,7 +65,7 @@ def read_sharpclaw_data(path: str) -> dict:
     for k in ("dt_variable", "time_integrator", "verbosity", "src_term", "mcapa", "maux",
               "tfluct_solver", "char_decomp", "meqn", "mwaves", "lim_type"):   # :93-104
         d[k] = nxt(conv=ival)
-    d["mthlim"] = [ival(v) for v in next(recs)[:d["mwaves"]]]          # :106
+    d["mthlim"] = nvals(d["mwaves"], ival)                              # :106
     d["t0"] = nxt()                                                     # :109
     d["xlower"], d["xupper"] = [], []
     for _ in range(d["ndim"]):                                          # :112-115

@@ -361,3 +361,18 @@ def stegoton(mx=200, char_decomp=0, tfluct_solver=1, mthbc=(1, 1), amp=0.05):
     po = O.make_params(meqn=2, mwaves=2, maux=3, rp=O.RP_STEGOTON, **kw)
     ps = S.ClawParams(rp=S.RP_STEGOTON, **kw)
     return po, ps, q, aux
+
+
+def oracle_riemann_window(job):
+    """Process-pool worker: the oracle's sharpclaw() on one 1-D Euler Riemann
+    instance of the batched workload (Roe + entropy fix, componentwise WENO5,
+    tfluct_solver 0, SSPRK(3,3), extrapolation bc) over [0, tend].  job =
+    (mx, dx, q, dt_initial, tend, (cfl_max, cfl_desired)); returns the final q
+    and the run's outputs as a dict."""
+    mx, dx, q, dt0, tend, (cfl_max, cfl_desired) = job
+    po = O.make_params(mx=mx, meqn=3, mwaves=3, dx=dx, rp=O.RP_EULER, gamma=1.4, mthbc=(1, 1),
+                       char_decomp=0, tfluct_solver=0)
+    qo, ro = O.sharpclaw(po, q, None, tstart=0.0, tend=tend, dt_initial=dt0, cfl_max=cfl_max,
+                         cfl_desired=cfl_desired, time_integrator=3)
+    return qo, dict(steps_taken=ro.steps_taken, rejected=ro.rejected, info=ro.info, tend=ro.tend,
+                    dt_last=ro.dt_last, cfl_maxused=ro.cfl_maxused)

@@ -120,3 +120,26 @@ def test_header_is_plain_c_and_links(tmp_path):
     assert "sm_100a" in first and first.endswith(" %d" % len(names))
     frame = (tmp_path / "fort.q0007").read_text()
     assert "0.10000000E+01" in frame and "0.40000000E+01" in frame
+
+
+def test_noalloc_refuses_a_host_array():
+    """scl_rk_step_noalloc takes caller-owned device memory; given a host
+    (numpy) array it launches nothing and returns an error status instead of
+    letting a kernel dereference host memory.  Without a GPU the call stops at
+    'no usable CUDA device'; the GPU test checks SCL_E_INVALID there."""
+    import numpy as np
+    import torch
+    p = S.ClawParams(rp=S.RP_EULER, mx=64, dx=0.1, mthbc=(1, 1), char_decomp=2, tfluct_solver=0,
+                     time_integrator=3)
+    cp = p.to_c(C.FP64)
+    q = np.ones((3, 70))
+    cfl = ctypes.c_double(0.0)
+    rc = C.lib().scl_rk_step_noalloc(ctypes.byref(cp), ctypes.c_void_p(q.ctypes.data), None, 1e-3,
+                                     ctypes.byref(cfl), None)
+    assert rc in (C.SCL_E_CUDA, C.SCL_E_INVALID)
+    msg = C.lib().scl_last_error()
+    if not torch.cuda.is_available():
+        assert b"no usable CUDA device" in msg
+    else:
+        assert rc == C.SCL_E_INVALID and b"q_dev" in msg
+    assert np.all(q == 1.0)

@@ -54,3 +54,30 @@ def test_read_2d_outstyle2(tmp_path):
     assert (p.mx, p.my, p.ndim) == (40, 30, 2) and p.dx == 5.0 / 40 and p.dy == 3.0 / 30
     assert p.ylower == -1.5 and tuple(p.mthbc) == (3, 1, 2, 2) and p.char_decomp == 1
     assert S.run_settings(d)["tout"] == [0.1, 0.25, 0.5]
+
+
+def test_list_directed_reads_continue_across_records(tmp_path):
+    """tout(1:nout) (main.f90:78) and mthlim(1:mwaves) (:106) are list-directed
+    reads: when one record holds fewer values they continue onto the next
+    records, and every later item is read from the record after them."""
+    f = tmp_path / "sharpclaw.data"
+    lines = [HEADER, "1 =: ndim", "200 =: mx", "5 =: nout", "2 =: outstyle",
+             "0.1 0.2", "0.3", "0.4 0.5 =: tout", "0.01 =: dt_initial", "1e99 =: dt_max", "0.9 =: cfl_max",
+             "0.8 =: cfl_desired", "500 =: max_steps", "1 =: dt_variable", "3 =: time_integrator",
+             "0 =: verbosity", "0 =: src_term", "0 =: mcapa", "0 =: maux", "0 =: tfluct_solver",
+             "2 =: char_decomp", "3 =: meqn", "3 =: mwaves", "2 =: lim_type", "1 2", "3 =: mthlim",
+             "0.0 =: t0", "-5.0 =: xlower", "5.0 =: xupper", "3 =: mbc", "1 =: mthbc_xlower",
+             "1 =: mthbc_xupper"]
+    f.write_text("\n".join(lines) + "\n")
+    d = S.read_sharpclaw_data(str(f))
+    assert d["tout"] == [0.1, 0.2, 0.3, 0.4, 0.5]
+    assert d["dt_initial"] == 0.01 and d["max_steps"] == 500
+    assert d["mthlim"] == [1, 2, 3] and d["t0"] == 0.0 and d["xlower"] == [-5.0] and d["mthbc"] == [1, 1]
+
+
+def test_truncated_file_is_an_error(tmp_path):
+    import pytest
+    f = tmp_path / "sharpclaw.data"
+    f.write_text(HEADER + "1 =: ndim\n200 =: mx\n4 =: nout\n2 =: outstyle\n0.1 0.2 =: tout\n")
+    with pytest.raises(ValueError, match="end of file"):
+        S.read_sharpclaw_data(str(f))
