@@ -233,6 +233,22 @@ int scl_kernels_per_step(scl_handle* h);
 #define SCL_RUN_RESIDENT 2
 int scl_set_run_mode(scl_handle* h, int mode);
 
+/* Conserved totals (no counterpart in the reference, which keeps none).
+ * With on = 1, scl_sharpclaw and scl_time_steps keep for every component m
+ *   T_m = sum over interior cells of q(i[,j],m) [* aux(i[,j],mcapa)] * dx [* dy]
+ * in FP64 with compensated (error-free two-sum) accumulation, whatever the
+ * arithmetic form of the stages: at the start of the run and after every
+ * accepted step, with the largest |T_m - T_m(start)| over the run's accepted
+ * steps.  It costs one kernel per step (one read of q).  Graph runs only:
+ * with totals on, SCL_RUN_AUTO uses graphs and SCL_RUN_RESIDENT is refused. */
+int scl_set_totals(scl_handle* h, int on);
+
+/* The totals of the last scl_sharpclaw / scl_time_steps: at its start (tot0),
+ * of the current state (tot) and the largest drift |tot - tot0| over its
+ * accepted steps (drift); meqn values each, any pointer may be NULL.
+ * SCL_E_INVALID when totals are off. */
+int scl_conserved_totals(scl_handle* h, double* tot0, double* tot, double* drift);
+
 /* The mode the last scl_sharpclaw / scl_time_steps ran in (SCL_RUN_GRAPH or
  * SCL_RUN_RESIDENT) and the kernels it launched (graph nodes counted one by
  * one); either out pointer may be NULL. */

@@ -283,6 +283,22 @@ class Solver:
         (default): resident up to 1016 cells."""
         C.check(C.lib().scl_set_run_mode(self._h, int(mode)), "scl_set_run_mode")
 
+    def set_totals(self, on: bool = True):
+        """Keep the conserved totals sum(q [* kappa]) * dx [* dy] of every
+        component in FP64 with compensated summation, at the start of each
+        sharpclaw() / time_steps() run and after every accepted step (one
+        kernel per step).  Graph runs only."""
+        C.check(C.lib().scl_set_totals(self._h, int(bool(on))), "scl_set_totals")
+
+    def conserved_totals(self):
+        """dict(tot0, tot, drift) of the last run: the totals at its start, of
+        the current state, and the largest |tot - tot0| over its accepted
+        steps (numpy arrays of meqn values)."""
+        m = self.params.meqn
+        a, b, c = (np.zeros(m) for _ in range(3))
+        C.check(C.lib().scl_conserved_totals(self._h, _ptr(a), _ptr(b), _ptr(c)), "scl_conserved_totals")
+        return {"tot0": a, "tot": b, "drift": c}
+
     def last_run(self):
         """(mode, kernel launches) of the last sharpclaw() / time_steps()."""
         m, n = ctypes.c_int(), ctypes.c_longlong()

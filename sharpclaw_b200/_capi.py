@@ -113,6 +113,8 @@ SIGNATURES = [
     ("scl_adjoint_step", ctypes.c_int, [_h, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_double]),
     ("scl_stream", ctypes.c_void_p, [_h]),
+    ("scl_set_totals", ctypes.c_int, [_h, ctypes.c_int]),
+    ("scl_conserved_totals", ctypes.c_int, [_h, _dp, _dp, _dp]),
 ]
 
 _lib = None

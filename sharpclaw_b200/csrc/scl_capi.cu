@@ -17,6 +17,7 @@
 #include "scl_ctl.cuh"
 #include "scl_frames.h"
 #include "scl_launch.h"
+#include "scl_totals.cuh"
 
 using namespace scl;
 
@@ -284,6 +285,9 @@ struct scl_handle {
   int run_mode = SCL_RUN_AUTO;
   int last_mode = SCL_RUN_AUTO;
   long long last_launches = 0;
+  // conserved totals (scl_set_totals): on/off and the totals kernel's per-CTA partial sums
+  int totals_on = 0;
+  double* tot_partials = nullptr;
 };
 
 namespace {
@@ -354,6 +358,30 @@ int download_ctl(scl_handle* h) {
   return SCL_OK;
 }
 
+// CTAs of the totals kernel (a few per SM, to keep HBM busy)
+constexpr int TOT_BLOCKS = 148 * 8;
+
+// Totals of the state in `role` (scl_totals.cuh): mode 0 -> the step's
+// candidate (tot_cand), mode 1 -> the run's start (tot0 = tot, drift = 0).
+void launch_totals(scl_handle* h, int role, int mode) {
+  TotalsArgs t{};
+  t.ctl = h->ctl;
+  for (int r = 0; r < NROLES; ++r) t.buf[r] = h->buf[r];
+  t.role = role;
+  t.mode = mode;
+  t.mx = h->p.mx;
+  t.my = h->p.ndim == 2 ? h->p.my : 1;
+  t.ndim = h->p.ndim;
+  t.meqn = h->p.meqn;
+  t.pitch = h->pitch;
+  t.plane = h->plane;
+  t.capa = h->p.mcapa > 0 ? static_cast<const char*>(h->aux) + h->ssize * h->plane * (h->p.mcapa - 1) : nullptr;
+  t.area = h->p.ndim == 2 ? h->p.dx * h->p.dy : h->p.dx;
+  t.partials = h->tot_partials;
+  if (h->ssize == sizeof(double)) k_totals<double><<<TOT_BLOCKS, TOT_NT, 0, h->stream>>>(t);
+  else k_totals<float><<<TOT_BLOCKS, TOT_NT, 0, h->stream>>>(t);
+}
+
 // enqueue the stages of one RK step on the handle's stream
 int enqueue_stages(scl_handle* h) {
   for (int s = 0; s < h->nstages; ++s) {
@@ -386,6 +414,7 @@ int enqueue_step(scl_handle* h, bool first = true, bool last = true) {
   }
   int rc = enqueue_stages(h);
   if (rc) return rc;
+  if (h->totals_on) launch_totals(h, h->final_role, 0);   // the candidate q^{n+1}; kept if accepted
   if (last) k_end_step<<<1, 1, 0, h->stream>>>(h->ctl, h->nstages - 1, h->final_role);
   else k_end_begin<<<1, 1, 0, h->stream>>>(h->ctl, h->nstages - 1, h->final_role);
   CK(cudaGetLastError());
@@ -394,7 +423,8 @@ int enqueue_step(scl_handle* h, bool first = true, bool last = true) {
 
 // launches per step inside a graph (plus one begin per graph replay)
 int kernels_per_step(const scl_handle* h) {
-  return h->nstages * (h->p.bc_user ? 2 : 1) + 1 + (h->L.ghost ? 1 : 0) + (h->b4kind != SCL_B4STEP_NONE ? 1 : 0);
+  return h->nstages * (h->p.bc_user ? 2 : 1) + 1 + (h->L.ghost ? 1 : 0) + (h->b4kind != SCL_B4STEP_NONE ? 1 : 0) +
+         (h->totals_on ? 1 : 0);
 }
 
 // Capture `steps` controller steps (begin, stages, end) into one executable
@@ -659,6 +689,7 @@ int scl_destroy(scl_handle* h) {
   if (h->stage64) cudaFree(h->stage64);
   if (h->adj) cudaFree(h->adj);
   if (h->aux0) cudaFree(h->aux0);
+  if (h->tot_partials) cudaFree(h->tot_partials);
   if (h->ctl) cudaFree(h->ctl);
   if (h->hctl) cudaFreeHost(h->hctl);
   if (h->hdone) cudaFreeHost(h->hdone);
@@ -775,9 +806,8 @@ int scl_flux1(scl_handle* h, const double* q1d, const double* aux1d, double* dq1
   const long ld = mx + 2 * p1.mbc, pitch = (ld + 31) / 32 * 32;
   const size_t ss = h->ssize;
   void *dq_in = nullptr, *dq_aux = nullptr;
-  double *d64 = nullptr, *dctl_dummy = nullptr;
+  double* d64 = nullptr;
   Ctl* dctl = nullptr;
-  (void)dctl_dummy;
   auto cleanup = [&]() {
     cudaFree(dq_in); cudaFree(dq_aux); cudaFree(d64); cudaFree(dctl);
   };
@@ -898,6 +928,7 @@ int init_run(scl_handle* h, const scl_run* run, int max_steps, scl_result* res, 
   c->info = 0;
   c->status = 0;
   c->dt_variable = run->dt_variable;
+  c->totals = h->totals_on;
   memset(res, 0, sizeof(*res));
   if (run->dt_variable == 0) {
     if (run->tend < run->tstart) {
@@ -917,6 +948,10 @@ int init_run(scl_handle* h, const scl_run* run, int max_steps, scl_result* res, 
     return SCL_OK;
   }
   int rc = upload_ctl(h);
+  if (rc == SCL_OK && h->totals_on) {
+    launch_totals(h, ROLE_Q, 1);   // the run's starting totals
+    CK(cudaGetLastError());
+  }
   if (rc == SCL_OK && h->nvariants > 1 && !h->tiles_fixed && !h->tiles_tuned) rc = tune_tiles(h);
   return rc;
 }
@@ -975,7 +1010,7 @@ int resident_tiles(const scl_handle* h) { return (h->p.mx + RES_NT - 2) / (RES_N
 // b4step hook (the hooks run as kernels of the step graph).
 bool resident_possible(const scl_handle* h) {
   return h->p.ndim == 1 && h->L.run != nullptr && h->b4kind == SCL_B4STEP_NONE && !h->p.bc_user &&
-         resident_tiles(h) <= RES_MAX_TILES;
+         !h->totals_on && resident_tiles(h) <= RES_MAX_TILES;
 }
 
 int use_resident(const scl_handle* h, bool* yes) {
@@ -983,7 +1018,8 @@ int use_resident(const scl_handle* h, bool* yes) {
   if (h->run_mode == SCL_RUN_GRAPH) return SCL_OK;
   if (h->run_mode == SCL_RUN_RESIDENT) {
     if (!resident_possible(h))
-      return fail(SCL_E_UNSUPPORTED, "resident run: needs a 1-D grid of at most 64 tiles, no b4step hook and no user bc");
+      return fail(SCL_E_UNSUPPORTED,
+                  "resident run: needs a 1-D grid of at most 64 tiles, no b4step hook, no user bc and no totals");
     *yes = true;
     return SCL_OK;
   }
@@ -1117,8 +1153,34 @@ int scl_set_run_mode(scl_handle* h, int mode) {
   if (mode != SCL_RUN_AUTO && mode != SCL_RUN_GRAPH && mode != SCL_RUN_RESIDENT)
     return fail(SCL_E_INVALID, "run mode must be SCL_RUN_AUTO, SCL_RUN_GRAPH or SCL_RUN_RESIDENT");
   if (mode == SCL_RUN_RESIDENT && !resident_possible(h))
-    return fail(SCL_E_UNSUPPORTED, "resident run: needs a 1-D grid of at most 64 tiles and no b4step hook");
+    return fail(SCL_E_UNSUPPORTED,
+                "resident run: needs a 1-D grid of at most 64 tiles, no b4step hook, no user bc and no totals");
   h->run_mode = mode;
+  return SCL_OK;
+}
+
+int scl_set_totals(scl_handle* h, int on) {
+  if (!h) return fail(SCL_E_INVALID, "null handle");
+  if (on != 0 && on != 1) return fail(SCL_E_INVALID, "on must be 0 or 1");
+  if (on && !h->tot_partials) {
+    if (cudaMalloc(&h->tot_partials, sizeof(double) * TOT_BLOCKS * MAXEQ * 2) != cudaSuccess)
+      return fail(SCL_E_CUDA, "cudaMalloc totals partials");
+  }
+  if (on && h->run_mode == SCL_RUN_RESIDENT) return fail(SCL_E_UNSUPPORTED, "totals are kept by graph runs only");
+  if (h->totals_on != on && h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }   // one kernel more or less per step
+  h->totals_on = on;
+  return SCL_OK;
+}
+
+int scl_conserved_totals(scl_handle* h, double* tot0, double* tot, double* drift) {
+  if (!h) return fail(SCL_E_INVALID, "null handle");
+  if (!h->totals_on) return fail(SCL_E_INVALID, "totals are off (scl_set_totals)");
+  const Ctl* c = h->hctl;   // as the last run left it (downloaded at its end)
+  for (int m = 0; m < h->p.meqn; ++m) {
+    if (tot0) tot0[m] = c->tot0[m];
+    if (tot) tot[m] = c->tot[m];
+    if (drift) drift[m] = c->drift[m];
+  }
   return SCL_OK;
 }
 

@@ -62,6 +62,11 @@ struct __align__(16) Ctl {
   int fresh;                    // 1: the current step is a new one (b4step runs), 0: a retake
   int bc_switched;              // the user bc switched both sides to periodic (persistent)
   int b4_done;                  // the time-reversal b4step has fired (persistent)
+  // conserved totals (scl_set_totals): per component, at the run's start, of
+  // the accepted state, of the step's candidate, and the largest |tot - tot0|
+  int totals;                   // 1: kept after every accepted step
+  unsigned int tot_ticket;      // CTAs of the totals kernel that are done (self-resetting)
+  double tot0[MAXEQ], tot[MAXEQ], tot_cand[MAXEQ], drift[MAXEQ];
 };
 
 // Physics constants of the plugins (COMMON blocks /comrp/, /param/).

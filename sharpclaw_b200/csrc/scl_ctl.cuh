@@ -60,6 +60,12 @@ __device__ __forceinline__ void ctl_end(Ctl* c, int last_stage, int final_role) 
     const int tmp = c->role[ROLE_Q];
     c->role[ROLE_Q] = c->role[final_role];
     c->role[final_role] = tmp;
+    if (c->totals) {                  // the accepted state's totals (scl_totals.cuh)
+      for (int m = 0; m < MAXEQ; ++m) {
+        c->tot[m] = c->tot_cand[m];
+        c->drift[m] = fmax(c->drift[m], fabs(c->tot[m] - c->tot0[m]));
+      }
+    }
   } else {                                                          // :198-216 reject
     c->t = c->told;
     c->rejected += 1;

@@ -43,9 +43,9 @@ namespace {
 
 // Three stage registers (A, B, R1) of at most SCL_NOALLOC_MAX_VALUES doubles
 // each, plus the controller block that carries dt, the buffer roles and the
-// per-stage CFL numbers: 3 * 196608 * 8 B + 256 B = 4.5 MiB + 256 B per GPU.
+// per-stage CFL numbers: 3 * 196608 * 8 B + 512 B = 4.5 MiB + 512 B per GPU.
 constexpr long kMaxValues = SCL_NOALLOC_MAX_VALUES;
-constexpr size_t kCtlBytes = 256;
+constexpr size_t kCtlBytes = 512;
 static_assert(sizeof(Ctl) <= kCtlBytes, "controller block does not fit its scratch slot");
 constexpr size_t kScratchBytes = kCtlBytes + 3 * sizeof(double) * kMaxValues;
 
