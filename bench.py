@@ -354,8 +354,10 @@ def run_gpu(args, rank, world, local_rank):
     def timed_steps(s):
         return s.time_steps(nstep, W["dt0"], cfl_max, cfl_des, tend=W["tend"], dt_variable=W["dt_variable"])
 
-    def device_run(precision, clocks):
+    def device_run(precision, clocks, totals=False):
         s = S.Solver(ps, precision)
+        if totals:
+            s.set_totals(True)
         if aux0 is not None:
             s.set_aux(aux0)
         s.set_q(q0)
@@ -388,6 +390,17 @@ def run_gpu(args, rank, world, local_rank):
     s_64, ms_64, res_64, taken_64, rej_64 = device_run("fp64", clocks)
     value64, s_max = job_rate(W["cells"] * W["stages"] * taken_64, ms_64 / 1000.0, world, dev)
     ms_64 = 1000.0 * s_max
+    # the headline form with the FP64 conserved-total bookkeeping on (one
+    # compensated-sum kernel per step); the drift is the largest change of
+    # the totals over a timed run (boundary fluxes included: this grid has
+    # extrapolation boundaries)
+    s_tot, ms_tot, _, taken_tot, _ = device_run(args.precision, clocks, totals=True)
+    value_tot, _ = job_rate(W["cells"] * W["stages"] * taken_tot, ms_tot / 1000.0, world, dev)
+    T = s_tot.conserved_totals()
+    totals = {"value": value_tot, "unit": UNIT, "overhead": value / value_tot - 1.0,
+              "tot0": T["tot0"].tolist(), "tot": T["tot"].tolist(), "drift": T["drift"].tolist(),
+              "note": "one FP64 compensated-sum kernel per time step; totals of the last timed run"}
+    s_tot.close()
 
     # the fused stage kernels alone (roofline): the stage launches of one step
     peak, peak_kind = measured_peaks()
@@ -549,6 +562,7 @@ def run_gpu(args, rank, world, local_rank):
                 "fp64": {"value": value64, "unit": UNIT, "ms_per_step": ms_64 / args.steps,
                          "roofline": roof["fp64"], "speedup_of_headline": value / value64},
                 "rejected_steps": rej_mix,
+                "totals": totals,
                 "accuracy": acc,
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,

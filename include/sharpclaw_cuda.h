@@ -239,8 +239,8 @@ int scl_set_run_mode(scl_handle* h, int mode);
  * in FP64 with compensated (error-free two-sum) accumulation, whatever the
  * arithmetic form of the stages: at the start of the run and after every
  * accepted step, with the largest |T_m - T_m(start)| over the run's accepted
- * steps.  It costs one kernel per step (one read of q).  Graph runs only:
- * with totals on, SCL_RUN_AUTO uses graphs and SCL_RUN_RESIDENT is refused. */
+ * steps.  Step graphs add one kernel per step (one read of q); a
+ * cluster-resident run sums the last stage's outputs in its tile code. */
 int scl_set_totals(scl_handle* h, int on);
 
 /* The totals of the last scl_sharpclaw / scl_time_steps: at its start (tot0),
@@ -248,6 +248,18 @@ int scl_set_totals(scl_handle* h, int on);
  * accepted steps (drift); meqn values each, any pointer may be NULL.
  * SCL_E_INVALID when totals are off. */
 int scl_conserved_totals(scl_handle* h, double* tot0, double* tot, double* drift);
+
+/* Failure-detection test hook (no counterpart in the reference).  The 1-D
+ * Euler stage kernels stage their tiles by bulk copies completed on an
+ * mbarrier, and every wait on it is bounded (1 s of device time): a thread whose wait runs
+ * out raises SCL_STATUS_TIMEOUT, waits once more (bounded) for copies still
+ * in flight and finishes; the controller then discards the step and stops
+ * the run (q = qold), and the call returns SCL_E_TIMEOUT.  With on = 1 the
+ * handle's stage launches announce 16 bytes more than they copy and bound
+ * each wait at 1 ms, so every wait runs out: this exercises that path on a
+ * GPU without faulting or hanging it (tests only; on = 0 restores normal
+ * operation). */
+int scl_test_wait_timeout(scl_handle* h, int on);
 
 /* The mode the last scl_sharpclaw / scl_time_steps ran in (SCL_RUN_GRAPH or
  * SCL_RUN_RESIDENT) and the kernels it launched (graph nodes counted one by

@@ -287,7 +287,8 @@ class Solver:
         """Keep the conserved totals sum(q [* kappa]) * dx [* dy] of every
         component in FP64 with compensated summation, at the start of each
         sharpclaw() / time_steps() run and after every accepted step (one
-        kernel per step).  Graph runs only."""
+        kernel per step in graph runs; summed by the tile code in
+        cluster-resident runs)."""
         C.check(C.lib().scl_set_totals(self._h, int(bool(on))), "scl_set_totals")
 
     def conserved_totals(self):

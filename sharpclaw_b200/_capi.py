@@ -115,6 +115,7 @@ SIGNATURES = [
     ("scl_stream", ctypes.c_void_p, [_h]),
     ("scl_set_totals", ctypes.c_int, [_h, ctypes.c_int]),
     ("scl_conserved_totals", ctypes.c_int, [_h, _dp, _dp, _dp]),
+    ("scl_test_wait_timeout", ctypes.c_int, [_h, ctypes.c_int]),
 ]
 
 _lib = None

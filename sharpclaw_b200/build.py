@@ -35,6 +35,10 @@ UNITS = {
     "scl_prec_fp64s.cu": ["--fmad=false"],
     "scl_prec_mixed.cu": ["--fmad=true"] + FAST32,
     "scl_prec_fp32.cu": ["--fmad=true"] + FAST32,
+    "scl_prec_fp64_2d.cu": ["--fmad=true"],
+    "scl_prec_fp64s_2d.cu": ["--fmad=false"],
+    "scl_prec_mixed_2d.cu": ["--fmad=true"] + FAST32,
+    "scl_prec_fp32_2d.cu": ["--fmad=true"] + FAST32,
 }
 
 
@@ -68,8 +72,10 @@ def _compile(unit, extra, verbose):
 
 def build(verbose: bool = False, jobs: int | None = None) -> str:
     os.makedirs(OBJ, exist_ok=True)
-    with cf.ThreadPoolExecutor(max_workers=jobs or min(8, os.cpu_count() or 4)) as ex:
-        objs = list(ex.map(lambda kv: _compile(kv[0], kv[1], verbose), UNITS.items()))
+    # the large per-form units first, so the small ones fill the gaps
+    order = sorted(UNITS.items(), key=lambda kv: not kv[0].startswith("scl_prec_"))
+    with cf.ThreadPoolExecutor(max_workers=jobs or min(12, os.cpu_count() or 4)) as ex:
+        objs = list(ex.map(lambda kv: _compile(kv[0], kv[1], verbose), order))
     if _stale(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-Xcompiler", "-fPIC", "-o", LIB] + objs
         r = subprocess.run(cmd, capture_output=True, text=True)

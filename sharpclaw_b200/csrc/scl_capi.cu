@@ -86,7 +86,7 @@ __global__ void k_b4step_reverse(StageArgs a, int ld, double trtime) {
     go = !c->done && c->fresh && !c->b4_done && c->told + (double)1.0e-10f >= trtime;
   __syncthreads();
   if (!go) return;
-  S* q = static_cast<S*>(a.buf[c->role[ROLE_Q]]) + a.plane;   // component 2
+  S* q = static_cast<S*>(pick_buf(a.buf, c->role[ROLE_Q])) + a.plane;   // component 2
   for (int i = threadIdx.x; i < ld; i += blockDim.x) q[i] = -q[i];
   if (threadIdx.x == 0) c->b4_done = 1;
 }
@@ -121,7 +121,7 @@ __global__ void k_bc_user1d(StageArgs a, int meqn, int maux) {
     vr = a2 * wall_g0((t - t2) / tw2);
   }
   __syncthreads();
-  S* q = static_cast<S*>(a.buf[c->role[a.sd.in]]);
+  S* q = static_cast<S*>(pick_buf(a.buf, c->role[a.sd.in]));
   S* aux = static_cast<S*>(const_cast<void*>(a.aux));
   const int mx = a.mx, k = threadIdx.x;
   const int bl = sw ? 2 : a.mthbc[0], br = sw ? 2 : a.mthbc[1];
@@ -288,6 +288,8 @@ struct scl_handle {
   // conserved totals (scl_set_totals): on/off and the totals kernel's per-CTA partial sums
   int totals_on = 0;
   double* tot_partials = nullptr;
+  // failure-detection test hook (scl_test_wait_timeout)
+  int test_timeout = 0;
 };
 
 namespace {
@@ -339,6 +341,10 @@ StageArgs make_args(const scl_handle* h, int s) {
   a.bc_user = h->p.bc_user;
   for (int k = 0; k < 6; ++k) a.wall[k] = h->p.wall[k];
   stage_time_form(h->p.time_integrator, s, &a.tform, &a.tc);
+  // bulk-copy waits: the default bound, or under the test hook a 1 ms bound
+  // and 16 bytes announced that no copy delivers
+  a.wait_ns = h->test_timeout ? 1000000ull : 0ull;
+  a.tx_extra = h->test_timeout ? 16u : 0u;
   return a;
 }
 
@@ -358,8 +364,16 @@ int download_ctl(scl_handle* h) {
   return SCL_OK;
 }
 
-// CTAs of the totals kernel (a few per SM, to keep HBM busy)
-constexpr int TOT_BLOCKS = 148 * 8;
+// CTAs of the totals kernel: at most four per SM (each takes the ticket with
+// one same-address atomic, which serialise in L2), fewer for small grids
+constexpr int TOT_BLOCKS = TOT_BLOCKS_MAX;
+
+template <class S, bool CAP>
+void launch_totals_m(int meqn, int nb, cudaStream_t st, const TotalsArgs& t) {
+  if (meqn == 1) k_totals<S, 1, CAP><<<nb, TOT_NT, 0, st>>>(t);
+  else if (meqn == 2) k_totals<S, 2, CAP><<<nb, TOT_NT, 0, st>>>(t);
+  else k_totals<S, 3, CAP><<<nb, TOT_NT, 0, st>>>(t);
+}
 
 // Totals of the state in `role` (scl_totals.cuh): mode 0 -> the step's
 // candidate (tot_cand), mode 1 -> the run's start (tot0 = tot, drift = 0).
@@ -378,8 +392,18 @@ void launch_totals(scl_handle* h, int role, int mode) {
   t.capa = h->p.mcapa > 0 ? static_cast<const char*>(h->aux) + h->ssize * h->plane * (h->p.mcapa - 1) : nullptr;
   t.area = h->p.ndim == 2 ? h->p.dx * h->p.dy : h->p.dx;
   t.partials = h->tot_partials;
-  if (h->ssize == sizeof(double)) k_totals<double><<<TOT_BLOCKS, TOT_NT, 0, h->stream>>>(t);
-  else k_totals<float><<<TOT_BLOCKS, TOT_NT, 0, h->stream>>>(t);
+  const long cells = (long)t.mx * t.my;
+  long nb = (cells + (long)TOT_U * TOT_NT - 1) / ((long)TOT_U * TOT_NT);
+  if (t.ndim == 2 && nb > t.my) nb = t.my;
+  nb = std::max(1L, std::min(nb, (long)TOT_BLOCKS));
+  const bool cap = t.capa != nullptr;
+  if (h->ssize == sizeof(double)) {
+    if (cap) launch_totals_m<double, true>(t.meqn, (int)nb, h->stream, t);
+    else launch_totals_m<double, false>(t.meqn, (int)nb, h->stream, t);
+  } else {
+    if (cap) launch_totals_m<float, true>(t.meqn, (int)nb, h->stream, t);
+    else launch_totals_m<float, false>(t.meqn, (int)nb, h->stream, t);
+  }
 }
 
 // enqueue the stages of one RK step on the handle's stream
@@ -784,6 +808,7 @@ int scl_step_dq(scl_handle* h, double* q, double* dq, double dt, double t, doubl
   rc = download_ctl(h);
   if (rc) return rc;
   if (cfl) *cfl = h->hctl->stage_cfl[0];
+  if (h->hctl->status & SCL_STATUS_TIMEOUT) return fail(SCL_E_TIMEOUT, "a bounded wait for staged data ran out");
   return SCL_OK;
 }
 
@@ -869,6 +894,8 @@ int scl_flux1(scl_handle* h, const double* q1d, const double* aux1d, double* dq1
         cudaMemcpyAsync(&c, dctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
         cudaStreamSynchronize(h->stream) != cudaSuccess)
       rc = fail(SCL_E_CUDA, "flux1 download");
+    else if (c.status & SCL_STATUS_TIMEOUT)
+      rc = fail(SCL_E_TIMEOUT, "a bounded wait for staged data ran out");
     else if (cfl)
       *cfl = c.stage_cfl[0];
   }
@@ -893,6 +920,7 @@ int scl_rk_step(scl_handle* h, double dt, double told, double* cfl) {
   rc = download_ctl(h);
   if (rc) return rc;
   const double cv = c->stage_cfl[h->nstages - 1];
+  if (c->status & SCL_STATUS_TIMEOUT) return fail(SCL_E_TIMEOUT, "a bounded wait for staged data ran out");
   std::swap(c->role[ROLE_Q], c->role[h->final_role]);
   if (cfl) *cfl = cv;
   if ((c->status & SCL_STATUS_NONFINITE) || cv != cv) return fail(SCL_E_NONFINITE, "non-finite stage output");
@@ -1010,7 +1038,7 @@ int resident_tiles(const scl_handle* h) { return (h->p.mx + RES_NT - 2) / (RES_N
 // b4step hook (the hooks run as kernels of the step graph).
 bool resident_possible(const scl_handle* h) {
   return h->p.ndim == 1 && h->L.run != nullptr && h->b4kind == SCL_B4STEP_NONE && !h->p.bc_user &&
-         !h->totals_on && resident_tiles(h) <= RES_MAX_TILES;
+         resident_tiles(h) <= RES_MAX_TILES;
 }
 
 int use_resident(const scl_handle* h, bool* yes) {
@@ -1018,8 +1046,7 @@ int use_resident(const scl_handle* h, bool* yes) {
   if (h->run_mode == SCL_RUN_GRAPH) return SCL_OK;
   if (h->run_mode == SCL_RUN_RESIDENT) {
     if (!resident_possible(h))
-      return fail(SCL_E_UNSUPPORTED,
-                  "resident run: needs a 1-D grid of at most 64 tiles, no b4step hook, no user bc and no totals");
+      return fail(SCL_E_UNSUPPORTED, "resident run: needs a 1-D grid of at most 64 tiles, no b4step hook and no user bc");
     *yes = true;
     return SCL_OK;
   }
@@ -1080,6 +1107,7 @@ int scl_sharpclaw(scl_handle* h, const scl_run* run, scl_result* res) {
   }
   if (rc) return rc;
   finish_run(h, res);
+  if (res->status & SCL_STATUS_TIMEOUT) return fail(SCL_E_TIMEOUT, "a bounded wait for staged data ran out");
   if (res->status & SCL_STATUS_NONFINITE) return fail(SCL_E_NONFINITE, "non-finite CFL number");
   return SCL_OK;
 }
@@ -1116,6 +1144,7 @@ int scl_time_steps(scl_handle* h, const scl_run* run, int nsteps, float* ms, scl
   }
   if (rc) return rc;
   finish_run(h, res);
+  if (res->status & SCL_STATUS_TIMEOUT) return fail(SCL_E_TIMEOUT, "a bounded wait for staged data ran out");
   return SCL_OK;
 }
 
@@ -1153,8 +1182,7 @@ int scl_set_run_mode(scl_handle* h, int mode) {
   if (mode != SCL_RUN_AUTO && mode != SCL_RUN_GRAPH && mode != SCL_RUN_RESIDENT)
     return fail(SCL_E_INVALID, "run mode must be SCL_RUN_AUTO, SCL_RUN_GRAPH or SCL_RUN_RESIDENT");
   if (mode == SCL_RUN_RESIDENT && !resident_possible(h))
-    return fail(SCL_E_UNSUPPORTED,
-                "resident run: needs a 1-D grid of at most 64 tiles, no b4step hook, no user bc and no totals");
+    return fail(SCL_E_UNSUPPORTED, "resident run: needs a 1-D grid of at most 64 tiles, no b4step hook and no user bc");
   h->run_mode = mode;
   return SCL_OK;
 }
@@ -1166,9 +1194,16 @@ int scl_set_totals(scl_handle* h, int on) {
     if (cudaMalloc(&h->tot_partials, sizeof(double) * TOT_BLOCKS * MAXEQ * 2) != cudaSuccess)
       return fail(SCL_E_CUDA, "cudaMalloc totals partials");
   }
-  if (on && h->run_mode == SCL_RUN_RESIDENT) return fail(SCL_E_UNSUPPORTED, "totals are kept by graph runs only");
   if (h->totals_on != on && h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }   // one kernel more or less per step
   h->totals_on = on;
+  return SCL_OK;
+}
+
+int scl_test_wait_timeout(scl_handle* h, int on) {
+  if (!h) return fail(SCL_E_INVALID, "null handle");
+  if (on != 0 && on != 1) return fail(SCL_E_INVALID, "on must be 0 or 1");
+  if (h->test_timeout != on && h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }   // captured arguments change
+  h->test_timeout = on;
   return SCL_OK;
 }
 

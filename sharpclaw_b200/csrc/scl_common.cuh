@@ -114,6 +114,12 @@ struct StageArgs {
   int bc_user, tform;
   double tc;
   double wall[6];
+  // bulk-copy staging: the bound of each mbarrier wait (ns of device time; 0
+  // means the default, 1 s) and extra bytes announced but never copied (0; a
+  // failure-detection test sets 16 so that every wait runs out, see
+  // scl_test_wait_timeout)
+  unsigned long long wait_ns;
+  unsigned int tx_extra;
 };
 
 // Arguments of a cluster-resident run of a 1-D grid (the whole controller
@@ -131,6 +137,17 @@ struct RunArgs {
 template <class R>
 __device__ __forceinline__ R nanmax(R a, R b) {
   return (b > a || b != b) ? b : a;
+}
+
+// The physical buffer of a role, buf[i] for a runtime i < NROLES, by selects:
+// indexing a kernel parameter array with a runtime index makes the compiler
+// copy the whole argument struct to local memory in every thread.
+template <class T>
+__device__ __forceinline__ T pick_buf(T const (&buf)[NROLES], int i) {
+  static_assert(NROLES == 4, "pick_buf selects among four buffers");
+  const T lo = i == 0 ? buf[0] : buf[1];
+  const T hi = i == 2 ? buf[2] : buf[3];
+  return i < 2 ? lo : hi;
 }
 
 // Atomic max of a non-negative double (or NaN) through its bit pattern:

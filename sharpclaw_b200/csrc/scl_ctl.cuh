@@ -26,6 +26,13 @@ __device__ __forceinline__ void ctl_begin(Ctl* c) {
 
 __device__ __forceinline__ void ctl_end(Ctl* c, int last_stage, int final_role) {
   if (c->done) return;
+  // A bounded wait of a stage kernel ran out (its staged data may be
+  // incomplete): discard the step and stop, q = qold; the host reports it.
+  if (c->status & SCL_STATUS_TIMEOUT) {
+    c->t = c->told;
+    c->done = 1;
+    return;
+  }
   const double cfl = c->stage_cfl[last_stage];   // the last stage's CFL (:184, A2)
   c->cfl_last = cfl;
   // A NaN CFL number cannot drive dt control (the reference would reject and

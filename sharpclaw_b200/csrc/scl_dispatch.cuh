@@ -1,7 +1,9 @@
 // scl_dispatch.cuh -- instantiates the stage kernels of one arithmetic form.
-// Included by one translation unit per form (scl_prec_*.cu) with
-// SCL_PREC_VALUE defined; the FP64_STRICT unit is compiled without FMA
-// contraction so its arithmetic follows the reference's evaluation order.
+// Included by two translation units per form (scl_prec_*.cu: the 1-D and
+// batched kernels, SCL_PART 1; scl_prec_*_2d.cu: the 2-D kernels, SCL_PART 2)
+// with SCL_PREC_VALUE defined, so the build compiles them in parallel; the
+// FP64_STRICT units are compiled without FMA contraction so their arithmetic
+// follows the reference's evaluation order.
 #pragma once
 #include <algorithm>
 #include <type_traits>
@@ -15,6 +17,9 @@
 #ifndef SCL_PREC_VALUE
 #error "SCL_PREC_VALUE must be defined"
 #endif
+#ifndef SCL_PART
+#error "SCL_PART must be defined (1: 1-D and batched kernels, 2: 2-D kernels)"
+#endif
 
 namespace scl {
 namespace SCL_PREC_NS {
@@ -25,21 +30,60 @@ using S = typename Prec<PREC>::S;
 
 constexpr int NT1 = 128;
 
+// Bulk-copy staging needs every role buffer on a 16-byte boundary and a
+// component stride that keeps the planes there (handles pad it to 32
+// elements; caller-owned arrays may not).
+inline bool bulk_staging_ok(const StageArgs& a) {
+  constexpr long AL = 16 / (long)sizeof(S);
+  if (a.plane % AL != 0) return false;
+  for (int r = 0; r < NROLES; ++r)
+    if (reinterpret_cast<uintptr_t>(a.buf[r]) % 16 != 0) return false;
+  return true;
+}
+
+// The Euler plugin in the FP64 forms: 118 registers unbounded (4 CTAs, 16
+// warps per SM); bounded to 6 CTAs per SM it spills a little and runs 9-12 %
+// faster, and its tiles are staged by bulk copies (measured at 2^20 and 2^23
+// cells).  Lighter plugins keep the compiler's register choice and stage by
+// the threads: their CTAs are short, and a bulk copy's latency then shows
+// (1-D advection at 2^26 cells: 777 us per stage staged by the threads,
+// 1027 us by bulk copies).
+template <class P>
+constexpr bool heavy1d() {
+  return std::is_same_v<P, PEuler> && Prec<PREC>::EXACT;
+}
+
 template <class P, int CD, int TF>
 void launch1d(const StageArgs& a, cudaStream_t st) {
   const int nb = (a.mx + NT1 - 2) / (NT1 - 1);
-  k_stage1d<P, CD, TF, PREC, NT1><<<nb, NT1, 0, st>>>(a);
+  if constexpr (heavy1d<P>()) {
+    if (bulk_staging_ok(a)) {
+      k_stage1d<P, CD, TF, PREC, NT1, true, 6><<<nb, NT1, 0, st>>>(a);
+      return;
+    }
+    k_stage1d<P, CD, TF, PREC, NT1, false, 6><<<nb, NT1, 0, st>>>(a);
+  } else {
+    k_stage1d<P, CD, TF, PREC, NT1><<<nb, NT1, 0, st>>>(a);
+  }
 }
 
-// One cluster of min(tiles, RES_CLUSTER) CTAs runs the controller loop.
+// One cluster of nc CTAs, T tiles each (T the fewest tiles per CTA with
+// nc <= RES_CLUSTER), runs the controller loop with the rows of every
+// buffer in shared memory.
 template <class P, int CD, int TF>
 cudaError_t launch_run1d(const RunArgs& a, cudaStream_t st) {
+  using S = typename Prec<PREC>::S;
   const int ntiles = (a.st.mx + RES_NT - 2) / (RES_NT - 1);
-  const int nc = std::min(ntiles, RES_CLUSTER);
+  const int T = (ntiles + RES_CLUSTER - 1) / RES_CLUSTER;
+  const int nc = (ntiles + T - 1) / T;
+  const size_t rows = run1d_rows_bytes<S>(P::MEQN, T, RES_NT);
+  auto k = k_run1d<P, CD, TF, PREC, RES_NT>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows);
+  if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nc, 1, 1);
-  cfg.blockDim = dim3(RES_NT, 1, 1);
-  cfg.dynamicSmemBytes = 0;
+  cfg.blockDim = dim3(run1d_threads<RES_NT>(), 1, 1);
+  cfg.dynamicSmemBytes = rows;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -48,7 +92,7 @@ cudaError_t launch_run1d(const RunArgs& a, cudaStream_t st) {
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_run1d<P, CD, TF, PREC, RES_NT>, a);
+  return cudaLaunchKernelEx(&cfg, k, a);
 }
 
 // 1-D Euler in the FP32 forms: two interfaces per thread in packed FP32
@@ -58,17 +102,6 @@ cudaError_t launch_run1d(const RunArgs& a, cudaStream_t st) {
 #endif
 constexpr int NTP = 128;
 
-// Bulk-copy staging needs every role buffer on a 16-byte boundary and a
-// component stride that keeps the planes there (handles pad it to 32
-// elements; caller-owned arrays may not).
-inline bool pair_tma_ok(const StageArgs& a) {
-  constexpr long AL = 16 / (long)sizeof(S);
-  if (a.plane % AL != 0) return false;
-  for (int r = 0; r < NROLES; ++r)
-    if (reinterpret_cast<uintptr_t>(a.buf[r]) % 16 != 0) return false;
-  return true;
-}
-
 template <int CD>
 void launch1d_pair(const StageArgs& a, cudaStream_t st) {
   if (a.mcapa > 0) {
@@ -76,7 +109,7 @@ void launch1d_pair(const StageArgs& a, cudaStream_t st) {
     return;
   }
   const int nb = a.mx / PairGeom<PREC, NTP>::STRIDE + 1;
-  if (pair_tma_ok(a)) k_stage1d_pair<CD, PREC, NTP, true><<<nb, NTP, 0, st>>>(a);
+  if (bulk_staging_ok(a)) k_stage1d_pair<CD, PREC, NTP, true><<<nb, NTP, 0, st>>>(a);
   else k_stage1d_pair<CD, PREC, NTP, false><<<nb, NTP, 0, st>>>(a);
 }
 
@@ -86,17 +119,28 @@ constexpr size_t smem2d() {
   return sizeof(S) * P::MEQN * T::WX * T::WY + sizeof(R) * 4 * P::MEQN * (T::NXI + T::NYI);
 }
 
+// CTAs per SM the 2-D kernel's registers are budgeted for: in the FP64 forms
+// the shallow-water kernel needs 120 registers unbounded (2 CTAs of 256
+// threads per SM); bounded to 3 (6 for the 128-thread shape) it spills a
+// little and runs 3.5-4 % faster at 4096^2 (16x15: 2196 -> 2119 us, 16x7:
+// 2438 -> 2340 us, 32x7: 2297 -> 2211 us).  The FP32 forms fit in 64
+// registers and keep the compiler's choice.
+template <int NT>
+constexpr int stage2d_minb() {
+  return Prec<PREC>::EXACT ? (NT == 256 ? 3 : 6) : 0;
+}
+
 template <class P, int CD, int TF, int TX, int TY, int NT>
 void launch2d(const StageArgs& a, cudaStream_t st) {
   dim3 grid((a.mx + TX - 1) / TX, (a.my + TY - 1) / TY);
-  k_stage2d<P, CD, TF, PREC, TX, TY, NT><<<grid, NT, smem2d<P, CD, TF, TX, TY, NT>(), st>>>(a);
+  k_stage2d<P, CD, TF, PREC, TX, TY, NT, stage2d_minb<NT>()><<<grid, NT, smem2d<P, CD, TF, TX, TY, NT>(), st>>>(a);
 }
 
 // dynamic shared memory above 48 KB must be opted into before launch (and
 // outside any stream capture), so it is done when the kernel is picked
 template <class P, int CD, int TF, int TX, int TY, int NT>
 bool prepare2d(Launchers* L) {
-  if (cudaFuncSetAttribute(k_stage2d<P, CD, TF, PREC, TX, TY, NT>,
+  if (cudaFuncSetAttribute(k_stage2d<P, CD, TF, PREC, TX, TY, NT, stage2d_minb<NT>()>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem2d<P, CD, TF, TX, TY, NT>()) != cudaSuccess)
     return false;
@@ -134,6 +178,7 @@ bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
   L->ghost = nullptr;
   L->run = nullptr;
   if (ndim == 1) {
+#if SCL_PART == 1
     if (variant != 0) return false;
     if (cd == 0 && tf == 0) fill1d<P, 0, 0>(L);
     if (cd == 1 && tf == 0) fill1d<P, 1, 0>(L);
@@ -162,7 +207,11 @@ bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
       if (cd == 2 && tf == 0) L->stage = &launch1d_pair<2>;
     }
     return L->stage != nullptr;
+#else
+    return false;
+#endif
   }
+#if SCL_PART == 2
   if constexpr (P::NDIM == 2) {
     if (cd == 0 && tf == 0) return fill2d<P, 0, 0>(variant, L);
     if (cd == 1 && tf == 0) return fill2d<P, 1, 0>(variant, L);
@@ -185,9 +234,11 @@ bool pick(int ndim, int cd, int tf, int variant, Launchers* L) {
       if (cd == 21 && tf == 1) return fill2d<P, 21, 1>(variant, L);
     }
   }
+#endif
   return false;
 }
 
+#if SCL_PART == 1
 // ---- batched persistent launchers ----
 template <class P, int CD, int TF, int NT>
 void launch_batch_stage(const BatchArgs& a, int grid, cudaStream_t st) {
@@ -261,8 +312,11 @@ bool pick_batch(int cd, int tf, int variant, BatchLaunchers* L) {
   return false;
 }
 
+#endif  // SCL_PART == 1
+
 }  // namespace SCL_PREC_NS
 
+#if SCL_PART == 1
 bool SCL_BATCH_GETTER(int rp, int cd, int tf, int variant, BatchLaunchers* L) {
   using namespace SCL_PREC_NS;
   switch (rp) {
@@ -273,26 +327,40 @@ bool SCL_BATCH_GETTER(int rp, int cd, int tf, int variant, BatchLaunchers* L) {
   return false;
 }
 
+bool SCL_PREC_GETTER_2D(int rp, int cd, int tf, int variant, Launchers* L);   // the form's 2-D unit
+
 bool SCL_PREC_GETTER(int rp, int ndim, int cd, int tf, int variant, Launchers* L) {
   using namespace SCL_PREC_NS;
+  if (ndim == 2) return SCL_PREC_GETTER_2D(rp, cd, tf, variant, L);
   switch (rp) {
-    case SCL_RP_ADVECTION: return ndim == 1 && pick<PAdvection>(ndim, cd, tf, variant, L);
-    case SCL_RP_EULER: return ndim == 1 && pick<PEuler>(ndim, cd, tf, variant, L);
+    case SCL_RP_ADVECTION: return pick<PAdvection>(ndim, cd, tf, variant, L);
+    case SCL_RP_EULER: return pick<PEuler>(ndim, cd, tf, variant, L);
     case SCL_RP_SW2D: return pick<PShallow2D>(ndim, cd, tf, variant, L);
-    case SCL_RP_ACOUSTICS1D: return ndim == 1 && pick<PAcoustics<2>>(ndim, cd, tf, variant, L);
+    case SCL_RP_ACOUSTICS1D: return pick<PAcoustics<2>>(ndim, cd, tf, variant, L);
     case SCL_RP_ACOUSTICS2D: return pick<PAcoustics<3>>(ndim, cd, tf, variant, L);
     case SCL_RP_ADVECTION2D: return pick<PAdvEdge2D>(ndim, cd, tf, variant, L);
-    case SCL_RP_SW1D: return ndim == 1 && pick<PShallow1D>(ndim, cd, tf, variant, L);
-    case SCL_RP_SWF_BATHY: return ndim == 1 && pick<PShallowF1D<0>>(ndim, cd, tf, variant, L);
-    case SCL_RP_SWF_RADIAL: return ndim == 1 && pick<PShallowF1D<1>>(ndim, cd, tf, variant, L);
-    case SCL_RP_SWF_KAPPA: return ndim == 1 && pick<PShallowF1D<2>>(ndim, cd, tf, variant, L);
-    case SCL_RP_ACOUSTICS_CONST: return ndim == 1 && pick<PAcousticsConst>(ndim, cd, tf, variant, L);
-    case SCL_RP_ACOUSTICS_FWAVE: return ndim == 1 && pick<PElasticFwave<0>>(ndim, cd, tf, variant, L);
-    case SCL_RP_STEGOTON: return ndim == 1 && pick<PElasticFwave<1>>(ndim, cd, tf, variant, L);
-    case SCL_RP_TRAFFIC: return ndim == 1 && pick<PTraffic>(ndim, cd, tf, variant, L);
-    case SCL_RP_ADVECTION_CONS: return ndim == 1 && pick<PAdvCons>(ndim, cd, tf, variant, L);
+    case SCL_RP_SW1D: return pick<PShallow1D>(ndim, cd, tf, variant, L);
+    case SCL_RP_SWF_BATHY: return pick<PShallowF1D<0>>(ndim, cd, tf, variant, L);
+    case SCL_RP_SWF_RADIAL: return pick<PShallowF1D<1>>(ndim, cd, tf, variant, L);
+    case SCL_RP_SWF_KAPPA: return pick<PShallowF1D<2>>(ndim, cd, tf, variant, L);
+    case SCL_RP_ACOUSTICS_CONST: return pick<PAcousticsConst>(ndim, cd, tf, variant, L);
+    case SCL_RP_ACOUSTICS_FWAVE: return pick<PElasticFwave<0>>(ndim, cd, tf, variant, L);
+    case SCL_RP_STEGOTON: return pick<PElasticFwave<1>>(ndim, cd, tf, variant, L);
+    case SCL_RP_TRAFFIC: return pick<PTraffic>(ndim, cd, tf, variant, L);
+    case SCL_RP_ADVECTION_CONS: return pick<PAdvCons>(ndim, cd, tf, variant, L);
   }
   return false;
 }
+#else
+bool SCL_PREC_GETTER_2D(int rp, int cd, int tf, int variant, Launchers* L) {
+  using namespace SCL_PREC_NS;
+  switch (rp) {
+    case SCL_RP_SW2D: return pick<PShallow2D>(2, cd, tf, variant, L);
+    case SCL_RP_ACOUSTICS2D: return pick<PAcoustics<3>>(2, cd, tf, variant, L);
+    case SCL_RP_ADVECTION2D: return pick<PAdvEdge2D>(2, cd, tf, variant, L);
+  }
+  return false;
+}
+#endif
 
 }  // namespace scl

@@ -8,10 +8,13 @@
 // stages its cells plus ghosts in shared memory, solves one interface per
 // thread into shared memory, then updates one cell per thread.
 #pragma once
+#include <cooperative_groups.h>
 #include <type_traits>
 
 #include "scl_common.cuh"
 #include "scl_plugins.cuh"
+#include "scl_tma.cuh"
+#include "scl_totals.cuh"
 #include "scl_weno.cuh"
 
 namespace scl {
@@ -391,43 +394,71 @@ __device__ __forceinline__ R load_aux(const void* aux, long off) {
 }
 
 // Running CFL maximum of flux1.f90:126-133 (max over waves of
-// max(dtdx(i)*s, -dtdx(i-1)*s)) and flux2.f90:47,80, kept in FP64 in every
-// arithmetic form.  The exact forms form the reference's products in double.
-// The FP32 forms keep the largest |s| per direction in R (exact) and
-// multiply it by dt/dx or dt/dy once, in double: with one dtdx per direction
-// max(dtdx s, -dtdx s) = dtdx |s|, and since rounding is monotonic that
-// product equals the maximum of the per-interface FP64 products.  Capacity
-// grids (a dtdx per cell) form each product in double.  NaN propagates.
+// max(dtdx(i)*s, -dtdx(i-1)*s)) and flux2.f90:47,80.  The exact forms form
+// the reference's products in double.  The FP32 forms keep the largest |s|
+// per direction (an exact FP32 maximum) and reduce it across the CTA in
+// FP32; one thread multiplies it by dt/dx (dt/dy) in double: with one dtdx
+// per direction max(dtdx s, -dtdx s) = dtdx |s|, and since rounding is
+// monotonic that product equals the maximum of the per-interface FP64
+// products, so the CFL number is FP64.  Capacity grids (a dtdx per cell)
+// form each product in FP64 and keep it rounded up to FP32 (an upper bound
+// within an FP32 ulp).  NaN propagates.
 template <class R>
 struct CflMax {
-  double v = 0.0;
-  R sx = (R)0, sy = (R)0;
+  double v = 0.0;          // exact forms
+  float sx = 0.f, sy = 0.f;  // FP32 forms: max |s| (or capacity products) along x / y
   template <int MW>
   __device__ __forceinline__ void add(const R* s, double d_c, double d_m, bool per_cell, bool isx) {
     if constexpr (std::is_same_v<R, double>) {
 #pragma unroll
       for (int w = 0; w < MW; ++w) v = nanmax(v, nanmax(d_c * s[w], -d_m * s[w]));
     } else {
+      float m = isx ? sx : sy;
       if (per_cell) {
 #pragma unroll
         for (int w = 0; w < MW; ++w) {
           const double sw = (double)s[w];
-          v = nanmax(v, nanmax(d_c * sw, -d_m * sw));
+          m = nanmax(m, __double2float_ru(nanmax(d_c * sw, -d_m * sw)));
         }
       } else {
-        R m = isx ? sx : sy;
 #pragma unroll
         for (int w = 0; w < MW; ++w) m = nanmax(m, fabsf(s[w]));
-        if (isx) sx = m; else sy = m;
       }
+      if (isx) sx = m; else sy = m;
     }
   }
-  // the thread's value, given the grid's dt/dx and dt/dy
-  __device__ __forceinline__ double value(double dtdx, double dtdy) const {
-    if constexpr (std::is_same_v<R, double>) return v;
-    else return nanmax(v, nanmax(dtdx * (double)sx, dtdy * (double)sy));
-  }
 };
+
+// CTA maximum of the threads' CflMax into one double, in thread 0 (the
+// other threads' return value is unused).  sred: NT/32 doubles, fred: 2 x
+// NT/32 floats of shared memory.  Contains the CTA barrier bar.sync and
+// returns the OR of `bad` over the CTA in *anybad.  Y: the y direction is
+// used (2-D).
+template <class R, int NT, bool Y = true>
+__device__ __forceinline__ double cfl_cta_max(const CflMax<R>& c, double dtdx, double dtdy, bool per_cell,
+                                              double* sred, float (*fred)[NT / 32], int bad, int* anybad) {
+  const int tid = threadIdx.x;
+  if constexpr (std::is_same_v<R, double>) {
+    const double w = warp_max(c.v);
+    if ((tid & 31) == 0) sred[tid >> 5] = w;
+    *anybad = __syncthreads_or(bad);
+    double v = 0.0;
+    if (tid < 32) v = warp_max((tid < NT / 32) ? sred[tid] : 0.0);
+    return v;
+  } else {
+    const float wx = warp_max(c.sx);
+    float wy = 0.f;
+    if constexpr (Y) wy = warp_max(c.sy);
+    if ((tid & 31) == 0) { fred[0][tid >> 5] = wx; fred[1][tid >> 5] = wy; }
+    *anybad = __syncthreads_or(bad);
+    float mx = 0.f, my = 0.f;
+    if (tid < 32) {
+      mx = warp_max((tid < NT / 32) ? fred[0][tid] : 0.f);
+      if constexpr (Y) my = warp_max((tid < NT / 32) ? fred[1][tid] : 0.f);
+    }
+    return per_cell ? nanmax((double)mx, (double)my) : nanmax(dtdx * (double)mx, dtdy * (double)my);
+  }
+}
 
 // ---------------------------------------------------------------------------
 // One line (a 1-D grid, a batched instance, or a line of a 2-D plugin) as a
@@ -450,7 +481,59 @@ struct Line {
   int src = SCL_SRC_NONE;  // source-term hook and the grid's lower edge (radial hook)
   double xlower = 0.0;
   double dt = 0.0;         // the controller's dt for this step (read with the roles)
+  unsigned long long wait_ns = MBAR_LIMIT_NS;   // bound of a bulk-copy wait
+  unsigned int tx_extra = 0;                    // test hook (StageArgs::tx_extra)
+  double dtdx = 0.0;       // dt/dx of the step (shared-memory resident runs)
 };
+
+// A tile of a cluster-resident run whose registers live in shared memory
+// (k_run1d).  The CTA of cluster rank r keeps, for each of the NROLES
+// physical buffers and each component, a row of rw = cspan + 6 elements:
+// the cspan cells of its chunk (cells 1 + r*cspan .. (r+1)*cspan, the tiles
+// r*T .. r*T + T - 1) and three halo cells on each side.  Row element k
+// holds element offset r*cspan + k of the buffer (cell r*cspan + k - 2), so
+// every row element equals the element of the buffer in global memory that
+// the step graphs would hold at that point of the run: a stage stores each
+// cell it updates in its own row and in every neighbour row that holds the
+// cell as a halo, and each ghost image in every row that holds the ghost
+// cell.  The row base of (buffer b, component m) is element (b*MEQN + m)*rw
+// of the dynamic shared memory.
+struct ResView {
+  int rw;             // elements per row
+  int rsh;            // row element of this tile's first window element (tile index in the chunk x (NT-1))
+  int cspan;          // cells per chunk
+  int rank, rlast;    // this CTA's cluster rank; the rank of the last chunk
+  int bin, bqo, bout, bout2;   // physical buffers of the stage input, pointwise input, outputs (-1: none)
+};
+
+// Store the value of cell c (1..mx) of component m in the row `row` (this
+// CTA's row of the output buffer) and in every other CTA's row of that
+// buffer that holds the cell: the neighbours' halos, and, when `edge`, the
+// rows that hold its ghost images (images_1d, negated as put_1d negates).
+template <class S, class A>
+__device__ __forceinline__ void res_put(const ResView& v, S* row, int m, int c, int mx, int bl, int br, bool edge,
+                                        A val) {
+  const int cf = v.rank * v.cspan;   // the chunk's cells are cf+1 .. cf+cspan
+  row[c + 2 - cf] = (S)val;
+  const bool near = c <= cf + 3 || c > cf + v.cspan - 3;
+  if (!near && !edge) return;
+  cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+  // every rank other than `skip` whose row holds `cell` (-2 .. mx+3)
+  auto scatter = [&](int cell, S x, int skip) {
+    int rc = cell < 1 ? 0 : (cell - 1) / v.cspan;
+    rc = rc > v.rlast ? v.rlast : rc;
+    const int rhi = rc + 1 < v.rlast ? rc + 1 : v.rlast;
+    for (int r = rc > 0 ? rc - 1 : 0; r <= rhi; ++r) {
+      const int k = cell + 2 - r * v.cspan;
+      if (r != skip && k >= 0 && k < v.rw) *cl.map_shared_rank(row + k, r) = x;
+    }
+  };
+  if (near) scatter(c, (S)val, v.rank);
+  if (edge) {
+    const Images im = images_1d(c, mx, bl, br);
+    for (int j = 1; j < im.n; ++j) scatter(im.idx[j], (S)((m == 1 && im.neg[j]) ? -val : val), -1);
+  }
+}
 
 // The source-term hooks, src(q,dq,aux,t,dt) of the app (src/1d/step1d.f90:23):
 // dq of cell c (1-based) from the stage input (h, hu) and the step's dt, in
@@ -474,41 +557,87 @@ __device__ __forceinline__ void source_1d(int kind, const Phys& ph, double xlowe
 
 template <class P, int PREC, int NT>
 struct Tile1DSmem {
-  typename Prec<PREC>::S sq[P::MEQN][NT + 8];
+  using S = typename Prec<PREC>::S;
+  static constexpr int AL = 16 / (int)sizeof(S);                  // elements per 16 bytes
+  static constexpr int SQW = (NT + 5 + AL - 1 + AL - 1) / AL * AL;  // staged window incl. alignment slack
+  __align__(16) S sq[P::MEQN][SQW];
   typename Prec<PREC>::R rec[4][P::MEQN][NT];   // 0: qr(c-1)  1: ql(c)  2: amdq(c)  3: apdq(c)
   double sred[NT / 32];
+  float fred[2][NT / 32];
   double dtdx;   // dt/dx, one division per tile
+  uint64_t bar;  // completion of the tile's bulk copies (TMA staging)
+  double tsum[NT / 32][MAXEQ][2];   // per-warp (sum, error) of the tile's outputs (TOT)
 };
 
 // One tile of a 1-D stage: the CTA solves interfaces c = c0 .. c0+NT-1 and
 // updates cells c0 .. c0+NT-2; neighbouring tiles both solve the interface on
 // their common edge (1/NT redundant work).  Ends with a CTA-wide barrier, so
 // a CTA may run tiles back to back.
-template <class P, int CD, int TF, int PREC, int NT>
+//
+// Staging: the cells c0-3 .. c0+NT+1 of every component (offsets c0-1 ..
+// c0+NT+3).  TMA: thread 0 copies the window from the 16-byte boundary at or
+// below offset c0-1 with one bulk copy per plane, completed on sm.bar (phase
+// `parity`; the caller initialised the barrier), and the stencil reads are
+// shifted by sh = (c0-1) - that boundary.  Otherwise the threads load it.
+// A thread whose bounded wait for the copies runs out raises
+// SCL_STATUS_TIMEOUT (the controller then stops the run and discards the
+// step), waits once more, bounded, for copies still in flight, and goes on.
+//
+// TOT: also add the conserved totals of the tile's outputs (sum over its
+// cells of the stored value, times the capacity when mcapa > 0) to the CTA's
+// running (sum, error) pairs tot2[m] with compensated sums (scl_totals.cuh).
+template <class P, int CD, int TF, int PREC, int NT, bool TMA = false, bool TOT = false>
 __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>& L, const Phys& ph,
-                                             int c0, Tile1DSmem<P, PREC, NT>& sm) {
+                                             int c0, Tile1DSmem<P, PREC, NT>& sm, uint32_t parity = 0,
+                                             double (*tot2)[2] = nullptr) {
   using R = typename Prec<PREC>::R;
   using S = typename Prec<PREC>::S;
   using Ac = typename Prec<PREC>::A;
+  using Sm = Tile1DSmem<P, PREC, NT>;
   constexpr int M = P::MEQN, MW = P::MWAVES, MA = P::MAUX;
   const int tid = threadIdx.x;
   const int mx = L.mx;
   const double dt = L.dt;
-  if (tid == 0) sm.dtdx = dt / L.dx;
-
-  // stage cells c0-3 .. c0+NT+1 (global offset c+2)
-  for (int k = tid; k < NT + 5; k += NT) {
-    const long g = (long)c0 - 1 + k;
-    const bool ok = g < (long)mx + 6;
+  int sh = 0;
+  // the window element j (0 .. NT+4) of component m of the stage input
+  auto qwin = [&](int m, int j) -> S { return sm.sq[m][sh + j]; };
+  if constexpr (TMA) {
+    const int a0 = (c0 - 1) / Sm::AL * Sm::AL;   // c0 >= 1
+    sh = c0 - 1 - a0;
+    if (tid == 0) {
+      const int hend = (mx + 6 + Sm::AL - 1) / Sm::AL * Sm::AL;   // <= plane (host-checked)
+      const int hi = a0 + Sm::SQW < hend ? a0 + Sm::SQW : hend;
+      const uint32_t bytes = (uint32_t)(hi - a0) * (uint32_t)sizeof(S);
+      sm.dtdx = dt / L.dx;
+      fence_proxy_async_smem();   // earlier reads of the window come before the copies' writes
+      mbar_arrive_expect_tx(&sm.bar, bytes * M + L.tx_extra);
 #pragma unroll
-    for (int m = 0; m < M; ++m) sm.sq[m][k] = ok ? L.qin[(long)m * L.plane + g] : (S)1;
+      for (int m = 0; m < M; ++m) bulk_g2s(&sm.sq[m][0], L.qin + (long)m * L.plane + a0, bytes, &sm.bar);
+    }
+    if (!mbar_wait_bounded(&sm.bar, parity, L.wait_ns)) {
+      atomicOr(&L.ctl->status, SCL_STATUS_TIMEOUT);
+      mbar_wait_bounded(&sm.bar, parity, L.wait_ns);   // let copies still in flight land
+    }
+  } else {
+    if (tid == 0) sm.dtdx = dt / L.dx;
+    for (int k = tid; k < NT + 5; k += NT) {
+      const long g = (long)c0 - 1 + k;
+      const bool ok = g < (long)mx + 6;
+#pragma unroll
+      for (int m = 0; m < M; ++m) sm.sq[m][k] = ok ? L.qin[(long)m * L.plane + g] : (S)1;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   const double dtdx0 = sm.dtdx;
 
   // ---- interface phase ----
   CflMax<R> cfl;
   int bad = 0;   // a non-finite stage output (reported through ctl->status)
+  [[maybe_unused]] CSum tacc[M];
+  if constexpr (TOT) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) tacc[m] = CSum{0.0, 0.0};
+  }
   {
     const int c = c0 + tid;
     if (c <= mx + 1) {
@@ -518,7 +647,7 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
         auxm[k] = load_aux<S>(L.aux, (long)k * L.plane + c + 1);
         aux0[k] = load_aux<S>(L.aux, (long)k * L.plane + c + 2);
       }
-      auto qs = [&](int k, int m) -> S { return sm.sq[m][tid + k]; };
+      auto qs = [&](int k, int m) -> S { return qwin(m, tid + k); };
       auto as = [&](int k, int j) -> R { return load_aux<S>(L.aux, (long)j * L.plane + c - 1 + k); };
       R xl[M], xr[M], am[M], ap[M], s[MW];
       solve_interface<P, CD, PREC>(ph, L.ixy, qs, as, auxm, aux0, xl, xr, am, ap, s);
@@ -546,7 +675,7 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
       R qc[M], qlc[M], qrc[M], apc[M], amc1[M], br[M];
 #pragma unroll
       for (int m = 0; m < M; ++m) {
-        qc[m] = (R)sm.sq[m][tid + 3];
+        qc[m] = (R)qwin(m, tid + 3);
         qlc[m] = sm.rec[1][m][tid];
         apc[m] = sm.rec[3][m][tid];
         qrc[m] = sm.rec[0][m][tid + 1];
@@ -572,7 +701,7 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
       const bool has_src = L.src != SCL_SRC_NONE;
       if constexpr (M == 2) {
         if (has_src)
-          source_1d<Ac, S>(L.src, ph, L.xlower, L.dx, dt, c, (Ac)sm.sq[0][tid + 3], (Ac)sm.sq[1][tid + 3],
+          source_1d<Ac, S>(L.src, ph, L.xlower, L.dx, dt, c, (Ac)qwin(0, tid + 3), (Ac)qwin(1, tid + 3),
                            L.aux, srcv);
       }
       auto dq_of = [&](int m) -> Ac {
@@ -593,11 +722,18 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
 #pragma unroll
         for (int m = 0; m < M; ++m) {
           Ac dqv = dq_of(m);
-          Ac qv = (Ac)sm.sq[m][tid + 3];
+          Ac qv = (Ac)qwin(m, tid + 3);
           Ac qov = L.qo ? (Ac)L.qo[(long)m * L.plane + c + 2] : (Ac)0;
           Ac o1, o2 = (Ac)0;
           combine<Ac, PREC == SCL_FP64_STRICT>(kind, qv, qov, dqv, o1, o2);
           bad |= !isfinite(o1);
+          if constexpr (TOT) {
+            const double v = (double)(S)o1;
+            if (L.mcapa > 0)
+              tacc[m].add(v * (double)static_cast<const S*>(L.aux)[(long)(L.mcapa - 1) * L.plane + c + 2]);
+            else
+              tacc[m].add(v);
+          }
           if (edge) put_1d<S, Ac>(L.out, L.plane, m, c, images_1d(c, mx, L.bl, L.br), o1);
           else L.out[(long)m * L.plane + c + 2] = (S)o1;
           if (L.out2) L.out2[(long)m * L.plane + c + 2] = (S)o2;
@@ -607,15 +743,228 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
   }
 
   // ---- CFL reduction: warp max, block max, one atomic per tile ----
-  double cflmax = warp_max(cfl.value(dtdx0, dtdx0));
-  if ((tid & 31) == 0) sm.sred[tid >> 5] = cflmax;
-  const int anybad = __syncthreads_or(bad);
+  if constexpr (TOT) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double os = __shfl_down_sync(0xffffffffu, tacc[m].s, o);
+        const double oc = __shfl_down_sync(0xffffffffu, tacc[m].c, o);
+        tacc[m].add(os, oc);
+      }
+      if ((tid & 31) == 0) { sm.tsum[tid >> 5][m][0] = tacc[m].s; sm.tsum[tid >> 5][m][1] = tacc[m].c; }
+    }
+  }
+  int anybad = 0;
+  const double v = cfl_cta_max<R, NT, false>(cfl, dtdx0, dtdx0, L.mcapa > 0, sm.sred, sm.fred, bad, &anybad);
   if (tid < 32) {
-    double v = (tid < NT / 32) ? sm.sred[tid] : 0.0;
-    v = warp_max(v);
     if (tid == 0) {
-      atomic_max_nonneg(&L.ctl->stage_cfl[L.stage], (double)v);
+      atomic_max_nonneg(&L.ctl->stage_cfl[L.stage], v);
       if (anybad) atomicOr(&L.ctl->status, SCL_STATUS_NONFINITE);
+      if constexpr (TOT) {
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          CSum t{tot2[m][0], tot2[m][1]};
+          for (int w = 0; w < NT / 32; ++w) t.add(sm.tsum[w][m][0], sm.tsum[w][m][1]);
+          tot2[m][0] = t.s;
+          tot2[m][1] = t.c;
+        }
+      }
+    }
+  }
+}
+
+// A value the compiler must treat as opaque: no multiply-add contraction
+// across it.  The step graphs pass the interface results through shared
+// memory between the interface and the cell phase, which keeps the cell
+// phase's additions from fusing with the interface phase's products; a
+// resident tile that keeps them in registers passes them through this.
+__device__ __forceinline__ float opaque(float x) {
+  asm volatile("" : "+f"(x));
+  return x;
+}
+__device__ __forceinline__ double opaque(double x) {
+  asm volatile("" : "+d"(x));
+  return x;
+}
+
+// The interface results one thread of a resident tile needs for its cell c:
+// ql(c), apdq(c) from interface c and qr(c), amdq(c+1) from interface c+1.
+template <class R, int M>
+struct ResIface {
+  R qlc[M], apc[M], qrc[M], amc1[M];
+};
+
+// Both interfaces of cell c = c0 + tid from the rows of buffer `bin`
+// (window element rsh + tid + j + k is cell c - 3 + j + k), with their CFL
+// contributions added to cfl when CFL.
+template <class P, int CD, int PREC>
+__device__ __forceinline__ void res_ifaces(const Line<typename Prec<PREC>::S>& L, const Phys& ph, int c,
+                                           const ResView& rv, int bin, bool CFL,
+                                           CflMax<typename Prec<PREC>::R>& cfl,
+                                           ResIface<typename Prec<PREC>::R, P::MEQN>& f) {
+  using R = typename Prec<PREC>::R;
+  using S = typename Prec<PREC>::S;
+  constexpr int M = P::MEQN, MW = P::MWAVES, MA = P::MAUX;
+  const int tid = threadIdx.x;
+  const double dt = L.dt;
+  const double dtdx0 = L.dtdx;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const S* qin = reinterpret_cast<const S*>(smem_raw) + (long)bin * M * rv.rw;
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int ci = c + j;   // interface ci-1/2
+    R auxm[MA > 0 ? MA : 1], aux0[MA > 0 ? MA : 1];
+#pragma unroll
+    for (int k = 0; k < MA; ++k) {
+      auxm[k] = load_aux<S>(L.aux, (long)k * L.plane + ci + 1);
+      aux0[k] = load_aux<S>(L.aux, (long)k * L.plane + ci + 2);
+    }
+    auto qs = [&](int k, int m) -> S { return qin[(long)m * rv.rw + rv.rsh + tid + j + k]; };
+    auto as = [&](int k, int jj) -> R { return load_aux<S>(L.aux, (long)jj * L.plane + ci - 1 + k); };
+    R xl[M], xr[M], am[M], ap[M], s[MW];
+    solve_interface<P, CD, PREC>(ph, L.ixy, qs, as, auxm, aux0, xl, xr, am, ap, s);
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      if (j == 0) { f.qlc[m] = opaque(xr[m]); f.apc[m] = opaque(ap[m]); }
+      else { f.qrc[m] = opaque(xl[m]); f.amc1[m] = opaque(am[m]); }
+    }
+    if (CFL) {
+      // flux1.f90:126-133: max(dtdx(i)*s, -dtdx(i-1)*s)
+      double dtdx_c = dtdx0, dtdx_m = dtdx0;
+      if (L.mcapa > 0) {
+        const S* cap = static_cast<const S*>(L.aux) + (long)(L.mcapa - 1) * L.plane;
+        dtdx_c = dt / (L.dx * (double)cap[ci + 2]);
+        dtdx_m = dt / (L.dx * (double)cap[ci + 1]);
+      }
+      cfl.template add<MW>(s, dtdx_c, dtdx_m, L.mcapa > 0, true);
+    }
+  }
+}
+
+// One tile of a stage of a shared-memory resident run (k_run1d): the cells
+// c0 .. c0+NT-2 (<= mx) of the rows of `rv`.  Thread tid owns cell
+// c = c0 + tid and solves both of its interfaces, c and c+1 (the next thread
+// solves c+1 again as its left interface), so the tile needs no record in
+// shared memory and no barrier: its input rows are complete once the cluster
+// barrier that ended the previous stage has passed, and its outputs go to
+// the rows (res_put: halos and ghost images included).  Every interface,
+// cell bracket, source term and combination is the code and the operands of
+// stage1d_tile, so the outputs are those of the step graphs bit for bit.
+// pre: the thread's interface results already solved from the stage input
+// (res_ifaces), or nullptr.
+//
+// CFL: the stage's CFL number and non-finite flag are reduced over each
+// warp and combined into part->stage_cfl[stage] / part->status by one atomic
+// per warp (the maximum is exact: dt/dx times a float and the conversions
+// are monotonic).  A resident run asks for them in the last stage only (CFL;
+// never with pre): the controller judges a step by its last stage, and a
+// non-finite output of an earlier stage reaches the last stage's output in
+// the same cell through the pointwise combinations.
+// TOT: the tile's conserved totals as (sum, error) pairs per warp, in
+// tsum[warp][m] (this CTA's shared memory; combined after the stage).
+template <class P, int CD, int TF, int PREC, int NT, bool TOT>
+__device__ __forceinline__ void stage1d_res(const Line<typename Prec<PREC>::S>& L, const Phys& ph, int c0,
+                                            const ResView& rv, bool CFL, Ctl* part, double (*tsum)[MAXEQ][2],
+                                            const ResIface<typename Prec<PREC>::R, P::MEQN>* pre = nullptr) {
+  using R = typename Prec<PREC>::R;
+  using S = typename Prec<PREC>::S;
+  using Ac = typename Prec<PREC>::A;
+  constexpr int M = P::MEQN, MA = P::MAUX;
+  const int tid = threadIdx.x;
+  const int mx = L.mx;
+  const double dt = L.dt;
+  const double dtdx0 = L.dtdx;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto rrow = [&](int b, int m) -> S* { return reinterpret_cast<S*>(smem_raw) + ((long)b * M + m) * rv.rw; };
+  const S* qin = rrow(rv.bin, 0);
+  // window element j (0 .. NT+4) of component m of the stage input
+  auto qwin = [&](int m, int j) -> S { return qin[(long)m * rv.rw + rv.rsh + j]; };
+  const int c = c0 + tid;
+  const bool own = tid < NT - 1 && c <= mx;
+  CflMax<R> cfl;
+  int bad = 0;
+  [[maybe_unused]] CSum tacc[M];
+  if constexpr (TOT) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) tacc[m] = CSum{0.0, 0.0};
+  }
+  if (own) {
+    ResIface<R, M> f;
+    if (pre) f = *pre;
+    else res_ifaces<P, CD, PREC>(L, ph, c, rv, rv.bin, CFL, cfl, f);
+    // ---- the cell ----
+    R qc[M], br[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) qc[m] = (R)qwin(m, tid + 3);
+    constexpr int NB = tfluct_nb<P>::value ? 3 : 1;
+    R auxc[NB * (MA > 0 ? MA : 1)];
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+#pragma unroll
+      for (int k = 0; k < MA; ++k)
+        auxc[j * MA + k] = load_aux<S>(L.aux, (long)k * L.plane + c + 2 + j - (NB - 1) / 2);
+    cell_bracket<P, TF, PREC>(ph, L.ixy, qc, auxc, f.qlc, f.qrc, f.apc, f.amc1, br);
+    double dtdx_c = dtdx0;
+    if (L.mcapa > 0) {
+      const S* cap = static_cast<const S*>(L.aux) + (long)(L.mcapa - 1) * L.plane;
+      dtdx_c = dt / (L.dx * (double)cap[c + 2]);
+    }
+    Ac srcv[M];
+    const bool has_src = L.src != SCL_SRC_NONE;
+    if constexpr (M == 2) {
+      if (has_src)
+        source_1d<Ac, S>(L.src, ph, L.xlower, L.dx, dt, c, (Ac)qwin(0, tid + 3), (Ac)qwin(1, tid + 3), L.aux, srcv);
+    }
+    auto dq_of = [&](int m) -> Ac {
+      if constexpr (M == 2) {
+        if (has_src) {
+          if constexpr (std::is_same_v<R, Ac>) return srcv[m] - (R)dtdx_c * br[m];
+          else return srcv[m] + (Ac)((R)0 - (R)dtdx_c * br[m]);
+        }
+      }
+      return (Ac)((R)0 - (R)dtdx_c * br[m]);
+    };
+    const bool edge = c <= 3 || c >= mx - 2;   // only these cells have ghost images
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      Ac dqv = dq_of(m);
+      Ac qv = (Ac)qwin(m, tid + 3);
+      Ac qov = rv.bqo >= 0 ? (Ac)rrow(rv.bqo, m)[rv.rsh + tid + 3] : (Ac)0;
+      Ac o1, o2 = (Ac)0;
+      combine<Ac, PREC == SCL_FP64_STRICT>(L.kind, qv, qov, dqv, o1, o2);
+      bad |= !isfinite(o1);
+      if constexpr (TOT) {
+        const double v = (double)(S)o1;
+        if (L.mcapa > 0)
+          tacc[m].add(v * (double)static_cast<const S*>(L.aux)[(long)(L.mcapa - 1) * L.plane + c + 2]);
+        else
+          tacc[m].add(v);
+      }
+      res_put<S, Ac>(rv, rrow(rv.bout, m), m, c, mx, L.bl, L.br, edge, o1);
+      if (rv.bout2 >= 0) res_put<S, Ac>(rv, rrow(rv.bout2, m), m, c, mx, 0, 0, false, o2);
+    }
+  }
+  const int lane = tid & 31;
+  if constexpr (TOT) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const CSum t = warp_csum(tacc[m]);
+      if (lane == 0) { tsum[tid >> 5][m][0] = t.s; tsum[tid >> 5][m][1] = t.c; }
+    }
+  }
+  if (CFL) {
+    double v;
+    if constexpr (std::is_same_v<R, double>) {
+      v = warp_max(cfl.v);
+    } else {
+      const float w = warp_max(cfl.sx);
+      v = L.mcapa > 0 ? nanmax((double)w, 0.0) : nanmax(dtdx0 * (double)w, dtdx0 * 0.0);
+    }
+    const int anybad = __any_sync(0xffffffffu, bad);
+    if (lane == 0) {
+      atomic_max_nonneg(&part->stage_cfl[L.stage], v);
+      if (anybad) atomicOr(&part->status, SCL_STATUS_NONFINITE);
     }
   }
 }
@@ -631,10 +980,10 @@ __device__ __forceinline__ Line<S> line1d(const StageArgs& a, const StageDesc& s
   Ctl* ctl = ctl_override ? ctl_override : a.ctl;
   Line<S> L;
   L.ctl = ctl;
-  L.qin = static_cast<const S*>(a.buf[ctl->role[sd.in]]);
-  L.qo = sd.aux_in >= 0 ? static_cast<const S*>(a.buf[ctl->role[sd.aux_in]]) : nullptr;
-  L.out = sd.kind == SK_DQ ? nullptr : static_cast<S*>(a.buf[ctl->role[sd.out]]);
-  L.out2 = sd.out2 >= 0 ? static_cast<S*>(a.buf[ctl->role[sd.out2]]) : nullptr;
+  L.qin = static_cast<const S*>(pick_buf(a.buf, ctl->role[sd.in]));
+  L.qo = sd.aux_in >= 0 ? static_cast<const S*>(pick_buf(a.buf, ctl->role[sd.aux_in])) : nullptr;
+  L.out = sd.kind == SK_DQ ? nullptr : static_cast<S*>(pick_buf(a.buf, ctl->role[sd.out]));
+  L.out2 = sd.out2 >= 0 ? static_cast<S*>(pick_buf(a.buf, ctl->role[sd.out2])) : nullptr;
   L.dq_out = a.dq_out;
   L.aux = a.aux;
   L.mx = a.mx;
@@ -649,15 +998,27 @@ __device__ __forceinline__ Line<S> line1d(const StageArgs& a, const StageDesc& s
   L.src = a.src_term;
   L.xlower = a.xlower;
   L.dt = ctl->dt;
+  L.wait_ns = a.wait_ns ? a.wait_ns : MBAR_LIMIT_NS;   // 0: the default bound
+  L.tx_extra = a.tx_extra;
   return L;
 }
 
-template <class P, int CD, int TF, int PREC, int NT>
-__global__ void __launch_bounds__(NT) k_stage1d(StageArgs a) {
+// TMA: the tile is staged by bulk copies (the launcher checked that every
+// role buffer starts on 16 bytes and the component stride keeps the planes
+// there).  MINB: CTAs per SM the registers are budgeted for (0: no bound).
+template <class P, int CD, int TF, int PREC, int NT, bool TMA = false, int MINB = 0>
+__global__ void __launch_bounds__(NT, MINB) k_stage1d(StageArgs a) {
   using S = typename Prec<PREC>::S;
   __shared__ Tile1DSmem<P, PREC, NT> sm;
   if (a.ctl->done) return;
-  stage1d_tile<P, CD, TF, PREC, NT>(line1d<S>(a, a.sd, a.stage), a.ph, 1 + blockIdx.x * (NT - 1), sm);
+  if constexpr (TMA) {
+    if (threadIdx.x == 0) {
+      mbar_init(&sm.bar, 1);
+      fence_mbar_init();
+    }
+    __syncthreads();   // the barrier is initialised before any thread waits on it
+  }
+  stage1d_tile<P, CD, TF, PREC, NT, TMA>(line1d<S>(a, a.sd, a.stage), a.ph, 1 + blockIdx.x * (NT - 1), sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -673,39 +1034,47 @@ struct Tile2D {
   static constexpr int NXI = (TX + 1) * TY, NYI = TX * (TY + 1);
 };
 
-template <class P, int CD, int TF, int PREC, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
+// The block is staged by the threads (coalesced loads of every row):
+// measured faster than one bulk copy per staged row, which issues dozens of
+// small (176-byte) copies per CTA.  MINB: CTAs per SM the registers are
+// budgeted for (0: no bound).
+template <class P, int CD, int TF, int PREC, int TX, int TY, int NT, int MINB = 0>
+__global__ void __launch_bounds__(NT, MINB) k_stage2d(StageArgs a) {
   using R = typename Prec<PREC>::R;
   using S = typename Prec<PREC>::S;
   using Ac = typename Prec<PREC>::A;
   using T = Tile2D<TX, TY>;
   constexpr int M = P::MEQN, MW = P::MWAVES, MA = P::MAUX;
+  constexpr int WXS = T::WX;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S* sq = reinterpret_cast<S*>(smem_raw);                                  // [M][WY][WX]
-  R* recx = reinterpret_cast<R*>(sq + M * T::WX * T::WY);                  // [4][M][NXI]
+  R* recx = reinterpret_cast<R*>(sq + M * WXS * T::WY);                    // [4][M][NXI]
   R* recy = recx + 4 * M * T::NXI;                                         // [4][M][NYI]
   __shared__ double sred[NT / 32];
+  __shared__ float fred[2][NT / 32];
 
   const Ctl* ctl = a.ctl;
   if (ctl->done) return;
   const int tid = threadIdx.x;
   const int nx = a.mx, ny = a.my;
   const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
-  const S* qin = static_cast<const S*>(a.buf[ctl->role[a.sd.in]]);
+  const S* qin = static_cast<const S*>(pick_buf(a.buf, ctl->role[a.sd.in]));
   const double dt = ctl->dt;
   __shared__ double s_dtd[2];   // dt/dx, dt/dy: two divisions per CTA
   if (tid == 0) { s_dtd[0] = dt / a.dx; s_dtd[1] = dt / a.dy; }
 
   // stage the block: cells (i0-3 .. i0+TX+2, j0-3 .. j0+TY+2)
-  for (int k = tid; k < T::WX * T::WY; k += NT) {
-    const int kx = k % T::WX, ky = k / T::WX;
-    const int gi = i0 - 3 + kx, gj = j0 - 3 + ky;  // 1-based cell indices
-    const bool ok = gi <= nx + 3 && gj <= ny + 3;
-    const long off = (long)(gj + 2) * a.pitch + (gi + 2);
+  {
+    for (int k = tid; k < T::WX * T::WY; k += NT) {
+      const int kx = k % T::WX, ky = k / T::WX;
+      const int gi = i0 - 3 + kx, gj = j0 - 3 + ky;  // 1-based cell indices
+      const bool ok = gi <= nx + 3 && gj <= ny + 3;
+      const long off = (long)(gj + 2) * a.pitch + (gi + 2);
 #pragma unroll
-    for (int m = 0; m < M; ++m) sq[(m * T::WY + ky) * T::WX + kx] = ok ? qin[(long)m * a.plane + off] : (S)1;
+      for (int m = 0; m < M; ++m) sq[(m * T::WY + ky) * WXS + kx] = ok ? qin[(long)m * a.plane + off] : (S)1;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   const double dtdx0 = s_dtd[0], dtdy0 = s_dtd[1];
 
   CflMax<R> cfl;
@@ -734,8 +1103,8 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
     // local smem coordinates of cell (gi, gj): (li+3, lj+3)
     const int bx = li + 3, by = lj + 3;
     auto qs = [&](int k, int m) -> S {
-      return isx ? sq[(m * T::WY + by) * T::WX + (bx - 3 + k)]
-                 : sq[(m * T::WY + (by - 3 + k)) * T::WX + bx];
+      return isx ? sq[(m * T::WY + by) * WXS + (bx - 3 + k)]
+                 : sq[(m * T::WY + (by - 3 + k)) * WXS + bx];
     };
     const long st = isx ? 1 : a.pitch;
     auto as = [&](int k, int j) -> R { return load_aux<S>(a.aux, (long)j * a.plane + o0 + (long)(k - 3) * st); };
@@ -775,7 +1144,7 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
     for (int k = 0; k < MA; ++k) auxc[k] = load_aux<S>(a.aux, (long)k * a.plane + o0);
     R qc[M];
 #pragma unroll
-    for (int m = 0; m < M; ++m) qc[m] = (R)sq[(m * T::WY + lj + 3) * T::WX + li + 3];
+    for (int m = 0; m < M; ++m) qc[m] = (R)sq[(m * T::WY + lj + 3) * WXS + li + 3];
     double dx_c = dtdx0, dy_c = dtdy0;
     if (a.mcapa > 0) {
       const S* cap = static_cast<const S*>(a.aux) + (long)(a.mcapa - 1) * a.plane;
@@ -817,13 +1186,13 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
 #pragma unroll
       for (int m = 0; m < M; ++m) a.dq_out[(long)m * a.plane + o0] = (double)dqs[m];
     } else {
-      S* out = static_cast<S*>(a.buf[ctl->role[a.sd.out]]);
-      S* out2 = a.sd.out2 >= 0 ? static_cast<S*>(a.buf[ctl->role[a.sd.out2]]) : nullptr;
-      const S* qo = a.sd.aux_in >= 0 ? static_cast<const S*>(a.buf[ctl->role[a.sd.aux_in]]) : nullptr;
+      S* out = static_cast<S*>(pick_buf(a.buf, ctl->role[a.sd.out]));
+      S* out2 = a.sd.out2 >= 0 ? static_cast<S*>(pick_buf(a.buf, ctl->role[a.sd.out2])) : nullptr;
+      const S* qo = a.sd.aux_in >= 0 ? static_cast<const S*>(pick_buf(a.buf, ctl->role[a.sd.aux_in])) : nullptr;
       const bool edge = gi <= 3 || gi >= nx - 2 || gj <= 3 || gj >= ny - 2;
 #pragma unroll
       for (int m = 0; m < M; ++m) {
-        Ac qv = (Ac)sq[(m * T::WY + lj + 3) * T::WX + li + 3];
+        Ac qv = (Ac)sq[(m * T::WY + lj + 3) * WXS + li + 3];
         Ac qov = qo ? (Ac)qo[(long)m * a.plane + o0] : (Ac)0;
         Ac o1, o2 = (Ac)0;
         combine<Ac, PREC == SCL_FP64_STRICT>(kind, qv, qov, (Ac)dqs[m], o1, o2);
@@ -838,14 +1207,11 @@ __global__ void __launch_bounds__(NT) k_stage2d(StageArgs a) {
     }
   }
 
-  const double cflmax = warp_max(cfl.value(dtdx0, dtdy0));
-  if ((tid & 31) == 0) sred[tid >> 5] = cflmax;
-  const int anybad = __syncthreads_or(bad);
+  int anybad = 0;
+  const double v = cfl_cta_max<R, NT>(cfl, dtdx0, dtdy0, a.mcapa > 0, sred, fred, bad, &anybad);
   if (tid < 32) {
-    double v = (tid < NT / 32) ? sred[tid] : 0.0;
-    v = warp_max(v);
     if (tid == 0) {
-      atomic_max_nonneg(&a.ctl->stage_cfl[a.stage], (double)v);
+      atomic_max_nonneg(&a.ctl->stage_cfl[a.stage], v);
       if (anybad) atomicOr(&a.ctl->status, SCL_STATUS_NONFINITE);
     }
   }
@@ -860,12 +1226,13 @@ __global__ void __launch_bounds__(128) k_ghost_cfl2d(StageArgs a) {
   using S = typename Prec<PREC>::S;
   constexpr int M = P::MEQN, MW = P::MWAVES, MA = P::MAUX;
   __shared__ double sred[4];
+  __shared__ float fred[2][4];
   const Ctl* ctl = a.ctl;
   if (ctl->done) return;
   const int nx = a.mx, ny = a.my;
   const int nxl = nx + 1, nyl = ny + 1;
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
-  const S* qin = static_cast<const S*>(a.buf[ctl->role[a.sd.in]]);
+  const S* qin = static_cast<const S*>(pick_buf(a.buf, ctl->role[a.sd.in]));
   const double dt = ctl->dt;
   CflMax<R> cfl;
   if (w < 2 * nxl + 2 * nyl) {
@@ -894,14 +1261,9 @@ __global__ void __launch_bounds__(128) k_ghost_cfl2d(StageArgs a) {
     }
     cfl.template add<MW>(s, d_c, d_m, a.mcapa > 0, ixy == 1);
   }
-  const double cflmax = warp_max(cfl.value(dt / a.dx, dt / a.dy));
-  if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = cflmax;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    double v = (threadIdx.x < 4) ? sred[threadIdx.x] : 0.0;
-    v = warp_max(v);
-    if (threadIdx.x == 0) atomic_max_nonneg(&a.ctl->stage_cfl[a.stage], (double)v);
-  }
+  int anybad = 0;
+  const double v = cfl_cta_max<R, 128>(cfl, dt / a.dx, dt / a.dy, a.mcapa > 0, sred, fred, 0, &anybad);
+  if (threadIdx.x == 0) atomic_max_nonneg(&a.ctl->stage_cfl[a.stage], v);
 }
 
 }  // namespace scl

@@ -18,6 +18,7 @@ constexpr int RES_NT = 128;
 constexpr int RES_CLUSTER = 8;
 constexpr int RES_AUTO_TILES = 8;   // one tile per CTA: beyond it the graphs are faster
 constexpr int RES_MAX_TILES = 64;
+constexpr int RES_TILES_PER_CTA = RES_MAX_TILES / RES_CLUSTER;   // tiles one CTA holds at most
 constexpr int RES_ITERS = 4096;
 
 // One getter per arithmetic form; `variant` selects a tile shape (2-D).

@@ -276,6 +276,7 @@ extern "C" int scl_rk_step_noalloc(const scl_params* p, double* q_dev, const dou
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail_na(SCL_E_CUDA, std::string("cfl readback: ") + cudaGetErrorString(e));
     *cfl = h.stage_cfl[ns - 1];
+    if (h.status & SCL_STATUS_TIMEOUT) return fail_na(SCL_E_TIMEOUT, "a bounded wait for staged data ran out");
     if ((h.status & SCL_STATUS_NONFINITE) || *cfl != *cfl)
       return fail_na(SCL_E_NONFINITE, "non-finite stage output");
   }

@@ -331,7 +331,7 @@ __device__ __forceinline__ void pair_issue(const Line<typename Prec<PREC>::S>& L
     }
   const uint32_t bytes = (uint32_t)(hi - lo) * (uint32_t)sizeof(S);
   fence_proxy_async_smem();   // earlier accesses of these buffers come before the copies' writes
-  mbar_arrive_expect_tx(bar, bytes * (wo ? 6u : 3u));
+  mbar_arrive_expect_tx(bar, bytes * (wo ? 6u : 3u) + L.tx_extra);
 #pragma unroll
   for (int m = 0; m < 3; ++m) bulk_g2s(&wq.v[m][lo - a0], L.qin + (long)m * L.plane + lo, bytes, bar);
   if (wo)
@@ -339,17 +339,16 @@ __device__ __forceinline__ void pair_issue(const Line<typename Prec<PREC>::S>& L
     for (int m = 0; m < 3; ++m) bulk_g2s(&wo->v[m][lo - a0], L.qo + (long)m * L.plane + lo, bytes, bar);
 }
 
-// Every thread waits for phase `parity` of bar; false on every thread when
-// the bounded wait ran out (SCL_STATUS_TIMEOUT is raised and the copies
-// still in flight are given a second bounded wait to land).
-__device__ __forceinline__ bool pair_wait(Ctl* ctl, uint64_t* bar, uint32_t parity) {
-  const bool ok = mbar_wait_bounded(bar, parity);
-  if (__syncthreads_or(!ok)) {
-    if (threadIdx.x == 0) atomicOr(&ctl->status, SCL_STATUS_TIMEOUT);
-    mbar_wait_bounded(bar, parity);
-    return false;
+// Every thread waits for phase `parity` of bar (an acquire: the copies' data
+// and what thread 0 wrote before its arrival are visible after it, so no CTA
+// barrier follows).  A thread whose bounded wait runs out raises
+// SCL_STATUS_TIMEOUT (the controller then stops the run and discards the
+// step), waits once more, bounded, for copies still in flight, and goes on.
+__device__ __forceinline__ void pair_wait(Ctl* ctl, uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+  if (!mbar_wait_bounded(bar, parity, limit_ns)) {
+    atomicOr(&ctl->status, SCL_STATUS_TIMEOUT);
+    mbar_wait_bounded(bar, parity, limit_ns);
   }
-  return true;
 }
 
 // The threads stage the window themselves (planes not on 16 bytes).
@@ -518,8 +517,9 @@ __device__ __forceinline__ void pair_compute(const Line<typename Prec<PREC>::S>&
 }
 
 // CTA maximum of smax, times dtdx in FP64, into the stage's CFL slot; the
-// non-finite flag into the status word.  Ends with a CTA-wide barrier.
-template <int NT>
+// non-finite flag into the status word.  REUSE: end with a CTA-wide barrier
+// (a persistent CTA reuses sred and the staged windows for its next tile).
+template <int NT, bool REUSE>
 __device__ __forceinline__ void pair_reduce(Ctl* ctl, int stage, float* sred, double dtdx, float smax, int bad) {
   const int tid = threadIdx.x;
   smax = warp_max(smax);
@@ -533,17 +533,17 @@ __device__ __forceinline__ void pair_reduce(Ctl* ctl, int stage, float* sred, do
       if (anybad) atomicOr(&ctl->status, SCL_STATUS_NONFINITE);
     }
   }
-  __syncthreads();   // sred and the staged windows are reused by the next tile
+  if constexpr (REUSE) __syncthreads();
 }
 
 template <class S>
 __device__ __forceinline__ Line<S> line_of(const StageArgs& a, Ctl* ctl) {
   Line<S> L;
   L.ctl = ctl;
-  L.qin = static_cast<const S*>(a.buf[ctl->role[a.sd.in]]);
-  L.qo = a.sd.aux_in >= 0 ? static_cast<const S*>(a.buf[ctl->role[a.sd.aux_in]]) : nullptr;
-  L.out = a.sd.kind == SK_DQ ? nullptr : static_cast<S*>(a.buf[ctl->role[a.sd.out]]);
-  L.out2 = a.sd.out2 >= 0 ? static_cast<S*>(a.buf[ctl->role[a.sd.out2]]) : nullptr;
+  L.qin = static_cast<const S*>(pick_buf(a.buf, ctl->role[a.sd.in]));
+  L.qo = a.sd.aux_in >= 0 ? static_cast<const S*>(pick_buf(a.buf, ctl->role[a.sd.aux_in])) : nullptr;
+  L.out = a.sd.kind == SK_DQ ? nullptr : static_cast<S*>(pick_buf(a.buf, ctl->role[a.sd.out]));
+  L.out2 = a.sd.out2 >= 0 ? static_cast<S*>(pick_buf(a.buf, ctl->role[a.sd.out2])) : nullptr;
   L.dq_out = a.dq_out;
   L.aux = a.aux;
   L.mx = a.mx;
@@ -556,6 +556,8 @@ __device__ __forceinline__ Line<S> line_of(const StageArgs& a, Ctl* ctl) {
   L.stage = a.stage;
   L.ixy = a.ixy;
   L.dt = ctl->dt;
+  L.wait_ns = a.wait_ns ? a.wait_ns : MBAR_LIMIT_NS;   // 0: the default bound
+  L.tx_extra = a.tx_extra;
   return L;
 }
 
@@ -579,7 +581,7 @@ __global__ void __launch_bounds__(NT, MINB) k_stage1d_pair(StageArgs a) {
       pair_issue<PREC, NT>(L, c0, sm.sq, wo, &sm.bar);
     }
     __syncthreads();   // the barrier is initialised before any thread waits on it
-    if (!pair_wait(ctl, &sm.bar, 0)) return;
+    pair_wait(ctl, &sm.bar, 0, L.wait_ns);
   } else {
     if (threadIdx.x == 0) sm.dtdx = L.dt / L.dx;
     pair_load<PREC, NT>(L, c0, sm.sq, wo);
@@ -588,7 +590,7 @@ __global__ void __launch_bounds__(NT, MINB) k_stage1d_pair(StageArgs a) {
   float smax = 0.0f;
   int bad = 0;
   pair_compute<CD, PREC, NT, TMA>(L, a.ph, c0, sm.sq, wo, sm.rec, sm.dtdx, smax, bad);
-  pair_reduce<NT>(ctl, a.stage, sm.sred, sm.dtdx, smax, bad);
+  pair_reduce<NT, false>(ctl, a.stage, sm.sred, sm.dtdx, smax, bad);
 }
 
 // Batched form: the persistent walk over the active instances' tiles of
@@ -642,11 +644,11 @@ __global__ void __launch_bounds__(NT, SCL_PAIR_MINB) k_batch_stage_pair(BatchArg
       sm.dtdx = L.dt / L.dx;
       pair_issue<PREC, NT>(L, c0, sm.sq, wo, &sm.bar);
     }
-    if (!pair_wait(ctl, &sm.bar, parity)) return;
+    pair_wait(ctl, &sm.bar, parity, MBAR_LIMIT_NS);
     float smax = 0.0f;
     int bad = 0;
     pair_compute<CD, PREC, NT, true>(L, a.ph, c0, sm.sq, wo, sm.rec, sm.dtdx, smax, bad);
-    pair_reduce<NT>(ctl, a.stage, sm.sred, sm.dtdx, smax, bad);
+    pair_reduce<NT, true>(ctl, a.stage, sm.sred, sm.dtdx, smax, bad);
   }
 }
 

@@ -4,22 +4,29 @@
 // stage kernel and controller kernel costs microseconds of launch latency
 // while its arithmetic takes less.  Here one thread-block cluster (at most
 // RES_CLUSTER CTAs, co-scheduled by the cluster launch) stays resident for up
-// to max_iters controller iterations of src/sharpclaw.f90:118-221:
-//   * CTA r computes tiles r, r + nc, ... of every stage with the tile code of
-//     the stage kernels (stage1d_tile), so the arithmetic, and therefore every
-//     result, is the step graphs';
-//   * a cluster barrier (arrive.release / wait.acquire at cluster scope)
-//     separates the stages, which orders each stage's global-memory output,
-//     ghost images included, before the next stage reads its halo;
-//   * the controller lives in CTA 0's shared memory for the whole launch
-//     (copied from and back to global memory at its ends): thread 0 of CTA 0
-//     runs it (ctl_end of the previous step, ctl_begin of the next) between
-//     steps, and every CTA reads its roles, dt and done flag through
-//     distributed shared memory, so no controller access waits on L2;
-//   * each CTA accumulates its stage CFL numbers and status in its own shared
-//     memory (the tile code's atomics stay CTA-local); the controller thread
-//     combines the CTAs' values of the last stage (maximum of the bit
-//     patterns, as the global atomic max does, and OR) before ctl_end.
+// to max_iters controller iterations of src/sharpclaw.f90:118-221, and the
+// run's registers stay in shared memory:
+//   * CTA r owns the chunk of T consecutive tiles r*T .. r*T+T-1 and keeps,
+//     for every physical buffer, the chunk's cells plus three halo cells on
+//     each side in shared memory (ResView, scl_kernels.cuh), loaded from
+//     global memory when the launch starts and written back when it ends;
+//   * each stage runs stage1d_res on those rows: the interface, cell and
+//     combination code of the stage kernels' tiles, so the arithmetic, and
+//     therefore every result, is the step graphs'; a thread solves both
+//     interfaces of its cell, so a tile has no barrier; a stage stores the
+//     cells next to a chunk edge, and the ghost images, straight into the
+//     neighbouring CTAs' rows through distributed shared memory;
+//   * one cluster barrier (arrive.release / wait.acquire) per stage orders
+//     those stores before the next stage reads its window, and is the only
+//     wait between CTAs;
+//   * every CTA keeps its own copy of the controller in shared memory and
+//     runs it (ctl_end of the previous step, ctl_begin of the next) on the
+//     same inputs: the CTAs' last-stage CFL maxima and status (and, with
+//     conserved totals on, their compensated (sum, error) pairs in rank
+//     order), read from every CTA through distributed shared memory.  These
+//     per-CTA values are double-buffered by step parity, so no barrier
+//     beyond the stages' is needed between the reads and the next step's
+//     writes.  CTA 0's copy goes back to global memory at the end.
 // The loop ends after max_iters iterations at most; the host relaunches while
 // the controller is not done.
 #pragma once
@@ -27,70 +34,222 @@
 
 #include "scl_ctl.cuh"
 #include "scl_kernels.cuh"
+#include "scl_launch.h"
 
 namespace scl {
 
+// Dynamic shared memory of a resident run with T tiles per CTA: the rows
+// of every physical buffer.
+template <class S>
+inline size_t run1d_rows_bytes(int meqn, int T, int nt) {
+  return sizeof(S) * (size_t)NROLES * (size_t)meqn * (size_t)(T * (nt - 1) + 6);
+}
+
+// Threads of a resident CTA: NT tile threads (warps 0 .. NT/32-1) and one
+// controller warp.
+template <int NT>
+constexpr int run1d_threads() { return NT + 32; }
+
 template <class P, int CD, int TF, int PREC, int NT>
-__global__ void __launch_bounds__(NT) k_run1d(RunArgs a) {
+__global__ void __launch_bounds__(run1d_threads<NT>(), 1) k_run1d(RunArgs a) {
   namespace cg = cooperative_groups;
   using S = typename Prec<PREC>::S;
-  __shared__ Tile1DSmem<P, PREC, NT> sm;
-  // this step's stage lines (roles and dt are fixed within a step); raw
-  // storage, as shared variables take no constructors
-  __shared__ __align__(16) unsigned char lines_raw[sizeof(Line<S>) * MAXSTAGES];
-  Line<S>* lines = reinterpret_cast<Line<S>*>(lines_raw);
-  __shared__ Ctl sctl;    // CTA 0's copy is the cluster's controller
-  __shared__ Ctl spart;   // this CTA's stage CFL maxima and status (only those fields)
+  using R = typename Prec<PREC>::R;
+  constexpr int M = P::MEQN;
+  constexpr int NTH = run1d_threads<NT>();
+  // per step parity: the step's stage lines and row views (roles and dt
+  // are fixed within a step); raw storage, as shared variables take no
+  // constructors
+  __shared__ __align__(16) unsigned char lines_raw[2][sizeof(Line<S>) * MAXSTAGES];
+  __shared__ ResView views[2][MAXSTAGES];
+  __shared__ StageDesc sds[MAXSTAGES];
+  __shared__ Ctl sctl;                    // this CTA's copy of the controller
+  __shared__ Ctl spart[2];                // per step parity: this CTA's stage CFL maxima and status
+  __shared__ double tpart[2][MAXEQ][2];   // per step parity: this CTA's totals of the last stage
+  __shared__ double tsum[RES_TILES_PER_CTA][NT / 32][MAXEQ][2];   // per tile and warp (sum, error)
+  __shared__ int sdone;                   // the loop ends (set by the controller warp)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* rows = reinterpret_cast<S*>(smem_raw);
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank(), nc = (int)cl.num_blocks();
-  const bool leader = rank == 0 && threadIdx.x == 0;
-  Ctl* gctl = a.st.ctl;
-  if (leader) sctl = *gctl;
-  cl.sync();
-  Ctl* ctl = cl.map_shared_rank(&sctl, 0);
-  const int ntiles = (a.st.mx + NT - 2) / (NT - 1);
+  const int tid = threadIdx.x;
+  const bool cw = tid >= NT;              // the controller warp
+  const int mx = a.st.mx;
+  const int ntiles = (mx + NT - 2) / (NT - 1);
+  const int T = (ntiles + nc - 1) / nc;   // the host launches nc = ceil(ntiles / T) CTAs
+  const int cspan = T * (NT - 1);
+  const int rw = cspan + 6;
+  const int t0 = rank * T, t1 = t0 + T < ntiles ? t0 + T : ntiles;
   const int last = a.nstages - 1;
+  const long e0 = (long)rank * cspan;     // element offset of row element 0
+  // the rows from global memory (elements past the buffer's ghost cells read
+  // 1, as the stage kernels' staging does)
+#pragma unroll
+  for (int b = 0; b < NROLES; ++b) {
+    const S* g = static_cast<const S*>(a.st.buf[b]);
+    if (!g) continue;
+    for (int m = 0; m < M; ++m)
+      for (int k = tid; k < rw; k += NTH)
+        rows[((long)b * M + m) * rw + k] = e0 + k < (long)mx + 6 ? g[(long)m * a.st.plane + e0 + k] : (S)1;
+  }
+  // the stage descriptors (constant indices: a runtime index into a kernel
+  // parameter array copies the whole argument struct to local memory)
+#pragma unroll
+  for (int s = 0; s < MAXSTAGES; ++s)
+    if (tid == s) sds[s] = a.sd[s];
+  {
+    const int* src = reinterpret_cast<const int*>(a.st.ctl);
+    int* dst = reinterpret_cast<int*>(&sctl);
+    for (int k = tid; k < (int)(sizeof(Ctl) / sizeof(int)); k += NTH) dst[k] = src[k];
+  }
+  // every CTA's rows are loaded before any stage stores into them
+  cl.sync();
+  // Speculation: while the controller warp judges step n, the tile threads
+  // solve the interfaces of step n+1's first stage (first tile) as if step n
+  // were accepted (its input is then the last stage's output); a rejected
+  // step or a one-stage integrator solves them after the controller.
+  const bool spec_ok = a.nstages > 1;
   for (int it = 0;; ++it) {
-    if (leader) {
+    const int p = it & 1;
+    Line<S>* lines = reinterpret_cast<Line<S>*>(lines_raw[p]);
+    ResIface<R, M> pre;
+    int spec_buf = -1;
+    if (cw) {
+      const int lane = tid - NT;
       if (it > 0) {
-        unsigned long long m = 0;
+        const int pp = p ^ 1;
+        unsigned long long bits = 0;
         int st = 0;
-        for (int r = 0; r < nc; ++r) {
-          const Ctl* pr = cl.map_shared_rank(&spart, r);
-          const unsigned long long b = __double_as_longlong(pr->stage_cfl[last]);
-          m = b > m ? b : m;
-          st |= pr->status;
+        double ts[MAXEQ], tc[MAXEQ];
+#pragma unroll
+        for (int q = 0; q < MAXEQ; ++q) { ts[q] = 0.0; tc[q] = 0.0; }
+        if (lane < nc) {
+          const Ctl* pr = cl.map_shared_rank(&spart[pp], lane);
+          bits = (unsigned long long)__double_as_longlong(pr->stage_cfl[last]);
+          st = pr->status;
+          if (sctl.totals) {
+            const double(*pt)[2] = cl.map_shared_rank(&tpart[pp][0], lane);
+#pragma unroll
+            for (int q = 0; q < MAXEQ; ++q) { ts[q] = pt[q][0]; tc[q] = pt[q][1]; }
+          }
         }
-        sctl.stage_cfl[last] = __longlong_as_double(m);
-        sctl.status |= st;
-        ctl_end(&sctl, last, a.final_role);
+        // maximum of the bit patterns (as the global atomic max), OR of status
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const unsigned long long ob = __shfl_xor_sync(0xffffffffu, bits, o);
+          bits = ob > bits ? ob : bits;
+          st |= __shfl_xor_sync(0xffffffffu, st, o);
+        }
+        double tv[MAXEQ];
+        if (sctl.totals) {
+#pragma unroll
+          for (int q = 0; q < MAXEQ; ++q) {
+            CSum t{0.0, 0.0};
+            for (int r = 0; r < nc; ++r) t.add(__shfl_sync(0xffffffffu, ts[q], r), __shfl_sync(0xffffffffu, tc[q], r));
+            tv[q] = (t.s + t.c) * a.st.dx;
+          }
+        }
+        if (lane == 0) {
+          sctl.stage_cfl[last] = __longlong_as_double((long long)bits);
+          sctl.status |= st;
+          if (sctl.totals) {
+#pragma unroll
+            for (int q = 0; q < MAXEQ; ++q) sctl.tot_cand[q] = tv[q];
+          }
+          ctl_end(&sctl, last, a.final_role);
+        }
       }
-      if (it < a.max_iters) ctl_begin(&sctl);
+      if (lane == 0) {
+        if (it < a.max_iters) ctl_begin(&sctl);
+        // the same value in every CTA: the copies run on the same inputs
+        sdone = it == a.max_iters || sctl.done;
+      }
+      __syncwarp();
+      if (lane < a.nstages) {
+        const StageDesc sd = sds[lane];
+        Line<S> L = line1d<S>(a.st, sd, lane, &sctl);
+        L.ctl = &spart[p];
+        L.dtdx = L.dt / L.dx;
+        lines[lane] = L;
+        ResView v;
+        v.rw = rw;
+        v.rsh = 0;
+        v.cspan = cspan;
+        v.rank = rank;
+        v.rlast = nc - 1;
+        v.bin = sctl.role[sd.in];
+        v.bqo = sd.aux_in >= 0 ? sctl.role[sd.aux_in] : -1;
+        v.bout = sd.kind == SK_DQ ? -1 : sctl.role[sd.out];
+        v.bout2 = sd.out2 >= 0 ? sctl.role[sd.out2] : -1;
+        views[p][lane] = v;
+        spart[p].stage_cfl[lane] = 0.0;
+      }
+      if (lane == 0) spart[p].status = 0;
+      if (lane < MAXEQ * 2) tpart[p][lane / 2][lane % 2] = 0.0;
+    } else if (spec_ok && it > 0) {
+      // step it-1's lines and views (the other parity) stay unchanged here
+      spec_buf = views[p ^ 1][last].bout;
+      const int c = 1 + t0 * (NT - 1) + tid;
+      if (tid < NT - 1 && c <= mx) {
+        const Line<S>& Lp = reinterpret_cast<const Line<S>*>(lines_raw[p ^ 1])[0];
+        ResView v = views[p ^ 1][0];
+        CflMax<R> unused;
+        res_ifaces<P, CD, PREC>(Lp, a.st.ph, c, v, spec_buf, false, unused, pre);
+      }
     }
-    cl.sync();
-    // The same value in every thread: the controller writes ctl only before
-    // the barrier that follows the last stage of this iteration.
-    if (it == a.max_iters || ctl->done) break;
-    // one read of the controller's roles and dt per step, all stages at once
-    if (threadIdx.x < a.nstages) {
-      Line<S> L = line1d<S>(a.st, a.sd[threadIdx.x], threadIdx.x, ctl);
-      L.ctl = &spart;
-      lines[threadIdx.x] = L;
-      spart.stage_cfl[threadIdx.x] = 0.0;
-    }
-    if (threadIdx.x == 0) spart.status = 0;
     __syncthreads();
+    if (sdone) break;
+    const bool tot = sctl.totals;
     for (int s = 0; s < a.nstages; ++s) {
-      const Line<S> L = lines[s];
-      for (int t = rank; t < ntiles; t += nc)
-        stage1d_tile<P, CD, TF, PREC, NT>(L, a.st.ph, 1 + t * (NT - 1), sm);
+      const bool lst = s == last;
+      if (!cw) {
+        const Line<S> L = lines[s];
+        ResView v = views[p][s];
+        for (int t = t0; t < t1; ++t) {
+          v.rsh = (t - t0) * (NT - 1);
+          const int c0 = 1 + t * (NT - 1);
+          const bool use_pre = s == 0 && t == t0 && spec_buf >= 0 && spec_buf == v.bin;
+          if (tot && lst)
+            stage1d_res<P, CD, TF, PREC, NT, true>(L, a.st.ph, c0, v, true, &spart[p], tsum[t - t0]);
+          else
+            stage1d_res<P, CD, TF, PREC, NT, false>(L, a.st.ph, c0, v, lst, &spart[p], nullptr,
+                                                    use_pre ? &pre : nullptr);
+        }
+      }
+      if (tot && lst) {
+        // this CTA's totals: its tiles' warps in order
+        __syncthreads();
+        if (tid == 0) {
+          for (int q = 0; q < M; ++q) {
+            CSum tt{0.0, 0.0};
+            for (int t = 0; t < t1 - t0; ++t)
+              for (int w = 0; w < NT / 32; ++w) tt.add(tsum[t][w][q][0], tsum[t][w][q][1]);
+            tpart[p][q][0] = tt.s;
+            tpart[p][q][1] = tt.c;
+          }
+        }
+      }
       cl.sync();
     }
   }
-  // every CTA has left the loop (no more reads of CTA 0's shared memory)
-  // before the controller goes back to global memory and CTA 0 exits
+  // the rows back to global memory: the chunk's cells, and the ghost cells
+  // of the two ends
+  const int klo = rank == 0 ? 0 : 3;
+  const int khi = (int)((rank == nc - 1 ? (long)mx + 6 : e0 + cspan + 3) - e0);   // exclusive
+#pragma unroll
+  for (int b = 0; b < NROLES; ++b) {
+    S* g = static_cast<S*>(a.st.buf[b]);
+    if (!g) continue;
+    for (int m = 0; m < M; ++m)
+      for (int k = klo + tid; k < khi; k += NTH) g[(long)m * a.st.plane + e0 + k] = rows[((long)b * M + m) * rw + k];
+  }
+  if (rank == 0) {
+    const int* src = reinterpret_cast<const int*>(&sctl);
+    int* dst = reinterpret_cast<int*>(a.st.ctl);
+    for (int k = tid; k < (int)(sizeof(Ctl) / sizeof(int)); k += NTH) dst[k] = src[k];
+  }
+  // no CTA exits while another may still read its shared memory
   cl.sync();
-  if (leader) *gctl = sctl;
 }
 
 }  // namespace scl

@@ -35,6 +35,12 @@ CASES = [
     ("swf_kappa", lambda: cases.fwave_radial(mx=200, kappa=True), 4, dict(tend=0.01, dt_initial=0.001, cfl_max=0.3, cfl_desired=0.2)),
     # first step rejected and retaken
     ("euler_reject", lambda: cases.shu_osher(mx=120), 3, dict(tend=0.05, dt_initial=0.05, cfl_max=0.9, cfl_desired=0.8)),
+    # a last chunk narrower than the halo: its left neighbour's row holds
+    # ghost images too (periodic: 127 + 1 cells; two tiles per CTA, 1017
+    # cells = 8 tiles of 127 + 1 cell on 5 CTAs; walls: 127 + 2 cells)
+    ("advection_128_periodic", lambda: cases.advection(mx=128), 3, dict(tend=0.1, dt_initial=0.005, cfl_max=0.85, cfl_desired=0.8)),
+    ("advection_1017_periodic", lambda: cases.advection(mx=1017), 4, dict(tend=0.01, dt_initial=0.001, cfl_max=2.5, cfl_desired=2.4)),
+    ("acoustics_129_walls", lambda: cases.acoustics1d(mx=129, mthbc=(3, 3)), 3, dict(tend=0.2, dt_initial=0.002, cfl_max=0.9, cfl_desired=0.8)),
 ]
 
 

@@ -11,7 +11,8 @@ arithmetic form of the stages.  Checked here:
   is FP64 round-off in the FP64 forms, and the round-off of FP32 fluxes or
   FP32 state in the reduced-precision forms;
 * a rejected step leaves the totals of the accepted state;
-* totals need graph runs: the resident mode is refused while they are on.
+* the cluster-resident run keeps them too (summed by its tile code), equal
+  to the graph run's to a few ulps.
 """
 import math
 
@@ -44,16 +45,18 @@ def _host_totals(q, ndim, area, kappa=None, fp32=False):
     return np.array(out), np.array(scale)
 
 
+@pytest.mark.parametrize("mode", [S.RUN_GRAPH, S.RUN_RESIDENT])
 @pytest.mark.parametrize("precision", FORMS)
-def test_periodic_advection_totals(precision):
+def test_periodic_advection_totals(precision, mode):
     po, ps, q, _ = cases.advection(mx=1000)
     ps.time_integrator = 3
     fp32 = precision == "fp32"
     with S.Solver(ps, precision) as s:
+        s.set_run_mode(mode)
         s.set_totals(True)
         s.set_q(q)
         res = s.sharpclaw(0.0, 0.5, 0.0008, 0.85, 0.8)
-        assert s.last_run()[0] == S.RUN_GRAPH           # AUTO picks graphs while totals are on
+        assert s.last_run()[0] == mode
         qf = s.get_q()
         T = s.conserved_totals()
     assert res["info"] == 0 and res["steps_taken"] > 500
@@ -117,16 +120,31 @@ def test_rejected_step_keeps_the_accepted_totals():
     assert np.all(np.abs(T["tot"] - t1) <= 4e-16 * scale)
 
 
-def test_totals_refuse_the_resident_mode():
+def test_resident_and_graph_totals_agree_with_capacity():
+    po, ps, q, aux = cases.with_capacity(cases.advection(mx=500))
+    ps.time_integrator = 4
+    out = {}
+    for mode in (S.RUN_GRAPH, S.RUN_RESIDENT):
+        with S.Solver(ps, "fp64_strict") as s:
+            s.set_run_mode(mode)
+            s.set_aux(aux)
+            s.set_totals(True)
+            s.set_q(q)
+            s.sharpclaw(0.0, 0.1, 0.001, 2.5, 2.4)
+            assert s.last_run()[0] == mode
+            out[mode] = (s.get_q(), s.conserved_totals())
+    qg, Tg = out[S.RUN_GRAPH]
+    qr, Tr = out[S.RUN_RESIDENT]
+    assert np.array_equal(qg, qr)                      # the same arithmetic in both modes
+    kappa = aux[ps.mcapa - 1]
+    t1, scale = _host_totals(qr, 1, ps.dx, kappa)
+    for T in (Tg, Tr):
+        assert np.all(np.abs(T["tot"] - t1) <= 4e-16 * scale)
+        assert np.all(T["drift"] <= 1e-13 * scale)
+
+
+def test_totals_off_is_an_error():
     po, ps, q, _ = cases.advection(mx=200)
     with S.Solver(ps, "fp64") as s:
-        s.set_run_mode(S.RUN_RESIDENT)
-        with pytest.raises(S.SharpClawError):
-            s.set_totals(True)
-        s.set_run_mode(S.RUN_AUTO)
-        s.set_totals(True)
-        with pytest.raises(S.SharpClawError):
-            s.set_run_mode(S.RUN_RESIDENT)
-        s.set_totals(False)
         with pytest.raises(S.SharpClawError):
             s.conserved_totals()
