@@ -436,6 +436,10 @@ def run_gpu(args, rank, world, local_rank):
         wi = counters.get(key, {}).get("warp_inst_per_cell") if key else None
         roof[name]["compute_key"] = key
         roof[name]["warp_inst_per_cell_stage"] = wi
+        # this form's own DRAM bytes per cell when its kernel was captured
+        tpc = counters.get(key, {}).get("dram_bytes_per_cell") if key else None
+        if tpc:
+            roof[name]["traffic"] = tpc * W["cells"]
 
     # end to end through the public API with host buffers
     qh = torch.from_numpy(q0.copy()).pin_memory()

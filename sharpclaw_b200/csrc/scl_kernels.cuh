@@ -89,11 +89,20 @@ __device__ __forceinline__ Images images_1d(int c, int n, int bl, int br) {
   return im;
 }
 
+// Store the value of cell c (1..n) of component m and its ghost images (the
+// images of images_1d, in its order, negated for component 1 at a wall),
+// written directly: no indexed array, so no local memory.
 template <class S, class A>
-__device__ __forceinline__ void put_1d(S* base, long plane, int m, int c, const Images& im, A v) {
+__device__ __forceinline__ void put_1d_img(S* base, long plane, int m, int c, int n, int bl, int br, A v) {
   S* p = base + (long)m * plane;
   p[c + 2] = (S)v;
-  for (int k = 1; k < im.n; ++k) p[im.idx[k] + 2] = (S)((m == 1 && im.neg[k]) ? -v : v);
+  auto g = [&](int gi, bool neg) { p[gi + 2] = (S)((m == 1 && neg) ? -v : v); };
+  if (bl == 1 && c == 1) { g(-2, false); g(-1, false); g(0, false); }
+  if (bl == 2 && c >= n - 2) g(c - n, false);
+  if (bl == 3 && c <= 3) g(1 - c, true);
+  if (br == 1 && c == n) { g(n + 1, false); g(n + 2, false); g(n + 3, false); }
+  if (br == 2 && c <= 3) g(c + n, false);
+  if (br == 3 && c >= n - 2) g(2 * n + 1 - c, true);
 }
 
 template <class S, class A>
@@ -509,29 +518,40 @@ struct ResView {
 // Store the value of cell c (1..mx) of component m in the row `row` (this
 // CTA's row of the output buffer) and in every other CTA's row of that
 // buffer that holds the cell: the neighbours' halos, and, when `edge`, the
-// rows that hold its ghost images (images_1d, negated as put_1d negates).
+// rows that hold its ghost images (the images of images_1d, negated as
+// put_1d_img negates).  No division and no indexed local array: only the
+// chunk-edge threads do more than the first store.
 template <class S, class A>
 __device__ __forceinline__ void res_put(const ResView& v, S* row, int m, int c, int mx, int bl, int br, bool edge,
                                         A val) {
   const int cf = v.rank * v.cspan;   // the chunk's cells are cf+1 .. cf+cspan
-  row[c + 2 - cf] = (S)val;
-  const bool near = c <= cf + 3 || c > cf + v.cspan - 3;
-  if (!near && !edge) return;
+  const S x = (S)val;
+  row[c + 2 - cf] = x;
+  const bool lo = v.rank > 0 && c <= cf + 3;                   // in the left neighbour's right halo
+  const bool hi = v.rank < v.rlast && c > cf + v.cspan - 3;    // in the right neighbour's left halo
+  if (!lo && !hi && !edge) return;
   cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
-  // every rank other than `skip` whose row holds `cell` (-2 .. mx+3)
-  auto scatter = [&](int cell, S x, int skip) {
-    int rc = cell < 1 ? 0 : (cell - 1) / v.cspan;
-    rc = rc > v.rlast ? v.rlast : rc;
-    const int rhi = rc + 1 < v.rlast ? rc + 1 : v.rlast;
-    for (int r = rc > 0 ? rc - 1 : 0; r <= rhi; ++r) {
-      const int k = cell + 2 - r * v.cspan;
-      if (r != skip && k >= 0 && k < v.rw) *cl.map_shared_rank(row + k, r) = x;
-    }
-  };
-  if (near) scatter(c, (S)val, v.rank);
+  if (lo) *cl.map_shared_rank(row + (c + 2 - cf + v.cspan), v.rank - 1) = x;
+  if (hi) *cl.map_shared_rank(row + (c + 2 - cf - v.cspan), v.rank + 1) = x;
   if (edge) {
-    const Images im = images_1d(c, mx, bl, br);
-    for (int j = 1; j < im.n; ++j) scatter(im.idx[j], (S)((m == 1 && im.neg[j]) ? -val : val), -1);
+    // ghost cell g: the first chunk's row (g <= 0), or the last chunk's row
+    // and the row before it when g lies in that row's right halo
+    auto ghost = [&](int g, bool neg) {
+      const S y = (S)((m == 1 && neg) ? -val : val);
+      if (g <= 0) {
+        *cl.map_shared_rank(row + (g + 2), 0) = y;
+        return;
+      }
+      const int r1 = v.rlast;
+      *cl.map_shared_rank(row + (g + 2 - r1 * v.cspan), r1) = y;
+      if (r1 > 0 && g + 2 - (r1 - 1) * v.cspan < v.rw) *cl.map_shared_rank(row + (g + 2 - (r1 - 1) * v.cspan), r1 - 1) = y;
+    };
+    if (bl == 1 && c == 1) { ghost(-2, false); ghost(-1, false); ghost(0, false); }
+    if (bl == 2 && c >= mx - 2) ghost(c - mx, false);
+    if (bl == 3 && c <= 3) ghost(1 - c, true);
+    if (br == 1 && c == mx) { ghost(mx + 1, false); ghost(mx + 2, false); ghost(mx + 3, false); }
+    if (br == 2 && c <= 3) ghost(c + mx, false);
+    if (br == 3 && c >= mx - 2) ghost(2 * mx + 1 - c, true);
   }
 }
 
@@ -734,7 +754,7 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
             else
               tacc[m].add(v);
           }
-          if (edge) put_1d<S, Ac>(L.out, L.plane, m, c, images_1d(c, mx, L.bl, L.br), o1);
+          if (edge) put_1d_img<S, Ac>(L.out, L.plane, m, c, mx, L.bl, L.br, o1);
           else L.out[(long)m * L.plane + c + 2] = (S)o1;
           if (L.out2) L.out2[(long)m * L.plane + c + 2] = (S)o2;
         }
@@ -778,7 +798,11 @@ __device__ __forceinline__ void stage1d_tile(const Line<typename Prec<PREC>::S>&
 // across it.  The step graphs pass the interface results through shared
 // memory between the interface and the cell phase, which keeps the cell
 // phase's additions from fusing with the interface phase's products; a
-// resident tile that keeps them in registers passes them through this.
+// resident tile that keeps them in registers passes them through this (an
+// empty volatile asm with a register operand: no instruction, but the
+// compiler can neither see that the result equals the operand nor move the
+// point where the value is fixed; a non-volatile one let the FP64 form
+// differ from the graphs in the last bit again).
 __device__ __forceinline__ float opaque(float x) {
   asm volatile("" : "+f"(x));
   return x;
@@ -830,14 +854,16 @@ __device__ __forceinline__ void res_ifaces(const Line<typename Prec<PREC>::S>& L
       else { f.qrc[m] = opaque(xl[m]); f.amc1[m] = opaque(am[m]); }
     }
     if (CFL) {
-      // flux1.f90:126-133: max(dtdx(i)*s, -dtdx(i-1)*s)
-      double dtdx_c = dtdx0, dtdx_m = dtdx0;
-      if (L.mcapa > 0) {
+      // flux1.f90:126-133: max(dtdx(i)*s, -dtdx(i-1)*s); capacity grids are
+      // the rare case (kept off the common path's registers)
+      if (__builtin_expect(L.mcapa > 0, 0)) {
         const S* cap = static_cast<const S*>(L.aux) + (long)(L.mcapa - 1) * L.plane;
-        dtdx_c = dt / (L.dx * (double)cap[ci + 2]);
-        dtdx_m = dt / (L.dx * (double)cap[ci + 1]);
+        const double dtdx_c = dt / (L.dx * (double)cap[ci + 2]);
+        const double dtdx_m = dt / (L.dx * (double)cap[ci + 1]);
+        cfl.template add<MW>(s, dtdx_c, dtdx_m, true, true);
+      } else {
+        cfl.template add<MW>(s, dtdx0, dtdx0, false, true);
       }
-      cfl.template add<MW>(s, dtdx_c, dtdx_m, L.mcapa > 0, true);
     }
   }
 }
@@ -851,8 +877,8 @@ __device__ __forceinline__ void res_ifaces(const Line<typename Prec<PREC>::S>& L
 // the rows (res_put: halos and ghost images included).  Every interface,
 // cell bracket, source term and combination is the code and the operands of
 // stage1d_tile, so the outputs are those of the step graphs bit for bit.
-// pre: the thread's interface results already solved from the stage input
-// (res_ifaces), or nullptr.
+// use_pre: take the thread's interface results from pre, already solved
+// from the stage input (res_ifaces).
 //
 // CFL: the stage's CFL number and non-finite flag are reduced over each
 // warp and combined into part->stage_cfl[stage] / part->status by one atomic
@@ -861,12 +887,10 @@ __device__ __forceinline__ void res_ifaces(const Line<typename Prec<PREC>::S>& L
 // never with pre): the controller judges a step by its last stage, and a
 // non-finite output of an earlier stage reaches the last stage's output in
 // the same cell through the pointwise combinations.
-// TOT: the tile's conserved totals as (sum, error) pairs per warp, in
-// tsum[warp][m] (this CTA's shared memory; combined after the stage).
-template <class P, int CD, int TF, int PREC, int NT, bool TOT>
+template <class P, int CD, int TF, int PREC, int NT>
 __device__ __forceinline__ void stage1d_res(const Line<typename Prec<PREC>::S>& L, const Phys& ph, int c0,
-                                            const ResView& rv, bool CFL, Ctl* part, double (*tsum)[MAXEQ][2],
-                                            const ResIface<typename Prec<PREC>::R, P::MEQN>* pre = nullptr) {
+                                            const ResView& rv, bool CFL, Ctl* part,
+                                            const ResIface<typename Prec<PREC>::R, P::MEQN>& pre, bool use_pre) {
   using R = typename Prec<PREC>::R;
   using S = typename Prec<PREC>::S;
   using Ac = typename Prec<PREC>::A;
@@ -884,14 +908,9 @@ __device__ __forceinline__ void stage1d_res(const Line<typename Prec<PREC>::S>& 
   const bool own = tid < NT - 1 && c <= mx;
   CflMax<R> cfl;
   int bad = 0;
-  [[maybe_unused]] CSum tacc[M];
-  if constexpr (TOT) {
-#pragma unroll
-    for (int m = 0; m < M; ++m) tacc[m] = CSum{0.0, 0.0};
-  }
   if (own) {
     ResIface<R, M> f;
-    if (pre) f = *pre;
+    if (use_pre) f = pre;
     else res_ifaces<P, CD, PREC>(L, ph, c, rv, rv.bin, CFL, cfl, f);
     // ---- the cell ----
     R qc[M], br[M];
@@ -906,7 +925,7 @@ __device__ __forceinline__ void stage1d_res(const Line<typename Prec<PREC>::S>& 
         auxc[j * MA + k] = load_aux<S>(L.aux, (long)k * L.plane + c + 2 + j - (NB - 1) / 2);
     cell_bracket<P, TF, PREC>(ph, L.ixy, qc, auxc, f.qlc, f.qrc, f.apc, f.amc1, br);
     double dtdx_c = dtdx0;
-    if (L.mcapa > 0) {
+    if (__builtin_expect(L.mcapa > 0, 0)) {
       const S* cap = static_cast<const S*>(L.aux) + (long)(L.mcapa - 1) * L.plane;
       dtdx_c = dt / (L.dx * (double)cap[c + 2]);
     }
@@ -934,25 +953,11 @@ __device__ __forceinline__ void stage1d_res(const Line<typename Prec<PREC>::S>& 
       Ac o1, o2 = (Ac)0;
       combine<Ac, PREC == SCL_FP64_STRICT>(L.kind, qv, qov, dqv, o1, o2);
       bad |= !isfinite(o1);
-      if constexpr (TOT) {
-        const double v = (double)(S)o1;
-        if (L.mcapa > 0)
-          tacc[m].add(v * (double)static_cast<const S*>(L.aux)[(long)(L.mcapa - 1) * L.plane + c + 2]);
-        else
-          tacc[m].add(v);
-      }
       res_put<S, Ac>(rv, rrow(rv.bout, m), m, c, mx, L.bl, L.br, edge, o1);
-      if (rv.bout2 >= 0) res_put<S, Ac>(rv, rrow(rv.bout2, m), m, c, mx, 0, 0, false, o2);
+      if (__builtin_expect(rv.bout2 >= 0, 0)) res_put<S, Ac>(rv, rrow(rv.bout2, m), m, c, mx, 0, 0, false, o2);
     }
   }
   const int lane = tid & 31;
-  if constexpr (TOT) {
-#pragma unroll
-    for (int m = 0; m < M; ++m) {
-      const CSum t = warp_csum(tacc[m]);
-      if (lane == 0) { tsum[tid >> 5][m][0] = t.s; tsum[tid >> 5][m][1] = t.c; }
-    }
-  }
   if (CFL) {
     double v;
     if constexpr (std::is_same_v<R, double>) {

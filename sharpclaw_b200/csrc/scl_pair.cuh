@@ -501,13 +501,13 @@ __device__ __forceinline__ void pair_compute(const Line<typename Prec<PREC>::S>&
         if (L.out2) stp<S>(L.out2 + (long)m * L.plane + c + 2, (S)o2x, (S)o2y);
       } else {
         if (vx) {
-          if (c <= 3 || c >= mx - 2) put_1d<S, Ac>(L.out, L.plane, m, c, images_1d(c, mx, L.bl, L.br), ox);
+          if (c <= 3 || c >= mx - 2) put_1d_img<S, Ac>(L.out, L.plane, m, c, mx, L.bl, L.br, ox);
           else po[0] = (S)ox;
           if (L.out2) L.out2[(long)m * L.plane + c + 2] = (S)o2x;
         }
         if (vy) {
           if (c + 1 <= 3 || c + 1 >= mx - 2)
-            put_1d<S, Ac>(L.out, L.plane, m, c + 1, images_1d(c + 1, mx, L.bl, L.br), oy);
+            put_1d_img<S, Ac>(L.out, L.plane, m, c + 1, mx, L.bl, L.br, oy);
           else po[1] = (S)oy;
           if (L.out2) L.out2[(long)m * L.plane + c + 3] = (S)o2y;
         }

@@ -50,6 +50,77 @@ inline size_t run1d_rows_bytes(int meqn, int T, int nt) {
 template <int NT>
 constexpr int run1d_threads() { return NT + 32; }
 
+// Conserved totals of this CTA's cells in row buffer v.bout (the step's last
+// stage output): per tile and warp a compensated (sum, error) pair, then
+// thread 0 combines them in tile-then-warp order into tp[m].  Called by every
+// thread of the CTA (it contains a CTA barrier); out of line, so that runs
+// without totals carry none of its code.
+template <class P, int PREC, int NT>
+__device__ __noinline__ void res_totals_cta(const Line<typename Prec<PREC>::S>& L, const ResView& v, int t0, int t1,
+                                            double (*tsum)[NT / 32][MAXEQ][2], double (*tp)[2]) {
+  using S = typename Prec<PREC>::S;
+  constexpr int M = P::MEQN;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tid = threadIdx.x, lane = tid & 31;
+  if (tid < NT) {
+    for (int t = t0; t < t1; ++t) {
+      const int c = 1 + t * (NT - 1) + tid;
+      const bool own = tid < NT - 1 && c <= L.mx;
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        CSum acc{0.0, 0.0};
+        if (own) {
+          const S* row = reinterpret_cast<const S*>(smem_raw) + ((long)v.bout * M + m) * v.rw;
+          const double x = (double)row[(t - t0) * (NT - 1) + tid + 3];
+          if (L.mcapa > 0)
+            acc.add(x * (double)static_cast<const S*>(L.aux)[(long)(L.mcapa - 1) * L.plane + c + 2]);
+          else
+            acc.add(x);
+        }
+        acc = warp_csum(acc);
+        if (lane == 0) { tsum[t - t0][tid >> 5][m][0] = acc.s; tsum[t - t0][tid >> 5][m][1] = acc.c; }
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int m = 0; m < M; ++m) {
+      CSum tt{0.0, 0.0};
+      for (int t = 0; t < t1 - t0; ++t)
+        for (int w = 0; w < NT / 32; ++w) tt.add(tsum[t][w][m][0], tsum[t][w][m][1]);
+      tp[m][0] = tt.s;
+      tp[m][1] = tt.c;
+    }
+  }
+}
+
+// The step's candidate totals from every CTA's (sum, error) pairs tp (this
+// CTA's copy, read in each rank through distributed shared memory), combined
+// in rank order; called by the 32 lanes of the controller warp, the result
+// in lane 0's cand[].  Out of line for the same reason.
+static __device__ __noinline__ void res_totals_gather(const double (*tp)[2], int nc, int meqn, double dx, double* cand) {
+  cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+  const int lane = threadIdx.x & 31;
+  double ts[MAXEQ], tc[MAXEQ];
+#pragma unroll
+  for (int q = 0; q < MAXEQ; ++q) { ts[q] = 0.0; tc[q] = 0.0; }
+  if (lane < nc) {
+    const double(*pt)[2] = cl.map_shared_rank(&tp[0], lane);
+#pragma unroll
+    for (int q = 0; q < MAXEQ; ++q) { ts[q] = pt[q][0]; tc[q] = pt[q][1]; }
+  }
+#pragma unroll
+  for (int q = 0; q < MAXEQ; ++q) {
+    if (q >= meqn) {
+      if (lane == 0) cand[q] = 0.0;
+      continue;
+    }
+    CSum t{0.0, 0.0};
+    for (int r = 0; r < nc; ++r) t.add(__shfl_sync(0xffffffffu, ts[q], r), __shfl_sync(0xffffffffu, tc[q], r));
+    if (lane == 0) cand[q] = (t.s + t.c) * dx;
+  }
+}
+
 template <class P, int CD, int TF, int PREC, int NT>
 __global__ void __launch_bounds__(run1d_threads<NT>(), 1) k_run1d(RunArgs a) {
   namespace cg = cooperative_groups;
@@ -120,18 +191,10 @@ __global__ void __launch_bounds__(run1d_threads<NT>(), 1) k_run1d(RunArgs a) {
         const int pp = p ^ 1;
         unsigned long long bits = 0;
         int st = 0;
-        double ts[MAXEQ], tc[MAXEQ];
-#pragma unroll
-        for (int q = 0; q < MAXEQ; ++q) { ts[q] = 0.0; tc[q] = 0.0; }
         if (lane < nc) {
           const Ctl* pr = cl.map_shared_rank(&spart[pp], lane);
           bits = (unsigned long long)__double_as_longlong(pr->stage_cfl[last]);
           st = pr->status;
-          if (sctl.totals) {
-            const double(*pt)[2] = cl.map_shared_rank(&tpart[pp][0], lane);
-#pragma unroll
-            for (int q = 0; q < MAXEQ; ++q) { ts[q] = pt[q][0]; tc[q] = pt[q][1]; }
-          }
         }
         // maximum of the bit patterns (as the global atomic max), OR of status
 #pragma unroll
@@ -140,22 +203,10 @@ __global__ void __launch_bounds__(run1d_threads<NT>(), 1) k_run1d(RunArgs a) {
           bits = ob > bits ? ob : bits;
           st |= __shfl_xor_sync(0xffffffffu, st, o);
         }
-        double tv[MAXEQ];
-        if (sctl.totals) {
-#pragma unroll
-          for (int q = 0; q < MAXEQ; ++q) {
-            CSum t{0.0, 0.0};
-            for (int r = 0; r < nc; ++r) t.add(__shfl_sync(0xffffffffu, ts[q], r), __shfl_sync(0xffffffffu, tc[q], r));
-            tv[q] = (t.s + t.c) * a.st.dx;
-          }
-        }
+        if (sctl.totals) res_totals_gather(tpart[pp], nc, M, a.st.dx, sctl.tot_cand);
         if (lane == 0) {
           sctl.stage_cfl[last] = __longlong_as_double((long long)bits);
           sctl.status |= st;
-          if (sctl.totals) {
-#pragma unroll
-            for (int q = 0; q < MAXEQ; ++q) sctl.tot_cand[q] = tv[q];
-          }
           ctl_end(&sctl, last, a.final_role);
         }
       }
@@ -209,26 +260,12 @@ __global__ void __launch_bounds__(run1d_threads<NT>(), 1) k_run1d(RunArgs a) {
           v.rsh = (t - t0) * (NT - 1);
           const int c0 = 1 + t * (NT - 1);
           const bool use_pre = s == 0 && t == t0 && spec_buf >= 0 && spec_buf == v.bin;
-          if (tot && lst)
-            stage1d_res<P, CD, TF, PREC, NT, true>(L, a.st.ph, c0, v, true, &spart[p], tsum[t - t0]);
-          else
-            stage1d_res<P, CD, TF, PREC, NT, false>(L, a.st.ph, c0, v, lst, &spart[p], nullptr,
-                                                    use_pre ? &pre : nullptr);
+          stage1d_res<P, CD, TF, PREC, NT>(L, a.st.ph, c0, v, lst, &spart[p], pre, use_pre);
         }
       }
-      if (tot && lst) {
-        // this CTA's totals: its tiles' warps in order
-        __syncthreads();
-        if (tid == 0) {
-          for (int q = 0; q < M; ++q) {
-            CSum tt{0.0, 0.0};
-            for (int t = 0; t < t1 - t0; ++t)
-              for (int w = 0; w < NT / 32; ++w) tt.add(tsum[t][w][q][0], tsum[t][w][q][1]);
-            tpart[p][q][0] = tt.s;
-            tpart[p][q][1] = tt.c;
-          }
-        }
-      }
+      // this CTA's totals of the step's output (its own cells: no wait
+      // beyond the CTA barrier inside)
+      if (tot && lst) res_totals_cta<P, PREC, NT>(lines[s], views[p][s], t0, t1, tsum, tpart[p]);
       cl.sync();
     }
   }
