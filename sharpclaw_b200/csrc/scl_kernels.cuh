@@ -520,7 +520,9 @@ struct ResView {
 // buffer that holds the cell: the neighbours' halos, and, when `edge`, the
 // rows that hold its ghost images (the images of images_1d, negated as
 // put_1d_img negates).  No division and no indexed local array: only the
-// chunk-edge threads do more than the first store.
+// chunk-edge threads do more than the first store.  (An out-of-line image
+// store measured slower: the few threads that call it are on the critical
+// path of the stage's cluster barrier.)
 template <class S, class A>
 __device__ __forceinline__ void res_put(const ResView& v, S* row, int m, int c, int mx, int bl, int br, bool edge,
                                         A val) {

@@ -143,6 +143,28 @@ def test_resident_and_graph_totals_agree_with_capacity():
         assert np.all(T["drift"] <= 1e-13 * scale)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_resident_totals_several_tiles_per_cta(precision):
+    """5000 cells: 40 tiles on a cluster of 8, five per CTA; the CTA sums its
+    tiles' warps in order, the controller warp the CTAs in rank order."""
+    po, ps, q, _ = cases.advection(mx=5000)
+    ps.time_integrator = 3
+    with S.Solver(ps, precision) as s:
+        s.set_run_mode(S.RUN_RESIDENT)
+        s.set_totals(True)
+        s.set_q(q)
+        res = s.sharpclaw(0.0, 0.01, 0.0001, 0.85, 0.8)
+        assert s.last_run()[0] == S.RUN_RESIDENT
+        qf = s.get_q()
+        T = s.conserved_totals()
+    assert res["info"] == 0 and res["steps_taken"] > 10
+    t0, scale = _host_totals(q, 1, ps.dx)
+    t1, _ = _host_totals(qf, 1, ps.dx)
+    assert np.all(np.abs(T["tot0"] - t0) <= 4e-16 * scale)
+    assert np.all(np.abs(T["tot"] - t1) <= 4e-16 * scale)
+    assert np.all(T["drift"] <= DRIFT[precision] * scale)
+
+
 def test_totals_off_is_an_error():
     po, ps, q, _ = cases.advection(mx=200)
     with S.Solver(ps, "fp64") as s:
