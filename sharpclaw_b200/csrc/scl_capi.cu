@@ -1064,6 +1064,7 @@ int run_resident(scl_handle* h, float* ms) {
   ra.nstages = h->nstages;
   ra.final_role = h->final_role;
   ra.max_iters = RES_ITERS;
+  ra.totals = h->totals_on ? 1 : 0;
   const long max_launches = (long)h->hctl->maxn / RES_ITERS + 1;
   if (ms) CK(cudaEventRecord(h->ev0, h->stream));
   h->last_mode = SCL_RUN_RESIDENT;

@@ -130,6 +130,7 @@ struct RunArgs {
   StageDesc sd[MAXSTAGES];
   int nstages, final_role;
   int max_iters;            // controller iterations of one launch
+  int totals;               // conserved totals are kept (Ctl::totals of the run)
 };
 
 // NaN-propagating maximum used for the CFL number: a NaN anywhere makes the

@@ -77,7 +77,9 @@ cudaError_t launch_run1d(const RunArgs& a, cudaStream_t st) {
   const int T = (ntiles + RES_CLUSTER - 1) / RES_CLUSTER;
   const int nc = (ntiles + T - 1) / T;
   const size_t rows = run1d_rows_bytes<S>(P::MEQN, T, RES_NT);
-  auto k = k_run1d<P, CD, TF, PREC, RES_NT>;
+  bool gen = a.st.mcapa > 0 || a.totals;
+  for (int s = 0; s < a.nstages; ++s) gen = gen || a.sd[s].out2 >= 0;
+  auto k = gen ? k_run1d<P, CD, TF, PREC, RES_NT, true> : k_run1d<P, CD, TF, PREC, RES_NT, false>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};

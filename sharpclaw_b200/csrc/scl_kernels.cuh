@@ -823,8 +823,9 @@ struct ResIface {
 
 // Both interfaces of cell c = c0 + tid from the rows of buffer `bin`
 // (window element rsh + tid + j + k is cell c - 3 + j + k), with their CFL
-// contributions added to cfl when CFL.
-template <class P, int CD, int PREC>
+// contributions added to cfl when CFL.  GEN: the grid may have a capacity
+// field (false: the caller checked that it has none).
+template <class P, int CD, int PREC, bool GEN>
 __device__ __forceinline__ void res_ifaces(const Line<typename Prec<PREC>::S>& L, const Phys& ph, int c,
                                            const ResView& rv, int bin, bool CFL,
                                            CflMax<typename Prec<PREC>::R>& cfl,
@@ -858,7 +859,7 @@ __device__ __forceinline__ void res_ifaces(const Line<typename Prec<PREC>::S>& L
     if (CFL) {
       // flux1.f90:126-133: max(dtdx(i)*s, -dtdx(i-1)*s); capacity grids are
       // the rare case (kept off the common path's registers)
-      if (__builtin_expect(L.mcapa > 0, 0)) {
+      if (GEN && __builtin_expect(L.mcapa > 0, 0)) {
         const S* cap = static_cast<const S*>(L.aux) + (long)(L.mcapa - 1) * L.plane;
         const double dtdx_c = dt / (L.dx * (double)cap[ci + 2]);
         const double dtdx_m = dt / (L.dx * (double)cap[ci + 1]);
@@ -880,7 +881,9 @@ __device__ __forceinline__ void res_ifaces(const Line<typename Prec<PREC>::S>& L
 // cell bracket, source term and combination is the code and the operands of
 // stage1d_tile, so the outputs are those of the step graphs bit for bit.
 // use_pre: take the thread's interface results from pre, already solved
-// from the stage input (res_ifaces).
+// from the stage input (res_ifaces).  GEN: the run may have a capacity field
+// or a stage with a second output (false: the caller checked that it has
+// neither, and their code is left out).
 //
 // CFL: the stage's CFL number and non-finite flag are reduced over each
 // warp and combined into part->stage_cfl[stage] / part->status by one atomic
@@ -889,7 +892,7 @@ __device__ __forceinline__ void res_ifaces(const Line<typename Prec<PREC>::S>& L
 // never with pre): the controller judges a step by its last stage, and a
 // non-finite output of an earlier stage reaches the last stage's output in
 // the same cell through the pointwise combinations.
-template <class P, int CD, int TF, int PREC, int NT>
+template <class P, int CD, int TF, int PREC, int NT, bool GEN>
 __device__ __forceinline__ void stage1d_res(const Line<typename Prec<PREC>::S>& L, const Phys& ph, int c0,
                                             const ResView& rv, bool CFL, Ctl* part,
                                             const ResIface<typename Prec<PREC>::R, P::MEQN>& pre, bool use_pre) {
@@ -913,7 +916,7 @@ __device__ __forceinline__ void stage1d_res(const Line<typename Prec<PREC>::S>& 
   if (own) {
     ResIface<R, M> f;
     if (use_pre) f = pre;
-    else res_ifaces<P, CD, PREC>(L, ph, c, rv, rv.bin, CFL, cfl, f);
+    else res_ifaces<P, CD, PREC, GEN>(L, ph, c, rv, rv.bin, CFL, cfl, f);
     // ---- the cell ----
     R qc[M], br[M];
 #pragma unroll
@@ -927,7 +930,7 @@ __device__ __forceinline__ void stage1d_res(const Line<typename Prec<PREC>::S>& 
         auxc[j * MA + k] = load_aux<S>(L.aux, (long)k * L.plane + c + 2 + j - (NB - 1) / 2);
     cell_bracket<P, TF, PREC>(ph, L.ixy, qc, auxc, f.qlc, f.qrc, f.apc, f.amc1, br);
     double dtdx_c = dtdx0;
-    if (__builtin_expect(L.mcapa > 0, 0)) {
+    if (GEN && __builtin_expect(L.mcapa > 0, 0)) {
       const S* cap = static_cast<const S*>(L.aux) + (long)(L.mcapa - 1) * L.plane;
       dtdx_c = dt / (L.dx * (double)cap[c + 2]);
     }
@@ -956,7 +959,7 @@ __device__ __forceinline__ void stage1d_res(const Line<typename Prec<PREC>::S>& 
       combine<Ac, PREC == SCL_FP64_STRICT>(L.kind, qv, qov, dqv, o1, o2);
       bad |= !isfinite(o1);
       res_put<S, Ac>(rv, rrow(rv.bout, m), m, c, mx, L.bl, L.br, edge, o1);
-      if (__builtin_expect(rv.bout2 >= 0, 0)) res_put<S, Ac>(rv, rrow(rv.bout2, m), m, c, mx, 0, 0, false, o2);
+      if (GEN && __builtin_expect(rv.bout2 >= 0, 0)) res_put<S, Ac>(rv, rrow(rv.bout2, m), m, c, mx, 0, 0, false, o2);
     }
   }
   const int lane = tid & 31;
@@ -966,7 +969,7 @@ __device__ __forceinline__ void stage1d_res(const Line<typename Prec<PREC>::S>& 
       v = warp_max(cfl.v);
     } else {
       const float w = warp_max(cfl.sx);
-      v = L.mcapa > 0 ? nanmax((double)w, 0.0) : nanmax(dtdx0 * (double)w, dtdx0 * 0.0);
+      v = (GEN && L.mcapa > 0) ? nanmax((double)w, 0.0) : nanmax(dtdx0 * (double)w, dtdx0 * 0.0);
     }
     const int anybad = __any_sync(0xffffffffu, bad);
     if (lane == 0) {
