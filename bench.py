@@ -532,6 +532,26 @@ def run_gpu(args, rank, world, local_rank):
     if args.workload == "c5" and rank == 0:
         adj = c5_adjoint(S, ps, q0, aux0, W["dt0"])
 
+    # the other single-grid configurations, a few timed steps each in the
+    # same process and the same way as the headline (device-resident state,
+    # L2 flushed between steps, CUDA events), headline form and plain FP64
+    others = None
+    if args.workload == "c2" and not args.no_batched:
+        others = {}
+        for wname in ("c1", "c3", "c5"):
+            Wo = workloads()[wname]()
+            entry = {"workload": Wo["desc"], "cells": Wo["cells"], "time_steps_per_step": Wo["nstep"]}
+            for prec in (args.precision, "fp64"):
+                key = "fp64" if prec == "fp64" else "headline"
+                try:
+                    rate, ms, mode = quick_config(S, Wo, prec, 3, 2, flush, world, dev, barrier)
+                except Exception as e:   # never lose the headline line to this block
+                    entry[key] = {"error": f"{type(e).__name__}: {e}"}
+                    continue
+                entry[key] = {"value": rate, "unit": UNIT, "precision": prec, "ms_per_step": ms,
+                              "time_loop": "cluster-resident launch" if mode == S.RUN_RESIDENT else "CUDA graphs"}
+            others[wname] = entry
+
     # kernels the library launched in one timed sharpclaw loop (graph nodes
     # counted one by one; one launch per 4096 steps for a cluster-resident run)
     run_mode, run_launches = s_mix.timed_run_record
@@ -577,10 +597,50 @@ def run_gpu(args, rank, world, local_rank):
             line["adjoint"] = adj
         if batched is not None:
             line["batched"] = batched
+        if others is not None:
+            line["other_configs"] = others
         print(json.dumps(line), flush=True)
     s_mix.close()
     s_64.close()
     return 0
+
+
+def quick_config(S, W, precision, steps, warmup, flush, world, dev, barrier):
+    """Cell-stage rate of workload W in one arithmetic form: `warmup` untimed
+    then `steps` timed runs of W's step (time_steps on the device-resident
+    state, CUDA events inside the library), L2 flushed before each; the
+    slowest rank's time.  Returns (rate, ms per step, run mode)."""
+    import torch
+    ps, q0, aux0 = W["params"], W["q"], W["aux"]
+    cfl_max, cfl_des = W["cfl"]
+    s = S.Solver(ps, precision)
+    try:
+        if aux0 is not None:
+            s.set_aux(aux0)
+        s.set_q(q0)
+
+        def one():
+            if W["tend"] < 1e29:
+                s.set_q(q0)
+            flush.zero_()
+            torch.cuda.synchronize()
+            return s.time_steps(W["nstep"], W["dt0"], cfl_max, cfl_des, tend=W["tend"],
+                                dt_variable=W["dt_variable"])
+
+        for _ in range(warmup):
+            one()
+        barrier()
+        total_ms, taken = 0.0, 0
+        for _ in range(steps):
+            ms, res = one()
+            assert res["status"] == 0 and res["info"] in (0, 11), res
+            total_ms += ms
+            taken += res["steps_taken"] - res["rejected"]
+        barrier()
+        rate, s_max = job_rate(W["cells"] * W["stages"] * taken, total_ms / 1000.0, world, dev)
+        return rate, 1000.0 * s_max / steps, s.last_run()[0]
+    finally:
+        s.close()
 
 
 def c5_adjoint(S, ps, q0, aux0, dt, nsteps=200, ckpt=20):

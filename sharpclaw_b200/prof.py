@@ -56,7 +56,24 @@ def advection1d(mx):
     return p, q, None, 0.8 * dx
 
 
-WORKLOADS = {"euler1d": euler1d, "sw2d": sw2d, "advection1d": advection1d}
+def acoustics2d(n):
+    """2-D variable-coefficient acoustics on [0,1]^2, periodic: smooth
+    impedance and sound-speed fields (aux = rho*c, c), a Gaussian pressure
+    pulse; componentwise WENO5, rpn2 + tfluct, SSPRK(3,3)."""
+    d = 1.0 / n
+    xc = (np.arange(-3, n + 3) + 0.5) * d
+    X, Y = np.meshgrid(xc, xc, indexing="xy")
+    rho = 1.0 + 0.3 * np.sin(2 * np.pi * X) * np.cos(2 * np.pi * Y)
+    c = 1.0 + 0.2 * np.cos(2 * np.pi * X)
+    aux = np.ascontiguousarray(np.stack([rho * c, c]))
+    q = np.zeros((3, n + 6, n + 6))
+    q[0] = np.exp(-((X - 0.5) ** 2 + (Y - 0.5) ** 2) / (2 * 0.05 ** 2))
+    p = S.ClawParams(rp=S.RP_ACOUSTICS2D, mx=n, my=n, dx=d, dy=d, mthbc=(2, 2, 2, 2), char_decomp=0,
+                     tfluct_solver=1, time_integrator=3)
+    return p, q, aux, 0.4 * d / 1.2
+
+
+WORKLOADS = {"euler1d": euler1d, "sw2d": sw2d, "advection1d": advection1d, "acoustics2d": acoustics2d}
 
 
 def main():
