@@ -324,7 +324,7 @@ def workloads():
                     nstep=20, cells=n * n, stages=3, bytes_cell_stage=8.0 / 3.0 * 3 * 8 + 2 * 8,
                     desc="2-D variable-coefficient acoustics 1024x1024 periodic, rho,K log-normal(0,0.3) "
                          "smoothed (periodic), p0 = 4 Gaussian bumps + 0.05 cos cos, WENO5 componentwise + "
-                         "rpn2/tfluct, SSPRK3, fixed dt, 20 steps per step", traffic_key=None,
+                         "rpn2/tfluct, SSPRK3, fixed dt, 20 steps per step", traffic_key="k_stage2d_acoustics_mixed",
                     oracle_steps=2)
 
     return {"c2": c2, "c1": c1, "c3": c3, "c5": c5}
