@@ -441,3 +441,109 @@ def test_time_reversal_returns_the_pulse():
     po.b4step = 0
     qn, _ = O.sharpclaw(po, q, aux, **run)
     assert np.abs(qn[0, 3:-3] - q[0, 3:-3]).max() >= 0.5 * scale
+
+
+def _weno5_written(q):
+    """src/reconstruct.f90:77-143 written out in Python floats (IEEE double,
+    no fused multiply-add), in the source's evaluation order: the REAL(4)
+    literals 13., 3., 6., 0.5, 0.25, 12. are exact, `x**2` is x*x,
+    epweno = 1.e-36 is the REAL(4) value widened (reconstruct.f90:6).
+    Fortran index i (1-based) is Python index i-1."""
+    eps = float(np.float32(1e-36))
+    mx2 = len(q)
+    qf = lambda i: float(q[i - 1])
+    d = {i: qf(i) - qf(i - 1) for i in range(2, mx2 + 1)}
+    d[1] = float("nan")   # dq1m(1) is never assigned in the reference: qr(2) (a ghost interface) is undefined
+    ql = [0.0] * mx2
+    qr = [0.0] * mx2
+    mbc = 3
+    for m1 in (1, 2):
+        im = 1 if m1 == 1 else -1
+        ione, inone, intwo = im, -im, -2 * im
+        for i in range(mbc, mx2 - mbc + 2):
+            t1 = im * (d[i + intwo] - d[i + inone])
+            t2 = im * (d[i + inone] - d[i])
+            t3 = im * (d[i] - d[i + ione])
+            x1 = d[i + intwo] - 3.0 * d[i + inone]
+            x2 = d[i + inone] + d[i]
+            x3 = 3.0 * d[i] - d[i + ione]
+            tt1 = 13.0 * (t1 * t1) + 3.0 * (x1 * x1)
+            tt2 = 13.0 * (t2 * t2) + 3.0 * (x2 * x2)
+            tt3 = 13.0 * (t3 * t3) + 3.0 * (x3 * x3)
+            tt1 = (eps + tt1) * (eps + tt1)
+            tt2 = (eps + tt2) * (eps + tt2)
+            tt3 = (eps + tt3) * (eps + tt3)
+            s1 = tt2 * tt3
+            s2 = (6.0 * tt1) * tt3
+            s3 = (3.0 * tt1) * tt2
+            t0 = 1.0 / ((s1 + s2) + s3)
+            s1 = s1 * t0
+            s3 = s3 * t0
+            uu = (s1 * (t2 - t1) + (0.5 * s3 - 0.25) * (t3 - t2)) / 3.0 \
+                + ((-qf(i - 2) + 7.0 * (qf(i - 1) + qf(i))) - qf(i + 1)) / 12.0
+            if m1 == 1:
+                qr[i - 2] = uu      # qr(i-1) = uu(i,1)
+            else:
+                ql[i - 1] = uu      # ql(i) = uu(i,2)
+    return ql, qr
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_weno5_matches_the_written_formulas_bit_for_bit(seed):
+    """The oracle's componentwise WENO5 against the reference formulas
+    written out independently above, on a smooth line, a jump and noise:
+    every reconstructed value identical to the last bit."""
+    rng = np.random.default_rng(seed)
+    mx2 = 16
+    x = np.linspace(0.0, 1.0, mx2)
+    lines = [np.sin(2 * np.pi * x) + 0.1 * x, np.where(x < 0.5, 1.0, 0.125), rng.standard_normal(mx2)]
+    q = np.stack(lines)
+    ql, qr = O.weno5(q)
+    for m in range(q.shape[0]):
+        wl, wr = _weno5_written(q[m])
+        for i in range(3, mx2 - 1):          # ql(i), i = mbc .. mx2-mbc+1 (1-based)
+            assert ql[m, i - 1] == wl[i - 1], (m, i)
+        for i in range(3, mx2 - 2):          # qr(i), i = mbc .. mx2-mbc (qr(2) is undefined, see above)
+            assert qr[m, i - 1] == wr[i - 1], (m, i)
+
+
+def test_euler_roe_waves_match_the_written_formulas_bit_for_bit():
+    """The oracle's Euler Riemann solver (Roe averages, wave strengths,
+    waves and speeds) against apps/euler/shockentropy/rp1eu.f:44-86 written
+    out independently in Python floats, in the source's evaluation order
+    (`x**2` as x*x, products and quotients left to right, dsqrt correctly
+    rounded): identical to the last bit at every interface."""
+    import math
+    rng = np.random.default_rng(21)
+    n = 24
+    p = O.make_params(mx=n - 6, meqn=3, mwaves=3, dx=0.1, rp=O.RP_EULER, mthbc=(1, 1))
+    gamma1 = p.gamma - 1.0
+    rho = rng.uniform(0.2, 3.0, n)
+    u = rng.uniform(-2.0, 2.0, n)
+    pr = rng.uniform(0.2, 3.0, n)
+    q = np.stack([rho, rho * u, pr / 0.4 + 0.5 * rho * u * u])
+    ql = q.copy()
+    qr = np.roll(q, 1, axis=1) * 1.01          # a jump at every interface
+    wave, s, _, _ = O.rp(p, ql, qr)
+    for i in range(1, n):
+        l1, l2, l3 = (float(v) for v in qr[:, i - 1])
+        r1, r2, r3 = (float(v) for v in ql[:, i])
+        rhsqrtl, rhsqrtr = math.sqrt(l1), math.sqrt(r1)
+        pl = gamma1 * (l3 - (0.5 * (l2 * l2)) / l1)
+        prr = gamma1 * (r3 - (0.5 * (r2 * r2)) / r1)
+        rhsq2 = rhsqrtl + rhsqrtr
+        ui = (l2 / rhsqrtl + r2 / rhsqrtr) / rhsq2
+        enth = ((l3 + pl) / rhsqrtl + (r3 + prr) / rhsqrtr) / rhsq2
+        ai = math.sqrt(gamma1 * (enth - 0.5 * (ui * ui)))
+        d1, d2, d3 = r1 - l1, r2 - l2, r3 - l3
+        a2 = (gamma1 / (ai * ai)) * (((enth - ui * ui) * d1 + ui * d2) - d3)
+        a3 = ((d2 + (ai - ui) * d1) - ai * a2) / (2.0 * ai)
+        a1 = (d1 - a2) - a3
+        want_w = [[a1, a1 * (ui - ai), a1 * (enth - ui * ai)],
+                  [a2, a2 * ui, (a2 * 0.5) * (ui * ui)],
+                  [a3, a3 * (ui + ai), a3 * (enth + ui * ai)]]
+        want_s = [ui - ai, ui, ui + ai]
+        for mw in range(3):
+            assert s[mw, i] == want_s[mw], (i, mw)
+            for m in range(3):
+                assert wave[mw, m, i] == want_w[mw][m], (i, mw, m)
