@@ -547,3 +547,75 @@ def test_euler_roe_waves_match_the_written_formulas_bit_for_bit():
             assert s[mw, i] == want_s[mw], (i, mw)
             for m in range(3):
                 assert wave[mw, m, i] == want_w[mw][m], (i, mw, m)
+
+
+def test_weno5_char_matches_the_written_formulas_bit_for_bit():
+    """The oracle's characteristic-wise WENO5 against src/reconstruct.f90:
+    146-241 written out independently (projection sums from 0 in component
+    order, the same WENO algebra on the projections, back-projection added
+    field by field), with arbitrary per-interface eigenvector matrices:
+    identical to the last bit at every interface the reference defines
+    (interface 3 reads projections hh(3,:) that the reference never sets)."""
+    import ctypes
+    rng = np.random.default_rng(5)
+    meqn, mx2 = 3, 18
+    q = rng.standard_normal((meqn, mx2)) + np.linspace(0, 2, mx2)
+    evl = rng.standard_normal((meqn, meqn, mx2))     # evl(i, ip, m) at [m, ip, i]
+    evr = rng.standard_normal((meqn, meqn, mx2))     # evr(i, m, ip) at [ip, m, i]
+    ql = np.zeros((meqn, mx2))
+    qr = np.zeros((meqn, mx2))
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    assert O.lib().ocl_weno5_char(mx2, meqn, dp(q), dp(evl), dp(evr), dp(ql), dp(qr)) == 0
+    eps = float(np.float32(1e-36))
+    Q = lambda i, m: float(q[m - 1, i - 1])
+    EL = lambda i, ip, m: float(evl[m - 1, ip - 1, i - 1])
+    ER = lambda i, m, ip: float(evr[ip - 1, m - 1, i - 1])
+    dq = {(i, m): Q(i, m) - Q(i - 1, m) for m in range(1, meqn + 1) for i in range(2, mx2 + 1)}
+    wl, wr = {}, {}
+    for m in range(1, meqn + 1):
+        for i in range(3, mx2):
+            c = ((-Q(i - 2, m)) + 7.0 * (Q(i - 1, m) + Q(i, m))) - Q(i + 1, m)
+            wr[(i - 1, m)] = c / 12.0
+            wl[(i, m)] = wr[(i - 1, m)]
+    for ip in range(1, meqn + 1):
+        hh = {}
+        for m2 in range(-2, 3):
+            for i in range(4, mx2 - 1):
+                h = 0.0
+                for m in range(1, meqn + 1):
+                    h = h + EL(i, ip, m) * dq[(i + m2, m)]
+                hh[(i, m2)] = h
+        for m2 in range(-2, 3):
+            hh[(3, m2)] = float("nan")
+        uu = {}
+        for m1 in (1, 2):
+            im = 1 if m1 == 1 else -1
+            ione, inone, intwo = im, -im, -2 * im
+            for i in range(3, mx2 - 1):
+                t1 = im * (hh[(i, intwo)] - hh[(i, inone)])
+                t2 = im * (hh[(i, inone)] - hh[(i, 0)])
+                t3 = im * (hh[(i, 0)] - hh[(i, ione)])
+                x1 = hh[(i, intwo)] - 3.0 * hh[(i, inone)]
+                x2 = hh[(i, inone)] + hh[(i, 0)]
+                x3 = 3.0 * hh[(i, 0)] - hh[(i, ione)]
+                tt1 = 13.0 * (t1 * t1) + 3.0 * (x1 * x1)
+                tt2 = 13.0 * (t2 * t2) + 3.0 * (x2 * x2)
+                tt3 = 13.0 * (t3 * t3) + 3.0 * (x3 * x3)
+                tt1 = (eps + tt1) * (eps + tt1)
+                tt2 = (eps + tt2) * (eps + tt2)
+                tt3 = (eps + tt3) * (eps + tt3)
+                s1 = tt2 * tt3
+                s2 = (6.0 * tt1) * tt3
+                s3 = (3.0 * tt1) * tt2
+                t0 = 1.0 / ((s1 + s2) + s3)
+                s1 = s1 * t0
+                s3 = s3 * t0
+                uu[(i, m1)] = (s1 * (t2 - t1) + (0.5 * s3 - 0.25) * (t3 - t2)) / 3.0
+        for m in range(1, meqn + 1):
+            for i in range(3, mx2 - 1):
+                wr[(i - 1, m)] = wr[(i - 1, m)] + ER(i, m, ip) * uu[(i, 1)]
+                wl[(i, m)] = wl[(i, m)] + ER(i, m, ip) * uu[(i, 2)]
+    for m in range(1, meqn + 1):
+        for i in range(4, mx2 - 1):          # interfaces 4 .. mx2-2: qr(i-1), ql(i)
+            assert qr[m - 1, i - 2] == wr[(i - 1, m)], (m, i)
+            assert ql[m - 1, i - 1] == wl[(i, m)], (m, i)
