@@ -619,3 +619,105 @@ def test_weno5_char_matches_the_written_formulas_bit_for_bit():
         for i in range(4, mx2 - 1):          # interfaces 4 .. mx2-2: qr(i-1), ql(i)
             assert qr[m - 1, i - 2] == wr[(i - 1, m)], (m, i)
             assert ql[m - 1, i - 1] == wl[(i, m)], (m, i)
+
+
+def _euler_roe_written(l, r, gamma):
+    """rp1eu.f:44-86 at one interface (left state l = qr(i-1), right r =
+    ql(i)): the waves [mw][m] and speeds, in the source's order."""
+    import math
+    gamma1 = gamma - 1.0
+    l1, l2, l3 = l
+    r1, r2, r3 = r
+    rhsqrtl, rhsqrtr = math.sqrt(l1), math.sqrt(r1)
+    pl = gamma1 * (l3 - (0.5 * (l2 * l2)) / l1)
+    prr = gamma1 * (r3 - (0.5 * (r2 * r2)) / r1)
+    rhsq2 = rhsqrtl + rhsqrtr
+    u = (l2 / rhsqrtl + r2 / rhsqrtr) / rhsq2
+    enth = ((l3 + pl) / rhsqrtl + (r3 + prr) / rhsqrtr) / rhsq2
+    a = math.sqrt(gamma1 * (enth - 0.5 * (u * u)))
+    d1, d2, d3 = r1 - l1, r2 - l2, r3 - l3
+    a2 = (gamma1 / (a * a)) * (((enth - u * u) * d1 + u * d2) - d3)
+    a3 = ((d2 + (a - u) * d1) - a * a2) / (2.0 * a)
+    a1 = (d1 - a2) - a3
+    w = [[a1, a1 * (u - a), a1 * (enth - u * a)],
+         [a2, a2 * u, (a2 * 0.5) * (u * u)],
+         [a3, a3 * (u + a), a3 * (enth + u * a)]]
+    return w, [u - a, u, u + a]
+
+
+def _euler_efix_written(l, r, w, s, gamma):
+    """rp1eu.f:116-213 (Harten-Hyman entropy fix) at one interface: amdq,
+    apdq and the branch taken for the 1- and 3-waves."""
+    import math
+    gamma1 = gamma - 1.0
+
+    def sound(rho, mom, en):
+        p = gamma1 * (en - (0.5 * (mom * mom)) / rho)
+        x = (gamma * p) / rho
+        return math.sqrt(x) if x >= 0.0 else float("nan")   # dsqrt of a negative: NaN
+
+    amdq = [0.0, 0.0, 0.0]
+    branch = "supersonic"
+    cim1 = sound(*l)
+    s0 = l[1] / l[0] - cim1
+    if not (s0 >= 0.0 and s[0] > 0.0):
+        rho1, rhou1, en1 = l[0] + w[0][0], l[1] + w[0][1], l[2] + w[0][2]
+        s1 = rhou1 / rho1 - sound(rho1, rhou1, en1)
+        if s0 < 0.0 and s1 > 0.0:
+            sfract, branch = (s0 * (s1 - s[0])) / (s1 - s0), "transonic-1"
+        elif s[0] < 0.0:
+            sfract, branch = s[0], "left-1"
+        else:
+            sfract, branch = 0.0, "right-1"
+        amdq = [sfract * w[0][m] for m in range(3)]
+        if not (s[1] >= 0.0):
+            amdq = [amdq[m] + s[1] * w[1][m] for m in range(3)]
+            ci = sound(*r)
+            s3 = r[1] / r[0] + ci
+            rho2, rhou2, en2 = r[0] - w[2][0], r[1] - w[2][1], r[2] - w[2][2]
+            s2 = rhou2 / rho2 + sound(rho2, rhou2, en2)
+            sf3 = None
+            if s2 < 0.0 and s3 > 0.0:
+                sf3, branch = (s2 * (s3 - s[2])) / (s3 - s2), branch + ",transonic-3"
+            elif s[2] < 0.0:
+                sf3, branch = s[2], branch + ",left-3"
+            if sf3 is not None:
+                amdq = [amdq[m] + sf3 * w[2][m] for m in range(3)]
+    apdq = []
+    for m in range(3):
+        df = 0.0
+        for mw in range(3):
+            df = df + s[mw] * w[mw][m]
+        apdq.append(df - amdq[m])
+    return amdq, apdq, branch
+
+
+def test_euler_entropy_fix_matches_the_written_formulas_bit_for_bit():
+    """The oracle's Euler solver with the Harten-Hyman entropy fix (the C2
+    headline's solver) against rp1eu.f:44-213 written out above: amdq and
+    apdq identical to the last bit at every interface of lines built to hit
+    the transonic 1- and 3-rarefactions as well as sub- and supersonic
+    interfaces."""
+    rng = np.random.default_rng(17)
+    n = 400
+    p = O.make_params(mx=n - 6, meqn=3, mwaves=3, dx=0.1, rp=O.RP_EULER, mthbc=(1, 1), efix=1)
+    rho = rng.uniform(0.3, 2.0, n)
+    pr = rng.uniform(0.3, 2.0, n)
+    c = np.sqrt(1.4 * pr / rho)
+    u = c * rng.uniform(-1.6, 1.6, n)            # Mach numbers across the sonic points
+    q = np.stack([rho, rho * u, pr / 0.4 + 0.5 * rho * u * u])
+    ql = q.copy()
+    qr = 0.75 * np.roll(q, 1, axis=1) + 0.25 * q   # moderate jumps: physical intermediate states
+    _, _, am, ap = O.rp(p, ql, qr)
+    branches = set()
+    for i in range(1, n):
+        left = tuple(float(v) for v in qr[:, i - 1])
+        right = tuple(float(v) for v in ql[:, i])
+        w, s = _euler_roe_written(left, right, p.gamma)
+        wam, wap, br = _euler_efix_written(left, right, w, s, p.gamma)
+        branches.add(br)
+        for m in range(3):
+            assert am[m, i] == wam[m], (i, m, br)
+            assert ap[m, i] == wap[m], (i, m, br)
+    assert any("transonic-1" in b for b in branches) and any("transonic-3" in b for b in branches)
+    assert "supersonic" in branches
