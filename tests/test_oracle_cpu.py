@@ -721,3 +721,31 @@ def test_euler_entropy_fix_matches_the_written_formulas_bit_for_bit():
             assert ap[m, i] == wap[m], (i, m, br)
     assert any("transonic-1" in b for b in branches) and any("transonic-3" in b for b in branches)
     assert "supersonic" in branches
+
+
+def test_ssp104_step_matches_the_written_integrator_bit_for_bit():
+    """The oracle's SSPRK(10,4) step (the C2 headline integrator) against
+    ts_ssp104 (src/sharpclaw.f90:380-464) written out with whole-array
+    numpy operations in the source's order around the oracle's own step()
+    (bc + flux1 -> dt*L(q)): identical to the last bit on a Shu-Osher line
+    with the entropy-fixed Roe solver and char-wise WENO5."""
+    po, _, q, aux = cases.shu_osher(mx=200)
+    po.char_decomp = 2
+    dt = 0.002
+    sixth = 1.0 / 6.0
+    qold = O.bc(po, q)
+    qq = qold.copy()
+    for _ in range(4):                                   # stages 1-4: q = q + 1/6 r1
+        qq, r1, _ = O.step(po, qq, aux, dt)
+        qq = qq + sixth * r1
+    qq, r1, _ = O.step(po, qq, aux, dt)                  # stage 5
+    r2 = qq + sixth * r1
+    r1 = 0.04 * qold + 0.36 * r2
+    qq = 0.6 * qold + 0.4 * r2
+    for _ in range(4):                                   # stages 6-9: q = q + 1/6 r2
+        qq, r2, _ = O.step(po, qq, aux, dt)
+        qq = qq + sixth * r2
+    qq, r2, _ = O.step(po, qq, aux, dt)                  # stage 10
+    qq = (r1 + 0.6 * qq) + 0.1 * r2
+    got, _ = O.rk_step(po, 4, qold, aux, dt)
+    assert np.array_equal(got[:, 3:-3], qq[:, 3:-3])
