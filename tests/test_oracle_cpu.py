@@ -749,3 +749,42 @@ def test_ssp104_step_matches_the_written_integrator_bit_for_bit():
     qq = (r1 + 0.6 * qq) + 0.1 * r2
     got, _ = O.rk_step(po, 4, qold, aux, dt)
     assert np.array_equal(got[:, 3:-3], qq[:, 3:-3])
+
+
+def test_flux1_matches_the_written_assembly_bit_for_bit():
+    """The oracle's flux1 for the C2 configuration (char-wise WENO5,
+    tfluct_solver = 0: the second Riemann solve inside each cell after the
+    in-place swap of src/flux1.f90:163-168) against src/flux1.f90:55-187
+    written out here around the oracle's own evec, weno5_char and rp: dq and
+    the CFL number identical to the last bit."""
+    import ctypes
+    po, _, q, aux = cases.shu_osher(mx=120)
+    po.char_decomp = 2
+    po.tfluct_solver = 0
+    dt = 0.003
+    qb = O.bc(po, q)
+    _, dq_oracle, cfl_oracle = O.step(po, qb, aux, dt)
+    meqn, mx2 = qb.shape
+    mx = mx2 - 6
+    dtdx = dt / po.dx
+    evl, evr = O.evec(po, qb)
+    ql = np.zeros_like(qb)
+    qr = np.zeros_like(qb)
+    dp = lambda a: np.ascontiguousarray(a).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    assert O.lib().ocl_weno5_char(mx2, meqn, dp(qb), dp(evl), dp(evr), dp(ql), dp(qr)) == 0
+    _, s, amdq, apdq = O.rp(po, ql, qr)
+    cfl = 0.0
+    for mw in range(s.shape[0]):
+        for i in range(1, mx + 2):                    # interfaces 1 .. mx+1 (array index i+2)
+            k = i + 2
+            cfl = max(cfl, dtdx * float(s[mw, k]), -dtdx * float(s[mw, k]))
+    ql2, qr2 = ql.copy(), qr.copy()
+    for k in range(1, mx2):                           # i = 1-mbc+1 .. mx+mbc, in order
+        qr2[:, k - 1] = ql2[:, k]
+        ql2[:, k] = qr2[:, k]
+    _, _, amdq2, apdq2 = O.rp(po, ql2, qr2)
+    dq = np.zeros_like(qb)
+    for k in range(3, mx + 3):                        # cells 1 .. mx
+        dq[:, k] = dq[:, k] - dtdx * (((amdq[:, k + 1] + apdq[:, k]) + amdq2[:, k]) + apdq2[:, k])
+    assert cfl == cfl_oracle
+    assert np.array_equal(dq[:, 3:-3], dq_oracle[:, 3:-3])
