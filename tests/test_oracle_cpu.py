@@ -788,3 +788,38 @@ def test_flux1_matches_the_written_assembly_bit_for_bit():
         dq[:, k] = dq[:, k] - dtdx * (((amdq[:, k + 1] + apdq[:, k]) + amdq2[:, k]) + apdq2[:, k])
     assert cfl == cfl_oracle
     assert np.array_equal(dq[:, 3:-3], dq_oracle[:, 3:-3])
+
+
+def test_flux2_matches_the_written_sweeps_bit_for_bit():
+    """The oracle's 2-D step (C3's shallow-water configuration: char-wise
+    WENO5, Roe rpn2 + tfluct) against src/2d/flux2.f90:28-92 written out
+    here around the oracle's own 1-D flux1: x sweeps over the rows
+    j = 0..ny+1, then y sweeps over the columns i = 0..nx+1 (the ghost lines
+    count in the CFL number), dq accumulated row sweep first: dq and the
+    CFL number identical to the last bit."""
+    import ctypes
+    po, _, q, aux = cases.radial_dam(n=20)
+    dt = 0.004
+    qb = O.bc(po, q)
+    _, dq_oracle, cfl_oracle = O.step(po, qb, aux, dt)
+    meqn, my2, mx2 = qb.shape
+    nx, ny = mx2 - 6, my2 - 6
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    dq = np.zeros_like(qb)
+    cfl = 0.0
+    for jj in range(2, ny + 4):                       # rows j = 0 .. ny+1
+        q1d = np.ascontiguousarray(qb[:, jj, :])
+        dq1d = np.zeros_like(q1d)
+        c1 = ctypes.c_double(0.0)
+        assert O.lib().ocl_flux1(ctypes.byref(po), dp(q1d), dp(dq1d), None, dt, ctypes.byref(c1), 1, nx) == 0
+        cfl = max(cfl, c1.value)
+        dq[:, jj, 3:nx + 3] = dq[:, jj, 3:nx + 3] + dq1d[:, 3:nx + 3]
+    for ii in range(2, nx + 4):                       # columns i = 0 .. nx+1
+        q1d = np.ascontiguousarray(qb[:, :, ii])
+        dq1d = np.zeros_like(q1d)
+        c1 = ctypes.c_double(0.0)
+        assert O.lib().ocl_flux1(ctypes.byref(po), dp(q1d), dp(dq1d), None, dt, ctypes.byref(c1), 2, ny) == 0
+        cfl = max(cfl, c1.value)
+        dq[:, 3:ny + 3, ii] = dq[:, 3:ny + 3, ii] + dq1d[:, 3:ny + 3]
+    assert cfl == cfl_oracle
+    assert np.array_equal(dq[:, 3:-3, 3:-3], dq_oracle[:, 3:-3, 3:-3])
