@@ -507,7 +507,7 @@ def test_weno5_matches_the_written_formulas_bit_for_bit(seed):
             assert qr[m, i - 1] == wr[i - 1], (m, i)
 
 
-def test_euler_roe_waves_match_the_written_formulas_bit_for_bit():
+def test_euler_roe_waves_matches_the_written_formulas_bit_for_bit():
     """The oracle's Euler Riemann solver (Roe averages, wave strengths,
     waves and speeds) against apps/euler/shockentropy/rp1eu.f:44-86 written
     out independently in Python floats, in the source's evaluation order
