@@ -94,6 +94,7 @@ def lib():
         _lib.ocl_sharpclaw.argtypes = [P, ctypes.POINTER(Run), dp, dp, ctypes.POINTER(Result)]
         _lib.ocl_rp.argtypes = [P, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp, dp, dp, dp]
         _lib.ocl_evec.argtypes = [P, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp]
+        _lib.ocl_tfluct.argtypes = [P, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp, dp]
         _lib.ocl_weno5_wave.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp]
         _lib.ocl_output.argtypes = [P, dp, dp, ctypes.c_double, ctypes.c_int, ctypes.c_char_p,
                                     ctypes.c_int]

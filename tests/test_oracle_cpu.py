@@ -889,3 +889,52 @@ def test_ssp33_step_matches_the_written_integrator_bit_for_bit():
     qq = (qold + 2.0 * (qq + r1)) / 3.0
     got, _ = O.rk_step(po, 3, qold, aux, dt)
     assert np.array_equal(got[:, 3:-3], qq[:, 3:-3])
+
+
+@pytest.mark.parametrize("ixy", [1, 2])
+def test_sw2d_tfluct_matches_the_written_formulas_bit_for_bit(ixy):
+    """The oracle's shallow-water total fluctuation inside each cell (C3's
+    tfluct_solver = 1) against apps/shallowWater/2dRadialDam/tfluct1sw.f:
+    78-140 written out here: the Roe solve from ql(i) to qr(i) of the same
+    cell, adq = amdq + apdq, identical to the last bit."""
+    import ctypes
+    import math
+    rng = np.random.default_rng(41 + ixy)
+    n = 30
+    p = O.make_params(ndim=2, mx=n - 6, my=n - 6, meqn=3, mwaves=3, dx=0.1, dy=0.1, rp=O.RP_SW2D,
+                      grav=1.0, mthbc=(1, 1, 1, 1))
+    hl = rng.uniform(0.5, 2.0, n)
+    ql = np.stack([hl, hl * rng.uniform(-1.5, 1.5, n), hl * rng.uniform(-1.5, 1.5, n)])
+    qr = ql * rng.uniform(0.8, 1.25, (3, n))
+    s = np.zeros((3, n))
+    adq = np.zeros((3, n))
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    assert O.lib().ocl_tfluct(ctypes.byref(p), ixy, n - 6, dp(ql), dp(qr), None, None, dp(s), dp(adq)) == 0
+    mu, mv = (1, 2) if ixy == 1 else (2, 1)
+    g = p.grav
+    for i in range(1, n):
+        l = [float(v) for v in ql[:, i]]
+        r = [float(v) for v in qr[:, i]]
+        hh = (l[0] + r[0]) * 0.5
+        hsqrtl, hsqrtr = math.sqrt(l[0]), math.sqrt(r[0])
+        hsq2 = hsqrtl + hsqrtr
+        u = (l[mu] / hsqrtl + r[mu] / hsqrtr) / hsq2
+        v = (l[mv] / hsqrtl + r[mv] / hsqrtr) / hsq2
+        a = math.sqrt(g * hh)
+        d1, d2, d3 = r[0] - l[0], r[mu] - l[mu], r[mv] - l[mv]
+        a1 = ((u + a) * d1 - d2) * (0.5 / a)
+        a2 = -v * d1 + d3
+        a3 = (-(u - a) * d1 + d2) * (0.5 / a)
+        w = [[0.0] * 3 for _ in range(3)]
+        w[0][0], w[0][mu], w[0][mv] = a1, a1 * (u - a), a1 * v
+        w[1][0], w[1][mu], w[1][mv] = 0.0, 0.0, a2
+        w[2][0], w[2][mu], w[2][mv] = a3, a3 * (u + a), a3 * v
+        sp = [u - a, u, u + a]
+        for m in range(3):
+            amdq, apdq = 0.0, 0.0
+            for mw in range(3):
+                if sp[mw] < 0.0:
+                    amdq = amdq + sp[mw] * w[mw][m]
+                else:
+                    apdq = apdq + sp[mw] * w[mw][m]
+            assert adq[m, i] == amdq + apdq, (i, m)
