@@ -938,3 +938,45 @@ def test_sw2d_tfluct_matches_the_written_formulas_bit_for_bit(ixy):
                 else:
                     apdq = apdq + sp[mw] * w[mw][m]
             assert adq[m, i] == amdq + apdq, (i, m)
+
+
+def test_acoustics_interface_solvers_match_the_written_formulas_bit_for_bit():
+    """The oracle's variable-coefficient acoustics Riemann solver and total
+    fluctuation (the reference's known-answer app) against
+    apps/acoustics/1d/interface/rp1acv.f:42-81 and tfluct1acv.f:42-81
+    written out here (impedance aux(:,1), sound speed aux(:,2); the total
+    fluctuation uses the cell's own coefficients on both sides): waves,
+    speeds, amdq, apdq and adq identical to the last bit."""
+    import ctypes
+    rng = np.random.default_rng(51)
+    n = 30
+    p = O.make_params(meqn=2, mwaves=2, maux=2, mx=n - 6, dx=0.1, rp=O.RP_ACOUSTICS1D, mthbc=(1, 1))
+    aux = np.stack([rng.uniform(0.5, 3.0, n), rng.uniform(0.5, 2.0, n)])
+    ql = rng.standard_normal((2, n))
+    qr = rng.standard_normal((2, n))
+    wave, s, am, ap = O.rp(p, ql, qr, aux, aux)
+    sf = np.zeros((2, n))
+    adq = np.zeros((2, n))
+    dp = lambda a: np.ascontiguousarray(a).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    assert O.lib().ocl_tfluct(ctypes.byref(p), 1, n - 6, dp(ql), dp(qr), dp(aux), dp(aux), dp(sf), dp(adq)) == 0
+    for i in range(1, n):
+        # rp1acv: interface i, left qr(i-1) with auxr(i-1), right ql(i) with auxl(i)
+        d1, d2 = float(ql[0, i]) - float(qr[0, i - 1]), float(ql[1, i]) - float(qr[1, i - 1])
+        zi, zim = float(aux[0, i]), float(aux[0, i - 1])
+        a1 = (-d1 + zi * d2) / (zim + zi)
+        a2 = (d1 + zim * d2) / (zim + zi)
+        w = [[-a1 * zim, a1], [a2 * zi, a2]]
+        sp = [-float(aux[1, i - 1]), float(aux[1, i])]
+        for m in range(2):
+            assert wave[0, m, i] == w[0][m] and wave[1, m, i] == w[1][m], (i, m)
+            assert am[m, i] == sp[0] * w[0][m] and ap[m, i] == sp[1] * w[1][m], (i, m)
+        assert s[0, i] == sp[0] and s[1, i] == sp[1], i
+        # tfluct1acv: inside cell i, from ql(i) to qr(i), both sides with aux(i)
+        d1, d2 = float(qr[0, i]) - float(ql[0, i]), float(qr[1, i]) - float(ql[1, i])
+        zi = zim = float(aux[0, i])
+        a1 = (-d1 + zi * d2) / (zim + zi)
+        a2 = (d1 + zim * d2) / (zim + zi)
+        w = [[-a1 * zim, a1], [a2 * zi, a2]]
+        sp = [-float(aux[1, i]), float(aux[1, i])]
+        for m in range(2):
+            assert adq[m, i] == sp[0] * w[0][m] + sp[1] * w[1][m], (i, m)
