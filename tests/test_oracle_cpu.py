@@ -940,7 +940,7 @@ def test_sw2d_tfluct_matches_the_written_formulas_bit_for_bit(ixy):
             assert adq[m, i] == amdq + apdq, (i, m)
 
 
-def test_acoustics_interface_solvers_match_the_written_formulas_bit_for_bit():
+def test_acoustics_interface_solvers_matches_the_written_formulas_bit_for_bit():
     """The oracle's variable-coefficient acoustics Riemann solver and total
     fluctuation (the reference's known-answer app) against
     apps/acoustics/1d/interface/rp1acv.f:42-81 and tfluct1acv.f:42-81
