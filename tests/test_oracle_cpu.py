@@ -980,3 +980,41 @@ def test_acoustics_interface_solvers_matches_the_written_formulas_bit_for_bit():
         sp = [-float(aux[1, i]), float(aux[1, i])]
         for m in range(2):
             assert adq[m, i] == sp[0] * w[0][m] + sp[1] * w[1][m], (i, m)
+
+
+@pytest.mark.parametrize("mthbc", [(1, 1), (2, 2), (3, 3), (1, 3), (3, 1)])
+def test_bc1_matches_the_written_formulas(mthbc):
+    """The oracle's 1-D ghost fill against src/1d/bc1.f90:40-109 written out
+    here: extrapolation copies the end cell, periodic wraps, a wall mirrors
+    with the second component negated; interior untouched."""
+    rng = np.random.default_rng(61)
+    mx, mbc = 9, 3
+    p = O.make_params(meqn=2, mwaves=2, mx=mx, dx=0.1, rp=O.RP_ACOUSTICS_CONST, rho=1.0, bulk=1.0,
+                      mthbc=mthbc)
+    q = rng.standard_normal((2, mx + 2 * mbc))
+    got = O.bc(p, q)
+    want = q.copy()
+    Q = lambda i: i + mbc - 1                 # Fortran cell index -> array index
+    for m in range(2):
+        for ibc in range(1, mbc + 1):
+            if mthbc[0] == 1:
+                want[m, Q(1 - ibc)] = want[m, Q(1)]
+            elif mthbc[0] == 2:
+                want[m, Q(1 - ibc)] = want[m, Q(mx + 1 - ibc)]
+            else:
+                want[m, Q(1 - ibc)] = want[m, Q(ibc)]
+    if mthbc[0] == 3:
+        for ibc in range(1, mbc + 1):
+            want[1, Q(1 - ibc)] = -want[1, Q(ibc)]
+    for m in range(2):
+        for ibc in range(1, mbc + 1):
+            if mthbc[1] == 1:
+                want[m, Q(mx + ibc)] = want[m, Q(mx)]
+            elif mthbc[1] == 2:
+                want[m, Q(mx + ibc)] = want[m, Q(ibc)]
+            else:
+                want[m, Q(mx + ibc)] = want[m, Q(mx + 1 - ibc)]
+    if mthbc[1] == 3:
+        for ibc in range(1, mbc + 1):
+            want[1, Q(mx + ibc)] = -want[1, Q(mx + 1 - ibc)]
+    assert np.array_equal(got, want)
