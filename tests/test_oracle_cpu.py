@@ -1018,3 +1018,49 @@ def test_bc1_matches_the_written_formulas(mthbc):
         for ibc in range(1, mbc + 1):
             want[1, Q(mx + ibc)] = -want[1, Q(mx + 1 - ibc)]
     assert np.array_equal(got, want)
+
+
+def _fill_side(a, axis, side, kind, n, mbc, neg_comp):
+    """One side of bc1/bc2 along `axis` of a (meqn, ..., n+2mbc) slab: the
+    written rules of src/2d/bc2.f90 (extrapolation, periodic, wall with
+    component neg_comp negated), over every line of the other axis."""
+    def sl(k):
+        idx = [slice(None)] * a.ndim
+        idx[axis] = k
+        return tuple(idx)
+    Q = lambda i: i + mbc - 1
+    for ibc in range(1, mbc + 1):
+        g = Q(1 - ibc) if side == 0 else Q(n + ibc)
+        if kind == 1:
+            src = Q(1) if side == 0 else Q(n)
+        elif kind == 2:
+            src = Q(n + 1 - ibc) if side == 0 else Q(ibc)
+        else:
+            src = Q(ibc) if side == 0 else Q(n + 1 - ibc)
+        a[sl(g)] = a[sl(src)]
+        if kind == 3:
+            gi = list(sl(g))
+            si = list(sl(src))
+            gi[0] = si[0] = neg_comp
+            a[tuple(gi)] = -a[tuple(si)]
+
+
+@pytest.mark.parametrize("mthbc", [(1, 1, 1, 1), (2, 2, 2, 2), (3, 3, 3, 3), (1, 3, 3, 1), (3, 3, 2, 2)])
+def test_bc2_matches_the_written_formulas(mthbc):
+    """The oracle's 2-D ghost fill against src/2d/bc2.f90 written out here:
+    the x sides first over every row (ghost rows included), then the y sides
+    over every column (ghost columns included), so the corners carry the
+    y rule applied to the x-filled columns; momentum component 2 negated at
+    x walls, 3 at y walls."""
+    rng = np.random.default_rng(71)
+    nx, ny, mbc = 7, 6, 3
+    p = O.make_params(ndim=2, meqn=3, mwaves=3, mx=nx, my=ny, dx=0.1, dy=0.1, rp=O.RP_SW2D,
+                      mthbc=mthbc)
+    q = rng.standard_normal((3, ny + 2 * mbc, nx + 2 * mbc))
+    got = O.bc(p, q)
+    want = q.copy()
+    _fill_side(want, 2, 0, mthbc[0], nx, mbc, 1)
+    _fill_side(want, 2, 1, mthbc[1], nx, mbc, 1)
+    _fill_side(want, 1, 0, mthbc[2], ny, mbc, 2)
+    _fill_side(want, 1, 1, mthbc[3], ny, mbc, 2)
+    assert np.array_equal(got, want)
